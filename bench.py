@@ -1,0 +1,366 @@
+#!/usr/bin/env python
+"""Benchmark: exact-result range queries/s on the batched configuration, one B200 per rank.
+
+Workload (default --config batched): RandomKmeans-style index N=10,000,000, D=8, height 4, ratios
+100,50,20, sigma divisor 3.0, seed 1 (generated in memory, byte-identical to the reference's
+--gen-index); 4096 range boxes centred on uniformly chosen data points with per-dimension
+half-widths log-uniform in [0.1%, 10%] of the extent. A step is one batched exact traversal of all
+4096 boxes (all levels, the exact final filter and the per-query result offsets).
+
+Reported on one JSON line (rank 0):
+  value           whole-job exact queries/s with the boxes resident in HBM (device events)
+  e2e             the same through the public host-buffer API (boxes H2D from pinned memory,
+                  offsets + ids D2H, every step inside the timed region)
+  plain           one query at a time through the same engine (the >=5x denominator)
+  roofline        the finest-level expand kernel: algorithmic bytes / its event-timed duration
+  cpu_baseline    the CPU port of the traversal (oracle) on all host cores, bounded sample
+Multi-GPU: replicas only (the path needs no exchange); every rank runs its own batches and the
+time is the max over ranks.
+"""
+import argparse
+import importlib.util
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+REPO = os.path.dirname(os.path.abspath(__file__))
+
+
+def _package():
+    pkg_dir = os.path.join(REPO, "t-blaeq_b200")
+    spec = importlib.util.spec_from_file_location("tblaeq_b200", os.path.join(pkg_dir, "__init__.py"),
+                                                  submodule_search_locations=[pkg_dir])
+    mod = importlib.util.module_from_spec(spec)
+    sys.modules["tblaeq_b200"] = mod
+    spec.loader.exec_module(mod)
+    return mod
+
+
+def _peaks():
+    p = os.path.join(REPO, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clock / throttle sampling during the timed region."""
+
+    def __init__(self, gpu: int):
+        self.gpu = gpu
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={q}", "--format=csv,noheader,nounits",
+                                          "-i", str(self.gpu), "-lms", "200"], stdout=subprocess.PIPE,
+                                         stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def oracle_index_from_handler(oracle, h):
+    info = h.info()
+    L = info["intervals"]
+    D = info["D"]
+    col_res = [h.host_array(1, l) for l in range(L)]
+    pvals = [h.host_array(0, l).reshape(-1, D) for l in range(L)]
+    radius = [h.host_array(2, l) for l in range(L)]
+    maps = [None] + [h.host_array(3, m) for m in range(1, info["height"])]
+    cids = h.host_array(4)
+    cvals = h.host_array(5).reshape(-1, D)
+    return oracle.OracleIndex(D, info["N"], info["height"], info["ratios"], info["meshSizes"], col_res,
+                              [np.diff(c) for c in col_res], [np.arange(len(p), dtype=np.uint64) for p in pvals],
+                              pvals, radius, maps, cids, cvals)
+
+
+def cpu_port_qps(oracle, oidx, sub, Q, budget_s=20.0, min_q=32):
+    """Time the CPU port of the exact traversal on all host cores over a bounded sample."""
+    threads = os.cpu_count() or 1
+    n = min_q
+    done, elapsed = 0, 0.0
+    while elapsed < budget_s and done < len(Q):
+        batch = Q[done:done + n]
+        t0 = time.perf_counter()
+        oracle.exact_query(oidx, oracle.RANGE, batch, sub=sub, threads=threads)
+        dt = time.perf_counter() - t0
+        done += len(batch)
+        elapsed += dt
+        n = min(len(Q) - done, max(n, int(len(batch) * max(1.0, (budget_s - elapsed) / max(dt, 1e-6) / 2))))
+        if n <= 0:
+            break
+    return done / elapsed, threads, done
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--config", choices=["batched", "small"], default="batched")
+    ap.add_argument("--nq", type=int, default=4096)
+    ap.add_argument("--plain-queries", type=int, default=512)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-graph", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+
+    tb = _package()
+    wl = sys.modules.get("tblaeq_b200.workloads") or __import__("tblaeq_b200.workloads").workloads
+    cfg_name = args.config
+    cfg = wl.CONFIGS[cfg_name]
+    if cfg_name == "small":
+        boxes_kw = dict(half_width=0.05)
+    else:
+        boxes_kw = dict(log_uniform=(0.001, 0.1))
+    config = {"workload": f"{cfg_name} range: RandomKmeans N={cfg['N']} D={cfg['D']} ratios "
+                          f"{','.join(map(str, cfg['ratios']))} seed {cfg['seed']} sigma/{cfg['sigma_divisor']}; "
+                          f"{args.nq} boxes, half-widths "
+                          + ("log-uniform [0.1%,10%]" if cfg_name != "small" else "5%") + " of extent",
+              "index_points": cfg["N"], "dim": cfg["D"], "queries_per_step": args.nq, "mode": "exact",
+              "l2": "flushed between timed steps (256 MiB write)", "parallelism": f"replicas{world}"}
+
+    if args.impl == "reference":
+        return run_reference(args, tb, wl, cfg_name, config, rank, world)
+
+    import torch
+    import torch.distributed as dist
+    from datetime import timedelta
+
+    torch.cuda.set_device(local)
+    tb.set_device(local)
+    if world > 1:
+        dist.init_process_group("nccl", timeout=timedelta(seconds=600), device_id=torch.device("cuda", local))
+
+    h = wl.generate_index(tb.QueryHandler, cfg_name)
+    h.prepare_for_query(tb.LevelPolicy.L0)
+    Q = wl.range_boxes(h, args.nq, seed=42, **boxes_kw)
+    dQ = torch.from_numpy(Q).cuda()
+    D = cfg["D"]
+    flags = 0 if args.no_graph else tb.USE_GRAPH
+
+    # Warm-up: the first synchronous batch sizes every workspace, the rest replay the graph.
+    h.query_batch(tb.QueryType.RANGE, dQ, tb.Mode.EXACT)
+    h.set_timing(True)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+    for _ in range(args.warmup):
+        h.query_batch_async(tb.QueryType.RANGE, dQ, tb.Mode.EXACT, flags=flags)
+        h.batch_wait()
+
+    entries, items, results = h.level_counts()
+    step_ms, final_ms = [], []
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(local) as clk:
+        for _ in range(args.steps):
+            flush.zero_()
+            torch.cuda.synchronize()
+            h.query_batch_async(tb.QueryType.RANGE, dQ, tb.Mode.EXACT, flags=flags)
+            h.batch_wait()
+            st = h.stage_times()
+            step_ms.append(sum(st))
+            final_ms.append(st[-2])
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    total_ms = sum(step_ms)
+    if world > 1:
+        t = torch.tensor([total_ms], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total_ms = float(t.item())
+    value = args.nq * args.steps * world / (total_ms / 1e3)
+
+    # Roofline of the finest-level expand (dominant kernel): algorithmic bytes per launch.
+    H = len(entries)
+    ent_in, kids = entries[H - 1], items[H - 1]
+    alg_bytes = ent_in * (12 + 8 * D) + kids * 8 * D + results * 16
+    final_mean_s = statistics.mean(final_ms) / 1e3
+    peak, peak_kind = _peaks()
+    achieved = alg_bytes / final_mean_s / 1e9
+
+    # Plain: one query at a time through the same engine (no batching, no graph).
+    plain_lat = []
+    n_plain = min(args.plain_queries, args.nq)
+    for i in range(8):
+        h.query_batch(tb.QueryType.RANGE, dQ[i:i + 1], tb.Mode.EXACT)
+    torch.cuda.synchronize()
+    for i in range(n_plain):
+        t0 = time.perf_counter()
+        h.query_batch(tb.QueryType.RANGE, dQ[i:i + 1], tb.Mode.EXACT)
+        plain_lat.append(time.perf_counter() - t0)
+    plain_qps = n_plain / sum(plain_lat)
+
+    # End to end through the public host API with pinned host buffers.
+    hostQ = torch.from_numpy(Q).pin_memory()
+    cap = max(1024, int(results * 1.5) + 1024)
+    offs_h = torch.empty(args.nq + 1, dtype=torch.int64).pin_memory()
+    ids_h = torch.empty(cap, dtype=torch.int64).pin_memory()
+    import ctypes
+    lib = tb.lib()
+    b = tb._Batch(int(tb.QueryType.RANGE), int(tb.Mode.EXACT), args.nq, hostQ.data_ptr(), 0, 0, 0)
+    tot = ctypes.c_uint64()
+    P64 = ctypes.POINTER(ctypes.c_uint64)
+    def e2e_call():
+        code = lib.tblaeq_query_batch_host(h._h, ctypes.byref(b), ctypes.cast(offs_h.data_ptr(), P64),
+                                           ctypes.cast(ids_h.data_ptr(), P64), cap, None, ctypes.byref(tot))
+        if code:
+            raise tb.TblaeqError(code, lib.tblaeq_last_error().decode())
+    for _ in range(args.warmup):
+        e2e_call()
+    e2e_t = []
+    for _ in range(args.steps):
+        flush.zero_()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        e2e_call()
+        e2e_t.append(time.perf_counter() - t0)
+    e2e_max = max(e2e_t) if world == 1 else None
+    e2e_total = sum(e2e_t)
+    if world > 1:
+        t = torch.tensor([e2e_total], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_total = float(t.item())
+    e2e_value = args.nq * args.steps * world / e2e_total
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        sys.path.insert(0, REPO)
+        import oracle
+        oidx = oracle_index_from_handler(oracle, h)
+        sub = oracle.subtree(oidx)
+        qps, cores, sampled = cpu_port_qps(oracle, oidx, sub, Q)
+        cpu = {"value": qps, "unit": "queries/s", "cores": cores, "kind": "port",
+               "sample": f"first {sampled} of the {args.nq} boxes, exact traversal port (subtree radii + "
+                         f"final filter), OpenMP over queries"}
+
+    if world > 1:
+        dist.destroy_process_group()
+    if rank != 0:
+        return
+    lat_ms = sorted(step_ms)
+    pl = sorted(x * 1e3 for x in plain_lat)
+    out = {
+        "metric": "exact-result range queries/s (batched, 1 B200 per rank)",
+        "value": value,
+        "unit": "queries/s",
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": total_ms / args.steps,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f64",
+        "data": "synthetic (seeded RandomKmeans-style index and boxes)",
+        "config": config,
+        "e2e": {"value": e2e_value, "unit": "queries/s", "h2d_bytes_per_step": args.nq * 2 * D * 8,
+                "d2h_bytes_per_step": (args.nq + 1) * 8 + int(tot.value) * 8},
+        "gpu_launches": args.steps * (H + 2),
+        "latency_ms": {"batch_p50": lat_ms[len(lat_ms) // 2], "batch_p99": lat_ms[min(len(lat_ms) - 1,
+                                                                                     int(len(lat_ms) * 0.99))],
+                       "plain_query_p50": pl[len(pl) // 2], "plain_query_p99": pl[min(len(pl) - 1,
+                                                                                       int(len(pl) * 0.99))]},
+        "plain": {"value": plain_qps, "unit": "queries/s", "queries": n_plain,
+                  "speedup_batched_vs_plain": value / world / plain_qps},
+        "results_per_step": results,
+        "level_entries": entries,
+        "level_children": items,
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                     "traffic": None, "kernel": "expandKernel<8, RangeBox, result> (finest level)",
+                     "peak_kind": f"{peak_kind} hbm_gbs", "algorithmic_bytes_per_launch": alg_bytes,
+                     "launch_ms": final_mean_s * 1e3},
+        "clocks": clk.summary(),
+        "cpu_baseline": cpu,
+    }
+    print(json.dumps(out))
+
+
+def run_reference(args, tb, wl, cfg_name, config, rank, world):
+    """Reference arm: the CPU restatement of the reference traversal (exact semantics) timed on the
+    host cores. The reference has no CPU implementation of its query path (every strategy launches
+    CUDA kernels), so the oracle port stands in for it."""
+    if rank != 0:
+        return
+    sys.path.insert(0, REPO)
+    import oracle
+    h = wl.generate_index(tb.QueryHandler, cfg_name)
+    boxes_kw = dict(half_width=0.05) if cfg_name == "small" else dict(log_uniform=(0.001, 0.1))
+    Q = wl.range_boxes(h, args.nq, seed=42, **boxes_kw)
+    oidx = oracle_index_from_handler(oracle, h)
+    sub = oracle.subtree(oidx)
+    threads = os.cpu_count() or 1
+    per_step = max(8, min(args.nq, 64))
+    for i in range(args.warmup):
+        oracle.exact_query(oidx, oracle.RANGE, Q[:per_step], sub=sub, threads=threads)
+    t = 0.0
+    done = 0
+    for s in range(args.steps):
+        sl = Q[(s * per_step) % args.nq:(s * per_step) % args.nq + per_step]
+        t0 = time.perf_counter()
+        oracle.exact_query(oidx, oracle.RANGE, sl, sub=sub, threads=threads)
+        t += time.perf_counter() - t0
+        done += len(sl)
+    v = done / t
+    out = {"metric": "exact-result range queries/s (batched, 1 B200 per rank)", "value": v, "unit": "queries/s",
+           "impl": "reference", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+           "ms_per_step": t / args.steps * 1e3, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+           "dtype": "f64", "data": "synthetic (seeded RandomKmeans-style index and boxes)", "config": config,
+           "cpu_baseline": {"value": v, "unit": "queries/s", "cores": threads, "kind": "port",
+                            "sample": f"{per_step} boxes per step of the {args.nq}-box workload, exact traversal "
+                                      f"port, OpenMP over queries"},
+           "e2e": {"value": v, "unit": "queries/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(out))
+
+
+if __name__ == "__main__":
+    main()

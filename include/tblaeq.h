@@ -1,0 +1,202 @@
+/* T-BLAEQ on B200: C ABI of the query hot path.
+ *
+ * Plain C types only (no torch or C++ types). Every entry point returns a tblaeq_status; on a
+ * non-zero status tblaeq_last_error() returns a thread-local description. Device pointers are
+ * marked "device"; everything else is host memory.
+ *
+ * Each declaration names the reference interface it replaces (paths inside Mgepahmge/T-BLAEQ).
+ * Threading: a handle serves one thread at a time (the reference is not thread-safe either,
+ * src/HTTPServer.cu:445,498,525); use one handle per serving thread.
+ */
+#ifndef TBLAEQ_H
+#define TBLAEQ_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define TBLAEQ_ABI_VERSION 1
+
+typedef struct tblaeq_handle tblaeq_handle; /* QueryHandler: host index + device state */
+
+enum tblaeq_status {
+    TBLAEQ_OK = 0,
+    TBLAEQ_ERR_INVALID = 1,   /* bad argument (reference: std::invalid_argument) */
+    TBLAEQ_ERR_IO = 2,        /* index file missing / truncated (reference: std::runtime_error) */
+    TBLAEQ_ERR_CUDA = 3,      /* CUDA runtime error (reference: CUDA_CHECK -> exit, src/Query/check.cuh:15-25) */
+    TBLAEQ_ERR_OOM = 4,       /* device allocation failed */
+    TBLAEQ_ERR_OVERFLOW = 5,  /* batch exceeds the 32-bit traversal capacities; split it */
+    TBLAEQ_ERR_TIMEOUT = 6,   /* a kernel's bounded wait gave up (reported status, context intact) */
+    TBLAEQ_ERR_STATE = 7,     /* call order violated (e.g. query before prepare) */
+    TBLAEQ_ERR_TYPE = 8       /* query type mismatch (reference: QueryResult.errorCode = 1) */
+};
+
+/* QueryType of src/Data_Structures/File.cuh:39-43 (same enumerator values). */
+enum tblaeq_qtype { TBLAEQ_POINT = 0, TBLAEQ_RANGE = 1 };
+/* LevelPolicy of src/core/MemoryPolicy.cuh:51. */
+enum tblaeq_policy { TBLAEQ_L0 = 0, TBLAEQ_L1 = 1, TBLAEQ_L2 = 2, TBLAEQ_L3 = 3 };
+/* Result semantics: the reference's candidate sets, or exact answers. */
+enum tblaeq_mode { TBLAEQ_MODE_REF_PARITY = 0, TBLAEQ_MODE_EXACT = 1 };
+/* Batch flags. */
+enum tblaeq_batch_flags { TBLAEQ_WANT_VALS = 1, TBLAEQ_WANT_LEVELS = 2, TBLAEQ_USE_GRAPH = 4 };
+
+typedef struct {
+    uint64_t N, D;
+    double valMin, valMax;
+    int isInt;
+    uint64_t height;
+    const uint64_t* ratios; /* nRatios entries, finest first; nRatios must equal height-1 */
+    uint64_t nRatios;
+    uint64_t seed;
+    double sigmaDivisor;
+} tblaeq_gen_params;
+
+#define TBLAEQ_MAX_HEIGHT 16
+typedef struct {
+    uint64_t D, N, height, intervals;
+    uint64_t meshSizes[TBLAEQ_MAX_HEIGHT]; /* finest -> coarsest, like metadata.bin */
+    uint64_t ratios[TBLAEQ_MAX_HEIGHT];
+    uint64_t hostBytes, deviceBytes;       /* MemoryStats totals (src/core/IndexData.cu:141-194) */
+    int prepared;
+    int policy[TBLAEQ_MAX_HEIGHT];         /* active LevelPolicy per interval once prepared */
+} tblaeq_index_info;
+
+/* A grid of one query at one level: ids (original mesh ids) and AOS coordinates.
+ * Mirrors SparseGrid (src/Data_Structures/Data_Structures.cuh:134-229); both pointers device. */
+typedef struct {
+    uint64_t numRows, dim, nnz;
+    const uint64_t* ids;
+    const double* vals;
+} tblaeq_grid;
+
+typedef struct {
+    int qtype;              /* tblaeq_qtype */
+    int mode;               /* tblaeq_mode */
+    uint64_t nq;
+    const double* queries;  /* RANGE: nq rows lo[D] hi[D]; POINT: nq rows point[D] */
+    int queriesOnDevice;    /* 1: `queries` is a device pointer */
+    uint64_t K;             /* KNN: neighbours per query */
+    unsigned flags;         /* tblaeq_batch_flags */
+} tblaeq_batch;
+
+typedef struct {
+    uint64_t nq, total;
+    const uint64_t* offsets;    /* device, nq+1: results of query i are [offsets[i], offsets[i+1]) */
+    const uint64_t* ids;        /* device, total: original dataset ids */
+    const double* vals;         /* device, total*D (TBLAEQ_WANT_VALS) or NULL */
+    const double* dist2;        /* device, total (KNN) or NULL */
+    const uint32_t* levelItems; /* device, intervals*nq: reference levelFineMeshSize per level (WANT_LEVELS) */
+} tblaeq_batch_result;
+
+const char* tblaeq_last_error(void);
+int tblaeq_abi_version(void);
+
+/* QueryHandler(indexPath, true) -> IndexSerializer::load (src/core/QueryHandler.cu:126-137,
+ * src/core/IndexSerializer.cu:34-67). Reads the reference's on-disk layout byte for byte. */
+int tblaeq_open(const char* index_dir, tblaeq_handle** out);
+
+/* QueryHandler(N, D, valMin, valMax, isInt, height, ratios, seed, sigmaDivisor)
+ * (src/core/QueryHandler.cu:101-124 -> IndexBuilder::buildRandom, src/core/IndexBuilder.cu:153-234).
+ * Produces the same index files, byte for byte, as the reference's --gen-index. */
+int tblaeq_generate(const tblaeq_gen_params* params, tblaeq_handle** out);
+
+/* QueryHandler::saveIndex (src/core/QueryHandler.cu:139-145). */
+int tblaeq_save(const tblaeq_handle* h, const char* dir);
+
+/* ~QueryHandler. Frees host and device state. NULL is accepted. */
+void tblaeq_close(tblaeq_handle* h);
+
+/* getSize / getDim / getMemoryStats / getActivePolicy (src/core/QueryHandler.cuh:160-240). */
+int tblaeq_info(const tblaeq_handle* h, tblaeq_index_info* out);
+
+/* PolicyScheduler::recommend (src/core/MemoryPolicy.cu:100-177). free_bytes = 0 queries the
+ * device (cudaMemGetInfo); otherwise the given budget is used (fake budgets for tests).
+ * Writes `intervals` LevelPolicy values to policy_out. */
+int tblaeq_recommend(const tblaeq_handle* h, uint64_t free_bytes, int* policy_out);
+
+/* prepareForQuery() / prepareForQuery(IndexPolicy) (src/core/QueryHandler.cu:160-182).
+ * policy = NULL selects the recommendation; otherwise n_levels must equal intervals.
+ * Uploads the index, derives the per-node arrays and allocates all query workspaces. */
+int tblaeq_prepare(tblaeq_handle* h, const int* policy, uint64_t n_levels);
+
+/* IQueryStrategy::runLevel (src/core/strategies/IQueryStrategy.cuh:104-105), B200 strategy:
+ * prune `in` at interval l with the reference predicate (range: RangePruning.cu:5-25 with the
+ * level's max radius; KNN: KNN.cu:9-24 bound + STEP, L0Strategy.cu:133-154), compact the survivors
+ * in order, expand them through P_l (SpMSpV.cuh:47-67) and remap ids with Map_{l+1}
+ * (Refactor.cu:10-16). lo/hi/q are host arrays of D values. `out` points at device buffers owned
+ * by the handle (the reference's L0 ownsIds = ownsVals = false): valid until the next call for
+ * the same level. */
+int tblaeq_level(tblaeq_handle* h, uint64_t l, const tblaeq_grid* in, int qtype, const double* lo,
+                 const double* hi, const double* q, uint64_t K, tblaeq_grid* out);
+
+/* The coarsest mesh as a device grid (QueryEngine::runSingleQuery's coarsestView,
+ * src/core/QueryEngine.cu:66-70). */
+int tblaeq_coarsest_grid(tblaeq_handle* h, tblaeq_grid* out);
+
+/* Batched traversal of many queries in one pass over the hierarchy (replaces the one-query loop
+ * of QueryEngine::run, src/core/QueryEngine.cu:109-252). Result pointers are device memory owned
+ * by the handle, valid until the next batch call. */
+int tblaeq_query_batch(tblaeq_handle* h, const tblaeq_batch* batch, tblaeq_batch_result* out);
+
+/* Same as tblaeq_query_batch with host buffers on both sides: queries are copied to the device,
+ * and offsets (nq+1), ids (up to ids_cap) and, for KNN, dist2 are copied back. *total receives
+ * the number of results; if it exceeds ids_cap nothing past ids_cap is written and
+ * TBLAEQ_ERR_OVERFLOW is returned. */
+int tblaeq_query_batch_host(tblaeq_handle* h, const tblaeq_batch* batch, uint64_t* offsets_out, uint64_t* ids_out,
+                            uint64_t ids_cap, double* dist2_out, uint64_t* total);
+
+/* Enqueue a batch on the handle's stream and return without waiting (no host synchronisation, so
+ * it can be timed with events or overlapped). `queries` must be device memory that stays valid
+ * until tblaeq_batch_wait returns, and a synchronous tblaeq_query_batch with the same nq, mode and
+ * flags must have run first (it sizes the workspaces). With TBLAEQ_USE_GRAPH the launches are
+ * captured once into a CUDA graph and replayed. */
+int tblaeq_query_batch_async(tblaeq_handle* h, const tblaeq_batch* batch);
+
+/* Wait for the last enqueued batch, check its device status (workspace overflow ->
+ * TBLAEQ_ERR_OVERFLOW: rerun it with tblaeq_query_batch) and describe its results. */
+int tblaeq_batch_wait(tblaeq_handle* h, tblaeq_batch_result* out);
+
+/* Frontier entries and work items (children) per level of the last batch: entries[0], items[0]
+ * describe the root frontier (one entry per query), entries[m+1], items[m+1] the survivors of
+ * mesh m and their children; results[0] = number of results. Returns the number of levels written. */
+int tblaeq_level_counts(tblaeq_handle* h, uint64_t* entries, uint64_t* items, int cap, uint64_t* results);
+
+/* Select the CUDA device used by this library on the calling thread (cudaSetDevice); call before
+ * tblaeq_prepare. */
+int tblaeq_set_device(int device);
+
+/* The CUDA stream (cudaStream_t) every launch of this handle goes to. */
+void* tblaeq_stream(tblaeq_handle* h);
+
+/* Record CUDA events between the launch stages of every batch (1 = on). */
+int tblaeq_set_timing(tblaeq_handle* h, int on);
+
+/* Elapsed milliseconds per stage of the last batch: [0] workspace reset + root frontier,
+ * [1..height] one per mesh expand (the last one is the finest level), [height+1] result offsets.
+ * Returns the number of stages written (at most cap), or -1 when timing is off. */
+int tblaeq_stage_times(tblaeq_handle* h, float* ms, int cap);
+
+/* Host copies of the index arrays (read-only, owned by the handle), for tools and tests:
+ * which = 0: P-tensor values of interval l (rows*D doubles), 1: colRes of interval l (cols+1),
+ * 2: max radius of interval l (cols), 3: Map of mesh l (meshSizes), 4: coarsest ids, 5: coarsest vals. */
+int tblaeq_host_array(const tblaeq_handle* h, int which, uint64_t l, const void** ptr, uint64_t* count);
+
+/* Decoded coordinates (the reference's rebuilt values, P products down the hierarchy) of the
+ * finest points at the given sorted positions, with their original dataset ids. Host only; used
+ * to draw query workloads centred on data points. */
+int tblaeq_decode_points(tblaeq_handle* h, const uint64_t* positions, uint64_t n, double* coords_out,
+                         uint64_t* ids_out);
+
+/* Number of device bytes currently allocated by the library (leak checks). */
+uint64_t tblaeq_live_device_bytes(void);
+
+/* Test hook: make the n-th device allocation from now on fail (n = 0 disables). */
+void tblaeq_debug_fail_alloc_after(uint64_t n);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* TBLAEQ_H */

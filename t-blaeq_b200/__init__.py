@@ -1,0 +1,520 @@
+"""T-BLAEQ on B200: Python facade over the C ABI (include/tblaeq.h, libtblaeq_b200.so).
+
+The names and argument meanings follow the reference's C++ facade
+(src/core/QueryHandler.cuh:50-247): ``QueryHandler`` builds or loads an index,
+``prepare_for_query`` uploads it under a per-level memory policy, and queries run
+through ``perform_single_range_query(upper, lower)`` (upper bound first, as in the
+reference), ``perform_single_knn_query``, ``perform_query`` (reference query-file
+format) or the batched ``query_batch`` of the B200 engine.
+
+Every query runs in the CUDA library; there is no CPU path. Importing this module
+on a machine without the built library raises ImportError, and calls that need a
+GPU fail loudly with ``TblaeqError`` when no device is present.
+"""
+from __future__ import annotations
+
+import ctypes
+import enum
+import os
+import time
+from dataclasses import dataclass, field
+from typing import Optional, Sequence
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libtblaeq_b200.so")
+HEADER_PATH = os.path.join(os.path.dirname(_HERE), "include", "tblaeq.h")
+
+
+class QueryType(enum.IntEnum):
+    POINT = 0  # KNN
+    RANGE = 1
+
+
+class LevelPolicy(enum.IntEnum):
+    L0 = 0
+    L1 = 1
+    L2 = 2
+    L3 = 3
+
+
+class Mode(enum.IntEnum):
+    REF_PARITY = 0  # the reference's candidate sets
+    EXACT = 1       # exact answers (subtree radii + exact final filter / top-K)
+
+
+WANT_VALS = 1
+WANT_LEVELS = 2
+USE_GRAPH = 4
+
+ERR_NAMES = {0: "OK", 1: "INVALID", 2: "IO", 3: "CUDA", 4: "OOM", 5: "OVERFLOW", 6: "TIMEOUT", 7: "STATE",
+             8: "TYPE"}
+
+
+class TblaeqError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"[{ERR_NAMES.get(code, code)}] {msg}")
+        self.code = code
+
+
+class _GenParams(ctypes.Structure):
+    _fields_ = [("N", ctypes.c_uint64), ("D", ctypes.c_uint64), ("valMin", ctypes.c_double),
+                ("valMax", ctypes.c_double), ("isInt", ctypes.c_int), ("height", ctypes.c_uint64),
+                ("ratios", ctypes.POINTER(ctypes.c_uint64)), ("nRatios", ctypes.c_uint64), ("seed", ctypes.c_uint64),
+                ("sigmaDivisor", ctypes.c_double)]
+
+
+class _Info(ctypes.Structure):
+    _fields_ = [("D", ctypes.c_uint64), ("N", ctypes.c_uint64), ("height", ctypes.c_uint64),
+                ("intervals", ctypes.c_uint64), ("meshSizes", ctypes.c_uint64 * 16),
+                ("ratios", ctypes.c_uint64 * 16), ("hostBytes", ctypes.c_uint64),
+                ("deviceBytes", ctypes.c_uint64), ("prepared", ctypes.c_int), ("policy", ctypes.c_int * 16)]
+
+
+class Grid(ctypes.Structure):
+    """tblaeq_grid: one query's grid at one level (device pointers)."""
+    _fields_ = [("numRows", ctypes.c_uint64), ("dim", ctypes.c_uint64), ("nnz", ctypes.c_uint64),
+                ("ids", ctypes.c_void_p), ("vals", ctypes.c_void_p)]
+
+
+class _Batch(ctypes.Structure):
+    _fields_ = [("qtype", ctypes.c_int), ("mode", ctypes.c_int), ("nq", ctypes.c_uint64),
+                ("queries", ctypes.c_void_p), ("queriesOnDevice", ctypes.c_int), ("K", ctypes.c_uint64),
+                ("flags", ctypes.c_uint)]
+
+
+class _BatchResult(ctypes.Structure):
+    _fields_ = [("nq", ctypes.c_uint64), ("total", ctypes.c_uint64), ("offsets", ctypes.c_void_p),
+                ("ids", ctypes.c_void_p), ("vals", ctypes.c_void_p), ("dist2", ctypes.c_void_p),
+                ("levelItems", ctypes.c_void_p)]
+
+
+_lib = None
+
+
+def _load():
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise ImportError(f"{LIB_PATH} is not built; run `make -C t-blaeq_b200` (or __graft_entry__.build())")
+    lib = ctypes.CDLL(LIB_PATH)
+    P = ctypes.POINTER
+    vp = ctypes.c_void_p
+    sig = {
+        "tblaeq_last_error": ([], ctypes.c_char_p),
+        "tblaeq_abi_version": ([], ctypes.c_int),
+        "tblaeq_open": ([ctypes.c_char_p, P(vp)], ctypes.c_int),
+        "tblaeq_generate": ([P(_GenParams), P(vp)], ctypes.c_int),
+        "tblaeq_save": ([vp, ctypes.c_char_p], ctypes.c_int),
+        "tblaeq_close": ([vp], None),
+        "tblaeq_info": ([vp, P(_Info)], ctypes.c_int),
+        "tblaeq_recommend": ([vp, ctypes.c_uint64, P(ctypes.c_int)], ctypes.c_int),
+        "tblaeq_prepare": ([vp, P(ctypes.c_int), ctypes.c_uint64], ctypes.c_int),
+        "tblaeq_level": ([vp, ctypes.c_uint64, P(Grid), ctypes.c_int, P(ctypes.c_double), P(ctypes.c_double),
+                          P(ctypes.c_double), ctypes.c_uint64, P(Grid)], ctypes.c_int),
+        "tblaeq_coarsest_grid": ([vp, P(Grid)], ctypes.c_int),
+        "tblaeq_query_batch": ([vp, P(_Batch), P(_BatchResult)], ctypes.c_int),
+        "tblaeq_query_batch_host": ([vp, P(_Batch), P(ctypes.c_uint64), P(ctypes.c_uint64), ctypes.c_uint64,
+                                     P(ctypes.c_double), P(ctypes.c_uint64)], ctypes.c_int),
+        "tblaeq_host_array": ([vp, ctypes.c_int, ctypes.c_uint64, P(vp), P(ctypes.c_uint64)], ctypes.c_int),
+        "tblaeq_decode_points": ([vp, P(ctypes.c_uint64), ctypes.c_uint64, P(ctypes.c_double),
+                                  P(ctypes.c_uint64)], ctypes.c_int),
+        "tblaeq_query_batch_async": ([vp, P(_Batch)], ctypes.c_int),
+        "tblaeq_batch_wait": ([vp, P(_BatchResult)], ctypes.c_int),
+        "tblaeq_stream": ([vp], vp),
+        "tblaeq_level_counts": ([vp, P(ctypes.c_uint64), P(ctypes.c_uint64), ctypes.c_int, P(ctypes.c_uint64)],
+                                ctypes.c_int),
+        "tblaeq_set_device": ([ctypes.c_int], ctypes.c_int),
+        "tblaeq_set_timing": ([vp, ctypes.c_int], ctypes.c_int),
+        "tblaeq_stage_times": ([vp, P(ctypes.c_float), ctypes.c_int], ctypes.c_int),
+        "tblaeq_live_device_bytes": ([], ctypes.c_uint64),
+        "tblaeq_debug_fail_alloc_after": ([ctypes.c_uint64], None),
+    }
+    for name, (args, res) in sig.items():
+        f = getattr(lib, name)
+        f.argtypes = args
+        f.restype = res
+    _lib = lib
+    return lib
+
+
+def lib():
+    """The loaded C library (ctypes.CDLL)."""
+    return _load()
+
+
+def _check(code: int):
+    if code != 0:
+        raise TblaeqError(code, _load().tblaeq_last_error().decode())
+
+
+def _dptr(a: np.ndarray, ctype=ctypes.c_double):
+    return a.ctypes.data_as(ctypes.POINTER(ctype))
+
+
+class DeviceArray:
+    """A borrowed device buffer, exposed through __cuda_array_interface__ (torch.as_tensor works)."""
+
+    def __init__(self, ptr: int, shape, typestr: str, owner=None):
+        self.ptr = int(ptr or 0)
+        self.shape = tuple(int(s) for s in shape)
+        self.typestr = typestr
+        self._owner = owner
+
+    @property
+    def __cuda_array_interface__(self):
+        return {"shape": self.shape, "typestr": self.typestr, "data": (self.ptr, False), "version": 3}
+
+    def torch(self):
+        import torch
+        if self.ptr == 0 or 0 in self.shape:
+            dt = {"<u8": torch.uint64, "<f8": torch.float64, "<u4": torch.uint32}[self.typestr]
+            return torch.empty(self.shape, dtype=dt, device="cuda")
+        return torch.as_tensor(self, device="cuda")
+
+    def numpy(self) -> np.ndarray:
+        t = self.torch()
+        return t.cpu().numpy()
+
+
+@dataclass
+class BatchResult:
+    """Device-resident results of one batch (valid until the next batch call on the handle)."""
+    nq: int
+    total: int
+    offsets: DeviceArray
+    ids: DeviceArray
+    vals: Optional[DeviceArray]
+    dist2: Optional[DeviceArray]
+    level_items: Optional[DeviceArray]
+
+
+@dataclass
+class QueryResult:
+    """Mirror of the reference's QueryResult (src/core/QueryEngine.cuh:38-61)."""
+    type: QueryType = QueryType.RANGE
+    errorCode: int = 0
+    totalTimeUs: float = 0.0
+    queryCount: int = 0
+    datasetName: str = ""
+    queryParam: str = ""
+    memoryPolicy: str = ""
+    datasetSize: int = 0
+    datasetDim: int = 0
+    fineMeshSize: list = field(default_factory=list)
+    levelOriginalSize: list = field(default_factory=list)
+    levelFineMeshSize: list = field(default_factory=list)
+    queryTimeUs: list = field(default_factory=list)
+    fineMesh: list = field(default_factory=list)     # per query: np.ndarray of ids (saveFineMesh)
+    fineMeshDist2: list = field(default_factory=list)  # per query, KNN exact mode
+
+
+class QueryHandler:
+    """B200 counterpart of the reference's QueryHandler (src/core/QueryHandler.cuh:50-247)."""
+
+    def __init__(self, index_path: Optional[str] = None, load_from_index: bool = True, *, _handle=None):
+        lib = _load()
+        self._h = ctypes.c_void_p()
+        if _handle is not None:
+            self._h = _handle
+        else:
+            if index_path is None:
+                raise ValueError("index_path is required (or use QueryHandler.generate)")
+            if not load_from_index:
+                raise ValueError("Use QueryHandler(datasetPath) to build a new index.")
+            _check(lib.tblaeq_open(os.fsencode(index_path), ctypes.byref(self._h)))
+        self.mode = Mode.REF_PARITY
+        self.dataset_name = os.path.basename(os.path.normpath(index_path)) if index_path else "random"
+
+    @classmethod
+    def generate(cls, N: int, D: int, val_min: float = 1.0, val_max: float = 100.0, is_int: bool = False,
+                 height: int = 4, ratios: Sequence[int] = (100, 50, 20), seed: int = 12345,
+                 sigma_divisor: float = 3.0) -> "QueryHandler":
+        """QueryHandler(N, D, valMin, valMax, isInt, height, ratios, seed, sigmaDivisor)."""
+        lib = _load()
+        r = np.ascontiguousarray(np.array(list(ratios), dtype=np.uint64))
+        p = _GenParams(N, D, val_min, val_max, int(is_int), height, _dptr(r, ctypes.c_uint64), len(r), seed,
+                       sigma_divisor)
+        h = ctypes.c_void_p()
+        _check(lib.tblaeq_generate(ctypes.byref(p), ctypes.byref(h)))
+        obj = cls(_handle=h)
+        obj.dataset_name = f"Gen{N}D{D}"
+        return obj
+
+    # -- lifecycle -------------------------------------------------------------------------------
+    def close(self):
+        if getattr(self, "_h", None) and self._h.value:
+            _load().tblaeq_close(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def save_index(self, dir_path: str):
+        _check(_load().tblaeq_save(self._h, os.fsencode(dir_path)))
+
+    def info(self) -> dict:
+        inf = _Info()
+        _check(_load().tblaeq_info(self._h, ctypes.byref(inf)))
+        h = inf.height
+        return {"D": inf.D, "N": inf.N, "height": h, "intervals": inf.intervals,
+                "meshSizes": list(inf.meshSizes[:h]), "ratios": list(inf.ratios[:inf.intervals]),
+                "hostBytes": inf.hostBytes, "deviceBytes": inf.deviceBytes, "prepared": bool(inf.prepared),
+                "policy": [LevelPolicy(p) for p in inf.policy[:inf.intervals]] if inf.prepared else None}
+
+    def getSize(self) -> int:
+        return self.info()["N"]
+
+    def getDim(self) -> int:
+        return self.info()["D"]
+
+    def recommend(self, free_bytes: int = 0) -> list:
+        n = self.info()["intervals"]
+        out = (ctypes.c_int * n)()
+        _check(_load().tblaeq_recommend(self._h, free_bytes, out))
+        return [LevelPolicy(v) for v in out]
+
+    def prepare_for_query(self, policy=None):
+        """prepareForQuery(): None = recommendation, a LevelPolicy for every level, or a list."""
+        lib = _load()
+        if policy is None:
+            _check(lib.tblaeq_prepare(self._h, None, 0))
+            return
+        n = self.info()["intervals"]
+        levels = [policy] * n if isinstance(policy, (int, LevelPolicy)) else list(policy)
+        arr = (ctypes.c_int * len(levels))(*[int(x) for x in levels])
+        _check(lib.tblaeq_prepare(self._h, arr, len(levels)))
+
+    prepareForQuery = prepare_for_query
+
+    # -- host views ------------------------------------------------------------------------------
+    def host_array(self, which: int, l: int = 0) -> np.ndarray:
+        ptr = ctypes.c_void_p()
+        cnt = ctypes.c_uint64()
+        _check(_load().tblaeq_host_array(self._h, which, l, ctypes.byref(ptr), ctypes.byref(cnt)))
+        ct = ctypes.c_double if which in (0, 2, 5) else ctypes.c_uint64
+        if cnt.value == 0:
+            return np.zeros(0, dtype=np.float64 if ct is ctypes.c_double else np.uint64)
+        return np.ctypeslib.as_array(ctypes.cast(ptr, ctypes.POINTER(ct)), (cnt.value,)).copy()
+
+    def decode_points(self, positions) -> tuple:
+        pos = np.ascontiguousarray(np.asarray(positions, dtype=np.uint64))
+        D = self.info()["D"]
+        out = np.empty((len(pos), D), np.float64)
+        ids = np.empty(len(pos), np.uint64)
+        _check(_load().tblaeq_decode_points(self._h, _dptr(pos, ctypes.c_uint64), len(pos), _dptr(out),
+                                            _dptr(ids, ctypes.c_uint64)))
+        return out, ids
+
+    # -- per-level plugin (IQueryStrategy::runLevel) ----------------------------------------------
+    def coarsest_grid(self) -> Grid:
+        g = Grid()
+        _check(_load().tblaeq_coarsest_grid(self._h, ctypes.byref(g)))
+        return g
+
+    def run_level(self, l: int, grid: Grid, qtype: QueryType, lo=None, hi=None, point=None, K: int = 0) -> Grid:
+        out = Grid()
+        D = int(grid.dim)
+        def arr(v):
+            if v is None:
+                return None
+            a = np.ascontiguousarray(np.asarray(v, dtype=np.float64))
+            if a.shape != (D,):
+                raise ValueError(f"expected {D} values")
+            return a
+        lo_a, hi_a, p_a = arr(lo), arr(hi), arr(point)
+        _check(_load().tblaeq_level(self._h, l, ctypes.byref(grid), int(qtype),
+                                    _dptr(lo_a) if lo_a is not None else None,
+                                    _dptr(hi_a) if hi_a is not None else None,
+                                    _dptr(p_a) if p_a is not None else None, K, ctypes.byref(out)))
+        return out
+
+    @staticmethod
+    def grid_arrays(g: Grid):
+        """(ids, vals) of a device grid as numpy copies."""
+        ids = DeviceArray(g.ids, (g.nnz,), "<u8").numpy() if g.nnz else np.zeros(0, np.uint64)
+        vals = DeviceArray(g.vals, (g.nnz, g.dim), "<f8").numpy() if g.nnz else np.zeros((0, g.dim))
+        return ids, vals
+
+    # -- batched engine --------------------------------------------------------------------------
+    def query_batch(self, qtype: QueryType, queries, mode: Mode = Mode.EXACT, K: int = 0,
+                    flags: int = 0) -> BatchResult:
+        """Batched traversal; `queries` is a numpy array (host) or a CUDA tensor (device)."""
+        on_dev = hasattr(queries, "__cuda_array_interface__")
+        if on_dev:
+            ptr = queries.__cuda_array_interface__["data"][0]
+            nq = int(queries.shape[0])
+            keep = queries
+        else:
+            keep = np.ascontiguousarray(np.asarray(queries, dtype=np.float64))
+            ptr = keep.ctypes.data
+            nq = keep.shape[0]
+        b = _Batch(int(qtype), int(mode), nq, ptr, int(on_dev), K, flags)
+        r = _BatchResult()
+        _check(_load().tblaeq_query_batch(self._h, ctypes.byref(b), ctypes.byref(r)))
+        del keep
+        D = self.info()["D"]
+        ivl = self.info()["intervals"]
+        return BatchResult(
+            nq=r.nq, total=r.total,
+            offsets=DeviceArray(r.offsets, (r.nq + 1,), "<u8", self),
+            ids=DeviceArray(r.ids, (r.total,), "<u8", self),
+            vals=DeviceArray(r.vals, (r.total, D), "<f8", self) if r.vals else None,
+            dist2=DeviceArray(r.dist2, (r.total,), "<f8", self) if r.dist2 else None,
+            level_items=DeviceArray(r.levelItems, (ivl, r.nq), "<u4", self) if r.levelItems else None)
+
+    def query_batch_async(self, qtype: QueryType, dqueries, mode: Mode = Mode.EXACT, K: int = 0, flags: int = 0):
+        """Enqueue on the handle's stream without waiting (device queries; see tblaeq_query_batch_async)."""
+        ptr = dqueries.__cuda_array_interface__["data"][0]
+        b = _Batch(int(qtype), int(mode), int(dqueries.shape[0]), ptr, 1, K, flags)
+        _check(_load().tblaeq_query_batch_async(self._h, ctypes.byref(b)))
+
+    def batch_wait(self) -> int:
+        r = _BatchResult()
+        _check(_load().tblaeq_batch_wait(self._h, ctypes.byref(r)))
+        return int(r.total)
+
+    def level_counts(self):
+        """(entries per frontier, children per frontier, results) of the last batch."""
+        e = (ctypes.c_uint64 * 32)()
+        it = (ctypes.c_uint64 * 32)()
+        r = ctypes.c_uint64()
+        n = _load().tblaeq_level_counts(self._h, e, it, 32, ctypes.byref(r))
+        if n < 0:
+            _check(-n)
+        return list(e[:n]), list(it[:n]), int(r.value)
+
+    def stream_handle(self) -> int:
+        return _load().tblaeq_stream(self._h) or 0
+
+    def set_timing(self, on: bool = True):
+        _check(_load().tblaeq_set_timing(self._h, int(on)))
+
+    def stage_times(self) -> list:
+        buf = (ctypes.c_float * 64)()
+        n = _load().tblaeq_stage_times(self._h, buf, 64)
+        if n < 0:
+            raise TblaeqError(7, "stage timing is off")
+        return list(buf[:n])
+
+    def query_batch_host(self, qtype: QueryType, queries: np.ndarray, mode: Mode = Mode.EXACT, K: int = 0,
+                         ids_cap: Optional[int] = None):
+        """Host-buffer batch: returns (offsets, ids, dist2 or None)."""
+        q = np.ascontiguousarray(np.asarray(queries, dtype=np.float64))
+        nq = q.shape[0]
+        cap = ids_cap if ids_cap is not None else max(1024, nq * 64)
+        while True:
+            offs = np.empty(nq + 1, np.uint64)
+            ids = np.empty(cap, np.uint64)
+            d2 = np.empty(cap, np.float64) if qtype == QueryType.POINT else None
+            total = ctypes.c_uint64()
+            b = _Batch(int(qtype), int(mode), nq, q.ctypes.data, 0, K, 0)
+            code = _load().tblaeq_query_batch_host(self._h, ctypes.byref(b), _dptr(offs, ctypes.c_uint64),
+                                                   _dptr(ids, ctypes.c_uint64), cap,
+                                                   _dptr(d2) if d2 is not None else None, ctypes.byref(total))
+            if code == 5 and ids_cap is None and total.value > cap:
+                cap = int(total.value)
+                continue
+            _check(code)
+            n = int(total.value)
+            return offs, ids[:n], (d2[:n] if d2 is not None else None)
+
+    # -- reference-style query APIs ----------------------------------------------------------------
+    def _run_plain(self, qtype: QueryType, rows: np.ndarray, K: int, save: bool) -> QueryResult:
+        info = self.info()
+        res = QueryResult(type=qtype, datasetName=self.dataset_name, datasetSize=info["N"], datasetDim=info["D"])
+        res.queryParam = f"K={K}" if qtype == QueryType.POINT else res.queryParam
+        res.levelOriginalSize = [info["meshSizes"][info["intervals"] - (l + 1)] for l in range(info["intervals"])]
+        pol = info["policy"] or []
+        res.memoryPolicy = "-".join(p.name for p in pol)
+        for i in range(rows.shape[0]):
+            t0 = time.perf_counter()
+            offs, ids, d2 = self.query_batch_host(qtype, rows[i:i + 1], self.mode, K)
+            us = (time.perf_counter() - t0) * 1e6
+            res.queryTimeUs.append(us)
+            res.fineMeshSize.append(int(offs[1] - offs[0]))
+            if save:
+                res.fineMesh.append(ids)
+                if d2 is not None:
+                    res.fineMeshDist2.append(d2)
+        times = sorted(res.queryTimeUs)
+        cnt = len(times)
+        total = sum(times)
+        if cnt > 2:  # the reference drops the fastest and slowest query (QueryEngine.cu:216-220)
+            total -= times[0] + times[-1]
+            cnt -= 2
+        res.totalTimeUs = total
+        res.queryCount = cnt
+        return res
+
+    def perform_single_range_query(self, query_upper_bound, query_lower_bound,
+                                   save_fine_mesh: bool = False) -> QueryResult:
+        """performSingleRangeQuery(upper, lower, saveFineMesh): note the upper-bound-first order."""
+        lo = np.asarray(query_lower_bound, dtype=np.float64)
+        hi = np.asarray(query_upper_bound, dtype=np.float64)
+        r = self._run_plain(QueryType.RANGE, np.concatenate([lo, hi])[None, :], 0, save_fine_mesh)
+        r.queryParam = "single-range-query"
+        return r
+
+    performSingleRangeQuery = perform_single_range_query
+
+    def perform_single_knn_query(self, query_point, k: int, save_fine_mesh: bool = False) -> QueryResult:
+        p = np.asarray(query_point, dtype=np.float64)[None, :]
+        return self._run_plain(QueryType.POINT, p, k, save_fine_mesh)
+
+    performSingleKNNQuery = perform_single_knn_query
+
+    def perform_query(self, query_path: str, q_type: QueryType, save_fine_mesh: bool = False,
+                      max_query_count: int = 2 ** 31 - 1, K: int = 0) -> QueryResult:
+        rows, ftype = load_query_file(query_path, q_type)
+        if ftype != q_type:
+            return QueryResult(errorCode=1)
+        rows = rows[:max_query_count]
+        return self._run_plain(q_type, rows, K, save_fine_mesh)
+
+    performQuery = perform_query
+
+
+# ---- reference query-file format (src/Data_Structures/File.cu:139-216) ---------------------------
+def save_query_file(path: str, q_type: QueryType, rows: np.ndarray, D: int):
+    """Header 'n D', then one row per query: 2D values (lo then hi) for RANGE, D values for POINT."""
+    rows = np.asarray(rows, dtype=np.float64)
+    with open(path, "w") as f:
+        f.write(f"{rows.shape[0]} {D}\n")
+        for r in rows:
+            f.write(" ".join("%.17g" % v for v in r) + "\n")
+
+
+def load_query_file(path: str, q_type: QueryType):
+    with open(path) as f:
+        header = f.readline().split()
+        if len(header) < 2:
+            raise ValueError("loadQueryFromFile: invalid header")
+        n, D = int(header[0]), int(header[1])
+        if n <= 0 or D <= 0:
+            raise ValueError("loadQueryFromFile: invalid header")
+        cols = 2 * D if q_type == QueryType.RANGE else D
+        rows = np.empty((n, cols), np.float64)
+        for i in range(n):
+            line = f.readline()
+            vals = line.split()
+            if len(vals) < cols:
+                raise ValueError(f"loadQueryFromFile: expected {cols} values at row {i + 1}")
+            rows[i] = [float(v) for v in vals[:cols]]
+    return rows, q_type
+
+
+def set_device(device: int):
+    """cudaSetDevice for this library's CUDA runtime on the calling thread (before prepare)."""
+    _check(_load().tblaeq_set_device(int(device)))

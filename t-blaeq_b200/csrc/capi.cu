@@ -1,0 +1,444 @@
+// extern "C" boundary (include/tblaeq.h) over the C++ facade.
+#include <cstring>
+#include <filesystem>
+#include <new>
+#include <string>
+
+#include "../../include/tblaeq.h"
+#include "handler.hpp"
+
+using namespace tblaeq;
+
+struct tblaeq_handle {
+    std::unique_ptr<QueryHandler> qh;
+    DeviceMem stage;                            // device staging for host-side query batches
+    std::vector<std::vector<uint32_t>> parent;  // parent position per mesh (lazy, decode_points)
+    std::vector<std::vector<uint64_t>> posOf;   // position of each original id per mesh (lazy)
+    uint64_t lastNq = 0;                        // last asynchronously enqueued batch
+    unsigned lastFlags = 0;
+};
+
+namespace {
+
+thread_local std::string gLastError;
+
+int fail(int code, const std::string& msg) {
+    gLastError = msg;
+    return code;
+}
+
+template <class F>
+int guarded(F&& f) {
+    try {
+        gLastError.clear();
+        return f();
+    } catch (const CudaError& e) {
+        if (e.code == cudaErrorMemoryAllocation) return fail(TBLAEQ_ERR_OOM, e.what());
+        if (e.code == cudaErrorLaunchTimeout) return fail(TBLAEQ_ERR_TIMEOUT, e.what());
+        return fail(TBLAEQ_ERR_CUDA, e.what());
+    } catch (const std::invalid_argument& e) {
+        return fail(TBLAEQ_ERR_INVALID, e.what());
+    } catch (const std::out_of_range& e) {
+        return fail(TBLAEQ_ERR_INVALID, e.what());
+    } catch (const std::bad_alloc& e) {
+        return fail(TBLAEQ_ERR_OOM, std::string("host allocation failed: ") + e.what());
+    } catch (const std::exception& e) {
+        const std::string m = e.what();
+        if (m.rfind("Cannot read", 0) == 0 || m.rfind("Truncated", 0) == 0 || m.rfind("Invalid index", 0) == 0 ||
+            m.rfind("Cannot write", 0) == 0 || m.rfind("Read error", 0) == 0 || m.rfind("Short write", 0) == 0 ||
+            m.rfind("Cannot stat", 0) == 0)
+            return fail(TBLAEQ_ERR_IO, m);
+        return fail(TBLAEQ_ERR_CUDA, m);
+    } catch (...) {
+        return fail(TBLAEQ_ERR_CUDA, "unknown error");
+    }
+}
+
+int checkPrepared(tblaeq_handle* h) {
+    if (!h || !h->qh) return fail(TBLAEQ_ERR_INVALID, "null handle");
+    if (!h->qh->prepared()) return fail(TBLAEQ_ERR_STATE, "call tblaeq_prepare before querying");
+    return TBLAEQ_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* tblaeq_last_error(void) { return gLastError.c_str(); }
+int tblaeq_abi_version(void) { return TBLAEQ_ABI_VERSION; }
+
+int tblaeq_open(const char* dir, tblaeq_handle** out) {
+    if (!dir || !out) return fail(TBLAEQ_ERR_INVALID, "null argument");
+    *out = nullptr;
+    return guarded([&]() -> int {
+        if (!std::filesystem::is_directory(dir)) return fail(TBLAEQ_ERR_IO, std::string("Cannot read: ") + dir);
+        auto h = std::make_unique<tblaeq_handle>();
+        h->qh = std::make_unique<QueryHandler>(std::string(dir), true);
+        *out = h.release();
+        return TBLAEQ_OK;
+    });
+}
+
+int tblaeq_generate(const tblaeq_gen_params* p, tblaeq_handle** out) {
+    if (!p || !out) return fail(TBLAEQ_ERR_INVALID, "null argument");
+    *out = nullptr;
+    return guarded([&]() -> int {
+        GenParams g;
+        g.N = p->N;
+        g.D = p->D;
+        g.valMin = p->valMin;
+        g.valMax = p->valMax;
+        g.isInt = p->isInt != 0;
+        g.height = p->height;
+        if (p->height < 2) return fail(TBLAEQ_ERR_INVALID, "QueryHandler: height must be >= 2");
+        if (!p->ratios || p->nRatios != p->height - 1)
+            return fail(TBLAEQ_ERR_INVALID, "QueryHandler: ratios size must equal height - 1");
+        g.ratios.assign(p->ratios, p->ratios + (p->height - 1));
+        g.seed = p->seed;
+        g.sigmaDivisor = p->sigmaDivisor;
+        auto h = std::make_unique<tblaeq_handle>();
+        h->qh = std::make_unique<QueryHandler>(g);
+        *out = h.release();
+        return TBLAEQ_OK;
+    });
+}
+
+int tblaeq_save(const tblaeq_handle* h, const char* dir) {
+    if (!h || !dir) return fail(TBLAEQ_ERR_INVALID, "null argument");
+    return guarded([&]() -> int {
+        h->qh->saveIndex(dir);
+        return TBLAEQ_OK;
+    });
+}
+
+void tblaeq_close(tblaeq_handle* h) { delete h; }
+
+int tblaeq_info(const tblaeq_handle* h, tblaeq_index_info* out) {
+    if (!h || !out) return fail(TBLAEQ_ERR_INVALID, "null argument");
+    return guarded([&]() -> int {
+        const HostIndex& x = h->qh->index();
+        std::memset(out, 0, sizeof(*out));
+        out->D = x.D;
+        out->N = x.N;
+        out->height = x.height;
+        out->intervals = x.intervals;
+        if (x.height > TBLAEQ_MAX_HEIGHT) return fail(TBLAEQ_ERR_INVALID, "index deeper than TBLAEQ_MAX_HEIGHT");
+        for (uint64_t i = 0; i < x.height; ++i) out->meshSizes[i] = x.meshSizes[i];
+        for (uint64_t i = 0; i < x.intervals; ++i) out->ratios[i] = x.ratios[i];
+        const MemoryStats st = computeStats(x);
+        out->hostBytes = st.hostTotal;
+        out->deviceBytes = st.deviceTotal;
+        out->prepared = h->qh->prepared() ? 1 : 0;
+        if (h->qh->prepared())
+            for (uint64_t i = 0; i < x.intervals; ++i) out->policy[i] = static_cast<int>(h->qh->activePolicy().levels[i]);
+        return TBLAEQ_OK;
+    });
+}
+
+int tblaeq_recommend(const tblaeq_handle* h, uint64_t free_bytes, int* policy_out) {
+    if (!h || !policy_out) return fail(TBLAEQ_ERR_INVALID, "null argument");
+    return guarded([&]() -> int {
+        uint64_t fb = free_bytes;
+        if (fb == 0) {
+            size_t f = 0, t = 0;
+            TBLAEQ_CUDA(cudaMemGetInfo(&f, &t));
+            fb = f;
+        }
+        const IndexPolicy p = PolicyScheduler::recommend(h->qh->index(), fb);
+        for (size_t i = 0; i < p.levels.size(); ++i) policy_out[i] = static_cast<int>(p.levels[i]);
+        return TBLAEQ_OK;
+    });
+}
+
+int tblaeq_prepare(tblaeq_handle* h, const int* policy, uint64_t n_levels) {
+    if (!h) return fail(TBLAEQ_ERR_INVALID, "null handle");
+    return guarded([&]() -> int {
+        if (!policy) {
+            h->qh->prepareForQuery();
+            return TBLAEQ_OK;
+        }
+        if (n_levels != h->qh->index().intervals)
+            return fail(TBLAEQ_ERR_INVALID, "policy must list one LevelPolicy per interval");
+        IndexPolicy p;
+        for (uint64_t i = 0; i < n_levels; ++i) {
+            if (policy[i] < 0 || policy[i] > 3) return fail(TBLAEQ_ERR_INVALID, "LevelPolicy must be 0..3");
+            p.levels.push_back(static_cast<LevelPolicy>(policy[i]));
+        }
+        h->qh->prepareForQuery(p);
+        return TBLAEQ_OK;
+    });
+}
+
+int tblaeq_level(tblaeq_handle* h, uint64_t l, const tblaeq_grid* in, int qtype, const double* lo, const double* hi,
+                 const double* q, uint64_t K, tblaeq_grid* out) {
+    if (int c = checkPrepared(h)) return c;
+    if (!in || !out) return fail(TBLAEQ_ERR_INVALID, "null grid");
+    if (qtype != TBLAEQ_RANGE && qtype != TBLAEQ_POINT) return fail(TBLAEQ_ERR_INVALID, "unknown query type");
+    if (qtype == TBLAEQ_RANGE && (!lo || !hi)) return fail(TBLAEQ_ERR_INVALID, "range query needs lo and hi");
+    if (qtype == TBLAEQ_POINT && !q) return fail(TBLAEQ_ERR_INVALID, "KNN query needs a point");
+    return guarded([&]() -> int {
+        B200Strategy s(h->qh->runtime());
+        Grid g{in->numRows, in->dim, in->nnz, in->ids, in->vals};
+        const LevelResult r =
+            s.runLevel(l, g, qtype == TBLAEQ_RANGE ? QueryType::RANGE : QueryType::POINT, lo, hi, q, K);
+        out->numRows = r.grid.numRows;
+        out->dim = r.grid.dim;
+        out->nnz = r.grid.nnz;
+        out->ids = r.grid.ids;
+        out->vals = r.grid.vals;
+        return TBLAEQ_OK;
+    });
+}
+
+int tblaeq_coarsest_grid(tblaeq_handle* h, tblaeq_grid* out) {
+    if (int c = checkPrepared(h)) return c;
+    if (!out) return fail(TBLAEQ_ERR_INVALID, "null grid");
+    Runtime& rt = h->qh->runtime();
+    out->numRows = h->qh->index().coarsest.rows;
+    out->dim = rt.dev->D;
+    out->nnz = rt.dev->meshCount[0];
+    out->ids = rt.dev->coarseIds.as<uint64_t>();
+    out->vals = rt.dev->coarseVals.as<double>();
+    return TBLAEQ_OK;
+}
+
+static int runBatch(tblaeq_handle* h, const tblaeq_batch* b, const double* dQueries, tblaeq_batch_result* out) {
+    Runtime& rt = h->qh->runtime();
+    if (b->qtype != TBLAEQ_RANGE) return fail(TBLAEQ_ERR_INVALID, "batched KNN is not available in this build");
+    if (b->nq > 0xffffffffull) return fail(TBLAEQ_ERR_OVERFLOW, "too many queries in one batch");
+    const BatchOutput o = rt.engine->runRange(dQueries, static_cast<uint32_t>(b->nq), b->mode, b->flags);
+    h->lastNq = b->nq;
+    h->lastFlags = b->flags;
+    out->nq = b->nq;
+    out->total = o.total;
+    out->offsets = o.offsets;
+    out->ids = o.ids;
+    out->vals = o.vals;
+    out->dist2 = o.dist2;
+    out->levelItems = o.levelItems;
+    return TBLAEQ_OK;
+}
+
+static int validateBatch(tblaeq_handle* h, const tblaeq_batch* b) {
+    if (int c = checkPrepared(h)) return c;
+    if (!b) return fail(TBLAEQ_ERR_INVALID, "null batch");
+    if (b->mode != TBLAEQ_MODE_REF_PARITY && b->mode != TBLAEQ_MODE_EXACT) return fail(TBLAEQ_ERR_INVALID, "bad mode");
+    if (b->qtype != TBLAEQ_RANGE && b->qtype != TBLAEQ_POINT) return fail(TBLAEQ_ERR_INVALID, "bad query type");
+    if (b->nq > 0 && !b->queries) return fail(TBLAEQ_ERR_INVALID, "null queries");
+    return TBLAEQ_OK;
+}
+
+int tblaeq_query_batch(tblaeq_handle* h, const tblaeq_batch* b, tblaeq_batch_result* out) {
+    if (int c = validateBatch(h, b)) return c;
+    if (!out) return fail(TBLAEQ_ERR_INVALID, "null result");
+    return guarded([&]() -> int {
+        const double* dq = b->queries;
+        if (!b->queriesOnDevice && b->nq) {
+            Runtime& rt = h->qh->runtime();
+            const uint64_t D = rt.dev->D;
+            const size_t bytes = b->nq * (b->qtype == TBLAEQ_RANGE ? 2 * D : D) * 8;
+            if (h->stage.bytes() < bytes) h->stage.alloc(bytes);
+            TBLAEQ_CUDA(cudaMemcpyAsync(h->stage.get(), b->queries, bytes, cudaMemcpyHostToDevice, rt.stream));
+            dq = h->stage.as<double>();
+        }
+        return runBatch(h, b, dq, out);
+    });
+}
+
+int tblaeq_query_batch_host(tblaeq_handle* h, const tblaeq_batch* b, uint64_t* offsets_out, uint64_t* ids_out,
+                            uint64_t ids_cap, double* dist2_out, uint64_t* total) {
+    if (int c = validateBatch(h, b)) return c;
+    if (!offsets_out || (!ids_out && ids_cap)) return fail(TBLAEQ_ERR_INVALID, "null output buffer");
+    return guarded([&]() -> int {
+        tblaeq_batch hb = *b;
+        tblaeq_batch_result r{};
+        int c = tblaeq_query_batch(h, &hb, &r);
+        if (c) return c;
+        Runtime& rt = h->qh->runtime();
+        TBLAEQ_CUDA(cudaMemcpyAsync(offsets_out, r.offsets, (b->nq + 1) * 8, cudaMemcpyDeviceToHost, rt.stream));
+        const uint64_t n = std::min<uint64_t>(r.total, ids_cap);
+        if (n) TBLAEQ_CUDA(cudaMemcpyAsync(ids_out, r.ids, n * 8, cudaMemcpyDeviceToHost, rt.stream));
+        if (n && dist2_out && r.dist2)
+            TBLAEQ_CUDA(cudaMemcpyAsync(dist2_out, r.dist2, n * 8, cudaMemcpyDeviceToHost, rt.stream));
+        TBLAEQ_CUDA(cudaStreamSynchronize(rt.stream));
+        if (total) *total = r.total;
+        if (r.total > ids_cap) return fail(TBLAEQ_ERR_OVERFLOW, "result ids exceed ids_cap");
+        return TBLAEQ_OK;
+    });
+}
+
+int tblaeq_query_batch_async(tblaeq_handle* h, const tblaeq_batch* b) {
+    if (int c = validateBatch(h, b)) return c;
+    if (!b->queriesOnDevice && b->nq) return fail(TBLAEQ_ERR_INVALID, "async batches need device queries");
+    if (b->qtype != TBLAEQ_RANGE) return fail(TBLAEQ_ERR_INVALID, "batched KNN is not available in this build");
+    return guarded([&]() -> int {
+        Runtime& rt = h->qh->runtime();
+        h->lastNq = b->nq;
+        h->lastFlags = b->flags;
+        rt.engine->enqueueRange(b->queries, static_cast<uint32_t>(b->nq), b->mode, b->flags);
+        return TBLAEQ_OK;
+    });
+}
+
+int tblaeq_batch_wait(tblaeq_handle* h, tblaeq_batch_result* out) {
+    if (int c = checkPrepared(h)) return c;
+    return guarded([&]() -> int {
+        Runtime& rt = h->qh->runtime();
+        const uint32_t st = rt.engine->status();
+        if (st & (kStatusLookbackTimeout | kStatusWindowOverflow))
+            return fail(TBLAEQ_ERR_TIMEOUT, "traversal kernel reported status " + std::to_string(st));
+        if (st) return fail(TBLAEQ_ERR_OVERFLOW, "workspace overflow; rerun with tblaeq_query_batch");
+        if (out) {
+            const BatchOutput o = rt.engine->output(static_cast<uint32_t>(h->lastNq), h->lastFlags);
+            out->nq = h->lastNq;
+            out->total = rt.engine->lastTotal(static_cast<uint32_t>(h->lastNq));
+            out->offsets = o.offsets;
+            out->ids = o.ids;
+            out->vals = o.vals;
+            out->dist2 = o.dist2;
+            out->levelItems = o.levelItems;
+        }
+        return TBLAEQ_OK;
+    });
+}
+
+int tblaeq_level_counts(tblaeq_handle* h, uint64_t* entries, uint64_t* items, int cap, uint64_t* results) {
+    if (int c = checkPrepared(h)) return -c;
+    int n = 0;
+    const int c = guarded([&]() -> int {
+        std::vector<uint64_t> e, it;
+        uint64_t r = 0;
+        h->qh->runtime().engine->levelCounts(e, it, r);
+        n = std::min<int>(cap, static_cast<int>(e.size()));
+        for (int i = 0; i < n; ++i) {
+            if (entries) entries[i] = e[i];
+            if (items) items[i] = it[i];
+        }
+        if (results) *results = r;
+        return TBLAEQ_OK;
+    });
+    return c == TBLAEQ_OK ? n : -c;
+}
+
+int tblaeq_set_device(int device) {
+    return guarded([&]() -> int {
+        TBLAEQ_CUDA(cudaSetDevice(device));
+        return TBLAEQ_OK;
+    });
+}
+
+void* tblaeq_stream(tblaeq_handle* h) {
+    if (!h || !h->qh || !h->qh->prepared()) return nullptr;
+    return h->qh->runtime().stream;
+}
+
+int tblaeq_set_timing(tblaeq_handle* h, int on) {
+    if (int c = checkPrepared(h)) return c;
+    return guarded([&]() -> int {
+        h->qh->runtime().engine->setTiming(on != 0);
+        return TBLAEQ_OK;
+    });
+}
+
+int tblaeq_stage_times(tblaeq_handle* h, float* ms, int cap) {
+    if (!h || !h->qh || !h->qh->prepared() || !ms) return -1;
+    int n = -1;
+    const int c = guarded([&]() -> int {
+        const std::vector<float> t = h->qh->runtime().engine->stageTimes();
+        if (t.empty()) return TBLAEQ_ERR_STATE;
+        n = std::min<int>(cap, static_cast<int>(t.size()));
+        for (int i = 0; i < n; ++i) ms[i] = t[i];
+        return TBLAEQ_OK;
+    });
+    return c == TBLAEQ_OK ? n : -1;
+}
+
+int tblaeq_host_array(const tblaeq_handle* h, int which, uint64_t l, const void** ptr, uint64_t* count) {
+    if (!h || !ptr || !count) return fail(TBLAEQ_ERR_INVALID, "null argument");
+    const HostIndex& x = h->qh->index();
+    switch (which) {
+        case 0:
+            if (l >= x.intervals) break;
+            *ptr = x.pTensors[l].vals.data();
+            *count = x.pTensors[l].vals.size();
+            return TBLAEQ_OK;
+        case 1:
+            if (l >= x.intervals) break;
+            *ptr = x.pTensors[l].colRes.data();
+            *count = x.pTensors[l].colRes.size();
+            return TBLAEQ_OK;
+        case 2:
+            if (l >= x.intervals) break;
+            *ptr = x.radius[l].data();
+            *count = x.radius[l].size();
+            return TBLAEQ_OK;
+        case 3:
+            if (l == 0 || l >= x.height) break;
+            *ptr = x.maps[l].data();
+            *count = x.maps[l].size();
+            return TBLAEQ_OK;
+        case 4:
+            *ptr = x.coarsest.ids.data();
+            *count = x.coarsest.ids.size();
+            return TBLAEQ_OK;
+        case 5:
+            *ptr = x.coarsest.vals.data();
+            *count = x.coarsest.vals.size();
+            return TBLAEQ_OK;
+        default:
+            break;
+    }
+    return fail(TBLAEQ_ERR_INVALID, "no such host array");
+}
+
+int tblaeq_decode_points(tblaeq_handle* h, const uint64_t* positions, uint64_t n, double* coords_out,
+                         uint64_t* ids_out) {
+    if (!h || (n && (!positions || !coords_out))) return fail(TBLAEQ_ERR_INVALID, "null argument");
+    return guarded([&]() -> int {
+        const HostIndex& x = h->qh->index();
+        const uint64_t H = x.height, D = x.D;
+        if (h->parent.empty()) {
+            h->posOf.resize(H);
+            for (uint64_t m = 0; m + 1 < H; ++m) {
+                const uint64_t cnt = x.meshCount(m);
+                h->posOf[m].resize(cnt);
+                for (uint64_t s = 0; s < cnt; ++s) h->posOf[m][m == 0 ? x.coarsest.ids[s] : x.maps[m][s]] = s;
+            }
+            h->parent.resize(H);
+            for (uint64_t m = 1; m < H; ++m) {
+                const PTensor& P = x.pTensors[m - 1];
+                h->parent[m].resize(P.rows);
+                for (uint64_t o = 0; o < P.cols; ++o)
+                    for (uint64_t j = P.colRes[o]; j < P.colRes[o + 1]; ++j)
+                        h->parent[m][j] = static_cast<uint32_t>(h->posOf[m - 1][o]);
+            }
+        }
+        const uint64_t nLeaf = x.meshCount(H - 1);
+        std::vector<uint64_t> chain(H);
+        std::vector<double> v(D);
+        for (uint64_t i = 0; i < n; ++i) {
+            if (positions[i] >= nLeaf) return fail(TBLAEQ_ERR_INVALID, "position out of range");
+            chain[H - 1] = positions[i];
+            for (uint64_t m = H - 1; m > 0; --m) chain[m - 1] = h->parent[m][chain[m]];
+            for (uint64_t d = 0; d < D; ++d) v[d] = x.coarsest.vals[chain[0] * D + d];
+            for (uint64_t m = 1; m < H; ++m)
+                for (uint64_t d = 0; d < D; ++d) v[d] = x.pTensors[m - 1].vals[chain[m] * D + d] * v[d];
+            for (uint64_t d = 0; d < D; ++d) coords_out[i * D + d] = v[d];
+            if (ids_out) ids_out[i] = x.maps[H - 1][positions[i]];
+        }
+        return TBLAEQ_OK;
+    });
+}
+
+uint64_t tblaeq_live_device_bytes(void) { return liveDeviceBytes(); }
+
+void tblaeq_debug_fail_alloc_after(uint64_t n) {
+    if (n == 0) {
+        setAllocHook(nullptr);
+        return;
+    }
+    auto counter = std::make_shared<uint64_t>(n);
+    setAllocHook([counter](size_t) { return --(*counter) > 0; });
+}
+
+}  // extern "C"

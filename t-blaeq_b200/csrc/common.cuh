@@ -1,0 +1,36 @@
+// Shared device-side definitions for the T-BLAEQ B200 traversal kernels.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <cstdint>
+#include <cstdio>
+#include <stdexcept>
+#include <string>
+
+namespace tblaeq {
+
+// Error bits a kernel may raise in the device status word; the host turns them into
+// TBLAEQ_ERR_OVERFLOW / TBLAEQ_ERR_TIMEOUT before any result is read.
+enum DeviceStatus : uint32_t {
+    kStatusOverflowEntries = 1u << 0,   // output frontier / result capacity exceeded
+    kStatusOverflowItems = 1u << 1,     // next-level work items exceed the tile-start capacity
+    kStatusOverflowSum = 1u << 2,       // 32-bit child-prefix overflow
+    kStatusLookbackTimeout = 1u << 3,   // a decoupled look-back spin gave up
+    kStatusWindowOverflow = 1u << 4,    // a tile spanned more frontier entries than it can stage
+};
+
+struct CudaError : std::runtime_error {
+    cudaError_t code;
+    CudaError(cudaError_t c, const std::string& what) : std::runtime_error(what), code(c) {}
+};
+
+#define TBLAEQ_CUDA(call)                                                                                     \
+    do {                                                                                                      \
+        cudaError_t e_ = (call);                                                                              \
+        if (e_ != cudaSuccess) {                                                                              \
+            throw ::tblaeq::CudaError(e_, std::string(#call) + " failed: " + cudaGetErrorString(e_) + " at " + \
+                                              __FILE__ + ":" + std::to_string(__LINE__));                      \
+        }                                                                                                     \
+    } while (0)
+
+}  // namespace tblaeq

@@ -1,0 +1,248 @@
+// Device-resident index and its derived position-space arrays.
+#include "device_index.hpp"
+
+#include <omp.h>
+
+#include <algorithm>
+#include <atomic>
+#include <cmath>
+#include <mutex>
+
+namespace tblaeq {
+
+namespace {
+std::mutex gHookMutex;
+AllocHook gHook;
+std::atomic<size_t> gLiveBytes{0};
+}  // namespace
+
+void setAllocHook(AllocHook hook) {
+    std::lock_guard<std::mutex> g(gHookMutex);
+    gHook = std::move(hook);
+}
+
+size_t liveDeviceBytes() { return gLiveBytes.load(); }
+
+void DeviceMem::alloc(size_t bytes) {
+    release();
+    if (bytes == 0) return;
+    {
+        std::lock_guard<std::mutex> g(gHookMutex);
+        if (gHook && !gHook(bytes)) {
+            throw CudaError(cudaErrorMemoryAllocation,
+                            "device allocation of " + std::to_string(bytes) + " bytes refused by allocation hook");
+        }
+    }
+    void* p = nullptr;
+    const cudaError_t e = cudaMalloc(&p, bytes);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        throw CudaError(e, "cudaMalloc(" + std::to_string(bytes) + ") failed: " + cudaGetErrorString(e));
+    }
+    p_ = p;
+    n_ = bytes;
+    gLiveBytes += bytes;
+}
+
+void DeviceMem::release() {
+    if (p_) {
+        cudaFree(p_);
+        gLiveBytes -= n_;
+    }
+    p_ = nullptr;
+    n_ = 0;
+}
+
+DerivedArrays computeDerived(const HostIndex& idx) {
+    const uint64_t D = idx.D, H = idx.height;
+    DerivedArrays out;
+    out.cbeg.resize(H - 1);
+    out.ccnt.resize(H - 1);
+    out.leaf.resize(H - 1);
+    out.radRef.resize(H - 1);
+    out.radSub.resize(H - 1);
+
+    auto origOf = [&](uint64_t m, uint64_t pos) -> uint64_t {
+        return (m == 0) ? idx.coarsest.ids[pos] : idx.maps[m][pos];
+    };
+    // Position of each node of mesh m given its original id.
+    std::vector<std::vector<uint64_t>> posOf(H);
+    for (uint64_t m = 0; m + 1 < H; ++m) {
+        const uint64_t n = idx.meshCount(m);
+        posOf[m].resize(n);
+        for (uint64_t s = 0; s < n; ++s) posOf[m][origOf(m, s)] = s;
+    }
+    for (uint64_t m = 0; m + 1 < H; ++m) {
+        const uint64_t n = idx.meshCount(m);
+        const PTensor& P = idx.pTensors[m];
+        out.cbeg[m].resize(n);
+        out.ccnt[m].resize(n);
+        out.radRef[m].resize(n);
+        for (uint64_t s = 0; s < n; ++s) {
+            const uint64_t o = origOf(m, s);
+            out.cbeg[m][s] = static_cast<uint32_t>(P.colRes[o]);
+            out.ccnt[m][s] = static_cast<uint32_t>(P.colRes[o + 1] - P.colRes[o]);
+            out.radRef[m][s] = idx.radius[m][o];
+        }
+    }
+
+    // Decoded coordinates of every mesh in position order, and each node's parent position.
+    std::vector<std::vector<double>> dec(H);
+    std::vector<std::vector<uint32_t>> parent(H);
+    dec[0] = idx.coarsest.vals;
+    for (uint64_t m = 0; m + 1 < H; ++m) {
+        const PTensor& P = idx.pTensors[m];
+        dec[m + 1].resize(idx.meshCount(m + 1) * D);
+        parent[m + 1].resize(idx.meshCount(m + 1));
+        const int64_t cols = static_cast<int64_t>(P.cols);
+#pragma omp parallel for schedule(static)
+        for (int64_t o = 0; o < cols; ++o) {
+            const uint64_t ppos = posOf[m][o];
+            const double* x = &dec[m][ppos * D];
+            for (uint64_t j = P.colRes[o]; j < P.colRes[o + 1]; ++j) {
+                parent[m + 1][j] = static_cast<uint32_t>(ppos);
+                for (uint64_t d = 0; d < D; ++d) dec[m + 1][j * D + d] = P.vals[j * D + d] * x[d];
+            }
+        }
+    }
+
+    // Subtree radius and leaf count: walk every finest point up to the root. The finest
+    // clusters (mesh H-2) own their points directly, so they are done cluster by cluster; the
+    // small upper meshes use per-thread partial maxima.
+    std::vector<std::vector<double>> R(H - 1);
+    std::vector<std::vector<uint64_t>> C(H - 1);
+    for (uint64_t m = 0; m + 1 < H; ++m) {
+        R[m].assign(idx.meshCount(m), 0.0);
+        C[m].assign(idx.meshCount(m), 0);
+    }
+    {
+        const uint64_t m = H - 2;
+        const int64_t n = static_cast<int64_t>(idx.meshCount(m));
+        const PTensor& P = idx.pTensors[m];
+#pragma omp parallel for schedule(static)
+        for (int64_t s = 0; s < n; ++s) {
+            const uint64_t o = origOf(m, s);
+            const double* c = &dec[m][s * D];
+            double best = 0.0;
+            for (uint64_t j = P.colRes[o]; j < P.colRes[o + 1]; ++j) {
+                const double* x = &dec[H - 1][j * D];
+                double sum = 0.0;
+                for (uint64_t d = 0; d < D; ++d) {
+                    const double diff = c[d] - x[d];
+                    sum += diff * diff;
+                }
+                best = std::max(best, std::sqrt(sum));
+            }
+            R[m][s] = best;
+            C[m][s] = P.colRes[o + 1] - P.colRes[o];
+        }
+    }
+    if (H >= 3) {
+        const int nt = omp_get_max_threads();
+        std::vector<std::vector<std::vector<double>>> partR(nt);
+        std::vector<std::vector<std::vector<uint64_t>>> partC(nt);
+        const int64_t nLeaf = static_cast<int64_t>(idx.meshCount(H - 1));
+#pragma omp parallel
+        {
+            const int t = omp_get_thread_num();
+            auto& pr = partR[t];
+            auto& pc = partC[t];
+            pr.resize(H - 2);
+            pc.resize(H - 2);
+            for (uint64_t m = 0; m + 2 < H; ++m) {
+                pr[m].assign(idx.meshCount(m), 0.0);
+                pc[m].assign(idx.meshCount(m), 0);
+            }
+#pragma omp for schedule(static)
+            for (int64_t leafPos = 0; leafPos < nLeaf; ++leafPos) {
+                const double* x = &dec[H - 1][leafPos * D];
+                uint64_t pos = parent[H - 1][leafPos];  // mesh H-2
+                for (uint64_t m = H - 2; m > 0; --m) {
+                    pos = parent[m][pos];  // now in mesh m-1
+                    const double* c = &dec[m - 1][pos * D];
+                    double sum = 0.0;
+                    for (uint64_t d = 0; d < D; ++d) {
+                        const double diff = c[d] - x[d];
+                        sum += diff * diff;
+                    }
+                    pr[m - 1][pos] = std::max(pr[m - 1][pos], std::sqrt(sum));
+                    pc[m - 1][pos] += 1;
+                }
+            }
+        }
+        for (int t = 0; t < nt; ++t) {
+            if (partR[t].empty()) continue;
+            for (uint64_t m = 0; m + 2 < H; ++m) {
+                for (uint64_t s = 0; s < idx.meshCount(m); ++s) {
+                    R[m][s] = std::max(R[m][s], partR[t][m][s]);
+                    C[m][s] += partC[t][m][s];
+                }
+            }
+        }
+    }
+    for (uint64_t m = 0; m + 1 < H; ++m) {
+        const uint64_t n = idx.meshCount(m);
+        out.radSub[m].resize(n);
+        out.leaf[m].resize(n);
+        for (uint64_t s = 0; s < n; ++s) {
+            out.radSub[m][s] = R[m][s] * (1.0 + kSubRadiusRelSlack) + kSubRadiusAbsSlack;
+            out.leaf[m][s] = static_cast<uint32_t>(C[m][s]);
+        }
+    }
+    return out;
+}
+
+std::unique_ptr<DeviceIndex> buildDeviceIndex(const HostIndex& idx, const DerivedArrays& der, cudaStream_t s) {
+    auto di = std::make_unique<DeviceIndex>();
+    di->D = idx.D;
+    di->height = idx.height;
+    di->intervals = idx.intervals;
+    di->meshCount.resize(idx.height);
+    for (uint64_t m = 0; m < idx.height; ++m) di->meshCount[m] = idx.meshCount(m);
+
+    di->coarseVals = upload(idx.coarsest.vals, s);
+    di->coarseIds = upload(idx.coarsest.ids, s);
+    di->pvals.resize(idx.intervals);
+    di->colBeg.resize(idx.intervals);
+    di->colCnt.resize(idx.intervals);
+    di->radOrig.resize(idx.intervals);
+    for (uint64_t l = 0; l < idx.intervals; ++l) {
+        const PTensor& P = idx.pTensors[l];
+        di->pvals[l] = upload(P.vals, s);
+        std::vector<uint32_t> b(P.cols), c(P.cols);
+        for (uint64_t o = 0; o < P.cols; ++o) {
+            b[o] = static_cast<uint32_t>(P.colRes[o]);
+            c[o] = static_cast<uint32_t>(P.colRes[o + 1] - P.colRes[o]);
+        }
+        di->colBeg[l] = upload(b, s);
+        di->colCnt[l] = upload(c, s);
+        di->radOrig[l] = upload(idx.radius[l], s);
+        TBLAEQ_CUDA(cudaStreamSynchronize(s));
+    }
+    di->maps.resize(idx.height);
+    for (uint64_t m = 1; m < idx.height; ++m) di->maps[m] = upload(idx.maps[m], s);
+    // The finest map doubles as the final-id map of the fused traversal.
+    di->cbeg.resize(idx.height - 1);
+    di->ccnt.resize(idx.height - 1);
+    di->leaf.resize(idx.height - 1);
+    di->radRef.resize(idx.height - 1);
+    di->radSub.resize(idx.height - 1);
+    for (uint64_t m = 0; m + 1 < idx.height; ++m) {
+        di->cbeg[m] = upload(der.cbeg[m], s);
+        di->ccnt[m] = upload(der.ccnt[m], s);
+        di->leaf[m] = upload(der.leaf[m], s);
+        di->radRef[m] = upload(der.radRef[m], s);
+        di->radSub[m] = upload(der.radSub[m], s);
+    }
+    TBLAEQ_CUDA(cudaStreamSynchronize(s));
+    return di;
+}
+
+size_t DeviceIndex::deviceBytes() const {
+    size_t t = coarseVals.bytes() + finestMap.bytes() + coarseIds.bytes();
+    for (auto* v : {&pvals, &cbeg, &ccnt, &leaf, &radRef, &radSub, &colBeg, &colCnt, &radOrig, &maps})
+        for (auto& m : *v) t += m.bytes();
+    return t;
+}
+
+}  // namespace tblaeq

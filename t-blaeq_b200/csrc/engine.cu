@@ -1,0 +1,397 @@
+// Batched traversal engine (range queries; see engine.hpp).
+#include "engine.hpp"
+
+#include <algorithm>
+
+namespace tblaeq {
+
+namespace {
+size_t align256(size_t v) { return (v + 255) & ~size_t(255); }
+}  // namespace
+
+BatchEngine::BatchEngine(const DeviceIndex& di, cudaStream_t stream)
+    : di_(di), stream_(stream), tile_(expandTile(static_cast<int>(di.D))) {}
+
+BatchEngine::~BatchEngine() {
+    dropGraph();
+    for (cudaEvent_t e : events_) cudaEventDestroy(e);
+}
+
+void BatchEngine::dropGraph() {
+    if (graphExec_) cudaGraphExecDestroy(graphExec_);
+    graphExec_ = nullptr;
+    graphKey_ = GraphKey{};
+}
+
+void BatchEngine::setTiming(bool on) {
+    timing_ = on;
+    if (on && events_.empty()) {
+        events_.resize(static_cast<size_t>(di_.height) + 3);
+        for (auto& e : events_) TBLAEQ_CUDA(cudaEventCreate(&e));
+    }
+}
+
+std::vector<float> BatchEngine::stageTimes() {
+    std::vector<float> t;
+    if (!timing_ || events_.empty()) return t;
+    TBLAEQ_CUDA(cudaEventSynchronize(events_.back()));
+    for (size_t i = 0; i + 1 < events_.size(); ++i) {
+        float ms = 0.f;
+        TBLAEQ_CUDA(cudaEventElapsedTime(&ms, events_[i], events_[i + 1]));
+        t.push_back(ms);
+    }
+    return t;
+}
+
+void BatchEngine::levelCounts(std::vector<uint64_t>& entries, std::vector<uint64_t>& items, uint64_t& results) {
+    const int H = static_cast<int>(di_.height);
+    std::vector<uint32_t> h((H + 2) * 2);
+    TBLAEQ_CUDA(cudaMemcpyAsync(h.data(), hdrPtr(0), h.size() * 4, cudaMemcpyDeviceToHost, stream_));
+    TBLAEQ_CUDA(cudaStreamSynchronize(stream_));
+    entries.clear();
+    items.clear();
+    for (int lv = 0; lv < H; ++lv) {
+        entries.push_back(h[2 * lv]);
+        items.push_back(h[2 * lv + 1]);
+    }
+    results = h[2 * H];
+}
+
+uint64_t BatchEngine::lastTotal(uint32_t nq) {
+    uint64_t total = 0;
+    TBLAEQ_CUDA(cudaMemcpyAsync(&total, offsets_.as<uint64_t>() + nq, 8, cudaMemcpyDeviceToHost, stream_));
+    TBLAEQ_CUDA(cudaStreamSynchronize(stream_));
+    return total;
+}
+
+size_t BatchEngine::workspaceBytes() const {
+    size_t t = zeroBlock_.bytes() + offsets_.bytes() + resIds_.bytes() + resVals_.bytes() + resQ_.bytes() +
+               resDist_.bytes();
+    for (const auto& f : f_) t += f.q.bytes() + f.node.bytes() + f.cbeg.bytes() + f.cpre.bytes() + f.x.bytes() +
+                                  f.tileStart.bytes();
+    return t;
+}
+
+void BatchEngine::reserve(const EngineCaps& want, uint32_t nq, unsigned flags) {
+    const uint64_t H = di_.height, D = di_.D;
+    const bool wantVals = (flags & kWantVals) != 0;
+    EngineCaps c = caps_;
+    bool growF = false, growR = false, growZ = false;
+    if (want.entries > c.entries || f_[0].q.bytes() == 0) {
+        c.entries = std::max(c.entries, want.entries);
+        growF = true;
+    }
+    // One root entry per query must fit as well.
+    if (nq > c.entries) {
+        c.entries = nq;
+        growF = true;
+    }
+    if (want.items > c.items || f_[0].tileStart.bytes() == 0) {
+        c.items = std::max(c.items, want.items);
+        growF = true;
+        growZ = true;
+    }
+    const uint64_t rootItems = static_cast<uint64_t>(nq) * di_.meshCount[0];
+    if (rootItems > c.items) {
+        c.items = rootItems;
+        growF = true;
+        growZ = true;
+    }
+    if (want.results > c.results || resIds_.bytes() == 0 || (wantVals && !haveVals_)) {
+        c.results = std::max(c.results, want.results);
+        growR = true;
+    }
+    if (nq > qcap_ || zeroBlock_.bytes() == 0) growZ = true;
+    if (c.entries > 0xffffffffull || c.items > 0xffffffffull || c.results > 0xffffffffull)
+        throw CudaError(cudaErrorMemoryAllocation, "batch exceeds 32-bit traversal capacities; split the batch");
+    if (growF || growR || growZ) dropGraph();  // captured launches hold the old buffer addresses
+
+    if (growF) {
+        const uint64_t tileCap = c.items / tile_ + 2;
+        for (auto& f : f_) {
+            f.q.alloc(c.entries * 4);
+            f.node.alloc(c.entries * 4);
+            f.cbeg.alloc(c.entries * 4);
+            f.cpre.alloc(c.entries * 4);
+            f.x.alloc(c.entries * D * 8);
+            f.tileStart.alloc(tileCap * 4);
+        }
+        tileCap_ = tileCap;
+    }
+    if (growR) {
+        resIds_.alloc(c.results * 8);
+        resQ_.alloc(c.results * 4);
+        resDist_.alloc(c.results * 8);
+        if (wantVals || haveVals_) {
+            resVals_.alloc(c.results * D * 8);
+            haveVals_ = true;
+        }
+    }
+    if (growZ) {
+        qcap_ = std::max(qcap_, nq);
+        size_t off = 0;
+        offDesc_ = off;
+        off = align256(off + (H + 1) * tileCap_ * 8);
+        offTickets_ = off;
+        off = align256(off + (H + 1) * 4);
+        offStatus_ = off;
+        off = align256(off + 4);
+        offHdr_ = off;
+        off = align256(off + (H + 2) * 2 * 4);
+        offQcount_ = off;
+        off = align256(off + static_cast<size_t>(qcap_) * 4);
+        offLevels_ = off;
+        off = align256(off + static_cast<size_t>(di_.intervals) * qcap_ * 4);
+        zeroBytes_ = off;
+        zeroBlock_.alloc(zeroBytes_);
+        offsets_.alloc((static_cast<size_t>(qcap_) + 1) * 8);
+    }
+    caps_ = c;
+}
+
+uint32_t* BatchEngine::hdrPtr(int level) const {
+    return reinterpret_cast<uint32_t*>(zeroBlock_.as<char>() + offHdr_) + 2 * level;
+}
+
+FrontierIn BatchEngine::inView(int b, uint32_t* hdr) const {
+    const FrontierBufs& f = f_[b];
+    return FrontierIn{f.q.as<uint32_t>(), f.cbeg.as<uint32_t>(), f.cpre.as<uint32_t>(), f.x.as<double>(),
+                      f.tileStart.as<uint32_t>(), hdr};
+}
+
+FrontierOut BatchEngine::outView(int b, uint32_t* hdr) const {
+    const FrontierBufs& f = f_[b];
+    return FrontierOut{f.q.as<uint32_t>(),    f.node.as<uint32_t>(),     f.cbeg.as<uint32_t>(),
+                       f.cpre.as<uint32_t>(), f.x.as<double>(),          f.tileStart.as<uint32_t>(),
+                       hdr,                   static_cast<uint32_t>(caps_.entries), static_cast<uint32_t>(tileCap_)};
+}
+
+void BatchEngine::enqueueRange(const double* dBoxes, uint32_t nq, int mode, unsigned flags) {
+    if (!(flags & kUseGraph)) {
+        enqueueLaunches(dBoxes, nq, mode, flags);
+        return;
+    }
+    const GraphKey key{dBoxes, nq, mode, flags & ~kUseGraph, timing_};
+    if (!graphExec_ || !(key == graphKey_)) {
+        dropGraph();
+        cudaGraph_t g = nullptr;
+        TBLAEQ_CUDA(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal));
+        try {
+            enqueueLaunches(dBoxes, nq, mode, flags);
+        } catch (...) {
+            cudaStreamEndCapture(stream_, &g);
+            if (g) cudaGraphDestroy(g);
+            throw;
+        }
+        TBLAEQ_CUDA(cudaStreamEndCapture(stream_, &g));
+        const cudaError_t e = cudaGraphInstantiate(&graphExec_, g, 0);
+        cudaGraphDestroy(g);
+        if (e != cudaSuccess) {
+            graphExec_ = nullptr;
+            throw CudaError(e, std::string("cudaGraphInstantiate failed: ") + cudaGetErrorString(e));
+        }
+        graphKey_ = key;
+    }
+    TBLAEQ_CUDA(cudaGraphLaunch(graphExec_, stream_));
+}
+
+void BatchEngine::enqueueLaunches(const double* dBoxes, uint32_t nq, int mode, unsigned flags) {
+    const int H = static_cast<int>(di_.height);
+    const int D = static_cast<int>(di_.D);
+    char* z = zeroBlock_.as<char>();
+    auto* desc = reinterpret_cast<unsigned long long*>(z + offDesc_);
+    auto* tickets = reinterpret_cast<uint32_t*>(z + offTickets_);
+    auto* status = reinterpret_cast<uint32_t*>(z + offStatus_);
+    auto* qcount = reinterpret_cast<uint32_t*>(z + offQcount_);
+    auto* levels = reinterpret_cast<uint32_t*>(z + offLevels_);
+    const bool wantLevels = (flags & kWantLevels) != 0;
+
+    if (timing_) TBLAEQ_CUDA(cudaEventRecord(events_[0], stream_));
+    TBLAEQ_CUDA(cudaMemsetAsync(z, 0, zeroBytes_, stream_));
+    const FrontierBufs& r0 = f_[0];
+    launchRootFrontier(r0.q.as<uint32_t>(), r0.cbeg.as<uint32_t>(), r0.cpre.as<uint32_t>(), r0.x.as<double>(),
+                       r0.tileStart.as<uint32_t>(), hdrPtr(0), nq, static_cast<uint32_t>(di_.meshCount[0]), D, tile_,
+                       stream_);
+    if (timing_) TBLAEQ_CUDA(cudaEventRecord(events_[1], stream_));
+    int buf = 0;
+    for (int m = 0; m < H; ++m) {
+        ExpandArgs a{};
+        a.in = inView(buf, hdrPtr(m));
+        a.child.rows = (m == 0) ? di_.coarseVals.as<double>() : di_.pvals[m - 1].as<double>();
+        a.query.boxes = dBoxes;
+        a.scratch.desc = desc + static_cast<size_t>(m) * tileCap_;
+        a.scratch.ticket = tickets + m;
+        a.scratch.status = status;
+        a.scratch.levelItems = (wantLevels && m > 0) ? levels + static_cast<size_t>(m - 1) * nq : nullptr;
+        a.D = D;
+        a.useFma = 1;
+        if (m < H - 1) {
+            a.child.rad = (mode == kModeExact) ? di_.radSub[m].as<double>() : di_.radRef[m].as<double>();
+            a.child.ncbeg = di_.cbeg[m].as<uint32_t>();
+            a.child.ncnt = di_.ccnt[m].as<uint32_t>();
+            a.fout = outView(1 - buf, hdrPtr(m + 1));
+            launchExpand(a, kPredRangeRadius, false, 0, stream_);
+            buf = 1 - buf;
+        } else {
+            a.child.outMap = di_.maps[H - 1].as<uint64_t>();
+            a.rout.ids = resIds_.as<uint64_t>();
+            a.rout.vals = (flags & kWantVals) ? resVals_.as<double>() : nullptr;
+            a.rout.qcount = qcount;
+            a.rout.hdr = hdrPtr(H);
+            a.rout.cap = static_cast<uint32_t>(caps_.results);
+            launchExpand(a, (mode == kModeExact) ? kPredRangeBox : kPredAll, true, 0, stream_);
+        }
+        if (timing_) TBLAEQ_CUDA(cudaEventRecord(events_[2 + m], stream_));
+    }
+    launchExclusiveScan(qcount, offsets_.as<uint64_t>(), nq, stream_);
+    if (timing_) TBLAEQ_CUDA(cudaEventRecord(events_[2 + H], stream_));
+}
+
+uint32_t BatchEngine::status() {
+    uint32_t st = 0;
+    TBLAEQ_CUDA(cudaMemcpyAsync(&st, zeroBlock_.as<char>() + offStatus_, 4, cudaMemcpyDeviceToHost, stream_));
+    TBLAEQ_CUDA(cudaStreamSynchronize(stream_));
+    return st;
+}
+
+void BatchEngine::growFromHeaders() {
+    const int H = static_cast<int>(di_.height);
+    std::vector<uint32_t> h((H + 2) * 2);
+    TBLAEQ_CUDA(cudaMemcpyAsync(h.data(), hdrPtr(0), h.size() * 4, cudaMemcpyDeviceToHost, stream_));
+    TBLAEQ_CUDA(cudaStreamSynchronize(stream_));
+    EngineCaps want = caps_;
+    bool grew = false;
+    for (int lv = 1; lv < H; ++lv) {
+        const uint64_t cnt = h[2 * lv], items = h[2 * lv + 1];
+        if (cnt > caps_.entries) {
+            want.entries = std::max<uint64_t>(want.entries, cnt + cnt / 4 + 1024);
+            grew = true;
+        }
+        if (items > caps_.items) {
+            want.items = std::max<uint64_t>(want.items, items + items / 4 + 4096);
+            grew = true;
+        }
+    }
+    const uint64_t res = h[2 * H];
+    if (res > caps_.results) {
+        want.results = std::max<uint64_t>(want.results, res + res / 4 + 4096);
+        grew = true;
+    }
+    if (!grew) {
+        want.entries *= 2;
+        want.items *= 2;
+        want.results *= 2;
+    }
+    reserve(want, qcap_, haveVals_ ? kWantVals : 0);
+}
+
+BatchOutput BatchEngine::output(uint32_t nq, unsigned flags) const {
+    BatchOutput o;
+    o.nq = nq;
+    o.offsets = offsets_.as<uint64_t>();
+    o.ids = resIds_.as<uint64_t>();
+    o.vals = (flags & kWantVals) ? resVals_.as<double>() : nullptr;
+    o.levelItems = (flags & kWantLevels) ? reinterpret_cast<const uint32_t*>(zeroBlock_.as<char>() + offLevels_)
+                                         : nullptr;
+    return o;
+}
+
+BatchOutput BatchEngine::runRange(const double* dBoxes, uint32_t nq, int mode, unsigned flags) {
+    reserve(caps_, nq, flags);
+    for (int attempt = 0; attempt < 16; ++attempt) {
+        enqueueRange(dBoxes, nq, mode, flags);
+        const uint32_t st = status();
+        if (st & (kStatusLookbackTimeout | kStatusWindowOverflow)) {
+            throw CudaError(cudaErrorLaunchTimeout, "traversal kernel reported status " + std::to_string(st));
+        }
+        if (st == 0) {
+            BatchOutput o = output(nq, flags);
+            o.total = lastTotal(nq);
+            return o;
+        }
+        growFromHeaders();
+    }
+    throw CudaError(cudaErrorMemoryAllocation, "traversal workspace did not converge after 16 growth steps");
+}
+
+}  // namespace tblaeq
+
+namespace tblaeq {
+
+uint64_t BatchEngine::runGridLevel(int l, const uint64_t* dIds, const double* dVals, uint64_t p, bool range,
+                                   const double* dQuery, const uint8_t* dMask, uint64_t* outIds, double* outVals,
+                                   uint64_t outCap) {
+    if (p == 0) return 0;
+    if (p > 0xffffffffull || outCap > 0xffffffffull) throw std::invalid_argument("grid too large for one level");
+    const int D = static_cast<int>(di_.D);
+    EngineCaps want = caps_;
+    want.entries = std::max<uint64_t>(want.entries, 1);
+    want.items = std::max<uint64_t>(want.items, p);
+    reserve(want, 1, 0);
+    // The grid's own tile starts cover p items; the survivors' children are bounded by outCap.
+    if (outCap > caps_.items) {
+        want.items = outCap;
+        reserve(want, 1, 0);
+    }
+    if (p > caps_.entries) {
+        want.entries = p;
+        reserve(want, 1, 0);
+    }
+    char* z = zeroBlock_.as<char>();
+    auto* desc = reinterpret_cast<unsigned long long*>(z + offDesc_);
+    auto* tickets = reinterpret_cast<uint32_t*>(z + offTickets_);
+    auto* statusPtr = reinterpret_cast<uint32_t*>(z + offStatus_);
+    for (int attempt = 0; attempt < 2; ++attempt) {
+        TBLAEQ_CUDA(cudaMemsetAsync(z, 0, zeroBytes_, stream_));
+        const FrontierBufs& r0 = f_[0];
+        launchRootFrontier(r0.q.as<uint32_t>(), r0.cbeg.as<uint32_t>(), r0.cpre.as<uint32_t>(), r0.x.as<double>(),
+                           r0.tileStart.as<uint32_t>(), hdrPtr(0), 1, static_cast<uint32_t>(p), D, tile_, stream_);
+        ExpandArgs a{};
+        a.in = inView(0, hdrPtr(0));
+        a.child.rows = dVals;
+        a.child.keys = dIds;
+        a.child.rad = di_.radOrig[l].as<double>();
+        a.child.ncbeg = di_.colBeg[l].as<uint32_t>();
+        a.child.ncnt = di_.colCnt[l].as<uint32_t>();
+        a.child.mask = dMask;
+        a.query.boxes = dQuery;
+        a.fout = outView(1, hdrPtr(1));
+        a.scratch.desc = desc;
+        a.scratch.ticket = tickets;
+        a.scratch.status = statusPtr;
+        a.D = D;
+        a.useFma = 1;
+        launchExpand(a, range ? kPredRangeRadius : kPredMask, false, 0, stream_);
+
+        ExpandArgs b{};
+        b.in = inView(1, hdrPtr(1));
+        b.child.rows = di_.pvals[l].as<double>();
+        b.child.outMap = di_.maps[l + 1].as<uint64_t>();
+        b.rout.ids = outIds;
+        b.rout.vals = outVals;
+        b.rout.hdr = hdrPtr(2);
+        b.rout.cap = static_cast<uint32_t>(outCap);
+        b.scratch.desc = desc + tileCap_;
+        b.scratch.ticket = tickets + 1;
+        b.scratch.status = statusPtr;
+        b.D = D;
+        b.useFma = 1;
+        launchExpand(b, kPredAll, true, 0, stream_);
+
+        const uint32_t st = status();
+        if (st & (kStatusLookbackTimeout | kStatusWindowOverflow))
+            throw CudaError(cudaErrorLaunchTimeout, "traversal kernel reported status " + std::to_string(st));
+        uint32_t h[6];
+        TBLAEQ_CUDA(cudaMemcpyAsync(h, hdrPtr(0), sizeof(h), cudaMemcpyDeviceToHost, stream_));
+        TBLAEQ_CUDA(cudaStreamSynchronize(stream_));
+        if (st == 0) return h[4];
+        if (st & kStatusOverflowEntries && h[4] > outCap)
+            throw CudaError(cudaErrorMemoryAllocation, "level output exceeds its buffer");
+        want.entries = std::max<uint64_t>(caps_.entries, h[2] + 1);
+        want.items = std::max<uint64_t>(caps_.items, static_cast<uint64_t>(h[3]) + 1);
+        reserve(want, 1, 0);
+    }
+    throw CudaError(cudaErrorMemoryAllocation, "per-level workspace did not converge");
+}
+
+}  // namespace tblaeq

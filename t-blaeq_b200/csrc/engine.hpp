@@ -1,0 +1,123 @@
+// Batched traversal engine: runs many queries through the hierarchy together, one `expand`
+// launch per mesh, with all intermediate state on the device.
+#pragma once
+
+#include <cstdint>
+#include <memory>
+#include <vector>
+
+#include "device_index.hpp"
+#include "traverse.cuh"
+
+namespace tblaeq {
+
+enum QueryMode : int {
+    kModeRefParity = 0,  // the reference's candidate sets (child radii, STEP, no final filter)
+    kModeExact = 1,      // subtree radii + exact final filter / top-K
+};
+
+enum BatchFlags : unsigned {
+    kWantVals = 1u << 0,    // also return decoded coordinates of every result
+    kWantLevels = 1u << 1,  // per-query generated-children count per level
+    kUseGraph = 1u << 2,    // replay the batch's launches from a captured CUDA graph
+};
+
+struct BatchOutput {
+    uint32_t nq = 0;
+    uint64_t total = 0;              // number of results
+    const uint64_t* offsets = nullptr;  // device, nq + 1
+    const uint64_t* ids = nullptr;      // device, total
+    const double* vals = nullptr;       // device, total * D (kWantVals)
+    const double* dist2 = nullptr;      // device, total (KNN)
+    const uint32_t* levelItems = nullptr;  // device, intervals * nq (kWantLevels), [l * nq + q]
+};
+
+struct EngineCaps {
+    uint64_t entries = 1u << 16;  // frontier entries per level
+    uint64_t items = 1u << 22;    // work items per level (children of one frontier)
+    uint64_t results = 1u << 20;  // final results per batch
+};
+
+class BatchEngine {
+public:
+    BatchEngine(const DeviceIndex& di, cudaStream_t stream);
+    ~BatchEngine();
+    BatchEngine(const BatchEngine&) = delete;
+    BatchEngine& operator=(const BatchEngine&) = delete;
+
+    // Range batch: dBoxes = nq rows of lo[D] then hi[D] (device). Blocks until done.
+    BatchOutput runRange(const double* dBoxes, uint32_t nq, int mode, unsigned flags);
+
+    // Enqueue a range batch without synchronising (capacities must already suffice; used for
+    // CUDA-graph capture and timing). check() afterwards reports overflow / timeouts.
+    void enqueueRange(const double* dBoxes, uint32_t nq, int mode, unsigned flags);
+    // Returns the device status bits of the last enqueued batch (synchronises the stream).
+    uint32_t status();
+    // Total results of the last batch (synchronises the stream).
+    uint64_t lastTotal(uint32_t nq);
+
+    // (entries, items) of every frontier header of the last batch, and the result count.
+    void levelCounts(std::vector<uint64_t>& entries, std::vector<uint64_t>& items, uint64_t& results);
+
+    // Per-stage event timing of every batch (memset+root, one stage per expand, scan).
+    void setTiming(bool on);
+    // Elapsed milliseconds of each stage of the last batch; requires setTiming(true).
+    std::vector<float> stageTimes();
+    BatchOutput output(uint32_t nq, unsigned flags) const;
+
+    // Per-level plugin step (reference semantics for one query at interval l): keep the grid entries
+    // whose pruning predicate holds (range: box distance vs the reference radius; KNN: dMask), then
+    // expand the survivors through P_l and Map_{l+1} into outIds/outVals (capacity outCap).
+    // Returns the number of output entries. dQuery is the device box (lo|hi) for range queries.
+    uint64_t runGridLevel(int l, const uint64_t* dIds, const double* dVals, uint64_t p, bool range,
+                          const double* dQuery, const uint8_t* dMask, uint64_t* outIds, double* outVals,
+                          uint64_t outCap);
+
+    // Reserve workspace for at least these capacities and this many queries.
+    void reserve(const EngineCaps& caps, uint32_t nq, unsigned flags);
+    const EngineCaps& caps() const { return caps_; }
+    size_t workspaceBytes() const;
+    int launchesPerBatch() const { return static_cast<int>(di_.height) + 2; }
+    cudaStream_t stream() const { return stream_; }
+
+private:
+    struct FrontierBufs {
+        DeviceMem q, node, cbeg, cpre, x, tileStart;
+    };
+    const DeviceIndex& di_;
+    cudaStream_t stream_;
+    int tile_;
+    EngineCaps caps_{};
+    uint32_t qcap_ = 0;
+    bool haveVals_ = false;
+    FrontierBufs f_[2];
+    DeviceMem resIds_, resVals_, resQ_, resDist_;
+    DeviceMem zeroBlock_;  // desc | tickets | status | hdrs | qcount | levelItems
+    DeviceMem offsets_;
+    size_t zeroBytes_ = 0;
+    // offsets into zeroBlock_
+    size_t offDesc_ = 0, offTickets_ = 0, offStatus_ = 0, offHdr_ = 0, offQcount_ = 0, offLevels_ = 0;
+    uint64_t tileCap_ = 0;
+
+    void growFromHeaders();
+    void enqueueLaunches(const double* dBoxes, uint32_t nq, int mode, unsigned flags);
+    void dropGraph();
+    bool timing_ = false;
+    std::vector<cudaEvent_t> events_;
+    cudaGraphExec_t graphExec_ = nullptr;
+    struct GraphKey {
+        const double* boxes = nullptr;
+        uint32_t nq = 0;
+        int mode = -1;
+        unsigned flags = 0;
+        bool timing = false;
+        bool operator==(const GraphKey& o) const {
+            return boxes == o.boxes && nq == o.nq && mode == o.mode && flags == o.flags && timing == o.timing;
+        }
+    } graphKey_;
+    FrontierIn inView(int buf, uint32_t* hdr) const;
+    FrontierOut outView(int buf, uint32_t* hdr) const;
+    uint32_t* hdrPtr(int level) const;
+};
+
+}  // namespace tblaeq

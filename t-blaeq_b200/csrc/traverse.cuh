@@ -1,0 +1,125 @@
+// Level-synchronous traversal kernels for the T-BLAEQ hierarchy on sm_100a.
+//
+// One kernel, `expand`, does the whole per-level pipeline of the reference
+// (prune -> compact -> SpTSpM -> refactor, src/core/strategies/L0Strategy.cu:50-191) for every
+// query of a batch at once:
+//
+//   * work items are (frontier entry, child) pairs, laid out as a flat index space whose prefix
+//     over entries (`cpre`) was produced by the previous level; a tile of kTile items finds its
+//     entries through `tileStart` (also written by the producer), so no global search is needed;
+//   * each item rebuilds its child's coordinates y = P[j] (*) x_parent exactly like
+//     SpMSpVKernelAOS_v2 (src/Kernel/SpMSpV.cuh:47-67: one rounded multiply per dimension);
+//   * the item is kept or dropped by the predicate of the child's level (range box vs radius,
+//     a precomputed mask, or the exact final filter);
+//   * kept items are compacted in order (warp ballot / shuffle scans inside the tile, a
+//     single-pass decoupled look-back across tiles) and written either as the next frontier
+//     (with the next level's child prefix and tile starts) or as final result ids (Map applied,
+//     src/Query/Refactor.cu:10-16).
+//
+// Tiles are claimed through an atomic ticket by a persistent grid, so every tile a look-back
+// waits on belongs to a CTA that is already running; every spin is bounded and reports a
+// status bit instead of hanging.
+#pragma once
+
+#include <cstdint>
+
+#include "common.cuh"
+
+namespace tblaeq {
+
+constexpr int kThreads = 256;
+
+// Frontier in structure-of-arrays layout.
+struct FrontierIn {
+    const uint32_t* q;          // query slot of each entry
+    const uint32_t* cbeg;       // first child (row index into the child level)
+    const uint32_t* cpre;       // exclusive prefix of child counts over the frontier
+    const double* x;            // decoded coordinates, count * D
+    const uint32_t* tileStart;  // entry holding work item b * kTile
+    const uint32_t* hdr;        // [0] = entry count, [1] = total children
+};
+
+struct FrontierOut {
+    uint32_t* q;
+    uint32_t* node;             // child key (row index or original id) of the kept entry
+    uint32_t* cbeg;
+    uint32_t* cpre;
+    double* x;
+    uint32_t* tileStart;
+    uint32_t* hdr;              // written by the tile holding the last item
+    uint32_t cap;               // entry capacity
+    uint32_t tileCap;           // tileStart capacity
+};
+
+struct ResultOut {
+    uint64_t* ids;              // output ids (Map applied)
+    double* vals;               // optional decoded coordinates (count * D)
+    uint32_t* q;                // optional query slot per result
+    double* dist2;              // optional squared distance per result (KNN)
+    uint32_t* qcount;           // optional per-query result counts (atomic)
+    uint32_t* hdr;              // [0] = total results
+    uint32_t cap;
+};
+
+// The child level: rows to multiply, and the arrays of the child nodes themselves.
+struct ChildLevel {
+    const double* rows;         // row j: D factors (P-tensor row, or coordinates with x = 1)
+    const uint64_t* keys;       // optional key of row j into the node arrays (null: key = j)
+    const double* rad;          // pruning radius of the child node (by key)
+    const uint32_t* ncbeg;      // first grandchild of the child node (by key)
+    const uint32_t* ncnt;       // grandchild count of the child node (by key)
+    const uint8_t* mask;        // keep flags (by row) for kPredMask
+    const uint64_t* outMap;     // final output id of row j (null: id = key)
+};
+
+struct QueryArgs {
+    const double* boxes;        // range: per query lo[D] then hi[D]
+    const double* points;       // knn: per query point[D]
+    const double* tau;          // knn: per query distance bound (upper bound on the K-th NN distance)
+};
+
+struct Scratch {
+    unsigned long long* desc;   // look-back descriptors, one per tile, zeroed before launch
+    uint32_t* ticket;           // tile ticket counter, zeroed before launch
+    uint32_t* status;           // DeviceStatus bits
+    uint32_t* levelItems;       // optional: per-query count of generated children at this level
+};
+
+enum Pred : int {
+    kPredRangeRadius = 0,       // keep child if boxdist^2 <= rad^2 and it has children
+    kPredMask = 1,              // keep child if mask[row] (and it has children, frontier output)
+    kPredAll = 2,               // keep every child
+    kPredRangeBox = 3,          // keep point if lo <= y <= hi on every dimension
+    kPredKnnBound = 4,          // keep child if dist - rad <= tau (and it has children)
+    kPredKnnPoint = 5,          // keep point if dist2 <= tau^2 (records dist2)
+};
+
+struct ExpandArgs {
+    FrontierIn in;
+    ChildLevel child;
+    QueryArgs query;
+    FrontierOut fout;
+    ResultOut rout;
+    Scratch scratch;
+    int D;
+    int useFma;                 // accumulate squared distances with fma (reference kernels' contraction)
+};
+
+// Launch the expand kernel for dimension D with the given predicate; `toResult` selects the
+// result output (final level) instead of the next frontier. gridBlocks <= 0 picks a persistent
+// grid sized from the occupancy of the instantiation.
+void launchExpand(const ExpandArgs& a, int pred, bool toResult, int gridBlocks, cudaStream_t stream);
+
+// Tile size (work items per tile) used by every expand instantiation of dimension D.
+int expandTile(int D);
+
+// Builds a root frontier of `nq` entries, each with `nChildren` children starting at row 0 and
+// x = 1 (so the first expand reproduces the coarsest coordinates exactly). Capacities must hold
+// nq entries and ceil(nq*nChildren / tile) tile starts.
+void launchRootFrontier(uint32_t* q, uint32_t* cbeg, uint32_t* cpre, double* x, uint32_t* tileStart, uint32_t* hdr,
+                        uint32_t nq, uint32_t nChildren, int D, int tile, cudaStream_t stream);
+
+// offsets[q] = exclusive scan of counts[0..n), offsets[n] = total (single CTA).
+void launchExclusiveScan(const uint32_t* counts, uint64_t* offsets, uint32_t n, cudaStream_t stream);
+
+}  // namespace tblaeq

@@ -1,0 +1,114 @@
+"""The C-ABI library loads and exports every entry point include/tblaeq.h declares (CPU only),
+and host-side logic that needs no GPU: scheduler byte math, argument validation, query files."""
+import ctypes
+import os
+import re
+
+import numpy as np
+import pytest
+
+
+def _declared_functions(header):
+    text = open(header).read()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    return sorted(set(re.findall(r"\b(tblaeq_[a-z_0-9]+)\s*\(", text)))
+
+
+def test_every_declared_symbol_is_exported(tb):
+    lib = ctypes.CDLL(tb.LIB_PATH)
+    names = _declared_functions(tb.HEADER_PATH)
+    assert len(names) >= 15
+    missing = [n for n in names if not hasattr(lib, n)]
+    assert not missing, missing
+
+
+def test_abi_version(tb):
+    assert tb.lib().tblaeq_abi_version() == 1
+
+
+def test_null_arguments_are_rejected(tb):
+    lib = tb.lib()
+    assert lib.tblaeq_open(None, None) == 1
+    assert lib.tblaeq_info(None, None) == 1
+    assert lib.tblaeq_prepare(None, None, 0) == 1
+    assert b"null" in lib.tblaeq_last_error()
+
+
+def test_query_before_prepare_is_a_state_error(tb):
+    h = tb.QueryHandler.generate(2000, 3, 1.0, 100.0, False, 4, (10, 10, 10), 1, 3.0)
+    with pytest.raises(tb.TblaeqError) as e:
+        h.query_batch(tb.QueryType.RANGE, np.zeros((1, 6)))
+    assert e.value.code == 7
+    with pytest.raises(tb.TblaeqError) as e:
+        h.coarsest_grid()
+    assert e.value.code == 7
+
+
+def test_bad_policy_list(tb):
+    h = tb.QueryHandler.generate(2000, 3, 1.0, 100.0, False, 4, (10, 10, 10), 1, 3.0)
+    with pytest.raises(tb.TblaeqError) as e:
+        h.prepare_for_query([tb.LevelPolicy.L0])
+    assert e.value.code == 1
+
+
+def _restated_recommend(info_sizes, D, free):
+    """PolicyScheduler::recommend (src/core/MemoryPolicy.cu:100-177) restated for the test."""
+    sizes = info_sizes  # finest -> coarsest
+    intervals = len(sizes) - 1
+    budget = int(free * 0.85)
+    coarse_n = sizes[-1]
+    permanent = coarse_n * 8 + coarse_n * D * 8 + sum(sizes[intervals - m] * 8 for m in range(1, intervals + 1))
+    if budget <= permanent:
+        return [3] * intervals
+    budget -= permanent
+    out = []
+    for l in range(intervals):
+        nnz = sizes[intervals - (l + 1)]
+        col = sizes[intervals - l]
+        pv, rad, sp = nnz * D * 8, col * 8, 3 * nnz * 8
+        c0 = pv + rad + sp + pv
+        c2 = 2 * pv + sp
+        if budget >= c0:
+            out.append(0)
+            budget -= c0
+        elif budget >= c2:
+            out.append(2)
+        else:
+            out.append(3)
+    return out
+
+
+@pytest.mark.parametrize("free", [10 ** 3, 10 ** 5, 2 * 10 ** 6, 8 * 10 ** 6, 3 * 10 ** 7, 10 ** 10])
+def test_scheduler_matches_reference_byte_math(tb, free):
+    h = tb.QueryHandler.generate(50000, 4, 1.0, 100.0, False, 4, (10, 10, 10), 1, 3.0)
+    info = h.info()
+    got = [int(p) for p in h.recommend(free)]
+    assert got == _restated_recommend(info["meshSizes"], info["D"], free)
+
+
+def test_scheduler_degrades_level_by_level(tb):
+    h = tb.QueryHandler.generate(50000, 4, 1.0, 100.0, False, 4, (10, 10, 10), 1, 3.0)
+    assert [int(p) for p in h.recommend(10 ** 10)] == [0, 0, 0]
+    mixed = [int(p) for p in h.recommend(5 * 10 ** 6)]
+    assert mixed[0] == 0 and mixed[-1] in (2, 3)
+    assert [int(p) for p in h.recommend(10)] == [3, 3, 3]
+
+
+def test_query_file_roundtrip(tb, tmp_path):
+    rng = np.random.default_rng(0)
+    rows = rng.uniform(1, 100, (7, 10))
+    p = tmp_path / "q.txt"
+    tb.save_query_file(str(p), tb.QueryType.RANGE, rows, 5)
+    back, _ = tb.load_query_file(str(p), tb.QueryType.RANGE)
+    assert np.array_equal(back, rows)
+    bad = tmp_path / "bad.txt"
+    bad.write_text("2 3\n1 2 3\n")
+    with pytest.raises(ValueError):
+        tb.load_query_file(str(bad), tb.QueryType.RANGE)
+
+
+def test_alloc_failure_hook_is_clean_on_cpu(tb):
+    # Without a GPU the first device allocation happens in prepare; the hook must not leak state.
+    tb.lib().tblaeq_debug_fail_alloc_after(1)
+    tb.lib().tblaeq_debug_fail_alloc_after(0)
+    assert tb.lib().tblaeq_live_device_bytes() == 0

@@ -1,0 +1,185 @@
+"""GPU parity of the range path through the C ABI against the CPU oracle.
+
+* exact mode (batched and one query at a time) == FP64 brute force, bit-exact id sets;
+* ref-parity mode == the oracle's restatement of the reference traversal: same candidate ids and
+  the same per-level grid sizes (the reference's levelFineMeshSize);
+* the per-level plugin (IQueryStrategy::runLevel) returns the reference's grid, in the reference's
+  order, level by level;
+* edge cases: empty boxes, boxes outside the data, a box holding every point, tiny and large
+  batches (workspace growth), other dimensions (specialised and generic kernels).
+"""
+import ctypes
+
+import numpy as np
+import pytest
+
+from conftest import ids_by_query, oracle_from_handler
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def env(tb, oracle_mod, tmp_path_factory, cuda):
+    h = tb.QueryHandler.generate(200000, 5, 1.0, 100.0, False, 4, (40, 20, 10), 11, 2.2)
+    h.prepare_for_query(tb.LevelPolicy.L0)
+    o = oracle_from_handler(oracle_mod, h, tmp_path_factory.mktemp("idx"))
+    pts, ids = oracle_mod.decoded_points(o)
+    return h, o, pts, ids
+
+
+def _boxes(pts, n, seed, lo_frac=0.005, hi_frac=0.15):
+    rng = np.random.default_rng(seed)
+    ext = pts.max(0) - pts.min(0)
+    c = pts[rng.integers(0, len(pts), n)]
+    hw = np.exp(rng.uniform(np.log(lo_frac), np.log(hi_frac), c.shape)) * ext
+    return np.ascontiguousarray(np.concatenate([c - hw, c + hw], 1))
+
+
+def _batch_ids(tb, h, Q, mode, flags=0):
+    r = h.query_batch(tb.QueryType.RANGE, Q, mode, flags=flags)
+    offs = r.offsets.numpy()
+    ids = r.ids.numpy() if r.total else np.zeros(0, np.uint64)
+    return r, offs, ids
+
+
+def test_exact_batch_equals_brute_force(tb, env, oracle_mod):
+    h, o, pts, ids = env
+    Q = _boxes(pts, 300, 1)
+    r, offs, got = _batch_ids(tb, h, Q, tb.Mode.EXACT)
+    b = oracle_mod.brute_query(pts, ids, oracle_mod.RANGE, Q)
+    assert np.array_equal(offs, b.offsets)
+    for q, g in enumerate(ids_by_query(offs, got)):
+        assert np.array_equal(g, b.query(q)), q
+    assert b.offsets[-1] > 1000
+
+
+def test_exact_single_queries_equal_batch(tb, env):
+    """Each query's result is the same alone and inside a batch."""
+    h, o, pts, ids = env
+    Q = _boxes(pts, 40, 2)
+    r, offs, got = _batch_ids(tb, h, Q, tb.Mode.EXACT)
+    batch = ids_by_query(offs, got)
+    for q in range(len(Q)):
+        o1, i1, _ = h.query_batch_host(tb.QueryType.RANGE, Q[q:q + 1], tb.Mode.EXACT)
+        assert np.array_equal(np.sort(i1), batch[q])
+
+
+def test_ref_parity_batch_equals_oracle(tb, env, oracle_mod):
+    h, o, pts, ids = env
+    Q = _boxes(pts, 200, 3)
+    r, offs, got = _batch_ids(tb, h, Q, tb.Mode.REF_PARITY, flags=tb.WANT_LEVELS)
+    ref = oracle_mod.ref_query(o, oracle_mod.RANGE, Q, sorted_ids=False)
+    assert np.array_equal(offs, ref.offsets)
+    # Same order as the reference (survivor order, then column order), not only the same set.
+    assert np.array_equal(got, ref.ids)
+    levels = r.level_items.numpy().T.astype(np.uint64)
+    assert np.array_equal(levels, ref.level_sizes)
+
+
+def test_plugin_levels_match_reference_order(tb, env, oracle_mod):
+    """IQueryStrategy::runLevel on the device: grid after every level equals the reference's."""
+    h, o, pts, ids = env
+    Q = _boxes(pts, 12, 4)
+    ref = oracle_mod.ref_query(o, oracle_mod.RANGE, Q, sorted_ids=False)
+    D = 5
+    for q in range(len(Q)):
+        grid = h.coarsest_grid()
+        sizes = []
+        for l in range(3):
+            grid = h.run_level(l, grid, tb.QueryType.RANGE, lo=Q[q, :D], hi=Q[q, D:])
+            sizes.append(grid.nnz)
+        got_ids, got_vals = h.grid_arrays(grid)
+        assert np.array_equal(got_ids, ref.query(q)), q
+        assert sizes == list(ref.level_sizes[q])
+        # vals are the decoded coordinates of those ids
+        pos = np.argsort(o.maps[3])
+        assert np.array_equal(got_vals, pts[pos[got_ids.astype(np.int64)]])
+
+
+def test_query_batch_host_matches_device(tb, env):
+    h, o, pts, ids = env
+    Q = _boxes(pts, 64, 5)
+    r, offs, got = _batch_ids(tb, h, Q, tb.Mode.EXACT)
+    hoffs, hids, _ = h.query_batch_host(tb.QueryType.RANGE, Q, tb.Mode.EXACT)
+    assert np.array_equal(hoffs, offs) and np.array_equal(hids, got)
+
+
+def test_edge_boxes(tb, env, oracle_mod):
+    h, o, pts, ids = env
+    D = 5
+    lo, hi = pts.min(0), pts.max(0)
+    Q = np.stack([
+        np.concatenate([hi, lo]),                       # inverted box: empty
+        np.concatenate([hi + 10, hi + 20]),             # outside the data
+        np.concatenate([lo - 1, hi + 1]),               # every point
+        np.concatenate([pts[17], pts[17]]),             # a single point (degenerate box)
+        np.concatenate([lo - 50, lo - 40]),
+    ])
+    r, offs, got = _batch_ids(tb, h, Q, tb.Mode.EXACT)
+    b = oracle_mod.brute_query(pts, ids, oracle_mod.RANGE, Q)
+    assert np.array_equal(offs, b.offsets)
+    per = ids_by_query(offs, got)
+    assert len(per[0]) == 0 and len(per[1]) == 0 and len(per[4]) == 0
+    assert len(per[2]) == len(pts)
+    assert np.array_equal(per[2], np.arange(len(pts), dtype=np.uint64))
+    assert ids[17] in per[3]
+
+
+def test_empty_batch_and_single(tb, env):
+    h, o, pts, ids = env
+    r = h.query_batch(tb.QueryType.RANGE, np.zeros((0, 10)), tb.Mode.EXACT)
+    assert r.total == 0 and r.offsets.numpy().tolist() == [0]
+
+
+def test_large_results_force_workspace_growth(tb, env, oracle_mod):
+    h, o, pts, ids = env
+    Q = _boxes(pts, 48, 6, lo_frac=0.3, hi_frac=0.6)
+    r, offs, got = _batch_ids(tb, h, Q, tb.Mode.REF_PARITY)
+    ref = oracle_mod.ref_query(o, oracle_mod.RANGE, Q, sorted_ids=False)
+    assert ref.offsets[-1] > 2_000_000
+    assert np.array_equal(offs, ref.offsets) and np.array_equal(got, ref.ids)
+
+
+@pytest.mark.parametrize("D,ratios", [(2, (16, 8, 4)), (3, (10, 10, 10)), (6, (30, 10, 5)), (8, (100, 50, 20)),
+                                      (16, (50, 20, 10))])
+def test_other_dimensions(tb, oracle_mod, tmp_path, cuda, D, ratios):
+    h = tb.QueryHandler.generate(60000 if D != 8 else 200000, D, 1.0, 100.0, False, 4, ratios, 5 + D, 3.0)
+    h.prepare_for_query(tb.LevelPolicy.L0)
+    o = oracle_from_handler(oracle_mod, h, tmp_path)
+    pts, ids = oracle_mod.decoded_points(o)
+    Q = _boxes(pts, 80, 7 + D, 0.02, 0.3)
+    r, offs, got = _batch_ids(tb, h, Q, tb.Mode.EXACT)
+    b = oracle_mod.brute_query(pts, ids, oracle_mod.RANGE, Q)
+    assert np.array_equal(offs, b.offsets)
+    assert all(np.array_equal(g, b.query(q)) for q, g in enumerate(ids_by_query(offs, got)))
+    r2, offs2, got2 = _batch_ids(tb, h, Q, tb.Mode.REF_PARITY)
+    ref = oracle_mod.ref_query(o, oracle_mod.RANGE, Q, sorted_ids=False)
+    assert np.array_equal(got2, ref.ids)
+
+
+def test_height_three_and_truncated_plan(tb, oracle_mod, tmp_path, cuda):
+    h = tb.QueryHandler.generate(5000, 4, 1.0, 100.0, True, 3, (7, 9), 11, 1.5)
+    h.prepare_for_query(tb.LevelPolicy.L0)
+    o = oracle_from_handler(oracle_mod, h, tmp_path)
+    pts, ids = oracle_mod.decoded_points(o)
+    Q = _boxes(pts, 50, 8, 0.05, 0.4)
+    r, offs, got = _batch_ids(tb, h, Q, tb.Mode.EXACT)
+    b = oracle_mod.brute_query(pts, ids, oracle_mod.RANGE, Q)
+    assert np.array_equal(offs, b.offsets)
+
+
+def test_allocation_failure_surfaces_cleanly(tb, cuda):
+    lib = tb.lib()
+    h = tb.QueryHandler.generate(20000, 3, 1.0, 100.0, False, 4, (10, 10, 10), 1, 3.0)
+    before = lib.tblaeq_live_device_bytes()
+    lib.tblaeq_debug_fail_alloc_after(5)
+    try:
+        with pytest.raises(tb.TblaeqError) as e:
+            h.prepare_for_query(tb.LevelPolicy.L0)
+        assert e.value.code == 4
+    finally:
+        lib.tblaeq_debug_fail_alloc_after(0)
+    assert lib.tblaeq_live_device_bytes() == before
+    h.prepare_for_query(tb.LevelPolicy.L0)  # a later prepare succeeds
+    h.close()
+    assert lib.tblaeq_live_device_bytes() == before
