@@ -155,8 +155,9 @@ uint32_t* BatchEngine::hdrPtr(int level) const {
 
 FrontierIn BatchEngine::inView(int b, uint32_t* hdr) const {
     const FrontierBufs& f = f_[b];
-    return FrontierIn{f.q.as<uint32_t>(), f.cbeg.as<uint32_t>(), f.cpre.as<uint32_t>(), f.x.as<double>(),
-                      f.tileStart.as<uint32_t>(), hdr};
+    return FrontierIn{f.q.as<uint32_t>(),         f.cbeg.as<uint32_t>(), f.cpre.as<uint32_t>(), f.x.as<double>(),
+                      f.tileStart.as<uint32_t>(), hdr,                   static_cast<uint32_t>(caps_.entries),
+                      static_cast<uint32_t>(tileCap_)};
 }
 
 FrontierOut BatchEngine::outView(int b, uint32_t* hdr) const {

@@ -150,6 +150,12 @@ __global__ void __launch_bounds__(kThreads) expandKernel(ExpandArgs a) {
     const uint32_t total = a.in.hdr[1];
     const uint32_t nTiles = (total + TILE - 1) / TILE;
     if (entries == 0 || total == 0) return;
+    // A producer that overflowed its capacities left this frontier incomplete: never read past
+    // the arrays (the host sees the status bit, grows the workspace and reruns the batch).
+    if (entries > a.in.cap || nTiles > a.in.tileCap) {
+        if (blockIdx.x == 0 && threadIdx.x == 0) atomicOr(a.scratch.status, kStatusOverflowEntries);
+        return;
+    }
 
     while (true) {
         if (tid == 0) sTile = atomicAdd(a.scratch.ticket, 1u);

@@ -37,6 +37,8 @@ struct FrontierIn {
     const double* x;            // decoded coordinates, count * D
     const uint32_t* tileStart;  // entry holding work item b * kTile
     const uint32_t* hdr;        // [0] = entry count, [1] = total children
+    uint32_t cap;               // entry capacity of the arrays above
+    uint32_t tileCap;           // tileStart capacity
 };
 
 struct FrontierOut {
