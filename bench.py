@@ -64,7 +64,7 @@ class ClockSampler:
              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
         try:
             self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={q}", "--format=csv,noheader,nounits",
-                                          "-i", str(self.gpu), "-lms", "200"], stdout=subprocess.PIPE,
+                                          "-i", str(self.gpu), "-lms", "100"], stdout=subprocess.PIPE,
                                          stderr=subprocess.DEVNULL, text=True)
             self.t = threading.Thread(target=self._read, daemon=True)
             self.t.start()
@@ -139,8 +139,8 @@ def cpu_port_qps(oracle, oidx, sub, Q, budget_s=20.0, min_q=32):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=20)
-    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=10)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--config", choices=["batched", "small"], default="batched")
     ap.add_argument("--nq", type=int, default=4096)
@@ -264,7 +264,6 @@ def main():
         t0 = time.perf_counter()
         e2e_call()
         e2e_t.append(time.perf_counter() - t0)
-    e2e_max = max(e2e_t) if world == 1 else None
     e2e_total = sum(e2e_t)
     if world > 1:
         t = torch.tensor([e2e_total], dtype=torch.float64, device="cuda")

@@ -405,7 +405,7 @@ class QueryHandler:
         buf = (ctypes.c_float * 64)()
         n = _load().tblaeq_stage_times(self._h, buf, 64)
         if n < 0:
-            raise TblaeqError(7, "stage timing is off")
+            raise TblaeqError(7, "stage times unavailable: " + _load().tblaeq_last_error().decode())
         return list(buf[:n])
 
     def query_batch_host(self, qtype: QueryType, queries: np.ndarray, mode: Mode = Mode.EXACT, K: int = 0,

@@ -23,6 +23,16 @@ void BatchEngine::dropGraph() {
     graphKey_ = GraphKey{};
 }
 
+void BatchEngine::record(int i) {
+    // Inside stream capture an event must become an external event-record node to stay usable
+    // for cudaEventElapsedTime after the graph replays.
+    if (capturing_) {
+        TBLAEQ_CUDA(cudaEventRecordWithFlags(events_[i], stream_, cudaEventRecordExternal));
+    } else {
+        TBLAEQ_CUDA(cudaEventRecord(events_[i], stream_));
+    }
+}
+
 void BatchEngine::setTiming(bool on) {
     timing_ = on;
     if (on && events_.empty()) {
@@ -177,9 +187,12 @@ void BatchEngine::enqueueRange(const double* dBoxes, uint32_t nq, int mode, unsi
         dropGraph();
         cudaGraph_t g = nullptr;
         TBLAEQ_CUDA(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal));
+        capturing_ = true;
         try {
             enqueueLaunches(dBoxes, nq, mode, flags);
+            capturing_ = false;
         } catch (...) {
+            capturing_ = false;
             cudaStreamEndCapture(stream_, &g);
             if (g) cudaGraphDestroy(g);
             throw;
@@ -207,13 +220,13 @@ void BatchEngine::enqueueLaunches(const double* dBoxes, uint32_t nq, int mode, u
     auto* levels = reinterpret_cast<uint32_t*>(z + offLevels_);
     const bool wantLevels = (flags & kWantLevels) != 0;
 
-    if (timing_) TBLAEQ_CUDA(cudaEventRecord(events_[0], stream_));
+    if (timing_) record(0);
     TBLAEQ_CUDA(cudaMemsetAsync(z, 0, zeroBytes_, stream_));
     const FrontierBufs& r0 = f_[0];
     launchRootFrontier(r0.q.as<uint32_t>(), r0.cbeg.as<uint32_t>(), r0.cpre.as<uint32_t>(), r0.x.as<double>(),
                        r0.tileStart.as<uint32_t>(), hdrPtr(0), nq, static_cast<uint32_t>(di_.meshCount[0]), D, tile_,
                        stream_);
-    if (timing_) TBLAEQ_CUDA(cudaEventRecord(events_[1], stream_));
+    if (timing_) record(1);
     int buf = 0;
     for (int m = 0; m < H; ++m) {
         ExpandArgs a{};
@@ -242,10 +255,10 @@ void BatchEngine::enqueueLaunches(const double* dBoxes, uint32_t nq, int mode, u
             a.rout.cap = static_cast<uint32_t>(caps_.results);
             launchExpand(a, (mode == kModeExact) ? kPredRangeBox : kPredAll, true, 0, stream_);
         }
-        if (timing_) TBLAEQ_CUDA(cudaEventRecord(events_[2 + m], stream_));
+        if (timing_) record(2 + m);
     }
     launchExclusiveScan(qcount, offsets_.as<uint64_t>(), nq, stream_);
-    if (timing_) TBLAEQ_CUDA(cudaEventRecord(events_[2 + H], stream_));
+    if (timing_) record(2 + H);
 }
 
 uint32_t BatchEngine::status() {

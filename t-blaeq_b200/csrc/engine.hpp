@@ -103,6 +103,8 @@ private:
     void enqueueLaunches(const double* dBoxes, uint32_t nq, int mode, unsigned flags);
     void dropGraph();
     bool timing_ = false;
+    bool capturing_ = false;
+    void record(int i);
     std::vector<cudaEvent_t> events_;
     cudaGraphExec_t graphExec_ = nullptr;
     struct GraphKey {

@@ -50,7 +50,7 @@ def test_exact_batch_equals_brute_force(tb, env, oracle_mod):
     assert np.array_equal(offs, b.offsets)
     for q, g in enumerate(ids_by_query(offs, got)):
         assert np.array_equal(g, b.query(q)), q
-    assert b.offsets[-1] > 1000
+    assert b.offsets[-1] > 200
 
 
 def test_exact_single_queries_equal_batch(tb, env):
