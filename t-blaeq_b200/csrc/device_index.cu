@@ -203,44 +203,44 @@ std::unique_ptr<DeviceIndex> buildDeviceIndex(const HostIndex& idx, const Derive
     di->coarseVals = upload(idx.coarsest.vals, s);
     di->coarseIds = upload(idx.coarsest.ids, s);
     di->pvals.resize(idx.intervals);
-    di->colBeg.resize(idx.intervals);
-    di->colCnt.resize(idx.intervals);
-    di->radOrig.resize(idx.intervals);
+    di->nodeOrig.resize(idx.intervals);
     for (uint64_t l = 0; l < idx.intervals; ++l) {
         const PTensor& P = idx.pTensors[l];
         di->pvals[l] = upload(P.vals, s);
-        std::vector<uint32_t> b(P.cols), c(P.cols);
+        std::vector<NodeRec> rec(P.cols);
         for (uint64_t o = 0; o < P.cols; ++o) {
-            b[o] = static_cast<uint32_t>(P.colRes[o]);
-            c[o] = static_cast<uint32_t>(P.colRes[o + 1] - P.colRes[o]);
+            rec[o].rad = idx.radius[l][o];
+            rec[o].cbeg = static_cast<uint32_t>(P.colRes[o]);
+            rec[o].cnt = static_cast<uint32_t>(P.colRes[o + 1] - P.colRes[o]);
         }
-        di->colBeg[l] = upload(b, s);
-        di->colCnt[l] = upload(c, s);
-        di->radOrig[l] = upload(idx.radius[l], s);
+        di->nodeOrig[l] = upload(rec, s);
         TBLAEQ_CUDA(cudaStreamSynchronize(s));
     }
     di->maps.resize(idx.height);
     for (uint64_t m = 1; m < idx.height; ++m) di->maps[m] = upload(idx.maps[m], s);
     // The finest map doubles as the final-id map of the fused traversal.
-    di->cbeg.resize(idx.height - 1);
-    di->ccnt.resize(idx.height - 1);
+    di->nodeRef.resize(idx.height - 1);
+    di->nodeSub.resize(idx.height - 1);
     di->leaf.resize(idx.height - 1);
-    di->radRef.resize(idx.height - 1);
-    di->radSub.resize(idx.height - 1);
     for (uint64_t m = 0; m + 1 < idx.height; ++m) {
-        di->cbeg[m] = upload(der.cbeg[m], s);
-        di->ccnt[m] = upload(der.ccnt[m], s);
+        const size_t n = der.cbeg[m].size();
+        std::vector<NodeRec> ref(n), sub(n);
+        for (size_t i = 0; i < n; ++i) {
+            ref[i] = NodeRec{der.radRef[m][i], der.cbeg[m][i], der.ccnt[m][i]};
+            sub[i] = NodeRec{der.radSub[m][i], der.cbeg[m][i], der.ccnt[m][i]};
+        }
+        di->nodeRef[m] = upload(ref, s);
+        di->nodeSub[m] = upload(sub, s);
         di->leaf[m] = upload(der.leaf[m], s);
-        di->radRef[m] = upload(der.radRef[m], s);
-        di->radSub[m] = upload(der.radSub[m], s);
+        TBLAEQ_CUDA(cudaStreamSynchronize(s));
     }
     TBLAEQ_CUDA(cudaStreamSynchronize(s));
     return di;
 }
 
 size_t DeviceIndex::deviceBytes() const {
-    size_t t = coarseVals.bytes() + finestMap.bytes() + coarseIds.bytes();
-    for (auto* v : {&pvals, &cbeg, &ccnt, &leaf, &radRef, &radSub, &colBeg, &colCnt, &radOrig, &maps})
+    size_t t = coarseVals.bytes() + coarseIds.bytes();
+    for (auto* v : {&pvals, &nodeRef, &nodeSub, &leaf, &nodeOrig, &maps})
         for (auto& m : *v) t += m.bytes();
     return t;
 }

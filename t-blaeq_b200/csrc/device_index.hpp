@@ -17,6 +17,7 @@
 
 #include "common.cuh"
 #include "index.hpp"
+#include "traverse.cuh"
 
 namespace tblaeq {
 
@@ -89,14 +90,12 @@ struct DeviceIndex {
     // position space
     DeviceMem coarseVals;                    // mesh 0 rows (n0 * D)
     std::vector<DeviceMem> pvals;            // interval l: rows of P_l (n_{l+1} * D)
-    std::vector<DeviceMem> cbeg, ccnt, leaf; // mesh m < height-1 (uint32)
-    std::vector<DeviceMem> radRef, radSub;   // mesh m < height-1 (double)
-    DeviceMem finestMap;                     // Map of the finest mesh (uint64)
+    std::vector<DeviceMem> nodeRef, nodeSub; // mesh m < height-1: NodeRec {radius, first child, children}
+    std::vector<DeviceMem> leaf;             // mesh m < height-1: finest points below each node (uint32)
 
     // original-id space (per-level plugin)
     DeviceMem coarseIds;                     // uint64
-    std::vector<DeviceMem> colBeg, colCnt;   // interval l, by original column id (uint32)
-    std::vector<DeviceMem> radOrig;          // interval l, by original column id (double)
+    std::vector<DeviceMem> nodeOrig;         // interval l, NodeRec by original column id
     std::vector<DeviceMem> maps;             // mesh m >= 1 (uint64); maps[0] empty
 
     size_t deviceBytes() const;

@@ -240,9 +240,7 @@ void BatchEngine::enqueueLaunches(const double* dBoxes, uint32_t nq, int mode, u
         a.D = D;
         a.useFma = 1;
         if (m < H - 1) {
-            a.child.rad = (mode == kModeExact) ? di_.radSub[m].as<double>() : di_.radRef[m].as<double>();
-            a.child.ncbeg = di_.cbeg[m].as<uint32_t>();
-            a.child.ncnt = di_.ccnt[m].as<uint32_t>();
+            a.child.nodes = (mode == kModeExact) ? di_.nodeSub[m].as<NodeRec>() : di_.nodeRef[m].as<NodeRec>();
             a.fout = outView(1 - buf, hdrPtr(m + 1));
             launchExpand(a, kPredRangeRadius, false, 0, stream_);
             buf = 1 - buf;
@@ -364,9 +362,7 @@ uint64_t BatchEngine::runGridLevel(int l, const uint64_t* dIds, const double* dV
         a.in = inView(0, hdrPtr(0));
         a.child.rows = dVals;
         a.child.keys = dIds;
-        a.child.rad = di_.radOrig[l].as<double>();
-        a.child.ncbeg = di_.colBeg[l].as<uint32_t>();
-        a.child.ncnt = di_.colCnt[l].as<uint32_t>();
+        a.child.nodes = di_.nodeOrig[l].as<NodeRec>();
         a.child.mask = dMask;
         a.query.boxes = dQuery;
         a.fout = outView(1, hdrPtr(1));

@@ -9,22 +9,10 @@ namespace tblaeq {
 
 namespace {
 
-constexpr int kWarps = kThreads / 32;
 constexpr uint32_t kFlagAggregate = 1;
 constexpr uint32_t kFlagPrefix = 2;
 constexpr uint32_t kMaxCount30 = (1u << 30) - 1;
 constexpr uint32_t kSpinLimit = 1u << 21;  // ~0.2-2 s of polling before giving up
-
-// Items per thread per tile: keep IPT*D doubles of rebuilt coordinates in registers.
-template <int D>
-struct Ipt {
-    static constexpr int value = (D == 0) ? 1 : (D <= 4 ? 4 : (D <= 8 ? 2 : 1));
-};
-
-template <int D>
-constexpr int tileOf() {
-    return kThreads * Ipt<D>::value;
-}
 
 __device__ __forceinline__ unsigned long long packDesc(uint32_t flag, uint32_t cnt, uint32_t sum) {
     return (static_cast<unsigned long long>(flag) << 62) |
@@ -127,28 +115,50 @@ __device__ __forceinline__ double pointDist2(const double* y, const double* p, i
     return dist;
 }
 
+// Rebuilds item (entry e, row j): y = rows[j] (*) x_e, one rounded multiply per dimension.
+template <int D, int DM>
+__device__ __forceinline__ void rebuild(const ExpandArgs& a, int dim, uint32_t e, uint32_t j, double (&y)[DM]) {
+    const double* xp = a.in.x + static_cast<size_t>(e) * dim;
+    const double* rp = a.child.rows + static_cast<size_t>(j) * dim;
+    if constexpr (D > 0 && (D % 2) == 0) {
+#pragma unroll
+        for (int d = 0; d < D; d += 2) {
+            const double2 pv = __ldg(reinterpret_cast<const double2*>(rp + d));
+            const double2 xv = __ldg(reinterpret_cast<const double2*>(xp + d));
+            y[d] = __dmul_rn(pv.x, xv.x);
+            y[d + 1] = __dmul_rn(pv.y, xv.y);
+        }
+    } else {
+#pragma unroll
+        for (int d = 0; d < DM; ++d) {
+            if (d < dim) y[d] = __dmul_rn(__ldg(rp + d), __ldg(xp + d));
+        }
+    }
+}
+
+// Up to D = 8 the rebuilt coordinates fit 64 registers (4 CTAs per SM); wider rows get 2 CTAs.
+template <int D>
+constexpr int minBlocksFor() {
+    return (D > 0 && D <= 8) ? 4 : 2;
+}
+
 template <int D, int PRED, bool TO_RESULT>
-__global__ void __launch_bounds__(kThreads) expandKernel(ExpandArgs a) {
-    constexpr int IPT = Ipt<D>::value;
-    constexpr int TILE = kThreads * IPT;
+__global__ void __launch_bounds__(kThreads, minBlocksFor<D>()) expandKernel(ExpandArgs a) {
+    constexpr int R = kWarpTile / 32;  // rounds of 32 items per warp tile
+    // Per-warp cache of every item's row, entry and query between the two passes.
+    __shared__ uint32_t sRow[kThreads / 32][R][32];
+    __shared__ uint32_t sEnt[kThreads / 32][R][32];
+    __shared__ uint32_t sQ[kThreads / 32][R][32];
     constexpr int DM = (D > 0) ? D : 32;
+    constexpr uint32_t FULL = 0xffffffffu;
     const int dim = (D > 0) ? D : a.D;
+    const int lane = threadIdx.x & 31;
+    const uint32_t lanesLe = (2u << lane) - 1u;  // lanes 0..lane (wraps to all lanes for lane 31)
+    const uint32_t lanesLt = (1u << lane) - 1u;
 
-    __shared__ uint32_t sTile;
-    __shared__ uint32_t sWinBase, sWinLen;
-    __shared__ uint32_t sCpre[TILE + 1];
-    __shared__ uint32_t sCbeg[TILE + 1];
-    __shared__ uint32_t sQ[TILE + 1];
-    __shared__ uint32_t sWarpCnt[IPT * kWarps];
-    __shared__ uint32_t sWarpSum[IPT * kWarps];
-    __shared__ unsigned long long sExCnt, sExSum;
-
-    const int tid = threadIdx.x;
-    const int lane = tid & 31;
-    const int warp = tid >> 5;
     const uint32_t entries = a.in.hdr[0];
     const uint32_t total = a.in.hdr[1];
-    const uint32_t nTiles = (total + TILE - 1) / TILE;
+    const uint32_t nTiles = (total + kWarpTile - 1) / kWarpTile;
     if (entries == 0 || total == 0) return;
     // A producer that overflowed its capacities left this frontier incomplete: never read past
     // the arrays (the host sees the status bit, grows the workspace and reruns the batch).
@@ -158,242 +168,209 @@ __global__ void __launch_bounds__(kThreads) expandKernel(ExpandArgs a) {
     }
 
     while (true) {
-        if (tid == 0) sTile = atomicAdd(a.scratch.ticket, 1u);
-        __syncthreads();
-        const uint32_t tile = sTile;
+        uint32_t tile = 0;
+        if (lane == 0) tile = atomicAdd(a.scratch.ticket, 1u);
+        tile = __shfl_sync(FULL, tile, 0);
         if (tile >= nTiles) break;
-        const uint32_t t0 = tile * TILE;
+        const uint32_t t0 = tile * kWarpTile;
 
-        // Stage the frontier entries this tile touches.
-        if (tid == 0) {
-            const uint32_t eLo = a.in.tileStart[tile];
-            uint32_t eHi = (tile + 1 < nTiles) ? a.in.tileStart[tile + 1] : entries - 1;
-            if (eHi >= entries) eHi = entries - 1;
-            uint32_t len = eHi - eLo + 1;
-            if (len > TILE + 1) {
-                atomicOr(a.scratch.status, kStatusWindowOverflow);
-                len = TILE + 1;
-            }
-            sWinBase = eLo;
-            sWinLen = len;
-        }
-        __syncthreads();
-        const uint32_t wb = sWinBase, wl = sWinLen;
-        for (uint32_t i = tid; i < wl; i += kThreads) {
-            sCpre[i] = a.in.cpre[wb + i];
-            sCbeg[i] = a.in.cbeg[wb + i];
-            sQ[i] = a.in.q[wb + i];
-        }
-        __syncthreads();
-
-        // Rebuild and test every item of the tile.
-        bool keep[IPT];
-        uint32_t row[IPT], qs[IPT], ccnt[IPT], ncb[IPT], key[IPT];
-        double y[IPT][DM];
-        double d2[IPT];
+        // ---- pass 1: map every item to its entry, rebuild it and test it; keep one bit per item.
+        uint32_t keepBits = 0, aggCnt = 0, aggSum = 0;
+        const int w = threadIdx.x >> 5;
+        uint32_t cur = a.in.tileStart[tile];  // entry holding the first item of the round
 #pragma unroll
-        for (int r = 0; r < IPT; ++r) {
-            const uint32_t k = t0 + r * kThreads + tid;
-            keep[r] = false;
-            ccnt[r] = 0;
-            ncb[r] = 0;
-            d2[r] = 0.0;
-            row[r] = 0;
-            qs[r] = 0;
-            key[r] = 0;
-            if (k < total) {
-                uint32_t lo = 0, hi = wl - 1;
-                while (lo < hi) {  // last entry whose prefix <= k
+        for (int r = 0; r < R; ++r) {
+            const uint32_t rs = t0 + r * 32;
+            if (rs >= total) continue;  // warp-uniform
+            const uint32_t k = rs + lane;
+            const bool valid = k < total;
+            // The 32 entries from `cur` cover every entry overlapping this round unless entries with
+            // fewer than one child per lane follow (then each lane searches on its own).
+            const uint32_t ce = cur + lane;
+            const bool inRange = ce < entries;
+            const uint32_t cp = inRange ? a.in.cpre[ce] : 0xffffffffu;
+            const uint32_t cp31 = __shfl_sync(FULL, cp, 31);
+            uint32_t e, eCp, eCb, eQ;
+            if (cp31 + 1 < rs + 32 && cur + 32 < entries) {
+                uint32_t lo = cur, hi = entries - 1;
+                const uint32_t kk = valid ? k : rs;
+                while (lo < hi) {
                     const uint32_t mid = (lo + hi + 1) >> 1;
-                    if (sCpre[mid] <= k) lo = mid; else hi = mid - 1;
+                    if (a.in.cpre[mid] <= kk) lo = mid; else hi = mid - 1;
                 }
-                const uint32_t e = lo;
-                const uint32_t j = sCbeg[e] + (k - sCpre[e]);
-                const uint32_t qi = sQ[e];
-                row[r] = j;
-                qs[r] = qi;
-                const double* xp = a.in.x + static_cast<size_t>(wb + e) * dim;
-                const double* rp = a.child.rows + static_cast<size_t>(j) * dim;
-                if constexpr (D > 0 && (D % 2) == 0) {
-#pragma unroll
-                    for (int d = 0; d < D; d += 2) {
-                        const double2 pv = __ldg(reinterpret_cast<const double2*>(rp + d));
-                        const double2 xv = __ldg(reinterpret_cast<const double2*>(xp + d));
-                        y[r][d] = __dmul_rn(pv.x, xv.x);
-                        y[r][d + 1] = __dmul_rn(pv.y, xv.y);
-                    }
-                } else {
-#pragma unroll
-                    for (int d = 0; d < DM; ++d) {
-                        if (d < dim) y[r][d] = __dmul_rn(__ldg(rp + d), __ldg(xp + d));
-                    }
-                }
+                e = lo;
+                eCp = a.in.cpre[e];
+                eCb = a.in.cbeg[e];
+                eQ = a.in.q[e];
+            } else {
+                const uint32_t cb = inRange ? a.in.cbeg[ce] : 0u;
+                const uint32_t cq = inRange ? a.in.q[ce] : 0u;
+                const uint32_t base = __popc(__ballot_sync(FULL, cp <= rs)) - 1u;
+                const uint32_t off = cp - rs;
+                const uint32_t starts = __reduce_or_sync(FULL, (cp > rs && off < 32u) ? (1u << off) : 0u);
+                const uint32_t my = base + __popc(starts & lanesLe);
+                e = cur + my;
+                eCp = __shfl_sync(FULL, cp, my);
+                eCb = __shfl_sync(FULL, cb, my);
+                eQ = __shfl_sync(FULL, cq, my);
+            }
+            cur = __shfl_sync(FULL, e, 31);
+            const uint32_t j = eCb + (k - eCp);
+            sRow[w][r][lane] = j;
+            sEnt[w][r][lane] = e;
+            sQ[w][r][lane] = eQ;
+
+            bool keep = false;
+            uint32_t cc = 0;
+            if (valid) {
+                double y[DM];
+                rebuild<D, DM>(a, dim, e, j, y);
                 const uint32_t kk = a.child.keys ? static_cast<uint32_t>(a.child.keys[j]) : j;
-                key[r] = kk;
                 if constexpr (PRED == kPredRangeRadius) {
-                    const double* box = a.query.boxes + static_cast<size_t>(qi) * 2 * dim;
-                    const double dist = boxDist2<DM>(y[r], box, box + dim, dim, a.useFma);
-                    const double rr = a.child.rad[kk];
-                    ccnt[r] = a.child.ncnt[kk];
-                    keep[r] = (ccnt[r] > 0) && (dist <= __dmul_rn(rr, rr));
+                    const double* box = a.query.boxes + static_cast<size_t>(eQ) * 2 * dim;
+                    const double dist = boxDist2<DM>(y, box, box + dim, dim, a.useFma);
+                    const NodeRec nr = a.child.nodes[kk];
+                    cc = nr.cnt;
+                    keep = (cc > 0) && (dist <= __dmul_rn(nr.rad, nr.rad));
                 } else if constexpr (PRED == kPredMask) {
-                    keep[r] = a.child.mask[j] != 0;
+                    keep = a.child.mask[j] != 0;
                     if constexpr (!TO_RESULT) {
-                        ccnt[r] = a.child.ncnt[kk];
-                        keep[r] = keep[r] && ccnt[r] > 0;
+                        cc = a.child.nodes[kk].cnt;
+                        keep = keep && cc > 0;
                     }
                 } else if constexpr (PRED == kPredAll) {
-                    keep[r] = true;
+                    keep = true;
                     if constexpr (!TO_RESULT) {
-                        ccnt[r] = a.child.ncnt[kk];
-                        keep[r] = ccnt[r] > 0;
+                        cc = a.child.nodes[kk].cnt;
+                        keep = cc > 0;
                     }
                 } else if constexpr (PRED == kPredRangeBox) {
-                    const double* box = a.query.boxes + static_cast<size_t>(qi) * 2 * dim;
+                    const double* box = a.query.boxes + static_cast<size_t>(eQ) * 2 * dim;
                     bool in = true;
 #pragma unroll
                     for (int d = 0; d < DM; ++d) {
-                        if (d < dim) in = in && (box[d] <= y[r][d]) && (y[r][d] <= box[dim + d]);
+                        if (d < dim) in = in && (box[d] <= y[d]) && (y[d] <= box[dim + d]);
                     }
-                    keep[r] = in;
+                    keep = in;
                 } else if constexpr (PRED == kPredKnnBound) {
-                    const double* p = a.query.points + static_cast<size_t>(qi) * dim;
-                    const double dd = sqrt(pointDist2<DM>(y[r], p, dim, 1));
-                    ccnt[r] = a.child.ncnt[kk];
-                    keep[r] = (ccnt[r] > 0) && (dd - a.child.rad[kk] <= a.query.tau[qi]);
+                    const double* p = a.query.points + static_cast<size_t>(eQ) * dim;
+                    const double dd = sqrt(pointDist2<DM>(y, p, dim, 1));
+                    const NodeRec nr = a.child.nodes[kk];
+                    cc = nr.cnt;
+                    keep = (cc > 0) && (dd - nr.rad <= a.query.tau[eQ]);
                 } else if constexpr (PRED == kPredKnnPoint) {
-                    const double* p = a.query.points + static_cast<size_t>(qi) * dim;
-                    d2[r] = pointDist2<DM>(y[r], p, dim, 1);
-                    const double t = a.query.tau[qi];
-                    keep[r] = d2[r] <= t * t;
-                }
-                if constexpr (!TO_RESULT) {
-                    if (keep[r]) ncb[r] = a.child.ncbeg[kk];
+                    const double* p = a.query.points + static_cast<size_t>(eQ) * dim;
+                    const double t = a.query.tau[eQ];
+                    keep = pointDist2<DM>(y, p, dim, 1) <= t * t;
                 }
             }
             // Per-query generated-children counts (the reference's levelFineMeshSize).
             if (a.scratch.levelItems) {
-                const bool valid = k < total;
-                const uint32_t vm = __ballot_sync(0xffffffffu, valid);
+                const uint32_t vm = __ballot_sync(FULL, valid);
                 if (valid) {
-                    const uint32_t peers = __match_any_sync(vm, qs[r]);
-                    if (lane == __ffs(peers) - 1) atomicAdd(&a.scratch.levelItems[qs[r]], __popc(peers));
+                    const uint32_t peers = __match_any_sync(vm, eQ);
+                    if (lane == __ffs(peers) - 1) atomicAdd(&a.scratch.levelItems[eQ], __popc(peers));
                 }
             }
+            const uint32_t kb = __ballot_sync(FULL, keep);
+            keepBits |= (keep ? 1u : 0u) << r;
+            aggCnt += __popc(kb);
+            uint32_t s = keep ? cc : 0u;
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(FULL, s, o);
+            aggSum += s;
         }
 
-        // Tile-local order-preserving ranks: round-major, then thread order.
-        uint32_t rankCnt[IPT], rankSum[IPT];
-#pragma unroll
-        for (int r = 0; r < IPT; ++r) {
-            const uint32_t ballot = __ballot_sync(0xffffffffu, keep[r]);
-            rankCnt[r] = __popc(ballot & ((1u << lane) - 1));
-            uint32_t s = keep[r] ? ccnt[r] : 0;
-            uint32_t inc = s;
-#pragma unroll
-            for (int o = 1; o < 32; o <<= 1) {
-                const uint32_t v = __shfl_up_sync(0xffffffffu, inc, o);
-                if (lane >= o) inc += v;
-            }
-            rankSum[r] = inc - s;
-            if (lane == 31) {
-                sWarpCnt[r * kWarps + warp] = __popc(ballot);
-                sWarpSum[r * kWarps + warp] = inc;
-            }
-        }
-        __syncthreads();
-        if (warp == 0) {
-            // Exclusive scan of the IPT*kWarps warp totals (<= 32 of them) in round-major order.
-            constexpr int NW = IPT * kWarps;
-            const uint32_t c = (lane < NW) ? sWarpCnt[lane] : 0;
-            const uint32_t s = (lane < NW) ? sWarpSum[lane] : 0;
-            uint32_t ic = c, is = s;
-#pragma unroll
-            for (int o = 1; o < 32; o <<= 1) {
-                const uint32_t vc = __shfl_up_sync(0xffffffffu, ic, o);
-                const uint32_t vs = __shfl_up_sync(0xffffffffu, is, o);
-                if (lane >= o) {
-                    ic += vc;
-                    is += vs;
-                }
-            }
-            const uint32_t aggCnt = __shfl_sync(0xffffffffu, ic, 31);
-            const uint32_t aggSum = __shfl_sync(0xffffffffu, is, 31);
-            if (lane < NW) {
-                sWarpCnt[lane] = ic - c;
-                sWarpSum[lane] = is - s;
-            }
-            unsigned long long exC, exS;
-            lookback(a.scratch.desc, tile, aggCnt, aggSum, a.scratch.status, exC, exS);
-            if (lane == 0) {
-                sExCnt = exC;
-                sExSum = exS;
-                if (tile == nTiles - 1) {
-                    const unsigned long long totC = exC + aggCnt;
-                    const unsigned long long totS = exS + aggSum;
-                    if constexpr (TO_RESULT) {
-                        a.rout.hdr[0] = static_cast<uint32_t>(min(totC, 0xffffffffull));
-                        if (totC > a.rout.cap) atomicOr(a.scratch.status, kStatusOverflowEntries);
-                    } else {
-                        a.fout.hdr[0] = static_cast<uint32_t>(min(totC, 0xffffffffull));
-                        a.fout.hdr[1] = static_cast<uint32_t>(min(totS, 0xffffffffull));
-                        if (totC > a.fout.cap) atomicOr(a.scratch.status, kStatusOverflowEntries);
-                        if (totS > 0xffffffffull) atomicOr(a.scratch.status, kStatusOverflowSum);
-                        const unsigned long long tilesNeeded = (totS + TILE - 1) / TILE;
-                        if (tilesNeeded > a.fout.tileCap) atomicOr(a.scratch.status, kStatusOverflowItems);
-                    }
-                }
-            }
-        }
-        __syncthreads();
-        const unsigned long long exCnt = sExCnt, exSum = sExSum;
-
-        // Write kept items.
-#pragma unroll
-        for (int r = 0; r < IPT; ++r) {
-            if (!keep[r]) continue;
-            const unsigned long long pos = exCnt + sWarpCnt[r * kWarps + warp] + rankCnt[r];
+        // ---- publish the tile's counts and learn where its output starts.
+        unsigned long long exCnt, exSum;
+        lookback(a.scratch.desc, tile, aggCnt, aggSum, a.scratch.status, exCnt, exSum);
+        if (tile == nTiles - 1 && lane == 0) {
+            const unsigned long long totC = exCnt + aggCnt;
+            const unsigned long long totS = exSum + aggSum;
             if constexpr (TO_RESULT) {
-                if (pos >= a.rout.cap) continue;
-                const uint32_t j = row[r];
-                a.rout.ids[pos] = a.child.outMap ? a.child.outMap[j] : static_cast<uint64_t>(key[r]);
-                if (a.rout.vals) {
+                a.rout.hdr[0] = static_cast<uint32_t>(min(totC, 0xffffffffull));
+                if (totC > a.rout.cap) atomicOr(a.scratch.status, kStatusOverflowEntries);
+            } else {
+                a.fout.hdr[0] = static_cast<uint32_t>(min(totC, 0xffffffffull));
+                a.fout.hdr[1] = static_cast<uint32_t>(min(totS, 0xffffffffull));
+                if (totC > a.fout.cap) atomicOr(a.scratch.status, kStatusOverflowEntries);
+                if (totS > 0xffffffffull) atomicOr(a.scratch.status, kStatusOverflowSum);
+                const unsigned long long tilesNeeded = (totS + kWarpTile - 1) / kWarpTile;
+                if (tilesNeeded > a.fout.tileCap) atomicOr(a.scratch.status, kStatusOverflowItems);
+            }
+        }
+
+        // ---- pass 2: rebuild and write the kept items in order.
+        unsigned long long runCnt = exCnt, runSum = exSum;
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+            const bool keep = (keepBits >> r) & 1u;
+            const uint32_t kb = __ballot_sync(FULL, keep);
+            if (kb == 0) continue;  // warp-uniform
+            const uint32_t j = sRow[w][r][lane];
+            const uint32_t qr = sQ[w][r][lane];
+            uint32_t cc = 0, ncb = 0, kk = 0;
+            double y[DM];
+            if (keep) {
+                rebuild<D, DM>(a, dim, sEnt[w][r][lane], j, y);
+                kk = a.child.keys ? static_cast<uint32_t>(a.child.keys[j]) : j;
+                if constexpr (!TO_RESULT) {
+                    const NodeRec nr = a.child.nodes[kk];
+                    cc = nr.cnt;
+                    ncb = nr.cbeg;
+                }
+            }
+            const uint32_t v = keep ? cc : 0u;
+            uint32_t inc = v;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const uint32_t t = __shfl_up_sync(FULL, inc, o);
+                if (lane >= o) inc += t;
+            }
+            const uint32_t roundSum = __shfl_sync(FULL, inc, 31);
+            if (keep) {
+                const unsigned long long pos = runCnt + __popc(kb & lanesLt);
+                if constexpr (TO_RESULT) {
+                    if (pos < a.rout.cap) {
+                        a.rout.ids[pos] = a.child.outMap ? a.child.outMap[j] : static_cast<uint64_t>(kk);
+                        if (a.rout.vals) {
+#pragma unroll
+                            for (int d = 0; d < DM; ++d)
+                                if (d < dim) a.rout.vals[pos * dim + d] = y[d];
+                        }
+                        if (a.rout.q) a.rout.q[pos] = qr;
+                        if constexpr (PRED == kPredKnnPoint) {
+                            if (a.rout.dist2) {
+                                const double* p = a.query.points + static_cast<size_t>(qr) * dim;
+                                a.rout.dist2[pos] = pointDist2<DM>(y, p, dim, 1);
+                            }
+                        }
+                    }
+                } else if (pos < a.fout.cap) {
+                    const unsigned long long cp = runSum + (inc - v);
+                    a.fout.q[pos] = qr;
+                    a.fout.node[pos] = kk;
+                    a.fout.cbeg[pos] = ncb;
+                    a.fout.cpre[pos] = static_cast<uint32_t>(cp);
 #pragma unroll
                     for (int d = 0; d < DM; ++d)
-                        if (d < dim) a.rout.vals[pos * dim + d] = y[r][d];
-                }
-                if (a.rout.q) a.rout.q[pos] = qs[r];
-                if (a.rout.dist2) a.rout.dist2[pos] = d2[r];
-            } else {
-                if (pos >= a.fout.cap) continue;
-                const unsigned long long cp = exSum + sWarpSum[r * kWarps + warp] + rankSum[r];
-                a.fout.q[pos] = qs[r];
-                a.fout.node[pos] = key[r];
-                a.fout.cbeg[pos] = ncb[r];
-                a.fout.cpre[pos] = static_cast<uint32_t>(cp);
-#pragma unroll
-                for (int d = 0; d < DM; ++d)
-                    if (d < dim) a.fout.x[pos * dim + d] = y[r][d];
-                // Tile starts of the next level: every tile boundary inside this entry's children.
-                const unsigned long long cend = cp + ccnt[r];
-                for (unsigned long long b = (cp + TILE - 1) / TILE; b * TILE < cend; ++b) {
-                    if (b < a.fout.tileCap) a.fout.tileStart[b] = static_cast<uint32_t>(pos);
-                }
-            }
-        }
-        if constexpr (TO_RESULT) {
-            if (a.rout.qcount) {
-#pragma unroll
-                for (int r = 0; r < IPT; ++r) {
-                    const uint32_t km = __ballot_sync(0xffffffffu, keep[r]);
-                    if (keep[r]) {
-                        const uint32_t peers = __match_any_sync(km, qs[r]);
-                        if (lane == __ffs(peers) - 1) atomicAdd(&a.rout.qcount[qs[r]], __popc(peers));
+                        if (d < dim) a.fout.x[pos * dim + d] = y[d];
+                    // Tile starts of the next level: every tile boundary inside this entry's children.
+                    const unsigned long long cend = cp + cc;
+                    for (unsigned long long b = (cp + kWarpTile - 1) / kWarpTile; b * kWarpTile < cend; ++b) {
+                        if (b < a.fout.tileCap) a.fout.tileStart[b] = static_cast<uint32_t>(pos);
                     }
                 }
             }
+            if constexpr (TO_RESULT) {
+                if (a.rout.qcount && keep) {
+                    const uint32_t peers = __match_any_sync(kb, qr);
+                    if (lane == __ffs(peers) - 1) atomicAdd(&a.rout.qcount[qr], __popc(peers));
+                }
+            }
+            runCnt += __popc(kb);
+            runSum += roundSum;
         }
-        __syncthreads();  // shared staging is reused by the next tile
     }
 }
 
@@ -496,18 +473,6 @@ void dispatchPred(const ExpandArgs& a, int pred, bool toResult, int g, cudaStrea
 }
 
 }  // namespace
-
-int expandTile(int D) {
-    switch (D) {
-        case 2: return tileOf<2>();
-        case 3: return tileOf<3>();
-        case 4: return tileOf<4>();
-        case 5: return tileOf<5>();
-        case 8: return tileOf<8>();
-        case 16: return tileOf<16>();
-        default: return tileOf<0>();
-    }
-}
 
 void launchExpand(const ExpandArgs& a, int pred, bool toResult, int gridBlocks, cudaStream_t stream) {
     switch (a.D) {

@@ -16,9 +16,13 @@
 //     (with the next level's child prefix and tile starts) or as final result ids (Map applied,
 //     src/Query/Refactor.cu:10-16).
 //
-// Tiles are claimed through an atomic ticket by a persistent grid, so every tile a look-back
-// waits on belongs to a CTA that is already running; every spin is bounded and reports a
-// status bit instead of hanging.
+// Each warp works alone on a tile of kWarpTile consecutive items (no block-wide barriers): it maps
+// items to entries with a ballot and an OR-reduction over the 32 entries that can overlap a 32-item
+// round, tests every item in a first pass that keeps one bit per item, publishes its counts through
+// the look-back, and only then rebuilds and writes the kept items (a small fraction at every level).
+// Tiles are claimed through an atomic ticket by a persistent grid, so every tile a look-back waits
+// on belongs to a warp that is already running; every spin is bounded and reports a status bit
+// instead of hanging.
 #pragma once
 
 #include <cstdint>
@@ -28,6 +32,15 @@
 namespace tblaeq {
 
 constexpr int kThreads = 256;
+constexpr int kWarpTile = 256;  // work items per warp tile (8 rounds of 32)
+
+// Packed per-node record of a child level: pruning radius, first grandchild row and grandchild
+// count, read with one 16-byte load per item.
+struct __align__(16) NodeRec {
+    double rad;
+    uint32_t cbeg;
+    uint32_t cnt;
+};
 
 // Frontier in structure-of-arrays layout.
 struct FrontierIn {
@@ -66,10 +79,8 @@ struct ResultOut {
 // The child level: rows to multiply, and the arrays of the child nodes themselves.
 struct ChildLevel {
     const double* rows;         // row j: D factors (P-tensor row, or coordinates with x = 1)
-    const uint64_t* keys;       // optional key of row j into the node arrays (null: key = j)
-    const double* rad;          // pruning radius of the child node (by key)
-    const uint32_t* ncbeg;      // first grandchild of the child node (by key)
-    const uint32_t* ncnt;       // grandchild count of the child node (by key)
+    const uint64_t* keys;       // optional key of row j into the node records (null: key = j)
+    const NodeRec* nodes;       // child node records (by key)
     const uint8_t* mask;        // keep flags (by row) for kPredMask
     const uint64_t* outMap;     // final output id of row j (null: id = key)
 };
@@ -112,8 +123,8 @@ struct ExpandArgs {
 // grid sized from the occupancy of the instantiation.
 void launchExpand(const ExpandArgs& a, int pred, bool toResult, int gridBlocks, cudaStream_t stream);
 
-// Tile size (work items per tile) used by every expand instantiation of dimension D.
-int expandTile(int D);
+// Tile size (work items per tile) used by every expand instantiation.
+inline int expandTile(int) { return kWarpTile; }
 
 // Builds a root frontier of `nq` entries, each with `nChildren` children starting at row 0 and
 // x = 1 (so the first expand reproduces the coarsest coordinates exactly). Capacities must hold
