@@ -188,8 +188,10 @@ def main():
     D = cfg["D"]
     flags = 0 if args.no_graph else tb.USE_GRAPH
 
-    # Warm-up: the first synchronous batch sizes every workspace, the rest replay the graph.
+    # Warm-up: the first synchronous batch sizes every workspace, the autotuner picks a kernel
+    # variant per level on this batch, the rest replay the graph.
     h.query_batch(tb.QueryType.RANGE, dQ, tb.Mode.EXACT)
+    variants, tuned_ms = h.autotune(dQ, tb.Mode.EXACT, reps=5)
     h.set_timing(True)
     flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
     for _ in range(args.warmup):
@@ -312,6 +314,7 @@ def main():
         "plain": {"value": plain_qps, "unit": "queries/s", "queries": n_plain,
                   "speedup_batched_vs_plain": value / world / plain_qps},
         "results_per_step": results,
+        "autotune": {"variants": ["staged" if v else "direct" for v in variants], "level_ms": tuned_ms},
         "level_entries": entries,
         "level_children": items,
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,

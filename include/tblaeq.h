@@ -179,6 +179,15 @@ int tblaeq_set_timing(tblaeq_handle* h, int on);
  * Returns the number of stages written (at most cap), or -1 when timing is off. */
 int tblaeq_stage_times(tblaeq_handle* h, float* ms, int cap);
 
+/* Autotuner: times each expand-kernel variant (registers / cp.async shared-memory ring) on this
+ * batch for every level and keeps the fastest per level (device queries, range batches).
+ * variants_out (height entries) receives the choice and ms_out (height entries, may be NULL) the
+ * median milliseconds of each chosen level. */
+int tblaeq_autotune(tblaeq_handle* h, const tblaeq_batch* batch, int reps, int* variants_out, float* ms_out);
+
+/* Set the expand-kernel variant per level (0 = direct, 1 = staged), e.g. from a tuning cache. */
+int tblaeq_set_variants(tblaeq_handle* h, const int* variants, uint64_t n);
+
 /* Host copies of the index arrays (read-only, owned by the handle), for tools and tests:
  * which = 0: P-tensor values of interval l (rows*D doubles), 1: colRes of interval l (cols+1),
  * 2: max radius of interval l (cols), 3: Map of mesh l (meshSizes), 4: coarsest ids, 5: coarsest vals. */

@@ -23,7 +23,8 @@ from typing import Optional, Sequence
 import numpy as np
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(_HERE, "libtblaeq_b200.so")
+# TBLAEQ_LIBRARY selects another build of the same library (e.g. a differently tuned one).
+LIB_PATH = os.environ.get("TBLAEQ_LIBRARY") or os.path.join(_HERE, "libtblaeq_b200.so")
 HEADER_PATH = os.path.join(os.path.dirname(_HERE), "include", "tblaeq.h")
 
 
@@ -129,6 +130,8 @@ def _load():
         "tblaeq_set_device": ([ctypes.c_int], ctypes.c_int),
         "tblaeq_set_timing": ([vp, ctypes.c_int], ctypes.c_int),
         "tblaeq_stage_times": ([vp, P(ctypes.c_float), ctypes.c_int], ctypes.c_int),
+        "tblaeq_autotune": ([vp, P(_Batch), ctypes.c_int, P(ctypes.c_int), P(ctypes.c_float)], ctypes.c_int),
+        "tblaeq_set_variants": ([vp, P(ctypes.c_int), ctypes.c_uint64], ctypes.c_int),
         "tblaeq_live_device_bytes": ([], ctypes.c_uint64),
         "tblaeq_debug_fail_alloc_after": ([ctypes.c_uint64], None),
     }
@@ -394,6 +397,20 @@ class QueryHandler:
         if n < 0:
             _check(-n)
         return list(e[:n]), list(it[:n]), int(r.value)
+
+    def autotune(self, dqueries, mode: Mode = Mode.EXACT, reps: int = 5, flags: int = 0):
+        """Pick the fastest expand-kernel variant per level on this batch; returns (variants, ms)."""
+        H = self.info()["height"]
+        ptr = dqueries.__cuda_array_interface__["data"][0]
+        b = _Batch(int(QueryType.RANGE), int(mode), int(dqueries.shape[0]), ptr, 1, 0, flags)
+        v = (ctypes.c_int * H)()
+        ms = (ctypes.c_float * H)()
+        _check(_load().tblaeq_autotune(self._h, ctypes.byref(b), reps, v, ms))
+        return list(v), list(ms)
+
+    def set_variants(self, variants):
+        arr = (ctypes.c_int * len(variants))(*[int(x) for x in variants])
+        _check(_load().tblaeq_set_variants(self._h, arr, len(variants)))
 
     def stream_handle(self) -> int:
         return _load().tblaeq_stream(self._h) or 0

@@ -353,6 +353,32 @@ int tblaeq_stage_times(tblaeq_handle* h, float* ms, int cap) {
     return c == TBLAEQ_OK ? n : -1;
 }
 
+int tblaeq_autotune(tblaeq_handle* h, const tblaeq_batch* b, int reps, int* variants_out, float* ms_out) {
+    if (int c = validateBatch(h, b)) return c;
+    if (!b->queriesOnDevice || b->qtype != TBLAEQ_RANGE)
+        return fail(TBLAEQ_ERR_INVALID, "autotune needs a range batch with device queries");
+    return guarded([&]() -> int {
+        Runtime& rt = h->qh->runtime();
+        const std::vector<float> t =
+            rt.engine->autotuneRange(b->queries, static_cast<uint32_t>(b->nq), b->mode, b->flags, reps);
+        const std::vector<int>& v = rt.engine->variants();
+        for (size_t i = 0; i < v.size(); ++i) {
+            if (variants_out) variants_out[i] = v[i];
+            if (ms_out) ms_out[i] = t[i];
+        }
+        return TBLAEQ_OK;
+    });
+}
+
+int tblaeq_set_variants(tblaeq_handle* h, const int* variants, uint64_t n) {
+    if (int c = checkPrepared(h)) return c;
+    if (!variants) return fail(TBLAEQ_ERR_INVALID, "null variants");
+    return guarded([&]() -> int {
+        h->qh->runtime().engine->setVariants(std::vector<int>(variants, variants + n));
+        return TBLAEQ_OK;
+    });
+}
+
 int tblaeq_host_array(const tblaeq_handle* h, int which, uint64_t l, const void** ptr, uint64_t* count) {
     if (!h || !ptr || !count) return fail(TBLAEQ_ERR_INVALID, "null argument");
     const HostIndex& x = h->qh->index();

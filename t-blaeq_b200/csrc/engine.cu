@@ -10,7 +10,53 @@ size_t align256(size_t v) { return (v + 255) & ~size_t(255); }
 }  // namespace
 
 BatchEngine::BatchEngine(const DeviceIndex& di, cudaStream_t stream)
-    : di_(di), stream_(stream), tile_(expandTile(static_cast<int>(di.D))) {}
+    : di_(di), stream_(stream), tile_(expandTile(static_cast<int>(di.D))),
+      variants_(static_cast<size_t>(di.height), kVariantDirect) {}
+
+void BatchEngine::setVariants(const std::vector<int>& v) {
+    if (v.size() != variants_.size()) throw std::invalid_argument("setVariants: one variant per expand launch");
+    for (int x : v)
+        if (x != kVariantDirect && x != kVariantStaged) throw std::invalid_argument("setVariants: unknown variant");
+    if (v != variants_) dropGraph();
+    variants_ = v;
+}
+
+std::vector<float> BatchEngine::autotuneRange(const double* dBoxes, uint32_t nq, int mode, unsigned flags, int reps) {
+    const int H = static_cast<int>(di_.height);
+    const bool wasTiming = timing_;
+    setTiming(true);
+    runRange(dBoxes, nq, mode, flags & ~kUseGraph);  // sizes the workspace
+    const std::vector<int> candidates{kVariantDirect, kVariantStaged};
+    std::vector<std::vector<float>> med(candidates.size(), std::vector<float>(H, 0.f));
+    for (size_t c = 0; c < candidates.size(); ++c) {
+        setVariants(std::vector<int>(H, candidates[c]));
+        enqueueRange(dBoxes, nq, mode, flags & ~kUseGraph);
+        status();
+        std::vector<std::vector<float>> samples(H);
+        for (int r = 0; r < std::max(1, reps); ++r) {
+            enqueueRange(dBoxes, nq, mode, flags & ~kUseGraph);
+            if (status() != 0) throw CudaError(cudaErrorLaunchFailure, "autotune batch reported a device status");
+            const std::vector<float> t = stageTimes();
+            for (int m = 0; m < H; ++m) samples[m].push_back(t[1 + m]);
+        }
+        for (int m = 0; m < H; ++m) {
+            std::sort(samples[m].begin(), samples[m].end());
+            med[c][m] = samples[m][samples[m].size() / 2];
+        }
+    }
+    std::vector<int> best(H, kVariantDirect);
+    std::vector<float> bestT(H, 0.f);
+    for (int m = 0; m < H; ++m) {
+        size_t bi = 0;
+        for (size_t c = 1; c < candidates.size(); ++c)
+            if (med[c][m] < med[bi][m]) bi = c;
+        best[m] = candidates[bi];
+        bestT[m] = med[bi][m];
+    }
+    setVariants(best);
+    setTiming(wasTiming);
+    return bestT;
+}
 
 BatchEngine::~BatchEngine() {
     dropGraph();
@@ -239,6 +285,7 @@ void BatchEngine::enqueueLaunches(const double* dBoxes, uint32_t nq, int mode, u
         a.scratch.levelItems = (wantLevels && m > 0) ? levels + static_cast<size_t>(m - 1) * nq : nullptr;
         a.D = D;
         a.useFma = 1;
+        a.variant = variants_[m];
         if (m < H - 1) {
             a.child.nodes = (mode == kModeExact) ? di_.nodeSub[m].as<NodeRec>() : di_.nodeRef[m].as<NodeRec>();
             a.fout = outView(1 - buf, hdrPtr(m + 1));

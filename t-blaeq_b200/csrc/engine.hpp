@@ -56,6 +56,13 @@ public:
     // Total results of the last batch (synchronises the stream).
     uint64_t lastTotal(uint32_t nq);
 
+    // Kernel variant (Variant) per expand launch m = 0..height-1; default direct everywhere.
+    void setVariants(const std::vector<int>& v);
+    const std::vector<int>& variants() const { return variants_; }
+    // Times every variant on this batch (median of `reps` runs per variant after a warm-up) and
+    // keeps the fastest per level. Returns the per-level median milliseconds of the choice.
+    std::vector<float> autotuneRange(const double* dBoxes, uint32_t nq, int mode, unsigned flags, int reps);
+
     // (entries, items) of every frontier header of the last batch, and the result count.
     void levelCounts(std::vector<uint64_t>& entries, std::vector<uint64_t>& items, uint64_t& results);
 
@@ -104,6 +111,7 @@ private:
     void dropGraph();
     bool timing_ = false;
     bool capturing_ = false;
+    std::vector<int> variants_;
     void record(int i);
     std::vector<cudaEvent_t> events_;
     cudaGraphExec_t graphExec_ = nullptr;

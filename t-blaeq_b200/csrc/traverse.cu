@@ -136,25 +136,182 @@ __device__ __forceinline__ void rebuild(const ExpandArgs& a, int dim, uint32_t e
     }
 }
 
-// Up to D = 8 the rebuilt coordinates fit 64 registers (4 CTAs per SM); wider rows get 2 CTAs.
-template <int D>
-constexpr int minBlocksFor() {
-    return (D > 0 && D <= 8) ? 4 : 2;
+// Shared-memory staging of child rows: every lane copies its own row with cp.async into a
+// per-warp ring of kStages rounds, so several rounds of loads are in flight per warp without
+// holding them in registers. Rows of even D move in 16-byte chunks with a padded stride (an odd
+// number of 16-byte chunks, so the eight lanes of a 128-bit shared-memory phase hit distinct
+// banks); rows of odd D move in 8-byte chunks (their 8*D-byte stride is already conflict-free).
+template <int D, bool STAGED>
+struct Staging {
+    static constexpr bool kOn = STAGED && D > 0;
+    static constexpr int kChunk = (D % 2 == 0) ? 16 : 8;
+    static constexpr int kChunks = kOn ? (8 * D) / kChunk : 0;
+    static constexpr int kStride = !kOn ? 0 : ((kChunk == 16 && (kChunks % 2) == 0) ? 8 * D + 16 : 8 * D);
+    static constexpr int kStages = 4;
+    static constexpr int kRounds = kWarpTile / 32;
+    static constexpr int kRowBytes = kOn ? kStages * 32 * kStride : 0;
+    static constexpr int kNodeBytes = kOn ? kStages * 32 * 16 : 0;
+    static constexpr int kCacheBytes = 3 * kRounds * 32 * 4;
+    static constexpr int kWindow = kWarpTile + 1;  // most entries a tile can overlap
+    static constexpr int kWindowBytes = 3 * kWindow * 4 + 4;
+    static constexpr int kWarpBytes = kRowBytes + kNodeBytes + kCacheBytes + ((kWindowBytes + 15) / 16) * 16;
+};
+
+// Launch shape of the expand kernels (independent warps per CTA and the register bound). These are
+// build-time tuning knobs; the defaults are the fastest measured on B200 for the benchmark index.
+#ifndef TBLAEQ_EXPAND_THREADS
+#define TBLAEQ_EXPAND_THREADS 128
+#endif
+#ifndef TBLAEQ_EXPAND_MIN_BLOCKS
+#define TBLAEQ_EXPAND_MIN_BLOCKS 8
+#endif
+#ifndef TBLAEQ_EXPAND_CACHE
+#define TBLAEQ_EXPAND_CACHE 0
+#endif
+constexpr int kExpandThreads = TBLAEQ_EXPAND_THREADS;
+
+template <int D, bool STAGED>
+constexpr size_t expandSmemBytes() {
+    return static_cast<size_t>(Staging<D, STAGED>::kWarpBytes) * (kExpandThreads / 32);
 }
 
-template <int D, int PRED, bool TO_RESULT>
-__global__ void __launch_bounds__(kThreads, minBlocksFor<D>()) expandKernel(ExpandArgs a) {
-    constexpr int R = kWarpTile / 32;  // rounds of 32 items per warp tile
-    // Per-warp cache of every item's row, entry and query between the two passes.
-    __shared__ uint32_t sRow[kThreads / 32][R][32];
-    __shared__ uint32_t sEnt[kThreads / 32][R][32];
-    __shared__ uint32_t sQ[kThreads / 32][R][32];
+__device__ __forceinline__ void cpAsync16(void* dst, const void* src) {
+    const unsigned s = static_cast<unsigned>(__cvta_generic_to_shared(dst));
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cpAsync8(void* dst, const void* src) {
+    const unsigned s = static_cast<unsigned>(__cvta_generic_to_shared(dst));
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(s), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cpAsyncCommit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cpAsyncWait() {
+    asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
+}
+
+template <int PRED, bool TO_RESULT>
+constexpr bool needsNode() {
+    return PRED == kPredRangeRadius || PRED == kPredKnnBound || (!TO_RESULT && (PRED == kPredMask || PRED == kPredAll));
+}
+
+// Applies the level predicate to a rebuilt item; cc receives the item's child count when the
+// output is a frontier.
+// Per-lane register cache of the current query's box (range) or point (KNN) and bound, reloaded
+// only when the item's query changes (queries change at entry boundaries, rarely within a warp).
+template <int DM, int PRED>
+struct QueryCache {
+    static constexpr bool kRange = PRED == kPredRangeRadius || PRED == kPredRangeBox;
+    static constexpr bool kKnn = PRED == kPredKnnBound || PRED == kPredKnnPoint;
+    uint32_t q = 0xffffffffu;
+    double lo[(kRange || kKnn) ? DM : 1];
+    double hi[kRange ? DM : 1];
+    double tau = 0.0;
+    __device__ __forceinline__ void load(const ExpandArgs& a, int dim, uint32_t nq) {
+        if (TBLAEQ_EXPAND_CACHE && nq == q) return;
+        q = nq;
+        if constexpr (kRange) {
+            const double* box = a.query.boxes + static_cast<size_t>(nq) * 2 * dim;
+#pragma unroll
+            for (int d = 0; d < DM; ++d) {
+                if (d < dim) {
+                    lo[d] = __ldg(box + d);
+                    hi[d] = __ldg(box + dim + d);
+                }
+            }
+        } else if constexpr (kKnn) {
+            const double* p = a.query.points + static_cast<size_t>(nq) * dim;
+#pragma unroll
+            for (int d = 0; d < DM; ++d)
+                if (d < dim) lo[d] = __ldg(p + d);
+            tau = __ldg(a.query.tau + nq);
+        }
+    }
+};
+
+// Per-lane register cache of the parent entry's coordinates.
+template <int D, int DM>
+struct ParentCache {
+    uint32_t e = 0xffffffffu;
+    double x[DM];
+    __device__ __forceinline__ void load(const ExpandArgs& a, int dim, uint32_t ne) {
+        if (TBLAEQ_EXPAND_CACHE && ne == e) return;
+        e = ne;
+        const double* xp = a.in.x + static_cast<size_t>(ne) * dim;
+        if constexpr (D > 0 && (D % 2) == 0) {
+#pragma unroll
+            for (int d = 0; d < D; d += 2) {
+                const double2 v = __ldg(reinterpret_cast<const double2*>(xp + d));
+                x[d] = v.x;
+                x[d + 1] = v.y;
+            }
+        } else {
+#pragma unroll
+            for (int d = 0; d < DM; ++d)
+                if (d < dim) x[d] = __ldg(xp + d);
+        }
+    }
+};
+
+template <int DM, int PRED, bool TO_RESULT>
+__device__ __forceinline__ bool testItem(const ExpandArgs& a, int dim, const double (&y)[DM],
+                                         const QueryCache<DM, PRED>& qc, uint32_t j, const NodeRec& nr,
+                                         uint32_t& cc) {
+    cc = 0;
+    if constexpr (PRED == kPredRangeRadius) {
+        const double dist = boxDist2<DM>(y, qc.lo, qc.hi, dim, a.useFma);
+        cc = nr.cnt;
+        return (cc > 0) && (dist <= __dmul_rn(nr.rad, nr.rad));
+    } else if constexpr (PRED == kPredMask) {
+        bool keep = a.child.mask[j] != 0;
+        if constexpr (!TO_RESULT) {
+            cc = nr.cnt;
+            keep = keep && cc > 0;
+        }
+        return keep;
+    } else if constexpr (PRED == kPredAll) {
+        if constexpr (!TO_RESULT) {
+            cc = nr.cnt;
+            return cc > 0;
+        }
+        return true;
+    } else if constexpr (PRED == kPredRangeBox) {
+        bool in = true;
+#pragma unroll
+        for (int d = 0; d < DM; ++d) {
+            if (d < dim) in = in && (qc.lo[d] <= y[d]) && (y[d] <= qc.hi[d]);
+        }
+        return in;
+    } else if constexpr (PRED == kPredKnnBound) {
+        const double dd = sqrt(pointDist2<DM>(y, qc.lo, dim, 1));
+        cc = nr.cnt;
+        return (cc > 0) && (dd - nr.rad <= qc.tau);
+    } else {  // kPredKnnPoint
+        return pointDist2<DM>(y, qc.lo, dim, 1) <= qc.tau * qc.tau;
+    }
+}
+
+template <int D, int PRED, bool TO_RESULT, bool STAGED>
+__global__ void __launch_bounds__(kExpandThreads, TBLAEQ_EXPAND_MIN_BLOCKS) expandKernel(ExpandArgs a) {
+    using S = Staging<D, STAGED>;
+    constexpr int R = S::kRounds;
     constexpr int DM = (D > 0) ? D : 32;
+    constexpr bool NODE = needsNode<PRED, TO_RESULT>();
     constexpr uint32_t FULL = 0xffffffffu;
+    extern __shared__ __align__(16) unsigned char smem[];
     const int dim = (D > 0) ? D : a.D;
     const int lane = threadIdx.x & 31;
+    const int w = threadIdx.x >> 5;
     const uint32_t lanesLe = (2u << lane) - 1u;  // lanes 0..lane (wraps to all lanes for lane 31)
     const uint32_t lanesLt = (1u << lane) - 1u;
+    unsigned char* warpSmem = smem + static_cast<size_t>(w) * S::kWarpBytes;
+    unsigned char* rowBuf = warpSmem;                                    // [kStages][32][kStride]
+    NodeRec* nodeBuf = reinterpret_cast<NodeRec*>(warpSmem + S::kRowBytes);  // [kStages][32]
+    uint32_t* sRow = reinterpret_cast<uint32_t*>(warpSmem + S::kRowBytes + S::kNodeBytes);  // [R][32]
+    uint32_t* sEnt = sRow + R * 32;
+    uint32_t* sQ = sEnt + R * 32;
+    uint32_t* wCp = sQ + R * 32;  // window of the tile's entries: prefix, first child, query
+    uint32_t* wCb = wCp + S::kWindow;
+    uint32_t* wQ = wCb + S::kWindow;
 
     const uint32_t entries = a.in.hdr[0];
     const uint32_t total = a.in.hdr[1];
@@ -174,111 +331,159 @@ __global__ void __launch_bounds__(kThreads, minBlocksFor<D>()) expandKernel(Expa
         if (tile >= nTiles) break;
         const uint32_t t0 = tile * kWarpTile;
 
-        // ---- pass 1: map every item to its entry, rebuild it and test it; keep one bit per item.
-        uint32_t keepBits = 0, aggCnt = 0, aggSum = 0;
-        const int w = threadIdx.x >> 5;
-        uint32_t cur = a.in.tileStart[tile];  // entry holding the first item of the round
+        // ---- phase A: stage the tile's entries in shared memory (one round of parallel loads),
+        // then map every item of the tile to its entry and child row.
+        const uint32_t eLo = a.in.tileStart[tile];
+        uint32_t eHi = (tile + 1 < nTiles) ? a.in.tileStart[tile + 1] : entries - 1;
+        if (eHi >= entries) eHi = entries - 1;
+        uint32_t W = eHi - eLo + 1;
+        if (W > S::kWindow) {
+            if (lane == 0) atomicOr(a.scratch.status, kStatusWindowOverflow);
+            W = S::kWindow;
+        }
+        for (uint32_t i = lane; i < W; i += 32) {
+            wCp[i] = a.in.cpre[eLo + i];
+            wCb[i] = a.in.cbeg[eLo + i];
+            wQ[i] = a.in.q[eLo + i];
+        }
+        __syncwarp();
+        uint32_t validBits = 0;
+        uint32_t cur = 0;  // window index of the entry holding the round's first item
 #pragma unroll
         for (int r = 0; r < R; ++r) {
             const uint32_t rs = t0 + r * 32;
             if (rs >= total) continue;  // warp-uniform
             const uint32_t k = rs + lane;
             const bool valid = k < total;
-            // The 32 entries from `cur` cover every entry overlapping this round unless entries with
-            // fewer than one child per lane follow (then each lane searches on its own).
+            // Every entry overlapping a 32-item round lies within the 32 window slots from `cur`:
+            // `cur` holds the round's first item and every other entry starts at a distinct item.
             const uint32_t ce = cur + lane;
-            const bool inRange = ce < entries;
-            const uint32_t cp = inRange ? a.in.cpre[ce] : 0xffffffffu;
-            const uint32_t cp31 = __shfl_sync(FULL, cp, 31);
-            uint32_t e, eCp, eCb, eQ;
-            if (cp31 + 1 < rs + 32 && cur + 32 < entries) {
-                uint32_t lo = cur, hi = entries - 1;
-                const uint32_t kk = valid ? k : rs;
-                while (lo < hi) {
-                    const uint32_t mid = (lo + hi + 1) >> 1;
-                    if (a.in.cpre[mid] <= kk) lo = mid; else hi = mid - 1;
-                }
-                e = lo;
-                eCp = a.in.cpre[e];
-                eCb = a.in.cbeg[e];
-                eQ = a.in.q[e];
-            } else {
-                const uint32_t cb = inRange ? a.in.cbeg[ce] : 0u;
-                const uint32_t cq = inRange ? a.in.q[ce] : 0u;
-                const uint32_t base = __popc(__ballot_sync(FULL, cp <= rs)) - 1u;
-                const uint32_t off = cp - rs;
-                const uint32_t starts = __reduce_or_sync(FULL, (cp > rs && off < 32u) ? (1u << off) : 0u);
-                const uint32_t my = base + __popc(starts & lanesLe);
-                e = cur + my;
-                eCp = __shfl_sync(FULL, cp, my);
-                eCb = __shfl_sync(FULL, cb, my);
-                eQ = __shfl_sync(FULL, cq, my);
-            }
-            cur = __shfl_sync(FULL, e, 31);
-            const uint32_t j = eCb + (k - eCp);
-            sRow[w][r][lane] = j;
-            sEnt[w][r][lane] = e;
-            sQ[w][r][lane] = eQ;
+            const uint32_t cp = ce < W ? wCp[ce] : 0xffffffffu;
+            const uint32_t base = __popc(__ballot_sync(FULL, cp <= rs)) - 1u;
+            const uint32_t off = cp - rs;
+            const uint32_t starts = __reduce_or_sync(FULL, (cp > rs && off < 32u) ? (1u << off) : 0u);
+            const uint32_t my = cur + base + __popc(starts & lanesLe);
+            const uint32_t e = my < W ? my : W - 1;
+            sRow[r * 32 + lane] = wCb[e] + (k - wCp[e]);
+            sEnt[r * 32 + lane] = eLo + e;
+            sQ[r * 32 + lane] = wQ[e];
+            validBits |= (valid ? 1u : 0u) << r;
+            // The next round's first item (rs + 32) lies in the entry holding this round's last item,
+            // or in the next entry when that one starts exactly there.
+            const uint32_t last = __shfl_sync(FULL, e, 31);
+            cur = (last + 1 < W && wCp[last + 1] == rs + 32) ? last + 1 : last;
+        }
+        __syncwarp();
 
+        // ---- phase B: stream the rows (and node records) through the cp.async ring and test.
+        auto issue = [&](int r) {
+            if constexpr (S::kOn) {
+                if ((validBits >> r) & 1u) {
+                    const uint32_t j = sRow[r * 32 + lane];
+                    const int slot = r % S::kStages;
+                    const unsigned char* src = reinterpret_cast<const unsigned char*>(a.child.rows) +
+                                               static_cast<size_t>(j) * (8 * D);
+                    unsigned char* dst = rowBuf + (slot * 32 + lane) * S::kStride;
+#pragma unroll
+                    for (int c = 0; c < S::kChunks; ++c) {
+                        if constexpr (S::kChunk == 16) {
+                            cpAsync16(dst + 16 * c, src + 16 * c);
+                        } else {
+                            cpAsync8(dst + 8 * c, src + 8 * c);
+                        }
+                    }
+                    if constexpr (NODE) {
+                        const uint32_t kk = a.child.keys ? static_cast<uint32_t>(a.child.keys[j]) : j;
+                        cpAsync16(&nodeBuf[slot * 32 + lane], &a.child.nodes[kk]);
+                    }
+                }
+            }
+        };
+        if constexpr (S::kOn) {
+#pragma unroll
+            for (int r = 0; r < S::kStages - 1; ++r) {
+                if (r < R) issue(r);
+                cpAsyncCommit();
+            }
+        }
+        uint32_t keepBits = 0, aggCnt = 0, aggSum = 0;
+        QueryCache<DM, PRED> qc;
+        ParentCache<D, DM> pc;
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+            if constexpr (S::kOn) {
+                if (r + S::kStages - 1 < R) issue(r + S::kStages - 1);
+                cpAsyncCommit();
+                cpAsyncWait<S::kStages - 1>();
+            }
+            if (t0 + r * 32 >= total) continue;  // warp-uniform
+            const bool valid = (validBits >> r) & 1u;
             bool keep = false;
             uint32_t cc = 0;
             if (valid) {
+                const uint32_t j = sRow[r * 32 + lane];
+                const uint32_t e = sEnt[r * 32 + lane];
+                const uint32_t q = sQ[r * 32 + lane];
                 double y[DM];
-                rebuild<D, DM>(a, dim, e, j, y);
-                const uint32_t kk = a.child.keys ? static_cast<uint32_t>(a.child.keys[j]) : j;
-                if constexpr (PRED == kPredRangeRadius) {
-                    const double* box = a.query.boxes + static_cast<size_t>(eQ) * 2 * dim;
-                    const double dist = boxDist2<DM>(y, box, box + dim, dim, a.useFma);
-                    const NodeRec nr = a.child.nodes[kk];
-                    cc = nr.cnt;
-                    keep = (cc > 0) && (dist <= __dmul_rn(nr.rad, nr.rad));
-                } else if constexpr (PRED == kPredMask) {
-                    keep = a.child.mask[j] != 0;
-                    if constexpr (!TO_RESULT) {
-                        cc = a.child.nodes[kk].cnt;
-                        keep = keep && cc > 0;
-                    }
-                } else if constexpr (PRED == kPredAll) {
-                    keep = true;
-                    if constexpr (!TO_RESULT) {
-                        cc = a.child.nodes[kk].cnt;
-                        keep = cc > 0;
-                    }
-                } else if constexpr (PRED == kPredRangeBox) {
-                    const double* box = a.query.boxes + static_cast<size_t>(eQ) * 2 * dim;
-                    bool in = true;
+                NodeRec nr{0.0, 0u, 0u};
+                qc.load(a, dim, q);
+                pc.load(a, dim, e);
+                if constexpr (S::kOn) {
+                    const int slot = r % S::kStages;
+                    const double* rowp = reinterpret_cast<const double*>(rowBuf + (slot * 32 + lane) * S::kStride);
+                    if constexpr (D % 2 == 0) {
 #pragma unroll
-                    for (int d = 0; d < DM; ++d) {
-                        if (d < dim) in = in && (box[d] <= y[d]) && (y[d] <= box[dim + d]);
+                        for (int d = 0; d < D; d += 2) {
+                            const double2 pv = *reinterpret_cast<const double2*>(rowp + d);
+                            y[d] = __dmul_rn(pv.x, pc.x[d]);
+                            y[d + 1] = __dmul_rn(pv.y, pc.x[d + 1]);
+                        }
+                    } else {
+#pragma unroll
+                        for (int d = 0; d < D; ++d) y[d] = __dmul_rn(rowp[d], pc.x[d]);
                     }
-                    keep = in;
-                } else if constexpr (PRED == kPredKnnBound) {
-                    const double* p = a.query.points + static_cast<size_t>(eQ) * dim;
-                    const double dd = sqrt(pointDist2<DM>(y, p, dim, 1));
-                    const NodeRec nr = a.child.nodes[kk];
-                    cc = nr.cnt;
-                    keep = (cc > 0) && (dd - nr.rad <= a.query.tau[eQ]);
-                } else if constexpr (PRED == kPredKnnPoint) {
-                    const double* p = a.query.points + static_cast<size_t>(eQ) * dim;
-                    const double t = a.query.tau[eQ];
-                    keep = pointDist2<DM>(y, p, dim, 1) <= t * t;
+                    if constexpr (NODE) nr = nodeBuf[slot * 32 + lane];
+                } else {
+                    const double* rp = a.child.rows + static_cast<size_t>(j) * dim;
+                    if constexpr (D > 0 && (D % 2) == 0) {
+#pragma unroll
+                        for (int d = 0; d < D; d += 2) {
+                            const double2 pv = __ldg(reinterpret_cast<const double2*>(rp + d));
+                            y[d] = __dmul_rn(pv.x, pc.x[d]);
+                            y[d + 1] = __dmul_rn(pv.y, pc.x[d + 1]);
+                        }
+                    } else {
+#pragma unroll
+                        for (int d = 0; d < DM; ++d)
+                            if (d < dim) y[d] = __dmul_rn(__ldg(rp + d), pc.x[d]);
+                    }
+                    if constexpr (NODE) {
+                        const uint32_t kk = a.child.keys ? static_cast<uint32_t>(a.child.keys[j]) : j;
+                        nr = a.child.nodes[kk];
+                    }
                 }
+                keep = testItem<DM, PRED, TO_RESULT>(a, dim, y, qc, j, nr, cc);
             }
             // Per-query generated-children counts (the reference's levelFineMeshSize).
             if (a.scratch.levelItems) {
                 const uint32_t vm = __ballot_sync(FULL, valid);
                 if (valid) {
-                    const uint32_t peers = __match_any_sync(vm, eQ);
-                    if (lane == __ffs(peers) - 1) atomicAdd(&a.scratch.levelItems[eQ], __popc(peers));
+                    const uint32_t q = sQ[r * 32 + lane];
+                    const uint32_t peers = __match_any_sync(vm, q);
+                    if (lane == __ffs(peers) - 1) atomicAdd(&a.scratch.levelItems[q], __popc(peers));
                 }
             }
             const uint32_t kb = __ballot_sync(FULL, keep);
-            keepBits |= (keep ? 1u : 0u) << r;
-            aggCnt += __popc(kb);
-            uint32_t s = keep ? cc : 0u;
+            if (kb) {  // warp-uniform
+                keepBits |= (keep ? 1u : 0u) << r;
+                aggCnt += __popc(kb);
+                if constexpr (!TO_RESULT) {
+                    uint32_t s = keep ? cc : 0u;
 #pragma unroll
-            for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(FULL, s, o);
-            aggSum += s;
+                    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(FULL, s, o);
+                    aggSum += s;
+                }
+            }
         }
 
         // ---- publish the tile's counts and learn where its output starts.
@@ -307,12 +512,12 @@ __global__ void __launch_bounds__(kThreads, minBlocksFor<D>()) expandKernel(Expa
             const bool keep = (keepBits >> r) & 1u;
             const uint32_t kb = __ballot_sync(FULL, keep);
             if (kb == 0) continue;  // warp-uniform
-            const uint32_t j = sRow[w][r][lane];
-            const uint32_t qr = sQ[w][r][lane];
+            const uint32_t j = sRow[r * 32 + lane];
+            const uint32_t qr = sQ[r * 32 + lane];
             uint32_t cc = 0, ncb = 0, kk = 0;
             double y[DM];
             if (keep) {
-                rebuild<D, DM>(a, dim, sEnt[w][r][lane], j, y);
+                rebuild<D, DM>(a, dim, sEnt[r * 32 + lane], j, y);
                 kk = a.child.keys ? static_cast<uint32_t>(a.child.keys[j]) : j;
                 if constexpr (!TO_RESULT) {
                     const NodeRec nr = a.child.nodes[kk];
@@ -322,12 +527,14 @@ __global__ void __launch_bounds__(kThreads, minBlocksFor<D>()) expandKernel(Expa
             }
             const uint32_t v = keep ? cc : 0u;
             uint32_t inc = v;
+            if constexpr (!TO_RESULT) {
 #pragma unroll
-            for (int o = 1; o < 32; o <<= 1) {
-                const uint32_t t = __shfl_up_sync(FULL, inc, o);
-                if (lane >= o) inc += t;
+                for (int o = 1; o < 32; o <<= 1) {
+                    const uint32_t t = __shfl_up_sync(FULL, inc, o);
+                    if (lane >= o) inc += t;
+                }
             }
-            const uint32_t roundSum = __shfl_sync(FULL, inc, 31);
+            const uint32_t roundSum = TO_RESULT ? 0u : __shfl_sync(FULL, inc, 31);
             if (keep) {
                 const unsigned long long pos = runCnt + __popc(kb & lanesLt);
                 if constexpr (TO_RESULT) {
@@ -432,59 +639,66 @@ __global__ void exclusiveScanKernel(const uint32_t* counts, uint64_t* offsets, u
     if (tid == 0) offsets[n] = sCarry;
 }
 
-template <int D, int PRED, bool TO_RESULT>
+template <int D, int PRED, bool TO_RESULT, bool STAGED>
 void launchOne(const ExpandArgs& a, int gridBlocks, cudaStream_t s) {
-    auto kern = expandKernel<D, PRED, TO_RESULT>;
-    if (gridBlocks <= 0) {
-        static int cached = 0;
-        if (cached == 0) {
-            int dev = 0, sms = 0, perSm = 0;
-            TBLAEQ_CUDA(cudaGetDevice(&dev));
-            TBLAEQ_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-            TBLAEQ_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, kern, kThreads, 0));
-            cached = std::max(1, sms * std::max(1, perSm));
-        }
-        gridBlocks = cached;
+    auto kern = expandKernel<D, PRED, TO_RESULT, STAGED>;
+    constexpr size_t smemBytes = expandSmemBytes<D, STAGED>();
+    static int cached = 0;
+    if (cached == 0) {
+        int dev = 0, sms = 0, perSm = 0;
+        TBLAEQ_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         static_cast<int>(smemBytes)));
+        TBLAEQ_CUDA(cudaGetDevice(&dev));
+        TBLAEQ_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+        TBLAEQ_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, kern, kExpandThreads, smemBytes));
+        cached = std::max(1, sms * std::max(1, perSm));
     }
-    kern<<<gridBlocks, kThreads, 0, s>>>(a);
+    if (gridBlocks <= 0) gridBlocks = cached;
+    kern<<<gridBlocks, kExpandThreads, smemBytes, s>>>(a);
     TBLAEQ_CUDA(cudaGetLastError());
 }
 
-template <int D>
+template <int D, bool ST>
 void dispatchPred(const ExpandArgs& a, int pred, bool toResult, int g, cudaStream_t s) {
     if (toResult) {
         switch (pred) {
-            case kPredAll: return launchOne<D, kPredAll, true>(a, g, s);
-            case kPredRangeBox: return launchOne<D, kPredRangeBox, true>(a, g, s);
-            case kPredMask: return launchOne<D, kPredMask, true>(a, g, s);
-            case kPredKnnPoint: return launchOne<D, kPredKnnPoint, true>(a, g, s);
+            case kPredAll: return launchOne<D, kPredAll, true, ST>(a, g, s);
+            case kPredRangeBox: return launchOne<D, kPredRangeBox, true, ST>(a, g, s);
+            case kPredMask: return launchOne<D, kPredMask, true, ST>(a, g, s);
+            case kPredKnnPoint: return launchOne<D, kPredKnnPoint, true, ST>(a, g, s);
             default: break;
         }
     } else {
         switch (pred) {
-            case kPredRangeRadius: return launchOne<D, kPredRangeRadius, false>(a, g, s);
-            case kPredMask: return launchOne<D, kPredMask, false>(a, g, s);
-            case kPredAll: return launchOne<D, kPredAll, false>(a, g, s);
-            case kPredKnnBound: return launchOne<D, kPredKnnBound, false>(a, g, s);
+            case kPredRangeRadius: return launchOne<D, kPredRangeRadius, false, ST>(a, g, s);
+            case kPredMask: return launchOne<D, kPredMask, false, ST>(a, g, s);
+            case kPredAll: return launchOne<D, kPredAll, false, ST>(a, g, s);
+            case kPredKnnBound: return launchOne<D, kPredKnnBound, false, ST>(a, g, s);
             default: break;
         }
     }
     throw std::invalid_argument("expand: unsupported predicate/output combination");
 }
 
+template <int D>
+void dispatchStaged(const ExpandArgs& a, int pred, bool toResult, int g, cudaStream_t s) {
+    if (a.variant == kVariantStaged) return dispatchPred<D, true>(a, pred, toResult, g, s);
+    return dispatchPred<D, false>(a, pred, toResult, g, s);
+}
+
 }  // namespace
 
 void launchExpand(const ExpandArgs& a, int pred, bool toResult, int gridBlocks, cudaStream_t stream) {
     switch (a.D) {
-        case 2: return dispatchPred<2>(a, pred, toResult, gridBlocks, stream);
-        case 3: return dispatchPred<3>(a, pred, toResult, gridBlocks, stream);
-        case 4: return dispatchPred<4>(a, pred, toResult, gridBlocks, stream);
-        case 5: return dispatchPred<5>(a, pred, toResult, gridBlocks, stream);
-        case 8: return dispatchPred<8>(a, pred, toResult, gridBlocks, stream);
-        case 16: return dispatchPred<16>(a, pred, toResult, gridBlocks, stream);
+        case 2: return dispatchStaged<2>(a, pred, toResult, gridBlocks, stream);
+        case 3: return dispatchStaged<3>(a, pred, toResult, gridBlocks, stream);
+        case 4: return dispatchStaged<4>(a, pred, toResult, gridBlocks, stream);
+        case 5: return dispatchStaged<5>(a, pred, toResult, gridBlocks, stream);
+        case 8: return dispatchStaged<8>(a, pred, toResult, gridBlocks, stream);
+        case 16: return dispatchStaged<16>(a, pred, toResult, gridBlocks, stream);
         default:
             if (a.D < 1 || a.D > 32) throw std::invalid_argument("expand: D must be in [1, 32]");
-            return dispatchPred<0>(a, pred, toResult, gridBlocks, stream);
+            return dispatchPred<0, false>(a, pred, toResult, gridBlocks, stream);
     }
 }
 

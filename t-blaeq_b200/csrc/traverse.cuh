@@ -107,6 +107,10 @@ enum Pred : int {
     kPredKnnPoint = 5,          // keep point if dist2 <= tau^2 (records dist2)
 };
 
+// Kernel variants an autotuner chooses between per level: rows loaded straight into registers,
+// or streamed through a per-warp cp.async ring in shared memory.
+enum Variant : int { kVariantDirect = 0, kVariantStaged = 1 };
+
 struct ExpandArgs {
     FrontierIn in;
     ChildLevel child;
@@ -116,6 +120,7 @@ struct ExpandArgs {
     Scratch scratch;
     int D;
     int useFma;                 // accumulate squared distances with fma (reference kernels' contraction)
+    int variant;                // Variant
 };
 
 // Launch the expand kernel for dimension D with the given predicate; `toResult` selects the
