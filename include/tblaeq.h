@@ -199,6 +199,23 @@ int tblaeq_host_array(const tblaeq_handle* h, int which, uint64_t l, const void*
 int tblaeq_decode_points(tblaeq_handle* h, const uint64_t* positions, uint64_t n, double* coords_out,
                          uint64_t* ids_out);
 
+/* Allocation-free per-level range step. No counterpart in the reference: it exists for callers
+ * that cannot allocate device memory while they query (a process that reserved its whole memory
+ * budget at start-up, or one whose rules forbid allocation between start-up and shutdown).
+ * Same result as tblaeq_level for a range query -- the grid of interval l after pruning, in the
+ * reference's order -- written into the caller's device buffers out_ids (out_cap entries) and
+ * out_vals (out_cap * D doubles); *out_n receives the number of entries.
+ * It calls no cudaMalloc/cudaFree and no allocating library routine: its scratch is one fixed
+ * array in device memory (about 2.4 MB), held by every GPU that loads the library until exit.
+ * Limits: in->nnz <= 16384, out_cap <= 1048576, D <= 16; larger requests fail with
+ * TBLAEQ_ERR_INVALID, outputs that do not fit with TBLAEQ_ERR_OVERFLOW.
+ * The first call on a device looks up the array's device address; make that first call before
+ * any stream capture. All calls on a device share the array: calls whose work overlaps on the
+ * GPU (other streams or handles on the same device) race and must be serialised by the caller. */
+int tblaeq_level_range_noalloc(tblaeq_handle* h, uint64_t l, const tblaeq_grid* in, const double* lo,
+                               const double* hi, uint64_t* out_ids, double* out_vals, uint64_t out_cap,
+                               uint64_t* out_n);
+
 /* Number of device bytes currently allocated by the library (leak checks). */
 uint64_t tblaeq_live_device_bytes(void);
 

@@ -6,6 +6,7 @@
 
 #include "../../include/tblaeq.h"
 #include "handler.hpp"
+#include "noalloc.hpp"
 
 using namespace tblaeq;
 
@@ -451,6 +452,23 @@ int tblaeq_decode_points(tblaeq_handle* h, const uint64_t* positions, uint64_t n
                 for (uint64_t d = 0; d < D; ++d) v[d] = x.pTensors[m - 1].vals[chain[m] * D + d] * v[d];
             for (uint64_t d = 0; d < D; ++d) coords_out[i * D + d] = v[d];
             if (ids_out) ids_out[i] = x.maps[H - 1][positions[i]];
+        }
+        return TBLAEQ_OK;
+    });
+}
+
+int tblaeq_level_range_noalloc(tblaeq_handle* h, uint64_t l, const tblaeq_grid* in, const double* lo,
+                               const double* hi, uint64_t* out_ids, double* out_vals, uint64_t out_cap,
+                               uint64_t* out_n) {
+    if (int c = checkPrepared(h)) return c;
+    if (!in || !lo || !hi || !out_n || (out_cap && (!out_ids || !out_vals)))
+        return fail(TBLAEQ_ERR_INVALID, "null argument");
+    return guarded([&]() -> int {
+        try {
+            *out_n = runLevelRangeNoAlloc(h->qh->runtime(), l, in->ids, in->vals, in->nnz, lo, hi, out_ids, out_vals,
+                                          out_cap);
+        } catch (const NoAllocOverflow& e) {
+            return fail(TBLAEQ_ERR_OVERFLOW, e.what());
         }
         return TBLAEQ_OK;
     });
