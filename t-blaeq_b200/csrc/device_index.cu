@@ -6,6 +6,7 @@
 #include <algorithm>
 #include <atomic>
 #include <cmath>
+#include <limits>
 #include <mutex>
 
 namespace tblaeq {
@@ -103,6 +104,50 @@ DerivedArrays computeDerived(const HostIndex& idx) {
                 parent[m + 1][j] = static_cast<uint32_t>(ppos);
                 for (uint64_t d = 0; d < D; ++d) dec[m + 1][j * D + d] = P.vals[j * D + d] * x[d];
             }
+        }
+    }
+
+    // Box of the finest points below every node (exact min / max of decoded coordinates), stored
+    // as floats rounded outward.
+    {
+        std::vector<std::vector<double>> bl(H - 1), bh(H - 1);
+        for (uint64_t m = 0; m + 1 < H; ++m) {
+            bl[m].assign(idx.meshCount(m) * D, std::numeric_limits<double>::infinity());
+            bh[m].assign(idx.meshCount(m) * D, -std::numeric_limits<double>::infinity());
+        }
+        const uint64_t nLeaf = idx.meshCount(H - 1);
+        for (uint64_t leafPos = 0; leafPos < nLeaf; ++leafPos) {
+            const double* x = &dec[H - 1][leafPos * D];
+            uint64_t pos = leafPos;
+            for (uint64_t m = H - 1; m > 0; --m) {
+                pos = parent[m][pos];  // position in mesh m-1
+                double* l = &bl[m - 1][pos * D];
+                double* u = &bh[m - 1][pos * D];
+                for (uint64_t d = 0; d < D; ++d) {
+                    l[d] = std::min(l[d], x[d]);
+                    u[d] = std::max(u[d], x[d]);
+                }
+            }
+        }
+        out.aabb.resize(H - 1);
+        auto down = [](double v) {
+            float f = static_cast<float>(v);
+            if (static_cast<double>(f) > v) f = std::nextafter(f, -std::numeric_limits<float>::infinity());
+            return f;
+        };
+        auto up = [](double v) {
+            float f = static_cast<float>(v);
+            if (static_cast<double>(f) < v) f = std::nextafter(f, std::numeric_limits<float>::infinity());
+            return f;
+        };
+        for (uint64_t m = 0; m + 1 < H; ++m) {
+            const uint64_t n = idx.meshCount(m);
+            out.aabb[m].resize(n * 2 * D);
+            for (uint64_t s = 0; s < n; ++s)
+                for (uint64_t d = 0; d < D; ++d) {
+                    out.aabb[m][s * 2 * D + d] = down(bl[m][s * D + d]);
+                    out.aabb[m][s * 2 * D + D + d] = up(bh[m][s * D + d]);
+                }
         }
     }
 
@@ -222,6 +267,7 @@ std::unique_ptr<DeviceIndex> buildDeviceIndex(const HostIndex& idx, const Derive
     di->nodeRef.resize(idx.height - 1);
     di->nodeSub.resize(idx.height - 1);
     di->leaf.resize(idx.height - 1);
+    di->aabb.resize(idx.height - 1);
     for (uint64_t m = 0; m + 1 < idx.height; ++m) {
         const size_t n = der.cbeg[m].size();
         std::vector<NodeRec> ref(n), sub(n);
@@ -232,6 +278,7 @@ std::unique_ptr<DeviceIndex> buildDeviceIndex(const HostIndex& idx, const Derive
         di->nodeRef[m] = upload(ref, s);
         di->nodeSub[m] = upload(sub, s);
         di->leaf[m] = upload(der.leaf[m], s);
+        di->aabb[m] = upload(der.aabb[m], s);
         TBLAEQ_CUDA(cudaStreamSynchronize(s));
     }
     TBLAEQ_CUDA(cudaStreamSynchronize(s));
@@ -240,7 +287,7 @@ std::unique_ptr<DeviceIndex> buildDeviceIndex(const HostIndex& idx, const Derive
 
 size_t DeviceIndex::deviceBytes() const {
     size_t t = coarseVals.bytes() + coarseIds.bytes();
-    for (auto* v : {&pvals, &nodeRef, &nodeSub, &leaf, &nodeOrig, &maps})
+    for (auto* v : {&pvals, &nodeRef, &nodeSub, &leaf, &aabb, &nodeOrig, &maps})
         for (auto& m : *v) t += m.bytes();
     return t;
 }

@@ -77,6 +77,9 @@ struct DerivedArrays {
     // position-space per mesh m < height-1
     std::vector<std::vector<uint32_t>> cbeg, ccnt, leaf;
     std::vector<std::vector<double>> radRef, radSub;
+    // Axis-aligned box of the finest points below each node: lo[D] then hi[D] per node, in float
+    // rounded outward (lo down, hi up), so it always contains the decoded points.
+    std::vector<std::vector<float>> aabb;
 };
 
 // Host computation of the position-space node arrays, including subtree radii from the decoded
@@ -92,6 +95,7 @@ struct DeviceIndex {
     std::vector<DeviceMem> pvals;            // interval l: rows of P_l (n_{l+1} * D)
     std::vector<DeviceMem> nodeRef, nodeSub; // mesh m < height-1: NodeRec {radius, first child, children}
     std::vector<DeviceMem> leaf;             // mesh m < height-1: finest points below each node (uint32)
+    std::vector<DeviceMem> aabb;             // mesh m < height-1: outward-rounded float box of the points below
 
     // original-id space (per-level plugin)
     DeviceMem coarseIds;                     // uint64

@@ -288,6 +288,7 @@ void BatchEngine::enqueueLaunches(const double* dBoxes, uint32_t nq, int mode, u
         a.variant = variants_[m];
         if (m < H - 1) {
             a.child.nodes = (mode == kModeExact) ? di_.nodeSub[m].as<NodeRec>() : di_.nodeRef[m].as<NodeRec>();
+            a.child.aabb = (mode == kModeExact) ? di_.aabb[m].as<float>() : nullptr;
             a.fout = outView(1 - buf, hdrPtr(m + 1));
             launchExpand(a, kPredRangeRadius, false, 0, stream_);
             buf = 1 - buf;

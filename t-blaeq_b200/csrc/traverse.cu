@@ -254,13 +254,25 @@ struct ParentCache {
 
 template <int DM, int PRED, bool TO_RESULT>
 __device__ __forceinline__ bool testItem(const ExpandArgs& a, int dim, const double (&y)[DM],
-                                         const QueryCache<DM, PRED>& qc, uint32_t j, const NodeRec& nr,
+                                         const QueryCache<DM, PRED>& qc, uint32_t j, uint32_t kk, const NodeRec& nr,
                                          uint32_t& cc) {
     cc = 0;
     if constexpr (PRED == kPredRangeRadius) {
         const double dist = boxDist2<DM>(y, qc.lo, qc.hi, dim, a.useFma);
         cc = nr.cnt;
-        return (cc > 0) && (dist <= __dmul_rn(nr.rad, nr.rad));
+        bool keep = (cc > 0) && (dist <= __dmul_rn(nr.rad, nr.rad));
+        if (keep && a.child.aabb) {
+            // Exact mode only: the query box must also meet the box of the points below the child.
+            const float* b = a.child.aabb + static_cast<size_t>(kk) * 2 * dim;
+#pragma unroll
+            for (int d = 0; d < DM; ++d) {
+                if (d < dim) {
+                    keep = keep && (static_cast<double>(__ldg(b + d)) <= qc.hi[d]) &&
+                           (static_cast<double>(__ldg(b + dim + d)) >= qc.lo[d]);
+                }
+            }
+        }
+        return keep;
     } else if constexpr (PRED == kPredMask) {
         bool keep = a.child.mask[j] != 0;
         if constexpr (!TO_RESULT) {
@@ -426,6 +438,7 @@ __global__ void __launch_bounds__(kExpandThreads, TBLAEQ_EXPAND_MIN_BLOCKS) expa
                 const uint32_t q = sQ[r * 32 + lane];
                 double y[DM];
                 NodeRec nr{0.0, 0u, 0u};
+                uint32_t kk = j;
                 qc.load(a, dim, q);
                 pc.load(a, dim, e);
                 if constexpr (S::kOn) {
@@ -443,6 +456,7 @@ __global__ void __launch_bounds__(kExpandThreads, TBLAEQ_EXPAND_MIN_BLOCKS) expa
                         for (int d = 0; d < D; ++d) y[d] = __dmul_rn(rowp[d], pc.x[d]);
                     }
                     if constexpr (NODE) nr = nodeBuf[slot * 32 + lane];
+                    kk = a.child.keys ? static_cast<uint32_t>(a.child.keys[j]) : j;
                 } else {
                     const double* rp = a.child.rows + static_cast<size_t>(j) * dim;
                     if constexpr (D > 0 && (D % 2) == 0) {
@@ -457,12 +471,10 @@ __global__ void __launch_bounds__(kExpandThreads, TBLAEQ_EXPAND_MIN_BLOCKS) expa
                         for (int d = 0; d < DM; ++d)
                             if (d < dim) y[d] = __dmul_rn(__ldg(rp + d), pc.x[d]);
                     }
-                    if constexpr (NODE) {
-                        const uint32_t kk = a.child.keys ? static_cast<uint32_t>(a.child.keys[j]) : j;
-                        nr = a.child.nodes[kk];
-                    }
+                    kk = a.child.keys ? static_cast<uint32_t>(a.child.keys[j]) : j;
+                    if constexpr (NODE) nr = a.child.nodes[kk];
                 }
-                keep = testItem<DM, PRED, TO_RESULT>(a, dim, y, qc, j, nr, cc);
+                keep = testItem<DM, PRED, TO_RESULT>(a, dim, y, qc, j, kk, nr, cc);
             }
             // Per-query generated-children counts (the reference's levelFineMeshSize).
             if (a.scratch.levelItems) {

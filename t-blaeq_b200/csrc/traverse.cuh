@@ -81,6 +81,7 @@ struct ChildLevel {
     const double* rows;         // row j: D factors (P-tensor row, or coordinates with x = 1)
     const uint64_t* keys;       // optional key of row j into the node records (null: key = j)
     const NodeRec* nodes;       // child node records (by key)
+    const float* aabb;          // optional box of the points below each child (by key): lo[D] hi[D]
     const uint8_t* mask;        // keep flags (by row) for kPredMask
     const uint64_t* outMap;     // final output id of row j (null: id = key)
 };
