@@ -249,7 +249,7 @@ def main():
     ids_h = torch.empty(cap, dtype=torch.int64).pin_memory()
     import ctypes
     lib = tb.lib()
-    b = tb._Batch(int(tb.QueryType.RANGE), int(tb.Mode.EXACT), args.nq, hostQ.data_ptr(), 0, 0, 0)
+    b = tb._Batch(int(tb.QueryType.RANGE), int(tb.Mode.EXACT), args.nq, hostQ.data_ptr(), 0, 0, 0, None)
     tot = ctypes.c_uint64()
     P64 = ctypes.POINTER(ctypes.c_uint64)
     def e2e_call():

@@ -78,8 +78,9 @@ typedef struct {
     uint64_t nq;
     const double* queries;  /* RANGE: nq rows lo[D] hi[D]; POINT: nq rows point[D] */
     int queriesOnDevice;    /* 1: `queries` is a device pointer */
-    uint64_t K;             /* KNN: neighbours per query */
+    uint64_t K;             /* KNN: neighbours per query (when kPerQuery is NULL) */
     unsigned flags;         /* tblaeq_batch_flags */
+    const uint32_t* kPerQuery; /* KNN: optional host array of nq neighbour counts */
 } tblaeq_batch;
 
 typedef struct {
@@ -138,7 +139,9 @@ int tblaeq_coarsest_grid(tblaeq_handle* h, tblaeq_grid* out);
 
 /* Batched traversal of many queries in one pass over the hierarchy (replaces the one-query loop
  * of QueryEngine::run, src/core/QueryEngine.cu:109-252). Result pointers are device memory owned
- * by the handle, valid until the next batch call. */
+ * by the handle, valid until the next batch call. KNN batches are exact (mode must be
+ * TBLAEQ_MODE_EXACT): each query's K nearest points by FP64 squared distance, ties broken by
+ * smaller id, ascending; the reference's per-level KNN candidate sets come from tblaeq_level. */
 int tblaeq_query_batch(tblaeq_handle* h, const tblaeq_batch* batch, tblaeq_batch_result* out);
 
 /* Same as tblaeq_query_batch with host buffers on both sides: queries are copied to the device,

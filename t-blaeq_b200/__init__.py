@@ -82,7 +82,7 @@ class Grid(ctypes.Structure):
 class _Batch(ctypes.Structure):
     _fields_ = [("qtype", ctypes.c_int), ("mode", ctypes.c_int), ("nq", ctypes.c_uint64),
                 ("queries", ctypes.c_void_p), ("queriesOnDevice", ctypes.c_int), ("K", ctypes.c_uint64),
-                ("flags", ctypes.c_uint)]
+                ("flags", ctypes.c_uint), ("kPerQuery", ctypes.c_void_p)]
 
 
 class _BatchResult(ctypes.Structure):
@@ -151,6 +151,16 @@ def lib():
 def _check(code: int):
     if code != 0:
         raise TblaeqError(code, _load().tblaeq_last_error().decode())
+
+
+def _k_args(K, nq):
+    """(per-query uint32 array or None, uniform K) for a batch."""
+    if np.isscalar(K):
+        return None, int(K)
+    kq = np.ascontiguousarray(np.asarray(K, dtype=np.uint32))
+    if kq.shape != (nq,):
+        raise ValueError("K must be an int or one value per query")
+    return kq, 0
 
 
 def _dptr(a: np.ndarray, ctype=ctypes.c_double):
@@ -351,9 +361,10 @@ class QueryHandler:
         return ids, vals
 
     # -- batched engine --------------------------------------------------------------------------
-    def query_batch(self, qtype: QueryType, queries, mode: Mode = Mode.EXACT, K: int = 0,
+    def query_batch(self, qtype: QueryType, queries, mode: Mode = Mode.EXACT, K=0,
                     flags: int = 0) -> BatchResult:
-        """Batched traversal; `queries` is a numpy array (host) or a CUDA tensor (device)."""
+        """Batched traversal; `queries` is a numpy array (host) or a CUDA tensor (device).
+        For KNN, K is an int or a per-query sequence."""
         on_dev = hasattr(queries, "__cuda_array_interface__")
         if on_dev:
             ptr = queries.__cuda_array_interface__["data"][0]
@@ -363,10 +374,11 @@ class QueryHandler:
             keep = np.ascontiguousarray(np.asarray(queries, dtype=np.float64))
             ptr = keep.ctypes.data
             nq = keep.shape[0]
-        b = _Batch(int(qtype), int(mode), nq, ptr, int(on_dev), K, flags)
+        kq, kval = _k_args(K, nq)
+        b = _Batch(int(qtype), int(mode), nq, ptr, int(on_dev), kval, flags, kq.ctypes.data if kq is not None else None)
         r = _BatchResult()
         _check(_load().tblaeq_query_batch(self._h, ctypes.byref(b), ctypes.byref(r)))
-        del keep
+        del keep, kq
         D = self.info()["D"]
         ivl = self.info()["intervals"]
         return BatchResult(
@@ -380,7 +392,7 @@ class QueryHandler:
     def query_batch_async(self, qtype: QueryType, dqueries, mode: Mode = Mode.EXACT, K: int = 0, flags: int = 0):
         """Enqueue on the handle's stream without waiting (device queries; see tblaeq_query_batch_async)."""
         ptr = dqueries.__cuda_array_interface__["data"][0]
-        b = _Batch(int(qtype), int(mode), int(dqueries.shape[0]), ptr, 1, K, flags)
+        b = _Batch(int(qtype), int(mode), int(dqueries.shape[0]), ptr, 1, K, flags, None)
         _check(_load().tblaeq_query_batch_async(self._h, ctypes.byref(b)))
 
     def batch_wait(self) -> int:
@@ -402,7 +414,7 @@ class QueryHandler:
         """Pick the fastest expand-kernel variant per level on this batch; returns (variants, ms)."""
         H = self.info()["height"]
         ptr = dqueries.__cuda_array_interface__["data"][0]
-        b = _Batch(int(QueryType.RANGE), int(mode), int(dqueries.shape[0]), ptr, 1, 0, flags)
+        b = _Batch(int(QueryType.RANGE), int(mode), int(dqueries.shape[0]), ptr, 1, 0, flags, None)
         v = (ctypes.c_int * H)()
         ms = (ctypes.c_float * H)()
         _check(_load().tblaeq_autotune(self._h, ctypes.byref(b), reps, v, ms))
@@ -436,7 +448,9 @@ class QueryHandler:
             ids = np.empty(cap, np.uint64)
             d2 = np.empty(cap, np.float64) if qtype == QueryType.POINT else None
             total = ctypes.c_uint64()
-            b = _Batch(int(qtype), int(mode), nq, q.ctypes.data, 0, K, 0)
+            kq, kval = _k_args(K, nq)
+            b = _Batch(int(qtype), int(mode), nq, q.ctypes.data, 0, kval, 0,
+                       kq.ctypes.data if kq is not None else None)
             code = _load().tblaeq_query_batch_host(self._h, ctypes.byref(b), _dptr(offs, ctypes.c_uint64),
                                                    _dptr(ids, ctypes.c_uint64), cap,
                                                    _dptr(d2) if d2 is not None else None, ctypes.byref(total))

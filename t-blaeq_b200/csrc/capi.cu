@@ -15,6 +15,7 @@ struct tblaeq_handle {
     DeviceMem stage;                            // device staging for host-side query batches
     std::vector<std::vector<uint32_t>> parent;  // parent position per mesh (lazy, decode_points)
     std::vector<std::vector<uint64_t>> posOf;   // position of each original id per mesh (lazy)
+    DeviceMem kStage;                           // per-query K of KNN batches
     uint64_t lastNq = 0;                        // last asynchronously enqueued batch
     unsigned lastFlags = 0;
 };
@@ -205,9 +206,26 @@ int tblaeq_coarsest_grid(tblaeq_handle* h, tblaeq_grid* out) {
 
 static int runBatch(tblaeq_handle* h, const tblaeq_batch* b, const double* dQueries, tblaeq_batch_result* out) {
     Runtime& rt = h->qh->runtime();
-    if (b->qtype != TBLAEQ_RANGE) return fail(TBLAEQ_ERR_INVALID, "batched KNN is not available in this build");
     if (b->nq > 0xffffffffull) return fail(TBLAEQ_ERR_OVERFLOW, "too many queries in one batch");
-    const BatchOutput o = rt.engine->runRange(dQueries, static_cast<uint32_t>(b->nq), b->mode, b->flags);
+    BatchOutput o;
+    if (b->qtype == TBLAEQ_POINT) {
+        if (b->mode != TBLAEQ_MODE_EXACT)
+            return fail(TBLAEQ_ERR_INVALID, "batched KNN is exact; use tblaeq_level for the reference's STEP sets");
+        std::vector<uint32_t> k(b->nq);
+        uint64_t sumK = 0;
+        for (uint64_t i = 0; i < b->nq; ++i) {
+            const uint64_t v = b->kPerQuery ? b->kPerQuery[i] : b->K;
+            if (v > 0xffffffffull) return fail(TBLAEQ_ERR_INVALID, "K too large");
+            k[i] = static_cast<uint32_t>(v);
+            sumK += v;
+        }
+        if (h->kStage.bytes() < std::max<size_t>(b->nq, 1) * 4) h->kStage.alloc(std::max<size_t>(b->nq, 1) * 4);
+        if (b->nq)
+            TBLAEQ_CUDA(cudaMemcpyAsync(h->kStage.get(), k.data(), b->nq * 4, cudaMemcpyHostToDevice, rt.stream));
+        o = rt.engine->runKnn(dQueries, static_cast<uint32_t>(b->nq), h->kStage.as<uint32_t>(), sumK, b->flags);
+    } else {
+        o = rt.engine->runRange(dQueries, static_cast<uint32_t>(b->nq), b->mode, b->flags);
+    }
     h->lastNq = b->nq;
     h->lastFlags = b->flags;
     out->nq = b->nq;

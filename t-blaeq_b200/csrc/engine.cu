@@ -1,6 +1,10 @@
 // Batched traversal engine (range queries; see engine.hpp).
 #include "engine.hpp"
 
+#include <limits>
+
+#include "knn.cuh"
+
 #include <algorithm>
 
 namespace tblaeq {
@@ -115,7 +119,8 @@ void BatchEngine::levelCounts(std::vector<uint64_t>& entries, std::vector<uint64
 
 uint64_t BatchEngine::lastTotal(uint32_t nq) {
     uint64_t total = 0;
-    TBLAEQ_CUDA(cudaMemcpyAsync(&total, offsets_.as<uint64_t>() + nq, 8, cudaMemcpyDeviceToHost, stream_));
+    const uint64_t* off = lastKnn_ ? knnOff_.as<uint64_t>() : offsets_.as<uint64_t>();
+    TBLAEQ_CUDA(cudaMemcpyAsync(&total, off + nq, 8, cudaMemcpyDeviceToHost, stream_));
     TBLAEQ_CUDA(cudaStreamSynchronize(stream_));
     return total;
 }
@@ -256,6 +261,7 @@ void BatchEngine::enqueueRange(const double* dBoxes, uint32_t nq, int mode, unsi
 }
 
 void BatchEngine::enqueueLaunches(const double* dBoxes, uint32_t nq, int mode, unsigned flags) {
+    lastKnn_ = false;
     const int H = static_cast<int>(di_.height);
     const int D = static_cast<int>(di_.D);
     char* z = zeroBlock_.as<char>();
@@ -348,6 +354,15 @@ void BatchEngine::growFromHeaders() {
 BatchOutput BatchEngine::output(uint32_t nq, unsigned flags) const {
     BatchOutput o;
     o.nq = nq;
+    if (lastKnn_) {
+        o.offsets = knnOff_.as<uint64_t>();
+        o.ids = knnIds_.as<uint64_t>();
+        o.dist2 = knnD2_.as<double>();
+        o.levelItems = (flags & kWantLevels)
+                           ? reinterpret_cast<const uint32_t*>(zeroBlock_.as<char>() + offLevels_)
+                           : nullptr;
+        return o;
+    }
     o.offsets = offsets_.as<uint64_t>();
     o.ids = resIds_.as<uint64_t>();
     o.vals = (flags & kWantVals) ? resVals_.as<double>() : nullptr;
@@ -450,6 +465,105 @@ uint64_t BatchEngine::runGridLevel(int l, const uint64_t* dIds, const double* dV
         reserve(want, 1, 0);
     }
     throw CudaError(cudaErrorMemoryAllocation, "per-level workspace did not converge");
+}
+
+}  // namespace tblaeq
+
+namespace tblaeq {
+
+void BatchEngine::enqueueKnn(const double* dPoints, uint32_t nq, const uint32_t* dK, unsigned flags) {
+    lastKnn_ = true;
+    const int H = static_cast<int>(di_.height);
+    const int D = static_cast<int>(di_.D);
+    char* z = zeroBlock_.as<char>();
+    auto* desc = reinterpret_cast<unsigned long long*>(z + offDesc_);
+    auto* tickets = reinterpret_cast<uint32_t*>(z + offTickets_);
+    auto* status = reinterpret_cast<uint32_t*>(z + offStatus_);
+    auto* qcount = reinterpret_cast<uint32_t*>(z + offQcount_);
+    auto* levels = reinterpret_cast<uint32_t*>(z + offLevels_);
+    const bool wantLevels = (flags & kWantLevels) != 0;
+    double* tau = tau_.as<double>();
+
+    if (timing_) record(0);
+    TBLAEQ_CUDA(cudaMemsetAsync(z, 0, zeroBytes_, stream_));
+    launchFillDouble(tau, std::numeric_limits<double>::infinity(), nq, stream_);
+    const FrontierBufs& r0 = f_[0];
+    launchRootFrontier(r0.q.as<uint32_t>(), r0.cbeg.as<uint32_t>(), r0.cpre.as<uint32_t>(), r0.x.as<double>(),
+                       r0.tileStart.as<uint32_t>(), hdrPtr(0), nq, static_cast<uint32_t>(di_.meshCount[0]), D, tile_,
+                       stream_);
+    if (timing_) record(1);
+    int buf = 0;
+    for (int m = 0; m < H; ++m) {
+        ExpandArgs a{};
+        a.in = inView(buf, hdrPtr(m));
+        a.child.rows = (m == 0) ? di_.coarseVals.as<double>() : di_.pvals[m - 1].as<double>();
+        a.query.points = dPoints;
+        a.query.tau = tau;
+        a.query.k = dK;
+        a.scratch.desc = desc + static_cast<size_t>(m) * tileCap_;
+        a.scratch.ticket = tickets + m;
+        a.scratch.status = status;
+        a.scratch.levelItems = (wantLevels && m > 0) ? levels + static_cast<size_t>(m - 1) * nq : nullptr;
+        a.D = D;
+        a.useFma = 1;
+        a.variant = kVariantDirect;
+        if (m < H - 1) {
+            a.child.nodes = di_.nodeSub[m].as<NodeRec>();
+            a.child.aabb = di_.aabb[m].as<float>();
+            a.child.leaf = di_.leaf[m].as<uint32_t>();
+            a.fout = outView(1 - buf, hdrPtr(m + 1));
+            launchExpand(a, kPredKnnBound, false, 0, stream_);
+            buf = 1 - buf;
+        } else {
+            a.child.outMap = di_.maps[H - 1].as<uint64_t>();
+            a.rout.ids = resIds_.as<uint64_t>();
+            a.rout.q = resQ_.as<uint32_t>();
+            a.rout.dist2 = resDist_.as<double>();
+            a.rout.qcount = qcount;
+            a.rout.hdr = hdrPtr(H);
+            a.rout.cap = static_cast<uint32_t>(caps_.results);
+            launchExpand(a, kPredKnnPoint, true, 0, stream_);
+        }
+        if (timing_) record(2 + m);
+    }
+    // Candidates are query-major, so per-query offsets follow from the per-query counts.
+    launchExclusiveScan(qcount, candOff_.as<uint64_t>(), nq, stream_);
+    launchClampCounts(candOff_.as<uint64_t>(), dK, nq, knnCount_.as<uint32_t>(), stream_);
+    launchExclusiveScan(knnCount_.as<uint32_t>(), knnOff_.as<uint64_t>(), nq, stream_);
+    launchTopK(candOff_.as<uint64_t>(), resIds_.as<uint64_t>(), resDist_.as<double>(), nullptr, nullptr, nullptr, dK,
+               nq, knnOff_.as<uint64_t>(), knnIds_.as<uint64_t>(), knnD2_.as<double>(), knnCount_.as<uint32_t>(),
+               status, stream_);
+    if (timing_) record(2 + H);
+}
+
+BatchOutput BatchEngine::runKnn(const double* dPoints, uint32_t nq, const uint32_t* dK, uint64_t sumK,
+                                unsigned flags) {
+    reserve(caps_, nq, flags);
+    if (tau_.bytes() < static_cast<size_t>(nq) * 8 || knnCount_.bytes() < static_cast<size_t>(nq) * 4) {
+        tau_.alloc(std::max<size_t>(nq, 1) * 8);
+        knnCount_.alloc(std::max<size_t>(nq, 1) * 4);
+        candOff_.alloc((static_cast<size_t>(nq) + 1) * 8);
+        knnOff_.alloc((static_cast<size_t>(nq) + 1) * 8);
+    }
+    if (knnCap_ < std::max<uint64_t>(sumK, 1)) {
+        knnCap_ = std::max<uint64_t>(sumK, 1);
+        knnIds_.alloc(knnCap_ * 8);
+        knnD2_.alloc(knnCap_ * 8);
+    }
+    for (int attempt = 0; attempt < 16; ++attempt) {
+        enqueueKnn(dPoints, nq, dK, flags);
+        const uint32_t st = status();
+        if (st & (kStatusLookbackTimeout | kStatusWindowOverflow))
+            throw CudaError(cudaErrorLaunchTimeout, "traversal kernel reported status " + std::to_string(st));
+        if (st == 0) {
+            BatchOutput o = output(nq, flags);
+            o.total = lastTotal(nq);
+            return o;
+        }
+        growFromHeaders();
+        if (tau_.bytes() < static_cast<size_t>(nq) * 8) tau_.alloc(static_cast<size_t>(nq) * 8);
+    }
+    throw CudaError(cudaErrorMemoryAllocation, "KNN workspace did not converge after 16 growth steps");
 }
 
 }  // namespace tblaeq

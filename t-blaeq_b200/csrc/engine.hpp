@@ -48,6 +48,12 @@ public:
     // Range batch: dBoxes = nq rows of lo[D] then hi[D] (device). Blocks until done.
     BatchOutput runRange(const double* dBoxes, uint32_t nq, int mode, unsigned flags);
 
+    // Exact KNN batch: dPoints = nq rows of D coordinates, dK = neighbours per query (device),
+    // sumK = sum of K over the batch (host). Results: per-query offsets, ids and squared distances,
+    // ascending by (distance, id). Blocks until done.
+    BatchOutput runKnn(const double* dPoints, uint32_t nq, const uint32_t* dK, uint64_t sumK, unsigned flags);
+    void enqueueKnn(const double* dPoints, uint32_t nq, const uint32_t* dK, unsigned flags);
+
     // Enqueue a range batch without synchronising (capacities must already suffice; used for
     // CUDA-graph capture and timing). check() afterwards reports overflow / timeouts.
     void enqueueRange(const double* dBoxes, uint32_t nq, int mode, unsigned flags);
@@ -101,6 +107,9 @@ private:
     DeviceMem resIds_, resVals_, resQ_, resDist_;
     DeviceMem zeroBlock_;  // desc | tickets | status | hdrs | qcount | levelItems
     DeviceMem offsets_;
+    DeviceMem tau_, candOff_, knnCount_, knnOff_, knnIds_, knnD2_;
+    uint64_t knnCap_ = 0;
+    bool lastKnn_ = false;
     size_t zeroBytes_ = 0;
     // offsets into zeroBlock_
     size_t offDesc_ = 0, offTickets_ = 0, offStatus_ = 0, offHdr_ = 0, offQcount_ = 0, offLevels_ = 0;

@@ -1,6 +1,8 @@
 // C++ host facade: QueryHandler, PolicyScheduler and the B200 per-level strategy.
 #include "handler.hpp"
 
+#include "knn.cuh"
+
 #include <algorithm>
 #include <iomanip>
 #include <iostream>
@@ -82,6 +84,12 @@ Runtime::~Runtime() {
     pluginEngine.reset();
     levelOut.clear();
     pluginMask.release();
+    knnKeys.release();
+    knnKeys2.release();
+    knnLabels.release();
+    knnLabels2.release();
+    knnCnt.release();
+    knnRr.release();
     scratchQuery.release();
     dev.reset();
     if (stream) cudaStreamDestroy(stream);
@@ -158,9 +166,34 @@ LevelResult B200Strategy::runLevel(size_t l, const Grid& cur, QueryType qType, c
                                            rt_.scratchQuery.as<double>(), nullptr, out.ids.as<uint64_t>(),
                                            out.vals.as<double>(), cap);
     } else {
-        (void)queryPoint;
-        (void)K;
-        throw std::runtime_error("runLevel: KNN per-level plugin is not available in this build");
+        // The reference's KNN level: lower bounds, sort, STEP -> mask, then the same expansion.
+        const uint64_t p = cur.nnz;
+        if (p > 0) {
+            if (rt_.knnCap < p) {
+                rt_.knnKeys.alloc(p * 8);
+                rt_.knnKeys2.alloc(p * 8);
+                rt_.knnLabels.alloc(p * 4);
+                rt_.knnLabels2.alloc(p * 4);
+                rt_.knnCnt.alloc(p * 4);
+                rt_.knnRr.alloc(p * 8);
+                rt_.pluginMask.alloc(p);
+                rt_.knnCap = p;
+            }
+            TBLAEQ_CUDA(cudaMemcpyAsync(rt_.scratchQuery.as<double>(), queryPoint, D * 8, cudaMemcpyHostToDevice,
+                                        rt_.stream));
+            TBLAEQ_CUDA(cudaMemsetAsync(rt_.pluginMask.get(), 0, p, rt_.stream));
+            launchKnnLowerBound(cur.ids, cur.vals, p, static_cast<int>(D), rt_.scratchQuery.as<double>(),
+                                rt_.dev->nodeOrig[l].as<NodeRec>(), rt_.knnKeys.as<uint64_t>(),
+                                rt_.knnLabels.as<uint32_t>(), rt_.knnCnt.as<uint32_t>(), rt_.knnRr.as<double>(),
+                                rt_.stream);
+            sortPairs(rt_.knnKeys.as<uint64_t>(), rt_.knnLabels.as<uint32_t>(), rt_.knnKeys2.as<uint64_t>(),
+                      rt_.knnLabels2.as<uint32_t>(), p, rt_.stream);
+            launchStep(rt_.knnKeys.as<uint64_t>(), rt_.knnLabels.as<uint32_t>(), rt_.knnCnt.as<uint32_t>(),
+                       rt_.knnRr.as<double>(), p, K, rt_.pluginMask.as<uint8_t>(), rt_.stream);
+        }
+        n = rt_.pluginEngine->runGridLevel(static_cast<int>(l), cur.ids, cur.vals, p, false, nullptr,
+                                           rt_.pluginMask.as<uint8_t>(), out.ids.as<uint64_t>(),
+                                           out.vals.as<double>(), cap);
     }
     LevelResult r;
     r.grid.numRows = h.meshCount(l + 1);

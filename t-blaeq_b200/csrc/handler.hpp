@@ -143,7 +143,9 @@ struct Runtime {
     };
     std::vector<LevelBufs> levelOut;
     std::unique_ptr<BatchEngine> pluginEngine;  // workspace for the plugin's two expands
-    DeviceMem pluginMask;
+    // Per-level KNN plugin scratch: bound keys, labels (+ sort scratch), child counts, STEP bounds, mask.
+    DeviceMem knnKeys, knnKeys2, knnLabels, knnLabels2, knnCnt, knnRr, pluginMask;
+    uint64_t knnCap = 0;
     DeviceMem scratchQuery;  // lo|hi or point staged on the device
     ~Runtime();
 };

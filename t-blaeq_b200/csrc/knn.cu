@@ -1,0 +1,367 @@
+// KNN building blocks (see knn.cuh).
+#include "knn.cuh"
+
+#include <algorithm>
+#include <cfloat>
+
+namespace tblaeq {
+
+namespace {
+
+constexpr int kSortTile = 2048;  // pairs per bitonic tile (1024 threads x 2)
+constexpr int kMergeItems = 8;   // outputs per thread in a merge pass
+
+__device__ __forceinline__ bool pairLess(uint64_t ka, uint32_t va, uint64_t kb, uint32_t vb) {
+    return ka < kb || (ka == kb && va < vb);
+}
+
+__global__ void knnLowerBoundKernel(const uint64_t* ids, const double* vals, uint64_t p, int D, const double* q,
+                                    const NodeRec* nodes, uint64_t* keys, uint32_t* labels, uint32_t* cnt,
+                                    double* rr) {
+    for (uint64_t i = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x; i < p;
+         i += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
+        double dist = 0.0;
+        for (int d = 0; d < D; ++d) {
+            const double diff = q[d] - vals[i * D + d];
+            dist = __fma_rn(diff, diff, dist);  // the reference kernel's contracted accumulation
+        }
+        const NodeRec nr = nodes[ids[i]];
+        const double lb = __dsqrt_rd(dist) - nr.rad;
+        keys[i] = orderKey(lb);
+        labels[i] = static_cast<uint32_t>(i);
+        cnt[i] = nr.cnt;
+        rr[i] = lb + 2.0 * nr.rad;
+    }
+}
+
+// Sorts one 2048-pair tile in shared memory (bitonic network), padding with +inf keys.
+__global__ void __launch_bounds__(1024) bitonicTileKernel(uint64_t* keys, uint32_t* labels, uint64_t n) {
+    __shared__ uint64_t sk[kSortTile];
+    __shared__ uint32_t sv[kSortTile];
+    const uint64_t base = static_cast<uint64_t>(blockIdx.x) * kSortTile;
+    for (int i = threadIdx.x; i < kSortTile; i += blockDim.x) {
+        const uint64_t g = base + i;
+        sk[i] = g < n ? keys[g] : ~0ull;
+        sv[i] = g < n ? labels[g] : 0xffffffffu;
+    }
+    __syncthreads();
+    for (int size = 2; size <= kSortTile; size <<= 1) {
+        for (int stride = size >> 1; stride > 0; stride >>= 1) {
+            for (int t = threadIdx.x; t < kSortTile / 2; t += blockDim.x) {
+                const int lo = 2 * t - (t & (stride - 1));
+                const int hi = lo + stride;
+                const bool asc = ((lo & size) == 0);
+                const bool swap = asc ? pairLess(sk[hi], sv[hi], sk[lo], sv[lo]) : pairLess(sk[lo], sv[lo], sk[hi], sv[hi]);
+                if (swap) {
+                    const uint64_t k = sk[lo];
+                    sk[lo] = sk[hi];
+                    sk[hi] = k;
+                    const uint32_t v = sv[lo];
+                    sv[lo] = sv[hi];
+                    sv[hi] = v;
+                }
+            }
+            __syncthreads();
+        }
+    }
+    for (int i = threadIdx.x; i < kSortTile; i += blockDim.x) {
+        const uint64_t g = base + i;
+        if (g < n) {
+            keys[g] = sk[i];
+            labels[g] = sv[i];
+        }
+    }
+}
+
+// One merge pass: sorted runs of `width` pairs are merged pairwise into runs of 2 * width. Each
+// thread finds its start on the merge path by a binary search and merges kMergeItems outputs.
+__global__ void mergePassKernel(const uint64_t* ki, const uint32_t* vi, uint64_t* ko, uint32_t* vo, uint64_t n,
+                                uint64_t width) {
+    const uint64_t nOut = (n + kMergeItems - 1) / kMergeItems;
+    for (uint64_t t = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x; t < nOut;
+         t += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
+        const uint64_t o0 = t * kMergeItems;
+        const uint64_t pairStart = (o0 / (2 * width)) * (2 * width);
+        const uint64_t aBeg = pairStart, aEnd = std::min(pairStart + width, n);
+        const uint64_t bBeg = aEnd, bEnd = std::min(pairStart + 2 * width, n);
+        const uint64_t aLen = aEnd - aBeg, bLen = bEnd - bBeg;
+        const uint64_t diag = o0 - pairStart;  // outputs of this pair before o0
+        // Largest i in [max(0, diag - bLen), min(diag, aLen)] with A[i-1] <= B[diag-i] (stable: A first).
+        uint64_t lo = diag > bLen ? diag - bLen : 0, hi = std::min(diag, aLen);
+        while (lo < hi) {
+            const uint64_t i = (lo + hi + 1) >> 1;  // candidate count taken from A
+            const uint64_t j = diag - i;
+            // Taking i from A is valid iff A[i-1] <= B[j] (ties go to A).
+            if (!pairLess(ki[bBeg + j], vi[bBeg + j], ki[aBeg + i - 1], vi[aBeg + i - 1])) lo = i; else hi = i - 1;
+        }
+        uint64_t ia = aBeg + lo, ib = bBeg + (diag - lo);
+        for (int r = 0; r < kMergeItems && o0 + r < n && o0 + r < pairStart + aLen + bLen; ++r) {
+            bool takeA;
+            if (ia >= aEnd) takeA = false;
+            else if (ib >= bEnd) takeA = true;
+            else takeA = !pairLess(ki[ib], vi[ib], ki[ia], vi[ia]);
+            if (takeA) {
+                ko[o0 + r] = ki[ia];
+                vo[o0 + r] = vi[ia];
+                ++ia;
+            } else {
+                ko[o0 + r] = ki[ib];
+                vo[o0 + r] = vi[ib];
+                ++ib;
+            }
+        }
+    }
+}
+
+// STEP in one CTA: n1 = entries whose preceding child count is below K (the part that feeds the
+// running bound), cur = max(0, max rr over them), then every later entry with lb <= cur.
+__global__ void __launch_bounds__(1024) stepKernel(const uint64_t* keys, const uint32_t* labels, const uint32_t* cnt,
+                                                   const double* rr, uint64_t n, uint64_t K, uint8_t* mask) {
+    __shared__ unsigned long long sCarry;
+    __shared__ unsigned long long sFirst;
+    __shared__ unsigned long long sWarp[32];
+    __shared__ double sMax[32];
+    __shared__ unsigned long long sEnd;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nw = blockDim.x / 32;
+    if (tid == 0) {
+        sCarry = 0;
+        sFirst = ~0ull;
+    }
+    __syncthreads();
+    // First index whose inclusive child-count prefix reaches K.
+    if (K > 0) {
+        for (uint64_t base = 0; base < n; base += blockDim.x) {
+            const uint64_t i = base + tid;
+            const unsigned long long c = i < n ? cnt[labels[i]] : 0;
+            unsigned long long inc = c;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const unsigned long long t = __shfl_up_sync(0xffffffffu, inc, o);
+                if (lane >= o) inc += t;
+            }
+            if (lane == 31) sWarp[warp] = inc;
+            __syncthreads();
+            if (warp == 0) {
+                unsigned long long w = lane < nw ? sWarp[lane] : 0, wi = w;
+#pragma unroll
+                for (int o = 1; o < 32; o <<= 1) {
+                    const unsigned long long t = __shfl_up_sync(0xffffffffu, wi, o);
+                    if (lane >= o) wi += t;
+                }
+                if (lane < nw) sWarp[lane] = wi - w;
+            }
+            __syncthreads();
+            const unsigned long long carry = sCarry;
+            const unsigned long long total = carry + sWarp[warp] + inc;
+            if (i < n && total >= K) atomicMin(&sFirst, static_cast<unsigned long long>(i));
+            __syncthreads();
+            if (tid == blockDim.x - 1) sCarry = carry + sWarp[warp] + inc;
+            __syncthreads();
+            if (sFirst != ~0ull) break;
+        }
+    }
+    __syncthreads();
+    const uint64_t n1 = (K == 0) ? 0 : (sFirst == ~0ull ? n : sFirst + 1);
+    // cur = max(0, max rr over the first n1 entries).
+    double m = 0.0;
+    for (uint64_t i = tid; i < n1; i += blockDim.x) m = fmax(m, rr[labels[i]]);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+    if (lane == 0) sMax[warp] = m;
+    __syncthreads();
+    if (tid == 0) {
+        double cur = 0.0;
+        for (int w = 0; w < nw; ++w) cur = fmax(cur, sMax[w]);
+        // Entries after n1 are taken while lb <= cur; keys are sorted, so find the first key above.
+        const uint64_t kc = orderKey(cur);
+        uint64_t lo = n1, hi = n;
+        while (lo < hi) {
+            const uint64_t mid = (lo + hi) >> 1;
+            if (keys[mid] > kc) hi = mid; else lo = mid + 1;
+        }
+        sEnd = (n1 >= n) ? n : lo;
+    }
+    __syncthreads();
+    const uint64_t end = sEnd;
+    for (uint64_t i = tid; i < end; i += blockDim.x) mask[labels[i]] = 1;
+}
+
+constexpr int kTopKStage = 4096;  // candidates a CTA sorts in shared memory
+
+__global__ void __launch_bounds__(512) topKKernel(const uint64_t* offA, const uint64_t* idsA, const double* d2A,
+                                                  const uint64_t* offB, const uint64_t* idsB, const double* d2B,
+                                                  const uint32_t* Kq, const uint64_t* outOff, uint64_t* outIds,
+                                                  double* outD2, uint32_t* outCount, uint32_t* status) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    uint64_t* sk = reinterpret_cast<uint64_t*>(smem);
+    uint64_t* sv = sk + kTopKStage;
+    const uint32_t q = blockIdx.x;
+    const uint64_t a0 = offA[q], na = offA[q + 1] - a0;
+    const uint64_t b0 = offB ? offB[q] : 0, nb = offB ? offB[q + 1] - b0 : 0;
+    const uint64_t n = na + nb;
+    const uint32_t K = Kq[q];
+    const uint64_t keep = std::min<uint64_t>(K, n);
+    auto keyAt = [&](uint64_t i) -> uint64_t { return i < na ? orderKey(d2A[a0 + i]) : orderKey(d2B[b0 + i - na]); };
+    auto idAt = [&](uint64_t i) -> uint64_t { return i < na ? idsA[a0 + i] : idsB[b0 + i - na]; };
+    if (threadIdx.x == 0) outCount[q] = static_cast<uint32_t>(keep);
+    if (keep == 0) return;
+    const uint64_t o = outOff[q];
+    if (n <= kTopKStage) {
+        int size = 1;
+        while (size < static_cast<int>(n)) size <<= 1;
+        for (int i = threadIdx.x; i < size; i += blockDim.x) {
+            sk[i] = i < static_cast<int>(n) ? keyAt(i) : ~0ull;
+            sv[i] = i < static_cast<int>(n) ? idAt(i) : ~0ull;
+        }
+        __syncthreads();
+        for (int s = 2; s <= size; s <<= 1) {
+            for (int stride = s >> 1; stride > 0; stride >>= 1) {
+                for (int t = threadIdx.x; t < size / 2; t += blockDim.x) {
+                    const int lo = 2 * t - (t & (stride - 1));
+                    const int hi = lo + stride;
+                    const bool asc = ((lo & s) == 0);
+                    const bool gt = sk[lo] > sk[hi] || (sk[lo] == sk[hi] && sv[lo] > sv[hi]);
+                    if (asc == gt) {
+                        const uint64_t k = sk[lo];
+                        sk[lo] = sk[hi];
+                        sk[hi] = k;
+                        const uint64_t v = sv[lo];
+                        sv[lo] = sv[hi];
+                        sv[hi] = v;
+                    }
+                }
+                __syncthreads();
+            }
+        }
+        for (uint64_t i = threadIdx.x; i < keep; i += blockDim.x) {
+            outIds[o + i] = sv[i];
+            uint64_t b = sk[i];
+            b = (b & 0x8000000000000000ull) ? (b & 0x7fffffffffffffffull) : ~b;
+            double d;
+            memcpy(&d, &b, 8);
+            outD2[o + i] = d;
+        }
+        return;
+    }
+    // More candidates than the stage holds: K rounds of a block-wide minimum above the last pick.
+    __shared__ unsigned long long sBestK, sBestV;
+    uint64_t lastK = 0, lastV = 0;
+    bool haveLast = false;
+    for (uint64_t r = 0; r < keep; ++r) {
+        if (threadIdx.x == 0) {
+            sBestK = ~0ull;
+            sBestV = ~0ull;
+        }
+        __syncthreads();
+        uint64_t bk = ~0ull, bv = ~0ull;
+        for (uint64_t i = threadIdx.x; i < n; i += blockDim.x) {
+            const uint64_t k = keyAt(i), v = idAt(i);
+            const bool above = !haveLast || k > lastK || (k == lastK && v > lastV);
+            if (above && (k < bk || (k == bk && v < bv))) {
+                bk = k;
+                bv = v;
+            }
+        }
+        // (key, id) minimum: first the key, then the id among equal keys.
+        atomicMin(&sBestK, static_cast<unsigned long long>(bk));
+        __syncthreads();
+        if (bk == sBestK) atomicMin(&sBestV, static_cast<unsigned long long>(bv));
+        __syncthreads();
+        lastK = sBestK;
+        lastV = sBestV;
+        haveLast = true;
+        if (threadIdx.x == 0) {
+            outIds[o + r] = lastV;
+            uint64_t b = lastK;
+            b = (b & 0x8000000000000000ull) ? (b & 0x7fffffffffffffffull) : ~b;
+            double d;
+            memcpy(&d, &b, 8);
+            outD2[o + r] = d;
+        }
+        __syncthreads();
+    }
+    (void)status;
+}
+
+__global__ void fillDoubleKernel(double* v, double value, uint32_t n) {
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) v[i] = value;
+}
+
+__global__ void clampCountsKernel(const uint64_t* off, const uint32_t* K, uint32_t nq, uint32_t* out) {
+    for (uint32_t q = blockIdx.x * blockDim.x + threadIdx.x; q < nq; q += gridDim.x * blockDim.x) {
+        const uint64_t n = off[q + 1] - off[q];
+        out[q] = static_cast<uint32_t>(n < K[q] ? n : K[q]);
+    }
+}
+
+int gridFor(uint64_t n, int threads) {
+    const uint64_t b = (n + threads - 1) / threads;
+    return static_cast<int>(std::max<uint64_t>(1, std::min<uint64_t>(b, 148ull * 16)));
+}
+
+}  // namespace
+
+void launchFillDouble(double* v, double value, uint32_t n, cudaStream_t s) {
+    if (n == 0) return;
+    fillDoubleKernel<<<gridFor(n, 256), 256, 0, s>>>(v, value, n);
+    TBLAEQ_CUDA(cudaGetLastError());
+}
+
+void launchClampCounts(const uint64_t* off, const uint32_t* K, uint32_t nq, uint32_t* out, cudaStream_t s) {
+    if (nq == 0) return;
+    clampCountsKernel<<<gridFor(nq, 256), 256, 0, s>>>(off, K, nq, out);
+    TBLAEQ_CUDA(cudaGetLastError());
+}
+
+void launchKnnLowerBound(const uint64_t* ids, const double* vals, uint64_t p, int D, const double* dPoint,
+                         const NodeRec* nodes, uint64_t* keys, uint32_t* labels, uint32_t* cnt, double* rr,
+                         cudaStream_t s) {
+    if (p == 0) return;
+    knnLowerBoundKernel<<<gridFor(p, 256), 256, 0, s>>>(ids, vals, p, D, dPoint, nodes, keys, labels, cnt, rr);
+    TBLAEQ_CUDA(cudaGetLastError());
+}
+
+void sortPairs(uint64_t* keys, uint32_t* labels, uint64_t* keys2, uint32_t* labels2, uint64_t n, cudaStream_t s) {
+    if (n <= 1) return;
+    const uint64_t tiles = (n + kSortTile - 1) / kSortTile;
+    bitonicTileKernel<<<static_cast<unsigned>(tiles), 1024, 0, s>>>(keys, labels, n);
+    TBLAEQ_CUDA(cudaGetLastError());
+    uint64_t* ka = keys;
+    uint32_t* va = labels;
+    uint64_t* kb = keys2;
+    uint32_t* vb = labels2;
+    for (uint64_t w = kSortTile; w < n; w *= 2) {
+        mergePassKernel<<<gridFor((n + kMergeItems - 1) / kMergeItems, 256), 256, 0, s>>>(ka, va, kb, vb, n, w);
+        TBLAEQ_CUDA(cudaGetLastError());
+        std::swap(ka, kb);
+        std::swap(va, vb);
+    }
+    if (ka != keys) {
+        TBLAEQ_CUDA(cudaMemcpyAsync(keys, ka, n * 8, cudaMemcpyDeviceToDevice, s));
+        TBLAEQ_CUDA(cudaMemcpyAsync(labels, va, n * 4, cudaMemcpyDeviceToDevice, s));
+    }
+}
+
+void launchStep(const uint64_t* keys, const uint32_t* labels, const uint32_t* cnt, const double* rr, uint64_t n,
+                uint64_t K, uint8_t* mask, cudaStream_t s) {
+    if (n == 0) return;
+    stepKernel<<<1, 1024, 0, s>>>(keys, labels, cnt, rr, n, K, mask);
+    TBLAEQ_CUDA(cudaGetLastError());
+}
+
+void launchTopK(const uint64_t* offA, const uint64_t* idsA, const double* d2A, const uint64_t* offB,
+                const uint64_t* idsB, const double* d2B, const uint32_t* K, uint32_t nq, const uint64_t* outOff,
+                uint64_t* outIds, double* outD2, uint32_t* outCount, uint32_t* status, cudaStream_t s) {
+    if (nq == 0) return;
+    const size_t smem = static_cast<size_t>(kTopKStage) * 16;
+    static bool attr = false;
+    if (!attr) {
+        TBLAEQ_CUDA(cudaFuncSetAttribute(topKKernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         static_cast<int>(smem)));
+        attr = true;
+    }
+    topKKernel<<<nq, 512, smem, s>>>(offA, idsA, d2A, offB, idsB, d2B, K, outOff, outIds, outD2, outCount, status);
+    TBLAEQ_CUDA(cudaGetLastError());
+}
+
+}  // namespace tblaeq

@@ -1,0 +1,54 @@
+// KNN building blocks on the device:
+//   * the reference's per-centroid lower bound (src/Query/KNN.cu:9-24) for the per-level plugin;
+//   * a sort of (key, label) pairs: bitonic 2048-element tiles in shared memory, then merge-path
+//     passes (the reference sorts 512-element tiles on the device and merges them on the host,
+//     src/MergeSort/MergeSort.cuh:240-313,628-696);
+//   * STEP selection (src/core/strategies/L0Strategy.cu:133-154) as a scan, a max-reduction and a
+//     search over the sorted bounds instead of a sequential host loop;
+//   * per-query top-K selection of candidate points for exact KNN.
+#pragma once
+
+#include <cstdint>
+
+#include "common.cuh"
+#include "traverse.cuh"
+
+namespace tblaeq {
+
+// Orderable 64-bit key of a double (total order equal to the numeric order for non-NaN values).
+__host__ __device__ inline uint64_t orderKey(double v) {
+    uint64_t b;
+    memcpy(&b, &v, 8);
+    return (b & 0x8000000000000000ull) ? ~b : (b | 0x8000000000000000ull);
+}
+
+// keys[i] = orderKey(sqrt_rd(|q - vals[i]|^2) - rad(ids[i])), labels[i] = i, cnt[i] / rr[i] = the
+// node's child count and lb + 2 * radius (the STEP inputs), for the p entries of a grid.
+void launchKnnLowerBound(const uint64_t* ids, const double* vals, uint64_t p, int D, const double* dPoint,
+                         const NodeRec* nodes, uint64_t* keys, uint32_t* labels, uint32_t* cnt, double* rr,
+                         cudaStream_t s);
+
+// Sorts n (key, label) pairs ascending by (key, label). Uses (keys2, labels2) as scratch of the
+// same size; the result ends in (keys, labels).
+void sortPairs(uint64_t* keys, uint32_t* labels, uint64_t* keys2, uint32_t* labels2, uint64_t n, cudaStream_t s);
+
+// STEP over sorted pairs: mask[label] = 1 for every selected entry (mask zeroed by the caller).
+void launchStep(const uint64_t* keys, const uint32_t* labels, const uint32_t* cnt, const double* rr, uint64_t n,
+                uint64_t K, uint8_t* mask, cudaStream_t s);
+
+// Per-query exact top-K: candidates of query q are the concatenation of
+// [offA[q], offA[q+1]) in (idsA, d2A) and [offB[q], offB[q+1]) in (idsB, d2B) (B may be null).
+// Writes the K[q] (or fewer) smallest by (dist2, id), ascending, to outIds/outD2 starting at
+// outOff[q]; outCount[q] receives how many. Status bit kStatusOverflowEntries when a query has
+// more candidates than the selection can stage.
+void launchTopK(const uint64_t* offA, const uint64_t* idsA, const double* d2A, const uint64_t* offB,
+                const uint64_t* idsB, const double* d2B, const uint32_t* K, uint32_t nq, const uint64_t* outOff,
+                uint64_t* outIds, double* outD2, uint32_t* outCount, uint32_t* status, cudaStream_t s);
+
+// v[i] = value for i < n.
+void launchFillDouble(double* v, double value, uint32_t n, cudaStream_t s);
+
+// out[q] = min(K[q], off[q+1] - off[q]).
+void launchClampCounts(const uint64_t* off, const uint32_t* K, uint32_t nq, uint32_t* out, cudaStream_t s);
+
+}  // namespace tblaeq

@@ -223,7 +223,6 @@ struct QueryCache {
 #pragma unroll
             for (int d = 0; d < DM; ++d)
                 if (d < dim) lo[d] = __ldg(p + d);
-            tau = __ldg(a.query.tau + nq);
         }
     }
 };
@@ -294,11 +293,38 @@ __device__ __forceinline__ bool testItem(const ExpandArgs& a, int dim, const dou
         }
         return in;
     } else if constexpr (PRED == kPredKnnBound) {
+        // Distance bounds of the points below the child: sphere (centre distance -/+ subtree radius)
+        // and, when present, its box (outward-rounded, so slightly widened bounds stay conservative).
         const double dd = sqrt(pointDist2<DM>(y, qc.lo, dim, 1));
+        double lb = dd - nr.rad, ub = dd + nr.rad;
+        if (a.child.aabb) {
+            const float* b = a.child.aabb + static_cast<size_t>(kk) * 2 * dim;
+            double gapSum = 0.0, farSum = 0.0;
+#pragma unroll
+            for (int d = 0; d < DM; ++d) {
+                if (d < dim) {
+                    const double l = static_cast<double>(__ldg(b + d)), h = static_cast<double>(__ldg(b + dim + d));
+                    const double g = fmax(fmax(l - qc.lo[d], qc.lo[d] - h), 0.0);
+                    const double f = fmax(qc.lo[d] - l, h - qc.lo[d]);
+                    gapSum = __fma_rn(g, g, gapSum);
+                    farSum = __fma_rn(f, f, farSum);
+                }
+            }
+            lb = fmax(lb, sqrt(gapSum) * (1.0 - 1e-12));
+            ub = fmin(ub, sqrt(farSum) * (1.0 + 1e-12));
+        }
         cc = nr.cnt;
-        return (cc > 0) && (dd - nr.rad <= qc.tau);
+        const uint32_t q = qc.q;
+        double tau = __ldcg(a.query.tau + q);
+        // Any child with K points below it bounds the K-th neighbour distance by its far distance.
+        if (ub < tau && __ldg(a.child.leaf + kk) >= __ldg(a.query.k + q)) {
+            atomicMin(reinterpret_cast<unsigned long long*>(a.query.tau + q), __double_as_longlong(ub));
+            tau = ub;
+        }
+        return (cc > 0) && (lb <= tau);
     } else {  // kPredKnnPoint
-        return pointDist2<DM>(y, qc.lo, dim, 1) <= qc.tau * qc.tau;
+        const double t = __ldcg(a.query.tau + qc.q);
+        return pointDist2<DM>(y, qc.lo, dim, 1) <= t * t * (1.0 + 1e-9);
     }
 }
 

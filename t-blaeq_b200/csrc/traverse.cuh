@@ -82,6 +82,7 @@ struct ChildLevel {
     const uint64_t* keys;       // optional key of row j into the node records (null: key = j)
     const NodeRec* nodes;       // child node records (by key)
     const float* aabb;          // optional box of the points below each child (by key): lo[D] hi[D]
+    const uint32_t* leaf;       // finest points below each child (by key), for the KNN bound
     const uint8_t* mask;        // keep flags (by row) for kPredMask
     const uint64_t* outMap;     // final output id of row j (null: id = key)
 };
@@ -89,7 +90,9 @@ struct ChildLevel {
 struct QueryArgs {
     const double* boxes;        // range: per query lo[D] then hi[D]
     const double* points;       // knn: per query point[D]
-    const double* tau;          // knn: per query distance bound (upper bound on the K-th NN distance)
+    double* tau;                // knn: per query upper bound on the K-th neighbour distance (tightened
+                                //      in place with an atomic minimum)
+    const uint32_t* k;          // knn: neighbours wanted per query
 };
 
 struct Scratch {

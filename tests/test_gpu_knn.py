@@ -1,0 +1,106 @@
+"""GPU parity of the KNN path through the C ABI.
+
+* the per-level plugin (IQueryStrategy::runLevel, KNN): device lower bounds (sqrt rounded down, like
+  __dsqrt_rd in the reference), device sort and STEP; every level's grid equals the reference
+  traversal's (oracle, pinned to the reference CUDA build), in the reference's order;
+* batched exact KNN: the K nearest points by FP64 squared distance with id tie-break, identical
+  ids and bit-identical squared distances to the FP64 brute force, for uniform and per-query K.
+"""
+import numpy as np
+import pytest
+
+from conftest import oracle_from_handler
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def env(tb, oracle_mod, tmp_path_factory, cuda):
+    h = tb.QueryHandler.generate(200000, 5, 1.0, 100.0, False, 4, (40, 20, 10), 31, 2.2)
+    h.prepare_for_query(tb.LevelPolicy.L0)
+    o = oracle_from_handler(oracle_mod, h, tmp_path_factory.mktemp("idx"))
+    pts, ids = oracle_mod.decoded_points(o)
+    return h, o, pts, ids
+
+
+def _points(pts, n, seed, noise=0.5):
+    rng = np.random.default_rng(seed)
+    return np.ascontiguousarray(pts[rng.integers(0, len(pts), n)] + rng.normal(0, noise, (n, pts.shape[1])))
+
+
+def test_plugin_knn_levels_match_reference(tb, env, oracle_mod):
+    h, o, pts, ids = env
+    P = _points(pts, 10, 1)
+    for K in (1, 10, 50):
+        ref = oracle_mod.ref_query(o, oracle_mod.KNN, P, K=K, sorted_ids=False)
+        for q in range(len(P)):
+            grid = h.coarsest_grid()
+            sizes = []
+            for l in range(3):
+                grid = h.run_level(l, grid, tb.QueryType.POINT, point=P[q], K=K)
+                sizes.append(grid.nnz)
+            got, _ = h.grid_arrays(grid)
+            assert sizes == list(ref.level_sizes[q]), (K, q)
+            assert np.array_equal(got, ref.query(q)), (K, q)
+
+
+def test_plugin_knn_large_grid_sort(tb, oracle_mod, tmp_path, cuda):
+    """A level whose grid exceeds one sort tile exercises the merge passes of the device sort."""
+    h = tb.QueryHandler.generate(300000, 3, 1.0, 100.0, False, 3, (10, 5), 9, 3.0)
+    h.prepare_for_query(tb.LevelPolicy.L0)
+    o = oracle_from_handler(oracle_mod, h, tmp_path)
+    pts, _ = oracle_mod.decoded_points(o)
+    P = _points(pts, 3, 2)
+    ref = oracle_mod.ref_query(o, oracle_mod.KNN, P, K=20, sorted_ids=False)
+    for q in range(3):
+        grid = h.coarsest_grid()
+        assert grid.nnz > 2048 * 4
+        for l in range(2):
+            grid = h.run_level(l, grid, tb.QueryType.POINT, point=P[q], K=20)
+        got, _ = h.grid_arrays(grid)
+        assert np.array_equal(got, ref.query(q))
+
+
+@pytest.mark.parametrize("K", [1, 10, 100])
+def test_batched_exact_knn_equals_brute_force(tb, env, oracle_mod, K):
+    h, o, pts, ids = env
+    P = _points(pts, 200, 3 + K)
+    r = h.query_batch(tb.QueryType.POINT, P, tb.Mode.EXACT, K=K)
+    offs, got, d2 = r.offsets.numpy(), r.ids.numpy(), r.dist2.numpy()
+    b = oracle_mod.brute_query(pts, ids, oracle_mod.KNN, P, K=K)
+    assert np.array_equal(offs, b.offsets)
+    assert np.array_equal(got, b.ids)
+    assert np.array_equal(d2, b.dist2)
+
+
+def test_batched_knn_per_query_k_and_edges(tb, env, oracle_mod):
+    h, o, pts, ids = env
+    P = _points(pts, 64, 7)
+    P[0] = pts.max(0) + 50.0   # far outside the data
+    P[1] = pts[123]            # exactly on a data point
+    Ks = np.array([1, 2, 5, 20, 100, 0, 256, 3] * 8, dtype=np.uint32)
+    r = h.query_batch(tb.QueryType.POINT, P, tb.Mode.EXACT, K=Ks)
+    offs, got, d2 = r.offsets.numpy(), r.ids.numpy(), r.dist2.numpy()
+    for q in range(len(P)):
+        b = oracle_mod.brute_query(pts, ids, oracle_mod.KNN, P[q:q + 1], K=int(Ks[q]))
+        assert np.array_equal(got[offs[q]:offs[q + 1]], b.ids), q
+        assert np.array_equal(d2[offs[q]:offs[q + 1]], b.dist2), q
+    assert offs[6] - offs[5] == 0          # K = 0
+    assert got[offs[1]] == ids[123] and d2[offs[1]] == 0.0
+
+
+def test_batched_knn_same_alone_and_in_batch(tb, env):
+    h, o, pts, ids = env
+    P = _points(pts, 32, 11)
+    r = h.query_batch(tb.QueryType.POINT, P, tb.Mode.EXACT, K=16)
+    offs, got = r.offsets.numpy(), r.ids.numpy()
+    for q in range(0, 32, 5):
+        o1, i1, d1 = h.query_batch_host(tb.QueryType.POINT, P[q:q + 1], tb.Mode.EXACT, K=16)
+        assert np.array_equal(i1, got[offs[q]:offs[q + 1]])
+
+
+def test_knn_ref_parity_batch_is_rejected(tb, env):
+    h, o, pts, ids = env
+    with pytest.raises(tb.TblaeqError) as e:
+        h.query_batch(tb.QueryType.POINT, pts[:2], tb.Mode.REF_PARITY, K=5)
+    assert e.value.code == 1
