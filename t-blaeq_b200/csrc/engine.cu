@@ -530,9 +530,9 @@ void BatchEngine::enqueueKnn(const double* dPoints, uint32_t nq, const uint32_t*
     launchExclusiveScan(qcount, candOff_.as<uint64_t>(), nq, stream_);
     launchClampCounts(candOff_.as<uint64_t>(), dK, nq, knnCount_.as<uint32_t>(), stream_);
     launchExclusiveScan(knnCount_.as<uint32_t>(), knnOff_.as<uint64_t>(), nq, stream_);
-    launchTopK(candOff_.as<uint64_t>(), resIds_.as<uint64_t>(), resDist_.as<double>(), nullptr, nullptr, nullptr, dK,
-               nq, knnOff_.as<uint64_t>(), knnIds_.as<uint64_t>(), knnD2_.as<double>(), knnCount_.as<uint32_t>(),
-               status, stream_);
+    launchTopK(candOff_.as<uint64_t>(), resIds_.as<uint64_t>(), resDist_.as<double>(), caps_.results, nullptr, nullptr,
+               nullptr, 0, dK, nq, knnOff_.as<uint64_t>(), knnIds_.as<uint64_t>(), knnD2_.as<double>(),
+               knnCount_.as<uint32_t>(), status, stream_);
     if (timing_) record(2 + H);
 }
 

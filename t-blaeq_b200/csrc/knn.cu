@@ -189,9 +189,10 @@ __global__ void __launch_bounds__(1024) stepKernel(const uint64_t* keys, const u
 constexpr int kTopKStage = 4096;  // candidates a CTA sorts in shared memory
 
 __global__ void __launch_bounds__(512) topKKernel(const uint64_t* offA, const uint64_t* idsA, const double* d2A,
-                                                  const uint64_t* offB, const uint64_t* idsB, const double* d2B,
-                                                  const uint32_t* Kq, const uint64_t* outOff, uint64_t* outIds,
-                                                  double* outD2, uint32_t* outCount, uint32_t* status) {
+                                                  uint64_t capA, const uint64_t* offB, const uint64_t* idsB,
+                                                  const double* d2B, uint64_t capB, const uint32_t* Kq,
+                                                  const uint64_t* outOff, uint64_t* outIds, double* outD2,
+                                                  uint32_t* outCount, uint32_t* status) {
     extern __shared__ __align__(16) unsigned char smem[];
     uint64_t* sk = reinterpret_cast<uint64_t*>(smem);
     uint64_t* sv = sk + kTopKStage;
@@ -200,6 +201,14 @@ __global__ void __launch_bounds__(512) topKKernel(const uint64_t* offA, const ui
     const uint64_t b0 = offB ? offB[q] : 0, nb = offB ? offB[q + 1] - b0 : 0;
     const uint64_t n = na + nb;
     const uint32_t K = Kq[q];
+    // Candidates beyond the arrays mean the producer overflowed: never read them.
+    if (a0 + na > capA || (offB && b0 + nb > capB)) {
+        if (threadIdx.x == 0) {
+            outCount[q] = 0;
+            atomicOr(status, kStatusOverflowEntries);
+        }
+        return;
+    }
     const uint64_t keep = std::min<uint64_t>(K, n);
     auto keyAt = [&](uint64_t i) -> uint64_t { return i < na ? orderKey(d2A[a0 + i]) : orderKey(d2B[b0 + i - na]); };
     auto idAt = [&](uint64_t i) -> uint64_t { return i < na ? idsA[a0 + i] : idsB[b0 + i - na]; };
@@ -280,7 +289,6 @@ __global__ void __launch_bounds__(512) topKKernel(const uint64_t* offA, const ui
         }
         __syncthreads();
     }
-    (void)status;
 }
 
 __global__ void fillDoubleKernel(double* v, double value, uint32_t n) {
@@ -349,9 +357,10 @@ void launchStep(const uint64_t* keys, const uint32_t* labels, const uint32_t* cn
     TBLAEQ_CUDA(cudaGetLastError());
 }
 
-void launchTopK(const uint64_t* offA, const uint64_t* idsA, const double* d2A, const uint64_t* offB,
-                const uint64_t* idsB, const double* d2B, const uint32_t* K, uint32_t nq, const uint64_t* outOff,
-                uint64_t* outIds, double* outD2, uint32_t* outCount, uint32_t* status, cudaStream_t s) {
+void launchTopK(const uint64_t* offA, const uint64_t* idsA, const double* d2A, uint64_t capA, const uint64_t* offB,
+                const uint64_t* idsB, const double* d2B, uint64_t capB, const uint32_t* K, uint32_t nq,
+                const uint64_t* outOff, uint64_t* outIds, double* outD2, uint32_t* outCount, uint32_t* status,
+                cudaStream_t s) {
     if (nq == 0) return;
     const size_t smem = static_cast<size_t>(kTopKStage) * 16;
     static bool attr = false;
@@ -360,7 +369,8 @@ void launchTopK(const uint64_t* offA, const uint64_t* idsA, const double* d2A, c
                                          static_cast<int>(smem)));
         attr = true;
     }
-    topKKernel<<<nq, 512, smem, s>>>(offA, idsA, d2A, offB, idsB, d2B, K, outOff, outIds, outD2, outCount, status);
+    topKKernel<<<nq, 512, smem, s>>>(offA, idsA, d2A, capA, offB, idsB, d2B, capB, K, outOff, outIds, outD2, outCount,
+                                     status);
     TBLAEQ_CUDA(cudaGetLastError());
 }
 

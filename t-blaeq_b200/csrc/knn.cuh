@@ -41,9 +41,12 @@ void launchStep(const uint64_t* keys, const uint32_t* labels, const uint32_t* cn
 // Writes the K[q] (or fewer) smallest by (dist2, id), ascending, to outIds/outD2 starting at
 // outOff[q]; outCount[q] receives how many. Status bit kStatusOverflowEntries when a query has
 // more candidates than the selection can stage.
-void launchTopK(const uint64_t* offA, const uint64_t* idsA, const double* d2A, const uint64_t* offB,
-                const uint64_t* idsB, const double* d2B, const uint32_t* K, uint32_t nq, const uint64_t* outOff,
-                uint64_t* outIds, double* outD2, uint32_t* outCount, uint32_t* status, cudaStream_t s);
+// capA / capB are the capacities of the candidate arrays: a query whose candidates lie beyond them
+// (the producer overflowed and the host will rerun the batch) is skipped and flagged.
+void launchTopK(const uint64_t* offA, const uint64_t* idsA, const double* d2A, uint64_t capA, const uint64_t* offB,
+                const uint64_t* idsB, const double* d2B, uint64_t capB, const uint32_t* K, uint32_t nq,
+                const uint64_t* outOff, uint64_t* outIds, double* outD2, uint32_t* outCount, uint32_t* status,
+                cudaStream_t s);
 
 // v[i] = value for i < n.
 void launchFillDouble(double* v, double value, uint32_t n, cudaStream_t s);

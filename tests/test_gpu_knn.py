@@ -46,7 +46,7 @@ def test_plugin_knn_levels_match_reference(tb, env, oracle_mod):
 
 def test_plugin_knn_large_grid_sort(tb, oracle_mod, tmp_path, cuda):
     """A level whose grid exceeds one sort tile exercises the merge passes of the device sort."""
-    h = tb.QueryHandler.generate(300000, 3, 1.0, 100.0, False, 3, (10, 5), 9, 3.0)
+    h = tb.QueryHandler.generate(300000, 3, 1.0, 100.0, False, 3, (5, 3), 9, 3.0)
     h.prepare_for_query(tb.LevelPolicy.L0)
     o = oracle_from_handler(oracle_mod, h, tmp_path)
     pts, _ = oracle_mod.decoded_points(o)
