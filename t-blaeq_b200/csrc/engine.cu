@@ -203,6 +203,10 @@ void BatchEngine::reserve(const EngineCaps& want, uint32_t nq, unsigned flags) {
         off = align256(off + static_cast<size_t>(qcap_) * 4);
         offLevels_ = off;
         off = align256(off + static_cast<size_t>(di_.intervals) * qcap_ * 4);
+        offQcountF_ = off;
+        off = align256(off + static_cast<size_t>(qcap_) * 4);
+        offQcountB_ = off;
+        off = align256(off + static_cast<size_t>(qcap_) * 4);
         zeroBytes_ = off;
         zeroBlock_.alloc(zeroBytes_);
         offsets_.alloc((static_cast<size_t>(qcap_) + 1) * 8);
@@ -471,6 +475,35 @@ uint64_t BatchEngine::runGridLevel(int l, const uint64_t* dIds, const double* dV
 
 namespace tblaeq {
 
+void BatchEngine::reserveKnn(uint32_t nq) {
+    if (knnQcap_ < std::max<uint32_t>(nq, 1)) {
+        knnQcap_ = std::max<uint32_t>(nq, 1);
+        tau_.alloc(knnQcap_ * 8ull);
+        knnCount_.alloc(knnQcap_ * 4ull);
+        candOff_.alloc((knnQcap_ + 1ull) * 8);
+        knnOff_.alloc((knnQcap_ + 1ull) * 8);
+        offF_.alloc((knnQcap_ + 1ull) * 8);
+        waveM_.alloc(knnQcap_ * 4ull);
+        selCount_.alloc(knnQcap_ * 4ull);
+        selOff_.alloc((knnQcap_ + 1ull) * 8);
+        selIds_.alloc(knnQcap_ * 32ull * 8);
+        selD2_.alloc(knnQcap_ * 32ull * 8);
+        candOffB_.alloc((knnQcap_ + 1ull) * 8);
+    }
+    if (entryCap_ < caps_.entries) {
+        entryCap_ = caps_.entries;
+        lbE_.alloc(entryCap_ * 8);
+        scoreE_.alloc(entryCap_ * 8);
+        sel_.alloc(entryCap_);
+    }
+    if (resCapB_ < caps_.results) {
+        resCapB_ = caps_.results;
+        resIdsB_.alloc(resCapB_ * 8);
+        resQB_.alloc(resCapB_ * 4);
+        resDistB_.alloc(resCapB_ * 8);
+    }
+}
+
 void BatchEngine::enqueueKnn(const double* dPoints, uint32_t nq, const uint32_t* dK, unsigned flags) {
     lastKnn_ = true;
     const int H = static_cast<int>(di_.height);
@@ -480,6 +513,8 @@ void BatchEngine::enqueueKnn(const double* dPoints, uint32_t nq, const uint32_t*
     auto* tickets = reinterpret_cast<uint32_t*>(z + offTickets_);
     auto* status = reinterpret_cast<uint32_t*>(z + offStatus_);
     auto* qcount = reinterpret_cast<uint32_t*>(z + offQcount_);
+    auto* qcountF = reinterpret_cast<uint32_t*>(z + offQcountF_);
+    auto* qcountB = reinterpret_cast<uint32_t*>(z + offQcountB_);
     auto* levels = reinterpret_cast<uint32_t*>(z + offLevels_);
     const bool wantLevels = (flags & kWantLevels) != 0;
     double* tau = tau_.as<double>();
@@ -492,8 +527,7 @@ void BatchEngine::enqueueKnn(const double* dPoints, uint32_t nq, const uint32_t*
                        r0.tileStart.as<uint32_t>(), hdrPtr(0), nq, static_cast<uint32_t>(di_.meshCount[0]), D, tile_,
                        stream_);
     if (timing_) record(1);
-    int buf = 0;
-    for (int m = 0; m < H; ++m) {
+    auto base = [&](int m, int buf) {
         ExpandArgs a{};
         a.in = inView(buf, hdrPtr(m));
         a.child.rows = (m == 0) ? di_.coarseVals.as<double>() : di_.pvals[m - 1].as<double>();
@@ -507,44 +541,98 @@ void BatchEngine::enqueueKnn(const double* dPoints, uint32_t nq, const uint32_t*
         a.D = D;
         a.useFma = 1;
         a.variant = kVariantDirect;
-        if (m < H - 1) {
-            a.child.nodes = di_.nodeSub[m].as<NodeRec>();
-            a.child.aabb = di_.aabb[m].as<float>();
-            a.child.leaf = di_.leaf[m].as<uint32_t>();
-            a.fout = outView(1 - buf, hdrPtr(m + 1));
-            launchExpand(a, kPredKnnBound, false, 0, stream_);
-            buf = 1 - buf;
-        } else {
-            a.child.outMap = di_.maps[H - 1].as<uint64_t>();
-            a.rout.ids = resIds_.as<uint64_t>();
-            a.rout.q = resQ_.as<uint32_t>();
-            a.rout.dist2 = resDist_.as<double>();
-            a.rout.qcount = qcount;
-            a.rout.hdr = hdrPtr(H);
-            a.rout.cap = static_cast<uint32_t>(caps_.results);
-            launchExpand(a, kPredKnnPoint, true, 0, stream_);
-        }
+        return a;
+    };
+    int buf = 0;
+    for (int m = 0; m < H - 1; ++m) {
+        ExpandArgs a = base(m, buf);
+        a.child.nodes = di_.nodeSub[m].as<NodeRec>();
+        a.child.aabb = di_.aabb[m].as<float>();
+        a.child.leaf = di_.leaf[m].as<uint32_t>();
+        a.fout = outView(1 - buf, hdrPtr(m + 1));
+        a.fout.qcount = (m == H - 2) ? qcountF : nullptr;
+        launchExpand(a, kPredKnnBound, false, 0, stream_);
+        buf = 1 - buf;
         if (timing_) record(2 + m);
     }
-    // Candidates are query-major, so per-query offsets follow from the per-query counts.
+    // `buf` now holds the last frontier F: the surviving finest clusters, query-major.
+    ExpandArgs fin = base(H - 1, buf);
+    fin.child.outMap = di_.maps[H - 1].as<uint64_t>();
+    fin.rout.ids = resIds_.as<uint64_t>();
+    fin.rout.q = resQ_.as<uint32_t>();
+    fin.rout.dist2 = resDist_.as<double>();
+    fin.rout.qcount = qcount;
+    fin.rout.hdr = hdrPtr(H);
+    fin.rout.cap = static_cast<uint32_t>(caps_.results);
+    if (!twoWave_) {
+        launchExpand(fin, kPredKnnPoint, true, 0, stream_);
+        if (timing_) record(1 + H);
+        launchExclusiveScan(qcount, candOff_.as<uint64_t>(), nq, stream_);
+        launchClampCounts(candOff_.as<uint64_t>(), dK, nq, knnCount_.as<uint32_t>(), stream_);
+        launchExclusiveScan(knnCount_.as<uint32_t>(), knnOff_.as<uint64_t>(), nq, stream_);
+        launchTopK(candOff_.as<uint64_t>(), resIds_.as<uint64_t>(), resDist_.as<double>(), caps_.results, nullptr,
+                   nullptr, nullptr, 0, dK, nq, knnOff_.as<uint64_t>(), knnIds_.as<uint64_t>(), knnD2_.as<double>(),
+                   knnCount_.as<uint32_t>(), status, stream_);
+        if (timing_) record(2 + H);
+        return;
+    }
+    const FrontierIn F = inView(buf, hdrPtr(H - 1));
+    const FrontierBufs& fb = f_[buf];
+    const uint32_t fcap = static_cast<uint32_t>(caps_.entries);
+    // Rank F's entries per query (lower bound, or the learned score) and select the best few.
+    launchExclusiveScan(qcountF, offF_.as<uint64_t>(), nq, stream_);
+    launchEntryBounds(F.q, fb.node.as<uint32_t>(), F.x, F.hdr, fcap, D, dPoints, di_.nodeSub[H - 2].as<NodeRec>(),
+                      di_.aabb[H - 2].as<float>(), lbE_.as<double>(), scoreE_.as<double>(), stream_);
+    if (scorer_) scorer_(scorerCtx_, F, fb.node.as<uint32_t>(), fcap, dPoints, scoreE_.as<double>(), stream_);
+    const double avgLeaf = static_cast<double>(di_.meshCount[H - 1]) / static_cast<double>(di_.meshCount[H - 2]);
+    launchWaveWidth(dK, nq, 1.0 / avgLeaf, waveM_.as<uint32_t>(), stream_);
+    launchClampCounts(offF_.as<uint64_t>(), waveM_.as<uint32_t>(), nq, selCount_.as<uint32_t>(), stream_);
+    launchExclusiveScan(selCount_.as<uint32_t>(), selOff_.as<uint64_t>(), nq, stream_);
+    launchTopK(offF_.as<uint64_t>(), nullptr, scoreE_.as<double>(), fcap, nullptr, nullptr, nullptr, 0,
+               waveM_.as<uint32_t>(), nq, selOff_.as<uint64_t>(), selIds_.as<uint64_t>(), selD2_.as<double>(),
+               selCount_.as<uint32_t>(), status, stream_);
+    TBLAEQ_CUDA(cudaMemsetAsync(sel_.get(), 0, entryCap_, stream_));
+    launchScatterSel(selIds_.as<uint64_t>(), selOff_.as<uint64_t>(), nq, sel_.as<uint8_t>(), stream_);
+    // Wave 1: every point of the selected clusters; their K-th distance bounds tau.
+    fin.child.entrySel = sel_.as<uint8_t>();
+    fin.child.entryLb = lbE_.as<double>();
+    fin.wave = 1;
+    launchExpand(fin, kPredKnnPoint, true, 0, stream_);
     launchExclusiveScan(qcount, candOff_.as<uint64_t>(), nq, stream_);
     launchClampCounts(candOff_.as<uint64_t>(), dK, nq, knnCount_.as<uint32_t>(), stream_);
     launchExclusiveScan(knnCount_.as<uint32_t>(), knnOff_.as<uint64_t>(), nq, stream_);
     launchTopK(candOff_.as<uint64_t>(), resIds_.as<uint64_t>(), resDist_.as<double>(), caps_.results, nullptr, nullptr,
                nullptr, 0, dK, nq, knnOff_.as<uint64_t>(), knnIds_.as<uint64_t>(), knnD2_.as<double>(),
                knnCount_.as<uint32_t>(), status, stream_);
+    launchTauFromTopK(knnOff_.as<uint64_t>(), knnD2_.as<double>(), dK, nq, tau, stream_);
+    // Wave 2: the other clusters whose lower bound tau cannot exclude, points within tau.
+    ExpandArgs w2 = fin;
+    w2.scratch.desc = desc + static_cast<size_t>(H) * tileCap_;
+    w2.scratch.ticket = tickets + H;
+    w2.scratch.levelItems = nullptr;
+    w2.rout.ids = resIdsB_.as<uint64_t>();
+    w2.rout.q = resQB_.as<uint32_t>();
+    w2.rout.dist2 = resDistB_.as<double>();
+    w2.rout.qcount = qcountB;
+    w2.rout.hdr = hdrPtr(H + 1);
+    w2.rout.cap = static_cast<uint32_t>(resCapB_);
+    w2.wave = 2;
+    launchExpand(w2, kPredKnnPoint, true, 0, stream_);
+    if (timing_) record(1 + H);
+    launchExclusiveScan(qcountB, candOffB_.as<uint64_t>(), nq, stream_);
+    launchClampCounts2(candOff_.as<uint64_t>(), candOffB_.as<uint64_t>(), dK, nq, knnCount_.as<uint32_t>(), stream_);
+    launchExclusiveScan(knnCount_.as<uint32_t>(), knnOff_.as<uint64_t>(), nq, stream_);
+    launchTopK(candOff_.as<uint64_t>(), resIds_.as<uint64_t>(), resDist_.as<double>(), caps_.results,
+               candOffB_.as<uint64_t>(), resIdsB_.as<uint64_t>(), resDistB_.as<double>(), resCapB_, dK, nq,
+               knnOff_.as<uint64_t>(), knnIds_.as<uint64_t>(), knnD2_.as<double>(), knnCount_.as<uint32_t>(), status,
+               stream_);
     if (timing_) record(2 + H);
 }
 
 BatchOutput BatchEngine::runKnn(const double* dPoints, uint32_t nq, const uint32_t* dK, uint64_t sumK,
                                 unsigned flags) {
     reserve(caps_, nq, flags);
-    if (tau_.bytes() < static_cast<size_t>(nq) * 8 || knnCount_.bytes() < static_cast<size_t>(nq) * 4) {
-        tau_.alloc(std::max<size_t>(nq, 1) * 8);
-        knnCount_.alloc(std::max<size_t>(nq, 1) * 4);
-        candOff_.alloc((static_cast<size_t>(nq) + 1) * 8);
-        knnOff_.alloc((static_cast<size_t>(nq) + 1) * 8);
-    }
+    reserveKnn(nq);
     if (knnCap_ < std::max<uint64_t>(sumK, 1)) {
         knnCap_ = std::max<uint64_t>(sumK, 1);
         knnIds_.alloc(knnCap_ * 8);
@@ -561,7 +649,7 @@ BatchOutput BatchEngine::runKnn(const double* dPoints, uint32_t nq, const uint32
             return o;
         }
         growFromHeaders();
-        if (tau_.bytes() < static_cast<size_t>(nq) * 8) tau_.alloc(static_cast<size_t>(nq) * 8);
+        reserveKnn(nq);
     }
     throw CudaError(cudaErrorMemoryAllocation, "KNN workspace did not converge after 16 growth steps");
 }

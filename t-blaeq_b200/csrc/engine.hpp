@@ -53,6 +53,19 @@ public:
     // ascending by (distance, id). Blocks until done.
     BatchOutput runKnn(const double* dPoints, uint32_t nq, const uint32_t* dK, uint64_t sumK, unsigned flags);
     void enqueueKnn(const double* dPoints, uint32_t nq, const uint32_t* dK, unsigned flags);
+    // Two-wave final level (default on): rank the last frontier's clusters, expand the best few per
+    // query to bound the K-th distance by real points, then expand only the clusters that bound
+    // cannot exclude. Off: one pass over every surviving cluster.
+    void setTwoWave(bool on) { twoWave_ = on; }
+    bool twoWave() const { return twoWave_; }
+    // Optional device scorer of the last frontier's entries (higher = expand earlier); when unset
+    // the entries are ranked by their lower bound. Called with (frontier, hdr, cap, points, out scores).
+    using EntryScorer = void (*)(void* ctx, const FrontierIn& f, const uint32_t* node, uint32_t cap,
+                                 const double* points, double* score, cudaStream_t s);
+    void setScorer(EntryScorer fn, void* ctx) {
+        scorer_ = fn;
+        scorerCtx_ = ctx;
+    }
 
     // Enqueue a range batch without synchronising (capacities must already suffice; used for
     // CUDA-graph capture and timing). check() afterwards reports overflow / timeouts.
@@ -110,6 +123,13 @@ private:
     DeviceMem tau_, candOff_, knnCount_, knnOff_, knnIds_, knnD2_;
     uint64_t knnCap_ = 0;
     bool lastKnn_ = false;
+    // Two-wave final level of exact KNN (see enqueueKnn).
+    DeviceMem lbE_, scoreE_, sel_, offF_, waveM_, selCount_, selOff_, selIds_, selD2_, candOffB_;
+    DeviceMem resIdsB_, resQB_, resDistB_;
+    uint64_t entryCap_ = 0, resCapB_ = 0;
+    uint32_t knnQcap_ = 0;
+    size_t offQcountF_ = 0, offQcountB_ = 0;
+    void reserveKnn(uint32_t nq);
     size_t zeroBytes_ = 0;
     // offsets into zeroBlock_
     size_t offDesc_ = 0, offTickets_ = 0, offStatus_ = 0, offHdr_ = 0, offQcount_ = 0, offLevels_ = 0;
@@ -120,6 +140,9 @@ private:
     void dropGraph();
     bool timing_ = false;
     bool capturing_ = false;
+    bool twoWave_ = true;
+    EntryScorer scorer_ = nullptr;
+    void* scorerCtx_ = nullptr;
     std::vector<int> variants_;
     void record(int i);
     std::vector<cudaEvent_t> events_;

@@ -211,7 +211,10 @@ __global__ void __launch_bounds__(512) topKKernel(const uint64_t* offA, const ui
     }
     const uint64_t keep = std::min<uint64_t>(K, n);
     auto keyAt = [&](uint64_t i) -> uint64_t { return i < na ? orderKey(d2A[a0 + i]) : orderKey(d2B[b0 + i - na]); };
-    auto idAt = [&](uint64_t i) -> uint64_t { return i < na ? idsA[a0 + i] : idsB[b0 + i - na]; };
+    auto idAt = [&](uint64_t i) -> uint64_t {
+        if (i < na) return idsA ? idsA[a0 + i] : a0 + i;  // no id array: the candidate's position
+        return idsB ? idsB[b0 + i - na] : b0 + i - na;
+    };
     if (threadIdx.x == 0) outCount[q] = static_cast<uint32_t>(keep);
     if (keep == 0) return;
     const uint64_t o = outOff[q];
@@ -302,12 +305,99 @@ __global__ void clampCountsKernel(const uint64_t* off, const uint32_t* K, uint32
     }
 }
 
+__global__ void entryBoundsKernel(const uint32_t* q, const uint32_t* node, const double* x, const uint32_t* hdr,
+                                  uint32_t cap, int D, const double* points, const NodeRec* nodes, const float* aabb,
+                                  double* lb, double* score) {
+    const uint32_t n = min(hdr[0], cap);
+    for (uint32_t e = blockIdx.x * blockDim.x + threadIdx.x; e < n; e += gridDim.x * blockDim.x) {
+        const double* p = points + static_cast<size_t>(q[e]) * D;
+        const double* c = x + static_cast<size_t>(e) * D;
+        const uint32_t k = node[e];
+        const float* b = aabb + static_cast<size_t>(k) * 2 * D;
+        double dist = 0.0, gap = 0.0;
+        for (int d = 0; d < D; ++d) {
+            const double diff = p[d] - c[d];
+            dist = __fma_rn(diff, diff, dist);
+            const double l = static_cast<double>(b[d]), h = static_cast<double>(b[D + d]);
+            const double g = fmax(fmax(l - p[d], p[d] - h), 0.0);
+            gap = __fma_rn(g, g, gap);
+        }
+        const double v = fmax(sqrt(dist) - nodes[k].rad, sqrt(gap) * (1.0 - 1e-12));
+        lb[e] = v;
+        score[e] = v;
+    }
+}
+
+__global__ void waveWidthKernel(const uint32_t* K, uint32_t nq, double factor, uint32_t* M) {
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < nq; i += gridDim.x * blockDim.x) {
+        const double m = ceil(factor * static_cast<double>(K[i])) + 1.0;
+        M[i] = static_cast<uint32_t>(fmin(32.0, fmax(2.0, m)));
+    }
+}
+
+__global__ void scatterSelKernel(const uint64_t* ids, const uint64_t* off, uint32_t nq, uint8_t* sel) {
+    const uint64_t n = off[nq];
+    for (uint64_t i = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x; i < n;
+         i += static_cast<uint64_t>(gridDim.x) * blockDim.x)
+        sel[ids[i]] = 1;
+}
+
+__global__ void tauFromTopKKernel(const uint64_t* off, const double* d2, const uint32_t* K, uint32_t nq, double* tau) {
+    for (uint32_t q = blockIdx.x * blockDim.x + threadIdx.x; q < nq; q += gridDim.x * blockDim.x) {
+        const uint64_t n = off[q + 1] - off[q];
+        if (K[q] > 0 && n == K[q]) {
+            const double t = sqrt(d2[off[q + 1] - 1]) * (1.0 + 1e-12);
+            if (t < tau[q]) tau[q] = t;
+        }
+    }
+}
+
+__global__ void clampCounts2Kernel(const uint64_t* offA, const uint64_t* offB, const uint32_t* K, uint32_t nq,
+                                   uint32_t* out) {
+    for (uint32_t q = blockIdx.x * blockDim.x + threadIdx.x; q < nq; q += gridDim.x * blockDim.x) {
+        const uint64_t n = (offA[q + 1] - offA[q]) + (offB[q + 1] - offB[q]);
+        out[q] = static_cast<uint32_t>(n < K[q] ? n : K[q]);
+    }
+}
+
 int gridFor(uint64_t n, int threads) {
     const uint64_t b = (n + threads - 1) / threads;
     return static_cast<int>(std::max<uint64_t>(1, std::min<uint64_t>(b, 148ull * 16)));
 }
 
 }  // namespace
+
+void launchEntryBounds(const uint32_t* q, const uint32_t* node, const double* x, const uint32_t* hdr, uint32_t cap,
+                       int D, const double* points, const NodeRec* nodes, const float* aabb, double* lb, double* score,
+                       cudaStream_t s) {
+    entryBoundsKernel<<<148 * 8, 256, 0, s>>>(q, node, x, hdr, cap, D, points, nodes, aabb, lb, score);
+    TBLAEQ_CUDA(cudaGetLastError());
+}
+
+void launchWaveWidth(const uint32_t* K, uint32_t nq, double factor, uint32_t* M, cudaStream_t s) {
+    if (nq == 0) return;
+    waveWidthKernel<<<gridFor(nq, 256), 256, 0, s>>>(K, nq, factor, M);
+    TBLAEQ_CUDA(cudaGetLastError());
+}
+
+void launchScatterSel(const uint64_t* ids, const uint64_t* off, uint32_t nq, uint8_t* sel, cudaStream_t s) {
+    scatterSelKernel<<<148 * 4, 256, 0, s>>>(ids, off, nq, sel);
+    TBLAEQ_CUDA(cudaGetLastError());
+}
+
+void launchTauFromTopK(const uint64_t* off, const double* d2, const uint32_t* K, uint32_t nq, double* tau,
+                       cudaStream_t s) {
+    if (nq == 0) return;
+    tauFromTopKKernel<<<gridFor(nq, 256), 256, 0, s>>>(off, d2, K, nq, tau);
+    TBLAEQ_CUDA(cudaGetLastError());
+}
+
+void launchClampCounts2(const uint64_t* offA, const uint64_t* offB, const uint32_t* K, uint32_t nq, uint32_t* out,
+                        cudaStream_t s) {
+    if (nq == 0) return;
+    clampCounts2Kernel<<<gridFor(nq, 256), 256, 0, s>>>(offA, offB, K, nq, out);
+    TBLAEQ_CUDA(cudaGetLastError());
+}
 
 void launchFillDouble(double* v, double value, uint32_t n, cudaStream_t s) {
     if (n == 0) return;

@@ -48,6 +48,26 @@ void launchTopK(const uint64_t* offA, const uint64_t* idsA, const double* d2A, u
                 const uint64_t* outOff, uint64_t* outIds, double* outD2, uint32_t* outCount, uint32_t* status,
                 cudaStream_t s);
 
+// Lower bound and ranking score of every entry of the last KNN frontier: lb = max(centre distance -
+// subtree radius, distance to the entry's box) (conservative), score = lb.
+void launchEntryBounds(const uint32_t* q, const uint32_t* node, const double* x, const uint32_t* hdr, uint32_t cap,
+                       int D, const double* points, const NodeRec* nodes, const float* aabb, double* lb, double* score,
+                       cudaStream_t s);
+
+// Wave-1 width per query: clamp(ceil(factor * K[q]) + 1, 2, 32) entries.
+void launchWaveWidth(const uint32_t* K, uint32_t nq, double factor, uint32_t* M, cudaStream_t s);
+
+// sel[ids[i]] = 1 for every selected entry position in [0, off[nq]).
+void launchScatterSel(const uint64_t* ids, const uint64_t* off, uint32_t nq, uint8_t* sel, cudaStream_t s);
+
+// tau[q] = min(tau[q], sqrt(d2 of the K[q]-th candidate) * (1 + 1e-12)) when a query has K[q] of them.
+void launchTauFromTopK(const uint64_t* off, const double* d2, const uint32_t* K, uint32_t nq, double* tau,
+                       cudaStream_t s);
+
+// out[q] = min(K[q], (offA[q+1] - offA[q]) + (offB[q+1] - offB[q])).
+void launchClampCounts2(const uint64_t* offA, const uint64_t* offB, const uint32_t* K, uint32_t nq, uint32_t* out,
+                        cudaStream_t s);
+
 // v[i] = value for i < n.
 void launchFillDouble(double* v, double value, uint32_t n, cudaStream_t s);
 

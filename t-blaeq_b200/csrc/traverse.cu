@@ -323,6 +323,7 @@ __device__ __forceinline__ bool testItem(const ExpandArgs& a, int dim, const dou
         }
         return (cc > 0) && (lb <= tau);
     } else {  // kPredKnnPoint
+        if (a.wave == 1) return true;  // every point of a selected entry
         const double t = __ldcg(a.query.tau + qc.q);
         return pointDist2<DM>(y, qc.lo, dim, 1) <= t * t * (1.0 + 1e-9);
     }
@@ -458,7 +459,18 @@ __global__ void __launch_bounds__(kExpandThreads, TBLAEQ_EXPAND_MIN_BLOCKS) expa
             const bool valid = (validBits >> r) & 1u;
             bool keep = false;
             uint32_t cc = 0;
-            if (valid) {
+            bool work = valid;
+            if (PRED == kPredKnnPoint && valid && a.wave != 0) {
+                // Two-wave KNN: decide from the entry alone before touching the child's row.
+                const uint32_t e = sEnt[r * 32 + lane];
+                const bool sel = __ldg(a.child.entrySel + e) != 0;
+                if (a.wave == 1) {
+                    work = sel;
+                } else {
+                    work = !sel && __ldg(a.child.entryLb + e) <= __ldcg(a.query.tau + sQ[r * 32 + lane]);
+                }
+            }
+            if (work) {
                 const uint32_t j = sRow[r * 32 + lane];
                 const uint32_t e = sEnt[r * 32 + lane];
                 const uint32_t q = sQ[r * 32 + lane];
@@ -607,10 +619,11 @@ __global__ void __launch_bounds__(kExpandThreads, TBLAEQ_EXPAND_MIN_BLOCKS) expa
                     }
                 }
             }
-            if constexpr (TO_RESULT) {
-                if (a.rout.qcount && keep) {
+            {
+                uint32_t* qc = TO_RESULT ? a.rout.qcount : a.fout.qcount;
+                if (qc && keep) {
                     const uint32_t peers = __match_any_sync(kb, qr);
-                    if (lane == __ffs(peers) - 1) atomicAdd(&a.rout.qcount[qr], __popc(peers));
+                    if (lane == __ffs(peers) - 1) atomicAdd(&qc[qr], __popc(peers));
                 }
             }
             runCnt += __popc(kb);

@@ -64,6 +64,7 @@ struct FrontierOut {
     uint32_t* hdr;              // written by the tile holding the last item
     uint32_t cap;               // entry capacity
     uint32_t tileCap;           // tileStart capacity
+    uint32_t* qcount;           // optional per-query kept-entry counts (atomic)
 };
 
 struct ResultOut {
@@ -83,6 +84,11 @@ struct ChildLevel {
     const NodeRec* nodes;       // child node records (by key)
     const float* aabb;          // optional box of the points below each child (by key): lo[D] hi[D]
     const uint32_t* leaf;       // finest points below each child (by key), for the KNN bound
+    // Two-wave KNN over the last frontier (by input entry): wave 1 keeps every point of the
+    // selected entries; wave 2 skips selected entries and entries whose lower bound exceeds tau
+    // (without loading their rows) and keeps the points within tau.
+    const uint8_t* entrySel;
+    const double* entryLb;
     const uint8_t* mask;        // keep flags (by row) for kPredMask
     const uint64_t* outMap;     // final output id of row j (null: id = key)
 };
@@ -125,6 +131,7 @@ struct ExpandArgs {
     int D;
     int useFma;                 // accumulate squared distances with fma (reference kernels' contraction)
     int variant;                // Variant
+    int wave;                   // 0: plain; 1 / 2: two-wave KNN final level (see ChildLevel)
 };
 
 // Launch the expand kernel for dimension D with the given predicate; `toResult` selects the
