@@ -191,6 +191,43 @@ int tblaeq_autotune(tblaeq_handle* h, const tblaeq_batch* batch, int reps, int* 
 /* Set the expand-kernel variant per level (0 = direct, 1 = staged), e.g. from a tuning cache. */
 int tblaeq_set_variants(tblaeq_handle* h, const int* variants, uint64_t n);
 
+/* ---- Exact KNN tuning and the learned frontier scorer (no counterpart in the reference) ----
+ * Exact KNN batches end with a two-wave finest level: each query's surviving finest clusters are
+ * ranked, the best few are expanded first so the K-th distance is bounded by real points, and only
+ * the clusters that bound cannot exclude are expanded next. The ranking is the clusters' lower
+ * bound, or the learned scorer (a 2x64 MLP over query || centroid || radius || level one-hot, BF16
+ * weights, FP32 accumulation) once trained. Exactness never depends on the ranking. */
+
+/* 1 (default) = two-wave finest level, 0 = one pass over every surviving cluster. */
+int tblaeq_set_two_wave(tblaeq_handle* h, int on);
+
+/* Counters of the last KNN batch: [0] final-frontier clusters, [1] wave-1 candidates,
+ * [2] wave-2 candidates, [3] points whose rows wave 2 loaded and tested. */
+int tblaeq_knn_counters(tblaeq_handle* h, uint64_t* out4);
+
+/* Trains the scorer on traces of exact KNN over the given training queries (host points, nq x D;
+ * per-query K or uniform K), sampling up to max_samples (query, cluster) examples; runs `epochs`
+ * of Adam with learning rate lr. loss_out (epochs entries, may be NULL) receives the mean loss of
+ * each epoch. Leaves the scorer enabled. */
+int tblaeq_scorer_train(tblaeq_handle* h, const double* points, uint64_t nq, const uint32_t* k_per_query, uint64_t K,
+                        uint64_t max_samples, int epochs, float lr, uint64_t seed, float* loss_out);
+
+/* Enable (1) or disable (0) the trained scorer for KNN ranking. */
+int tblaeq_scorer_enable(tblaeq_handle* h, int on);
+
+/* Scorer parameters as FP32 (layout W1[in][64] | b1[64] | W2[64][64] | b2[64] | w3[64] | b3 with
+ * in = 2D + 1 + (height-1)): *n receives the count; get copies up to cap values. */
+int tblaeq_scorer_get_params(tblaeq_handle* h, float* out, uint64_t cap, uint64_t* n);
+int tblaeq_scorer_set_params(tblaeq_handle* h, const float* params, uint64_t n);
+
+/* Mean binary cross-entropy of host samples X (n x in) / labels y under the current parameters
+ * (BF16 forward, FP32 accumulation) and its gradient (params-sized) -- for gradient checks. */
+int tblaeq_scorer_loss_grad(tblaeq_handle* h, const float* X, const float* y, uint64_t n, float* grad_out,
+                            float* loss_out);
+
+/* Logits of host samples X (n x in). */
+int tblaeq_scorer_logits(tblaeq_handle* h, const float* X, uint64_t n, float* z_out);
+
 /* Host copies of the index arrays (read-only, owned by the handle), for tools and tests:
  * which = 0: P-tensor values of interval l (rows*D doubles), 1: colRes of interval l (cols+1),
  * 2: max radius of interval l (cols), 3: Map of mesh l (meshSizes), 4: coarsest ids, 5: coarsest vals. */

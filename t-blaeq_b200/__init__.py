@@ -132,6 +132,16 @@ def _load():
         "tblaeq_stage_times": ([vp, P(ctypes.c_float), ctypes.c_int], ctypes.c_int),
         "tblaeq_autotune": ([vp, P(_Batch), ctypes.c_int, P(ctypes.c_int), P(ctypes.c_float)], ctypes.c_int),
         "tblaeq_set_variants": ([vp, P(ctypes.c_int), ctypes.c_uint64], ctypes.c_int),
+        "tblaeq_set_two_wave": ([vp, ctypes.c_int], ctypes.c_int),
+        "tblaeq_knn_counters": ([vp, P(ctypes.c_uint64)], ctypes.c_int),
+        "tblaeq_scorer_train": ([vp, P(ctypes.c_double), ctypes.c_uint64, vp, ctypes.c_uint64, ctypes.c_uint64,
+                                 ctypes.c_int, ctypes.c_float, ctypes.c_uint64, P(ctypes.c_float)], ctypes.c_int),
+        "tblaeq_scorer_enable": ([vp, ctypes.c_int], ctypes.c_int),
+        "tblaeq_scorer_get_params": ([vp, P(ctypes.c_float), ctypes.c_uint64, P(ctypes.c_uint64)], ctypes.c_int),
+        "tblaeq_scorer_set_params": ([vp, P(ctypes.c_float), ctypes.c_uint64], ctypes.c_int),
+        "tblaeq_scorer_loss_grad": ([vp, P(ctypes.c_float), P(ctypes.c_float), ctypes.c_uint64, P(ctypes.c_float),
+                                     P(ctypes.c_float)], ctypes.c_int),
+        "tblaeq_scorer_logits": ([vp, P(ctypes.c_float), ctypes.c_uint64, P(ctypes.c_float)], ctypes.c_int),
         "tblaeq_live_device_bytes": ([], ctypes.c_uint64),
         "tblaeq_debug_fail_alloc_after": ([ctypes.c_uint64], None),
     }
@@ -423,6 +433,54 @@ class QueryHandler:
     def set_variants(self, variants):
         arr = (ctypes.c_int * len(variants))(*[int(x) for x in variants])
         _check(_load().tblaeq_set_variants(self._h, arr, len(variants)))
+
+    # -- exact KNN tuning and the learned scorer ----------------------------------------------------
+    def set_two_wave(self, on: bool):
+        _check(_load().tblaeq_set_two_wave(self._h, int(on)))
+
+    def knn_counters(self) -> dict:
+        out = (ctypes.c_uint64 * 4)()
+        _check(_load().tblaeq_knn_counters(self._h, out))
+        return {"frontier": out[0], "wave1": out[1], "wave2": out[2], "wave2_rows": out[3]}
+
+    def scorer_train(self, points, K=10, max_samples: int = 200000, epochs: int = 8, lr: float = 3e-3,
+                     seed: int = 1) -> list:
+        p = np.ascontiguousarray(np.asarray(points, dtype=np.float64))
+        nq = p.shape[0]
+        kq, kval = _k_args(K, nq)
+        losses = (ctypes.c_float * epochs)()
+        _check(_load().tblaeq_scorer_train(self._h, _dptr(p), nq, kq.ctypes.data if kq is not None else None, kval,
+                                           max_samples, epochs, lr, seed, losses))
+        return list(losses)
+
+    def scorer_enable(self, on: bool = True):
+        _check(_load().tblaeq_scorer_enable(self._h, int(on)))
+
+    def scorer_params(self) -> np.ndarray:
+        n = ctypes.c_uint64()
+        _check(_load().tblaeq_scorer_get_params(self._h, None, 0, ctypes.byref(n)))
+        out = np.empty(n.value, np.float32)
+        _check(_load().tblaeq_scorer_get_params(self._h, _dptr(out, ctypes.c_float), n.value, ctypes.byref(n)))
+        return out
+
+    def scorer_set_params(self, params):
+        p = np.ascontiguousarray(np.asarray(params, dtype=np.float32))
+        _check(_load().tblaeq_scorer_set_params(self._h, _dptr(p, ctypes.c_float), p.size))
+
+    def scorer_loss_grad(self, X, y):
+        X = np.ascontiguousarray(np.asarray(X, dtype=np.float32))
+        y = np.ascontiguousarray(np.asarray(y, dtype=np.float32))
+        grad = np.empty(self.scorer_params().size, np.float32)
+        loss = ctypes.c_float()
+        _check(_load().tblaeq_scorer_loss_grad(self._h, _dptr(X, ctypes.c_float), _dptr(y, ctypes.c_float), X.shape[0],
+                                               _dptr(grad, ctypes.c_float), ctypes.byref(loss)))
+        return float(loss.value), grad
+
+    def scorer_logits(self, X) -> np.ndarray:
+        X = np.ascontiguousarray(np.asarray(X, dtype=np.float32))
+        z = np.empty(X.shape[0], np.float32)
+        _check(_load().tblaeq_scorer_logits(self._h, _dptr(X, ctypes.c_float), X.shape[0], _dptr(z, ctypes.c_float)))
+        return z
 
     def stream_handle(self) -> int:
         return _load().tblaeq_stream(self._h) or 0

@@ -7,6 +7,7 @@
 #include "../../include/tblaeq.h"
 #include "handler.hpp"
 #include "noalloc.hpp"
+#include "scorer.hpp"
 
 using namespace tblaeq;
 
@@ -394,6 +395,106 @@ int tblaeq_set_variants(tblaeq_handle* h, const int* variants, uint64_t n) {
     if (!variants) return fail(TBLAEQ_ERR_INVALID, "null variants");
     return guarded([&]() -> int {
         h->qh->runtime().engine->setVariants(std::vector<int>(variants, variants + n));
+        return TBLAEQ_OK;
+    });
+}
+
+int tblaeq_set_two_wave(tblaeq_handle* h, int on) {
+    if (int c = checkPrepared(h)) return c;
+    h->qh->runtime().engine->setTwoWave(on != 0);
+    return TBLAEQ_OK;
+}
+
+int tblaeq_knn_counters(tblaeq_handle* h, uint64_t* out4) {
+    if (int c = checkPrepared(h)) return c;
+    if (!out4) return fail(TBLAEQ_ERR_INVALID, "null output");
+    return guarded([&]() -> int {
+        const std::vector<uint64_t> v = h->qh->runtime().engine->knnCounters();
+        for (int i = 0; i < 4; ++i) out4[i] = v[i];
+        return TBLAEQ_OK;
+    });
+}
+
+int tblaeq_scorer_train(tblaeq_handle* h, const double* points, uint64_t nq, const uint32_t* k_per_query, uint64_t K,
+                        uint64_t max_samples, int epochs, float lr, uint64_t seed, float* loss_out) {
+    if (int c = checkPrepared(h)) return c;
+    if (!points || nq == 0 || nq > 0xffffffffull || epochs < 1 || max_samples == 0)
+        return fail(TBLAEQ_ERR_INVALID, "scorer training needs queries, epochs >= 1 and samples > 0");
+    return guarded([&]() -> int {
+        Runtime& rt = h->qh->runtime();
+        std::vector<uint32_t> k(nq);
+        for (uint64_t i = 0; i < nq; ++i) k[i] = static_cast<uint32_t>(k_per_query ? k_per_query[i] : K);
+        ScorerTrainConfig cfg;
+        cfg.maxSamples = max_samples;
+        cfg.epochs = epochs;
+        cfg.lr = lr;
+        cfg.seed = seed;
+        const std::vector<float> losses = trainScorer(rt, points, static_cast<uint32_t>(nq), k, cfg);
+        if (loss_out) std::copy(losses.begin(), losses.end(), loss_out);
+        enableScorer(rt, true);
+        return TBLAEQ_OK;
+    });
+}
+
+int tblaeq_scorer_enable(tblaeq_handle* h, int on) {
+    if (int c = checkPrepared(h)) return c;
+    return guarded([&]() -> int {
+        enableScorer(h->qh->runtime(), on != 0);
+        return TBLAEQ_OK;
+    });
+}
+
+int tblaeq_scorer_get_params(tblaeq_handle* h, float* out, uint64_t cap, uint64_t* n) {
+    if (int c = checkPrepared(h)) return c;
+    return guarded([&]() -> int {
+        const std::vector<float> p = ensureScorer(h->qh->runtime()).getParams();
+        if (n) *n = p.size();
+        if (out) std::copy(p.begin(), p.begin() + std::min<uint64_t>(cap, p.size()), out);
+        return TBLAEQ_OK;
+    });
+}
+
+int tblaeq_scorer_set_params(tblaeq_handle* h, const float* params, uint64_t n) {
+    if (int c = checkPrepared(h)) return c;
+    if (!params) return fail(TBLAEQ_ERR_INVALID, "null parameters");
+    return guarded([&]() -> int {
+        Runtime& rt = h->qh->runtime();
+        ensureScorer(rt).setParams(std::vector<float>(params, params + n), rt.stream);
+        return TBLAEQ_OK;
+    });
+}
+
+int tblaeq_scorer_loss_grad(tblaeq_handle* h, const float* X, const float* y, uint64_t n, float* grad_out,
+                            float* loss_out) {
+    if (int c = checkPrepared(h)) return c;
+    if (!X || !y || !grad_out || n == 0 || n > 0xffffffffull) return fail(TBLAEQ_ERR_INVALID, "bad samples");
+    return guarded([&]() -> int {
+        Runtime& rt = h->qh->runtime();
+        Mlp& m = ensureScorer(rt);
+        const int in = m.shape().in();
+        DeviceMem dX(n * in * 4), dy(n * 4), dg(m.shape().params() * 4);
+        TBLAEQ_CUDA(cudaMemcpyAsync(dX.get(), X, n * in * 4, cudaMemcpyHostToDevice, rt.stream));
+        TBLAEQ_CUDA(cudaMemcpyAsync(dy.get(), y, n * 4, cudaMemcpyHostToDevice, rt.stream));
+        const float loss = m.lossAndGrad(dX.as<float>(), dy.as<float>(), static_cast<uint32_t>(n), dg.as<float>(), rt.stream);
+        TBLAEQ_CUDA(cudaMemcpyAsync(grad_out, dg.get(), m.shape().params() * 4, cudaMemcpyDeviceToHost, rt.stream));
+        TBLAEQ_CUDA(cudaStreamSynchronize(rt.stream));
+        if (loss_out) *loss_out = loss;
+        return TBLAEQ_OK;
+    });
+}
+
+int tblaeq_scorer_logits(tblaeq_handle* h, const float* X, uint64_t n, float* z_out) {
+    if (int c = checkPrepared(h)) return c;
+    if (!X || !z_out || n > 0xffffffffull) return fail(TBLAEQ_ERR_INVALID, "bad samples");
+    return guarded([&]() -> int {
+        Runtime& rt = h->qh->runtime();
+        Mlp& m = ensureScorer(rt);
+        const int in = m.shape().in();
+        DeviceMem dX(std::max<uint64_t>(n, 1) * in * 4), dz(std::max<uint64_t>(n, 1) * 4);
+        TBLAEQ_CUDA(cudaMemcpyAsync(dX.get(), X, n * in * 4, cudaMemcpyHostToDevice, rt.stream));
+        m.logits(dX.as<float>(), static_cast<uint32_t>(n), dz.as<float>(), rt.stream);
+        TBLAEQ_CUDA(cudaMemcpyAsync(z_out, dz.get(), n * 4, cudaMemcpyDeviceToHost, rt.stream));
+        TBLAEQ_CUDA(cudaStreamSynchronize(rt.stream));
         return TBLAEQ_OK;
     });
 }

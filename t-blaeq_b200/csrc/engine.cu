@@ -207,6 +207,8 @@ void BatchEngine::reserve(const EngineCaps& want, uint32_t nq, unsigned flags) {
         off = align256(off + static_cast<size_t>(qcap_) * 4);
         offQcountB_ = off;
         off = align256(off + static_cast<size_t>(qcap_) * 4);
+        offWork_ = off;
+        off = align256(off + 8);
         zeroBytes_ = off;
         zeroBlock_.alloc(zeroBytes_);
         offsets_.alloc((static_cast<size_t>(qcap_) + 1) * 8);
@@ -475,6 +477,26 @@ uint64_t BatchEngine::runGridLevel(int l, const uint64_t* dIds, const double* dV
 
 namespace tblaeq {
 
+BatchEngine::FrontierView BatchEngine::lastKnnFrontier() const {
+    const int H = static_cast<int>(di_.height);
+    FrontierView v;
+    v.in = inView(lastKnnBuf_, hdrPtr(H - 1));
+    v.node = f_[lastKnnBuf_].node.as<uint32_t>();
+    v.cap = static_cast<uint32_t>(caps_.entries);
+    v.offsets = twoWave_ ? offF_.as<uint64_t>() : nullptr;
+    return v;
+}
+
+std::vector<uint64_t> BatchEngine::knnCounters() {
+    const int H = static_cast<int>(di_.height);
+    std::vector<uint32_t> h((H + 2) * 2);
+    unsigned long long work = 0;
+    TBLAEQ_CUDA(cudaMemcpyAsync(h.data(), hdrPtr(0), h.size() * 4, cudaMemcpyDeviceToHost, stream_));
+    TBLAEQ_CUDA(cudaMemcpyAsync(&work, zeroBlock_.as<char>() + offWork_, 8, cudaMemcpyDeviceToHost, stream_));
+    TBLAEQ_CUDA(cudaStreamSynchronize(stream_));
+    return {h[2 * (H - 1)], h[2 * H], h[2 * (H + 1)], work};
+}
+
 void BatchEngine::reserveKnn(uint32_t nq) {
     if (knnQcap_ < std::max<uint32_t>(nq, 1)) {
         knnQcap_ = std::max<uint32_t>(nq, 1);
@@ -556,6 +578,7 @@ void BatchEngine::enqueueKnn(const double* dPoints, uint32_t nq, const uint32_t*
         if (timing_) record(2 + m);
     }
     // `buf` now holds the last frontier F: the surviving finest clusters, query-major.
+    lastKnnBuf_ = buf;
     ExpandArgs fin = base(H - 1, buf);
     fin.child.outMap = di_.maps[H - 1].as<uint64_t>();
     fin.rout.ids = resIds_.as<uint64_t>();
@@ -617,6 +640,7 @@ void BatchEngine::enqueueKnn(const double* dPoints, uint32_t nq, const uint32_t*
     w2.rout.hdr = hdrPtr(H + 1);
     w2.rout.cap = static_cast<uint32_t>(resCapB_);
     w2.wave = 2;
+    w2.scratch.work = reinterpret_cast<unsigned long long*>(z + offWork_);
     launchExpand(w2, kPredKnnPoint, true, 0, stream_);
     if (timing_) record(1 + H);
     launchExclusiveScan(qcountB, candOffB_.as<uint64_t>(), nq, stream_);

@@ -62,6 +62,18 @@ public:
     // the entries are ranked by their lower bound. Called with (frontier, hdr, cap, points, out scores).
     using EntryScorer = void (*)(void* ctx, const FrontierIn& f, const uint32_t* node, uint32_t cap,
                                  const double* points, double* score, cudaStream_t s);
+    // The last KNN batch's final frontier (surviving finest clusters, query-major): view, node
+    // positions and capacity; valid until the next batch.
+    struct FrontierView {
+        FrontierIn in;
+        const uint32_t* node;
+        uint32_t cap;
+        const uint64_t* offsets;  // per-query entry offsets (nq + 1), two-wave batches only
+    };
+    FrontierView lastKnnFrontier() const;
+    // Counters of the last KNN batch: [0] final-frontier entries, [1] wave-1 candidates,
+    // [2] wave-2 candidates, [3] rows loaded in wave 2 (the work the ranking saves).
+    std::vector<uint64_t> knnCounters();
     void setScorer(EntryScorer fn, void* ctx) {
         scorer_ = fn;
         scorerCtx_ = ctx;
@@ -128,7 +140,8 @@ private:
     DeviceMem resIdsB_, resQB_, resDistB_;
     uint64_t entryCap_ = 0, resCapB_ = 0;
     uint32_t knnQcap_ = 0;
-    size_t offQcountF_ = 0, offQcountB_ = 0;
+    size_t offQcountF_ = 0, offQcountB_ = 0, offWork_ = 0;
+    int lastKnnBuf_ = 0;
     void reserveKnn(uint32_t nq);
     size_t zeroBytes_ = 0;
     // offsets into zeroBlock_

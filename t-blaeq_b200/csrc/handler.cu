@@ -80,6 +80,9 @@ IndexPolicy PolicyScheduler::recommend(const HostIndex& idx, uint64_t freeBytes)
 }
 
 Runtime::~Runtime() {
+    scorer.reset();
+    invMapFinest.release();
+    parentFinest.release();
     engine.reset();
     pluginEngine.reset();
     levelOut.clear();

@@ -15,6 +15,7 @@
 #include "device_index.hpp"
 #include "engine.hpp"
 #include "index.hpp"
+#include "mlp.cuh"
 
 namespace tblaeq {
 
@@ -147,6 +148,11 @@ struct Runtime {
     DeviceMem knnKeys, knnKeys2, knnLabels, knnLabels2, knnCnt, knnRr, pluginMask;
     uint64_t knnCap = 0;
     DeviceMem scratchQuery;  // lo|hi or point staged on the device
+    // Learned frontier scorer and the maps its training labels need.
+    std::unique_ptr<Mlp> scorer;
+    double scorerInvScale = 1.0;
+    uint64_t scorerSamples = 0, scorerPositives = 0;
+    DeviceMem invMapFinest, parentFinest;
     ~Runtime();
 };
 

@@ -514,6 +514,10 @@ __global__ void __launch_bounds__(kExpandThreads, TBLAEQ_EXPAND_MIN_BLOCKS) expa
                 }
                 keep = testItem<DM, PRED, TO_RESULT>(a, dim, y, qc, j, kk, nr, cc);
             }
+            if (a.scratch.work) {
+                const uint32_t wm = __ballot_sync(FULL, work);
+                if (lane == 0 && wm) atomicAdd(a.scratch.work, static_cast<unsigned long long>(__popc(wm)));
+            }
             // Per-query generated-children counts (the reference's levelFineMeshSize).
             if (a.scratch.levelItems) {
                 const uint32_t vm = __ballot_sync(FULL, valid);

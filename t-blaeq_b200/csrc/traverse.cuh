@@ -106,6 +106,7 @@ struct Scratch {
     uint32_t* ticket;           // tile ticket counter, zeroed before launch
     uint32_t* status;           // DeviceStatus bits
     uint32_t* levelItems;       // optional: per-query count of generated children at this level
+    unsigned long long* work;   // optional: number of child rows actually loaded and tested
 };
 
 enum Pred : int {
