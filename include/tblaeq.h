@@ -202,8 +202,9 @@ int tblaeq_set_variants(tblaeq_handle* h, const int* variants, uint64_t n);
 int tblaeq_set_two_wave(tblaeq_handle* h, int on);
 
 /* Counters of the last KNN batch: [0] final-frontier clusters, [1] wave-1 candidates,
- * [2] wave-2 candidates, [3] points whose rows wave 2 loaded and tested. */
-int tblaeq_knn_counters(tblaeq_handle* h, uint64_t* out4);
+ * [2] wave-2 candidates, [3] points whose rows wave 1 loaded and tested (the single pass, when
+ * two-wave is off), [4] points whose rows wave 2 loaded and tested. */
+int tblaeq_knn_counters(tblaeq_handle* h, uint64_t* out5);
 
 /* Trains the scorer on traces of exact KNN over the given training queries (host points, nq x D;
  * per-query K or uniform K), sampling up to max_samples (query, cluster) examples; runs `epochs`

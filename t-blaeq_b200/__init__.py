@@ -439,9 +439,10 @@ class QueryHandler:
         _check(_load().tblaeq_set_two_wave(self._h, int(on)))
 
     def knn_counters(self) -> dict:
-        out = (ctypes.c_uint64 * 4)()
+        out = (ctypes.c_uint64 * 5)()
         _check(_load().tblaeq_knn_counters(self._h, out))
-        return {"frontier": out[0], "wave1": out[1], "wave2": out[2], "wave2_rows": out[3]}
+        return {"frontier": out[0], "wave1": out[1], "wave2": out[2], "rows1": out[3], "rows2": out[4],
+                "rows": out[3] + out[4]}
 
     def scorer_train(self, points, K=10, max_samples: int = 200000, epochs: int = 8, lr: float = 3e-3,
                      seed: int = 1) -> list:

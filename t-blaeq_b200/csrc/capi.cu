@@ -405,12 +405,12 @@ int tblaeq_set_two_wave(tblaeq_handle* h, int on) {
     return TBLAEQ_OK;
 }
 
-int tblaeq_knn_counters(tblaeq_handle* h, uint64_t* out4) {
+int tblaeq_knn_counters(tblaeq_handle* h, uint64_t* out5) {
     if (int c = checkPrepared(h)) return c;
-    if (!out4) return fail(TBLAEQ_ERR_INVALID, "null output");
+    if (!out5) return fail(TBLAEQ_ERR_INVALID, "null output");
     return guarded([&]() -> int {
         const std::vector<uint64_t> v = h->qh->runtime().engine->knnCounters();
-        for (int i = 0; i < 4; ++i) out4[i] = v[i];
+        for (int i = 0; i < 5; ++i) out5[i] = v[i];
         return TBLAEQ_OK;
     });
 }

@@ -208,7 +208,7 @@ void BatchEngine::reserve(const EngineCaps& want, uint32_t nq, unsigned flags) {
         offQcountB_ = off;
         off = align256(off + static_cast<size_t>(qcap_) * 4);
         offWork_ = off;
-        off = align256(off + 8);
+        off = align256(off + 2 * 8);
         zeroBytes_ = off;
         zeroBlock_.alloc(zeroBytes_);
         offsets_.alloc((static_cast<size_t>(qcap_) + 1) * 8);
@@ -344,17 +344,27 @@ void BatchEngine::growFromHeaders() {
             grew = true;
         }
     }
-    const uint64_t res = h[2 * H];
+    // Results: slot H holds the one-pass (or wave-1) results, slot H+1 the wave-2 results of a
+    // two-wave KNN batch (whose buffer follows the same capacity).
+    const uint64_t res = std::max<uint64_t>(h[2 * H], h[2 * (H + 1)]);
     if (res > caps_.results) {
         want.results = std::max<uint64_t>(want.results, res + res / 4 + 4096);
         grew = true;
     }
     if (!grew) {
+        // Every capacity is tracked by a header above; an overflow none of them shows is not
+        // expected. Entry and result buffers double (cheap); item capacity is exact from the sums.
         want.entries *= 2;
-        want.items *= 2;
         want.results *= 2;
     }
-    reserve(want, qcap_, haveVals_ ? kWantVals : 0);
+    try {
+        reserve(want, qcap_, haveVals_ ? kWantVals : 0);
+    } catch (const CudaError& e) {
+        std::string msg = std::string(e.what()) + " (status " + std::to_string(status()) + "; level entries/items:";
+        for (int lv = 0; lv < H + 2; ++lv) msg += " " + std::to_string(h[2 * lv]) + "/" + std::to_string(h[2 * lv + 1]);
+        msg += ")";
+        throw CudaError(cudaErrorMemoryAllocation, msg);
+    }
 }
 
 BatchOutput BatchEngine::output(uint32_t nq, unsigned flags) const {
@@ -385,6 +395,8 @@ BatchOutput BatchEngine::runRange(const double* dBoxes, uint32_t nq, int mode, u
         if (st & (kStatusLookbackTimeout | kStatusWindowOverflow)) {
             throw CudaError(cudaErrorLaunchTimeout, "traversal kernel reported status " + std::to_string(st));
         }
+        if (st & kStatusOverflowSum)
+            throw CudaError(cudaErrorMemoryAllocation, "a level generates more than 2^32 items; split the batch");
         if (st == 0) {
             BatchOutput o = output(nq, flags);
             o.total = lastTotal(nq);
@@ -490,11 +502,13 @@ BatchEngine::FrontierView BatchEngine::lastKnnFrontier() const {
 std::vector<uint64_t> BatchEngine::knnCounters() {
     const int H = static_cast<int>(di_.height);
     std::vector<uint32_t> h((H + 2) * 2);
-    unsigned long long work = 0;
+    unsigned long long work[2] = {0, 0};
     TBLAEQ_CUDA(cudaMemcpyAsync(h.data(), hdrPtr(0), h.size() * 4, cudaMemcpyDeviceToHost, stream_));
-    TBLAEQ_CUDA(cudaMemcpyAsync(&work, zeroBlock_.as<char>() + offWork_, 8, cudaMemcpyDeviceToHost, stream_));
+    TBLAEQ_CUDA(cudaMemcpyAsync(work, zeroBlock_.as<char>() + offWork_, 16, cudaMemcpyDeviceToHost, stream_));
     TBLAEQ_CUDA(cudaStreamSynchronize(stream_));
-    return {h[2 * (H - 1)], h[2 * H], h[2 * (H + 1)], work};
+    // One-pass traversal loads every child row of the final frontier: its item count.
+    const uint64_t rows1 = twoWave_ ? work[0] : h[2 * (H - 1) + 1];
+    return {h[2 * (H - 1)], h[2 * H], h[2 * (H + 1)], rows1, twoWave_ ? work[1] : 0};
 }
 
 void BatchEngine::reserveKnn(uint32_t nq) {
@@ -620,6 +634,7 @@ void BatchEngine::enqueueKnn(const double* dPoints, uint32_t nq, const uint32_t*
     fin.child.entrySel = sel_.as<uint8_t>();
     fin.child.entryLb = lbE_.as<double>();
     fin.wave = 1;
+    fin.scratch.work = reinterpret_cast<unsigned long long*>(z + offWork_);
     launchExpand(fin, kPredKnnPoint, true, 0, stream_);
     launchExclusiveScan(qcount, candOff_.as<uint64_t>(), nq, stream_);
     launchClampCounts(candOff_.as<uint64_t>(), dK, nq, knnCount_.as<uint32_t>(), stream_);
@@ -640,7 +655,7 @@ void BatchEngine::enqueueKnn(const double* dPoints, uint32_t nq, const uint32_t*
     w2.rout.hdr = hdrPtr(H + 1);
     w2.rout.cap = static_cast<uint32_t>(resCapB_);
     w2.wave = 2;
-    w2.scratch.work = reinterpret_cast<unsigned long long*>(z + offWork_);
+    w2.scratch.work = reinterpret_cast<unsigned long long*>(z + offWork_) + 1;
     launchExpand(w2, kPredKnnPoint, true, 0, stream_);
     if (timing_) record(1 + H);
     launchExclusiveScan(qcountB, candOffB_.as<uint64_t>(), nq, stream_);
@@ -667,6 +682,8 @@ BatchOutput BatchEngine::runKnn(const double* dPoints, uint32_t nq, const uint32
         const uint32_t st = status();
         if (st & (kStatusLookbackTimeout | kStatusWindowOverflow))
             throw CudaError(cudaErrorLaunchTimeout, "traversal kernel reported status " + std::to_string(st));
+        if (st & kStatusOverflowSum)
+            throw CudaError(cudaErrorMemoryAllocation, "a level generates more than 2^32 items; split the batch");
         if (st == 0) {
             BatchOutput o = output(nq, flags);
             o.total = lastTotal(nq);

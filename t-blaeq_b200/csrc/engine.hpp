@@ -72,7 +72,8 @@ public:
     };
     FrontierView lastKnnFrontier() const;
     // Counters of the last KNN batch: [0] final-frontier entries, [1] wave-1 candidates,
-    // [2] wave-2 candidates, [3] rows loaded in wave 2 (the work the ranking saves).
+    // [2] wave-2 candidates, [3] point rows loaded by wave 1 (by the single pass when two-wave is
+    // off), [4] point rows loaded by wave 2. [3] + [4] is the finest-level work the ranking saves.
     std::vector<uint64_t> knnCounters();
     void setScorer(EntryScorer fn, void* ctx) {
         scorer_ = fn;

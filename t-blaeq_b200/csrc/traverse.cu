@@ -363,11 +363,15 @@ __global__ void __launch_bounds__(kExpandThreads, TBLAEQ_EXPAND_MIN_BLOCKS) expa
         return;
     }
 
+    unsigned long long warpRows = 0;  // child rows this warp loaded (two-wave work counter)
     while (true) {
         uint32_t tile = 0;
         if (lane == 0) tile = atomicAdd(a.scratch.ticket, 1u);
         tile = __shfl_sync(FULL, tile, 0);
-        if (tile >= nTiles) break;
+        if (tile >= nTiles) {
+            if (a.scratch.work && lane == 0 && warpRows) atomicAdd(a.scratch.work, warpRows);
+            break;
+        }
         const uint32_t t0 = tile * kWarpTile;
 
         // ---- phase A: stage the tile's entries in shared memory (one round of parallel loads),
@@ -514,10 +518,7 @@ __global__ void __launch_bounds__(kExpandThreads, TBLAEQ_EXPAND_MIN_BLOCKS) expa
                 }
                 keep = testItem<DM, PRED, TO_RESULT>(a, dim, y, qc, j, kk, nr, cc);
             }
-            if (a.scratch.work) {
-                const uint32_t wm = __ballot_sync(FULL, work);
-                if (lane == 0 && wm) atomicAdd(a.scratch.work, static_cast<unsigned long long>(__popc(wm)));
-            }
+            if (a.scratch.work) warpRows += __popc(__ballot_sync(FULL, work));
             // Per-query generated-children counts (the reference's levelFineMeshSize).
             if (a.scratch.levelItems) {
                 const uint32_t vm = __ballot_sync(FULL, valid);

@@ -104,3 +104,20 @@ def test_knn_ref_parity_batch_is_rejected(tb, env):
     with pytest.raises(tb.TblaeqError) as e:
         h.query_batch(tb.QueryType.POINT, pts[:2], tb.Mode.REF_PARITY, K=5)
     assert e.value.code == 1
+
+
+def test_knn_first_batch_grows_every_buffer(tb, oracle_mod, cuda):
+    """A fresh engine whose first KNN batch overflows the wave-2 result buffer grows it and reruns
+    (wave-2 results have their own header; growth must read it, not double blindly)."""
+    h = tb.QueryHandler.generate(100000, 8, 1.0, 100.0, False, 3, (100, 20), 57, 2.5)
+    h.prepare_for_query(tb.LevelPolicy.L0)
+    pts, ids = h.decode_points(np.arange(100000))
+    P = _points(pts, 2000, 11, noise=1.0)
+    r = h.query_batch(tb.QueryType.POINT, P, tb.Mode.EXACT, K=20)
+    c = h.knn_counters()
+    assert c["wave2"] > 0
+    b = oracle_mod.brute_query(pts, ids, oracle_mod.KNN, P[:64], K=20)
+    off = r.offsets.numpy()
+    assert np.array_equal(off[:65], b.offsets)
+    assert np.array_equal(r.ids.numpy()[:off[64]], b.ids)
+    assert np.array_equal(r.dist2.numpy()[:off[64]], b.dist2)

@@ -63,7 +63,6 @@ def env(tb, oracle_mod, tmp_path_factory, cuda):
 def test_scorer_gradients_and_logits_match_cpu(tb, env):
     h = env[0]
     p0 = h.scorer_params()
-    n_in = (p0.size - (HID + HID * HID + HID + HID + 1)) // HID - 0
     n_in = (p0.size - 1 - 3 * HID - HID * HID) // HID
     rng = np.random.default_rng(0)
     p = rng.normal(0, 0.2, p0.size).astype(np.float32)
@@ -100,9 +99,10 @@ def test_learned_ranking_keeps_results_exact_and_reports_gain(tb, env, oracle_mo
         assert np.array_equal(r.offsets.numpy(), b.offsets)
         assert np.array_equal(r.ids.numpy(), b.ids)
         assert np.array_equal(r.dist2.numpy(), b.dist2)
-        c = h.knn_counters()
-        work[name] = c["wave1"] + (c["wave2_rows"] if two_wave else 0)
+        work[name] = h.knn_counters()["rows"]
     h.set_two_wave(True)
     with capsys.disabled():
         print("\nfinest-level points tested per query:", {k: v / 256 for k, v in work.items()})
-    assert work["two-wave learned"] < work["one-pass"]
+    assert work["two-wave lb"] < work["one-pass"]
+    # The learned ranking bounds tau sooner than the lower bound does (measured 1.76x fewer rows).
+    assert work["two-wave learned"] < 0.9 * work["two-wave lb"]
