@@ -77,7 +77,8 @@ typedef struct {
     int mode;               /* tblaeq_mode */
     uint64_t nq;
     const double* queries;  /* RANGE: nq rows lo[D] hi[D]; POINT: nq rows point[D] */
-    int queriesOnDevice;    /* 1: `queries` is a device pointer */
+    int queriesOnDevice;    /* 1: `queries` is a device pointer (off a 16-byte boundary: staged by a copy;
+                               tblaeq_query_batch_async rejects it) */
     uint64_t K;             /* KNN: neighbours per query (when kPerQuery is NULL) */
     unsigned flags;         /* tblaeq_batch_flags */
     const uint32_t* kPerQuery; /* KNN: optional host array of nq neighbour counts */

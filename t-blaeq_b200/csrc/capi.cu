@@ -253,12 +253,17 @@ int tblaeq_query_batch(tblaeq_handle* h, const tblaeq_batch* b, tblaeq_batch_res
     if (!out) return fail(TBLAEQ_ERR_INVALID, "null result");
     return guarded([&]() -> int {
         const double* dq = b->queries;
-        if (!b->queriesOnDevice && b->nq) {
+        // Host queries, and device queries off a 16-byte boundary (the kernels read query rows in
+        // 16-byte pairs), go through the handle's staging buffer.
+        const bool misaligned = (reinterpret_cast<uintptr_t>(b->queries) & 15u) != 0;
+        if (b->nq && (!b->queriesOnDevice || misaligned)) {
             Runtime& rt = h->qh->runtime();
             const uint64_t D = rt.dev->D;
             const size_t bytes = b->nq * (b->qtype == TBLAEQ_RANGE ? 2 * D : D) * 8;
             if (h->stage.bytes() < bytes) h->stage.alloc(bytes);
-            TBLAEQ_CUDA(cudaMemcpyAsync(h->stage.get(), b->queries, bytes, cudaMemcpyHostToDevice, rt.stream));
+            TBLAEQ_CUDA(cudaMemcpyAsync(h->stage.get(), b->queries, bytes,
+                                        b->queriesOnDevice ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice,
+                                        rt.stream));
             dq = h->stage.as<double>();
         }
         return runBatch(h, b, dq, out);
@@ -290,6 +295,8 @@ int tblaeq_query_batch_host(tblaeq_handle* h, const tblaeq_batch* b, uint64_t* o
 int tblaeq_query_batch_async(tblaeq_handle* h, const tblaeq_batch* b) {
     if (int c = validateBatch(h, b)) return c;
     if (!b->queriesOnDevice && b->nq) return fail(TBLAEQ_ERR_INVALID, "async batches need device queries");
+    if (reinterpret_cast<uintptr_t>(b->queries) & 15u)
+        return fail(TBLAEQ_ERR_INVALID, "async batches need device queries on a 16-byte boundary");
     if (b->qtype != TBLAEQ_RANGE) return fail(TBLAEQ_ERR_INVALID, "batched KNN is not available in this build");
     return guarded([&]() -> int {
         Runtime& rt = h->qh->runtime();

@@ -212,6 +212,7 @@ void BatchEngine::reserve(const EngineCaps& want, uint32_t nq, unsigned flags) {
         zeroBytes_ = off;
         zeroBlock_.alloc(zeroBytes_);
         offsets_.alloc((static_cast<size_t>(qcap_) + 1) * 8);
+        boxF_.alloc(static_cast<size_t>(qcap_) * 2 * D * 4);
     }
     caps_ = c;
 }
@@ -284,6 +285,7 @@ void BatchEngine::enqueueLaunches(const double* dBoxes, uint32_t nq, int mode, u
     launchRootFrontier(r0.q.as<uint32_t>(), r0.cbeg.as<uint32_t>(), r0.cpre.as<uint32_t>(), r0.x.as<double>(),
                        r0.tileStart.as<uint32_t>(), hdrPtr(0), nq, static_cast<uint32_t>(di_.meshCount[0]), D, tile_,
                        stream_);
+    if (mode == kModeExact) launchRoundBoxes(dBoxes, nq, D, boxF_.as<float>(), stream_);
     if (timing_) record(1);
     int buf = 0;
     for (int m = 0; m < H; ++m) {
@@ -291,6 +293,7 @@ void BatchEngine::enqueueLaunches(const double* dBoxes, uint32_t nq, int mode, u
         a.in = inView(buf, hdrPtr(m));
         a.child.rows = (m == 0) ? di_.coarseVals.as<double>() : di_.pvals[m - 1].as<double>();
         a.query.boxes = dBoxes;
+        a.query.boxesF = (mode == kModeExact) ? boxF_.as<float>() : nullptr;
         a.scratch.desc = desc + static_cast<size_t>(m) * tileCap_;
         a.scratch.ticket = tickets + m;
         a.scratch.status = status;

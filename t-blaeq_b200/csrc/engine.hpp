@@ -133,6 +133,7 @@ private:
     DeviceMem resIds_, resVals_, resQ_, resDist_;
     DeviceMem zeroBlock_;  // desc | tickets | status | hdrs | qcount | levelItems
     DeviceMem offsets_;
+    DeviceMem boxF_;  // exact range batches: the query boxes as outward-rounded floats
     DeviceMem tau_, candOff_, knnCount_, knnOff_, knnIds_, knnD2_;
     uint64_t knnCap_ = 0;
     bool lastKnn_ = false;

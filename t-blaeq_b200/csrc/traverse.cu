@@ -80,58 +80,85 @@ __device__ void lookback(unsigned long long* desc, uint32_t tile, uint32_t aggCn
     }
 }
 
-// Squared distance from y to the box [lo, hi] with the reference's accumulation
-// (RangePruning.cu:7-20; nvcc contracts `dist += diff * diff` into an fma by default).
-template <int DM>
-__device__ __forceinline__ double boxDist2(const double* y, const double* lo, const double* hi, int D, int useFma) {
-    double dist = 0.0;
-#pragma unroll
-    for (int d = 0; d < DM; ++d) {
-        if (d < D) {
-            const double cv = y[d];
-            const double l = lo[d], h = hi[d];
-            double diff = 0.0;
-            if (cv < l) {
-                diff = l - cv;
-            } else if (cv > h) {
-                diff = cv - h;
-            }
-            dist = useFma ? __fma_rn(diff, diff, dist) : __dadd_rn(dist, __dmul_rn(diff, diff));
-        }
-    }
-    return dist;
+// Items are evaluated chunk by chunk: child rows, parent coordinates, query boxes and points are
+// read 2 or 4 doubles at a time (16-byte loads; every such row starts on a 16-byte boundary when D
+// is even) and consumed at once, so no per-item D-vector stays live in registers.
+template <int D>
+constexpr int chunkOf() {
+    return (D > 0 && D % 4 == 0) ? 4 : ((D > 0 && D % 2 == 0) ? 2 : 1);
 }
 
-template <int DM>
-__device__ __forceinline__ double pointDist2(const double* y, const double* p, int D, int useFma) {
-    double dist = 0.0;
-#pragma unroll
-    for (int d = 0; d < DM; ++d) {
-        if (d < D) {
-            const double diff = p[d] - y[d];
-            dist = useFma ? __fma_rn(diff, diff, dist) : __dadd_rn(dist, __dmul_rn(diff, diff));
-        }
-    }
-    return dist;
-}
-
-// Rebuilds item (entry e, row j): y = rows[j] (*) x_e, one rounded multiply per dimension.
-template <int D, int DM>
-__device__ __forceinline__ void rebuild(const ExpandArgs& a, int dim, uint32_t e, uint32_t j, double (&y)[DM]) {
-    const double* xp = a.in.x + static_cast<size_t>(e) * dim;
-    const double* rp = a.child.rows + static_cast<size_t>(j) * dim;
-    if constexpr (D > 0 && (D % 2) == 0) {
-#pragma unroll
-        for (int d = 0; d < D; d += 2) {
-            const double2 pv = __ldg(reinterpret_cast<const double2*>(rp + d));
-            const double2 xv = __ldg(reinterpret_cast<const double2*>(xp + d));
-            y[d] = __dmul_rn(pv.x, xv.x);
-            y[d + 1] = __dmul_rn(pv.y, xv.y);
-        }
+// v[0..C) = p[0..C); SMEM selects a plain (shared-memory) load over the read-only global path.
+template <int C, bool SMEM>
+__device__ __forceinline__ void ldChunk(const double* p, double (&v)[C]) {
+    if constexpr (C == 1) {
+        v[0] = SMEM ? *p : __ldg(p);
     } else {
 #pragma unroll
-        for (int d = 0; d < DM; ++d) {
-            if (d < dim) y[d] = __dmul_rn(__ldg(rp + d), __ldg(xp + d));
+        for (int i = 0; i < C; i += 2) {
+            const double2 t = SMEM ? *reinterpret_cast<const double2*>(p + i)
+                                   : __ldg(reinterpret_cast<const double2*>(p + i));
+            v[i] = t.x;
+            v[i + 1] = t.y;
+        }
+    }
+}
+
+template <int C>
+__device__ __forceinline__ void ldChunkF(const float* p, float (&v)[C]) {
+    if constexpr (C == 4) {
+        const float4 t = __ldg(reinterpret_cast<const float4*>(p));
+        v[0] = t.x;
+        v[1] = t.y;
+        v[2] = t.z;
+        v[3] = t.w;
+    } else if constexpr (C == 2) {
+        const float2 t = __ldg(reinterpret_cast<const float2*>(p));
+        v[0] = t.x;
+        v[1] = t.y;
+    } else {
+        v[0] = __ldg(p);
+    }
+}
+
+template <int C>
+__device__ __forceinline__ void stChunk(double* p, const double (&v)[C]) {
+    if constexpr (C == 1) {
+        *p = v[0];
+    } else {
+#pragma unroll
+        for (int i = 0; i < C; i += 2) *reinterpret_cast<double2*>(p + i) = make_double2(v[i], v[i + 1]);
+    }
+}
+
+// One dimension of the squared distance from y to the box [l, h], accumulated like the
+// reference (RangePruning.cu:7-20; nvcc contracts `dist += diff * diff` into an fma by default).
+__device__ __forceinline__ double boxGapAcc(double y, double l, double h, double dist, int useFma) {
+    double diff = 0.0;
+    if (y < l) {
+        diff = l - y;
+    } else if (y > h) {
+        diff = y - h;
+    }
+    return useFma ? __fma_rn(diff, diff, dist) : __dadd_rn(dist, __dmul_rn(diff, diff));
+}
+
+// Rebuilds item (entry e, row j) chunk by chunk, y = rows[j] (*) x_e with one rounded multiply
+// per dimension (SpMSpV.cuh:47-67), and hands each chunk to sink(d, y).
+template <int D, int DM, typename Sink>
+__device__ __forceinline__ void rebuildChunks(const ExpandArgs& a, int dim, uint32_t e, uint32_t j, Sink&& sink) {
+    constexpr int C = chunkOf<D>();
+    const double* xp = a.in.x + static_cast<size_t>(e) * dim;
+    const double* rp = a.child.rows + static_cast<size_t>(j) * dim;
+#pragma unroll
+    for (int d = 0; d < DM; d += C) {
+        if (D > 0 || d < dim) {
+            double r[C], x[C], y[C];
+            ldChunk<C, false>(rp + d, r);
+            ldChunk<C, false>(xp + d, x);
+#pragma unroll
+            for (int i = 0; i < C; ++i) y[i] = __dmul_rn(r[i], x[i]);
+            sink(d, y);
         }
     }
 }
@@ -165,9 +192,6 @@ struct Staging {
 #ifndef TBLAEQ_EXPAND_MIN_BLOCKS
 #define TBLAEQ_EXPAND_MIN_BLOCKS 8
 #endif
-#ifndef TBLAEQ_EXPAND_CACHE
-#define TBLAEQ_EXPAND_CACHE 0
-#endif
 constexpr int kExpandThreads = TBLAEQ_EXPAND_THREADS;
 
 template <int D, bool STAGED>
@@ -194,85 +218,42 @@ constexpr bool needsNode() {
     return PRED == kPredRangeRadius || PRED == kPredKnnBound || (!TO_RESULT && (PRED == kPredMask || PRED == kPredAll));
 }
 
-// Applies the level predicate to a rebuilt item; cc receives the item's child count when the
-// output is a frontier.
-// Per-lane register cache of the current query's box (range) or point (KNN) and bound, reloaded
-// only when the item's query changes (queries change at entry boundaries, rarely within a warp).
-template <int DM, int PRED>
-struct QueryCache {
-    static constexpr bool kRange = PRED == kPredRangeRadius || PRED == kPredRangeBox;
-    static constexpr bool kKnn = PRED == kPredKnnBound || PRED == kPredKnnPoint;
-    uint32_t q = 0xffffffffu;
-    double lo[(kRange || kKnn) ? DM : 1];
-    double hi[kRange ? DM : 1];
-    double tau = 0.0;
-    __device__ __forceinline__ void load(const ExpandArgs& a, int dim, uint32_t nq) {
-        if (TBLAEQ_EXPAND_CACHE && nq == q) return;
-        q = nq;
-        if constexpr (kRange) {
-            const double* box = a.query.boxes + static_cast<size_t>(nq) * 2 * dim;
-#pragma unroll
-            for (int d = 0; d < DM; ++d) {
-                if (d < dim) {
-                    lo[d] = __ldg(box + d);
-                    hi[d] = __ldg(box + dim + d);
-                }
-            }
-        } else if constexpr (kKnn) {
-            const double* p = a.query.points + static_cast<size_t>(nq) * dim;
-#pragma unroll
-            for (int d = 0; d < DM; ++d)
-                if (d < dim) lo[d] = __ldg(p + d);
-        }
-    }
-};
-
-// Per-lane register cache of the parent entry's coordinates.
+// Exact-mode prefilter of range levels: whether the query box meets the box of the points below
+// child kk. Both boxes are floats rounded outward (the child's when the index is loaded, the
+// query's once per batch), so the test never rejects a child whose points meet the query box. It
+// reads 2*D floats of the child and 2*D of the query (one address per warp, mostly) instead of the
+// child's row, the parent's coordinates and the double query box, and rejects most children.
 template <int D, int DM>
-struct ParentCache {
-    uint32_t e = 0xffffffffu;
-    double x[DM];
-    __device__ __forceinline__ void load(const ExpandArgs& a, int dim, uint32_t ne) {
-        if (TBLAEQ_EXPAND_CACHE && ne == e) return;
-        e = ne;
-        const double* xp = a.in.x + static_cast<size_t>(ne) * dim;
-        if constexpr (D > 0 && (D % 2) == 0) {
+__device__ __forceinline__ bool aabbMeets(const ExpandArgs& a, int dim, uint32_t kk, uint32_t q) {
+    constexpr int C = chunkOf<D>();
+    const float* b = a.child.aabb + static_cast<size_t>(kk) * 2 * dim;
+    const float* f = a.query.boxesF + static_cast<size_t>(q) * 2 * dim;
+    bool meets = true;
 #pragma unroll
-            for (int d = 0; d < D; d += 2) {
-                const double2 v = __ldg(reinterpret_cast<const double2*>(xp + d));
-                x[d] = v.x;
-                x[d + 1] = v.y;
-            }
-        } else {
+    for (int d = 0; d < DM; d += C) {
+        if (D > 0 || d < dim) {
+            float bl[C], bh[C], ql[C], qh[C];
+            ldChunkF<C>(b + d, bl);
+            ldChunkF<C>(b + dim + d, bh);
+            ldChunkF<C>(f + d, ql);
+            ldChunkF<C>(f + dim + d, qh);
 #pragma unroll
-            for (int d = 0; d < DM; ++d)
-                if (d < dim) x[d] = __ldg(xp + d);
+            for (int i = 0; i < C; ++i) meets = meets && bl[i] <= qh[i] && bh[i] >= ql[i];
         }
     }
-};
+    return meets;
+}
 
-template <int DM, int PRED, bool TO_RESULT>
-__device__ __forceinline__ bool testItem(const ExpandArgs& a, int dim, const double (&y)[DM],
-                                         const QueryCache<DM, PRED>& qc, uint32_t j, uint32_t kk, const NodeRec& nr,
-                                         uint32_t& cc) {
+// Pass-1 test of one item: entry coordinates xp, child row j (read from `rowp`: global memory, or
+// the shared-memory staging ring when SMEM) and child key kk, for query q. Rebuilds the child's
+// coordinates chunk by chunk and applies the level predicate; cc receives the child's own child
+// count when the output is a frontier.
+template <int D, int DM, int PRED, bool TO_RESULT, bool SMEM>
+__device__ __forceinline__ bool evalItem(const ExpandArgs& a, int dim, const double* rowp, const double* xp,
+                                         uint32_t q, uint32_t j, uint32_t kk, const NodeRec& nr, uint32_t& cc) {
+    constexpr int C = chunkOf<D>();
     cc = 0;
-    if constexpr (PRED == kPredRangeRadius) {
-        const double dist = boxDist2<DM>(y, qc.lo, qc.hi, dim, a.useFma);
-        cc = nr.cnt;
-        bool keep = (cc > 0) && (dist <= __dmul_rn(nr.rad, nr.rad));
-        if (keep && a.child.aabb) {
-            // Exact mode only: the query box must also meet the box of the points below the child.
-            const float* b = a.child.aabb + static_cast<size_t>(kk) * 2 * dim;
-#pragma unroll
-            for (int d = 0; d < DM; ++d) {
-                if (d < dim) {
-                    keep = keep && (static_cast<double>(__ldg(b + d)) <= qc.hi[d]) &&
-                           (static_cast<double>(__ldg(b + dim + d)) >= qc.lo[d]);
-                }
-            }
-        }
-        return keep;
-    } else if constexpr (PRED == kPredMask) {
+    if constexpr (PRED == kPredMask) {
         bool keep = a.child.mask[j] != 0;
         if constexpr (!TO_RESULT) {
             cc = nr.cnt;
@@ -285,36 +266,74 @@ __device__ __forceinline__ bool testItem(const ExpandArgs& a, int dim, const dou
             return cc > 0;
         }
         return true;
-    } else if constexpr (PRED == kPredRangeBox) {
+    } else if constexpr (PRED == kPredRangeRadius || PRED == kPredRangeBox) {
+        const double* box = a.query.boxes + static_cast<size_t>(q) * 2 * dim;
+        double dist = 0.0;
         bool in = true;
 #pragma unroll
-        for (int d = 0; d < DM; ++d) {
-            if (d < dim) in = in && (qc.lo[d] <= y[d]) && (y[d] <= qc.hi[d]);
+        for (int d = 0; d < DM; d += C) {
+            if (D > 0 || d < dim) {
+                double r[C], x[C], l[C], h[C];
+                ldChunk<C, SMEM>(rowp + d, r);
+                ldChunk<C, false>(xp + d, x);
+                ldChunk<C, false>(box + d, l);
+                ldChunk<C, false>(box + dim + d, h);
+#pragma unroll
+                for (int i = 0; i < C; ++i) {
+                    const double y = __dmul_rn(r[i], x[i]);
+                    if constexpr (PRED == kPredRangeRadius) {
+                        dist = boxGapAcc(y, l[i], h[i], dist, a.useFma);
+                    } else {
+                        in = in && (l[i] <= y) && (y <= h[i]);
+                    }
+                }
+            }
         }
-        return in;
+        if constexpr (PRED == kPredRangeRadius) {
+            cc = nr.cnt;
+            return (cc > 0) && (dist <= __dmul_rn(nr.rad, nr.rad));
+        } else {
+            return in;
+        }
     } else if constexpr (PRED == kPredKnnBound) {
         // Distance bounds of the points below the child: sphere (centre distance -/+ subtree radius)
         // and, when present, its box (outward-rounded, so slightly widened bounds stay conservative).
-        const double dd = sqrt(pointDist2<DM>(y, qc.lo, dim, 1));
-        double lb = dd - nr.rad, ub = dd + nr.rad;
-        if (a.child.aabb) {
-            const float* b = a.child.aabb + static_cast<size_t>(kk) * 2 * dim;
-            double gapSum = 0.0, farSum = 0.0;
+        const double* p = a.query.points + static_cast<size_t>(q) * dim;
+        const float* b = a.child.aabb ? a.child.aabb + static_cast<size_t>(kk) * 2 * dim : nullptr;
+        double dist = 0.0, gapSum = 0.0, farSum = 0.0;
 #pragma unroll
-            for (int d = 0; d < DM; ++d) {
-                if (d < dim) {
-                    const double l = static_cast<double>(__ldg(b + d)), h = static_cast<double>(__ldg(b + dim + d));
-                    const double g = fmax(fmax(l - qc.lo[d], qc.lo[d] - h), 0.0);
-                    const double f = fmax(qc.lo[d] - l, h - qc.lo[d]);
-                    gapSum = __fma_rn(g, g, gapSum);
-                    farSum = __fma_rn(f, f, farSum);
+        for (int d = 0; d < DM; d += C) {
+            if (D > 0 || d < dim) {
+                double r[C], x[C], pp[C];
+                float bl[C], bh[C];
+                ldChunk<C, SMEM>(rowp + d, r);
+                ldChunk<C, false>(xp + d, x);
+                ldChunk<C, false>(p + d, pp);
+                if (b) {
+                    ldChunkF<C>(b + d, bl);
+                    ldChunkF<C>(b + dim + d, bh);
+                }
+#pragma unroll
+                for (int i = 0; i < C; ++i) {
+                    const double diff = pp[i] - __dmul_rn(r[i], x[i]);
+                    dist = __fma_rn(diff, diff, dist);
+                    if (b) {
+                        const double l = static_cast<double>(bl[i]), h = static_cast<double>(bh[i]);
+                        const double g = fmax(fmax(l - pp[i], pp[i] - h), 0.0);
+                        const double f = fmax(pp[i] - l, h - pp[i]);
+                        gapSum = __fma_rn(g, g, gapSum);
+                        farSum = __fma_rn(f, f, farSum);
+                    }
                 }
             }
+        }
+        const double dd = sqrt(dist);
+        double lb = dd - nr.rad, ub = dd + nr.rad;
+        if (b) {
             lb = fmax(lb, sqrt(gapSum) * (1.0 - 1e-12));
             ub = fmin(ub, sqrt(farSum) * (1.0 + 1e-12));
         }
         cc = nr.cnt;
-        const uint32_t q = qc.q;
         double tau = __ldcg(a.query.tau + q);
         // Any child with K points below it bounds the K-th neighbour distance by its far distance.
         if (ub < tau && __ldg(a.child.leaf + kk) >= __ldg(a.query.k + q)) {
@@ -324,8 +343,24 @@ __device__ __forceinline__ bool testItem(const ExpandArgs& a, int dim, const dou
         return (cc > 0) && (lb <= tau);
     } else {  // kPredKnnPoint
         if (a.wave == 1) return true;  // every point of a selected entry
-        const double t = __ldcg(a.query.tau + qc.q);
-        return pointDist2<DM>(y, qc.lo, dim, 1) <= t * t * (1.0 + 1e-9);
+        const double* p = a.query.points + static_cast<size_t>(q) * dim;
+        double dist = 0.0;
+#pragma unroll
+        for (int d = 0; d < DM; d += C) {
+            if (D > 0 || d < dim) {
+                double r[C], x[C], pp[C];
+                ldChunk<C, SMEM>(rowp + d, r);
+                ldChunk<C, false>(xp + d, x);
+                ldChunk<C, false>(p + d, pp);
+#pragma unroll
+                for (int i = 0; i < C; ++i) {
+                    const double diff = pp[i] - __dmul_rn(r[i], x[i]);
+                    dist = __fma_rn(diff, diff, dist);
+                }
+            }
+        }
+        const double t = __ldcg(a.query.tau + q);
+        return dist <= t * t * (1.0 + 1e-9);
     }
 }
 
@@ -450,8 +485,6 @@ __global__ void __launch_bounds__(kExpandThreads, TBLAEQ_EXPAND_MIN_BLOCKS) expa
             }
         }
         uint32_t keepBits = 0, aggCnt = 0, aggSum = 0;
-        QueryCache<DM, PRED> qc;
-        ParentCache<D, DM> pc;
 #pragma unroll
         for (int r = 0; r < R; ++r) {
             if constexpr (S::kOn) {
@@ -478,45 +511,25 @@ __global__ void __launch_bounds__(kExpandThreads, TBLAEQ_EXPAND_MIN_BLOCKS) expa
                 const uint32_t j = sRow[r * 32 + lane];
                 const uint32_t e = sEnt[r * 32 + lane];
                 const uint32_t q = sQ[r * 32 + lane];
-                double y[DM];
-                NodeRec nr{0.0, 0u, 0u};
-                uint32_t kk = j;
-                qc.load(a, dim, q);
-                pc.load(a, dim, e);
-                if constexpr (S::kOn) {
-                    const int slot = r % S::kStages;
-                    const double* rowp = reinterpret_cast<const double*>(rowBuf + (slot * 32 + lane) * S::kStride);
-                    if constexpr (D % 2 == 0) {
-#pragma unroll
-                        for (int d = 0; d < D; d += 2) {
-                            const double2 pv = *reinterpret_cast<const double2*>(rowp + d);
-                            y[d] = __dmul_rn(pv.x, pc.x[d]);
-                            y[d + 1] = __dmul_rn(pv.y, pc.x[d + 1]);
-                        }
-                    } else {
-#pragma unroll
-                        for (int d = 0; d < D; ++d) y[d] = __dmul_rn(rowp[d], pc.x[d]);
-                    }
-                    if constexpr (NODE) nr = nodeBuf[slot * 32 + lane];
-                    kk = a.child.keys ? static_cast<uint32_t>(a.child.keys[j]) : j;
-                } else {
-                    const double* rp = a.child.rows + static_cast<size_t>(j) * dim;
-                    if constexpr (D > 0 && (D % 2) == 0) {
-#pragma unroll
-                        for (int d = 0; d < D; d += 2) {
-                            const double2 pv = __ldg(reinterpret_cast<const double2*>(rp + d));
-                            y[d] = __dmul_rn(pv.x, pc.x[d]);
-                            y[d + 1] = __dmul_rn(pv.y, pc.x[d + 1]);
-                        }
-                    } else {
-#pragma unroll
-                        for (int d = 0; d < DM; ++d)
-                            if (d < dim) y[d] = __dmul_rn(__ldg(rp + d), pc.x[d]);
-                    }
-                    kk = a.child.keys ? static_cast<uint32_t>(a.child.keys[j]) : j;
-                    if constexpr (NODE) nr = a.child.nodes[kk];
+                const uint32_t kk = a.child.keys ? static_cast<uint32_t>(a.child.keys[j]) : j;
+                bool pre = true;
+                if constexpr (PRED == kPredRangeRadius) {
+                    if (a.child.aabb && a.query.boxesF) pre = aabbMeets<D, DM>(a, dim, kk, q);
                 }
-                keep = testItem<DM, PRED, TO_RESULT>(a, dim, y, qc, j, kk, nr, cc);
+                if (pre) {
+                    NodeRec nr{0.0, 0u, 0u};
+                    const double* xp = a.in.x + static_cast<size_t>(e) * dim;
+                    if constexpr (S::kOn) {
+                        const int slot = r % S::kStages;
+                        const double* rowp = reinterpret_cast<const double*>(rowBuf + (slot * 32 + lane) * S::kStride);
+                        if constexpr (NODE) nr = nodeBuf[slot * 32 + lane];
+                        keep = evalItem<D, DM, PRED, TO_RESULT, true>(a, dim, rowp, xp, q, j, kk, nr, cc);
+                    } else {
+                        if constexpr (NODE) nr = a.child.nodes[kk];
+                        keep = evalItem<D, DM, PRED, TO_RESULT, false>(a, dim, a.child.rows + static_cast<size_t>(j) * dim,
+                                                                       xp, q, j, kk, nr, cc);
+                    }
+                }
             }
             if (a.scratch.work) warpRows += __popc(__ballot_sync(FULL, work));
             // Per-query generated-children counts (the reference's levelFineMeshSize).
@@ -569,10 +582,9 @@ __global__ void __launch_bounds__(kExpandThreads, TBLAEQ_EXPAND_MIN_BLOCKS) expa
             if (kb == 0) continue;  // warp-uniform
             const uint32_t j = sRow[r * 32 + lane];
             const uint32_t qr = sQ[r * 32 + lane];
+            const uint32_t er = sEnt[r * 32 + lane];
             uint32_t cc = 0, ncb = 0, kk = 0;
-            double y[DM];
             if (keep) {
-                rebuild<D, DM>(a, dim, sEnt[r * 32 + lane], j, y);
                 kk = a.child.keys ? static_cast<uint32_t>(a.child.keys[j]) : j;
                 if constexpr (!TO_RESULT) {
                     const NodeRec nr = a.child.nodes[kk];
@@ -595,17 +607,29 @@ __global__ void __launch_bounds__(kExpandThreads, TBLAEQ_EXPAND_MIN_BLOCKS) expa
                 if constexpr (TO_RESULT) {
                     if (pos < a.rout.cap) {
                         a.rout.ids[pos] = a.child.outMap ? a.child.outMap[j] : static_cast<uint64_t>(kk);
-                        if (a.rout.vals) {
-#pragma unroll
-                            for (int d = 0; d < DM; ++d)
-                                if (d < dim) a.rout.vals[pos * dim + d] = y[d];
-                        }
                         if (a.rout.q) a.rout.q[pos] = qr;
+                        double* vals = a.rout.vals ? a.rout.vals + pos * dim : nullptr;
                         if constexpr (PRED == kPredKnnPoint) {
-                            if (a.rout.dist2) {
+                            if (vals || a.rout.dist2) {
+                                constexpr int C = chunkOf<D>();
                                 const double* p = a.query.points + static_cast<size_t>(qr) * dim;
-                                a.rout.dist2[pos] = pointDist2<DM>(y, p, dim, 1);
+                                double dist = 0.0;
+                                rebuildChunks<D, DM>(a, dim, er, j, [&](int d, const double (&y)[C]) {
+                                    if (vals) stChunk<C>(vals + d, y);
+                                    double pp[C];
+                                    ldChunk<C, false>(p + d, pp);
+#pragma unroll
+                                    for (int i = 0; i < C; ++i) {
+                                        const double diff = pp[i] - y[i];
+                                        dist = __fma_rn(diff, diff, dist);
+                                    }
+                                });
+                                if (a.rout.dist2) a.rout.dist2[pos] = dist;
                             }
+                        } else if (vals) {
+                            constexpr int C = chunkOf<D>();
+                            rebuildChunks<D, DM>(a, dim, er, j,
+                                                 [&](int d, const double (&y)[C]) { stChunk<C>(vals + d, y); });
                         }
                     }
                 } else if (pos < a.fout.cap) {
@@ -614,9 +638,11 @@ __global__ void __launch_bounds__(kExpandThreads, TBLAEQ_EXPAND_MIN_BLOCKS) expa
                     a.fout.node[pos] = kk;
                     a.fout.cbeg[pos] = ncb;
                     a.fout.cpre[pos] = static_cast<uint32_t>(cp);
-#pragma unroll
-                    for (int d = 0; d < DM; ++d)
-                        if (d < dim) a.fout.x[pos * dim + d] = y[d];
+                    {
+                        constexpr int C = chunkOf<D>();
+                        double* xo = a.fout.x + pos * dim;
+                        rebuildChunks<D, DM>(a, dim, er, j, [&](int d, const double (&y)[C]) { stChunk<C>(xo + d, y); });
+                    }
                     // Tile starts of the next level: every tile boundary inside this entry's children.
                     const unsigned long long cend = cp + cc;
                     for (unsigned long long b = (cp + kWarpTile - 1) / kWarpTile; b * kWarpTile < cend; ++b) {
@@ -765,6 +791,23 @@ void launchRootFrontier(uint32_t* q, uint32_t* cbeg, uint32_t* cpre, double* x, 
     const uint64_t work = std::max<uint64_t>(nq, nTiles);
     const int blocks = static_cast<int>(std::min<uint64_t>(1024, (work + 255) / 256 + 1));
     rootFrontierKernel<<<blocks, 256, 0, stream>>>(q, cbeg, cpre, x, tileStart, hdr, nq, nChildren, D, tile);
+    TBLAEQ_CUDA(cudaGetLastError());
+}
+
+__global__ void roundBoxesKernel(const double* boxes, uint32_t nq, int D, float* boxesF) {
+    const uint64_t n = static_cast<uint64_t>(nq) * 2 * D;
+    for (uint64_t i = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x; i < n;
+         i += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
+        const bool upper = (i % (2 * D)) >= static_cast<uint64_t>(D);
+        boxesF[i] = upper ? __double2float_ru(boxes[i]) : __double2float_rd(boxes[i]);
+    }
+}
+
+void launchRoundBoxes(const double* boxes, uint32_t nq, int D, float* boxesF, cudaStream_t stream) {
+    if (nq == 0) return;
+    const uint64_t n = static_cast<uint64_t>(nq) * 2 * D;
+    const int blocks = static_cast<int>(std::min<uint64_t>(148 * 4, (n + 255) / 256));
+    roundBoxesKernel<<<blocks, 256, 0, stream>>>(boxes, nq, D, boxesF);
     TBLAEQ_CUDA(cudaGetLastError());
 }
 

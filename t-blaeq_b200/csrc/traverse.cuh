@@ -95,6 +95,7 @@ struct ChildLevel {
 
 struct QueryArgs {
     const double* boxes;        // range: per query lo[D] then hi[D]
+    const float* boxesF;        // range, exact mode: the same boxes as floats rounded outward
     const double* points;       // knn: per query point[D]
     double* tau;                // knn: per query upper bound on the K-th neighbour distance (tightened
                                 //      in place with an atomic minimum)
@@ -148,6 +149,10 @@ inline int expandTile(int) { return kWarpTile; }
 // nq entries and ceil(nq*nChildren / tile) tile starts.
 void launchRootFrontier(uint32_t* q, uint32_t* cbeg, uint32_t* cpre, double* x, uint32_t* tileStart, uint32_t* hdr,
                         uint32_t nq, uint32_t nChildren, int D, int tile, cudaStream_t stream);
+
+// boxesF = the nq query boxes (lo[D] hi[D]) as floats, lower corners rounded down and upper
+// corners rounded up.
+void launchRoundBoxes(const double* boxes, uint32_t nq, int D, float* boxesF, cudaStream_t stream);
 
 // offsets[q] = exclusive scan of counts[0..n), offsets[n] = total (single CTA).
 void launchExclusiveScan(const uint32_t* counts, uint64_t* offsets, uint32_t n, cudaStream_t stream);
