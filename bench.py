@@ -118,6 +118,19 @@ def oracle_index_from_handler(oracle, h):
                               pvals, radius, maps, cids, cvals)
 
 
+def profiled_traffic(cfg_name, nq):
+    """DRAM bytes (read + write) of one finest-level expand launch of this exact workload, from the
+    committed ncu summary (one capture of the same command; ncu is never run by the benchmark)."""
+    if cfg_name != "batched" or nq != 4096:
+        return None
+    path = os.path.join(REPO, "profiles", "expand_batched_range_n10m_d8.md")
+    if not os.path.exists(path):
+        return None
+    import re
+    m = re.search(r"^traffic_bytes_per_launch_finest:\s*(\d+)", open(path).read(), re.M)
+    return int(m.group(1)) if m else None
+
+
 def cpu_port_qps(oracle, oidx, sub, Q, budget_s=20.0, min_q=32):
     """Time the CPU port of the exact traversal on all host cores over a bounded sample."""
     threads = os.cpu_count() or 1
@@ -203,6 +216,7 @@ def main():
     if world > 1:
         dist.barrier()
     torch.cuda.synchronize()
+    torch.cuda.nvtx.range_push("timed")  # profilers select the timed steps by this range
     with ClockSampler(local) as clk:
         for _ in range(args.steps):
             flush.zero_()
@@ -213,6 +227,7 @@ def main():
             step_ms.append(sum(st))
             final_ms.append(st[-2])
     torch.cuda.synchronize()
+    torch.cuda.nvtx.range_pop()
     if world > 1:
         dist.barrier()
     total_ms = sum(step_ms)
@@ -306,7 +321,8 @@ def main():
         "config": config,
         "e2e": {"value": e2e_value, "unit": "queries/s", "h2d_bytes_per_step": args.nq * 2 * D * 8,
                 "d2h_bytes_per_step": (args.nq + 1) * 8 + int(tot.value) * 8},
-        "gpu_launches": args.steps * (H + 2),
+        # per step: root frontier, query-box rounding, one expand per level, offsets scan
+        "gpu_launches": args.steps * (H + 3),
         "latency_ms": {"batch_p50": lat_ms[len(lat_ms) // 2], "batch_p99": lat_ms[min(len(lat_ms) - 1,
                                                                                      int(len(lat_ms) * 0.99))],
                        "plain_query_p50": pl[len(pl) // 2], "plain_query_p99": pl[min(len(pl) - 1,
@@ -318,7 +334,8 @@ def main():
         "level_entries": entries,
         "level_children": items,
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                     "traffic": None, "kernel": "expandKernel<8, RangeBox, result> (finest level)",
+                     "traffic": profiled_traffic(cfg_name, args.nq),
+                     "kernel": "expandKernel<8, RangeBox, result> (finest level)",
                      "peak_kind": f"{peak_kind} hbm_gbs", "algorithmic_bytes_per_launch": alg_bytes,
                      "launch_ms": final_mean_s * 1e3},
         "clocks": clk.summary(),
