@@ -178,7 +178,7 @@ struct Staging {
     static constexpr int kRounds = kWarpTile / 32;
     static constexpr int kRowBytes = kOn ? kStages * 32 * kStride : 0;
     static constexpr int kNodeBytes = kOn ? kStages * 32 * 16 : 0;
-    static constexpr int kCacheBytes = 3 * kRounds * 32 * 4;
+    static constexpr int kCacheBytes = kRounds * 32 * (4 + 2);  // per item: row (u32), window slot (u16)
     static constexpr int kWindow = kWarpTile + 1;  // most entries a tile can overlap
     static constexpr int kWindowBytes = 3 * kWindow * 4 + 4;
     static constexpr int kWarpBytes = kRowBytes + kNodeBytes + kCacheBytes + ((kWindowBytes + 15) / 16) * 16;
@@ -190,9 +190,21 @@ struct Staging {
 #define TBLAEQ_EXPAND_THREADS 128
 #endif
 #ifndef TBLAEQ_EXPAND_MIN_BLOCKS
-#define TBLAEQ_EXPAND_MIN_BLOCKS 8
+#define TBLAEQ_EXPAND_MIN_BLOCKS 10
+#endif
+#ifndef TBLAEQ_EXPAND_MIN_BLOCKS_BOUND
+#define TBLAEQ_EXPAND_MIN_BLOCKS_BOUND 8
 #endif
 constexpr int kExpandThreads = TBLAEQ_EXPAND_THREADS;
+
+// Resident CTAs per SM the register allocation is sized for (128 threads: 10 CTAs = 51 registers,
+// 8 CTAs = 64). Levels that prune inner nodes (range radius + box, KNN sphere + box bounds) keep
+// more state live and get the larger budget; point levels and plain expansions the smaller one.
+template <int PRED>
+constexpr int expandMinBlocks() {
+    return (PRED == kPredKnnBound || PRED == kPredRangeRadius) ? TBLAEQ_EXPAND_MIN_BLOCKS_BOUND
+                                                               : TBLAEQ_EXPAND_MIN_BLOCKS;
+}
 
 template <int D, bool STAGED>
 constexpr size_t expandSmemBytes() {
@@ -211,6 +223,45 @@ __device__ __forceinline__ void cpAsyncCommit() { asm volatile("cp.async.commit_
 template <int N>
 __device__ __forceinline__ void cpAsyncWait() {
     asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
+}
+
+// Bulk L2 prefetch of a contiguous byte range (16-byte aligned start, size a multiple of 16).
+__device__ __forceinline__ void bulkPrefetchL2(const void* p, uint32_t bytes) {
+    asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;\n" ::"l"(p), "r"(bytes) : "memory");
+}
+
+// Whether a level's kernel prefetches its tile's rows: predicates that read every child row, for
+// row sizes that keep every row on a 16-byte boundary.
+template <int D, int PRED>
+constexpr bool prefetchesRows() {
+    return D > 0 && (8 * D) % 16 == 0 &&
+           (PRED == kPredRangeBox || PRED == kPredKnnPoint || PRED == kPredKnnBound || PRED == kPredRangeRadius);
+}
+
+// Prefetches into L2 the child rows of tile `t`: one contiguous run per frontier entry that the
+// tile overlaps, one bulk prefetch per run (lanes take entries in turn). Levels that decide most
+// children without loading their rows (the box prefilter, two-wave KNN) prefetch nothing.
+template <int D, int PRED>
+__device__ __forceinline__ void prefetchTileRows(const ExpandArgs& a, uint32_t t, uint32_t nTiles, uint32_t entries,
+                                                 uint32_t total, int lane) {
+    if (t >= nTiles) return;
+    if (PRED == kPredRangeRadius && a.child.aabb) return;
+    if (PRED == kPredKnnPoint && a.wave != 0) return;
+    const uint32_t t0 = t * kWarpTile;
+    const uint32_t itemEnd = min(t0 + static_cast<uint32_t>(kWarpTile), total);
+    const uint32_t eLo = a.in.tileStart[t];
+    uint32_t eHi = (t + 1 < nTiles) ? a.in.tileStart[t + 1] : entries - 1;
+    if (eHi >= entries) eHi = entries - 1;
+    for (uint32_t e = eLo + lane; e <= eHi; e += 32) {
+        const uint32_t cpi = a.in.cpre[e];
+        const uint32_t from = max(t0, cpi);
+        const uint32_t to = (e + 1 < entries) ? min(itemEnd, a.in.cpre[e + 1]) : itemEnd;
+        if (to > from) {
+            const unsigned char* src = reinterpret_cast<const unsigned char*>(a.child.rows) +
+                                       (static_cast<size_t>(a.in.cbeg[e]) + (from - cpi)) * (8 * D);
+            bulkPrefetchL2(src, (to - from) * (8u * D));
+        }
+    }
 }
 
 template <int PRED, bool TO_RESULT>
@@ -365,7 +416,7 @@ __device__ __forceinline__ bool evalItem(const ExpandArgs& a, int dim, const dou
 }
 
 template <int D, int PRED, bool TO_RESULT, bool STAGED>
-__global__ void __launch_bounds__(kExpandThreads, TBLAEQ_EXPAND_MIN_BLOCKS) expandKernel(ExpandArgs a) {
+__global__ void __launch_bounds__(kExpandThreads, expandMinBlocks<PRED>()) expandKernel(ExpandArgs a) {
     using S = Staging<D, STAGED>;
     constexpr int R = S::kRounds;
     constexpr int DM = (D > 0) ? D : 32;
@@ -381,9 +432,8 @@ __global__ void __launch_bounds__(kExpandThreads, TBLAEQ_EXPAND_MIN_BLOCKS) expa
     unsigned char* rowBuf = warpSmem;                                    // [kStages][32][kStride]
     NodeRec* nodeBuf = reinterpret_cast<NodeRec*>(warpSmem + S::kRowBytes);  // [kStages][32]
     uint32_t* sRow = reinterpret_cast<uint32_t*>(warpSmem + S::kRowBytes + S::kNodeBytes);  // [R][32]
-    uint32_t* sEnt = sRow + R * 32;
-    uint32_t* sQ = sEnt + R * 32;
-    uint32_t* wCp = sQ + R * 32;  // window of the tile's entries: prefix, first child, query
+    uint16_t* sWin = reinterpret_cast<uint16_t*>(sRow + R * 32);  // item -> window slot of its entry
+    uint32_t* wCp = reinterpret_cast<uint32_t*>(sWin + R * 32);  // window of the tile's entries: prefix, first child, query
     uint32_t* wCb = wCp + S::kWindow;
     uint32_t* wQ = wCb + S::kWindow;
 
@@ -407,6 +457,9 @@ __global__ void __launch_bounds__(kExpandThreads, TBLAEQ_EXPAND_MIN_BLOCKS) expa
             if (a.scratch.work && lane == 0 && warpRows) atomicAdd(a.scratch.work, warpRows);
             break;
         }
+        // The tile's rows are one contiguous run per entry: the TMA unit brings each run into L2
+        // now (one instruction per run, no registers), ahead of the per-round row loads.
+        if constexpr (prefetchesRows<D, PRED>()) prefetchTileRows<D, PRED>(a, tile, nTiles, entries, total, lane);
         const uint32_t t0 = tile * kWarpTile;
 
         // ---- phase A: stage the tile's entries in shared memory (one round of parallel loads),
@@ -443,8 +496,7 @@ __global__ void __launch_bounds__(kExpandThreads, TBLAEQ_EXPAND_MIN_BLOCKS) expa
             const uint32_t my = cur + base + __popc(starts & lanesLe);
             const uint32_t e = my < W ? my : W - 1;
             sRow[r * 32 + lane] = wCb[e] + (k - wCp[e]);
-            sEnt[r * 32 + lane] = eLo + e;
-            sQ[r * 32 + lane] = wQ[e];
+            sWin[r * 32 + lane] = static_cast<uint16_t>(e);
             validBits |= (valid ? 1u : 0u) << r;
             // The next round's first item (rs + 32) lies in the entry holding this round's last item,
             // or in the next entry when that one starts exactly there.
@@ -456,21 +508,32 @@ __global__ void __launch_bounds__(kExpandThreads, TBLAEQ_EXPAND_MIN_BLOCKS) expa
         // ---- phase B: stream the rows (and node records) through the cp.async ring and test.
         auto issue = [&](int r) {
             if constexpr (S::kOn) {
-                if ((validBits >> r) & 1u) {
-                    const uint32_t j = sRow[r * 32 + lane];
-                    const int slot = r % S::kStages;
-                    const unsigned char* src = reinterpret_cast<const unsigned char*>(a.child.rows) +
-                                               static_cast<size_t>(j) * (8 * D);
-                    unsigned char* dst = rowBuf + (slot * 32 + lane) * S::kStride;
+                // The round's rows move as 32 * kChunks chunk copies spread over the warp so that
+                // consecutive lanes copy consecutive chunks: rows of one entry are consecutive in
+                // the P-tensor, so each copy instruction reads whole sectors (a lane copying its own
+                // row would touch a different sector per lane). Each row still lands in its own
+                // lane's padded slot, and the lane later reads it back whole.
+                const int slot = r % S::kStages;
+                const uint32_t rs = t0 + r * 32;
 #pragma unroll
-                    for (int c = 0; c < S::kChunks; ++c) {
+                for (int i = 0; i < S::kChunks; ++i) {
+                    const uint32_t t = static_cast<uint32_t>(i) * 32u + lane;
+                    const uint32_t it = t / S::kChunks, c = t % S::kChunks;
+                    if (rs + it < total) {
+                        const uint32_t j = sRow[r * 32 + it];
+                        const unsigned char* src = reinterpret_cast<const unsigned char*>(a.child.rows) +
+                                                   static_cast<size_t>(j) * (8 * D) + c * S::kChunk;
+                        unsigned char* dst = rowBuf + (slot * 32 + it) * S::kStride + c * S::kChunk;
                         if constexpr (S::kChunk == 16) {
-                            cpAsync16(dst + 16 * c, src + 16 * c);
+                            cpAsync16(dst, src);
                         } else {
-                            cpAsync8(dst + 8 * c, src + 8 * c);
+                            cpAsync8(dst, src);
                         }
                     }
-                    if constexpr (NODE) {
+                }
+                if constexpr (NODE) {
+                    if ((validBits >> r) & 1u) {
+                        const uint32_t j = sRow[r * 32 + lane];
                         const uint32_t kk = a.child.keys ? static_cast<uint32_t>(a.child.keys[j]) : j;
                         cpAsync16(&nodeBuf[slot * 32 + lane], &a.child.nodes[kk]);
                     }
@@ -478,6 +541,7 @@ __global__ void __launch_bounds__(kExpandThreads, TBLAEQ_EXPAND_MIN_BLOCKS) expa
             }
         };
         if constexpr (S::kOn) {
+            __syncwarp();
 #pragma unroll
             for (int r = 0; r < S::kStages - 1; ++r) {
                 if (r < R) issue(r);
@@ -488,9 +552,13 @@ __global__ void __launch_bounds__(kExpandThreads, TBLAEQ_EXPAND_MIN_BLOCKS) expa
 #pragma unroll
         for (int r = 0; r < R; ++r) {
             if constexpr (S::kOn) {
+                // Lanes copy each other's rows: the slot being refilled must be read out by every
+                // lane first, and a landed round is visible to the warp only after its barrier.
+                __syncwarp();
                 if (r + S::kStages - 1 < R) issue(r + S::kStages - 1);
                 cpAsyncCommit();
                 cpAsyncWait<S::kStages - 1>();
+                __syncwarp();
             }
             if (t0 + r * 32 >= total) continue;  // warp-uniform
             const bool valid = (validBits >> r) & 1u;
@@ -499,18 +567,19 @@ __global__ void __launch_bounds__(kExpandThreads, TBLAEQ_EXPAND_MIN_BLOCKS) expa
             bool work = valid;
             if (PRED == kPredKnnPoint && valid && a.wave != 0) {
                 // Two-wave KNN: decide from the entry alone before touching the child's row.
-                const uint32_t e = sEnt[r * 32 + lane];
+                const uint32_t e = eLo + sWin[r * 32 + lane];
                 const bool sel = __ldg(a.child.entrySel + e) != 0;
                 if (a.wave == 1) {
                     work = sel;
                 } else {
-                    work = !sel && __ldg(a.child.entryLb + e) <= __ldcg(a.query.tau + sQ[r * 32 + lane]);
+                    work = !sel && __ldg(a.child.entryLb + e) <= __ldcg(a.query.tau + wQ[sWin[r * 32 + lane]]);
                 }
             }
             if (work) {
                 const uint32_t j = sRow[r * 32 + lane];
-                const uint32_t e = sEnt[r * 32 + lane];
-                const uint32_t q = sQ[r * 32 + lane];
+                const uint32_t w = sWin[r * 32 + lane];
+                const uint32_t e = eLo + w;
+                const uint32_t q = wQ[w];
                 const uint32_t kk = a.child.keys ? static_cast<uint32_t>(a.child.keys[j]) : j;
                 bool pre = true;
                 if constexpr (PRED == kPredRangeRadius) {
@@ -536,7 +605,7 @@ __global__ void __launch_bounds__(kExpandThreads, TBLAEQ_EXPAND_MIN_BLOCKS) expa
             if (a.scratch.levelItems) {
                 const uint32_t vm = __ballot_sync(FULL, valid);
                 if (valid) {
-                    const uint32_t q = sQ[r * 32 + lane];
+                    const uint32_t q = wQ[sWin[r * 32 + lane]];
                     const uint32_t peers = __match_any_sync(vm, q);
                     if (lane == __ffs(peers) - 1) atomicAdd(&a.scratch.levelItems[q], __popc(peers));
                 }
@@ -581,8 +650,9 @@ __global__ void __launch_bounds__(kExpandThreads, TBLAEQ_EXPAND_MIN_BLOCKS) expa
             const uint32_t kb = __ballot_sync(FULL, keep);
             if (kb == 0) continue;  // warp-uniform
             const uint32_t j = sRow[r * 32 + lane];
-            const uint32_t qr = sQ[r * 32 + lane];
-            const uint32_t er = sEnt[r * 32 + lane];
+            const uint32_t wr = sWin[r * 32 + lane];
+            const uint32_t qr = wQ[wr];
+            const uint32_t er = eLo + wr;
             uint32_t cc = 0, ncb = 0, kk = 0;
             if (keep) {
                 kk = a.child.keys ? static_cast<uint32_t>(a.child.keys[j]) : j;

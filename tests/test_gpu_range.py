@@ -140,21 +140,25 @@ def test_large_results_force_workspace_growth(tb, env, oracle_mod):
     assert np.array_equal(offs, ref.offsets) and np.array_equal(got, ref.ids)
 
 
-@pytest.mark.parametrize("D,ratios", [(2, (16, 8, 4)), (3, (10, 10, 10)), (6, (30, 10, 5)), (8, (100, 50, 20)),
-                                      (16, (50, 20, 10))])
+@pytest.mark.parametrize("D,ratios", [(2, (16, 8, 4)), (3, (10, 10, 10)), (5, (40, 20, 10)), (6, (30, 10, 5)),
+                                      (8, (100, 50, 20)), (16, (50, 20, 10))])
 def test_other_dimensions(tb, oracle_mod, tmp_path, cuda, D, ratios):
+    """Both kernel variants (rows read straight into registers, or staged through shared memory by
+    warp-wide chunk copies) give the oracle's results at every level, for even and odd D."""
     h = tb.QueryHandler.generate(60000 if D != 8 else 200000, D, 1.0, 100.0, False, 4, ratios, 5 + D, 3.0)
     h.prepare_for_query(tb.LevelPolicy.L0)
     o = oracle_from_handler(oracle_mod, h, tmp_path)
     pts, ids = oracle_mod.decoded_points(o)
     Q = _boxes(pts, 80, 7 + D, 0.02, 0.3)
-    r, offs, got = _batch_ids(tb, h, Q, tb.Mode.EXACT)
     b = oracle_mod.brute_query(pts, ids, oracle_mod.RANGE, Q)
-    assert np.array_equal(offs, b.offsets)
-    assert all(np.array_equal(g, b.query(q)) for q, g in enumerate(ids_by_query(offs, got)))
-    r2, offs2, got2 = _batch_ids(tb, h, Q, tb.Mode.REF_PARITY)
     ref = oracle_mod.ref_query(o, oracle_mod.RANGE, Q, sorted_ids=False)
-    assert np.array_equal(got2, ref.ids)
+    for variant in (0, 1):
+        h.set_variants([variant] * 4)
+        r, offs, got = _batch_ids(tb, h, Q, tb.Mode.EXACT)
+        assert np.array_equal(offs, b.offsets), variant
+        assert all(np.array_equal(g, b.query(q)) for q, g in enumerate(ids_by_query(offs, got))), variant
+        r2, offs2, got2 = _batch_ids(tb, h, Q, tb.Mode.REF_PARITY)
+        assert np.array_equal(got2, ref.ids), variant
 
 
 def test_height_three_and_truncated_plan(tb, oracle_mod, tmp_path, cuda):
