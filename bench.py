@@ -155,7 +155,8 @@ def main():
     ap.add_argument("--steps", type=int, default=200)
     ap.add_argument("--warmup", type=int, default=10)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--config", choices=["batched", "small"], default="batched")
+    ap.add_argument("--config", choices=["batched", "small", "knn"], default="batched")
+    ap.add_argument("--train-queries", type=int, default=2048, help="knn: separately seeded scorer training queries")
     ap.add_argument("--nq", type=int, default=4096)
     ap.add_argument("--plain-queries", type=int, default=512)
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -182,6 +183,8 @@ def main():
               "index_points": cfg["N"], "dim": cfg["D"], "queries_per_step": args.nq, "mode": "exact",
               "l2": "flushed between timed steps (256 MiB write)", "parallelism": f"replicas{world}"}
 
+    if cfg_name == "knn":
+        return run_knn(args, tb, wl, rank, world, local)
     if args.impl == "reference":
         return run_reference(args, tb, wl, cfg_name, config, rank, world)
 
@@ -342,6 +345,153 @@ def main():
         "cpu_baseline": cpu,
     }
     print(json.dumps(out))
+
+
+def knn_workload(tb, wl, nq, seed):
+    """KNN workload of the batched-KNN configuration: data points + N(0, (2% extent)^2) noise per
+    dimension, alternating K=20 and K=100 (half of each)."""
+    h = wl.generate_index(tb.QueryHandler, "knn")
+    P = wl.knn_points(h, nq, seed=seed, noise=0.02)
+    K = np.where(np.arange(nq) % 2 == 0, 20, 100).astype(np.uint32)
+    return h, P, K
+
+
+def run_knn(args, tb, wl, rank, world, local):
+    """Batched exact KNN (N=50M, D=16, 4096 queries, K in {20, 100}) with the learned frontier
+    ranking, beside the lower-bound ranking, the one-pass finest level and one query at a time.
+    Each step is one synchronous batch through the C ABI (a batch this large runs as several
+    traversals, split by the library); it is timed on the host around the call, synchronised on
+    both sides. Replicas only for N > 1."""
+    cfg = wl.CONFIGS["knn"]
+    config = {"workload": f"knn: RandomKmeans N={cfg['N']} D={cfg['D']} ratios "
+                          f"{','.join(map(str, cfg['ratios']))} seed {cfg['seed']} sigma/{cfg['sigma_divisor']}; "
+                          f"{args.nq} points (data + N(0,(2% extent)^2)), K=20 and K=100 alternating",
+              "index_points": cfg["N"], "dim": cfg["D"], "queries_per_step": args.nq, "mode": "exact",
+              "l2": "inputs larger than L2 (6.4 GB of rows per step)", "parallelism": f"replicas{world}"}
+    steps = args.steps if args.steps != 200 else 2
+    if args.impl == "reference":
+        if rank != 0:
+            return
+        sys.path.insert(0, REPO)
+        import oracle
+        h, P, K = knn_workload(tb, wl, args.nq, seed=1234)
+        pts, ids = h.decode_points(np.arange(cfg["N"], dtype=np.uint64))
+        threads = os.cpu_count() or 1
+        per = 4
+        t = 0.0
+        for s in range(steps):
+            sl = slice((s * per) % args.nq, (s * per) % args.nq + per)
+            t0 = time.perf_counter()
+            for kv in (20, 100):
+                m = K[sl] == kv
+                if m.any():
+                    oracle.brute_query(pts, ids, oracle.KNN, P[sl][m], K=kv, threads=threads)
+            t += time.perf_counter() - t0
+        v = per * steps / t
+        print(json.dumps({"metric": "exact-result KNN queries/s (batched + learned ranking, 1 B200 per rank)",
+                          "value": v, "unit": "queries/s", "impl": "reference", "n_gpus": world, "steps": steps,
+                          "warmup": 0, "ms_per_step": t / steps * 1e3, "higher_is_better": True, "scaling": "weak",
+                          "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": config,
+                          "cpu_baseline": {"value": v, "unit": "queries/s", "cores": threads, "kind": "port",
+                                           "sample": f"{per} points per step, FP64 brute force over all {cfg['N']} "
+                                                     f"points (the reference's KNN is approximate; exact needs a scan)"},
+                          "e2e": {"value": v, "unit": "queries/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}))
+        return
+    import torch
+    torch.cuda.set_device(local)
+    tb.set_device(local)
+    h, P, K = knn_workload(tb, wl, args.nq, seed=1234)
+    h.prepare_for_query(tb.LevelPolicy.L0)
+    D = cfg["D"]
+    dP = torch.from_numpy(P).cuda()
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+
+    # Scorer: trained on traces of separately seeded queries (up to 200,000 samples).
+    T = wl.knn_points(h, args.train_queries, seed=4321, noise=0.02)
+    KT = np.where(np.arange(args.train_queries) % 2 == 0, 20, 100).astype(np.uint32)
+    t0 = time.perf_counter()
+    losses = h.scorer_train(T, K=KT, max_samples=200000, epochs=8, lr=3e-3, seed=9)
+    train_s = time.perf_counter() - t0
+    stats = h.scorer_stats()
+
+    def leg(two_wave, learned, n_steps):
+        h.set_two_wave(two_wave)
+        h.scorer_enable(learned)
+        h.query_batch(tb.QueryType.POINT, dP, tb.Mode.EXACT, K=K)  # sizes every workspace
+        ts = []
+        for _ in range(n_steps):
+            flush.zero_()
+            torch.cuda.synchronize()
+            t1 = time.perf_counter()
+            h.query_batch(tb.QueryType.POINT, dP, tb.Mode.EXACT, K=K)
+            torch.cuda.synchronize()
+            ts.append(time.perf_counter() - t1)
+        c = h.knn_counters()
+        return args.nq * n_steps / sum(ts), c["rows"] / args.nq, ts
+
+    with ClockSampler(local) as clk:
+        learned_qps, learned_rows, step_s = leg(True, True, steps)
+    lb_qps, lb_rows, _ = leg(True, False, 1)
+    one_qps, one_rows, _ = leg(False, False, 1)
+
+    # End to end: host points in, offsets + ids + distances out (learned ranking).
+    h.set_two_wave(True)
+    h.scorer_enable(True)
+    e2e_t = []
+    tot = 0
+    for _ in range(steps):
+        t1 = time.perf_counter()
+        offs, ids_h, d2 = h.query_batch_host(tb.QueryType.POINT, P, tb.Mode.EXACT, K=K, ids_cap=int(K.sum()))
+        e2e_t.append(time.perf_counter() - t1)
+        tot = len(ids_h)
+    e2e_value = args.nq * steps / sum(e2e_t)
+
+    # Plain: one query at a time through the same engine (learned ranking on).
+    n_plain = min(args.plain_queries, 32)
+    lat = []
+    for i in range(n_plain):
+        torch.cuda.synchronize()
+        t1 = time.perf_counter()
+        h.query_batch(tb.QueryType.POINT, dP[i:i + 1], tb.Mode.EXACT, K=K[i:i + 1])
+        torch.cuda.synchronize()
+        lat.append(time.perf_counter() - t1)
+    plain_qps = n_plain / sum(lat)
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        sys.path.insert(0, REPO)
+        import oracle
+        pts, ids = h.decode_points(np.arange(cfg["N"], dtype=np.uint64))
+        threads = os.cpu_count() or 1
+        t1 = time.perf_counter()
+        for kv in (20, 100):
+            oracle.brute_query(pts, ids, oracle.KNN, P[:4][K[:4] == kv], K=kv, threads=threads)
+        cpu = {"value": 4 / (time.perf_counter() - t1), "unit": "queries/s", "cores": threads, "kind": "port",
+               "sample": "the first 4 points, FP64 brute force over all points, OpenMP over points"}
+    if rank != 0:
+        return
+    pl = sorted(x * 1e3 for x in lat)
+    value = learned_qps * world
+    print(json.dumps({
+        "metric": "exact-result KNN queries/s (batched + learned ranking, 1 B200 per rank)",
+        "value": value, "unit": "queries/s", "n_gpus": world, "steps": steps, "warmup": 1,
+        "ms_per_step": statistics.mean(step_s) * 1e3, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded RandomKmeans-style index and points)",
+        "config": config,
+        "e2e": {"value": e2e_value, "unit": "queries/s", "h2d_bytes_per_step": args.nq * D * 8 + args.nq * 4,
+                "d2h_bytes_per_step": (args.nq + 1) * 8 + tot * 16},
+        "gpu_launches": None,
+        "ranking": {"learned": {"qps": learned_qps, "rows_per_query": learned_rows},
+                    "lower_bound": {"qps": lb_qps, "rows_per_query": lb_rows},
+                    "one_pass": {"qps": one_qps, "rows_per_query": one_rows}},
+        "plain": {"value": plain_qps, "unit": "queries/s", "queries": n_plain,
+                  "speedup_batched_vs_plain": learned_qps / plain_qps,
+                  "latency_ms_p50": pl[len(pl) // 2], "latency_ms_p99": pl[min(len(pl) - 1, int(len(pl) * 0.99))]},
+        "scorer": {"train_queries": args.train_queries, "samples": stats["samples"], "positives": stats["positives"],
+                   "train_s": train_s, "epoch_loss": losses},
+        "clocks": clk.summary(),
+        "cpu_baseline": cpu,
+    }))
 
 
 def run_reference(args, tb, wl, cfg_name, config, rank, world):

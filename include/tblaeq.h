@@ -202,7 +202,8 @@ int tblaeq_set_variants(tblaeq_handle* h, const int* variants, uint64_t n);
 /* 1 (default) = two-wave finest level, 0 = one pass over every surviving cluster. */
 int tblaeq_set_two_wave(tblaeq_handle* h, int on);
 
-/* Counters of the last KNN batch: [0] final-frontier clusters, [1] wave-1 candidates,
+/* Counters of the last KNN batch (summed over its chunks when it ran in several): [0] final-frontier
+ * clusters, [1] wave-1 candidates,
  * [2] wave-2 candidates, [3] points whose rows wave 1 loaded and tested (the single pass, when
  * two-wave is off), [4] points whose rows wave 2 loaded and tested. */
 int tblaeq_knn_counters(tblaeq_handle* h, uint64_t* out5);
@@ -229,6 +230,10 @@ int tblaeq_scorer_loss_grad(tblaeq_handle* h, const float* X, const float* y, ui
 
 /* Logits of host samples X (n x in). */
 int tblaeq_scorer_logits(tblaeq_handle* h, const float* X, uint64_t n, float* z_out);
+
+/* The last training's sample count and how many of the traced (query, cluster) pairs were
+ * positives (the cluster holds one of the query's K nearest points). */
+int tblaeq_scorer_stats(tblaeq_handle* h, uint64_t* samples, uint64_t* positives);
 
 /* Host copies of the index arrays (read-only, owned by the handle), for tools and tests:
  * which = 0: P-tensor values of interval l (rows*D doubles), 1: colRes of interval l (cols+1),
@@ -263,6 +268,10 @@ uint64_t tblaeq_live_device_bytes(void);
 
 /* Test hook: make the n-th device allocation from now on fail (n = 0 disables). */
 void tblaeq_debug_fail_alloc_after(uint64_t n);
+
+/* Test hook: treat traversal workspaces above `limit` frontier entries or work items as too large
+ * (0 restores the 32-bit limit), so that small indexes exercise the chunked KNN batches. */
+int tblaeq_debug_split_above(tblaeq_handle* h, uint64_t limit);
 
 #ifdef __cplusplus
 }

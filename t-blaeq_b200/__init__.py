@@ -142,8 +142,10 @@ def _load():
         "tblaeq_scorer_loss_grad": ([vp, P(ctypes.c_float), P(ctypes.c_float), ctypes.c_uint64, P(ctypes.c_float),
                                      P(ctypes.c_float)], ctypes.c_int),
         "tblaeq_scorer_logits": ([vp, P(ctypes.c_float), ctypes.c_uint64, P(ctypes.c_float)], ctypes.c_int),
+        "tblaeq_scorer_stats": ([vp, P(ctypes.c_uint64), P(ctypes.c_uint64)], ctypes.c_int),
         "tblaeq_live_device_bytes": ([], ctypes.c_uint64),
         "tblaeq_debug_fail_alloc_after": ([ctypes.c_uint64], None),
+        "tblaeq_debug_split_above": ([vp, ctypes.c_uint64], ctypes.c_int),
     }
     for name, (args, res) in sig.items():
         f = getattr(lib, name)
@@ -482,6 +484,11 @@ class QueryHandler:
         z = np.empty(X.shape[0], np.float32)
         _check(_load().tblaeq_scorer_logits(self._h, _dptr(X, ctypes.c_float), X.shape[0], _dptr(z, ctypes.c_float)))
         return z
+
+    def scorer_stats(self) -> dict:
+        s, p = ctypes.c_uint64(), ctypes.c_uint64()
+        _check(_load().tblaeq_scorer_stats(self._h, ctypes.byref(s), ctypes.byref(p)))
+        return {"samples": s.value, "positives": p.value}
 
     def stream_handle(self) -> int:
         return _load().tblaeq_stream(self._h) or 0

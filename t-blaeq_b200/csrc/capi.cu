@@ -17,6 +17,8 @@ struct tblaeq_handle {
     std::vector<std::vector<uint32_t>> parent;  // parent position per mesh (lazy, decode_points)
     std::vector<std::vector<uint64_t>> posOf;   // position of each original id per mesh (lazy)
     DeviceMem kStage;                           // per-query K of KNN batches
+    DeviceMem knnOff, knnIds, knnD2;            // results of KNN batches run in chunks
+    std::vector<uint64_t> knnSum;               // counters summed over the last batch's chunks (empty: one run)
     uint64_t lastNq = 0;                        // last asynchronously enqueued batch
     unsigned lastFlags = 0;
 };
@@ -205,6 +207,63 @@ int tblaeq_coarsest_grid(tblaeq_handle* h, tblaeq_grid* out) {
     return TBLAEQ_OK;
 }
 
+// A KNN batch too large for one traversal (high dimensions keep most clusters alive, so the
+// frontier outgrows the 32-bit item space) runs as consecutive chunks, halved until each fits; the
+// chunks' results are gathered into the handle's buffers in query order. Per-level counts are not
+// kept for chunked batches.
+static BatchOutput runKnnChunked(tblaeq_handle* h, const double* dQueries, uint64_t nq, const std::vector<uint32_t>& k,
+                                 unsigned flags) {
+    Runtime& rt = h->qh->runtime();
+    const uint64_t D = rt.dev->D;
+    uint64_t sumK = 0;
+    for (uint32_t v : k) sumK += v;
+    if (h->knnIds.bytes() < std::max<uint64_t>(sumK, 1) * 8) {
+        h->knnIds.alloc(std::max<uint64_t>(sumK, 1) * 8);
+        h->knnD2.alloc(std::max<uint64_t>(sumK, 1) * 8);
+    }
+    if (h->knnOff.bytes() < (nq + 1) * 8) h->knnOff.alloc((nq + 1) * 8);
+    std::vector<uint64_t> offs(nq + 1, 0), part;
+    std::vector<uint64_t> sum(5, 0);
+    uint64_t chunk = (nq + 1) / 2, i = 0;
+    while (i < nq) {
+        const uint64_t c = std::min(chunk, nq - i);
+        uint64_t sk = 0;
+        for (uint64_t q = i; q < i + c; ++q) sk += k[q];
+        BatchOutput co;
+        try {
+            co = rt.engine->runKnn(dQueries + i * D, static_cast<uint32_t>(c), h->kStage.as<uint32_t>() + i, sk,
+                                   flags & ~static_cast<unsigned>(TBLAEQ_WANT_LEVELS));
+        } catch (const SplitBatch&) {
+            if (c == 1) throw;
+            chunk = (c + 1) / 2;
+            continue;
+        }
+        part.resize(c + 1);
+        TBLAEQ_CUDA(cudaMemcpyAsync(part.data(), co.offsets, (c + 1) * 8, cudaMemcpyDeviceToHost, rt.stream));
+        TBLAEQ_CUDA(cudaStreamSynchronize(rt.stream));
+        if (part[c]) {
+            TBLAEQ_CUDA(cudaMemcpyAsync(h->knnIds.as<uint64_t>() + offs[i], co.ids, part[c] * 8, cudaMemcpyDeviceToDevice,
+                                        rt.stream));
+            TBLAEQ_CUDA(cudaMemcpyAsync(h->knnD2.as<double>() + offs[i], co.dist2, part[c] * 8,
+                                        cudaMemcpyDeviceToDevice, rt.stream));
+        }
+        for (uint64_t q = 0; q < c; ++q) offs[i + q + 1] = offs[i] + part[q + 1];
+        const std::vector<uint64_t> cn = rt.engine->knnCounters();
+        for (size_t t = 0; t < sum.size() && t < cn.size(); ++t) sum[t] += cn[t];
+        i += c;
+    }
+    h->knnSum = sum;
+    TBLAEQ_CUDA(cudaMemcpyAsync(h->knnOff.get(), offs.data(), (nq + 1) * 8, cudaMemcpyHostToDevice, rt.stream));
+    TBLAEQ_CUDA(cudaStreamSynchronize(rt.stream));
+    BatchOutput o;
+    o.nq = static_cast<uint32_t>(nq);
+    o.total = offs[nq];
+    o.offsets = h->knnOff.as<uint64_t>();
+    o.ids = h->knnIds.as<uint64_t>();
+    o.dist2 = h->knnD2.as<double>();
+    return o;
+}
+
 static int runBatch(tblaeq_handle* h, const tblaeq_batch* b, const double* dQueries, tblaeq_batch_result* out) {
     Runtime& rt = h->qh->runtime();
     if (b->nq > 0xffffffffull) return fail(TBLAEQ_ERR_OVERFLOW, "too many queries in one batch");
@@ -223,7 +282,13 @@ static int runBatch(tblaeq_handle* h, const tblaeq_batch* b, const double* dQuer
         if (h->kStage.bytes() < std::max<size_t>(b->nq, 1) * 4) h->kStage.alloc(std::max<size_t>(b->nq, 1) * 4);
         if (b->nq)
             TBLAEQ_CUDA(cudaMemcpyAsync(h->kStage.get(), k.data(), b->nq * 4, cudaMemcpyHostToDevice, rt.stream));
-        o = rt.engine->runKnn(dQueries, static_cast<uint32_t>(b->nq), h->kStage.as<uint32_t>(), sumK, b->flags);
+        h->knnSum.clear();
+        try {
+            o = rt.engine->runKnn(dQueries, static_cast<uint32_t>(b->nq), h->kStage.as<uint32_t>(), sumK, b->flags);
+        } catch (const SplitBatch&) {
+            if (b->nq < 2) throw;
+            o = runKnnChunked(h, dQueries, b->nq, k, b->flags);
+        }
     } else {
         o = rt.engine->runRange(dQueries, static_cast<uint32_t>(b->nq), b->mode, b->flags);
     }
@@ -416,7 +481,7 @@ int tblaeq_knn_counters(tblaeq_handle* h, uint64_t* out5) {
     if (int c = checkPrepared(h)) return c;
     if (!out5) return fail(TBLAEQ_ERR_INVALID, "null output");
     return guarded([&]() -> int {
-        const std::vector<uint64_t> v = h->qh->runtime().engine->knnCounters();
+        const std::vector<uint64_t> v = h->knnSum.empty() ? h->qh->runtime().engine->knnCounters() : h->knnSum;
         for (int i = 0; i < 5; ++i) out5[i] = v[i];
         return TBLAEQ_OK;
     });
@@ -441,6 +506,14 @@ int tblaeq_scorer_train(tblaeq_handle* h, const double* points, uint64_t nq, con
         enableScorer(rt, true);
         return TBLAEQ_OK;
     });
+}
+
+int tblaeq_scorer_stats(tblaeq_handle* h, uint64_t* samples, uint64_t* positives) {
+    if (int c = checkPrepared(h)) return c;
+    Runtime& rt = h->qh->runtime();
+    if (samples) *samples = rt.scorerSamples;
+    if (positives) *positives = rt.scorerPositives;
+    return TBLAEQ_OK;
 }
 
 int tblaeq_scorer_enable(tblaeq_handle* h, int on) {
@@ -601,6 +674,12 @@ int tblaeq_level_range_noalloc(tblaeq_handle* h, uint64_t l, const tblaeq_grid* 
 }
 
 uint64_t tblaeq_live_device_bytes(void) { return liveDeviceBytes(); }
+
+int tblaeq_debug_split_above(tblaeq_handle* h, uint64_t limit) {
+    if (int c = checkPrepared(h)) return c;
+    h->qh->runtime().engine->setSplitLimit(limit ? limit : 0xffffffffull);
+    return TBLAEQ_OK;
+}
 
 void tblaeq_debug_fail_alloc_after(uint64_t n) {
     if (n == 0) {

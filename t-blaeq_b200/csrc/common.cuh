@@ -24,6 +24,11 @@ struct CudaError : std::runtime_error {
     CudaError(cudaError_t c, const std::string& what) : std::runtime_error(what), code(c) {}
 };
 
+// A batch whose traversal does not fit the 32-bit item and entry space; smaller batches do.
+struct SplitBatch : CudaError {
+    explicit SplitBatch(const std::string& what) : CudaError(cudaErrorMemoryAllocation, what) {}
+};
+
 #define TBLAEQ_CUDA(call)                                                                                     \
     do {                                                                                                      \
         cudaError_t e_ = (call);                                                                              \

@@ -164,7 +164,19 @@ void BatchEngine::reserve(const EngineCaps& want, uint32_t nq, unsigned flags) {
     }
     if (nq > qcap_ || zeroBlock_.bytes() == 0) growZ = true;
     if (c.entries > 0xffffffffull || c.items > 0xffffffffull || c.results > 0xffffffffull)
-        throw CudaError(cudaErrorMemoryAllocation, "batch exceeds 32-bit traversal capacities; split the batch");
+        throw SplitBatch("batch exceeds 32-bit traversal capacities; split the batch");
+    // Frontier and result buffers that would not fit in device memory (beside what this engine
+    // already holds and will release) also call for a smaller batch, not an allocation failure.
+    {
+        const uint64_t needF = growF ? 2 * (c.entries * (16 + 8 * D) + (c.items / tile_ + 2) * 4) : 0;
+        const uint64_t needR = growR ? c.results * (20 + ((wantVals || haveVals_) ? 8 * D : 0)) : 0;
+        size_t freeB = 0, totalB = 0;
+        TBLAEQ_CUDA(cudaMemGetInfo(&freeB, &totalB));
+        const uint64_t held = workspaceBytes(), margin = 512ull << 20;
+        if (needF + needR > freeB + held && needF + needR > margin)
+            throw SplitBatch("batch workspace (" + std::to_string((needF + needR) >> 20) +
+                             " MiB) exceeds free device memory; split the batch");
+    }
     if (growF || growR || growZ) dropGraph();  // captured launches hold the old buffer addresses
 
     if (growF) {
@@ -329,6 +341,16 @@ uint32_t BatchEngine::status() {
     return st;
 }
 
+void BatchEngine::checkSplitLimit() {
+    const int H = static_cast<int>(di_.height);
+    std::vector<uint32_t> h((H + 2) * 2);
+    TBLAEQ_CUDA(cudaMemcpyAsync(h.data(), hdrPtr(0), h.size() * 4, cudaMemcpyDeviceToHost, stream_));
+    TBLAEQ_CUDA(cudaStreamSynchronize(stream_));
+    for (int lv = 1; lv < H; ++lv)
+        if (h[2 * lv] > splitLimit_ || h[2 * lv + 1] > splitLimit_)
+            throw SplitBatch("level " + std::to_string(lv) + " exceeds the traversal limit; split the batch");
+}
+
 void BatchEngine::growFromHeaders() {
     const int H = static_cast<int>(di_.height);
     std::vector<uint32_t> h((H + 2) * 2);
@@ -338,6 +360,8 @@ void BatchEngine::growFromHeaders() {
     bool grew = false;
     for (int lv = 1; lv < H; ++lv) {
         const uint64_t cnt = h[2 * lv], items = h[2 * lv + 1];
+        if (cnt > splitLimit_ || items > splitLimit_)
+            throw SplitBatch("level " + std::to_string(lv) + " exceeds the traversal limit; split the batch");
         if (cnt > caps_.entries) {
             want.entries = std::max<uint64_t>(want.entries, cnt + cnt / 4 + 1024);
             grew = true;
@@ -362,11 +386,11 @@ void BatchEngine::growFromHeaders() {
     }
     try {
         reserve(want, qcap_, haveVals_ ? kWantVals : 0);
-    } catch (const CudaError& e) {
+    } catch (const SplitBatch& e) {
         std::string msg = std::string(e.what()) + " (status " + std::to_string(status()) + "; level entries/items:";
         for (int lv = 0; lv < H + 2; ++lv) msg += " " + std::to_string(h[2 * lv]) + "/" + std::to_string(h[2 * lv + 1]);
         msg += ")";
-        throw CudaError(cudaErrorMemoryAllocation, msg);
+        throw SplitBatch(msg);
     }
 }
 
@@ -399,7 +423,7 @@ BatchOutput BatchEngine::runRange(const double* dBoxes, uint32_t nq, int mode, u
             throw CudaError(cudaErrorLaunchTimeout, "traversal kernel reported status " + std::to_string(st));
         }
         if (st & kStatusOverflowSum)
-            throw CudaError(cudaErrorMemoryAllocation, "a level generates more than 2^32 items; split the batch");
+            throw SplitBatch("a level generates more than 2^32 items; split the batch");
         if (st == 0) {
             BatchOutput o = output(nq, flags);
             o.total = lastTotal(nq);
@@ -632,7 +656,7 @@ void BatchEngine::enqueueKnn(const double* dPoints, uint32_t nq, const uint32_t*
                waveM_.as<uint32_t>(), nq, selOff_.as<uint64_t>(), selIds_.as<uint64_t>(), selD2_.as<double>(),
                selCount_.as<uint32_t>(), status, stream_);
     TBLAEQ_CUDA(cudaMemsetAsync(sel_.get(), 0, entryCap_, stream_));
-    launchScatterSel(selIds_.as<uint64_t>(), selOff_.as<uint64_t>(), nq, sel_.as<uint8_t>(), stream_);
+    launchScatterSel(selIds_.as<uint64_t>(), selOff_.as<uint64_t>(), nq, fcap, sel_.as<uint8_t>(), stream_);
     // Wave 1: every point of the selected clusters; their K-th distance bounds tau.
     fin.child.entrySel = sel_.as<uint8_t>();
     fin.child.entryLb = lbE_.as<double>();
@@ -686,8 +710,9 @@ BatchOutput BatchEngine::runKnn(const double* dPoints, uint32_t nq, const uint32
         if (st & (kStatusLookbackTimeout | kStatusWindowOverflow))
             throw CudaError(cudaErrorLaunchTimeout, "traversal kernel reported status " + std::to_string(st));
         if (st & kStatusOverflowSum)
-            throw CudaError(cudaErrorMemoryAllocation, "a level generates more than 2^32 items; split the batch");
+            throw SplitBatch("a level generates more than 2^32 items; split the batch");
         if (st == 0) {
+            if (splitLimit_ < 0xffffffffull) checkSplitLimit();
             BatchOutput o = output(nq, flags);
             o.total = lastTotal(nq);
             return o;

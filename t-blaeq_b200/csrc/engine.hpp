@@ -57,6 +57,8 @@ public:
     // query to bound the K-th distance by real points, then expand only the clusters that bound
     // cannot exclude. Off: one pass over every surviving cluster.
     void setTwoWave(bool on) { twoWave_ = on; }
+    // Largest entry / item capacity a batch may use before it must be split (tests lower it).
+    void setSplitLimit(uint64_t limit) { splitLimit_ = limit; }
     bool twoWave() const { return twoWave_; }
     // Optional device scorer of the last frontier's entries (higher = expand earlier); when unset
     // the entries are ranked by their lower bound. Called with (frontier, hdr, cap, points, out scores).
@@ -132,6 +134,7 @@ private:
     FrontierBufs f_[2];
     DeviceMem resIds_, resVals_, resQ_, resDist_;
     DeviceMem zeroBlock_;  // desc | tickets | status | hdrs | qcount | levelItems
+    uint64_t splitLimit_ = 0xffffffffull;
     DeviceMem offsets_;
     DeviceMem boxF_;  // exact range batches: the query boxes as outward-rounded floats
     DeviceMem tau_, candOff_, knnCount_, knnOff_, knnIds_, knnD2_;
@@ -151,6 +154,7 @@ private:
     uint64_t tileCap_ = 0;
 
     void growFromHeaders();
+    void checkSplitLimit();  // throws SplitBatch when the last batch's levels exceed splitLimit_
     void enqueueLaunches(const double* dBoxes, uint32_t nq, int mode, unsigned flags);
     void dropGraph();
     bool timing_ = false;

@@ -335,11 +335,16 @@ __global__ void waveWidthKernel(const uint32_t* K, uint32_t nq, double factor, u
     }
 }
 
-__global__ void scatterSelKernel(const uint64_t* ids, const uint64_t* off, uint32_t nq, uint8_t* sel) {
+// The selection offsets are counted before the selection top-K runs; a query the top-K had to
+// skip (its frontier overflowed: the batch is rerun after growth) leaves its slots unwritten, so
+// every id is checked against the entry capacity before it is used as an index.
+__global__ void scatterSelKernel(const uint64_t* ids, const uint64_t* off, uint32_t nq, uint64_t cap, uint8_t* sel) {
     const uint64_t n = off[nq];
     for (uint64_t i = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x; i < n;
-         i += static_cast<uint64_t>(gridDim.x) * blockDim.x)
-        sel[ids[i]] = 1;
+         i += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
+        const uint64_t e = ids[i];
+        if (e < cap) sel[e] = 1;
+    }
 }
 
 __global__ void tauFromTopKKernel(const uint64_t* off, const double* d2, const uint32_t* K, uint32_t nq, double* tau) {
@@ -380,8 +385,9 @@ void launchWaveWidth(const uint32_t* K, uint32_t nq, double factor, uint32_t* M,
     TBLAEQ_CUDA(cudaGetLastError());
 }
 
-void launchScatterSel(const uint64_t* ids, const uint64_t* off, uint32_t nq, uint8_t* sel, cudaStream_t s) {
-    scatterSelKernel<<<148 * 4, 256, 0, s>>>(ids, off, nq, sel);
+void launchScatterSel(const uint64_t* ids, const uint64_t* off, uint32_t nq, uint64_t cap, uint8_t* sel,
+                      cudaStream_t s) {
+    scatterSelKernel<<<148 * 4, 256, 0, s>>>(ids, off, nq, cap, sel);
     TBLAEQ_CUDA(cudaGetLastError());
 }
 

@@ -57,8 +57,10 @@ void launchEntryBounds(const uint32_t* q, const uint32_t* node, const double* x,
 // Wave-1 width per query: clamp(ceil(factor * K[q]) + 1, 2, 32) entries.
 void launchWaveWidth(const uint32_t* K, uint32_t nq, double factor, uint32_t* M, cudaStream_t s);
 
-// sel[ids[i]] = 1 for every selected entry position in [0, off[nq]).
-void launchScatterSel(const uint64_t* ids, const uint64_t* off, uint32_t nq, uint8_t* sel, cudaStream_t s);
+// sel[ids[i]] = 1 for every selected entry position in [0, off[nq]) below cap (positions at or
+// above cap come from slots a skipped query never wrote).
+void launchScatterSel(const uint64_t* ids, const uint64_t* off, uint32_t nq, uint64_t cap, uint8_t* sel,
+                      cudaStream_t s);
 
 // tau[q] = min(tau[q], sqrt(d2 of the K[q]-th candidate) * (1 + 1e-12)) when a query has K[q] of them.
 void launchTauFromTopK(const uint64_t* off, const double* d2, const uint32_t* K, uint32_t nq, double* tau,

@@ -99,52 +99,90 @@ std::vector<float> trainScorer(Runtime& rt, const double* hostPoints, uint32_t n
     const uint32_t level = static_cast<uint32_t>(rt.dev->height - 2);
     cudaStream_t s = rt.stream;
     BatchEngine& eng = *rt.engine;
+    const int in = mlp.shape().in();
 
-    // Traces: plain two-wave KNN (lower-bound ranking) over the training queries.
+    // Traces: plain two-wave KNN (lower-bound ranking) over the training queries, in chunks small
+    // enough for one traversal each. Every chunk contributes all its positives and its share of
+    // random negatives; the union is subsampled to maxSamples at the end.
     DeviceMem dPoints(std::max<size_t>(nq, 1) * D * 8), dK(std::max<size_t>(nq, 1) * 4);
     TBLAEQ_CUDA(cudaMemcpyAsync(dPoints.get(), hostPoints, static_cast<size_t>(nq) * D * 8, cudaMemcpyHostToDevice, s));
     TBLAEQ_CUDA(cudaMemcpyAsync(dK.get(), K.data(), static_cast<size_t>(nq) * 4, cudaMemcpyHostToDevice, s));
-    uint64_t sumK = 0;
-    for (uint32_t k : K) sumK += k;
     eng.setScorer(nullptr, nullptr);  // traces come from the lower-bound ranking
     const bool wasTwoWave = eng.twoWave();
     eng.setTwoWave(true);
-    const BatchOutput res = eng.runKnn(dPoints.as<double>(), nq, dK.as<uint32_t>(), sumK, 0);
-    eng.setTwoWave(wasTwoWave);
-    const BatchEngine::FrontierView fv = eng.lastKnnFrontier();
-    uint32_t fCount = 0;
-    TBLAEQ_CUDA(cudaMemcpyAsync(&fCount, fv.in.hdr, 4, cudaMemcpyDeviceToHost, s));
-    TBLAEQ_CUDA(cudaStreamSynchronize(s));
-    fCount = std::min(fCount, fv.cap);
-    if (fCount == 0) throw std::runtime_error("scorer training: the traversal left no clusters to learn from");
-
-    DeviceMem label(fCount);
-    TBLAEQ_CUDA(cudaMemsetAsync(label.get(), 0, fCount, s));
-    labelFrontierKernel<<<std::min<uint32_t>(nq, 4096), 128, 0, s>>>(res.offsets, res.ids, fv.offsets, fv.node,
-                                                                    rt.invMapFinest.as<uint32_t>(),
-                                                                    rt.parentFinest.as<uint32_t>(), nq,
-                                                                    label.as<uint8_t>());
-    TBLAEQ_CUDA(cudaGetLastError());
-    std::vector<uint8_t> hl(fCount);
-    TBLAEQ_CUDA(cudaMemcpyAsync(hl.data(), label.get(), fCount, cudaMemcpyDeviceToHost, s));
-    TBLAEQ_CUDA(cudaStreamSynchronize(s));
-
-    // Sample: every positive, negatives at random up to maxSamples.
     std::mt19937_64 rng(cfg.seed);
-    std::vector<uint32_t> pos, neg;
-    for (uint32_t e = 0; e < fCount; ++e) (hl[e] ? pos : neg).push_back(e);
-    std::shuffle(neg.begin(), neg.end(), rng);
-    std::vector<uint32_t> idx = pos;
-    if (idx.size() > cfg.maxSamples) idx.resize(cfg.maxSamples);
-    const size_t room = cfg.maxSamples > idx.size() ? cfg.maxSamples - idx.size() : 0;
-    idx.insert(idx.end(), neg.begin(), neg.begin() + std::min(room, neg.size()));
-    const uint32_t n = static_cast<uint32_t>(idx.size());
-    const int in = mlp.shape().in();
-    DeviceMem dIdx = upload(idx, s), X(static_cast<size_t>(n) * in * 4), y(static_cast<size_t>(n) * 4);
-    mlp.frontierFeatures(fv.in, fv.node, dIdx.as<uint32_t>(), n, dPoints.as<double>(), rt.dev->nodeSub[level].as<NodeRec>(),
-                         level, rt.scorerInvScale, X.as<float>(), s);
-    gatherLabelsKernel<<<148, 256, 0, s>>>(label.as<uint8_t>(), dIdx.as<uint32_t>(), n, y.as<float>());
-    TBLAEQ_CUDA(cudaGetLastError());
+    std::vector<float> hostX, hostY;
+    uint64_t positives = 0;
+    uint32_t chunk = nq, i = 0;
+    while (i < nq) {
+        const uint32_t c = std::min(chunk, nq - i);
+        uint64_t sumK = 0;
+        for (uint32_t q = i; q < i + c; ++q) sumK += K[q];
+        const double* pts = dPoints.as<double>() + static_cast<size_t>(i) * D;
+        BatchOutput res;
+        try {
+            res = eng.runKnn(pts, c, dK.as<uint32_t>() + i, sumK, 0);
+        } catch (const SplitBatch&) {
+            if (c == 1) {
+                eng.setTwoWave(wasTwoWave);
+                throw;
+            }
+            chunk = (c + 1) / 2;
+            continue;
+        }
+        const BatchEngine::FrontierView fv = eng.lastKnnFrontier();
+        uint32_t fCount = 0;
+        TBLAEQ_CUDA(cudaMemcpyAsync(&fCount, fv.in.hdr, 4, cudaMemcpyDeviceToHost, s));
+        TBLAEQ_CUDA(cudaStreamSynchronize(s));
+        fCount = std::min(fCount, fv.cap);
+        if (fCount > 0) {
+            DeviceMem label(fCount);
+            TBLAEQ_CUDA(cudaMemsetAsync(label.get(), 0, fCount, s));
+            labelFrontierKernel<<<std::min<uint32_t>(c, 4096), 128, 0, s>>>(
+                res.offsets, res.ids, fv.offsets, fv.node, rt.invMapFinest.as<uint32_t>(),
+                rt.parentFinest.as<uint32_t>(), c, label.as<uint8_t>());
+            TBLAEQ_CUDA(cudaGetLastError());
+            std::vector<uint8_t> hl(fCount);
+            TBLAEQ_CUDA(cudaMemcpyAsync(hl.data(), label.get(), fCount, cudaMemcpyDeviceToHost, s));
+            TBLAEQ_CUDA(cudaStreamSynchronize(s));
+            std::vector<uint32_t> pos, neg;
+            for (uint32_t e = 0; e < fCount; ++e) (hl[e] ? pos : neg).push_back(e);
+            std::shuffle(neg.begin(), neg.end(), rng);
+            const uint64_t quota = (static_cast<uint64_t>(cfg.maxSamples) * c + nq - 1) / nq;
+            std::vector<uint32_t> idx = pos;
+            if (quota > idx.size()) idx.insert(idx.end(), neg.begin(), neg.begin() + std::min<size_t>(quota - idx.size(), neg.size()));
+            positives += pos.size();
+            const uint32_t n = static_cast<uint32_t>(idx.size());
+            DeviceMem dIdx = upload(idx, s), X(static_cast<size_t>(std::max<uint32_t>(n, 1)) * in * 4),
+                      y(static_cast<size_t>(std::max<uint32_t>(n, 1)) * 4);
+            mlp.frontierFeatures(fv.in, fv.node, dIdx.as<uint32_t>(), n, pts, rt.dev->nodeSub[level].as<NodeRec>(), level,
+                                 rt.scorerInvScale, X.as<float>(), s);
+            gatherLabelsKernel<<<148, 256, 0, s>>>(label.as<uint8_t>(), dIdx.as<uint32_t>(), n, y.as<float>());
+            TBLAEQ_CUDA(cudaGetLastError());
+            const size_t x0 = hostX.size(), y0 = hostY.size();
+            hostX.resize(x0 + static_cast<size_t>(n) * in);
+            hostY.resize(y0 + n);
+            TBLAEQ_CUDA(cudaMemcpyAsync(hostX.data() + x0, X.get(), static_cast<size_t>(n) * in * 4,
+                                        cudaMemcpyDeviceToHost, s));
+            TBLAEQ_CUDA(cudaMemcpyAsync(hostY.data() + y0, y.get(), static_cast<size_t>(n) * 4, cudaMemcpyDeviceToHost, s));
+            TBLAEQ_CUDA(cudaStreamSynchronize(s));
+        }
+        i += c;
+    }
+    eng.setTwoWave(wasTwoWave);
+    if (hostY.empty()) throw std::runtime_error("scorer training: the traversal left no clusters to learn from");
+    // Subsample the union to maxSamples (keeping the sample order random either way).
+    std::vector<uint32_t> keep(hostY.size());
+    std::iota(keep.begin(), keep.end(), 0u);
+    std::shuffle(keep.begin(), keep.end(), rng);
+    if (keep.size() > cfg.maxSamples) keep.resize(cfg.maxSamples);
+    const uint32_t n = static_cast<uint32_t>(keep.size());
+    std::vector<float> sx(static_cast<size_t>(n) * in), sy(n);
+    for (uint32_t t = 0; t < n; ++t) {
+        std::copy_n(hostX.data() + static_cast<size_t>(keep[t]) * in, in, sx.data() + static_cast<size_t>(t) * in);
+        sy[t] = hostY[keep[t]];
+    }
+    DeviceMem X = upload(sx, s), y = upload(sy, s);
 
     // Adam over shuffled mini-batches.
     DeviceMem Xp(static_cast<size_t>(n) * in * 4), yp(static_cast<size_t>(n) * 4), grad(mlp.shape().params() * 4);
@@ -169,7 +207,7 @@ std::vector<float> trainScorer(Runtime& rt, const double* hostPoints, uint32_t n
         losses.push_back(static_cast<float>(sum / std::max(1, batches)));
     }
     TBLAEQ_CUDA(cudaStreamSynchronize(s));
-    rt.scorerPositives = pos.size();
+    rt.scorerPositives = positives;
     rt.scorerSamples = n;
     return losses;
 }

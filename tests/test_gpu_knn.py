@@ -121,3 +121,30 @@ def test_knn_first_batch_grows_every_buffer(tb, oracle_mod, cuda):
     assert np.array_equal(off[:65], b.offsets)
     assert np.array_equal(r.ids.numpy()[:off[64]], b.ids)
     assert np.array_equal(r.dist2.numpy()[:off[64]], b.dist2)
+
+
+def test_knn_batch_split_into_chunks(tb, env, oracle_mod):
+    """A KNN batch whose workspace exceeds the traversal limit runs as chunks with the same results
+    as one traversal (the limit is lowered here so a small index needs several chunks)."""
+    h, o, pts, ids = env
+    P = _points(pts, 400, 21)
+    Kq = np.where(np.arange(400) % 2 == 0, 20, 100).astype(np.uint32)
+    whole = h.query_batch(tb.QueryType.POINT, P, tb.Mode.EXACT, K=Kq)
+    w_off, w_ids, w_d2 = whole.offsets.numpy(), whole.ids.numpy(), whole.dist2.numpy()
+    lib = tb.lib()
+    assert lib.tblaeq_debug_split_above(h._h, 1 << 18) == 0
+    try:
+        r = h.query_batch(tb.QueryType.POINT, P, tb.Mode.EXACT, K=Kq)
+        assert np.array_equal(r.offsets.numpy(), w_off)
+        assert np.array_equal(r.ids.numpy(), w_ids)
+        assert np.array_equal(r.dist2.numpy(), w_d2)
+        # (Counters are not compared: which clusters survive depends on when concurrent tau
+        # tightenings land, while the results do not.)
+        assert lib.tblaeq_debug_split_above(h._h, 50) == 0
+        with pytest.raises(tb.TblaeqError):
+            h.query_batch(tb.QueryType.POINT, P[:1], tb.Mode.EXACT, K=20)
+    finally:
+        lib.tblaeq_debug_split_above(h._h, 0)
+    b = oracle_mod.brute_query(pts, ids, oracle_mod.KNN, P[:50], K=20)
+    r2 = h.query_batch(tb.QueryType.POINT, P[:50], tb.Mode.EXACT, K=20)
+    assert np.array_equal(r2.ids.numpy(), b.ids) and np.array_equal(r2.dist2.numpy(), b.dist2)
