@@ -273,6 +273,49 @@ void tblaeq_debug_fail_alloc_after(uint64_t n);
  * (0 restores the 32-bit limit), so that small indexes exercise the chunked KNN batches. */
 int tblaeq_debug_split_above(tblaeq_handle* h, uint64_t limit);
 
+/* ---- Serving loop ------------------------------------------------------------------------------
+ * Replaces the reference's one-query-at-a-time request loop behind its HTTP front end
+ * (src/HTTPServer.cu:414-550; the HTTP layer itself is not part of this library). A server owns two
+ * lanes (range and KNN), each a worker thread with its own device workspace and CUDA stream; each
+ * lane batches continuously (requests that arrive while its batch is on the GPU form the next
+ * batch), with slots per batch bounded by max_batch and by the lane's device-memory budget.
+ * Requests are exact (KNN always; range in `mode`). The handle must stay open and prepared while a
+ * server runs; other calls on the same handle may run concurrently from one other thread. */
+typedef struct tblaeq_server tblaeq_server;
+
+typedef struct {
+    uint32_t max_batch;      /* requests per batch and lane (0: 4096) */
+    uint64_t memory_budget;  /* traversal workspace bytes per lane (0: a quarter of free memory) */
+    int mode;                /* tblaeq_mode for range requests */
+    int learned;             /* rank KNN frontiers with the trained scorer, when one exists */
+    int lanes;               /* 2 (range and KNN lanes, default when 0) or 1 (one lane, arrival order) */
+} tblaeq_serve_config;
+
+typedef struct {
+    uint64_t submitted, completed, failed, batches, max_batch;
+    double mean_batch;
+    double p50_us, p99_us, mean_us, max_us; /* arrival to result, per request */
+    double span_s;                          /* first arrival to last completion */
+} tblaeq_serve_metrics;
+
+int tblaeq_serve_start(tblaeq_handle* h, const tblaeq_serve_config* cfg, tblaeq_server** out);
+/* qtype TBLAEQ_POINT: query = point[D], K neighbours; TBLAEQ_RANGE: query = lo[D] hi[D]. */
+int tblaeq_serve_submit(tblaeq_server* s, int qtype, const double* query, uint64_t K, uint64_t* ticket);
+/* Submits n requests from the calling thread, request i at arrival_us[i] microseconds after the
+ * call (a replayed arrival schedule); its query starts at queries + offsets[i]. */
+int tblaeq_serve_replay(tblaeq_server* s, uint64_t n, const int* qtypes, const double* queries,
+                        const uint64_t* offsets, const uint32_t* K, const double* arrival_us, uint64_t* tickets);
+/* Waits up to wait_ms for the ticket's result. TBLAEQ_OK: *n_out ids (and squared distances for
+ * KNN) copied, ticket released. TBLAEQ_ERR_TIMEOUT: not done yet. TBLAEQ_ERR_OVERFLOW: cap < *n_out,
+ * the result stays. A failed request returns its error code and message and is released. */
+int tblaeq_serve_poll(tblaeq_server* s, uint64_t ticket, int wait_ms, uint64_t* ids_out, double* dist2_out,
+                      uint64_t cap, uint64_t* n_out, double* latency_us);
+/* TBLAEQ_OK once every submitted request has completed, TBLAEQ_ERR_TIMEOUT after wait_ms. */
+int tblaeq_serve_wait_idle(tblaeq_server* s, int wait_ms);
+int tblaeq_serve_stats(tblaeq_server* s, int reset, tblaeq_serve_metrics* out);
+/* Drains the queued requests, joins the workers and frees the server (its results go with it). */
+int tblaeq_serve_stop(tblaeq_server* s);
+
 #ifdef __cplusplus
 }
 #endif

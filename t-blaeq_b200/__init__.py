@@ -146,6 +146,16 @@ def _load():
         "tblaeq_live_device_bytes": ([], ctypes.c_uint64),
         "tblaeq_debug_fail_alloc_after": ([ctypes.c_uint64], None),
         "tblaeq_debug_split_above": ([vp, ctypes.c_uint64], ctypes.c_int),
+        "tblaeq_serve_start": ([vp, P(_ServeConfig), P(vp)], ctypes.c_int),
+        "tblaeq_serve_submit": ([vp, ctypes.c_int, P(ctypes.c_double), ctypes.c_uint64, P(ctypes.c_uint64)],
+                                ctypes.c_int),
+        "tblaeq_serve_replay": ([vp, ctypes.c_uint64, P(ctypes.c_int), P(ctypes.c_double), P(ctypes.c_uint64),
+                                 P(ctypes.c_uint32), P(ctypes.c_double), P(ctypes.c_uint64)], ctypes.c_int),
+        "tblaeq_serve_poll": ([vp, ctypes.c_uint64, ctypes.c_int, P(ctypes.c_uint64), P(ctypes.c_double),
+                               ctypes.c_uint64, P(ctypes.c_uint64), P(ctypes.c_double)], ctypes.c_int),
+        "tblaeq_serve_wait_idle": ([vp, ctypes.c_int], ctypes.c_int),
+        "tblaeq_serve_stats": ([vp, ctypes.c_int, P(_ServeMetrics)], ctypes.c_int),
+        "tblaeq_serve_stop": ([vp], ctypes.c_int),
     }
     for name, (args, res) in sig.items():
         f = getattr(lib, name)
@@ -153,6 +163,18 @@ def _load():
         f.restype = res
     _lib = lib
     return lib
+
+
+class _ServeConfig(ctypes.Structure):
+    _fields_ = [("max_batch", ctypes.c_uint32), ("memory_budget", ctypes.c_uint64), ("mode", ctypes.c_int),
+                ("learned", ctypes.c_int), ("lanes", ctypes.c_int)]
+
+
+class _ServeMetrics(ctypes.Structure):
+    _fields_ = [("submitted", ctypes.c_uint64), ("completed", ctypes.c_uint64), ("failed", ctypes.c_uint64),
+                ("batches", ctypes.c_uint64), ("max_batch", ctypes.c_uint64), ("mean_batch", ctypes.c_double),
+                ("p50_us", ctypes.c_double), ("p99_us", ctypes.c_double), ("mean_us", ctypes.c_double),
+                ("max_us", ctypes.c_double), ("span_s", ctypes.c_double)]
 
 
 def lib():
@@ -584,6 +606,90 @@ class QueryHandler:
 
 
 # ---- reference query-file format (src/Data_Structures/File.cu:139-216) ---------------------------
+class Server:
+    """Serving loop over a prepared handle: continuous batching of range and KNN requests
+    (the batched replacement for the reference's one-query-at-a-time request loop,
+    src/HTTPServer.cu:414-550). Results are exact; KNN results carry squared distances."""
+
+    def __init__(self, handler: "QueryHandler", max_batch: int = 4096, memory_budget: int = 0,
+                 mode: Mode = Mode.EXACT, learned: bool = True, lanes: int = 2):
+        self._owner = handler
+        self._D = handler.info()["D"]
+        cfg = _ServeConfig(max_batch, memory_budget, int(mode), int(learned), lanes)
+        s = ctypes.c_void_p()
+        _check(_load().tblaeq_serve_start(handler._h, ctypes.byref(cfg), ctypes.byref(s)))
+        self._s = s
+
+    def submit(self, qtype: QueryType, query, K: int = 0) -> int:
+        q = np.ascontiguousarray(np.asarray(query, dtype=np.float64).ravel())
+        t = ctypes.c_uint64()
+        _check(_load().tblaeq_serve_submit(self._s, int(qtype), _dptr(q), int(K), ctypes.byref(t)))
+        return t.value
+
+    def replay(self, qtypes, queries, K, arrival_us) -> np.ndarray:
+        """Submit request i at arrival_us[i] µs from now; queries[i] is a row (2D values for range, D
+        for KNN, any padding after them ignored). Returns the tickets."""
+        qt = np.ascontiguousarray(np.asarray(qtypes, dtype=np.int32))
+        Q = np.ascontiguousarray(np.asarray(queries, dtype=np.float64))
+        n = len(qt)
+        offs = (np.arange(n, dtype=np.uint64) * np.uint64(Q.shape[1])).astype(np.uint64)
+        k = np.ascontiguousarray(np.asarray(K, dtype=np.uint32))
+        at = np.ascontiguousarray(np.asarray(arrival_us, dtype=np.float64))
+        tickets = np.empty(n, np.uint64)
+        _check(_load().tblaeq_serve_replay(self._s, n, qt.ctypes.data_as(ctypes.POINTER(ctypes.c_int)), _dptr(Q),
+                                           _dptr(offs, ctypes.c_uint64), k.ctypes.data_as(ctypes.POINTER(ctypes.c_uint32)),
+                                           _dptr(at), _dptr(tickets, ctypes.c_uint64)))
+        return tickets
+
+    def poll(self, ticket: int, wait_ms: int = 10000):
+        """(ids, dist2 or None, latency_us) once done; None if not done within wait_ms."""
+        lib = _load()
+        cap = 1024
+        while True:
+            ids = np.empty(cap, np.uint64)
+            d2 = np.empty(cap, np.float64)
+            n, lat = ctypes.c_uint64(), ctypes.c_double()
+            code = lib.tblaeq_serve_poll(self._s, int(ticket), wait_ms, _dptr(ids, ctypes.c_uint64), _dptr(d2), cap,
+                                         ctypes.byref(n), ctypes.byref(lat))
+            if code == 6:
+                return None
+            if code == 5:
+                cap = int(n.value)
+                continue
+            _check(code)
+            k = int(n.value)
+            return ids[:k], d2[:k], lat.value
+
+    def wait_idle(self, wait_ms: int = 60000) -> bool:
+        code = _load().tblaeq_serve_wait_idle(self._s, wait_ms)
+        if code == 6:
+            return False
+        _check(code)
+        return True
+
+    def stats(self, reset: bool = False) -> dict:
+        m = _ServeMetrics()
+        _check(_load().tblaeq_serve_stats(self._s, int(reset), ctypes.byref(m)))
+        return {f: getattr(m, f) for f, _ in _ServeMetrics._fields_}
+
+    def stop(self):
+        if self._s:
+            _check(_load().tblaeq_serve_stop(self._s))
+            self._s = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.stop()
+
+    def __del__(self):
+        try:
+            self.stop()
+        except Exception:
+            pass
+
+
 def save_query_file(path: str, q_type: QueryType, rows: np.ndarray, D: int):
     """Header 'n D', then one row per query: 2D values (lo then hi) for RANGE, D values for POINT."""
     rows = np.asarray(rows, dtype=np.float64)

@@ -8,6 +8,7 @@
 #include "handler.hpp"
 #include "noalloc.hpp"
 #include "scorer.hpp"
+#include "serve.hpp"
 
 using namespace tblaeq;
 
@@ -688,6 +689,113 @@ void tblaeq_debug_fail_alloc_after(uint64_t n) {
     }
     auto counter = std::make_shared<uint64_t>(n);
     setAllocHook([counter](size_t) { return --(*counter) > 0; });
+}
+
+}  // extern "C"
+
+struct tblaeq_server {
+    std::unique_ptr<tblaeq::Server> server;
+};
+
+extern "C" {
+
+int tblaeq_serve_start(tblaeq_handle* h, const tblaeq_serve_config* cfg, tblaeq_server** out) {
+    if (int c = checkPrepared(h)) return c;
+    if (!out) return fail(TBLAEQ_ERR_INVALID, "null output");
+    return guarded([&]() -> int {
+        ServeConfig sc;
+        if (cfg) {
+            if (cfg->max_batch) sc.maxBatch = cfg->max_batch;
+            sc.memoryBudget = cfg->memory_budget;
+            if (cfg->mode != TBLAEQ_MODE_REF_PARITY && cfg->mode != TBLAEQ_MODE_EXACT)
+                return fail(TBLAEQ_ERR_INVALID, "bad mode");
+            sc.mode = cfg->mode;
+            sc.learned = cfg->learned != 0;
+            if (cfg->lanes) sc.lanes = cfg->lanes;
+        }
+        auto s = std::make_unique<tblaeq_server>();
+        s->server = std::make_unique<Server>(h->qh->runtime(), sc);
+        *out = s.release();
+        return TBLAEQ_OK;
+    });
+}
+
+int tblaeq_serve_submit(tblaeq_server* s, int qtype, const double* query, uint64_t K, uint64_t* ticket) {
+    if (!s || !s->server) return fail(TBLAEQ_ERR_INVALID, "null server");
+    if (K > 0xffffffffull) return fail(TBLAEQ_ERR_INVALID, "K too large");
+    return guarded([&]() -> int {
+        const uint64_t t = s->server->submit(qtype, query, static_cast<uint32_t>(K), Server::Clock::now());
+        if (ticket) *ticket = t;
+        return TBLAEQ_OK;
+    });
+}
+
+int tblaeq_serve_replay(tblaeq_server* s, uint64_t n, const int* qtypes, const double* queries,
+                        const uint64_t* offsets, const uint32_t* K, const double* arrival_us, uint64_t* tickets) {
+    if (!s || !s->server) return fail(TBLAEQ_ERR_INVALID, "null server");
+    if (n && (!qtypes || !queries || !offsets || !arrival_us)) return fail(TBLAEQ_ERR_INVALID, "null argument");
+    return guarded([&]() -> int {
+        const std::vector<uint64_t> t = s->server->replay(n, qtypes, queries, offsets, K, arrival_us);
+        if (tickets) std::copy(t.begin(), t.end(), tickets);
+        return TBLAEQ_OK;
+    });
+}
+
+int tblaeq_serve_poll(tblaeq_server* s, uint64_t ticket, int wait_ms, uint64_t* ids_out, double* dist2_out,
+                      uint64_t cap, uint64_t* n_out, double* latency_us) {
+    if (!s || !s->server) return fail(TBLAEQ_ERR_INVALID, "null server");
+    return guarded([&]() -> int {
+        Server::Result r;
+        if (!s->server->poll(ticket, r, wait_ms)) return fail(TBLAEQ_ERR_TIMEOUT, "request not done yet");
+        if (latency_us) *latency_us = r.latencyUs;
+        if (n_out) *n_out = r.ids.size();
+        if (r.status != 0) return fail(r.status, r.error);
+        if (r.ids.size() > cap) {
+            // Keep the result for a call with a larger buffer.
+            const uint64_t need = r.ids.size();
+            s->server->repost(ticket, std::move(r));
+            if (n_out) *n_out = need;
+            return fail(TBLAEQ_ERR_OVERFLOW, "result larger than cap");
+        }
+        if (ids_out && !r.ids.empty()) std::copy(r.ids.begin(), r.ids.end(), ids_out);
+        if (dist2_out && !r.dist2.empty()) std::copy(r.dist2.begin(), r.dist2.end(), dist2_out);
+        return TBLAEQ_OK;
+    });
+}
+
+int tblaeq_serve_wait_idle(tblaeq_server* s, int wait_ms) {
+    if (!s || !s->server) return fail(TBLAEQ_ERR_INVALID, "null server");
+    return guarded([&]() -> int {
+        return s->server->waitIdle(wait_ms) ? TBLAEQ_OK : fail(TBLAEQ_ERR_TIMEOUT, "requests still in flight");
+    });
+}
+
+int tblaeq_serve_stats(tblaeq_server* s, int reset, tblaeq_serve_metrics* out) {
+    if (!s || !s->server || !out) return fail(TBLAEQ_ERR_INVALID, "null argument");
+    return guarded([&]() -> int {
+        const ServeStats st = s->server->stats(reset != 0);
+        out->submitted = st.submitted;
+        out->completed = st.completed;
+        out->failed = st.failed;
+        out->batches = st.batches;
+        out->max_batch = st.maxBatch;
+        out->mean_batch = st.meanBatch;
+        out->p50_us = st.p50Us;
+        out->p99_us = st.p99Us;
+        out->mean_us = st.meanUs;
+        out->max_us = st.maxUs;
+        out->span_s = st.spanS;
+        return TBLAEQ_OK;
+    });
+}
+
+int tblaeq_serve_stop(tblaeq_server* s) {
+    if (!s) return fail(TBLAEQ_ERR_INVALID, "null server");
+    return guarded([&]() -> int {
+        if (s->server) s->server->stop();
+        delete s;
+        return TBLAEQ_OK;
+    });
 }
 
 }  // extern "C"

@@ -82,6 +82,10 @@ Mlp& ensureScorer(Runtime& rt) {
     return *rt.scorer;
 }
 
+bool scorerTrained(const Runtime& rt) { return rt.scorer && rt.scorerSamples > 0; }
+
+void attachScorer(Runtime& rt, BatchEngine& engine) { engine.setScorer(&scorerHook, &rt); }
+
 void enableScorer(Runtime& rt, bool on) {
     if (on) {
         ensureScorer(rt);

@@ -30,4 +30,8 @@ std::vector<float> trainScorer(Runtime& rt, const double* hostPoints, uint32_t n
 // Turns the scorer on or off for the two-wave ranking of KNN batches.
 void enableScorer(Runtime& rt, bool on);
 
+// Whether the handle has a trained scorer, and hooking it into another engine (serving lanes).
+bool scorerTrained(const Runtime& rt);
+void attachScorer(Runtime& rt, BatchEngine& engine);
+
 }  // namespace tblaeq
