@@ -273,6 +273,39 @@ void tblaeq_debug_fail_alloc_after(uint64_t n);
  * (0 restores the 32-bit limit), so that small indexes exercise the chunked KNN batches. */
 int tblaeq_debug_split_above(tblaeq_handle* h, uint64_t limit);
 
+/* ---- Index build -------------------------------------------------------------------------------
+ * Replaces IndexBuilder::build (src/core/IndexBuilder.cu:44-151: cuVS k-means per level, then
+ * Genenate_One_P_Tensor / Compute_Max_Radius, src/Setup/Setup.cuh:87-171): Lloyd's k-means per
+ * level on the GPU, k = floor(n / ratio) centroids sampled from the data (seeded), `iters`
+ * iterations, then the same P-tensor / map / radius assembly (rows grouped by label in input
+ * order). precision: 0 = tensor cores (tcgen05; TF32 hi/lo split operands, FP32 accumulation;
+ * D <= 16, larger D uses 1), 1 = FP32 CUDA cores, 2 = FP64 CUDA cores (the precision reference).
+ * Centroid sums accumulate in FP64; objectives are sum ||x - c(x)||^2 in FP64. */
+typedef struct {
+    int iters;         /* Lloyd iterations per level (0: 20) */
+    uint64_t seed;
+    int precision;
+} tblaeq_build_config;
+
+typedef struct {
+    uint64_t n, k;          /* points and centroids of the level */
+    int iters;
+    double objective;       /* after the last iteration */
+    double assign_seconds;  /* device time of the assignment passes */
+    double seconds;         /* the whole level, including the index assembly on the host */
+} tblaeq_build_report;
+
+/* Builds an index over host FP32 points (N x D) with `height` levels and `ratios` (finest first, as
+ * in the reference). *out receives an unprepared handle (like tblaeq_open); report (height - 1
+ * entries, finest level first, may be NULL). */
+int tblaeq_kmeans_build(const float* points, uint64_t N, uint64_t D, uint64_t height, const uint64_t* ratios,
+                        const tblaeq_build_config* cfg, tblaeq_handle** out, tblaeq_build_report* report);
+
+/* One level of k-means on the current device (no index): centroids_out (k x D) and labels_out (n)
+ * may be NULL; objectives_out receives one FP64 objective per iteration. */
+int tblaeq_kmeans(const float* points, uint64_t n, uint64_t D, uint64_t k, const tblaeq_build_config* cfg,
+                  float* centroids_out, uint32_t* labels_out, double* objectives_out);
+
 /* ---- Serving loop ------------------------------------------------------------------------------
  * Replaces the reference's one-query-at-a-time request loop behind its HTTP front end
  * (src/HTTPServer.cu:414-550; the HTTP layer itself is not part of this library). A server owns two

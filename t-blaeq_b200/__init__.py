@@ -66,6 +66,21 @@ class _GenParams(ctypes.Structure):
                 ("sigmaDivisor", ctypes.c_double)]
 
 
+class _BuildConfig(ctypes.Structure):
+    _fields_ = [("iters", ctypes.c_int), ("seed", ctypes.c_uint64), ("precision", ctypes.c_int)]
+
+
+class _BuildReport(ctypes.Structure):
+    _fields_ = [("n", ctypes.c_uint64), ("k", ctypes.c_uint64), ("iters", ctypes.c_int),
+                ("objective", ctypes.c_double), ("assign_seconds", ctypes.c_double), ("seconds", ctypes.c_double)]
+
+
+class KmeansPrecision(enum.IntEnum):
+    TENSOR = 0   # tcgen05 tensor cores, TF32 hi/lo split operands, FP32 accumulation
+    FP32 = 1     # CUDA cores, FP32
+    FP64 = 2     # CUDA cores, FP64 (the precision reference)
+
+
 class _Info(ctypes.Structure):
     _fields_ = [("D", ctypes.c_uint64), ("N", ctypes.c_uint64), ("height", ctypes.c_uint64),
                 ("intervals", ctypes.c_uint64), ("meshSizes", ctypes.c_uint64 * 16),
@@ -146,6 +161,10 @@ def _load():
         "tblaeq_live_device_bytes": ([], ctypes.c_uint64),
         "tblaeq_debug_fail_alloc_after": ([ctypes.c_uint64], None),
         "tblaeq_debug_split_above": ([vp, ctypes.c_uint64], ctypes.c_int),
+        "tblaeq_kmeans_build": ([P(ctypes.c_float), ctypes.c_uint64, ctypes.c_uint64, ctypes.c_uint64,
+                                 P(ctypes.c_uint64), P(_BuildConfig), P(vp), P(_BuildReport)], ctypes.c_int),
+        "tblaeq_kmeans": ([P(ctypes.c_float), ctypes.c_uint64, ctypes.c_uint64, ctypes.c_uint64, P(_BuildConfig),
+                           P(ctypes.c_float), P(ctypes.c_uint32), P(ctypes.c_double)], ctypes.c_int),
         "tblaeq_serve_start": ([vp, P(_ServeConfig), P(vp)], ctypes.c_int),
         "tblaeq_serve_submit": ([vp, ctypes.c_int, P(ctypes.c_double), ctypes.c_uint64, P(ctypes.c_uint64)],
                                 ctypes.c_int),
@@ -289,6 +308,24 @@ class QueryHandler:
         obj = cls(_handle=h)
         obj.dataset_name = f"Gen{N}D{D}"
         return obj
+
+    @classmethod
+    def build(cls, points, height: int = 4, ratios: Sequence[int] = (100, 50, 20), iters: int = 20, seed: int = 1,
+              precision: "KmeansPrecision" = None) -> tuple:
+        """IndexBuilder::build over FP32 points (N x D): GPU k-means per level, then the reference's
+        P-tensor / map / radius assembly. Returns (handler, per-level reports, finest first)."""
+        X = np.ascontiguousarray(np.asarray(points, dtype=np.float32))
+        N, D = X.shape
+        r = np.ascontiguousarray(np.array(list(ratios), dtype=np.uint64))
+        prec = KmeansPrecision.TENSOR if precision is None else precision
+        cfg = _BuildConfig(iters, seed, int(prec))
+        reps = (_BuildReport * max(1, height - 1))()
+        h = ctypes.c_void_p()
+        _check(_load().tblaeq_kmeans_build(_dptr(X, ctypes.c_float), N, D, height, _dptr(r, ctypes.c_uint64),
+                                           ctypes.byref(cfg), ctypes.byref(h), reps))
+        obj = cls(_handle=h)
+        obj.dataset_name = f"Kmeans{N}D{D}"
+        return obj, [{f: getattr(x, f) for f, _ in _BuildReport._fields_} for x in reps[:height - 1]]
 
     # -- lifecycle -------------------------------------------------------------------------------
     def close(self):
@@ -688,6 +725,19 @@ class Server:
             self.stop()
         except Exception:
             pass
+
+
+def kmeans(points, k: int, iters: int = 20, seed: int = 1, precision: KmeansPrecision = KmeansPrecision.TENSOR):
+    """One level of GPU k-means: (centroids k x D FP32, labels, FP64 objective per iteration)."""
+    X = np.ascontiguousarray(np.asarray(points, dtype=np.float32))
+    n, D = X.shape
+    C = np.empty((k, D), np.float32)
+    L = np.empty(n, np.uint32)
+    obj = np.empty(iters, np.float64)
+    cfg = _BuildConfig(iters, seed, int(precision))
+    _check(_load().tblaeq_kmeans(_dptr(X, ctypes.c_float), n, D, k, ctypes.byref(cfg), _dptr(C, ctypes.c_float),
+                                 L.ctypes.data_as(ctypes.POINTER(ctypes.c_uint32)), _dptr(obj)))
+    return C, L, obj
 
 
 def save_query_file(path: str, q_type: QueryType, rows: np.ndarray, D: int):

@@ -9,6 +9,7 @@
 #include "noalloc.hpp"
 #include "scorer.hpp"
 #include "serve.hpp"
+#include "kmeans.cuh"
 
 using namespace tblaeq;
 
@@ -794,6 +795,82 @@ int tblaeq_serve_stop(tblaeq_server* s) {
     return guarded([&]() -> int {
         if (s->server) s->server->stop();
         delete s;
+        return TBLAEQ_OK;
+    });
+}
+
+}  // extern "C"
+
+extern "C" {
+
+static KmeansConfig kmeansConfigOf(const tblaeq_build_config* cfg) {
+    KmeansConfig c;
+    if (cfg) {
+        if (cfg->iters > 0) c.iters = cfg->iters;
+        c.seed = cfg->seed;
+        c.precision = cfg->precision;
+    }
+    return c;
+}
+
+int tblaeq_kmeans_build(const float* points, uint64_t N, uint64_t D, uint64_t height, const uint64_t* ratios,
+                        const tblaeq_build_config* cfg, tblaeq_handle** out, tblaeq_build_report* report) {
+    if (!points || !out || (height > 1 && !ratios)) return fail(TBLAEQ_ERR_INVALID, "null argument");
+    if (cfg && (cfg->precision < 0 || cfg->precision > 2)) return fail(TBLAEQ_ERR_INVALID, "bad precision");
+    *out = nullptr;
+    return guarded([&]() -> int {
+        const KmeansConfig c = kmeansConfigOf(cfg);
+        std::vector<uint64_t> r(ratios, ratios + (height > 1 ? height - 1 : 0));
+        std::vector<KmeansLevelReport> reps;
+        cudaStream_t s = nullptr;
+        TBLAEQ_CUDA(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+        HostIndex idx;
+        try {
+            idx = kmeansBuild(points, N, D, height, r, c, reps, s);
+        } catch (...) {
+            cudaStreamDestroy(s);
+            throw;
+        }
+        cudaStreamDestroy(s);
+        if (report) {
+            for (size_t i = 0; i < reps.size(); ++i) {
+                report[i].n = reps[i].n;
+                report[i].k = reps[i].k;
+                report[i].iters = reps[i].iters;
+                report[i].objective = reps[i].objective;
+                report[i].assign_seconds = reps[i].assignSeconds;
+                report[i].seconds = reps[i].seconds;
+            }
+        }
+        auto h = std::make_unique<tblaeq_handle>();
+        h->qh = std::make_unique<QueryHandler>(std::move(idx));
+        *out = h.release();
+        return TBLAEQ_OK;
+    });
+}
+
+int tblaeq_kmeans(const float* points, uint64_t n, uint64_t D, uint64_t k, const tblaeq_build_config* cfg,
+                  float* centroids_out, uint32_t* labels_out, double* objectives_out) {
+    if (!points) return fail(TBLAEQ_ERR_INVALID, "null points");
+    if (cfg && (cfg->precision < 0 || cfg->precision > 2)) return fail(TBLAEQ_ERR_INVALID, "bad precision");
+    return guarded([&]() -> int {
+        const KmeansConfig c = kmeansConfigOf(cfg);
+        cudaStream_t s = nullptr;
+        TBLAEQ_CUDA(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+        try {
+            DeviceMem dX(n * D * 4), C, L;
+            TBLAEQ_CUDA(cudaMemcpyAsync(dX.get(), points, n * D * 4, cudaMemcpyHostToDevice, s));
+            KmeansLevelReport rep;
+            kmeansRun(dX.as<float>(), n, D, k, c, C, L, rep, s);
+            if (centroids_out) TBLAEQ_CUDA(cudaMemcpyAsync(centroids_out, C.get(), k * D * 4, cudaMemcpyDeviceToHost, s));
+            if (labels_out) TBLAEQ_CUDA(cudaMemcpyAsync(labels_out, L.get(), n * 4, cudaMemcpyDeviceToHost, s));
+            TBLAEQ_CUDA(cudaStreamSynchronize(s));
+            if (objectives_out) std::copy(rep.objectives.begin(), rep.objectives.end(), objectives_out);
+        } catch (...) {
+            cudaStreamDestroy(s);
+            throw;
+        }
+        cudaStreamDestroy(s);
         return TBLAEQ_OK;
     });
 }

@@ -105,6 +105,8 @@ QueryHandler::QueryHandler(const std::string& indexPath, bool loadFromIndex) {
 
 QueryHandler::QueryHandler(const GenParams& gen) { host_ = std::make_unique<HostIndex>(generateRandomIndex(gen)); }
 
+QueryHandler::QueryHandler(HostIndex&& built) { host_ = std::make_unique<HostIndex>(std::move(built)); }
+
 QueryHandler::~QueryHandler() = default;
 
 void QueryHandler::saveIndex(const std::string& dirPath) const { tblaeq::saveIndex(*host_, dirPath); }

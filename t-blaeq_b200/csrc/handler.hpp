@@ -105,6 +105,7 @@ class QueryHandler {
 public:
     explicit QueryHandler(const std::string& indexPath, bool loadFromIndex);
     explicit QueryHandler(const GenParams& gen);
+    explicit QueryHandler(HostIndex&& built);  // an index built in memory (k-means build)
     ~QueryHandler();
     QueryHandler(const QueryHandler&) = delete;
     QueryHandler& operator=(const QueryHandler&) = delete;

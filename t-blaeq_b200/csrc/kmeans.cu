@@ -1,0 +1,610 @@
+// Hierarchical k-means build (see kmeans.cuh).
+#include "kmeans.cuh"
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <limits>
+#include <numeric>
+#include <random>
+#include <stdexcept>
+#include <unordered_map>
+
+namespace tblaeq {
+
+namespace {
+
+// ---- tensor-core assignment: layout constants ---------------------------------------------------
+constexpr int kTileM = 128;                                  // points per tile = TMEM lanes
+constexpr int kTileN = 128;                                  // centroids per tile = TMEM columns per buffer
+constexpr int kKPad = 16;                                    // D <= 16, zero-padded; two K=8 TF32 MMAs
+constexpr int kImage = kTileM * kKPad * 4;                   // one K-major TF32 operand image: 8192 B
+constexpr int kPointTileBytes = 2 * kImage;                  // hi | lo
+constexpr int kCentTileBytes = 2 * kImage + kTileN * 4;      // hi | lo | ||c||^2 (FP32): 16896 B
+constexpr int kAssignThreads = 128;                          // 4 warps = the 4 TMEM lane quarters
+constexpr uint32_t kTmemCols = 2 * kTileN;                   // two accumulator buffers
+// Shared memory requested per CTA: enough that at most two CTAs share an SM, so the two sets of
+// 256 tensor-memory columns always fit and an allocation never waits.
+constexpr size_t kAssignSmem = 100 * 1024;
+constexpr uint32_t kSpinLimit = 1u << 22;                    // bounded mbarrier waits
+
+// Instruction descriptor of tcgen05.mma kind::tf32: D = F32 (bits 4-5 = 1), A = B = TF32 (bits 7-9,
+// 10-12 = 2), both K-major, N = 128 (bits 17-22 = N/8), M = 128 (bits 24-28 = M/16).
+constexpr uint32_t kIdesc = (1u << 4) | (2u << 7) | (2u << 10) | (static_cast<uint32_t>(kTileN >> 3) << 17) |
+                            (static_cast<uint32_t>(kTileM >> 4) << 24);
+
+// Byte offset of element (row r, column k) in a K-major, non-swizzled operand image: 8-row x
+// 16-byte core matrices (4 values per row), the four K quarters of a row group 128 B apart
+// (leading-dimension offset) and row groups 512 B apart (stride-dimension offset). One K=8 MMA
+// reads two K quarters; the second MMA starts 256 B further.
+__host__ __device__ constexpr uint32_t imageOffset(uint32_t r, uint32_t k) {
+    return (r >> 3) * 512u + (k >> 2) * 128u + (r & 7u) * 16u + (k & 3u) * 4u;
+}
+constexpr uint32_t kSecondK = 256;  // byte offset of K = 8..15 within an image row group
+
+__device__ __forceinline__ uint32_t smemAddr(const void* p) {
+    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+// Shared-memory matrix descriptor (sm100 version 1), no swizzle, LBO = 128 B, SBO = 512 B.
+__device__ __forceinline__ uint64_t ummaDesc(uint32_t saddr) {
+    return static_cast<uint64_t>((saddr & 0x3FFFFu) >> 4) | (static_cast<uint64_t>(128u >> 4) << 16) |
+           (static_cast<uint64_t>(512u >> 4) << 32) | (1ull << 46);
+}
+
+__device__ __forceinline__ void mbarInit(uint64_t* bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smemAddr(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbarExpectTx(uint64_t* bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smemAddr(bar)), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ bool mbarTryWait(uint64_t* bar, uint32_t phase) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\tselp.u32 %0, 1, 0, p;\n\t}\n"
+        : "=r"(ok)
+        : "r"(smemAddr(bar)), "r"(phase)
+        : "memory");
+    return ok != 0;
+}
+// Bounded wait for a phase of an mbarrier; false when it gave up.
+__device__ __forceinline__ bool mbarWait(uint64_t* bar, uint32_t phase) {
+    for (uint32_t i = 0; i < kSpinLimit; ++i)
+        if (mbarTryWait(bar, phase)) return true;
+    return false;
+}
+__device__ __forceinline__ void bulkLoad(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                     smemAddr(dst)),
+                 "l"(src), "r"(bytes), "r"(smemAddr(bar))
+                 : "memory");
+}
+__device__ __forceinline__ void tcFenceBefore() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void tcFenceAfter() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void mmaTf32(uint32_t dtmem, uint64_t adesc, uint64_t bdesc, uint32_t accumulate) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n" ::"r"(dtmem),
+        "l"(adesc), "l"(bdesc), "r"(kIdesc), "r"(accumulate), "r"(0u), "r"(0u), "r"(0u), "r"(0u)
+        : "memory");
+}
+__device__ __forceinline__ void mmaCommit(uint64_t* bar) {
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smemAddr(bar))
+                 : "memory");
+}
+__device__ __forceinline__ void tmemLoad32(uint32_t taddr, uint32_t (&r)[32]) {
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, "
+        "%15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31}, [%32];"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]),
+          "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]),
+          "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+        : "r"(taddr));
+}
+__device__ __forceinline__ void tmemWaitLoad() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
+
+// ---- packing ----------------------------------------------------------------------------------
+// v = h + l: h is v rounded to nearest-even at TF32 precision (10 fraction bits), l = v - h is
+// exact in FP32 and is read by the tensor core at TF32 precision, leaving ~2^-21 |v| unrepresented.
+__device__ __forceinline__ void splitTf32(float v, float& h, float& l) {
+    uint32_t u = __float_as_uint(v);
+    if ((u & 0x7f800000u) != 0x7f800000u) u = (u + 0xfffu + ((u >> 13) & 1u)) & 0xffffe000u;
+    h = __uint_as_float(u);
+    l = v - h;
+}
+
+// Points -> per 128-point tile: hi image | lo image (rows past n stay zero: the buffer is cleared).
+__global__ void packPointsKernel(const float* X, uint64_t n, int D, uint8_t* out) {
+    for (uint64_t p = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x; p < n;
+         p += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
+        uint8_t* base = out + (p / kTileM) * kPointTileBytes;
+        const uint32_t r = static_cast<uint32_t>(p % kTileM);
+        for (int k = 0; k < kKPad; ++k) {
+            float h, l;
+            splitTf32(k < D ? X[p * D + k] : 0.f, h, l);
+            *reinterpret_cast<float*>(base + imageOffset(r, k)) = h;
+            *reinterpret_cast<float*>(base + kImage + imageOffset(r, k)) = l;
+        }
+    }
+}
+
+// Centroids -> per 128-centroid tile: hi image | lo image | ||c||^2. Slots past k get zero rows and
+// an infinite norm, so they never win.
+__global__ void packCentroidsKernel(const float* C, uint64_t k, uint64_t kPad, int D, uint8_t* out) {
+    for (uint64_t c = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x; c < kPad;
+         c += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
+        uint8_t* base = out + (c / kTileN) * kCentTileBytes;
+        const uint32_t r = static_cast<uint32_t>(c % kTileN);
+        float nrm = INFINITY;
+        if (c < k) {
+            nrm = 0.f;
+            for (int d = 0; d < D; ++d) nrm = fmaf(C[c * D + d], C[c * D + d], nrm);
+        }
+        for (int kk = 0; kk < kKPad; ++kk) {
+            float h, l;
+            splitTf32((c < k && kk < D) ? C[c * D + kk] : 0.f, h, l);
+            *reinterpret_cast<float*>(base + imageOffset(r, kk)) = h;
+            *reinterpret_cast<float*>(base + kImage + imageOffset(r, kk)) = l;
+        }
+        reinterpret_cast<float*>(base + 2 * kImage)[r] = nrm;
+    }
+}
+
+// ---- tensor-core assignment ---------------------------------------------------------------------
+// One CTA per 128-point tile; it streams every centroid tile through two shared-memory stages
+// (bulk copies) and two tensor-memory accumulators, so the MMAs of tile t+1 run while the four
+// warps reduce tile t: thread i owns point row i (TMEM lane i) and keeps the smallest
+// ||c||^2 - 2 x.c (the argmin of ||x - c||^2) with four independent trackers for ILP.
+__global__ void __launch_bounds__(kAssignThreads, 1)
+    assignTcKernel(const uint8_t* points, const uint8_t* cents, uint64_t n, uint32_t nTiles, uint32_t* labels,
+                   uint32_t* status) {
+    extern __shared__ __align__(1024) uint8_t smem[];
+    uint8_t* sA = smem;
+    uint8_t* sB[2] = {smem + kPointTileBytes, smem + kPointTileBytes + kCentTileBytes};
+    // bars: [0] A loaded, [1 + s] stage s loaded, [3 + s] MMAs into accumulator s done
+    uint64_t* bars = reinterpret_cast<uint64_t*>(smem + kPointTileBytes + 2 * kCentTileBytes);
+    uint32_t* sTmem = reinterpret_cast<uint32_t*>(bars + 5);
+    volatile int* sAbort = reinterpret_cast<volatile int*>(sTmem + 1);
+    const int tid = threadIdx.x;
+    const int warp = tid >> 5;
+    const uint64_t tile = blockIdx.x;
+
+    if (tid == 0) {
+        for (int i = 0; i < 5; ++i) mbarInit(&bars[i], 1);
+        *sAbort = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smemAddr(sTmem)),
+                     "r"(kTmemCols)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    tcFenceBefore();
+    __syncthreads();
+    tcFenceAfter();
+    const uint32_t tbase = *sTmem;
+
+    // Thread 0 produces: loads and MMAs. Counters let an aborting CTA drain what is in flight.
+    uint32_t loads[2] = {0, 0}, loadWaits[2] = {0, 0}, mmas[2] = {0, 0};
+    if (tid == 0) {
+        mbarExpectTx(&bars[0], kPointTileBytes);
+        bulkLoad(sA, points + tile * kPointTileBytes, kPointTileBytes, &bars[0]);
+        for (uint32_t t = 0; t < 2 && t < nTiles; ++t) {
+            mbarExpectTx(&bars[1 + t], kCentTileBytes);
+            bulkLoad(sB[t], cents + static_cast<uint64_t>(t) * kCentTileBytes, kCentTileBytes, &bars[1 + t]);
+            ++loads[t];
+        }
+    }
+    const uint32_t a0 = smemAddr(sA);
+    auto issue = [&](uint32_t t) -> bool {  // thread 0: MMAs of centroid tile t into accumulator t & 1
+        const int s = t & 1;
+        if (t == 0 && !mbarWait(&bars[0], 0)) return false;
+        if (!mbarWait(&bars[1 + s], loadWaits[s] & 1u)) return false;
+        ++loadWaits[s];
+        tcFenceAfter();
+        const uint32_t b0 = smemAddr(sB[s]);
+        const uint32_t d = tbase + static_cast<uint32_t>(s * kTileN);
+        // x.c ~ xh.ch + xh.cl + xl.ch, each as two K=8 halves
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+            const uint32_t ko = h * kSecondK;
+            mmaTf32(d, ummaDesc(a0 + ko), ummaDesc(b0 + ko), h);
+            mmaTf32(d, ummaDesc(a0 + ko), ummaDesc(b0 + kImage + ko), 1);
+            mmaTf32(d, ummaDesc(a0 + kImage + ko), ummaDesc(b0 + ko), 1);
+        }
+        mmaCommit(&bars[3 + s]);
+        ++mmas[s];
+        return true;
+    };
+    if (tid == 0 && nTiles > 0 && !issue(0)) {
+        atomicOr(status, 1u);
+        *sAbort = 1;
+    }
+
+    float bv[4] = {INFINITY, INFINITY, INFINITY, INFINITY};
+    uint32_t bi[4] = {0, 0, 0, 0};
+    uint32_t mmaWaits[2] = {0, 0};
+    for (uint32_t t = 0; t < nTiles; ++t) {
+        const int s = t & 1;
+        if (tid == 0 && t + 1 < nTiles && !*sAbort && !issue(t + 1)) {
+            atomicOr(status, 1u);
+            *sAbort = 1;
+        }
+        bool ok = mbarWait(&bars[3 + s], mmaWaits[s] & 1u);
+        ++mmaWaits[s];
+        ok = __syncthreads_and(ok && !*sAbort) != 0;
+        if (!ok) {
+            if (tid == 0) {
+                atomicOr(status, 1u);
+                *sAbort = 1;
+            }
+            break;
+        }
+        tcFenceAfter();
+        const float* cn = reinterpret_cast<const float*>(sB[s] + 2 * kImage);
+        const uint32_t base = tbase + static_cast<uint32_t>(s * kTileN) + (static_cast<uint32_t>(warp * 32) << 16);
+#pragma unroll 1
+        for (int c0 = 0; c0 < kTileN; c0 += 32) {
+            uint32_t r[32];
+            tmemLoad32(base + static_cast<uint32_t>(c0), r);
+            tmemWaitLoad();
+            const uint32_t col0 = t * kTileN + static_cast<uint32_t>(c0);
+#pragma unroll
+            for (int j = 0; j < 32; j += 4) {
+                const float4 c4 = *reinterpret_cast<const float4*>(cn + c0 + j);
+                const float v0 = fmaf(-2.f, __uint_as_float(r[j]), c4.x);
+                const float v1 = fmaf(-2.f, __uint_as_float(r[j + 1]), c4.y);
+                const float v2 = fmaf(-2.f, __uint_as_float(r[j + 2]), c4.z);
+                const float v3 = fmaf(-2.f, __uint_as_float(r[j + 3]), c4.w);
+                if (v0 < bv[0]) { bv[0] = v0; bi[0] = col0 + j; }
+                if (v1 < bv[1]) { bv[1] = v1; bi[1] = col0 + j + 1; }
+                if (v2 < bv[2]) { bv[2] = v2; bi[2] = col0 + j + 2; }
+                if (v3 < bv[3]) { bv[3] = v3; bi[3] = col0 + j + 3; }
+            }
+        }
+        tcFenceBefore();
+        __syncthreads();
+        tcFenceAfter();
+        // Stage s has been read by the MMAs of tile t and by the epilogue: refill it with tile t+2.
+        if (tid == 0 && t + 2 < nTiles) {
+            mbarExpectTx(&bars[1 + s], kCentTileBytes);
+            bulkLoad(sB[s], cents + static_cast<uint64_t>(t + 2) * kCentTileBytes, kCentTileBytes, &bars[1 + s]);
+            ++loads[s];
+        }
+    }
+    // An aborted CTA first waits (bounded) for its own copies and MMAs still in flight.
+    if (tid == 0 && *sAbort) {
+        for (int s = 0; s < 2; ++s) {
+            while (loadWaits[s] < loads[s]) {
+                mbarWait(&bars[1 + s], loadWaits[s] & 1u);
+                ++loadWaits[s];
+            }
+            while (mmaWaits[s] < mmas[s]) {
+                mbarWait(&bars[3 + s], mmaWaits[s] & 1u);
+                ++mmaWaits[s];
+            }
+        }
+    }
+    tcFenceBefore();
+    __syncthreads();
+    tcFenceAfter();
+    if (warp == 0) {
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tbase), "r"(kTmemCols) : "memory");
+    }
+    // Merge the four trackers: smallest value, then smallest index.
+    float v = bv[0];
+    uint32_t b = bi[0];
+#pragma unroll
+    for (int q = 1; q < 4; ++q) {
+        if (bv[q] < v || (bv[q] == v && bi[q] < b)) {
+            v = bv[q];
+            b = bi[q];
+        }
+    }
+    const uint64_t p = tile * kTileM + static_cast<uint64_t>(tid);
+    if (p < n && !*sAbort) labels[p] = b;
+}
+
+// ---- CUDA-core assignment (FP32 or FP64) -------------------------------------------------------
+template <typename T>
+__global__ void __launch_bounds__(256) assignScalarKernel(const float* X, uint64_t n, int D, const T* C, uint64_t k,
+                                                          uint32_t* labels) {
+    constexpr int kChunk = 128;
+    extern __shared__ __align__(16) unsigned char smemRaw[];
+    T* sC = reinterpret_cast<T*>(smemRaw);
+    const uint64_t p = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x;
+    T x[32];
+    for (int d = 0; d < 32; ++d) x[d] = (p < n && d < D) ? static_cast<T>(X[p * D + d]) : T(0);
+    T best = std::numeric_limits<T>::infinity();
+    uint32_t bestI = 0;
+    for (uint64_t c0 = 0; c0 < k; c0 += kChunk) {
+        const uint64_t m = std::min<uint64_t>(kChunk, k - c0);
+        __syncthreads();
+        for (uint64_t i = threadIdx.x; i < m * D; i += blockDim.x) sC[i] = C[c0 * D + i];
+        __syncthreads();
+        for (uint64_t c = 0; c < m; ++c) {
+            T dist = 0;
+            for (int d = 0; d < D; ++d) {
+                const T diff = x[d] - sC[c * D + d];
+                if constexpr (sizeof(T) == 4) {
+                    dist = __fmaf_rn(diff, diff, dist);
+                } else {
+                    dist = __fma_rn(diff, diff, dist);
+                }
+            }
+            if (dist < best) {
+                best = dist;
+                bestI = static_cast<uint32_t>(c0 + c);
+            }
+        }
+    }
+    if (p < n) labels[p] = bestI;
+}
+
+// ---- update and objective -----------------------------------------------------------------------
+__global__ void accumulateKernel(const float* X, const uint32_t* labels, uint64_t n, int D, double* sums,
+                                 unsigned long long* counts) {
+    for (uint64_t p = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x; p < n;
+         p += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
+        const uint32_t l = labels[p];
+        atomicAdd(&counts[l], 1ull);
+        for (int d = 0; d < D; ++d) atomicAdd(&sums[static_cast<uint64_t>(l) * D + d], static_cast<double>(X[p * D + d]));
+    }
+}
+
+// Moves each centroid with points to their mean (FP64), keeps empty ones.
+__global__ void finalizeKernel(const double* sums, const unsigned long long* counts, uint64_t k, int D, double* Cd,
+                               float* C) {
+    for (uint64_t i = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x; i < k * D;
+         i += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
+        const uint64_t c = i / D;
+        if (counts[c] > 0) {
+            const double v = sums[i] / static_cast<double>(counts[c]);
+            Cd[i] = v;
+            C[i] = static_cast<float>(v);
+        }
+    }
+}
+
+__global__ void objectiveKernel(const float* X, const uint32_t* labels, const double* Cd, uint64_t n, int D,
+                                double* out) {
+    __shared__ double part[256 / 32];
+    double acc = 0.0;
+    for (uint64_t p = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x; p < n;
+         p += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
+        const double* c = Cd + static_cast<uint64_t>(labels[p]) * D;
+        for (int d = 0; d < D; ++d) {
+            const double diff = static_cast<double>(X[p * D + d]) - c[d];
+            acc = fma(diff, diff, acc);
+        }
+    }
+    for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+    if ((threadIdx.x & 31) == 0) part[threadIdx.x >> 5] = acc;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double s = 0.0;
+        for (int w = 0; w < static_cast<int>(blockDim.x / 32); ++w) s += part[w];
+        atomicAdd(out, s);
+    }
+}
+
+__global__ void gatherKernel(const float* X, const uint64_t* idx, uint64_t k, int D, double* Cd, float* C) {
+    for (uint64_t i = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x; i < k * D;
+         i += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
+        const float v = X[idx[i / D] * D + i % D];
+        C[i] = v;
+        Cd[i] = static_cast<double>(v);
+    }
+}
+
+int gridFor(uint64_t work, int threads) {
+    return static_cast<int>(std::max<uint64_t>(1, std::min<uint64_t>((work + threads - 1) / threads, 148ull * 32)));
+}
+
+// Assembles interval pIdx of the index from one level's labels, like the reference's
+// Genenate_One_P_Tensor + Compute_Max_Radius: rows grouped by label (in input order within a
+// label), values fine / coarse, radius = largest distance from a centroid to its members.
+void assembleInterval(HostIndex& idx, uint64_t pIdx, uint64_t fineMesh, const float* fine, uint64_t nF,
+                      const float* coarse, uint64_t nC, const uint32_t* labels) {
+    const uint64_t D = idx.D;
+    PTensor& P = idx.pTensors[pIdx];
+    P.D = D;
+    P.rows = nF;
+    P.cols = nC;
+    P.nnz = nF;
+    P.isAos = 1;
+    P.nnzPerCol.assign(nC, 0);
+    for (uint64_t i = 0; i < nF; ++i) ++P.nnzPerCol[labels[i]];
+    P.colRes.assign(nC + 1, 0);
+    for (uint64_t c = 0; c < nC; ++c) P.colRes[c + 1] = P.colRes[c] + P.nnzPerCol[c];
+    P.rowIds.resize(nF);
+    std::iota(P.rowIds.begin(), P.rowIds.end(), uint64_t{0});
+    std::vector<uint64_t> order(nF), next(P.colRes.begin(), P.colRes.end() - 1);
+    for (uint64_t i = 0; i < nF; ++i) order[next[labels[i]]++] = i;
+    P.vals.resize(nF * D);
+    idx.radius[pIdx].assign(nC, 0.0);
+    const int64_t cols = static_cast<int64_t>(nC);
+    bool zeroCoord = false;
+#pragma omp parallel for schedule(dynamic, 256) reduction(|| : zeroCoord)
+    for (int64_t c = 0; c < cols; ++c) {
+        double maxDist = 0.0;
+        for (uint64_t pos = P.colRes[c]; pos < P.colRes[c + 1]; ++pos) {
+            const float* fv = fine + order[pos] * D;
+            double sum = 0.0;
+            for (uint64_t d = 0; d < D; ++d) {
+                const double cv = static_cast<double>(coarse[c * D + d]);
+                const double f = static_cast<double>(fv[d]);
+                if (cv == 0.0) zeroCoord = true;
+                P.vals[pos * D + d] = f / cv;
+                const double diff = cv - f;
+                sum += diff * diff;
+            }
+            maxDist = std::max(maxDist, std::sqrt(sum));
+        }
+        idx.radius[pIdx][c] = maxDist;
+    }
+    if (zeroCoord) throw std::runtime_error("division by zero in P-tensor build: a centroid coordinate is 0");
+    idx.maps[fineMesh] = std::move(order);
+}
+
+}  // namespace
+
+void kmeansRun(const float* dX, uint64_t n, uint64_t D, uint64_t k, const KmeansConfig& cfg, DeviceMem& centroids,
+               DeviceMem& labels, KmeansLevelReport& report, cudaStream_t s) {
+    if (n == 0 || k == 0 || k > n) throw std::invalid_argument("k-means needs 0 < k <= n");
+    if (D == 0 || D > 32) throw std::invalid_argument("k-means supports 1 <= D <= 32");
+    if (k > 0xffffffffull || n > (1ull << 40)) throw std::invalid_argument("k-means sizes out of range");
+    int precision = cfg.precision;
+    if (precision == kKmTensor && !kmeansTensorSupports(D)) precision = kKmFp32;
+    report.n = n;
+    report.k = k;
+    report.iters = cfg.iters;
+    report.objectives.clear();
+    const int Di = static_cast<int>(D);
+
+    // Initial centroids: k distinct data points, chosen with a seeded partial Fisher-Yates shuffle.
+    std::vector<uint64_t> pick(k);
+    {
+        std::mt19937_64 rng(cfg.seed);
+        std::unordered_map<uint64_t, uint64_t> swapped;
+        for (uint64_t i = 0; i < k; ++i) {
+            const uint64_t j = i + std::uniform_int_distribution<uint64_t>(0, n - 1 - i)(rng);
+            auto vi = swapped.find(i), vj = swapped.find(j);
+            const uint64_t a = vi == swapped.end() ? i : vi->second, b = vj == swapped.end() ? j : vj->second;
+            pick[i] = b;
+            swapped[j] = a;
+        }
+    }
+    DeviceMem dPick = upload(pick, s);
+    centroids.alloc(k * D * 4);
+    DeviceMem Cd(k * D * 8), sums(k * D * 8), counts(k * 8), obj(8);
+    labels.alloc(n * 4);
+    gatherKernel<<<gridFor(k * D, 256), 256, 0, s>>>(dX, dPick.as<uint64_t>(), k, Di, Cd.as<double>(), centroids.as<float>());
+    TBLAEQ_CUDA(cudaGetLastError());
+
+    const uint64_t nTilesP = (n + kTileM - 1) / kTileM, nTilesC = (k + kTileN - 1) / kTileN;
+    DeviceMem packedP, packedC, status(4);
+    if (precision == kKmTensor) {
+        packedP.alloc(nTilesP * kPointTileBytes);
+        packedC.alloc(nTilesC * kCentTileBytes);
+        TBLAEQ_CUDA(cudaMemsetAsync(packedP.get(), 0, nTilesP * kPointTileBytes, s));
+        packPointsKernel<<<gridFor(n, 256), 256, 0, s>>>(dX, n, Di, packedP.as<uint8_t>());
+        TBLAEQ_CUDA(cudaGetLastError());
+        TBLAEQ_CUDA(cudaFuncSetAttribute(assignTcKernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         static_cast<int>(kAssignSmem)));
+    }
+    TBLAEQ_CUDA(cudaMemsetAsync(status.get(), 0, 4, s));
+    cudaEvent_t e0, e1;
+    TBLAEQ_CUDA(cudaEventCreate(&e0));
+    TBLAEQ_CUDA(cudaEventCreate(&e1));
+    double assignMs = 0.0;
+    for (int it = 0; it < cfg.iters; ++it) {
+        TBLAEQ_CUDA(cudaEventRecord(e0, s));
+        if (precision == kKmTensor) {
+            packCentroidsKernel<<<gridFor(nTilesC * kTileN, 256), 256, 0, s>>>(centroids.as<float>(), k,
+                                                                              nTilesC * kTileN, Di,
+                                                                              packedC.as<uint8_t>());
+            TBLAEQ_CUDA(cudaGetLastError());
+            assignTcKernel<<<static_cast<unsigned>(nTilesP), kAssignThreads, kAssignSmem, s>>>(
+                packedP.as<uint8_t>(), packedC.as<uint8_t>(), n, static_cast<uint32_t>(nTilesC), labels.as<uint32_t>(),
+                status.as<uint32_t>());
+        } else if (precision == kKmFp32) {
+            assignScalarKernel<float><<<static_cast<unsigned>((n + 255) / 256), 256, 128 * D * 4, s>>>(
+                dX, n, Di, centroids.as<float>(), k, labels.as<uint32_t>());
+        } else {
+            assignScalarKernel<double><<<static_cast<unsigned>((n + 255) / 256), 256, 128 * D * 8, s>>>(
+                dX, n, Di, Cd.as<double>(), k, labels.as<uint32_t>());
+        }
+        TBLAEQ_CUDA(cudaGetLastError());
+        TBLAEQ_CUDA(cudaEventRecord(e1, s));
+        TBLAEQ_CUDA(cudaMemsetAsync(sums.get(), 0, k * D * 8, s));
+        TBLAEQ_CUDA(cudaMemsetAsync(counts.get(), 0, k * 8, s));
+        accumulateKernel<<<gridFor(n, 256), 256, 0, s>>>(dX, labels.as<uint32_t>(), n, Di, sums.as<double>(),
+                                                         counts.as<unsigned long long>());
+        finalizeKernel<<<gridFor(k * D, 256), 256, 0, s>>>(sums.as<double>(), counts.as<unsigned long long>(), k, Di,
+                                                           Cd.as<double>(), centroids.as<float>());
+        TBLAEQ_CUDA(cudaMemsetAsync(obj.get(), 0, 8, s));
+        objectiveKernel<<<gridFor(n, 256), 256, 0, s>>>(dX, labels.as<uint32_t>(), Cd.as<double>(), n, Di,
+                                                        obj.as<double>());
+        TBLAEQ_CUDA(cudaGetLastError());
+        double o = 0.0;
+        uint32_t st = 0;
+        TBLAEQ_CUDA(cudaMemcpyAsync(&o, obj.get(), 8, cudaMemcpyDeviceToHost, s));
+        TBLAEQ_CUDA(cudaMemcpyAsync(&st, status.get(), 4, cudaMemcpyDeviceToHost, s));
+        TBLAEQ_CUDA(cudaStreamSynchronize(s));
+        if (st) throw CudaError(cudaErrorLaunchTimeout, "k-means assignment kernel gave up waiting (status " +
+                                                            std::to_string(st) + ")");
+        float ms = 0.f;
+        TBLAEQ_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+        assignMs += ms;
+        report.objectives.push_back(o);
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    report.objective = report.objectives.empty() ? 0.0 : report.objectives.back();
+    report.assignSeconds = assignMs / 1e3;
+}
+
+HostIndex kmeansBuild(const float* hostPoints, uint64_t N, uint64_t D, uint64_t height,
+                      const std::vector<uint64_t>& ratios, const KmeansConfig& cfg,
+                      std::vector<KmeansLevelReport>& reports, cudaStream_t s) {
+    if (height < 2) throw std::invalid_argument("k-means build: height must be >= 2");
+    if (ratios.size() != height - 1) throw std::invalid_argument("k-means build: ratios size must equal height - 1");
+    if (!hostPoints || N == 0 || D == 0) throw std::invalid_argument("k-means build: no points");
+    HostIndex idx;
+    idx.D = D;
+    idx.N = N;
+    idx.height = height;
+    idx.intervals = height - 1;
+    idx.isAos = 1;
+    idx.ratios = ratios;
+    idx.pTensors.resize(idx.intervals);
+    idx.radius.resize(idx.intervals);
+    idx.maps.resize(height);
+    idx.datasetName = "Kmeans" + std::to_string(N) + "D" + std::to_string(D);
+    reports.assign(idx.intervals, KmeansLevelReport{});
+
+    DeviceMem dX(N * D * 4);
+    TBLAEQ_CUDA(cudaMemcpyAsync(dX.get(), hostPoints, N * D * 4, cudaMemcpyHostToDevice, s));
+    std::vector<float> fineHost;  // the current level's data on the host (the points for level 0)
+    const float* fine = hostPoints;
+    uint64_t n = N;
+    for (uint64_t i = 0; i < idx.intervals; ++i) {
+        const auto t0 = std::chrono::steady_clock::now();
+        const uint64_t k = (ratios[i] == 0 || n / ratios[i] == 0) ? 1 : n / ratios[i];  // IndexBuilder.cu:14-19
+        const uint64_t fineMesh = idx.intervals - i, pIdx = fineMesh - 1;
+        idx.meshSizes.push_back(n);
+        DeviceMem C, L;
+        KmeansConfig c = cfg;
+        c.seed = cfg.seed + i;
+        kmeansRun(dX.as<float>(), n, D, k, c, C, L, reports[i], s);
+        std::vector<float> coarse(k * D);
+        std::vector<uint32_t> labels(n);
+        TBLAEQ_CUDA(cudaMemcpyAsync(coarse.data(), C.get(), k * D * 4, cudaMemcpyDeviceToHost, s));
+        TBLAEQ_CUDA(cudaMemcpyAsync(labels.data(), L.get(), n * 4, cudaMemcpyDeviceToHost, s));
+        TBLAEQ_CUDA(cudaStreamSynchronize(s));
+        assembleInterval(idx, pIdx, fineMesh, fine, n, coarse.data(), k, labels.data());
+        if (i + 2 == height) {
+            idx.meshSizes.push_back(k);
+            idx.coarsest.rows = k;
+            idx.coarsest.dim = D;
+            idx.coarsest.nnz = k;
+            idx.coarsest.isAos = 1;
+            idx.coarsest.ids.resize(k);
+            std::iota(idx.coarsest.ids.begin(), idx.coarsest.ids.end(), uint64_t{0});
+            idx.coarsest.vals.assign(coarse.begin(), coarse.end());
+        }
+        // The centroids are the next level's data.
+        fineHost = std::move(coarse);
+        fine = fineHost.data();
+        dX = std::move(C);
+        n = k;
+        reports[i].seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    }
+    idx.validate();
+    return idx;
+}
+
+}  // namespace tblaeq
