@@ -154,10 +154,25 @@ __global__ void packCentroidsKernel(const float* C, uint64_t k, uint64_t kPad, i
 // ---- tensor-core assignment ---------------------------------------------------------------------
 // One CTA per 128-point tile; it streams every centroid tile through two shared-memory stages
 // (bulk copies) and two tensor-memory accumulators, so the MMAs of tile t+1 run while the four
-// warps reduce tile t: thread i owns point row i (TMEM lane i) and keeps the smallest
-// ||c||^2 - 2 x.c (the argmin of ||x - c||^2) with four independent trackers for ILP.
+// warps reduce tile t: thread i owns point row i (TMEM lane i) and keeps the two smallest
+// ||c||^2 - 2 x.c (the two nearest centroids) with two independent trackers for ILP. An FP64
+// step then picks between the two candidates.
+__device__ __forceinline__ void keepTwo(float v, uint32_t i, float& s1, uint32_t& i1, float& s2, uint32_t& i2) {
+    if (v < s2) {
+        if (v < s1) {
+            s2 = s1;
+            i2 = i1;
+            s1 = v;
+            i1 = i;
+        } else {
+            s2 = v;
+            i2 = i;
+        }
+    }
+}
+
 __global__ void __launch_bounds__(kAssignThreads, 1)
-    assignTcKernel(const uint8_t* points, const uint8_t* cents, uint64_t n, uint32_t nTiles, uint32_t* labels,
+    assignTcKernel(const uint8_t* points, const uint8_t* cents, uint64_t n, uint32_t nTiles, uint2* cand,
                    uint32_t* status) {
     extern __shared__ __align__(1024) uint8_t smem[];
     uint8_t* sA = smem;
@@ -223,8 +238,9 @@ __global__ void __launch_bounds__(kAssignThreads, 1)
         *sAbort = 1;
     }
 
-    float bv[4] = {INFINITY, INFINITY, INFINITY, INFINITY};
-    uint32_t bi[4] = {0, 0, 0, 0};
+    // two trackers (even / odd columns), each with its best and second best
+    float a1 = INFINITY, a2 = INFINITY, b1 = INFINITY, b2 = INFINITY;
+    uint32_t ai1 = 0, ai2 = 0, bi1 = 0, bi2 = 0;
     uint32_t mmaWaits[2] = {0, 0};
     for (uint32_t t = 0; t < nTiles; ++t) {
         const int s = t & 1;
@@ -258,10 +274,10 @@ __global__ void __launch_bounds__(kAssignThreads, 1)
                 const float v1 = fmaf(-2.f, __uint_as_float(r[j + 1]), c4.y);
                 const float v2 = fmaf(-2.f, __uint_as_float(r[j + 2]), c4.z);
                 const float v3 = fmaf(-2.f, __uint_as_float(r[j + 3]), c4.w);
-                if (v0 < bv[0]) { bv[0] = v0; bi[0] = col0 + j; }
-                if (v1 < bv[1]) { bv[1] = v1; bi[1] = col0 + j + 1; }
-                if (v2 < bv[2]) { bv[2] = v2; bi[2] = col0 + j + 2; }
-                if (v3 < bv[3]) { bv[3] = v3; bi[3] = col0 + j + 3; }
+                keepTwo(v0, col0 + j, a1, ai1, a2, ai2);
+                keepTwo(v1, col0 + j + 1, b1, bi1, b2, bi2);
+                keepTwo(v2, col0 + j + 2, a1, ai1, a2, ai2);
+                keepTwo(v3, col0 + j + 3, b1, bi1, b2, bi2);
             }
         }
         tcFenceBefore();
@@ -293,18 +309,29 @@ __global__ void __launch_bounds__(kAssignThreads, 1)
     if (warp == 0) {
         asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tbase), "r"(kTmemCols) : "memory");
     }
-    // Merge the four trackers: smallest value, then smallest index.
-    float v = bv[0];
-    uint32_t b = bi[0];
-#pragma unroll
-    for (int q = 1; q < 4; ++q) {
-        if (bv[q] < v || (bv[q] == v && bi[q] < b)) {
-            v = bv[q];
-            b = bi[q];
-        }
-    }
+    // Merge the trackers into the overall two best.
+    keepTwo(b1, bi1, a1, ai1, a2, ai2);
+    keepTwo(b2, bi2, a1, ai1, a2, ai2);
     const uint64_t p = tile * kTileM + static_cast<uint64_t>(tid);
-    if (p < n && !*sAbort) labels[p] = b;
+    if (p < n && !*sAbort) cand[p] = make_uint2(ai1, a2 < INFINITY ? ai2 : ai1);
+}
+
+// FP64 choice between the two tensor-core candidates of every point (ties: the smaller index).
+__global__ void refineKernel(const float* X, const uint2* cand, const double* Cd, uint64_t n, int D,
+                             uint32_t* labels) {
+    for (uint64_t p = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x; p < n;
+         p += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
+        const uint2 c = cand[p];
+        double d0 = 0.0, d1 = 0.0;
+        for (int d = 0; d < D; ++d) {
+            const double x = static_cast<double>(X[p * D + d]);
+            const double e0 = x - Cd[static_cast<uint64_t>(c.x) * D + d];
+            const double e1 = x - Cd[static_cast<uint64_t>(c.y) * D + d];
+            d0 = __fma_rn(e0, e0, d0);
+            d1 = __fma_rn(e1, e1, d1);
+        }
+        labels[p] = (d1 < d0 || (d1 == d0 && c.y < c.x)) ? c.y : c.x;
+    }
 }
 
 // ---- CUDA-core assignment (FP32 or FP64) -------------------------------------------------------
@@ -485,8 +512,9 @@ void kmeansRun(const float* dX, uint64_t n, uint64_t D, uint64_t k, const Kmeans
     TBLAEQ_CUDA(cudaGetLastError());
 
     const uint64_t nTilesP = (n + kTileM - 1) / kTileM, nTilesC = (k + kTileN - 1) / kTileN;
-    DeviceMem packedP, packedC, status(4);
+    DeviceMem packedP, packedC, cand, status(4);
     if (precision == kKmTensor) {
+        cand.alloc(n * 8);
         packedP.alloc(nTilesP * kPointTileBytes);
         packedC.alloc(nTilesC * kCentTileBytes);
         TBLAEQ_CUDA(cudaMemsetAsync(packedP.get(), 0, nTilesP * kPointTileBytes, s));
@@ -508,8 +536,11 @@ void kmeansRun(const float* dX, uint64_t n, uint64_t D, uint64_t k, const Kmeans
                                                                               packedC.as<uint8_t>());
             TBLAEQ_CUDA(cudaGetLastError());
             assignTcKernel<<<static_cast<unsigned>(nTilesP), kAssignThreads, kAssignSmem, s>>>(
-                packedP.as<uint8_t>(), packedC.as<uint8_t>(), n, static_cast<uint32_t>(nTilesC), labels.as<uint32_t>(),
+                packedP.as<uint8_t>(), packedC.as<uint8_t>(), n, static_cast<uint32_t>(nTilesC), cand.as<uint2>(),
                 status.as<uint32_t>());
+            TBLAEQ_CUDA(cudaGetLastError());
+            refineKernel<<<gridFor(n, 256), 256, 0, s>>>(dX, cand.as<uint2>(), Cd.as<double>(), n, Di,
+                                                         labels.as<uint32_t>());
         } else if (precision == kKmFp32) {
             assignScalarKernel<float><<<static_cast<unsigned>((n + 255) / 256), 256, 128 * D * 4, s>>>(
                 dX, n, Di, centroids.as<float>(), k, labels.as<uint32_t>());
