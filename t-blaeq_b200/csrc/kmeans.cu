@@ -21,7 +21,7 @@ constexpr int kKPad = 16;                                    // D <= 16, zero-pa
 constexpr int kImage = kTileM * kKPad * 4;                   // one K-major TF32 operand image: 8192 B
 constexpr int kPointTileBytes = 2 * kImage;                  // hi | lo
 constexpr int kCentTileBytes = 2 * kImage + kTileN * 4;      // hi | lo | ||c||^2 (FP32): 16896 B
-constexpr int kAssignThreads = 128;                          // 4 warps = the 4 TMEM lane quarters
+constexpr int kAssignThreads = 256;  // 8 warps: two per TMEM lane quarter, each reducing half the columns
 constexpr uint32_t kTmemCols = 2 * kTileN;                   // two accumulator buffers
 // Shared memory requested per CTA: enough that at most two CTAs share an SM, so the two sets of
 // 256 tensor-memory columns always fit and an allocation never waits.
@@ -153,10 +153,12 @@ __global__ void packCentroidsKernel(const float* C, uint64_t k, uint64_t kPad, i
 
 // ---- tensor-core assignment ---------------------------------------------------------------------
 // One CTA per 128-point tile; it streams every centroid tile through two shared-memory stages
-// (bulk copies) and two tensor-memory accumulators, so the MMAs of tile t+1 run while the four
-// warps reduce tile t: thread i owns point row i (TMEM lane i) and keeps the two smallest
-// ||c||^2 - 2 x.c (the two nearest centroids) with two independent trackers for ILP. An FP64
-// step then picks between the two candidates.
+// (bulk copies) and two tensor-memory accumulators, so the MMAs of tile t+1 run while the eight
+// warps reduce tile t. Warps w and w+4 read TMEM lane quarter w (point rows 32w..32w+31), each half
+// of the columns, and keep the two smallest ||c||^2 - 2 x.c (the two nearest centroids): per
+// 32-column chunk one fused multiply-add and one min per value, and the top-2 update only for
+// chunks whose minimum beats the current second best (rare once the first tiles have passed).
+// The halves merge through shared memory; an FP64 step then picks between the two candidates.
 __device__ __forceinline__ void keepTwo(float v, uint32_t i, float& s1, uint32_t& i1, float& s2, uint32_t& i2) {
     if (v < s2) {
         if (v < s1) {
@@ -171,7 +173,7 @@ __device__ __forceinline__ void keepTwo(float v, uint32_t i, float& s1, uint32_t
     }
 }
 
-__global__ void __launch_bounds__(kAssignThreads, 1)
+__global__ void __launch_bounds__(kAssignThreads, 2)
     assignTcKernel(const uint8_t* points, const uint8_t* cents, uint64_t n, uint32_t nTiles, uint2* cand,
                    uint32_t* status) {
     extern __shared__ __align__(1024) uint8_t smem[];
@@ -238,9 +240,9 @@ __global__ void __launch_bounds__(kAssignThreads, 1)
         *sAbort = 1;
     }
 
-    // two trackers (even / odd columns), each with its best and second best
-    float a1 = INFINITY, a2 = INFINITY, b1 = INFINITY, b2 = INFINITY;
-    uint32_t ai1 = 0, ai2 = 0, bi1 = 0, bi2 = 0;
+    float s1 = INFINITY, s2 = INFINITY;
+    uint32_t i1 = 0, i2 = 0;
+    const int half = warp >> 2;  // which 64 columns of every tile this warp reduces
     uint32_t mmaWaits[2] = {0, 0};
     for (uint32_t t = 0; t < nTiles; ++t) {
         const int s = t & 1;
@@ -259,25 +261,38 @@ __global__ void __launch_bounds__(kAssignThreads, 1)
             break;
         }
         tcFenceAfter();
-        const float* cn = reinterpret_cast<const float*>(sB[s] + 2 * kImage);
-        const uint32_t base = tbase + static_cast<uint32_t>(s * kTileN) + (static_cast<uint32_t>(warp * 32) << 16);
-#pragma unroll 1
-        for (int c0 = 0; c0 < kTileN; c0 += 32) {
-            uint32_t r[32];
-            tmemLoad32(base + static_cast<uint32_t>(c0), r);
+        const float* cn = reinterpret_cast<const float*>(sB[s] + 2 * kImage) + half * 64;
+        const uint32_t base = tbase + static_cast<uint32_t>(s * kTileN + half * 64) +
+                              (static_cast<uint32_t>((warp & 3) * 32) << 16);
+        uint32_t r[64];
+        {
+            uint32_t (&r0)[32] = *reinterpret_cast<uint32_t(*)[32]>(&r[0]);
+            uint32_t (&r1)[32] = *reinterpret_cast<uint32_t(*)[32]>(&r[32]);
+            tmemLoad32(base, r0);
+            tmemLoad32(base + 32u, r1);
             tmemWaitLoad();
-            const uint32_t col0 = t * kTileN + static_cast<uint32_t>(c0);
+        }
+        const uint32_t col0 = t * kTileN + static_cast<uint32_t>(half * 64);
+#pragma unroll
+        for (int c = 0; c < 64; c += 32) {
+            float m0 = INFINITY, m1 = INFINITY;
 #pragma unroll
             for (int j = 0; j < 32; j += 4) {
-                const float4 c4 = *reinterpret_cast<const float4*>(cn + c0 + j);
-                const float v0 = fmaf(-2.f, __uint_as_float(r[j]), c4.x);
-                const float v1 = fmaf(-2.f, __uint_as_float(r[j + 1]), c4.y);
-                const float v2 = fmaf(-2.f, __uint_as_float(r[j + 2]), c4.z);
-                const float v3 = fmaf(-2.f, __uint_as_float(r[j + 3]), c4.w);
-                keepTwo(v0, col0 + j, a1, ai1, a2, ai2);
-                keepTwo(v1, col0 + j + 1, b1, bi1, b2, bi2);
-                keepTwo(v2, col0 + j + 2, a1, ai1, a2, ai2);
-                keepTwo(v3, col0 + j + 3, b1, bi1, b2, bi2);
+                const float4 c4 = *reinterpret_cast<const float4*>(cn + c + j);
+                const float v0 = fmaf(-2.f, __uint_as_float(r[c + j]), c4.x);
+                const float v1 = fmaf(-2.f, __uint_as_float(r[c + j + 1]), c4.y);
+                const float v2 = fmaf(-2.f, __uint_as_float(r[c + j + 2]), c4.z);
+                const float v3 = fmaf(-2.f, __uint_as_float(r[c + j + 3]), c4.w);
+                r[c + j] = __float_as_uint(v0);
+                r[c + j + 1] = __float_as_uint(v1);
+                r[c + j + 2] = __float_as_uint(v2);
+                r[c + j + 3] = __float_as_uint(v3);
+                m0 = fminf(m0, fminf(v0, v1));
+                m1 = fminf(m1, fminf(v2, v3));
+            }
+            if (fminf(m0, m1) < s2) {
+#pragma unroll
+                for (int j = 0; j < 32; ++j) keepTwo(__uint_as_float(r[c + j]), col0 + c + j, s1, i1, s2, i2);
             }
         }
         tcFenceBefore();
@@ -309,11 +324,23 @@ __global__ void __launch_bounds__(kAssignThreads, 1)
     if (warp == 0) {
         asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tbase), "r"(kTmemCols) : "memory");
     }
-    // Merge the trackers into the overall two best.
-    keepTwo(b1, bi1, a1, ai1, a2, ai2);
-    keepTwo(b2, bi2, a1, ai1, a2, ai2);
-    const uint64_t p = tile * kTileM + static_cast<uint64_t>(tid);
-    if (p < n && !*sAbort) cand[p] = make_uint2(ai1, a2 < INFINITY ? ai2 : ai1);
+    // Merge the two column halves of every row through shared memory (the operand stages are idle).
+    float* mv = reinterpret_cast<float*>(sB[0]);
+    uint32_t* mi = reinterpret_cast<uint32_t*>(sB[0] + 2 * kTileM * 4);
+    const int row = (warp & 3) * 32 + (tid & 31);
+    if (half == 1) {
+        mv[2 * row] = s1;
+        mv[2 * row + 1] = s2;
+        mi[2 * row] = i1;
+        mi[2 * row + 1] = i2;
+    }
+    __syncthreads();
+    if (half == 0) {
+        keepTwo(mv[2 * row], mi[2 * row], s1, i1, s2, i2);
+        keepTwo(mv[2 * row + 1], mi[2 * row + 1], s1, i1, s2, i2);
+        const uint64_t p = tile * kTileM + static_cast<uint64_t>(row);
+        if (p < n && !*sAbort) cand[p] = make_uint2(i1, s2 < INFINITY ? i2 : i1);
+    }
 }
 
 // FP64 choice between the two tensor-core candidates of every point (ties: the smaller index).
