@@ -21,7 +21,7 @@ constexpr int kKPad = 16;                                    // D <= 16, zero-pa
 constexpr int kImage = kTileM * kKPad * 4;                   // one K-major TF32 operand image: 8192 B
 constexpr int kPointTileBytes = 2 * kImage;                  // hi | lo
 constexpr int kCentTileBytes = 2 * kImage + kTileN * 4;      // hi | lo | ||c||^2 (FP32): 16896 B
-constexpr int kAssignThreads = 256;  // 8 warps: two per TMEM lane quarter, each reducing half the columns
+constexpr int kAssignThreads = 288;  // 8 consumer warps (two per TMEM lane quarter) + 1 producer warp
 constexpr uint32_t kTmemCols = 2 * kTileN;                   // two accumulator buffers
 // Shared memory requested per CTA: enough that at most two CTAs share an SM, so the two sets of
 // 256 tensor-memory columns always fit and an allocation never waits.
@@ -152,13 +152,20 @@ __global__ void packCentroidsKernel(const float* C, uint64_t k, uint64_t kPad, i
 }
 
 // ---- tensor-core assignment ---------------------------------------------------------------------
-// One CTA per 128-point tile; it streams every centroid tile through two shared-memory stages
-// (bulk copies) and two tensor-memory accumulators, so the MMAs of tile t+1 run while the eight
-// warps reduce tile t. Warps w and w+4 read TMEM lane quarter w (point rows 32w..32w+31), each half
-// of the columns, and keep the two smallest ||c||^2 - 2 x.c (the two nearest centroids): per
-// 32-column chunk one fused multiply-add and one min per value, and the top-2 update only for
-// chunks whose minimum beats the current second best (rare once the first tiles have passed).
-// The halves merge through shared memory; an FP64 step then picks between the two candidates.
+// One CTA per 128-point tile, warp-specialised. The producer warp (warp 8, one lane) streams the
+// centroid tiles through four shared-memory stages with bulk copies and issues the six TF32 MMAs of
+// each tile into one of two tensor-memory accumulators. Eight consumer warps reduce: warps w and
+// w+4 read TMEM lane quarter w (point rows 32w..32w+31), each half of the columns, and keep the two
+// smallest ||c||^2 - 2 x.c (the two nearest centroids): per 32-column chunk one fused multiply-add
+// and one min per value, and the top-2 update only when a lane's chunk minimum beats its current
+// second best (rare once the first tiles have passed). Hand-offs are mbarriers: a stage is
+// "full" when its copy lands, an accumulator "done" when its MMAs commit, and both are "free"
+// again once all eight consumer warps have arrived; no CTA-wide barrier runs per tile. The two
+// column halves merge through shared memory at the end, and an FP64 step then picks between the
+// two candidates of every point.
+constexpr int kStages = 4;
+constexpr int kConsumerWarps = 8;
+
 __device__ __forceinline__ void keepTwo(float v, uint32_t i, float& s1, uint32_t& i1, float& s2, uint32_t& i2) {
     if (v < s2) {
         if (v < s1) {
@@ -173,22 +180,38 @@ __device__ __forceinline__ void keepTwo(float v, uint32_t i, float& s1, uint32_t
     }
 }
 
+__device__ __forceinline__ void mbarArrive(uint64_t* bar) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smemAddr(bar)) : "memory");
+}
+
 __global__ void __launch_bounds__(kAssignThreads, 2)
     assignTcKernel(const uint8_t* points, const uint8_t* cents, uint64_t n, uint32_t nTiles, uint2* cand,
                    uint32_t* status) {
     extern __shared__ __align__(1024) uint8_t smem[];
     uint8_t* sA = smem;
-    uint8_t* sB[2] = {smem + kPointTileBytes, smem + kPointTileBytes + kCentTileBytes};
-    // bars: [0] A loaded, [1 + s] stage s loaded, [3 + s] MMAs into accumulator s done
-    uint64_t* bars = reinterpret_cast<uint64_t*>(smem + kPointTileBytes + 2 * kCentTileBytes);
-    uint32_t* sTmem = reinterpret_cast<uint32_t*>(bars + 5);
+    uint8_t* sB = smem + kPointTileBytes;  // kStages stages of kCentTileBytes
+    uint64_t* bars = reinterpret_cast<uint64_t*>(sB + kStages * kCentTileBytes);
+    uint64_t* barA = bars;                          // A tile landed
+    uint64_t* full = bars + 1;                      // [kStages] stage landed
+    uint64_t* stageFree = full + kStages;           // [kStages] consumers done with a stage
+    uint64_t* mmaDone = stageFree + kStages;        // [2] accumulator written
+    uint64_t* accFree = mmaDone + 2;                // [2] consumers done with an accumulator
+    uint32_t* sTmem = reinterpret_cast<uint32_t*>(accFree + 2);
     volatile int* sAbort = reinterpret_cast<volatile int*>(sTmem + 1);
     const int tid = threadIdx.x;
-    const int warp = tid >> 5;
+    const int warp = tid >> 5, lane = tid & 31;
     const uint64_t tile = blockIdx.x;
 
     if (tid == 0) {
-        for (int i = 0; i < 5; ++i) mbarInit(&bars[i], 1);
+        mbarInit(barA, 1);
+        for (int i = 0; i < kStages; ++i) {
+            mbarInit(&full[i], 1);
+            mbarInit(&stageFree[i], kConsumerWarps);
+        }
+        for (int i = 0; i < 2; ++i) {
+            mbarInit(&mmaDone[i], 1);
+            mbarInit(&accFree[i], kConsumerWarps);
+        }
         *sAbort = 0;
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
@@ -203,120 +226,112 @@ __global__ void __launch_bounds__(kAssignThreads, 2)
     tcFenceAfter();
     const uint32_t tbase = *sTmem;
 
-    // Thread 0 produces: loads and MMAs. Counters let an aborting CTA drain what is in flight.
-    uint32_t loads[2] = {0, 0}, loadWaits[2] = {0, 0}, mmas[2] = {0, 0};
-    if (tid == 0) {
-        mbarExpectTx(&bars[0], kPointTileBytes);
-        bulkLoad(sA, points + tile * kPointTileBytes, kPointTileBytes, &bars[0]);
-        for (uint32_t t = 0; t < 2 && t < nTiles; ++t) {
-            mbarExpectTx(&bars[1 + t], kCentTileBytes);
-            bulkLoad(sB[t], cents + static_cast<uint64_t>(t) * kCentTileBytes, kCentTileBytes, &bars[1 + t]);
-            ++loads[t];
-        }
-    }
-    const uint32_t a0 = smemAddr(sA);
-    auto issue = [&](uint32_t t) -> bool {  // thread 0: MMAs of centroid tile t into accumulator t & 1
-        const int s = t & 1;
-        if (t == 0 && !mbarWait(&bars[0], 0)) return false;
-        if (!mbarWait(&bars[1 + s], loadWaits[s] & 1u)) return false;
-        ++loadWaits[s];
-        tcFenceAfter();
-        const uint32_t b0 = smemAddr(sB[s]);
-        const uint32_t d = tbase + static_cast<uint32_t>(s * kTileN);
-        // x.c ~ xh.ch + xh.cl + xl.ch, each as two K=8 halves
-#pragma unroll
-        for (int h = 0; h < 2; ++h) {
-            const uint32_t ko = h * kSecondK;
-            mmaTf32(d, ummaDesc(a0 + ko), ummaDesc(b0 + ko), h);
-            mmaTf32(d, ummaDesc(a0 + ko), ummaDesc(b0 + kImage + ko), 1);
-            mmaTf32(d, ummaDesc(a0 + kImage + ko), ummaDesc(b0 + ko), 1);
-        }
-        mmaCommit(&bars[3 + s]);
-        ++mmas[s];
-        return true;
-    };
-    if (tid == 0 && nTiles > 0 && !issue(0)) {
-        atomicOr(status, 1u);
-        *sAbort = 1;
-    }
-
+    // Producer bookkeeping (lane 0 of warp 8): what was issued, so an aborted CTA can drain it.
+    uint32_t loadsIssued = 0, mmasIssued = 0;
     float s1 = INFINITY, s2 = INFINITY;
     uint32_t i1 = 0, i2 = 0;
-    const int half = warp >> 2;  // which 64 columns of every tile this warp reduces
-    uint32_t mmaWaits[2] = {0, 0};
-    for (uint32_t t = 0; t < nTiles; ++t) {
-        const int s = t & 1;
-        if (tid == 0 && t + 1 < nTiles && !*sAbort && !issue(t + 1)) {
-            atomicOr(status, 1u);
-            *sAbort = 1;
-        }
-        bool ok = mbarWait(&bars[3 + s], mmaWaits[s] & 1u);
-        ++mmaWaits[s];
-        ok = __syncthreads_and(ok && !*sAbort) != 0;
-        if (!ok) {
-            if (tid == 0) {
+    const int half = warp >> 2;  // consumers: which 64 columns of every tile this warp reduces
+
+    if (warp == kConsumerWarps) {
+        if (lane == 0) {
+            mbarExpectTx(barA, kPointTileBytes);
+            bulkLoad(sA, points + tile * kPointTileBytes, kPointTileBytes, barA);
+            for (uint32_t t = 0; t < static_cast<uint32_t>(kStages) && t < nTiles; ++t) {
+                mbarExpectTx(&full[t], kCentTileBytes);
+                bulkLoad(sB + t * kCentTileBytes, cents + static_cast<uint64_t>(t) * kCentTileBytes, kCentTileBytes,
+                         &full[t]);
+                ++loadsIssued;
+            }
+            const uint32_t a0 = smemAddr(sA);
+            bool ok = mbarWait(barA, 0);
+            for (uint32_t t = 0; ok && t < nTiles; ++t) {
+                const uint32_t b = t & 1u, st = t % kStages;
+                // accumulator b: the consumers of tile t-2 are done with it
+                if (t >= 2) ok = mbarWait(&accFree[b], ((t - 2) >> 1) & 1u);
+                ok = ok && mbarWait(&full[st], (t / kStages) & 1u);
+                if (!ok || *sAbort) break;
+                tcFenceAfter();
+                const uint32_t b0 = smemAddr(sB + st * kCentTileBytes);
+                const uint32_t d = tbase + b * kTileN;
+                // x.c ~ xh.ch + xh.cl + xl.ch, each as two K=8 halves
+#pragma unroll
+                for (int h = 0; h < 2; ++h) {
+                    const uint32_t ko = h * kSecondK;
+                    mmaTf32(d, ummaDesc(a0 + ko), ummaDesc(b0 + ko), h);
+                    mmaTf32(d, ummaDesc(a0 + ko), ummaDesc(b0 + kImage + ko), 1);
+                    mmaTf32(d, ummaDesc(a0 + kImage + ko), ummaDesc(b0 + ko), 1);
+                }
+                mmaCommit(&mmaDone[b]);
+                ++mmasIssued;
+                // refill the stage of tile t-1 with tile t+3 once its consumers released it
+                if (t >= 1 && t + kStages - 1 < nTiles) {
+                    const uint32_t ls = (t - 1) % kStages;
+                    ok = mbarWait(&stageFree[ls], ((t - 1) / kStages) & 1u);
+                    if (!ok) break;
+                    mbarExpectTx(&full[ls], kCentTileBytes);
+                    bulkLoad(sB + ls * kCentTileBytes, cents + static_cast<uint64_t>(t + kStages - 1) * kCentTileBytes,
+                             kCentTileBytes, &full[ls]);
+                    ++loadsIssued;
+                }
+            }
+            if (!ok) {
                 atomicOr(status, 1u);
                 *sAbort = 1;
             }
-            break;
         }
-        tcFenceAfter();
-        const float* cn = reinterpret_cast<const float*>(sB[s] + 2 * kImage) + half * 64;
-        const uint32_t base = tbase + static_cast<uint32_t>(s * kTileN + half * 64) +
-                              (static_cast<uint32_t>((warp & 3) * 32) << 16);
-        uint32_t r[64];
-        {
-            uint32_t (&r0)[32] = *reinterpret_cast<uint32_t(*)[32]>(&r[0]);
-            uint32_t (&r1)[32] = *reinterpret_cast<uint32_t(*)[32]>(&r[32]);
-            tmemLoad32(base, r0);
-            tmemLoad32(base + 32u, r1);
-            tmemWaitLoad();
-        }
-        const uint32_t col0 = t * kTileN + static_cast<uint32_t>(half * 64);
-#pragma unroll
-        for (int c = 0; c < 64; c += 32) {
-            float m0 = INFINITY, m1 = INFINITY;
-#pragma unroll
-            for (int j = 0; j < 32; j += 4) {
-                const float4 c4 = *reinterpret_cast<const float4*>(cn + c + j);
-                const float v0 = fmaf(-2.f, __uint_as_float(r[c + j]), c4.x);
-                const float v1 = fmaf(-2.f, __uint_as_float(r[c + j + 1]), c4.y);
-                const float v2 = fmaf(-2.f, __uint_as_float(r[c + j + 2]), c4.z);
-                const float v3 = fmaf(-2.f, __uint_as_float(r[c + j + 3]), c4.w);
-                r[c + j] = __float_as_uint(v0);
-                r[c + j + 1] = __float_as_uint(v1);
-                r[c + j + 2] = __float_as_uint(v2);
-                r[c + j + 3] = __float_as_uint(v3);
-                m0 = fminf(m0, fminf(v0, v1));
-                m1 = fminf(m1, fminf(v2, v3));
+    } else {
+        const uint32_t rowBase = static_cast<uint32_t>((warp & 3) * 32) << 16;
+        for (uint32_t t = 0; t < nTiles; ++t) {
+            const uint32_t b = t & 1u, st = t % kStages;
+            if (!mbarWait(&mmaDone[b], (t >> 1) & 1u) || *sAbort) {
+                if (lane == 0) {
+                    atomicOr(status, 1u);
+                    *sAbort = 1;
+                }
+                break;
             }
-            if (fminf(m0, m1) < s2) {
+            tcFenceAfter();
+            const float* cn = reinterpret_cast<const float*>(sB + st * kCentTileBytes + 2 * kImage) + half * 64;
+            const uint32_t base = tbase + b * kTileN + static_cast<uint32_t>(half * 64) + rowBase;
+            const uint32_t col0 = t * kTileN + static_cast<uint32_t>(half * 64);
 #pragma unroll
-                for (int j = 0; j < 32; ++j) keepTwo(__uint_as_float(r[c + j]), col0 + c + j, s1, i1, s2, i2);
+            for (int c = 0; c < 64; c += 32) {
+                uint32_t r[32];
+                tmemLoad32(base + static_cast<uint32_t>(c), r);
+                tmemWaitLoad();
+                float m0 = INFINITY, m1 = INFINITY;
+#pragma unroll
+                for (int j = 0; j < 32; j += 4) {
+                    const float4 c4 = *reinterpret_cast<const float4*>(cn + c + j);
+                    const float v0 = fmaf(-2.f, __uint_as_float(r[j]), c4.x);
+                    const float v1 = fmaf(-2.f, __uint_as_float(r[j + 1]), c4.y);
+                    const float v2 = fmaf(-2.f, __uint_as_float(r[j + 2]), c4.z);
+                    const float v3 = fmaf(-2.f, __uint_as_float(r[j + 3]), c4.w);
+                    r[j] = __float_as_uint(v0);
+                    r[j + 1] = __float_as_uint(v1);
+                    r[j + 2] = __float_as_uint(v2);
+                    r[j + 3] = __float_as_uint(v3);
+                    m0 = fminf(m0, fminf(v0, v1));
+                    m1 = fminf(m1, fminf(v2, v3));
+                }
+                if (fminf(m0, m1) < s2) {
+#pragma unroll
+                    for (int j = 0; j < 32; ++j) keepTwo(__uint_as_float(r[j]), col0 + c + j, s1, i1, s2, i2);
+                }
             }
-        }
-        tcFenceBefore();
-        __syncthreads();
-        tcFenceAfter();
-        // Stage s has been read by the MMAs of tile t and by the epilogue: refill it with tile t+2.
-        if (tid == 0 && t + 2 < nTiles) {
-            mbarExpectTx(&bars[1 + s], kCentTileBytes);
-            bulkLoad(sB[s], cents + static_cast<uint64_t>(t + 2) * kCentTileBytes, kCentTileBytes, &bars[1 + s]);
-            ++loads[s];
+            tcFenceBefore();
+            __syncwarp();
+            if (lane == 0) {
+                mbarArrive(&accFree[b]);
+                mbarArrive(&stageFree[st]);
+            }
         }
     }
-    // An aborted CTA first waits (bounded) for its own copies and MMAs still in flight.
-    if (tid == 0 && *sAbort) {
-        for (int s = 0; s < 2; ++s) {
-            while (loadWaits[s] < loads[s]) {
-                mbarWait(&bars[1 + s], loadWaits[s] & 1u);
-                ++loadWaits[s];
-            }
-            while (mmaWaits[s] < mmas[s]) {
-                mbarWait(&bars[3 + s], mmaWaits[s] & 1u);
-                ++mmaWaits[s];
-            }
-        }
+    __syncthreads();
+    // An aborted CTA waits (bounded) for its own copies and MMAs still in flight before freeing.
+    if (warp == kConsumerWarps && lane == 0 && *sAbort) {
+        for (uint32_t t = 0; t < loadsIssued; ++t) mbarWait(&full[t % kStages], (t / kStages) & 1u);
+        for (uint32_t t = 0; t < mmasIssued; ++t) mbarWait(&mmaDone[t & 1u], (t >> 1) & 1u);
     }
     tcFenceBefore();
     __syncthreads();
@@ -324,18 +339,18 @@ __global__ void __launch_bounds__(kAssignThreads, 2)
     if (warp == 0) {
         asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tbase), "r"(kTmemCols) : "memory");
     }
-    // Merge the two column halves of every row through shared memory (the operand stages are idle).
-    float* mv = reinterpret_cast<float*>(sB[0]);
-    uint32_t* mi = reinterpret_cast<uint32_t*>(sB[0] + 2 * kTileM * 4);
-    const int row = (warp & 3) * 32 + (tid & 31);
-    if (half == 1) {
+    // Merge the two column halves of every row through shared memory (the stages are idle now).
+    float* mv = reinterpret_cast<float*>(sB);
+    uint32_t* mi = reinterpret_cast<uint32_t*>(sB + 2 * kTileM * 4);
+    const int row = (warp & 3) * 32 + lane;
+    if (warp < kConsumerWarps && half == 1) {
         mv[2 * row] = s1;
         mv[2 * row + 1] = s2;
         mi[2 * row] = i1;
         mi[2 * row + 1] = i2;
     }
     __syncthreads();
-    if (half == 0) {
+    if (warp < kConsumerWarps && half == 0) {
         keepTwo(mv[2 * row], mi[2 * row], s1, i1, s2, i2);
         keepTwo(mv[2 * row + 1], mi[2 * row + 1], s1, i1, s2, i2);
         const uint64_t p = tile * kTileM + static_cast<uint64_t>(row);
