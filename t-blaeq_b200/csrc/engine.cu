@@ -210,7 +210,7 @@ void BatchEngine::reserve(const EngineCaps& want, uint32_t nq, unsigned flags) {
         offStatus_ = off;
         off = align256(off + 4);
         offHdr_ = off;
-        off = align256(off + (H + 2) * 2 * 4);
+        off = align256(off + (H + 3) * 2 * 4);
         offQcount_ = off;
         off = align256(off + static_cast<size_t>(qcap_) * 4);
         offLevels_ = off;
@@ -552,6 +552,10 @@ void BatchEngine::reserveKnn(uint32_t nq) {
         selIds_.alloc(knnQcap_ * 32ull * 8);
         selD2_.alloc(knnQcap_ * 32ull * 8);
         candOffB_.alloc((knnQcap_ + 1ull) * 8);
+        cmpCnt_.alloc(knnQcap_ * 4ull);
+        cmpKids_.alloc(knnQcap_ * 4ull);
+        cmpEntryOff_.alloc((knnQcap_ + 1ull) * 8);
+        cmpKidOff_.alloc((knnQcap_ + 1ull) * 8);
     }
     if (entryCap_ < caps_.entries) {
         entryCap_ = caps_.entries;
@@ -657,9 +661,19 @@ void BatchEngine::enqueueKnn(const double* dPoints, uint32_t nq, const uint32_t*
                selCount_.as<uint32_t>(), status, stream_);
     TBLAEQ_CUDA(cudaMemsetAsync(sel_.get(), 0, entryCap_, stream_));
     launchScatterSel(selIds_.as<uint64_t>(), selOff_.as<uint64_t>(), nq, fcap, sel_.as<uint8_t>(), stream_);
+    // Each wave expands a compacted copy of its own entries (in the other frontier buffer), so no
+    // item of a skipped cluster is visited.
+    const int cbuf = 1 - buf;
+    auto compact = [&](int mode) {
+        launchCompactFrontier(F, offF_.as<uint64_t>(), nq, mode, sel_.as<uint8_t>(), lbE_.as<double>(), tau, D,
+                              cmpCnt_.as<uint32_t>(), cmpKids_.as<uint32_t>(), cmpEntryOff_.as<uint64_t>(),
+                              cmpKidOff_.as<uint64_t>(), outView(cbuf, hdrPtr(H + 2)), stream_);
+    };
     // Wave 1: every point of the selected clusters; their K-th distance bounds tau.
-    fin.child.entrySel = sel_.as<uint8_t>();
-    fin.child.entryLb = lbE_.as<double>();
+    compact(1);
+    fin.in = inView(cbuf, hdrPtr(H + 2));
+    fin.child.entrySel = nullptr;
+    fin.child.entryLb = nullptr;
     fin.wave = 1;
     fin.scratch.work = reinterpret_cast<unsigned long long*>(z + offWork_);
     launchExpand(fin, kPredKnnPoint, true, 0, stream_);
@@ -671,6 +685,7 @@ void BatchEngine::enqueueKnn(const double* dPoints, uint32_t nq, const uint32_t*
                knnCount_.as<uint32_t>(), status, stream_);
     launchTauFromTopK(knnOff_.as<uint64_t>(), knnD2_.as<double>(), dK, nq, tau, stream_);
     // Wave 2: the other clusters whose lower bound tau cannot exclude, points within tau.
+    compact(2);
     ExpandArgs w2 = fin;
     w2.scratch.desc = desc + static_cast<size_t>(H) * tileCap_;
     w2.scratch.ticket = tickets + H;

@@ -135,6 +135,7 @@ private:
     DeviceMem resIds_, resVals_, resQ_, resDist_;
     DeviceMem zeroBlock_;  // desc | tickets | status | hdrs | qcount | levelItems
     uint64_t splitLimit_ = 0xffffffffull;
+    DeviceMem cmpCnt_, cmpKids_, cmpEntryOff_, cmpKidOff_;  // frontier compaction scratch (per query)
     DeviceMem offsets_;
     DeviceMem boxF_;  // exact range batches: the query boxes as outward-rounded floats
     DeviceMem tau_, candOff_, knnCount_, knnOff_, knnIds_, knnD2_;

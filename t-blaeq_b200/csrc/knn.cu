@@ -470,4 +470,151 @@ void launchTopK(const uint64_t* offA, const uint64_t* idsA, const double* d2A, u
     TBLAEQ_CUDA(cudaGetLastError());
 }
 
+// ---- frontier compaction for the two finest-level waves ------------------------------------------
+namespace {
+
+constexpr int kCompactThreads = 256;
+
+__device__ __forceinline__ bool keepEntry(int mode, uint64_t e, uint32_t q, const uint8_t* sel, const double* lb,
+                                          const double* tau) {
+    return mode == 1 ? sel[e] != 0 : (sel[e] == 0 && lb[e] <= tau[q]);
+}
+
+__device__ __forceinline__ uint32_t childrenOf(const FrontierIn& F, uint64_t e, uint32_t entries) {
+    const uint32_t end = (e + 1 < entries) ? F.cpre[e + 1] : F.hdr[1];
+    return end - F.cpre[e];
+}
+
+// Pass 1, one block per query: kept entries and their children.
+// A frontier whose producer overflowed its capacity is incomplete (the batch is rerun after the
+// workspace grows): it compacts to nothing rather than to entries with inconsistent prefixes.
+__device__ __forceinline__ uint32_t usableEntries(const FrontierIn& F) { return F.hdr[0] <= F.cap ? F.hdr[0] : 0u; }
+
+__global__ void __launch_bounds__(kCompactThreads) compactCountKernel(FrontierIn F, const uint64_t* offF, uint32_t nq,
+                                                                     int mode, const uint8_t* sel, const double* lb,
+                                                                     const double* tau, uint32_t* cnt, uint32_t* kids) {
+    __shared__ unsigned long long sC[kCompactThreads / 32], sK[kCompactThreads / 32];
+    const uint32_t entries = usableEntries(F);
+    for (uint32_t q = blockIdx.x; q < nq; q += gridDim.x) {
+        const uint64_t e0 = offF[q], e1 = offF[q + 1] < entries ? offF[q + 1] : static_cast<uint64_t>(entries);
+        unsigned long long c = 0, k = 0;
+        for (uint64_t e = e0 + threadIdx.x; e < e1; e += blockDim.x) {
+            if (keepEntry(mode, e, q, sel, lb, tau)) {
+                ++c;
+                k += childrenOf(F, e, entries);
+            }
+        }
+        for (int o = 16; o > 0; o >>= 1) {
+            c += __shfl_xor_sync(0xffffffffu, c, o);
+            k += __shfl_xor_sync(0xffffffffu, k, o);
+        }
+        if ((threadIdx.x & 31) == 0) {
+            sC[threadIdx.x >> 5] = c;
+            sK[threadIdx.x >> 5] = k;
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            unsigned long long tc = 0, tk = 0;
+            for (int w = 0; w < kCompactThreads / 32; ++w) {
+                tc += sC[w];
+                tk += sK[w];
+            }
+            cnt[q] = static_cast<uint32_t>(tc);
+            kids[q] = static_cast<uint32_t>(tk < 0xffffffffull ? tk : 0xffffffffull);
+        }
+        __syncthreads();
+    }
+}
+
+// Pass 2, one block per query: writes the kept entries in order, with their child prefix and the
+// tile starts of the compacted item space (as the expand producer would have).
+__global__ void __launch_bounds__(kCompactThreads) compactWriteKernel(FrontierIn F, const uint64_t* offF, uint32_t nq,
+                                                                     int mode, const uint8_t* sel, const double* lb,
+                                                                     const double* tau, const uint64_t* entryOff,
+                                                                     const uint64_t* kidOff, int D, FrontierOut out) {
+    __shared__ uint32_t sCnt[kCompactThreads / 32], sKid[kCompactThreads / 32];
+    __shared__ uint32_t sRunC, sRunK;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const uint32_t entries = usableEntries(F);
+    for (uint32_t q = blockIdx.x; q < nq; q += gridDim.x) {
+        const uint64_t e0 = offF[q], e1 = offF[q + 1] < entries ? offF[q + 1] : static_cast<uint64_t>(entries);
+        if (threadIdx.x == 0) {
+            sRunC = 0;
+            sRunK = 0;
+        }
+        __syncthreads();
+        for (uint64_t base = e0; base < e1; base += blockDim.x) {
+            const uint64_t e = base + threadIdx.x;
+            const bool keep = e < e1 && keepEntry(mode, e, q, sel, lb, tau);
+            const uint32_t kc = keep ? childrenOf(F, e, entries) : 0u;
+            // block-wide exclusive scans of (keep, kids)
+            uint32_t c = keep ? 1u : 0u, k = kc;
+            for (int o = 1; o < 32; o <<= 1) {
+                const uint32_t tc = __shfl_up_sync(0xffffffffu, c, o), tk = __shfl_up_sync(0xffffffffu, k, o);
+                if (lane >= o) {
+                    c += tc;
+                    k += tk;
+                }
+            }
+            if (lane == 31) {
+                sCnt[warp] = c;
+                sKid[warp] = k;
+            }
+            __syncthreads();
+            uint32_t wc = 0, wk = 0;
+            for (int w = 0; w < warp; ++w) {
+                wc += sCnt[w];
+                wk += sKid[w];
+            }
+            const uint32_t exC = sRunC + wc + c - (keep ? 1u : 0u), exK = sRunK + wk + k - kc;
+            if (keep) {
+                const uint64_t pos = entryOff[q] + exC;
+                const uint64_t cp = kidOff[q] + exK;
+                if (pos < out.cap) {
+                    out.q[pos] = q;
+                    out.cbeg[pos] = F.cbeg[e];
+                    out.cpre[pos] = static_cast<uint32_t>(cp);
+                    for (int d = 0; d < D; ++d) out.x[pos * D + d] = F.x[e * D + d];
+                    for (unsigned long long b = (cp + kWarpTile - 1) / kWarpTile; b * kWarpTile < cp + kc; ++b)
+                        if (b < out.tileCap) out.tileStart[b] = static_cast<uint32_t>(pos);
+                }
+            }
+            __syncthreads();
+            if (threadIdx.x == blockDim.x - 1) {
+                uint32_t tc = 0, tk = 0;
+                for (int w = 0; w < kCompactThreads / 32; ++w) {
+                    tc += sCnt[w];
+                    tk += sKid[w];
+                }
+                sRunC += tc;
+                sRunK += tk;
+            }
+            __syncthreads();
+        }
+    }
+}
+
+__global__ void compactHeaderKernel(const uint64_t* entryOff, const uint64_t* kidOff, uint32_t nq, uint32_t* hdr) {
+    const unsigned long long c = entryOff[nq], k = kidOff[nq];
+    hdr[0] = static_cast<uint32_t>(c < 0xffffffffull ? c : 0xffffffffull);
+    hdr[1] = static_cast<uint32_t>(k < 0xffffffffull ? k : 0xffffffffull);
+}
+
+}  // namespace
+
+void launchCompactFrontier(const FrontierIn& F, const uint64_t* offF, uint32_t nq, int mode, const uint8_t* sel,
+                           const double* lb, const double* tau, int D, uint32_t* cnt, uint32_t* kids,
+                           uint64_t* entryOff, uint64_t* kidOff, const FrontierOut& out, cudaStream_t s) {
+    if (nq == 0) return;
+    const unsigned blocks = std::min<unsigned>(nq, 148u * 8u);
+    compactCountKernel<<<blocks, kCompactThreads, 0, s>>>(F, offF, nq, mode, sel, lb, tau, cnt, kids);
+    TBLAEQ_CUDA(cudaGetLastError());
+    launchExclusiveScan(cnt, entryOff, nq, s);
+    launchExclusiveScan(kids, kidOff, nq, s);
+    compactWriteKernel<<<blocks, kCompactThreads, 0, s>>>(F, offF, nq, mode, sel, lb, tau, entryOff, kidOff, D, out);
+    TBLAEQ_CUDA(cudaGetLastError());
+    compactHeaderKernel<<<1, 1, 0, s>>>(entryOff, kidOff, nq, out.hdr);
+    TBLAEQ_CUDA(cudaGetLastError());
+}
+
 }  // namespace tblaeq

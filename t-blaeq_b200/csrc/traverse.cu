@@ -246,7 +246,7 @@ __device__ __forceinline__ void prefetchTileRows(const ExpandArgs& a, uint32_t t
                                                  uint32_t total, int lane) {
     if (t >= nTiles) return;
     if (PRED == kPredRangeRadius && a.child.aabb) return;
-    if (PRED == kPredKnnPoint && a.wave != 0) return;
+    if (PRED == kPredKnnPoint && a.wave != 0 && a.child.entrySel) return;
     const uint32_t t0 = t * kWarpTile;
     const uint32_t itemEnd = min(t0 + static_cast<uint32_t>(kWarpTile), total);
     const uint32_t eLo = a.in.tileStart[t];
@@ -467,7 +467,11 @@ __global__ void __launch_bounds__(kExpandThreads, expandMinBlocks<PRED>()) expan
         const uint32_t eLo = a.in.tileStart[tile];
         uint32_t eHi = (tile + 1 < nTiles) ? a.in.tileStart[tile + 1] : entries - 1;
         if (eHi >= entries) eHi = entries - 1;
-        uint32_t W = eHi - eLo + 1;
+        // A tile start outside the frontier means an inconsistent input (an overflowed producer):
+        // the tile is processed as empty, so it still publishes its (zero) counts to the look-back.
+        const bool tileOk = eLo <= eHi;
+        if (!tileOk && lane == 0) atomicOr(a.scratch.status, kStatusOverflowEntries);
+        uint32_t W = tileOk ? eHi - eLo + 1 : 0u;
         if (W > S::kWindow) {
             if (lane == 0) atomicOr(a.scratch.status, kStatusWindowOverflow);
             W = S::kWindow;
@@ -483,7 +487,7 @@ __global__ void __launch_bounds__(kExpandThreads, expandMinBlocks<PRED>()) expan
 #pragma unroll
         for (int r = 0; r < R; ++r) {
             const uint32_t rs = t0 + r * 32;
-            if (rs >= total) continue;  // warp-uniform
+            if (rs >= total || W == 0) continue;  // warp-uniform
             const uint32_t k = rs + lane;
             const bool valid = k < total;
             // Every entry overlapping a 32-item round lies within the 32 window slots from `cur`:
@@ -508,6 +512,7 @@ __global__ void __launch_bounds__(kExpandThreads, expandMinBlocks<PRED>()) expan
         // ---- phase B: stream the rows (and node records) through the cp.async ring and test.
         auto issue = [&](int r) {
             if constexpr (S::kOn) {
+                if (W == 0) return;  // an empty (inconsistent) tile has no rows to stage
                 // The round's rows move as 32 * kChunks chunk copies spread over the warp so that
                 // consecutive lanes copy consecutive chunks: rows of one entry are consecutive in
                 // the P-tensor, so each copy instruction reads whole sectors (a lane copying its own
@@ -565,7 +570,7 @@ __global__ void __launch_bounds__(kExpandThreads, expandMinBlocks<PRED>()) expan
             bool keep = false;
             uint32_t cc = 0;
             bool work = valid;
-            if (PRED == kPredKnnPoint && valid && a.wave != 0) {
+            if (PRED == kPredKnnPoint && valid && a.wave != 0 && a.child.entrySel) {
                 // Two-wave KNN: decide from the entry alone before touching the child's row.
                 const uint32_t e = eLo + sWin[r * 32 + lane];
                 const bool sel = __ldg(a.child.entrySel + e) != 0;

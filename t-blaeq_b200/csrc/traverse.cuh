@@ -86,7 +86,8 @@ struct ChildLevel {
     const uint32_t* leaf;       // finest points below each child (by key), for the KNN bound
     // Two-wave KNN over the last frontier (by input entry): wave 1 keeps every point of the
     // selected entries; wave 2 skips selected entries and entries whose lower bound exceeds tau
-    // (without loading their rows) and keeps the points within tau.
+    // (without loading their rows) and keeps the points within tau. Null entrySel: the input
+    // frontier already holds only the wave's entries (compacted).
     const uint8_t* entrySel;
     const double* entryLb;
     const uint8_t* mask;        // keep flags (by row) for kPredMask
