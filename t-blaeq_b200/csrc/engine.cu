@@ -552,13 +552,14 @@ void BatchEngine::reserveKnn(uint32_t nq) {
         selIds_.alloc(knnQcap_ * 32ull * 8);
         selD2_.alloc(knnQcap_ * 32ull * 8);
         candOffB_.alloc((knnQcap_ + 1ull) * 8);
-        cmpCnt_.alloc(knnQcap_ * 4ull);
-        cmpKids_.alloc(knnQcap_ * 4ull);
-        cmpEntryOff_.alloc((knnQcap_ + 1ull) * 8);
-        cmpKidOff_.alloc((knnQcap_ + 1ull) * 8);
     }
     if (entryCap_ < caps_.entries) {
         entryCap_ = caps_.entries;
+        const uint64_t seg = compactSegments(entryCap_);
+        cmpCnt_.alloc(seg * 4);
+        cmpKids_.alloc(seg * 4);
+        cmpEntryOff_.alloc((seg + 1) * 8);
+        cmpKidOff_.alloc((seg + 1) * 8);
         lbE_.alloc(entryCap_ * 8);
         scoreE_.alloc(entryCap_ * 8);
         sel_.alloc(entryCap_);
@@ -665,9 +666,9 @@ void BatchEngine::enqueueKnn(const double* dPoints, uint32_t nq, const uint32_t*
     // item of a skipped cluster is visited.
     const int cbuf = 1 - buf;
     auto compact = [&](int mode) {
-        launchCompactFrontier(F, offF_.as<uint64_t>(), nq, mode, sel_.as<uint8_t>(), lbE_.as<double>(), tau, D,
-                              cmpCnt_.as<uint32_t>(), cmpKids_.as<uint32_t>(), cmpEntryOff_.as<uint64_t>(),
-                              cmpKidOff_.as<uint64_t>(), outView(cbuf, hdrPtr(H + 2)), stream_);
+        launchCompactFrontier(F, fcap, mode, sel_.as<uint8_t>(), lbE_.as<double>(), tau, D, cmpCnt_.as<uint32_t>(),
+                              cmpKids_.as<uint32_t>(), cmpEntryOff_.as<uint64_t>(), cmpKidOff_.as<uint64_t>(),
+                              outView(cbuf, hdrPtr(H + 2)), stream_);
     };
     // Wave 1: every point of the selected clusters; their K-th distance bounds tau.
     compact(1);

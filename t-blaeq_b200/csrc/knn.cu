@@ -218,12 +218,13 @@ __global__ void __launch_bounds__(512) topKKernel(const uint64_t* offA, const ui
     if (threadIdx.x == 0) outCount[q] = static_cast<uint32_t>(keep);
     if (keep == 0) return;
     const uint64_t o = outOff[q];
-    if (n <= kTopKStage) {
+    // Sorts sk/sv[0, count) by (key, id) with a bitonic network and writes the first `keep`.
+    auto sortAndWrite = [&](uint32_t count) {
         int size = 1;
-        while (size < static_cast<int>(n)) size <<= 1;
-        for (int i = threadIdx.x; i < size; i += blockDim.x) {
-            sk[i] = i < static_cast<int>(n) ? keyAt(i) : ~0ull;
-            sv[i] = i < static_cast<int>(n) ? idAt(i) : ~0ull;
+        while (size < static_cast<int>(count)) size <<= 1;
+        for (int i = static_cast<int>(count) + threadIdx.x; i < size; i += blockDim.x) {
+            sk[i] = ~0ull;
+            sv[i] = ~0ull;
         }
         __syncthreads();
         for (int s = 2; s <= size; s <<= 1) {
@@ -253,7 +254,77 @@ __global__ void __launch_bounds__(512) topKKernel(const uint64_t* offA, const ui
             memcpy(&d, &b, 8);
             outD2[o + i] = d;
         }
+    };
+    if (n <= kTopKStage) {
+        for (int i = threadIdx.x; i < static_cast<int>(n); i += blockDim.x) {
+            sk[i] = keyAt(i);
+            sv[i] = idAt(i);
+        }
+        sortAndWrite(static_cast<uint32_t>(n));
         return;
+    }
+    if (keep <= kTopKStage) {
+        // Radix selection of the keep-th smallest key: eight passes over the candidates, each a
+        // 256-bin histogram of the next 8-bit digit among the keys that share the digits chosen
+        // so far. Then every key below the boundary and the ties on it are gathered and sorted.
+        __shared__ uint32_t hist[256];
+        __shared__ unsigned long long sPrefix, sMask;
+        __shared__ uint32_t sNeed, sLess, sEq;
+        if (threadIdx.x == 0) {
+            sPrefix = 0;
+            sMask = 0;
+            sNeed = static_cast<uint32_t>(keep);
+        }
+        __syncthreads();
+        for (int shift = 56; shift >= 0; shift -= 8) {
+            for (int i = threadIdx.x; i < 256; i += blockDim.x) hist[i] = 0;
+            __syncthreads();
+            const uint64_t prefix = sPrefix, mask = sMask;
+            for (uint64_t i = threadIdx.x; i < n; i += blockDim.x) {
+                const uint64_t key = keyAt(i);
+                if ((key & mask) == prefix) atomicAdd(&hist[(key >> shift) & 255u], 1u);
+            }
+            __syncthreads();
+            if (threadIdx.x == 0) {
+                uint32_t need = sNeed, cum = 0, d = 0;
+                while (d < 255u && cum + hist[d] < need) cum += hist[d++];
+                sNeed = need - cum;
+                sPrefix = prefix | (static_cast<unsigned long long>(d) << shift);
+                sMask = mask | (255ull << shift);
+            }
+            __syncthreads();
+        }
+        const uint64_t kb = sPrefix;
+        const uint32_t less = static_cast<uint32_t>(keep) - sNeed;
+        const uint32_t room = static_cast<uint32_t>(kTopKStage) - less;
+        if (threadIdx.x == 0) {
+            sLess = 0;
+            sEq = 0;
+        }
+        __syncthreads();
+        for (uint64_t i = threadIdx.x; i < n; i += blockDim.x) {
+            const uint64_t key = keyAt(i);
+            if (key < kb) {
+                const uint32_t slot = atomicAdd(&sLess, 1u);
+                if (slot < less) {
+                    sk[slot] = key;
+                    sv[slot] = idAt(i);
+                }
+            } else if (key == kb) {
+                const uint32_t slot = atomicAdd(&sEq, 1u);
+                if (slot < room) {
+                    sk[less + slot] = key;
+                    sv[less + slot] = idAt(i);
+                }
+            }
+        }
+        __syncthreads();
+        if (sLess == less && sEq <= room) {
+            sortAndWrite(less + sEq);
+            return;
+        }
+        __syncthreads();
+        // (ties on the boundary key overflow the stage: fall back to the rounds below)
     }
     // More candidates than the stage holds: K rounds of a block-wide minimum above the last pick.
     __shared__ unsigned long long sBestK, sBestV;
@@ -485,136 +556,135 @@ __device__ __forceinline__ uint32_t childrenOf(const FrontierIn& F, uint64_t e, 
     return end - F.cpre[e];
 }
 
-// Pass 1, one block per query: kept entries and their children.
 // A frontier whose producer overflowed its capacity is incomplete (the batch is rerun after the
 // workspace grows): it compacts to nothing rather than to entries with inconsistent prefixes.
 __device__ __forceinline__ uint32_t usableEntries(const FrontierIn& F) { return F.hdr[0] <= F.cap ? F.hdr[0] : 0u; }
 
-__global__ void __launch_bounds__(kCompactThreads) compactCountKernel(FrontierIn F, const uint64_t* offF, uint32_t nq,
-                                                                     int mode, const uint8_t* sel, const double* lb,
-                                                                     const double* tau, uint32_t* cnt, uint32_t* kids) {
-    __shared__ unsigned long long sC[kCompactThreads / 32], sK[kCompactThreads / 32];
+constexpr uint32_t kSegment = 4096;  // frontier entries per compaction block
+
+// Pass 1, one block per segment of the (query-major) frontier: kept entries and their children.
+__global__ void __launch_bounds__(kCompactThreads) compactCountKernel(FrontierIn F, int mode, const uint8_t* sel,
+                                                                     const double* lb, const double* tau,
+                                                                     uint32_t* cnt, uint32_t* kids) {
+    __shared__ uint32_t sC[kCompactThreads / 32], sK[kCompactThreads / 32];
     const uint32_t entries = usableEntries(F);
-    for (uint32_t q = blockIdx.x; q < nq; q += gridDim.x) {
-        const uint64_t e0 = offF[q], e1 = offF[q + 1] < entries ? offF[q + 1] : static_cast<uint64_t>(entries);
-        unsigned long long c = 0, k = 0;
-        for (uint64_t e = e0 + threadIdx.x; e < e1; e += blockDim.x) {
-            if (keepEntry(mode, e, q, sel, lb, tau)) {
-                ++c;
-                k += childrenOf(F, e, entries);
-            }
+    const uint64_t e0 = static_cast<uint64_t>(blockIdx.x) * kSegment;
+    const uint64_t e1 = min(e0 + kSegment, static_cast<uint64_t>(entries));
+    uint32_t c = 0, k = 0;
+    for (uint64_t e = e0 + threadIdx.x; e < e1; e += blockDim.x) {
+        if (keepEntry(mode, e, F.q[e], sel, lb, tau)) {
+            ++c;
+            k += childrenOf(F, e, entries);
         }
-        for (int o = 16; o > 0; o >>= 1) {
-            c += __shfl_xor_sync(0xffffffffu, c, o);
-            k += __shfl_xor_sync(0xffffffffu, k, o);
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        c += __shfl_xor_sync(0xffffffffu, c, o);
+        k += __shfl_xor_sync(0xffffffffu, k, o);
+    }
+    if ((threadIdx.x & 31) == 0) {
+        sC[threadIdx.x >> 5] = c;
+        sK[threadIdx.x >> 5] = k;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        uint32_t tc = 0, tk = 0;
+        for (int w = 0; w < kCompactThreads / 32; ++w) {
+            tc += sC[w];
+            tk += sK[w];
         }
-        if ((threadIdx.x & 31) == 0) {
-            sC[threadIdx.x >> 5] = c;
-            sK[threadIdx.x >> 5] = k;
-        }
-        __syncthreads();
-        if (threadIdx.x == 0) {
-            unsigned long long tc = 0, tk = 0;
-            for (int w = 0; w < kCompactThreads / 32; ++w) {
-                tc += sC[w];
-                tk += sK[w];
-            }
-            cnt[q] = static_cast<uint32_t>(tc);
-            kids[q] = static_cast<uint32_t>(tk < 0xffffffffull ? tk : 0xffffffffull);
-        }
-        __syncthreads();
+        cnt[blockIdx.x] = tc;
+        kids[blockIdx.x] = tk;
     }
 }
 
-// Pass 2, one block per query: writes the kept entries in order, with their child prefix and the
-// tile starts of the compacted item space (as the expand producer would have).
-__global__ void __launch_bounds__(kCompactThreads) compactWriteKernel(FrontierIn F, const uint64_t* offF, uint32_t nq,
-                                                                     int mode, const uint8_t* sel, const double* lb,
-                                                                     const double* tau, const uint64_t* entryOff,
-                                                                     const uint64_t* kidOff, int D, FrontierOut out) {
+// Pass 2, one block per segment: writes the kept entries in order, with their child prefix and
+// the tile starts of the compacted item space (as the expand producer would have).
+__global__ void __launch_bounds__(kCompactThreads) compactWriteKernel(FrontierIn F, int mode, const uint8_t* sel,
+                                                                     const double* lb, const double* tau,
+                                                                     const uint64_t* entryOff, const uint64_t* kidOff,
+                                                                     int D, FrontierOut out) {
     __shared__ uint32_t sCnt[kCompactThreads / 32], sKid[kCompactThreads / 32];
     __shared__ uint32_t sRunC, sRunK;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const uint32_t entries = usableEntries(F);
-    for (uint32_t q = blockIdx.x; q < nq; q += gridDim.x) {
-        const uint64_t e0 = offF[q], e1 = offF[q + 1] < entries ? offF[q + 1] : static_cast<uint64_t>(entries);
-        if (threadIdx.x == 0) {
-            sRunC = 0;
-            sRunK = 0;
+    const uint64_t e0 = static_cast<uint64_t>(blockIdx.x) * kSegment;
+    const uint64_t e1 = min(e0 + kSegment, static_cast<uint64_t>(entries));
+    if (threadIdx.x == 0) {
+        sRunC = 0;
+        sRunK = 0;
+    }
+    __syncthreads();
+    for (uint64_t base = e0; base < e1; base += blockDim.x) {
+        const uint64_t e = base + threadIdx.x;
+        const uint32_t q = e < e1 ? F.q[e] : 0u;
+        const bool keep = e < e1 && keepEntry(mode, e, q, sel, lb, tau);
+        const uint32_t kc = keep ? childrenOf(F, e, entries) : 0u;
+        uint32_t c = keep ? 1u : 0u, k = kc;
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t tc = __shfl_up_sync(0xffffffffu, c, o), tk = __shfl_up_sync(0xffffffffu, k, o);
+            if (lane >= o) {
+                c += tc;
+                k += tk;
+            }
+        }
+        if (lane == 31) {
+            sCnt[warp] = c;
+            sKid[warp] = k;
         }
         __syncthreads();
-        for (uint64_t base = e0; base < e1; base += blockDim.x) {
-            const uint64_t e = base + threadIdx.x;
-            const bool keep = e < e1 && keepEntry(mode, e, q, sel, lb, tau);
-            const uint32_t kc = keep ? childrenOf(F, e, entries) : 0u;
-            // block-wide exclusive scans of (keep, kids)
-            uint32_t c = keep ? 1u : 0u, k = kc;
-            for (int o = 1; o < 32; o <<= 1) {
-                const uint32_t tc = __shfl_up_sync(0xffffffffu, c, o), tk = __shfl_up_sync(0xffffffffu, k, o);
-                if (lane >= o) {
-                    c += tc;
-                    k += tk;
-                }
-            }
-            if (lane == 31) {
-                sCnt[warp] = c;
-                sKid[warp] = k;
-            }
-            __syncthreads();
-            uint32_t wc = 0, wk = 0;
-            for (int w = 0; w < warp; ++w) {
-                wc += sCnt[w];
-                wk += sKid[w];
-            }
-            const uint32_t exC = sRunC + wc + c - (keep ? 1u : 0u), exK = sRunK + wk + k - kc;
-            if (keep) {
-                const uint64_t pos = entryOff[q] + exC;
-                const uint64_t cp = kidOff[q] + exK;
-                if (pos < out.cap) {
-                    out.q[pos] = q;
-                    out.cbeg[pos] = F.cbeg[e];
-                    out.cpre[pos] = static_cast<uint32_t>(cp);
-                    for (int d = 0; d < D; ++d) out.x[pos * D + d] = F.x[e * D + d];
-                    for (unsigned long long b = (cp + kWarpTile - 1) / kWarpTile; b * kWarpTile < cp + kc; ++b)
-                        if (b < out.tileCap) out.tileStart[b] = static_cast<uint32_t>(pos);
-                }
-            }
-            __syncthreads();
-            if (threadIdx.x == blockDim.x - 1) {
-                uint32_t tc = 0, tk = 0;
-                for (int w = 0; w < kCompactThreads / 32; ++w) {
-                    tc += sCnt[w];
-                    tk += sKid[w];
-                }
-                sRunC += tc;
-                sRunK += tk;
-            }
-            __syncthreads();
+        uint32_t wc = 0, wk = 0;
+        for (int w = 0; w < warp; ++w) {
+            wc += sCnt[w];
+            wk += sKid[w];
         }
+        if (keep) {
+            const uint64_t pos = entryOff[blockIdx.x] + sRunC + wc + c - 1u;
+            const uint64_t cp = kidOff[blockIdx.x] + sRunK + wk + k - kc;
+            if (pos < out.cap && cp + kc <= 0xffffffffull) {
+                out.q[pos] = q;
+                out.cbeg[pos] = F.cbeg[e];
+                out.cpre[pos] = static_cast<uint32_t>(cp);
+                for (int d = 0; d < D; ++d) out.x[pos * D + d] = F.x[e * D + d];
+                for (unsigned long long b = (cp + kWarpTile - 1) / kWarpTile; b * kWarpTile < cp + kc; ++b)
+                    if (b < out.tileCap) out.tileStart[b] = static_cast<uint32_t>(pos);
+            }
+        }
+        __syncthreads();
+        if (threadIdx.x == blockDim.x - 1) {
+            uint32_t tc = 0, tk = 0;
+            for (int w = 0; w < kCompactThreads / 32; ++w) {
+                tc += sCnt[w];
+                tk += sKid[w];
+            }
+            sRunC += tc;
+            sRunK += tk;
+        }
+        __syncthreads();
     }
 }
 
-__global__ void compactHeaderKernel(const uint64_t* entryOff, const uint64_t* kidOff, uint32_t nq, uint32_t* hdr) {
-    const unsigned long long c = entryOff[nq], k = kidOff[nq];
+__global__ void compactHeaderKernel(const uint64_t* entryOff, const uint64_t* kidOff, uint32_t nSeg, uint32_t* hdr) {
+    const unsigned long long c = entryOff[nSeg], k = kidOff[nSeg];
     hdr[0] = static_cast<uint32_t>(c < 0xffffffffull ? c : 0xffffffffull);
     hdr[1] = static_cast<uint32_t>(k < 0xffffffffull ? k : 0xffffffffull);
 }
 
 }  // namespace
 
-void launchCompactFrontier(const FrontierIn& F, const uint64_t* offF, uint32_t nq, int mode, const uint8_t* sel,
-                           const double* lb, const double* tau, int D, uint32_t* cnt, uint32_t* kids,
-                           uint64_t* entryOff, uint64_t* kidOff, const FrontierOut& out, cudaStream_t s) {
-    if (nq == 0) return;
-    const unsigned blocks = std::min<unsigned>(nq, 148u * 8u);
-    compactCountKernel<<<blocks, kCompactThreads, 0, s>>>(F, offF, nq, mode, sel, lb, tau, cnt, kids);
+void launchCompactFrontier(const FrontierIn& F, uint32_t cap, int mode, const uint8_t* sel, const double* lb,
+                           const double* tau, int D, uint32_t* cnt, uint32_t* kids, uint64_t* entryOff,
+                           uint64_t* kidOff, const FrontierOut& out, cudaStream_t s) {
+    const uint32_t nSeg = std::max<uint32_t>(1u, (cap + kSegment - 1) / kSegment);
+    compactCountKernel<<<nSeg, kCompactThreads, 0, s>>>(F, mode, sel, lb, tau, cnt, kids);
     TBLAEQ_CUDA(cudaGetLastError());
-    launchExclusiveScan(cnt, entryOff, nq, s);
-    launchExclusiveScan(kids, kidOff, nq, s);
-    compactWriteKernel<<<blocks, kCompactThreads, 0, s>>>(F, offF, nq, mode, sel, lb, tau, entryOff, kidOff, D, out);
+    launchExclusiveScan(cnt, entryOff, nSeg, s);
+    launchExclusiveScan(kids, kidOff, nSeg, s);
+    compactWriteKernel<<<nSeg, kCompactThreads, 0, s>>>(F, mode, sel, lb, tau, entryOff, kidOff, D, out);
     TBLAEQ_CUDA(cudaGetLastError());
-    compactHeaderKernel<<<1, 1, 0, s>>>(entryOff, kidOff, nq, out.hdr);
+    compactHeaderKernel<<<1, 1, 0, s>>>(entryOff, kidOff, nSeg, out.hdr);
     TBLAEQ_CUDA(cudaGetLastError());
 }
+
+uint32_t compactSegments(uint64_t cap) { return static_cast<uint32_t>(std::max<uint64_t>(1, (cap + kSegment - 1) / kSegment)); }
 
 }  // namespace tblaeq

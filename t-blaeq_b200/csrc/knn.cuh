@@ -57,14 +57,15 @@ void launchEntryBounds(const uint32_t* q, const uint32_t* node, const double* x,
 // Wave-1 width per query: clamp(ceil(factor * K[q]) + 1, 2, 32) entries.
 void launchWaveWidth(const uint32_t* K, uint32_t nq, double factor, uint32_t* M, cudaStream_t s);
 
-// Compacts the last KNN frontier F (query-major, per-query entry offsets offF) into `out`: mode 1
-// keeps the selected entries (sel), mode 2 the others whose lower bound is within their query's
-// tau. Order is kept; the child prefix, tile starts and header (count, children) of `out` are
-// rebuilt, so a wave expands only its own entries. Scratch: cnt, kids (nq), entryOff, kidOff
-// (nq + 1).
-void launchCompactFrontier(const FrontierIn& F, const uint64_t* offF, uint32_t nq, int mode, const uint8_t* sel,
-                           const double* lb, const double* tau, int D, uint32_t* cnt, uint32_t* kids,
-                           uint64_t* entryOff, uint64_t* kidOff, const FrontierOut& out, cudaStream_t s);
+// Compacts the last KNN frontier F (query-major) into `out`: mode 1 keeps the selected entries
+// (sel), mode 2 the others whose lower bound is within their query's tau. Order is kept; the child
+// prefix, tile starts and header (count, children) of `out` are rebuilt, so a wave expands only
+// its own entries. Blocks work on fixed segments of F's capacity `cap`; scratch: cnt, kids
+// (compactSegments(cap)), entryOff, kidOff (compactSegments(cap) + 1).
+void launchCompactFrontier(const FrontierIn& F, uint32_t cap, int mode, const uint8_t* sel, const double* lb,
+                           const double* tau, int D, uint32_t* cnt, uint32_t* kids, uint64_t* entryOff,
+                           uint64_t* kidOff, const FrontierOut& out, cudaStream_t s);
+uint32_t compactSegments(uint64_t cap);
 
 // sel[ids[i]] = 1 for every selected entry position in [0, off[nq]) below cap (positions at or
 // above cap come from slots a skipped query never wrote).
