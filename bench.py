@@ -118,6 +118,25 @@ def oracle_index_from_handler(oracle, h):
                               pvals, radius, maps, cids, cvals)
 
 
+def max_over_ranks(value: float) -> float:
+    """The largest of every rank's value (1 rank: the value itself). Replicas are timed on their own
+    device and the job takes as long as its slowest rank; NCCL reduces on the GPU, other backends
+    on the host."""
+    import torch.distributed as dist
+    if not (dist.is_available() and dist.is_initialized()) or dist.get_world_size() == 1:
+        return float(value)
+    import torch
+    device = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([float(value)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def job_throughput(units_per_rank: float, world: int, seconds_max: float) -> float:
+    """Whole-job throughput: every replica processed units_per_rank in at most seconds_max."""
+    return units_per_rank * world / seconds_max
+
+
 def profiled_traffic(cfg_name, nq):
     """DRAM bytes (read + write) of one finest-level expand launch of this exact workload, from the
     committed ncu summary (one capture of the same command; ncu is never run by the benchmark)."""
@@ -239,12 +258,8 @@ def main():
     torch.cuda.nvtx.range_pop()
     if world > 1:
         dist.barrier()
-    total_ms = sum(step_ms)
-    if world > 1:
-        t = torch.tensor([total_ms], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        total_ms = float(t.item())
-    value = args.nq * args.steps * world / (total_ms / 1e3)
+    total_ms = max_over_ranks(sum(step_ms))
+    value = job_throughput(args.nq * args.steps, world, total_ms / 1e3)
 
     # Roofline of the finest-level expand (dominant kernel): algorithmic bytes per launch.
     H = len(entries)
@@ -290,12 +305,8 @@ def main():
         t0 = time.perf_counter()
         e2e_call()
         e2e_t.append(time.perf_counter() - t0)
-    e2e_total = sum(e2e_t)
-    if world > 1:
-        t = torch.tensor([e2e_total], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_total = float(t.item())
-    e2e_value = args.nq * args.steps * world / e2e_total
+    e2e_total = max_over_ranks(sum(e2e_t))
+    e2e_value = job_throughput(args.nq * args.steps, world, e2e_total)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
