@@ -235,6 +235,11 @@ int tblaeq_scorer_logits(tblaeq_handle* h, const float* X, uint64_t n, float* z_
  * positives (the cluster holds one of the query's K nearest points). */
 int tblaeq_scorer_stats(tblaeq_handle* h, uint64_t* samples, uint64_t* positives);
 
+/* Saves the trained scorer (parameters, feature scale, training counts) to a file, or loads one
+ * (checked against the index's dimension and height) and enables it. */
+int tblaeq_scorer_save(tblaeq_handle* h, const char* path);
+int tblaeq_scorer_load(tblaeq_handle* h, const char* path);
+
 /* Host copies of the index arrays (read-only, owned by the handle), for tools and tests:
  * which = 0: P-tensor values of interval l (rows*D doubles), 1: colRes of interval l (cols+1),
  * 2: max radius of interval l (cols), 3: Map of mesh l (meshSizes), 4: coarsest ids, 5: coarsest vals. */

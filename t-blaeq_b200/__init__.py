@@ -158,6 +158,8 @@ def _load():
                                      P(ctypes.c_float)], ctypes.c_int),
         "tblaeq_scorer_logits": ([vp, P(ctypes.c_float), ctypes.c_uint64, P(ctypes.c_float)], ctypes.c_int),
         "tblaeq_scorer_stats": ([vp, P(ctypes.c_uint64), P(ctypes.c_uint64)], ctypes.c_int),
+        "tblaeq_scorer_save": ([vp, ctypes.c_char_p], ctypes.c_int),
+        "tblaeq_scorer_load": ([vp, ctypes.c_char_p], ctypes.c_int),
         "tblaeq_live_device_bytes": ([], ctypes.c_uint64),
         "tblaeq_debug_fail_alloc_after": ([ctypes.c_uint64], None),
         "tblaeq_debug_split_above": ([vp, ctypes.c_uint64], ctypes.c_int),
@@ -543,6 +545,13 @@ class QueryHandler:
         z = np.empty(X.shape[0], np.float32)
         _check(_load().tblaeq_scorer_logits(self._h, _dptr(X, ctypes.c_float), X.shape[0], _dptr(z, ctypes.c_float)))
         return z
+
+    def scorer_save(self, path: str):
+        _check(_load().tblaeq_scorer_save(self._h, os.fsencode(path)))
+
+    def scorer_load(self, path: str):
+        """Loads a saved scorer (same index shape) and enables it."""
+        _check(_load().tblaeq_scorer_load(self._h, os.fsencode(path)))
 
     def scorer_stats(self) -> dict:
         s, p = ctypes.c_uint64(), ctypes.c_uint64()

@@ -1,4 +1,5 @@
 // extern "C" boundary (include/tblaeq.h) over the C++ facade.
+#include <cstdio>
 #include <cstring>
 #include <filesystem>
 #include <new>
@@ -516,6 +517,59 @@ int tblaeq_scorer_stats(tblaeq_handle* h, uint64_t* samples, uint64_t* positives
     if (samples) *samples = rt.scorerSamples;
     if (positives) *positives = rt.scorerPositives;
     return TBLAEQ_OK;
+}
+
+namespace {
+constexpr char kScorerMagic[8] = {'T', 'B', 'L', 'Q', 'S', 'C', 'R', '1'};
+}
+
+int tblaeq_scorer_save(tblaeq_handle* h, const char* path) {
+    if (int c = checkPrepared(h)) return c;
+    if (!path) return fail(TBLAEQ_ERR_INVALID, "null path");
+    return guarded([&]() -> int {
+        Runtime& rt = h->qh->runtime();
+        if (!rt.scorer) return fail(TBLAEQ_ERR_STATE, "no scorer to save (train or load one first)");
+        const std::vector<float> p = rt.scorer->getParams();
+        FILE* f = std::fopen(path, "wb");
+        if (!f) return fail(TBLAEQ_ERR_IO, std::string("Cannot write ") + path);
+        const uint64_t head[5] = {static_cast<uint64_t>(rt.scorer->shape().D),
+                                  static_cast<uint64_t>(rt.scorer->shape().levels), p.size(), rt.scorerSamples,
+                                  rt.scorerPositives};
+        bool ok = std::fwrite(kScorerMagic, 1, 8, f) == 8 && std::fwrite(head, 8, 5, f) == 5 &&
+                  std::fwrite(&rt.scorerInvScale, 8, 1, f) == 1 && std::fwrite(p.data(), 4, p.size(), f) == p.size();
+        ok = (std::fclose(f) == 0) && ok;
+        return ok ? TBLAEQ_OK : fail(TBLAEQ_ERR_IO, std::string("Short write ") + path);
+    });
+}
+
+int tblaeq_scorer_load(tblaeq_handle* h, const char* path) {
+    if (int c = checkPrepared(h)) return c;
+    if (!path) return fail(TBLAEQ_ERR_INVALID, "null path");
+    return guarded([&]() -> int {
+        Runtime& rt = h->qh->runtime();
+        FILE* f = std::fopen(path, "rb");
+        if (!f) return fail(TBLAEQ_ERR_IO, std::string("Cannot read ") + path);
+        char magic[8];
+        uint64_t head[5];
+        double inv = 0.0;
+        bool ok = std::fread(magic, 1, 8, f) == 8 && std::memcmp(magic, kScorerMagic, 8) == 0 &&
+                  std::fread(head, 8, 5, f) == 5 && std::fread(&inv, 8, 1, f) == 1;
+        Mlp& m = ensureScorer(rt);
+        ok = ok && head[0] == static_cast<uint64_t>(m.shape().D) && head[1] == static_cast<uint64_t>(m.shape().levels) &&
+             head[2] == m.shape().params();
+        std::vector<float> p(ok ? head[2] : 0);
+        ok = ok && std::fread(p.data(), 4, p.size(), f) == p.size();
+        std::fclose(f);
+        if (!ok) return fail(TBLAEQ_ERR_IO, std::string("Invalid index: scorer file ") + path +
+                                                " is truncated or was trained for another index shape");
+        m.setParams(p, rt.stream);
+        rt.scorerInvScale = inv;
+        rt.scorerSamples = head[3];
+        rt.scorerPositives = head[4];
+        enableScorer(rt, true);
+        TBLAEQ_CUDA(cudaStreamSynchronize(rt.stream));
+        return TBLAEQ_OK;
+    });
 }
 
 int tblaeq_scorer_enable(tblaeq_handle* h, int on) {

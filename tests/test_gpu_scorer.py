@@ -106,3 +106,17 @@ def test_learned_ranking_keeps_results_exact_and_reports_gain(tb, env, oracle_mo
     assert work["two-wave lb"] < work["one-pass"]
     # The learned ranking bounds tau sooner than the lower bound does (measured 1.76x fewer rows).
     assert work["two-wave learned"] < 0.9 * work["two-wave lb"]
+
+
+def test_scorer_save_load_round_trip(tb, env, tmp_path):
+    h = env[0]
+    path = str(tmp_path / "scorer.bin")
+    h.scorer_save(path)
+    p = h.scorer_params()
+    h.scorer_set_params(np.zeros_like(p))
+    h.scorer_load(path)
+    assert np.array_equal(h.scorer_params(), p)
+    with open(path, "r+b") as f:
+        f.truncate(40)
+    with pytest.raises(tb.TblaeqError):
+        h.scorer_load(path)

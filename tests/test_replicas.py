@@ -33,7 +33,7 @@ def _rank(rank, world, port, out):
 
 def test_two_replicas_time_by_slowest_rank():
     world, port = 2, _free_port()
-    out = mp.Manager().dict()
+    out = mp.get_context("spawn").Manager().dict()
     mp.spawn(_rank, args=(world, port, out), nprocs=world, join=True)
     assert out[0] == out[1]
     slowest, qps = out[0]
