@@ -228,8 +228,13 @@ int tblaeq_scorer_set_params(tblaeq_handle* h, const float* params, uint64_t n);
 int tblaeq_scorer_loss_grad(tblaeq_handle* h, const float* X, const float* y, uint64_t n, float* grad_out,
                             float* loss_out);
 
-/* Logits of host samples X (n x in). */
+/* Logits of host samples X (n x in): CUDA-core forward (BF16 weights, FP32 activations). */
 int tblaeq_scorer_logits(tblaeq_handle* h, const float* X, uint64_t n, float* z_out);
+
+/* The same logits through the kernel that scores KNN frontiers: tcgen05 BF16 MMAs with FP32
+ * accumulation, so X and the hidden layer are rounded to BF16. TBLAEQ_ERR_TIMEOUT if the kernel
+ * gave up waiting for its MMAs. No counterpart in the reference (it ranks frontiers by bound). */
+int tblaeq_scorer_logits_tensor(tblaeq_handle* h, const float* X, uint64_t n, float* z_out);
 
 /* The last training's sample count and how many of the traced (query, cluster) pairs were
  * positives (the cluster holds one of the query's K nearest points). */

@@ -157,6 +157,7 @@ def _load():
         "tblaeq_scorer_loss_grad": ([vp, P(ctypes.c_float), P(ctypes.c_float), ctypes.c_uint64, P(ctypes.c_float),
                                      P(ctypes.c_float)], ctypes.c_int),
         "tblaeq_scorer_logits": ([vp, P(ctypes.c_float), ctypes.c_uint64, P(ctypes.c_float)], ctypes.c_int),
+        "tblaeq_scorer_logits_tensor": ([vp, P(ctypes.c_float), ctypes.c_uint64, P(ctypes.c_float)], ctypes.c_int),
         "tblaeq_scorer_stats": ([vp, P(ctypes.c_uint64), P(ctypes.c_uint64)], ctypes.c_int),
         "tblaeq_scorer_save": ([vp, ctypes.c_char_p], ctypes.c_int),
         "tblaeq_scorer_load": ([vp, ctypes.c_char_p], ctypes.c_int),
@@ -540,10 +541,13 @@ class QueryHandler:
                                                _dptr(grad, ctypes.c_float), ctypes.byref(loss)))
         return float(loss.value), grad
 
-    def scorer_logits(self, X) -> np.ndarray:
+    def scorer_logits(self, X, tensor: bool = False) -> np.ndarray:
+        """Logits of feature rows X (n x in). tensor=True runs the tensor-core kernel that scores KNN
+        frontiers (BF16 inputs and hidden layer, FP32 accumulation)."""
         X = np.ascontiguousarray(np.asarray(X, dtype=np.float32))
         z = np.empty(X.shape[0], np.float32)
-        _check(_load().tblaeq_scorer_logits(self._h, _dptr(X, ctypes.c_float), X.shape[0], _dptr(z, ctypes.c_float)))
+        fn = _load().tblaeq_scorer_logits_tensor if tensor else _load().tblaeq_scorer_logits
+        _check(fn(self._h, _dptr(X, ctypes.c_float), X.shape[0], _dptr(z, ctypes.c_float)))
         return z
 
     def scorer_save(self, path: str):

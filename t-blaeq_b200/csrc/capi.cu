@@ -619,7 +619,7 @@ int tblaeq_scorer_loss_grad(tblaeq_handle* h, const float* X, const float* y, ui
     });
 }
 
-int tblaeq_scorer_logits(tblaeq_handle* h, const float* X, uint64_t n, float* z_out) {
+static int scorerLogits(tblaeq_handle* h, const float* X, uint64_t n, float* z_out, bool tensor) {
     if (int c = checkPrepared(h)) return c;
     if (!X || !z_out || n > 0xffffffffull) return fail(TBLAEQ_ERR_INVALID, "bad samples");
     return guarded([&]() -> int {
@@ -628,11 +628,23 @@ int tblaeq_scorer_logits(tblaeq_handle* h, const float* X, uint64_t n, float* z_
         const int in = m.shape().in();
         DeviceMem dX(std::max<uint64_t>(n, 1) * in * 4), dz(std::max<uint64_t>(n, 1) * 4);
         TBLAEQ_CUDA(cudaMemcpyAsync(dX.get(), X, n * in * 4, cudaMemcpyHostToDevice, rt.stream));
-        m.logits(dX.as<float>(), static_cast<uint32_t>(n), dz.as<float>(), rt.stream);
+        if (tensor)
+            m.logitsTensor(dX.as<float>(), static_cast<uint32_t>(n), dz.as<float>(), rt.stream);
+        else
+            m.logits(dX.as<float>(), static_cast<uint32_t>(n), dz.as<float>(), rt.stream);
         TBLAEQ_CUDA(cudaMemcpyAsync(z_out, dz.get(), n * 4, cudaMemcpyDeviceToHost, rt.stream));
         TBLAEQ_CUDA(cudaStreamSynchronize(rt.stream));
+        if (tensor && m.tensorStatus(rt.stream)) return fail(TBLAEQ_ERR_TIMEOUT, "tensor-core scorer gave up waiting");
         return TBLAEQ_OK;
     });
+}
+
+int tblaeq_scorer_logits(tblaeq_handle* h, const float* X, uint64_t n, float* z_out) {
+    return scorerLogits(h, X, n, z_out, false);
+}
+
+int tblaeq_scorer_logits_tensor(tblaeq_handle* h, const float* X, uint64_t n, float* z_out) {
+    return scorerLogits(h, X, n, z_out, true);
 }
 
 int tblaeq_host_array(const tblaeq_handle* h, int which, uint64_t l, const void** ptr, uint64_t* count) {

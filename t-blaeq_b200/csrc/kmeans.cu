@@ -1,5 +1,6 @@
 // Hierarchical k-means build (see kmeans.cuh).
 #include "kmeans.cuh"
+#include "tcgen05.cuh"
 
 #include <algorithm>
 #include <chrono>
@@ -28,10 +29,7 @@ constexpr uint32_t kTmemCols = 2 * kTileN;                   // two accumulator 
 constexpr size_t kAssignSmem = 100 * 1024;
 constexpr uint32_t kSpinLimit = 1u << 22;                    // bounded mbarrier waits
 
-// Instruction descriptor of tcgen05.mma kind::tf32: D = F32 (bits 4-5 = 1), A = B = TF32 (bits 7-9,
-// 10-12 = 2), both K-major, N = 128 (bits 17-22 = N/8), M = 128 (bits 24-28 = M/16).
-constexpr uint32_t kIdesc = (1u << 4) | (2u << 7) | (2u << 10) | (static_cast<uint32_t>(kTileN >> 3) << 17) |
-                            (static_cast<uint32_t>(kTileM >> 4) << 24);
+constexpr uint32_t kIdesc = tc::instrDesc(tc::kFmtTf32, kTileM, kTileN);
 
 // Byte offset of element (row r, column k) in a K-major, non-swizzled operand image: 8-row x
 // 16-byte core matrices (4 values per row), the four K quarters of a row group 128 B apart
@@ -42,67 +40,23 @@ __host__ __device__ constexpr uint32_t imageOffset(uint32_t r, uint32_t k) {
 }
 constexpr uint32_t kSecondK = 256;  // byte offset of K = 8..15 within an image row group
 
-__device__ __forceinline__ uint32_t smemAddr(const void* p) {
-    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
-}
+using tc::bulkLoad;
+using tc::mbarArrive;
+using tc::mbarExpectTx;
+using tc::mbarInit;
+using tc::mmaCommit;
+using tc::smemAddr;
+using tc::tcFenceAfter;
+using tc::tcFenceBefore;
+using tc::tmemLoad32;
+using tc::tmemWaitLoad;
 
-// Shared-memory matrix descriptor (sm100 version 1), no swizzle, LBO = 128 B, SBO = 512 B.
-__device__ __forceinline__ uint64_t ummaDesc(uint32_t saddr) {
-    return static_cast<uint64_t>((saddr & 0x3FFFFu) >> 4) | (static_cast<uint64_t>(128u >> 4) << 16) |
-           (static_cast<uint64_t>(512u >> 4) << 32) | (1ull << 46);
-}
-
-__device__ __forceinline__ void mbarInit(uint64_t* bar, uint32_t count) {
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smemAddr(bar)), "r"(count) : "memory");
-}
-__device__ __forceinline__ void mbarExpectTx(uint64_t* bar, uint32_t bytes) {
-    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smemAddr(bar)), "r"(bytes) : "memory");
-}
-__device__ __forceinline__ bool mbarTryWait(uint64_t* bar, uint32_t phase) {
-    uint32_t ok;
-    asm volatile(
-        "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\tselp.u32 %0, 1, 0, p;\n\t}\n"
-        : "=r"(ok)
-        : "r"(smemAddr(bar)), "r"(phase)
-        : "memory");
-    return ok != 0;
-}
-// Bounded wait for a phase of an mbarrier; false when it gave up.
-__device__ __forceinline__ bool mbarWait(uint64_t* bar, uint32_t phase) {
-    for (uint32_t i = 0; i < kSpinLimit; ++i)
-        if (mbarTryWait(bar, phase)) return true;
-    return false;
-}
-__device__ __forceinline__ void bulkLoad(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
-    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
-                     smemAddr(dst)),
-                 "l"(src), "r"(bytes), "r"(smemAddr(bar))
-                 : "memory");
-}
-__device__ __forceinline__ void tcFenceBefore() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
-__device__ __forceinline__ void tcFenceAfter() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+// No swizzle, LBO = 128 B, SBO = 512 B (see imageOffset).
+__device__ __forceinline__ uint64_t ummaDesc(uint32_t saddr) { return tc::smemDesc(saddr, 128, 512); }
+__device__ __forceinline__ bool mbarWait(uint64_t* bar, uint32_t phase) { return tc::mbarWait(bar, phase, kSpinLimit); }
 __device__ __forceinline__ void mmaTf32(uint32_t dtmem, uint64_t adesc, uint64_t bdesc, uint32_t accumulate) {
-    asm volatile(
-        "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
-        "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n" ::"r"(dtmem),
-        "l"(adesc), "l"(bdesc), "r"(kIdesc), "r"(accumulate), "r"(0u), "r"(0u), "r"(0u), "r"(0u)
-        : "memory");
+    tc::mma<tc::kKindTf32>(dtmem, adesc, bdesc, kIdesc, accumulate);
 }
-__device__ __forceinline__ void mmaCommit(uint64_t* bar) {
-    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smemAddr(bar))
-                 : "memory");
-}
-__device__ __forceinline__ void tmemLoad32(uint32_t taddr, uint32_t (&r)[32]) {
-    asm volatile(
-        "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, "
-        "%15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31}, [%32];"
-        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
-          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]),
-          "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]),
-          "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
-        : "r"(taddr));
-}
-__device__ __forceinline__ void tmemWaitLoad() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
 
 // ---- packing ----------------------------------------------------------------------------------
 // v = h + l: h is v rounded to nearest-even at TF32 precision (10 fraction bits), l = v - h is
@@ -180,10 +134,6 @@ __device__ __forceinline__ void keepTwo(float v, uint32_t i, float& s1, uint32_t
     }
 }
 
-__device__ __forceinline__ void mbarArrive(uint64_t* bar) {
-    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smemAddr(bar)) : "memory");
-}
-
 __global__ void __launch_bounds__(kAssignThreads, 2)
     assignTcKernel(const uint8_t* points, const uint8_t* cents, uint64_t n, uint32_t nTiles, uint2* cand,
                    uint32_t* status) {
@@ -213,13 +163,10 @@ __global__ void __launch_bounds__(kAssignThreads, 2)
             mbarInit(&accFree[i], kConsumerWarps);
         }
         *sAbort = 0;
-        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        tc::mbarInitFence();
     }
     if (warp == 0) {
-        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smemAddr(sTmem)),
-                     "r"(kTmemCols)
-                     : "memory");
-        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+        tc::tmemAlloc(sTmem, kTmemCols);
     }
     tcFenceBefore();
     __syncthreads();
@@ -337,7 +284,7 @@ __global__ void __launch_bounds__(kAssignThreads, 2)
     __syncthreads();
     tcFenceAfter();
     if (warp == 0) {
-        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tbase), "r"(kTmemCols) : "memory");
+        tc::tmemDealloc(tbase, kTmemCols);
     }
     // Merge the two column halves of every row through shared memory (the stages are idle now).
     float* mv = reinterpret_cast<float*>(sB);

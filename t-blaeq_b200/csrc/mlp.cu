@@ -1,5 +1,6 @@
 // Learned frontier scorer (see mlp.cuh): feature build, forward, backward and Adam kernels.
 #include "mlp.cuh"
+#include "tcgen05.cuh"
 
 #include <cuda_bf16.h>
 
@@ -187,28 +188,225 @@ __global__ void toBf16Kernel(const float* w, size_t n, __nv_bfloat16* wb) {
         wb[i] = __float2bfloat16(w[i]);
 }
 
-// Scores the entries of a KNN frontier in place: features from the entry's centre, its query
-// point and its subtree radius; score = -logit.
-__global__ void scoreFrontierKernel(const __nv_bfloat16* p, int nParams, const uint32_t* q, const uint32_t* node,
-                                    const double* x, const uint32_t* hdr, uint32_t cap, const double* points,
-                                    const NodeRec* nodes, uint32_t level, int levels, int D, double inv,
-                                    double* score) {
-    extern __shared__ float w[];
-    loadWeights(p, nParams, w);
-    const int in = 2 * D + 1 + levels;
-    const uint32_t n = min(hdr[0], cap);
-    float feat[kMlpMaxIn];
-    for (uint32_t e = blockIdx.x * blockDim.x + threadIdx.x; e < n; e += gridDim.x * blockDim.x) {
-        const double* pt = points + static_cast<size_t>(q[e]) * D;
-        const double* c = x + static_cast<size_t>(e) * D;
-        for (int d = 0; d < D; ++d) {
-            feat[d] = static_cast<float>(pt[d] * inv);
-            feat[D + d] = static_cast<float>(c[d] * inv);
-        }
-        feat[2 * D] = static_cast<float>(nodes[node[e]].rad * inv);
-        for (int l = 0; l < levels; ++l) feat[2 * D + 1 + l] = (l == static_cast<int>(level)) ? 1.f : 0.f;
-        score[e] = -static_cast<double>(forwardOne<false>(feat, in, w, nullptr, nullptr));
+// ---- tensor-core forward (tcgen05, BF16 operands, FP32 accumulation in tensor memory) ----------
+//
+// One CTA of 128 threads takes 128 samples at a time: thread r builds sample r's features into a
+// BF16 K-major operand image, one thread issues layer 1 (M=128, N=64, K=16 per MMA) into tensor
+// memory columns 0-63, every thread reads its row back, applies bias + ReLU and writes BF16 h1 into
+// a second image, layer 2 lands in columns 64-127, and the epilogue finishes ReLU, the w3 dot
+// product and the logit. The weights' BF16 images stay in shared memory for the CTA's lifetime.
+constexpr int kTcRows = 128;
+constexpr uint32_t kTcCols = 128;
+constexpr uint32_t kTcSpin = 1u << 22;
+constexpr uint32_t kTcIdesc = tc::instrDesc(tc::kFmtBf16, kTcRows, H);
+// Shared memory requested per CTA: at most four CTAs share an SM, so their 4 x 128 tensor-memory
+// columns always fit and an allocation never waits.
+constexpr size_t kTcSmemRequest = 54 * 1024;
+constexpr int kTcCtasPerSm = 4;
+
+// Byte offset of (row r, column k) in a K-major, non-swizzled BF16 image with K columns: 8-row x
+// 16-byte core matrices (8 values per row), K-adjacent core matrices 128 B apart, 8-row groups
+// K * 16 B apart. One K=16 MMA reads two core matrices; the next K slice starts 256 B further.
+__host__ __device__ constexpr uint32_t bf16Offset(uint32_t r, uint32_t k, uint32_t K) {
+    return (r >> 3) * (K / 8u) * 128u + (k >> 3) * 128u + (r & 7u) * 16u + (k & 7u) * 2u;
+}
+
+struct TcLayout {
+    uint32_t kp = 0;  // input width rounded up to 16
+    uint32_t w1 = 0, w2 = 0, f = 0, h = 0, b1 = 0, b2 = 0, w3 = 0, bar = 0, tmem = 0, end = 0;  // byte offsets
+    __host__ __device__ constexpr explicit TcLayout(int in) {
+        kp = (static_cast<uint32_t>(in) + 15u) & ~15u;
+        w1 = 0;                             // B of layer 1: 64 rows (hidden unit) x kp (input)
+        w2 = w1 + 64u * kp * 2u;            // B of layer 2: 64 x 64
+        f = w2 + 64u * 64u * 2u;            // A of layer 1: 128 samples x kp
+        h = f + 128u * kp * 2u;             // A of layer 2: 128 samples x 64
+        b1 = h + 128u * 64u * 2u;           // FP32 b1[64], b2[64], w3[64], b3
+        b2 = b1 + 256u;
+        w3 = b2 + 256u;
+        bar = (w3 + 260u + 7u) & ~7u;
+        tmem = bar + 8u;
+        end = tmem + 4u;
     }
+};
+static_assert(TcLayout(kMlpMaxIn).end <= kTcSmemRequest, "scorer tile layout exceeds its shared memory");
+
+// Eight consecutive values packed as BF16 into one 16-byte core-matrix row.
+__device__ __forceinline__ uint4 packBf16x8(const float (&v)[8]) {
+    uint4 u;
+    uint32_t* w = reinterpret_cast<uint32_t*>(&u);
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+        const __nv_bfloat162 b = __floats2bfloat162_rn(v[2 * i], v[2 * i + 1]);
+        w[i] = *reinterpret_cast<const uint32_t*>(&b);
+    }
+    return u;
+}
+
+struct FeatureSrc {
+    // Frontier features: query point, cluster centre, subtree radius, level one-hot.
+    const uint32_t* q;
+    const uint32_t* node;
+    const double* x;
+    const double* points;
+    const NodeRec* nodes;
+    uint32_t level;
+    double inv;
+    // Plain features: X[n][in].
+    const float* X;
+};
+
+// Feature k (< in) of frontier entry e, as frontierFeaturesKernel builds it.
+__device__ __forceinline__ float frontierFeature(const FeatureSrc& s, uint32_t e, int k, int D) {
+    if (k < D) return static_cast<float>(s.points[static_cast<size_t>(s.q[e]) * D + k] * s.inv);
+    if (k < 2 * D) return static_cast<float>(s.x[static_cast<size_t>(e) * D + (k - D)] * s.inv);
+    if (k == 2 * D) return static_cast<float>(s.nodes[s.node[e]].rad * s.inv);
+    return (k - 2 * D - 1 == static_cast<int>(s.level)) ? 1.f : 0.f;
+}
+
+// FRONTIER: n = min(hdr[0], cap) frontier entries, out = score (double, -logit).
+// Plain:    n samples of X[n][in], out = logit (float).
+template <bool FRONTIER>
+__global__ void __launch_bounds__(kTcRows) forwardTcKernel(const __nv_bfloat16* p, int D, int levels,
+                                                          FeatureSrc src, const uint32_t* hdr, uint32_t nPlain,
+                                                          uint32_t cap, void* out, uint32_t* status) {
+    extern __shared__ __align__(1024) uint8_t smem[];
+    const int in = 2 * D + 1 + levels;
+    const TcLayout L(in);
+    const uint32_t n = FRONTIER ? min(hdr[0], cap) : nPlain;
+    if (static_cast<uint64_t>(blockIdx.x) * kTcRows >= n) return;
+    const int tid = threadIdx.x, warp = tid >> 5;
+    uint64_t* bar = reinterpret_cast<uint64_t*>(smem + L.bar);
+    uint32_t* sTmem = reinterpret_cast<uint32_t*>(smem + L.tmem);
+    float* b1 = reinterpret_cast<float*>(smem + L.b1);
+    float* b2 = reinterpret_cast<float*>(smem + L.b2);
+    float* w3 = reinterpret_cast<float*>(smem + L.w3);
+
+    // Weights: B images hold W^T (row = hidden unit j, column = input k), zero past `in`.
+    const size_t oB1 = static_cast<size_t>(in) * H, oW2 = oB1 + H, oB2 = oW2 + H * H, oW3 = oB2 + H;
+    for (uint32_t i = tid; i < 64u * L.kp; i += blockDim.x) {
+        const uint32_t j = i / L.kp, k = i % L.kp;
+        *reinterpret_cast<__nv_bfloat16*>(smem + L.w1 + bf16Offset(j, k, L.kp)) =
+            k < static_cast<uint32_t>(in) ? p[static_cast<size_t>(k) * H + j] : __float2bfloat16(0.f);
+    }
+    for (uint32_t i = tid; i < 64u * 64u; i += blockDim.x) {
+        const uint32_t j = i / 64u, k = i % 64u;
+        *reinterpret_cast<__nv_bfloat16*>(smem + L.w2 + bf16Offset(j, k, 64)) = p[oW2 + static_cast<size_t>(k) * H + j];
+    }
+    for (int j = tid; j < H; j += blockDim.x) {
+        b1[j] = __bfloat162float(p[oB1 + j]);
+        b2[j] = __bfloat162float(p[oB2 + j]);
+        w3[j] = __bfloat162float(p[oW3 + j]);
+    }
+    if (tid == 0) {
+        w3[H] = __bfloat162float(p[oW3 + H]);
+        tc::mbarInit(bar, 1);
+        tc::mbarInitFence();
+    }
+    if (warp == 0) tc::tmemAlloc(sTmem, kTcCols);
+    tc::fenceProxyAsync();
+    tc::tcFenceBefore();
+    __syncthreads();
+    tc::tcFenceAfter();
+    const uint32_t tbase = *sTmem;
+    const uint32_t laneBase = static_cast<uint32_t>(warp * 32) << 16;
+    const uint32_t fAddr = tc::smemAddr(smem + L.f), hAddr = tc::smemAddr(smem + L.h);
+    const uint32_t w1Addr = tc::smemAddr(smem + L.w1), w2Addr = tc::smemAddr(smem + L.w2);
+    uint32_t phase = 0, pending = 0;
+    bool ok = true;
+
+    for (uint64_t tile = blockIdx.x; tile * kTcRows < n; tile += gridDim.x) {
+        const uint32_t e = static_cast<uint32_t>(tile * kTcRows) + tid;
+        const bool live = e < n;
+        // Features of this thread's sample, 8 columns (one 16-byte core-matrix row) at a time.
+        for (uint32_t k0 = 0; k0 < L.kp; k0 += 8) {
+            float v[8];
+#pragma unroll
+            for (int i = 0; i < 8; ++i) {
+                const int k = static_cast<int>(k0) + i;
+                float f = 0.f;
+                if (live && k < in) {
+                    if constexpr (FRONTIER)
+                        f = frontierFeature(src, e, k, D);
+                    else
+                        f = src.X[static_cast<size_t>(e) * in + k];
+                }
+                v[i] = f;
+            }
+            *reinterpret_cast<uint4*>(smem + L.f + bf16Offset(tid, k0, L.kp)) = packBf16x8(v);
+        }
+        tc::fenceProxyAsync();
+        tc::tcFenceBefore();
+        __syncthreads();
+        tc::tcFenceAfter();
+        if (tid == 0) {
+            for (uint32_t ks = 0; ks < L.kp / 16; ++ks)
+                tc::mma<tc::kKindF16>(tbase, tc::smemDesc(fAddr + ks * 256u, 128, L.kp * 16u),
+                                      tc::smemDesc(w1Addr + ks * 256u, 128, L.kp * 16u), kTcIdesc, ks);
+            tc::mmaCommit(bar);
+        }
+        ++pending;
+        ok = __syncthreads_and(tc::mbarWait(bar, phase, kTcSpin)) != 0;
+        phase ^= 1u;
+        if (!ok) break;
+        --pending;
+        tc::tcFenceAfter();
+        // h1 = relu(acc + b1) as BF16 into the layer-2 A image.
+#pragma unroll
+        for (int c = 0; c < 64; c += 32) {
+            uint32_t r[32];
+            tc::tmemLoad32(tbase + laneBase + static_cast<uint32_t>(c), r);
+            tc::tmemWaitLoad();
+#pragma unroll
+            for (int g = 0; g < 32; g += 8) {
+                float v[8];
+#pragma unroll
+                for (int i = 0; i < 8; ++i) v[i] = fmaxf(__uint_as_float(r[g + i]) + b1[c + g + i], 0.f);
+                *reinterpret_cast<uint4*>(smem + L.h + bf16Offset(tid, c + g, 64)) = packBf16x8(v);
+            }
+        }
+        tc::fenceProxyAsync();
+        tc::tcFenceBefore();
+        __syncthreads();
+        tc::tcFenceAfter();
+        if (tid == 0) {
+#pragma unroll
+            for (uint32_t ks = 0; ks < 4; ++ks)
+                tc::mma<tc::kKindF16>(tbase + 64u, tc::smemDesc(hAddr + ks * 256u, 128, 1024),
+                                      tc::smemDesc(w2Addr + ks * 256u, 128, 1024), kTcIdesc, ks);
+            tc::mmaCommit(bar);
+        }
+        ++pending;
+        ok = __syncthreads_and(tc::mbarWait(bar, phase, kTcSpin)) != 0;
+        phase ^= 1u;
+        if (!ok) break;
+        --pending;
+        tc::tcFenceAfter();
+        float z = w3[H];
+#pragma unroll
+        for (int c = 0; c < 64; c += 32) {
+            uint32_t r[32];
+            tc::tmemLoad32(tbase + laneBase + 64u + static_cast<uint32_t>(c), r);
+            tc::tmemWaitLoad();
+#pragma unroll
+            for (int i = 0; i < 32; ++i) z = fmaf(fmaxf(__uint_as_float(r[i]) + b2[c + i], 0.f), w3[c + i], z);
+        }
+        if (live) {
+            if (FRONTIER)
+                static_cast<double*>(out)[e] = -static_cast<double>(z);
+            else
+                static_cast<float*>(out)[e] = z;
+        }
+        tc::tcFenceBefore();
+    }
+    // A CTA that gave up waits once more (bounded) for its MMAs still in flight before freeing.
+    if (!ok) {
+        if (tid == 0) atomicOr(status, 1u);
+        if (pending) tc::mbarWait(bar, phase ^ 1u, kTcSpin);
+    }
+    tc::tcFenceBefore();
+    __syncthreads();
+    tc::tcFenceAfter();
+    if (warp == 0) tc::tmemDealloc(tbase, kTcCols);
 }
 
 __global__ void frontierFeaturesKernel(const uint32_t* q, const uint32_t* node, const double* x, const uint32_t* idx,
@@ -240,6 +438,8 @@ Mlp::Mlp(MlpShape shape) : shape_(shape) {
     bf16_.alloc(n * 2);
     adamM_.alloc(n * 4);
     adamV_.alloc(n * 4);
+    tcStatus_.alloc(4);
+    TBLAEQ_CUDA(cudaMemset(tcStatus_.get(), 0, 4));
 }
 
 void Mlp::refreshBf16(cudaStream_t s) {
@@ -344,16 +544,37 @@ void Mlp::frontierFeatures(const FrontierIn& f, const uint32_t* node, const uint
     TBLAEQ_CUDA(cudaGetLastError());
 }
 
+void Mlp::launchTc(bool frontier, const void* srcPtr, const uint32_t* hdr, uint32_t n, uint32_t cap, void* out,
+                   cudaStream_t s) const {
+    const FeatureSrc* src = static_cast<const FeatureSrc*>(srcPtr);
+    const uint32_t rows = frontier ? cap : n;
+    if (rows == 0) return;
+    const uint32_t tiles = (rows + kTcRows - 1) / kTcRows;
+    const unsigned grid = std::min<uint32_t>(tiles, 148u * kTcCtasPerSm);
+    const auto kern = frontier ? forwardTcKernel<true> : forwardTcKernel<false>;
+    TBLAEQ_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     static_cast<int>(kTcSmemRequest)));
+    kern<<<grid, kTcRows, kTcSmemRequest, s>>>(bf16_.as<__nv_bfloat16>(), shape_.D, shape_.levels, *src, hdr, n, cap,
+                                               out, tcStatus_.as<uint32_t>());
+    TBLAEQ_CUDA(cudaGetLastError());
+}
+
 void Mlp::scoreFrontier(const FrontierIn& f, const uint32_t* node, uint32_t cap, const double* points,
                         const NodeRec* nodes, uint32_t level, double invScale, double* score, cudaStream_t s) const {
-    const Offsets o = offsetsOf(shape_);
-    const size_t smem = o.total * 4;
-    TBLAEQ_CUDA(cudaFuncSetAttribute(scoreFrontierKernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     static_cast<int>(smem)));
-    scoreFrontierKernel<<<148 * 2, 128, smem, s>>>(bf16_.as<__nv_bfloat16>(), static_cast<int>(o.total), f.q, node,
-                                                  f.x, f.hdr, cap, points, nodes, level, shape_.levels, shape_.D,
-                                                  invScale, score);
-    TBLAEQ_CUDA(cudaGetLastError());
+    FeatureSrc src{f.q, node, f.x, points, nodes, level, invScale, nullptr};
+    launchTc(true, &src, f.hdr, 0, cap, score, s);
+}
+
+void Mlp::logitsTensor(const float* X, uint32_t n, float* z, cudaStream_t s) const {
+    FeatureSrc src{nullptr, nullptr, nullptr, nullptr, nullptr, 0, 0.0, X};
+    launchTc(false, &src, nullptr, n, 0, z, s);
+}
+
+uint32_t Mlp::tensorStatus(cudaStream_t s) const {
+    uint32_t v = 0;
+    TBLAEQ_CUDA(cudaMemcpyAsync(&v, tcStatus_.get(), 4, cudaMemcpyDeviceToHost, s));
+    TBLAEQ_CUDA(cudaStreamSynchronize(s));
+    return v;
 }
 
 }  // namespace tblaeq

@@ -9,7 +9,8 @@
 //   z  = w3 . h2 + b3                    logit of "the cluster holds one of the query's K nearest"
 //
 // Weights are kept as an FP32 master copy for training and a BF16 copy used by every forward pass
-// (training and inference); accumulation is FP32.
+// (training and inference); accumulation is FP32. Training runs on CUDA cores; frontier inference
+// runs on the tcgen05 tensor cores.
 #pragma once
 
 #include <cstdint>
@@ -62,16 +63,27 @@ public:
                           const double* points, const NodeRec* nodes, uint32_t level, double invScale, float* X,
                           cudaStream_t s) const;
 
-    // Scores the entries of a KNN frontier: score[e] = -logit (ascending order = most promising).
+    // Scores the entries of a KNN frontier on the tensor cores: score[e] = -logit (ascending order =
+    // most promising). Features are built in the kernel; both layers are tcgen05 BF16 MMAs with FP32
+    // accumulation in tensor memory, so h1 is rounded to BF16 between the layers.
     void scoreFrontier(const FrontierIn& f, const uint32_t* node, uint32_t cap, const double* points,
                        const NodeRec* nodes, uint32_t level, double invScale, double* score, cudaStream_t s) const;
 
+    // Logits of n samples through the same tensor-core kernel as scoreFrontier.
+    void logitsTensor(const float* X, uint32_t n, float* z, cudaStream_t s) const;
+
+    // Nonzero once a tensor-core launch gave up waiting for its MMAs (sticky; never expected).
+    // A frontier scored by such a launch only changes the expansion order, never a result.
+    uint32_t tensorStatus(cudaStream_t s) const;
+
 private:
     MlpShape shape_;
-    DeviceMem master_, bf16_, adamM_, adamV_, work_;
+    DeviceMem master_, bf16_, adamM_, adamV_, work_, tcStatus_;
     size_t workCap_ = 0;
     int step_ = 0;
     void refreshBf16(cudaStream_t s);
+    void launchTc(bool frontier, const void* src, const uint32_t* hdr, uint32_t n, uint32_t cap, void* out,
+                  cudaStream_t s) const;
 };
 
 }  // namespace tblaeq

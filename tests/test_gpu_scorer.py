@@ -78,6 +78,29 @@ def test_scorer_gradients_and_logits_match_cpu(tb, env):
     assert np.allclose(z, ref_z, rtol=2e-3, atol=1e-3)
 
 
+def test_tensor_core_logits_match_bf16_model(tb, env):
+    """The frontier-scoring kernel (tcgen05, BF16 operands, FP32 accumulation in tensor memory)
+    against the float64 model with the same roundings: features and h1 in BF16. Sizes cover one
+    row, a ragged tile and many tiles per CTA (the persistent loop)."""
+    h = env[0]
+    p0 = h.scorer_params()
+    n_in = (p0.size - 1 - 3 * HID - HID * HID) // HID
+    rng = np.random.default_rng(4)
+    p = rng.normal(0, 0.2, p0.size).astype(np.float32)
+    h.scorer_set_params(p)
+    W1, b1, W2, b2, w3, b3 = split(bf16(p), n_in)
+    for n in (1, 300, 200000):
+        X = rng.uniform(-1, 1, (n, n_in)).astype(np.float32)
+        h1 = bf16(np.maximum(bf16(X) @ W1 + b1, 0))
+        ref = np.maximum(h1 @ W2 + b2, 0) @ w3 + b3
+        z = h.scorer_logits(X, tensor=True)
+        assert np.allclose(z, ref, rtol=2e-3, atol=2e-3 * np.abs(ref).max()), n
+        # against the CUDA-core forward (FP32 features and h1): the BF16 roundings only
+        z32 = h.scorer_logits(X)
+        assert np.abs(z - z32).max() <= 0.05 * np.abs(z32).max() + 0.05, n
+    assert h.scorer_logits(np.zeros((0, n_in), np.float32), tensor=True).size == 0
+
+
 def _points(pts, n, seed, noise):
     rng = np.random.default_rng(seed)
     return np.ascontiguousarray(pts[rng.integers(0, len(pts), n)] + rng.normal(0, noise, (n, pts.shape[1])))
