@@ -316,6 +316,13 @@ int tblaeq_kmeans_build(const float* points, uint64_t N, uint64_t D, uint64_t he
 int tblaeq_kmeans(const float* points, uint64_t n, uint64_t D, uint64_t k, const tblaeq_build_config* cfg,
                   float* centroids_out, uint32_t* labels_out, double* objectives_out);
 
+/* Dataset text file (reference loadFromFile, src/Data_Structures/File.cu:8-50): a header "N D",
+ * then N rows of D values. With points_out == NULL only the header is read into *n and *d; with a
+ * buffer of cap >= N * D doubles the rows are parsed into it, row-major. TBLAEQ_ERR_IO carries the
+ * reference's message (cannot open, empty file, invalid header, dimension mismatch at row r, row
+ * count mismatch); TBLAEQ_ERR_INVALID when cap is too small. */
+int tblaeq_load_points_text(const char* path, double* points_out, uint64_t cap, uint64_t* n, uint64_t* d);
+
 /* ---- Serving loop ------------------------------------------------------------------------------
  * Replaces the reference's one-query-at-a-time request loop behind its HTTP front end
  * (src/HTTPServer.cu:414-550; the HTTP layer itself is not part of this library). A server owns two
@@ -332,6 +339,7 @@ typedef struct {
     int mode;                /* tblaeq_mode for range requests */
     int learned;             /* rank KNN frontiers with the trained scorer, when one exists */
     int lanes;               /* 2 (range and KNN lanes, default when 0) or 1 (one lane, arrival order) */
+    int levels;              /* 1: record each request's per-level child counts (tblaeq_serve_poll_levels) */
 } tblaeq_serve_config;
 
 typedef struct {
@@ -353,6 +361,14 @@ int tblaeq_serve_replay(tblaeq_server* s, uint64_t n, const int* qtypes, const d
  * the result stays. A failed request returns its error code and message and is released. */
 int tblaeq_serve_poll(tblaeq_server* s, uint64_t ticket, int wait_ms, uint64_t* ids_out, double* dist2_out,
                       uint64_t cap, uint64_t* n_out, double* latency_us);
+/* As tblaeq_serve_poll, and the request's generated-children count per level (the reference's
+ * QueryResult::levelFineMeshSize of a single query, src/core/QueryEngine.cu:65-81; one value per
+ * interval, coarsest first) into levels_out when the server records them (config `levels`);
+ * *n_levels receives their count (0 otherwise; at most levels_cap are copied). Serves the HTTP
+ * front end's `level_pruned_sizes` (src/HTTPServer.cu:466-468). */
+int tblaeq_serve_poll_levels(tblaeq_server* s, uint64_t ticket, int wait_ms, uint64_t* ids_out, double* dist2_out,
+                             uint64_t cap, uint64_t* n_out, double* latency_us, uint32_t* levels_out,
+                             uint64_t levels_cap, uint64_t* n_levels);
 /* TBLAEQ_OK once every submitted request has completed, TBLAEQ_ERR_TIMEOUT after wait_ms. */
 int tblaeq_serve_wait_idle(tblaeq_server* s, int wait_ms);
 int tblaeq_serve_stats(tblaeq_server* s, int reset, tblaeq_serve_metrics* out);

@@ -175,7 +175,12 @@ def _load():
                                  P(ctypes.c_uint32), P(ctypes.c_double), P(ctypes.c_uint64)], ctypes.c_int),
         "tblaeq_serve_poll": ([vp, ctypes.c_uint64, ctypes.c_int, P(ctypes.c_uint64), P(ctypes.c_double),
                                ctypes.c_uint64, P(ctypes.c_uint64), P(ctypes.c_double)], ctypes.c_int),
+        "tblaeq_serve_poll_levels": ([vp, ctypes.c_uint64, ctypes.c_int, P(ctypes.c_uint64), P(ctypes.c_double),
+                                      ctypes.c_uint64, P(ctypes.c_uint64), P(ctypes.c_double), P(ctypes.c_uint32),
+                                      ctypes.c_uint64, P(ctypes.c_uint64)], ctypes.c_int),
         "tblaeq_serve_wait_idle": ([vp, ctypes.c_int], ctypes.c_int),
+        "tblaeq_load_points_text": ([ctypes.c_char_p, P(ctypes.c_double), ctypes.c_uint64, P(ctypes.c_uint64),
+                                     P(ctypes.c_uint64)], ctypes.c_int),
         "tblaeq_serve_stats": ([vp, ctypes.c_int, P(_ServeMetrics)], ctypes.c_int),
         "tblaeq_serve_stop": ([vp], ctypes.c_int),
     }
@@ -189,7 +194,7 @@ def _load():
 
 class _ServeConfig(ctypes.Structure):
     _fields_ = [("max_batch", ctypes.c_uint32), ("memory_budget", ctypes.c_uint64), ("mode", ctypes.c_int),
-                ("learned", ctypes.c_int), ("lanes", ctypes.c_int)]
+                ("learned", ctypes.c_int), ("lanes", ctypes.c_int), ("levels", ctypes.c_int)]
 
 
 class _ServeMetrics(ctypes.Structure):
@@ -311,6 +316,20 @@ class QueryHandler:
         obj = cls(_handle=h)
         obj.dataset_name = f"Gen{N}D{D}"
         return obj
+
+    @classmethod
+    def build_from_file(cls, dataset_path: str, force_cpu: bool = False, height: int = 4,
+                        ratios: Sequence[int] = (100, 50, 20), iters: int = 20, seed: int = 1) -> tuple:
+        """QueryHandler(forceUseCPU, datasetPath, height, ratios) (src/core/QueryHandler.cu:60-77):
+        reads the dataset text file, truncates the plan like adjustBuildPlan and builds on the GPU.
+        force_cpu (the reference's CPU k-means) selects the FP64 CUDA-core assignment here: the
+        precision of a CPU build, still on the device. Returns (handler, per-level reports)."""
+        X = load_dataset_file(dataset_path)
+        height, ratios = adjust_build_plan(X.shape[0], height, ratios)
+        prec = KmeansPrecision.FP64 if force_cpu else KmeansPrecision.TENSOR
+        h, rep = cls.build(X, height=height, ratios=ratios, iters=iters, seed=seed, precision=prec)
+        h.dataset_name = extract_dataset_name(dataset_path)
+        return h, rep
 
     @classmethod
     def build(cls, points, height: int = 4, ratios: Sequence[int] = (100, 50, 20), iters: int = 20, seed: int = 1,
@@ -662,10 +681,13 @@ class Server:
     src/HTTPServer.cu:414-550). Results are exact; KNN results carry squared distances."""
 
     def __init__(self, handler: "QueryHandler", max_batch: int = 4096, memory_budget: int = 0,
-                 mode: Mode = Mode.EXACT, learned: bool = True, lanes: int = 2):
+                 mode: Mode = Mode.EXACT, learned: bool = True, lanes: int = 2, levels: bool = False):
+        """levels=True records every request's generated-children count per level (returned by
+        poll_levels), at the cost of per-query counters in every expand launch."""
         self._owner = handler
         self._D = handler.info()["D"]
-        cfg = _ServeConfig(max_batch, memory_budget, int(mode), int(learned), lanes)
+        self._intervals = handler.info()["intervals"]
+        cfg = _ServeConfig(max_batch, memory_budget, int(mode), int(learned), lanes, int(levels))
         s = ctypes.c_void_p()
         _check(_load().tblaeq_serve_start(handler._h, ctypes.byref(cfg), ctypes.byref(s)))
         self._s = s
@@ -693,14 +715,23 @@ class Server:
 
     def poll(self, ticket: int, wait_ms: int = 10000):
         """(ids, dist2 or None, latency_us) once done; None if not done within wait_ms."""
+        r = self.poll_levels(ticket, wait_ms)
+        return None if r is None else r[:3]
+
+    def poll_levels(self, ticket: int, wait_ms: int = 10000):
+        """(ids, dist2, latency_us, per-level child counts) once done (the counts are empty unless
+        the server was started with levels=True); None if not done within wait_ms."""
         lib = _load()
         cap = 1024
         while True:
             ids = np.empty(cap, np.uint64)
             d2 = np.empty(cap, np.float64)
-            n, lat = ctypes.c_uint64(), ctypes.c_double()
-            code = lib.tblaeq_serve_poll(self._s, int(ticket), wait_ms, _dptr(ids, ctypes.c_uint64), _dptr(d2), cap,
-                                         ctypes.byref(n), ctypes.byref(lat))
+            lv = np.zeros(max(1, self._intervals), np.uint32)
+            n, lat, nl = ctypes.c_uint64(), ctypes.c_double(), ctypes.c_uint64()
+            code = lib.tblaeq_serve_poll_levels(self._s, int(ticket), wait_ms, _dptr(ids, ctypes.c_uint64), _dptr(d2),
+                                                cap, ctypes.byref(n), ctypes.byref(lat),
+                                                lv.ctypes.data_as(ctypes.POINTER(ctypes.c_uint32)), len(lv),
+                                                ctypes.byref(nl))
             if code == 6:
                 return None
             if code == 5:
@@ -708,7 +739,7 @@ class Server:
                 continue
             _check(code)
             k = int(n.value)
-            return ids[:k], d2[:k], lat.value
+            return ids[:k], d2[:k], lat.value, lv[:min(int(nl.value), len(lv))].astype(np.int64)
 
     def wait_idle(self, wait_ms: int = 60000) -> bool:
         code = _load().tblaeq_serve_wait_idle(self._s, wait_ms)
@@ -760,6 +791,43 @@ def save_query_file(path: str, q_type: QueryType, rows: np.ndarray, D: int):
         f.write(f"{rows.shape[0]} {D}\n")
         for r in rows:
             f.write(" ".join("%.17g" % v for v in r) + "\n")
+
+
+def load_dataset_file(path: str) -> np.ndarray:
+    """Dataset text file (loadFromFile, src/Data_Structures/File.cu:8-50): header "N D", then N rows
+    of D values; returns an (N, D) float64 array. Raises TblaeqError (TBLAEQ_ERR_IO) with the
+    reference's message on a malformed file."""
+    lib = _load()
+    n, d = ctypes.c_uint64(), ctypes.c_uint64()
+    _check(lib.tblaeq_load_points_text(os.fsencode(path), None, 0, ctypes.byref(n), ctypes.byref(d)))
+    X = np.empty((n.value, d.value), np.float64)
+    _check(lib.tblaeq_load_points_text(os.fsencode(path), _dptr(X), X.size, ctypes.byref(n), ctypes.byref(d)))
+    return X
+
+
+def adjust_build_plan(N: int, height: int, ratios: Sequence[int]):
+    """adjustBuildPlan (src/core/QueryHandler.cu:23-45): drops the levels above the first one that
+    would hold a single centroid. Returns (height, ratios)."""
+    if height < 2:
+        raise ValueError("QueryHandler: height must be >= 2")
+    ratios = [int(r) for r in ratios]
+    if len(ratios) != height - 1:
+        raise ValueError("QueryHandler: ratios size must equal height - 1")
+    n, keep = int(N), len(ratios)
+    for i, r in enumerate(ratios):
+        c = 1 if r == 0 or n // r == 0 else n // r
+        if c == 1:
+            keep = i + 1
+            break
+        n = c
+    return keep + 1, ratios[:keep]
+
+
+def extract_dataset_name(path: str) -> str:
+    """extractDatasetName (src/utils/Utils.cu:6-10): the file name up to its first '_'."""
+    base = path[path.rfind("/") + 1:]
+    cut = base.find("_")
+    return base if cut < 0 else base[:cut]
 
 
 def load_query_file(path: str, q_type: QueryType):

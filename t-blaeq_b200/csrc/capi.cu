@@ -779,6 +779,7 @@ int tblaeq_serve_start(tblaeq_handle* h, const tblaeq_serve_config* cfg, tblaeq_
             sc.mode = cfg->mode;
             sc.learned = cfg->learned != 0;
             if (cfg->lanes) sc.lanes = cfg->lanes;
+            sc.levels = cfg->levels != 0;
         }
         auto s = std::make_unique<tblaeq_server>();
         s->server = std::make_unique<Server>(h->qh->runtime(), sc);
@@ -808,14 +809,16 @@ int tblaeq_serve_replay(tblaeq_server* s, uint64_t n, const int* qtypes, const d
     });
 }
 
-int tblaeq_serve_poll(tblaeq_server* s, uint64_t ticket, int wait_ms, uint64_t* ids_out, double* dist2_out,
-                      uint64_t cap, uint64_t* n_out, double* latency_us) {
+static int servePoll(tblaeq_server* s, uint64_t ticket, int wait_ms, uint64_t* ids_out, double* dist2_out,
+                     uint64_t cap, uint64_t* n_out, double* latency_us, uint32_t* levels_out, uint64_t levels_cap,
+                     uint64_t* n_levels) {
     if (!s || !s->server) return fail(TBLAEQ_ERR_INVALID, "null server");
     return guarded([&]() -> int {
         Server::Result r;
         if (!s->server->poll(ticket, r, wait_ms)) return fail(TBLAEQ_ERR_TIMEOUT, "request not done yet");
         if (latency_us) *latency_us = r.latencyUs;
         if (n_out) *n_out = r.ids.size();
+        if (n_levels) *n_levels = r.levels.size();
         if (r.status != 0) return fail(r.status, r.error);
         if (r.ids.size() > cap) {
             // Keep the result for a call with a larger buffer.
@@ -826,8 +829,22 @@ int tblaeq_serve_poll(tblaeq_server* s, uint64_t ticket, int wait_ms, uint64_t* 
         }
         if (ids_out && !r.ids.empty()) std::copy(r.ids.begin(), r.ids.end(), ids_out);
         if (dist2_out && !r.dist2.empty()) std::copy(r.dist2.begin(), r.dist2.end(), dist2_out);
+        if (levels_out)
+            std::copy_n(r.levels.begin(), std::min<uint64_t>(levels_cap, r.levels.size()), levels_out);
         return TBLAEQ_OK;
     });
+}
+
+int tblaeq_serve_poll(tblaeq_server* s, uint64_t ticket, int wait_ms, uint64_t* ids_out, double* dist2_out,
+                      uint64_t cap, uint64_t* n_out, double* latency_us) {
+    return servePoll(s, ticket, wait_ms, ids_out, dist2_out, cap, n_out, latency_us, nullptr, 0, nullptr);
+}
+
+int tblaeq_serve_poll_levels(tblaeq_server* s, uint64_t ticket, int wait_ms, uint64_t* ids_out, double* dist2_out,
+                             uint64_t cap, uint64_t* n_out, double* latency_us, uint32_t* levels_out,
+                             uint64_t levels_cap, uint64_t* n_levels) {
+    return servePoll(s, ticket, wait_ms, ids_out, dist2_out, cap, n_out, latency_us, levels_out, levels_cap,
+                     n_levels);
 }
 
 int tblaeq_serve_wait_idle(tblaeq_server* s, int wait_ms) {
@@ -911,6 +928,28 @@ int tblaeq_kmeans_build(const float* points, uint64_t N, uint64_t D, uint64_t he
         auto h = std::make_unique<tblaeq_handle>();
         h->qh = std::make_unique<QueryHandler>(std::move(idx));
         *out = h.release();
+        return TBLAEQ_OK;
+    });
+}
+
+int tblaeq_load_points_text(const char* path, double* points_out, uint64_t cap, uint64_t* n, uint64_t* d) {
+    if (!path || !n || !d) return fail(TBLAEQ_ERR_INVALID, "null argument");
+    return guarded([&]() -> int {
+        uint64_t rows = 0, dim = 0;
+        try {
+            loadPointsText(path, rows, dim, nullptr);
+            *n = rows;
+            *d = dim;
+            if (!points_out) return TBLAEQ_OK;
+            if (cap < rows * dim) return fail(TBLAEQ_ERR_INVALID, "points buffer smaller than N * D");
+            std::vector<double> pts;
+            loadPointsText(path, rows, dim, &pts);
+            std::copy(pts.begin(), pts.end(), points_out);
+        } catch (const std::bad_alloc&) {
+            throw;
+        } catch (const std::exception& e) {
+            return fail(TBLAEQ_ERR_IO, e.what());
+        }
         return TBLAEQ_OK;
     });
 }

@@ -5,7 +5,9 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
+#include <memory>
 #include <filesystem>
 #include <numeric>
 #include <random>
@@ -405,6 +407,47 @@ HostIndex generateRandomIndex(const GenParams& p) {
     }
     idx.datasetName = "Gen" + std::to_string(p.N) + "D" + std::to_string(D);
     return idx;
+}
+
+void loadPointsText(const std::string& path, uint64_t& n, uint64_t& d, std::vector<double>* points) {
+    std::unique_ptr<FILE, int (*)(FILE*)> f(std::fopen(path.c_str(), "r"), &std::fclose);
+    if (!f) throw std::runtime_error("loadFromFile: cannot open '" + path + "'");
+    struct LineBuf {
+        char* p = nullptr;
+        size_t cap = 0;
+        ~LineBuf() { std::free(p); }
+    } buf;
+    char*& line = buf.p;
+    auto next = [&]() -> bool { return getline(&buf.p, &buf.cap, f.get()) >= 0; };
+    if (!next()) throw std::runtime_error("loadFromFile: empty file '" + path + "'");
+    {
+        // Two integers, both positive (the reference reads them as int).
+        char* end = nullptr;
+        const long long a = std::strtoll(line, &end, 10);
+        char* end2 = nullptr;
+        const long long b = (end != line) ? std::strtoll(end, &end2, 10) : 0;
+        if (end == line || end2 == end || a <= 0 || b <= 0 || a > 0x7fffffffLL || b > 0x7fffffffLL)
+            throw std::runtime_error("loadFromFile: invalid header in '" + path + "'");
+        n = static_cast<uint64_t>(a);
+        d = static_cast<uint64_t>(b);
+    }
+    if (!points) return;
+    points->assign(n * d, 0.0);
+    uint64_t row = 0;
+    while (row < n && next()) {
+        char* p = line;
+        uint64_t col = 0;
+        while (col < d) {
+            char* end = nullptr;
+            const double v = std::strtod(p, &end);
+            if (end == p) break;
+            (*points)[row * d + col++] = v;
+            p = end;
+        }
+        if (col != d) throw std::runtime_error("loadFromFile: dimension mismatch at row " + std::to_string(row + 1));
+        ++row;
+    }
+    if (row != n) throw std::runtime_error("loadFromFile: row count mismatch in '" + path + "'");
 }
 
 }  // namespace tblaeq

@@ -58,6 +58,13 @@ struct HostIndex {
 void saveIndex(const HostIndex& idx, const std::string& dir);
 HostIndex loadIndex(const std::string& dir);
 
+// Dataset text file (src/Data_Structures/File.cu:8-50): a header "N D" (both > 0), then N rows of
+// whitespace-separated values; a row must hold at least D values (the rest of the row is ignored)
+// and lines after row N are not read. Only the header is read when `points` is null; otherwise the
+// rows are parsed into points (N * D values). Errors throw std::runtime_error with the reference's
+// messages.
+void loadPointsText(const std::string& path, uint64_t& n, uint64_t& d, std::vector<double>* points);
+
 // Parameters of the synthetic RandomKmeans-style hierarchy
 // (src/core/QueryHandler.cu:101-124 -> src/core/IndexBuilder.cu:153-234).
 struct GenParams {

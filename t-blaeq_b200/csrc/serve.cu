@@ -220,6 +220,8 @@ void Server::runGroup(Lane& lane, std::vector<Request>& batch, size_t begin, siz
     const size_t row = (qtype == kQtypeRange) ? 2 * D_ : D_;
     std::vector<uint64_t> offs, ids;
     std::vector<double> d2;
+    std::vector<uint32_t> lv;
+    const unsigned flags = cfg_.levels ? kWantLevels : 0u;
     try {
         std::vector<double> hq(n * row);
         std::vector<uint32_t> hk(n);
@@ -233,12 +235,13 @@ void Server::runGroup(Lane& lane, std::vector<Request>& batch, size_t begin, siz
         TBLAEQ_CUDA(cudaMemcpyAsync(lane.dq.get(), hq.data(), hq.size() * 8, cudaMemcpyHostToDevice, lane.stream));
         BatchOutput o;
         if (qtype == kQtypeRange) {
-            o = lane.engine->runRange(lane.dq.as<double>(), static_cast<uint32_t>(n), cfg_.mode, 0);
+            o = lane.engine->runRange(lane.dq.as<double>(), static_cast<uint32_t>(n), cfg_.mode, flags);
         } else {
             if (lane.dk.bytes() < n * 4) lane.dk.alloc(n * 4);
             TBLAEQ_CUDA(cudaMemcpyAsync(lane.dk.get(), hk.data(), n * 4, cudaMemcpyHostToDevice, lane.stream));
             try {
-                o = lane.engine->runKnn(lane.dq.as<double>(), static_cast<uint32_t>(n), lane.dk.as<uint32_t>(), sumK, 0);
+                o = lane.engine->runKnn(lane.dq.as<double>(), static_cast<uint32_t>(n), lane.dk.as<uint32_t>(), sumK,
+                                        flags);
             } catch (const SplitBatch&) {
                 if (n == 1) throw;
                 const size_t mid = begin + n / 2;
@@ -256,18 +259,23 @@ void Server::runGroup(Lane& lane, std::vector<Request>& batch, size_t begin, siz
             d2.resize(offs[n]);
             TBLAEQ_CUDA(cudaMemcpyAsync(d2.data(), o.dist2, offs[n] * 8, cudaMemcpyDeviceToHost, lane.stream));
         }
+        if (o.levelItems) {  // [l * n + q]
+            lv.resize(rt_.dev->intervals * n);
+            TBLAEQ_CUDA(cudaMemcpyAsync(lv.data(), o.levelItems, lv.size() * 4, cudaMemcpyDeviceToHost, lane.stream));
+        }
         TBLAEQ_CUDA(cudaStreamSynchronize(lane.stream));
     } catch (const CudaError& e) {
-        post(batch, begin, end, offs, ids, d2, e.code == cudaErrorMemoryAllocation ? 4 : 3, e.what());
+        post(batch, begin, end, lv, offs, ids, d2, e.code == cudaErrorMemoryAllocation ? 4 : 3, e.what());
         return;
     } catch (const std::exception& e) {
-        post(batch, begin, end, offs, ids, d2, 3, e.what());
+        post(batch, begin, end, lv, offs, ids, d2, 3, e.what());
         return;
     }
-    post(batch, begin, end, offs, ids, d2, 0, "");
+    post(batch, begin, end, lv, offs, ids, d2, 0, "");
 }
 
-void Server::post(std::vector<Request>& batch, size_t begin, size_t end, const std::vector<uint64_t>& offs,
+void Server::post(std::vector<Request>& batch, size_t begin, size_t end, const std::vector<uint32_t>& levels,
+                  const std::vector<uint64_t>& offs,
                   const std::vector<uint64_t>& ids, const std::vector<double>& d2, int status,
                   const std::string& err) {
     const Clock::time_point now = Clock::now();
@@ -282,6 +290,8 @@ void Server::post(std::vector<Request>& batch, size_t begin, size_t end, const s
                 r.ids.assign(ids.begin() + static_cast<ptrdiff_t>(offs[q]), ids.begin() + static_cast<ptrdiff_t>(offs[q + 1]));
                 if (!d2.empty())
                     r.dist2.assign(d2.begin() + static_cast<ptrdiff_t>(offs[q]), d2.begin() + static_cast<ptrdiff_t>(offs[q + 1]));
+                const size_t n = end - begin, L = n ? levels.size() / n : 0;
+                for (size_t l = 0; l < L; ++l) r.levels.push_back(levels[l * n + q]);
             }
             r.latencyUs = std::chrono::duration<double, std::micro>(now - batch[i].arrival).count();
             latUs_.push_back(r.latencyUs);

@@ -36,6 +36,7 @@ struct ServeConfig {
     int mode = kModeExact;      // range mode; KNN is always exact
     bool learned = true;        // rank KNN frontiers with the trained scorer, when there is one
     int lanes = 2;              // 2: range and KNN lanes; 1: one lane serves both, in arrival order
+    bool levels = false;        // also record every request's generated-children count per level
 };
 
 struct ServeStats {
@@ -54,6 +55,7 @@ public:
         std::vector<uint64_t> ids;
         std::vector<double> dist2;  // KNN
         double latencyUs = 0;
+        std::vector<uint32_t> levels;  // per interval, coarsest first (ServeConfig::levels)
     };
 
     Server(Runtime& rt, const ServeConfig& cfg);
@@ -96,7 +98,8 @@ private:
 
     void work(Lane& lane);
     void runGroup(Lane& lane, std::vector<Request>& batch, size_t begin, size_t end);
-    void post(std::vector<Request>& batch, size_t begin, size_t end, const std::vector<uint64_t>& offs,
+    void post(std::vector<Request>& batch, size_t begin, size_t end, const std::vector<uint32_t>& levels,
+              const std::vector<uint64_t>& offs,
               const std::vector<uint64_t>& ids, const std::vector<double>& d2, int status, const std::string& err);
 
     Runtime& rt_;
