@@ -237,7 +237,43 @@ DerivedArrays computeDerived(const HostIndex& idx) {
     return out;
 }
 
-std::unique_ptr<DeviceIndex> buildDeviceIndex(const HostIndex& idx, const DerivedArrays& der, cudaStream_t s) {
+HostMapping::HostMapping(const void* host, size_t bytes) {
+    if (!host || bytes == 0) return;
+    int dev = 0, readOnly = 0;
+    TBLAEQ_CUDA(cudaGetDevice(&dev));
+    TBLAEQ_CUDA(cudaDeviceGetAttribute(&readOnly, cudaDevAttrHostRegisterReadOnlySupported, dev));
+    unsigned flags = cudaHostRegisterMapped | (readOnly ? cudaHostRegisterReadOnly : 0u);
+    void* h = const_cast<void*>(host);
+    TBLAEQ_CUDA(cudaHostRegister(h, bytes, flags));
+    void* d = nullptr;
+    const cudaError_t e = cudaHostGetDevicePointer(&d, h, 0);
+    if (e != cudaSuccess) {
+        cudaHostUnregister(h);
+        throw CudaError(e, "cudaHostGetDevicePointer");
+    }
+    host_ = h;
+    dev_ = d;
+}
+
+HostMapping::~HostMapping() {
+    if (host_) cudaHostUnregister(host_);
+}
+
+HostMapping& HostMapping::operator=(HostMapping&& o) noexcept {
+    if (this != &o) {
+        if (host_) cudaHostUnregister(host_);
+        host_ = o.host_;
+        dev_ = o.dev_;
+        o.host_ = o.dev_ = nullptr;
+    }
+    return *this;
+}
+
+std::unique_ptr<DeviceIndex> buildDeviceIndex(const HostIndex& idx, const DerivedArrays& der, cudaStream_t s,
+                                              const std::vector<int>& residency) {
+    if (!residency.empty() && residency.size() != idx.intervals)
+        throw std::invalid_argument("buildDeviceIndex: one residency per interval");
+    auto res = [&](uint64_t l) { return residency.empty() ? static_cast<int>(kResident) : residency[l]; };
     auto di = std::make_unique<DeviceIndex>();
     di->D = idx.D;
     di->height = idx.height;
@@ -248,10 +284,20 @@ std::unique_ptr<DeviceIndex> buildDeviceIndex(const HostIndex& idx, const Derive
     di->coarseVals = upload(idx.coarsest.vals, s);
     di->coarseIds = upload(idx.coarsest.ids, s);
     di->pvals.resize(idx.intervals);
+    di->rows.assign(idx.intervals, nullptr);
+    di->rowsOnHost.assign(idx.intervals, 0);
     di->nodeOrig.resize(idx.intervals);
+    di->hostMaps.reserve(2 * idx.intervals);
     for (uint64_t l = 0; l < idx.intervals; ++l) {
         const PTensor& P = idx.pTensors[l];
-        di->pvals[l] = upload(P.vals, s);
+        if (res(l) == kResident || P.vals.empty()) {
+            di->pvals[l] = upload(P.vals, s);
+            di->rows[l] = di->pvals[l].as<double>();
+        } else {
+            di->hostMaps.emplace_back(P.vals.data(), P.vals.size() * sizeof(double));
+            di->rows[l] = static_cast<const double*>(di->hostMaps.back().device());
+            di->rowsOnHost[l] = 1;
+        }
         std::vector<NodeRec> rec(P.cols);
         for (uint64_t o = 0; o < P.cols; ++o) {
             rec[o].rad = idx.radius[l][o];
@@ -262,7 +308,17 @@ std::unique_ptr<DeviceIndex> buildDeviceIndex(const HostIndex& idx, const Derive
         TBLAEQ_CUDA(cudaStreamSynchronize(s));
     }
     di->maps.resize(idx.height);
-    for (uint64_t m = 1; m < idx.height; ++m) di->maps[m] = upload(idx.maps[m], s);
+    di->mapPtr.assign(idx.height, nullptr);
+    for (uint64_t m = 1; m < idx.height; ++m) {
+        // Map m belongs to interval m-1 (it maps that interval's output rows to original ids).
+        if (res(m - 1) == kRowsAndMapOnHost && !idx.maps[m].empty()) {
+            di->hostMaps.emplace_back(idx.maps[m].data(), idx.maps[m].size() * sizeof(uint64_t));
+            di->mapPtr[m] = static_cast<const uint64_t*>(di->hostMaps.back().device());
+        } else {
+            di->maps[m] = upload(idx.maps[m], s);
+            di->mapPtr[m] = di->maps[m].as<uint64_t>();
+        }
+    }
     // The finest map doubles as the final-id map of the fused traversal.
     di->nodeRef.resize(idx.height - 1);
     di->nodeSub.resize(idx.height - 1);

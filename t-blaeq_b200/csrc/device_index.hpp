@@ -86,13 +86,47 @@ struct DerivedArrays {
 // hierarchy (decoded exactly like the traversal: y = P[j] * x_parent, one rounded multiply).
 DerivedArrays computeDerived(const HostIndex& idx);
 
+// A page-locked host range mapped into the device address space (zero-copy reads by kernels);
+// unregistered when destroyed. The host memory must outlive it and must not move.
+class HostMapping {
+public:
+    HostMapping() = default;
+    HostMapping(const void* host, size_t bytes);
+    ~HostMapping();
+    HostMapping(const HostMapping&) = delete;
+    HostMapping& operator=(const HostMapping&) = delete;
+    HostMapping(HostMapping&& o) noexcept : host_(o.host_), dev_(o.dev_) { o.host_ = o.dev_ = nullptr; }
+    HostMapping& operator=(HostMapping&& o) noexcept;
+    const void* device() const { return dev_; }
+
+private:
+    void* host_ = nullptr;
+    void* dev_ = nullptr;
+};
+
+// Residency of one interval's arrays, from the level policy (the reference's L0..L3,
+// docs/memory_policies.md):
+//   L0, L1  P values and maps in device memory (the library never allocates in the query path
+//           either way, so the two coincide here);
+//   L2      P values stay in page-locked host memory mapped into the device address space: the
+//           traversal reads only the rows of the children it expands, across the host link, with
+//           no host-side gather and no upload (the reference collects the surviving columns on
+//           the host and uploads them, SpMSpV.cu:107-198);
+//   L3      as L2, and the interval's sort-to-original map is read from host memory too.
+// Node records, radii and boxes (one entry per cluster) and the coarsest mesh are always resident.
+enum Residency : int { kResident = 0, kRowsOnHost = 1, kRowsAndMapOnHost = 2 };
+
 struct DeviceIndex {
     uint64_t D = 0, height = 0, intervals = 0;
     std::vector<uint64_t> meshCount;  // by mesh m (0 = coarsest)
 
     // position space
     DeviceMem coarseVals;                    // mesh 0 rows (n0 * D)
-    std::vector<DeviceMem> pvals;            // interval l: rows of P_l (n_{l+1} * D)
+    std::vector<DeviceMem> pvals;            // interval l: rows of P_l (n_{l+1} * D) when resident
+    std::vector<const double*> rows;         // interval l: device-visible rows (pvals or mapped host memory)
+    std::vector<uint8_t> rowsOnHost;         // interval l: rows are read from mapped host memory
+    std::vector<const uint64_t*> mapPtr;     // mesh m >= 1: device-visible Map (maps or mapped host memory)
+    std::vector<HostMapping> hostMaps;       // host ranges mapped for streamed intervals
     std::vector<DeviceMem> nodeRef, nodeSub; // mesh m < height-1: NodeRec {radius, first child, children}
     std::vector<DeviceMem> leaf;             // mesh m < height-1: finest points below each node (uint32)
     std::vector<DeviceMem> aabb;             // mesh m < height-1: outward-rounded float box of the points below
@@ -105,6 +139,8 @@ struct DeviceIndex {
     size_t deviceBytes() const;
 };
 
-std::unique_ptr<DeviceIndex> buildDeviceIndex(const HostIndex& idx, const DerivedArrays& der, cudaStream_t s);
+// `residency` has one Residency per interval (empty: every interval resident).
+std::unique_ptr<DeviceIndex> buildDeviceIndex(const HostIndex& idx, const DerivedArrays& der, cudaStream_t s,
+                                              const std::vector<int>& residency = {});
 
 }  // namespace tblaeq

@@ -303,7 +303,8 @@ void BatchEngine::enqueueLaunches(const double* dBoxes, uint32_t nq, int mode, u
     for (int m = 0; m < H; ++m) {
         ExpandArgs a{};
         a.in = inView(buf, hdrPtr(m));
-        a.child.rows = (m == 0) ? di_.coarseVals.as<double>() : di_.pvals[m - 1].as<double>();
+        a.child.rows = (m == 0) ? di_.coarseVals.as<double>() : di_.rows[m - 1];
+        a.child.rowsOnHost = (m == 0) ? 0 : di_.rowsOnHost[m - 1];
         a.query.boxes = dBoxes;
         a.query.boxesF = (mode == kModeExact) ? boxF_.as<float>() : nullptr;
         a.scratch.desc = desc + static_cast<size_t>(m) * tileCap_;
@@ -320,7 +321,7 @@ void BatchEngine::enqueueLaunches(const double* dBoxes, uint32_t nq, int mode, u
             launchExpand(a, kPredRangeRadius, false, 0, stream_);
             buf = 1 - buf;
         } else {
-            a.child.outMap = di_.maps[H - 1].as<uint64_t>();
+            a.child.outMap = di_.mapPtr[H - 1];
             a.rout.ids = resIds_.as<uint64_t>();
             a.rout.vals = (flags & kWantVals) ? resVals_.as<double>() : nullptr;
             a.rout.qcount = qcount;
@@ -483,8 +484,9 @@ uint64_t BatchEngine::runGridLevel(int l, const uint64_t* dIds, const double* dV
 
         ExpandArgs b{};
         b.in = inView(1, hdrPtr(1));
-        b.child.rows = di_.pvals[l].as<double>();
-        b.child.outMap = di_.maps[l + 1].as<uint64_t>();
+        b.child.rows = di_.rows[l];
+        b.child.rowsOnHost = di_.rowsOnHost[l];
+        b.child.outMap = di_.mapPtr[l + 1];
         b.rout.ids = outIds;
         b.rout.vals = outVals;
         b.rout.hdr = hdrPtr(2);
@@ -598,7 +600,8 @@ void BatchEngine::enqueueKnn(const double* dPoints, uint32_t nq, const uint32_t*
     auto base = [&](int m, int buf) {
         ExpandArgs a{};
         a.in = inView(buf, hdrPtr(m));
-        a.child.rows = (m == 0) ? di_.coarseVals.as<double>() : di_.pvals[m - 1].as<double>();
+        a.child.rows = (m == 0) ? di_.coarseVals.as<double>() : di_.rows[m - 1];
+        a.child.rowsOnHost = (m == 0) ? 0 : di_.rowsOnHost[m - 1];
         a.query.points = dPoints;
         a.query.tau = tau;
         a.query.k = dK;
@@ -626,7 +629,7 @@ void BatchEngine::enqueueKnn(const double* dPoints, uint32_t nq, const uint32_t*
     // `buf` now holds the last frontier F: the surviving finest clusters, query-major.
     lastKnnBuf_ = buf;
     ExpandArgs fin = base(H - 1, buf);
-    fin.child.outMap = di_.maps[H - 1].as<uint64_t>();
+    fin.child.outMap = di_.mapPtr[H - 1];
     fin.rout.ids = resIds_.as<uint64_t>();
     fin.rout.q = resQ_.as<uint32_t>();
     fin.rout.dist2 = resDist_.as<double>();

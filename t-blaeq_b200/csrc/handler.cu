@@ -137,7 +137,12 @@ void QueryHandler::prepareForQuery(const IndexPolicy& policy) {
     rt->host = host_.get();
     TBLAEQ_CUDA(cudaStreamCreateWithFlags(&rt->stream, cudaStreamNonBlocking));
     const DerivedArrays der = computeDerived(*host_);
-    rt->dev = buildDeviceIndex(*host_, der, rt->stream);
+    std::vector<int> residency(host_->intervals, kResident);
+    for (size_t l = 0; l < residency.size(); ++l) {
+        if (policy.levels[l] == LevelPolicy::L2) residency[l] = kRowsOnHost;
+        if (policy.levels[l] == LevelPolicy::L3) residency[l] = kRowsAndMapOnHost;
+    }
+    rt->dev = buildDeviceIndex(*host_, der, rt->stream, residency);
     rt->engine = std::make_unique<BatchEngine>(*rt->dev, rt->stream);
     rt->pluginEngine = std::make_unique<BatchEngine>(*rt->dev, rt->stream);
     rt->levelOut.resize(host_->intervals);
@@ -147,7 +152,10 @@ void QueryHandler::prepareForQuery(const IndexPolicy& policy) {
 }
 
 void B200Strategy::prepare(std::ostream& reportOs) {
-    reportOs << "B200 strategy: index resident on device (" << rt_.dev->deviceBytes() << " bytes)\n";
+    size_t streamed = 0;
+    for (uint8_t o : rt_.dev->rowsOnHost) streamed += o;
+    reportOs << "B200 strategy: " << rt_.dev->deviceBytes() << " bytes on the device; " << streamed
+             << " interval(s) read from mapped host memory\n";
 }
 
 LevelResult B200Strategy::runLevel(size_t l, const Grid& cur, QueryType qType, const double* lo, const double* hi,

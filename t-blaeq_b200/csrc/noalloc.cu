@@ -132,8 +132,9 @@ uint64_t runLevelRangeNoAlloc(Runtime& rt, uint64_t l, const uint64_t* dIds, con
                       reinterpret_cast<uint32_t*>(sv + kSurvCpre), reinterpret_cast<double*>(sv + kSurvX),
                       reinterpret_cast<uint32_t*>(sv + kSurvTiles), hdr + 2,
                       static_cast<uint32_t>(kNoAllocMaxGrid),      static_cast<uint32_t>(kTilesOut)};
-    b.child.rows = di.pvals[l].as<double>();
-    b.child.outMap = di.maps[l + 1].as<uint64_t>();
+    b.child.rows = di.rows[l];
+    b.child.rowsOnHost = di.rowsOnHost[l];
+    b.child.outMap = di.mapPtr[l + 1];
     b.rout.ids = outIds;
     b.rout.vals = outVals;
     b.rout.hdr = hdr + 4;

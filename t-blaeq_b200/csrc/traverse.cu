@@ -245,6 +245,7 @@ template <int D, int PRED>
 __device__ __forceinline__ void prefetchTileRows(const ExpandArgs& a, uint32_t t, uint32_t nTiles, uint32_t entries,
                                                  uint32_t total, int lane) {
     if (t >= nTiles) return;
+    if (a.child.rowsOnHost) return;  // bulk prefetches are for device memory
     if (PRED == kPredRangeRadius && a.child.aabb) return;
     if (PRED == kPredKnnPoint && a.wave != 0 && a.child.entrySel) return;
     const uint32_t t0 = t * kWarpTile;
@@ -839,7 +840,8 @@ void dispatchPred(const ExpandArgs& a, int pred, bool toResult, int g, cudaStrea
 
 template <int D>
 void dispatchStaged(const ExpandArgs& a, int pred, bool toResult, int g, cudaStream_t s) {
-    if (a.variant == kVariantStaged) return dispatchPred<D, true>(a, pred, toResult, g, s);
+    // Rows in mapped host memory are read with plain loads only (no cp.async staging).
+    if (a.variant == kVariantStaged && !a.child.rowsOnHost) return dispatchPred<D, true>(a, pred, toResult, g, s);
     return dispatchPred<D, false>(a, pred, toResult, g, s);
 }
 

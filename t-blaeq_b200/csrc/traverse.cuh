@@ -92,6 +92,7 @@ struct ChildLevel {
     const double* entryLb;
     const uint8_t* mask;        // keep flags (by row) for kPredMask
     const uint64_t* outMap;     // final output id of row j (null: id = key)
+    int rowsOnHost;             // rows (and possibly outMap) are mapped host memory: plain loads only
 };
 
 struct QueryArgs {

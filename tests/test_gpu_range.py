@@ -187,3 +187,31 @@ def test_allocation_failure_surfaces_cleanly(tb, cuda):
     h.prepare_for_query(tb.LevelPolicy.L0)  # a later prepare succeeds
     h.close()
     assert lib.tblaeq_live_device_bytes() == before
+
+
+@pytest.mark.parametrize("policy", [("L0", "L0", "L2"), ("L3", "L3", "L3"), ("L2", "L3", "L1")])
+def test_streamed_levels_equal_resident(tb, oracle_mod, tmp_path, cuda, policy):
+    """Intervals under L2 / L3 read their P rows (L3: and their maps) from page-locked host memory
+    mapped into the device address space; every variant falls back to plain loads there. Results
+    equal the resident index's: exact range and KNN against the FP64 brute force, ref-parity range
+    against the oracle's restatement of the reference, in the reference's order."""
+    h = tb.QueryHandler.generate(200000, 8, 1.0, 100.0, False, 4, (100, 50, 20), 9, 3.0)
+    h.prepare_for_query([tb.LevelPolicy[p] for p in policy])
+    assert [p.name for p in h.info()["policy"]] == list(policy)
+    o = oracle_from_handler(oracle_mod, h, tmp_path)
+    pts, ids = oracle_mod.decoded_points(o)
+    Q = _boxes(pts, 120, 21)
+    b = oracle_mod.brute_query(pts, ids, oracle_mod.RANGE, Q)
+    ref = oracle_mod.ref_query(o, oracle_mod.RANGE, Q, sorted_ids=False)
+    for variant in (0, 1):
+        h.set_variants([variant] * 4)
+        r, offs, got = _batch_ids(tb, h, Q, tb.Mode.EXACT)
+        assert np.array_equal(offs, b.offsets), variant
+        assert all(np.array_equal(g, b.query(q)) for q, g in enumerate(ids_by_query(offs, got))), variant
+        r2, offs2, got2 = _batch_ids(tb, h, Q, tb.Mode.REF_PARITY)
+        assert np.array_equal(offs2, ref.offsets) and np.array_equal(got2, ref.ids), variant
+    rng = np.random.default_rng(4)
+    P = np.ascontiguousarray(pts[rng.integers(0, len(pts), 60)] + rng.normal(0, 0.5, (60, 8)))
+    rk = h.query_batch(tb.QueryType.POINT, P, tb.Mode.EXACT, K=15)
+    bk = oracle_mod.brute_query(pts, ids, oracle_mod.KNN, P, K=15)
+    assert np.array_equal(rk.ids.numpy(), bk.ids) and np.array_equal(rk.dist2.numpy(), bk.dist2)
