@@ -195,6 +195,19 @@ struct Staging {
 #ifndef TBLAEQ_EXPAND_MIN_BLOCKS_BOUND
 #define TBLAEQ_EXPAND_MIN_BLOCKS_BOUND 8
 #endif
+// Unroll factors of the per-round loops of the range levels that output a frontier (build-time
+// knobs, like the launch shape): the item test and pass 2. Measured on B200: fully unrolled, these
+// levels stall on instruction fetch (the loop body holds the box prefilter, the radius test, the
+// node loads and the frontier writes); rolling the test to 2 and pass 2 to 1 cut the mesh-2 range
+// level from 0.65 to 0.45 ms; a rolled pass 2 also frees registers at the finest range level. The
+// test loop of point levels, every loop of the KNN levels and the item-to-entry mapping are
+// fastest fully unrolled (the KNN step measured 10% slower with its bound levels rolled).
+#ifndef TBLAEQ_UNROLL_RANGE_TEST
+#define TBLAEQ_UNROLL_RANGE_TEST 2
+#endif
+#ifndef TBLAEQ_UNROLL_RANGE_PASS2
+#define TBLAEQ_UNROLL_RANGE_PASS2 1
+#endif
 constexpr int kExpandThreads = TBLAEQ_EXPAND_THREADS;
 
 // Resident CTAs per SM the register allocation is sized for (128 threads: 10 CTAs = 51 registers,
@@ -422,6 +435,11 @@ __global__ void __launch_bounds__(kExpandThreads, expandMinBlocks<PRED>()) expan
     constexpr int R = S::kRounds;
     constexpr int DM = (D > 0) ? D : 32;
     constexpr bool NODE = needsNode<PRED, TO_RESULT>();
+    // Code size (see TBLAEQ_UNROLL_RANGE_TEST): range levels that output a frontier keep their
+    // test loop rolled, every range level its pass-2 loop; the KNN levels unroll all R rounds.
+    constexpr bool kKnn = PRED == kPredKnnBound || PRED == kPredKnnPoint;
+    constexpr int kUnrollTest = (!TO_RESULT && !kKnn) ? TBLAEQ_UNROLL_RANGE_TEST : R;
+    constexpr int kUnrollPass2 = kKnn ? R : TBLAEQ_UNROLL_RANGE_PASS2;
     constexpr uint32_t FULL = 0xffffffffu;
     extern __shared__ __align__(16) unsigned char smem[];
     const int dim = (D > 0) ? D : a.D;
@@ -555,7 +573,7 @@ __global__ void __launch_bounds__(kExpandThreads, expandMinBlocks<PRED>()) expan
             }
         }
         uint32_t keepBits = 0, aggCnt = 0, aggSum = 0;
-#pragma unroll
+#pragma unroll kUnrollTest
         for (int r = 0; r < R; ++r) {
             if constexpr (S::kOn) {
                 // Lanes copy each other's rows: the slot being refilled must be read out by every
@@ -650,7 +668,7 @@ __global__ void __launch_bounds__(kExpandThreads, expandMinBlocks<PRED>()) expan
 
         // ---- pass 2: rebuild and write the kept items in order.
         unsigned long long runCnt = exCnt, runSum = exSum;
-#pragma unroll
+#pragma unroll kUnrollPass2
         for (int r = 0; r < R; ++r) {
             const bool keep = (keepBits >> r) & 1u;
             const uint32_t kb = __ballot_sync(FULL, keep);

@@ -284,9 +284,11 @@ def make_server(service: QueryService, host: str = "0.0.0.0", port: int = 8080) 
         def log_message(self, fmt, *args):  # keep request logging off the hot path
             pass
 
-    httpd = ThreadingHTTPServer((host, port), Handler)
-    httpd.daemon_threads = True
-    return httpd
+    class Server(ThreadingHTTPServer):
+        daemon_threads = True
+        request_queue_size = 1024  # listen backlog: bursts of clients queue instead of being reset
+
+    return Server((host, port), Handler)
 
 
 def main(argv=None):

@@ -24,16 +24,19 @@ class FakeServer:
         self.tb = tb
         self.requests = []
         self.results = {}
+        self.lock = threading.Lock()  # HTTP handler threads submit concurrently
 
     def submit(self, qtype, query, K=0):
-        t = len(self.requests)
-        self.requests.append((qtype, list(query), K))
         n = K if qtype == self.tb.QueryType.POINT else 3
-        self.results[t] = (np.arange(n, dtype=np.uint64), np.zeros(n), 1234.4, np.array([5, 7, 2]))
+        with self.lock:
+            t = len(self.requests)
+            self.requests.append((qtype, list(query), K))
+            self.results[t] = (np.arange(n, dtype=np.uint64), np.zeros(n), 1234.4, np.array([5, 7, 2]))
         return t
 
     def poll_levels(self, ticket, wait_ms):
-        return self.results.pop(ticket)
+        with self.lock:
+            return self.results.pop(ticket)
 
 
 class FakeManager:
@@ -183,3 +186,27 @@ def test_index_manager_lists_cached_indexes(http, tmp_path):
     with pytest.raises(http.ApiError) as e:
         m.get_or_load("zzz")
     assert e.value.status == 400 and e.value.message == "Dataset index does not exist: zzz"
+
+
+def test_burst_of_concurrent_clients(svc, http):
+    """More simultaneous connections than the socket module's default listen backlog (5): every
+    client is answered (the server's backlog is raised, so bursts queue instead of being reset)."""
+    from concurrent.futures import ThreadPoolExecutor
+    httpd = http.make_server(svc, "127.0.0.1", 0)
+    t = threading.Thread(target=httpd.serve_forever, daemon=True)
+    t.start()
+    url = f"http://127.0.0.1:{httpd.server_address[1]}/query"
+    body = json.dumps({"dataset_name": "ds", "query_type": "KNN", "query_point": [0, 0, 0], "k": 3}).encode()
+
+    def one(_):
+        req = urllib.request.Request(url, data=body, headers={"Content-Type": "application/json"}, method="POST")
+        with urllib.request.urlopen(req, timeout=30) as r:
+            return r.status, json.loads(r.read())["result"]
+
+    try:
+        with ThreadPoolExecutor(64) as ex:
+            out = list(ex.map(one, range(256)))
+        assert all(s == 200 and res == [0, 1, 2] for s, res in out)
+    finally:
+        httpd.shutdown()
+        httpd.server_close()
