@@ -429,6 +429,48 @@ __device__ __forceinline__ bool evalItem(const ExpandArgs& a, int dim, const dou
     }
 }
 
+// Finest range level, a round whose 32 items all belong to one frontier entry: the items' rows
+// are 32 consecutive P rows, so the warp reads them as one contiguous block, each lane taking one
+// 16-byte piece (two dimensions) of a row per load, and tests its piece against the same two
+// dimensions of the entry's coordinates and query box (constant over the round). A ballot per
+// load collects the pieces; an item is kept when all D/2 pieces of its row are inside the box.
+// Same products and comparisons as evalItem, so the kept set is identical. Returns whether the
+// calling lane's own item (item `lane` of the round) is kept.
+template <int D>
+constexpr bool coalescedBox() {
+    return D >= 4 && D % 2 == 0 && 32 % (D >= 2 ? D / 2 : 1) == 0;
+}
+template <int D>
+__device__ __forceinline__ bool singleEntryRangeBox(const ExpandArgs& a, uint32_t j0, uint32_t e, uint32_t q,
+                                                    int lane) {
+    constexpr int L = D / 2;   // lanes (16-byte pieces) per row
+    constexpr int G = 32 / L;  // rows per load
+    constexpr uint32_t kAll = (1u << L) - 1u;
+    const int c = lane % L;
+    const double2* rows2 = reinterpret_cast<const double2*>(a.child.rows + static_cast<size_t>(j0) * D);
+    const double2 xv = __ldg(reinterpret_cast<const double2*>(a.in.x + static_cast<size_t>(e) * D) + c);
+    const double* box = a.query.boxes + static_cast<size_t>(q) * 2 * D;
+    const double2 lo = __ldg(reinterpret_cast<const double2*>(box) + c);
+    const double2 hi = __ldg(reinterpret_cast<const double2*>(box + D) + c);
+    // Two loads in flight at a time: enough to overlap, few enough registers to avoid spills.
+    constexpr int P = L >= 2 ? 2 : 1;
+    uint32_t mine = 0;
+#pragma unroll 1
+    for (int s0 = 0; s0 < L; s0 += P) {
+        double2 rv[P];
+#pragma unroll
+        for (int i = 0; i < P; ++i) rv[i] = __ldg(rows2 + (s0 + i) * 32 + lane);
+#pragma unroll
+        for (int i = 0; i < P; ++i) {
+            const double y0 = __dmul_rn(rv[i].x, xv.x), y1 = __dmul_rn(rv[i].y, xv.y);
+            const bool pass = (lo.x <= y0) & (y0 <= hi.x) & (lo.y <= y1) & (y1 <= hi.y);
+            const uint32_t b = __ballot_sync(0xffffffffu, pass);
+            if (s0 + i == lane / G) mine = b;
+        }
+    }
+    return ((mine >> ((lane % G) * L)) & kAll) == kAll;
+}
+
 template <int D, int PRED, bool TO_RESULT, bool STAGED>
 __global__ void __launch_bounds__(kExpandThreads, expandMinBlocks<PRED>()) expandKernel(ExpandArgs a) {
     using S = Staging<D, STAGED>;
@@ -440,6 +482,7 @@ __global__ void __launch_bounds__(kExpandThreads, expandMinBlocks<PRED>()) expan
     constexpr bool kKnn = PRED == kPredKnnBound || PRED == kPredKnnPoint;
     constexpr int kUnrollTest = (!TO_RESULT && !kKnn) ? TBLAEQ_UNROLL_RANGE_TEST : R;
     constexpr int kUnrollPass2 = kKnn ? R : TBLAEQ_UNROLL_RANGE_PASS2;
+    constexpr bool kFastBox = PRED == kPredRangeBox && TO_RESULT && !STAGED && coalescedBox<D>();
     constexpr uint32_t FULL = 0xffffffffu;
     extern __shared__ __align__(16) unsigned char smem[];
     const int dim = (D > 0) ? D : a.D;
@@ -599,7 +642,16 @@ __global__ void __launch_bounds__(kExpandThreads, expandMinBlocks<PRED>()) expan
                     work = !sel && __ldg(a.child.entryLb + e) <= __ldcg(a.query.tau + wQ[sWin[r * 32 + lane]]);
                 }
             }
-            if (work) {
+            bool done = false;
+            if constexpr (kFastBox) {
+                // Warp-uniform: a full round inside one entry (its first and last item share it).
+                const uint32_t w0 = sWin[r * 32], w31 = sWin[r * 32 + 31];
+                if (W != 0 && t0 + r * 32 + 32 <= total && w0 == w31 && !a.child.rowsOnHost) {
+                    keep = singleEntryRangeBox<D>(a, sRow[r * 32], eLo + w0, wQ[w0], lane);
+                    done = true;
+                }
+            }
+            if (work && !done) {
                 const uint32_t j = sRow[r * 32 + lane];
                 const uint32_t w = sWin[r * 32 + lane];
                 const uint32_t e = eLo + w;
