@@ -51,6 +51,13 @@ using tc::tcFenceBefore;
 using tc::tmemLoad32;
 using tc::tmemWaitLoad;
 
+// min(a, b, c) in one instruction (sm_100 three-input min.f32); equal to fminf(a, fminf(b, c)).
+__device__ __forceinline__ float min3f(float a, float b, float c) {
+    float r;
+    asm("min.f32 %0, %1, %2, %3;" : "=f"(r) : "f"(a), "f"(b), "f"(c));
+    return r;
+}
+
 // No swizzle, LBO = 128 B, SBO = 512 B (see imageOffset).
 __device__ __forceinline__ uint64_t ummaDesc(uint32_t saddr) { return tc::smemDesc(saddr, 128, 512); }
 __device__ __forceinline__ bool mbarWait(uint64_t* bar, uint32_t phase) { return tc::mbarWait(bar, phase, kSpinLimit); }
@@ -249,17 +256,19 @@ __global__ void __launch_bounds__(kAssignThreads, 2)
                 float m0 = INFINITY, m1 = INFINITY;
 #pragma unroll
                 for (int j = 0; j < 32; j += 4) {
+                    // ||c||^2 - 2 x.c for four columns: two packed FMAs, two three-input minima
+                    // (the same roundings as four fmaf and four fminf).
                     const float4 c4 = *reinterpret_cast<const float4*>(cn + c + j);
-                    const float v0 = fmaf(-2.f, __uint_as_float(r[j]), c4.x);
-                    const float v1 = fmaf(-2.f, __uint_as_float(r[j + 1]), c4.y);
-                    const float v2 = fmaf(-2.f, __uint_as_float(r[j + 2]), c4.z);
-                    const float v3 = fmaf(-2.f, __uint_as_float(r[j + 3]), c4.w);
-                    r[j] = __float_as_uint(v0);
-                    r[j + 1] = __float_as_uint(v1);
-                    r[j + 2] = __float_as_uint(v2);
-                    r[j + 3] = __float_as_uint(v3);
-                    m0 = fminf(m0, fminf(v0, v1));
-                    m1 = fminf(m1, fminf(v2, v3));
+                    const float2 va = __ffma2_rn(make_float2(__uint_as_float(r[j]), __uint_as_float(r[j + 1])),
+                                                 make_float2(-2.f, -2.f), make_float2(c4.x, c4.y));
+                    const float2 vb = __ffma2_rn(make_float2(__uint_as_float(r[j + 2]), __uint_as_float(r[j + 3])),
+                                                 make_float2(-2.f, -2.f), make_float2(c4.z, c4.w));
+                    r[j] = __float_as_uint(va.x);
+                    r[j + 1] = __float_as_uint(va.y);
+                    r[j + 2] = __float_as_uint(vb.x);
+                    r[j + 3] = __float_as_uint(vb.y);
+                    m0 = min3f(m0, va.x, va.y);
+                    m1 = min3f(m1, vb.x, vb.y);
                 }
                 if (fminf(m0, m1) < s2) {
 #pragma unroll
