@@ -195,18 +195,18 @@ struct Staging {
 #ifndef TBLAEQ_EXPAND_MIN_BLOCKS_BOUND
 #define TBLAEQ_EXPAND_MIN_BLOCKS_BOUND 8
 #endif
-// Unroll factors of the per-round loops of the range levels that output a frontier (build-time
-// knobs, like the launch shape): the item test and pass 2. Measured on B200: fully unrolled, these
-// levels stall on instruction fetch (the loop body holds the box prefilter, the radius test, the
-// node loads and the frontier writes); rolling the test to 2 and pass 2 to 1 cut the mesh-2 range
-// level from 0.65 to 0.45 ms; a rolled pass 2 also frees registers at the finest range level. The
-// test loop of point levels, every loop of the KNN levels and the item-to-entry mapping are
-// fastest fully unrolled (the KNN step measured 10% slower with its bound levels rolled).
-#ifndef TBLAEQ_UNROLL_RANGE_TEST
-#define TBLAEQ_UNROLL_RANGE_TEST 2
+// Unroll factors of the per-round loops (build-time knobs, like the launch shape): the item test
+// of levels that output a frontier, and pass 2 of every level. Measured on B200: fully unrolled,
+// the frontier levels stall on instruction fetch (their loop body holds the box prefilter, the
+// radius or bound test, the node loads and the frontier writes); with the test unrolled twice and
+// pass 2 rolled, the mesh-2 range level went from 0.65 to 0.45 ms and the KNN levels above the
+// finest from 1.92 to 1.75 ms (2M x 16, 512 queries); a rolled pass 2 also frees registers at the
+// point levels. The test loop of point levels and the item-to-entry mapping stay fully unrolled.
+#ifndef TBLAEQ_UNROLL_FRONTIER_TEST
+#define TBLAEQ_UNROLL_FRONTIER_TEST 2
 #endif
-#ifndef TBLAEQ_UNROLL_RANGE_PASS2
-#define TBLAEQ_UNROLL_RANGE_PASS2 1
+#ifndef TBLAEQ_UNROLL_PASS2
+#define TBLAEQ_UNROLL_PASS2 1
 #endif
 constexpr int kExpandThreads = TBLAEQ_EXPAND_THREADS;
 
@@ -429,6 +429,12 @@ __device__ __forceinline__ bool evalItem(const ExpandArgs& a, int dim, const dou
     }
 }
 
+// Row pieces each lane keeps in flight in singleEntryRangeBox. Measured on B200 (finest range
+// level, D = 8): 2 pieces 0.322 ms, all 4 pieces of the round 0.303 ms, although the latter spills
+// 72 bytes (outside the fast path) at the point levels' 48-register bound.
+#ifndef TBLAEQ_FAST_PIECES
+#define TBLAEQ_FAST_PIECES 4
+#endif
 // Finest range level, a round whose 32 items all belong to one frontier entry: the items' rows
 // are 32 consecutive P rows, so the warp reads them as one contiguous block, each lane taking one
 // 16-byte piece (two dimensions) of a row per load, and tests its piece against the same two
@@ -452,8 +458,8 @@ __device__ __forceinline__ bool singleEntryRangeBox(const ExpandArgs& a, uint32_
     const double* box = a.query.boxes + static_cast<size_t>(q) * 2 * D;
     const double2 lo = __ldg(reinterpret_cast<const double2*>(box) + c);
     const double2 hi = __ldg(reinterpret_cast<const double2*>(box + D) + c);
-    // Two loads in flight at a time: enough to overlap, few enough registers to avoid spills.
-    constexpr int P = L >= 2 ? 2 : 1;
+    // Loads in flight per lane (TBLAEQ_FAST_PIECES).
+    constexpr int P = L >= TBLAEQ_FAST_PIECES ? TBLAEQ_FAST_PIECES : L;
     uint32_t mine = 0;
 #pragma unroll 1
     for (int s0 = 0; s0 < L; s0 += P) {
@@ -477,11 +483,9 @@ __global__ void __launch_bounds__(kExpandThreads, expandMinBlocks<PRED>()) expan
     constexpr int R = S::kRounds;
     constexpr int DM = (D > 0) ? D : 32;
     constexpr bool NODE = needsNode<PRED, TO_RESULT>();
-    // Code size (see TBLAEQ_UNROLL_RANGE_TEST): range levels that output a frontier keep their
-    // test loop rolled, every range level its pass-2 loop; the KNN levels unroll all R rounds.
-    constexpr bool kKnn = PRED == kPredKnnBound || PRED == kPredKnnPoint;
-    constexpr int kUnrollTest = (!TO_RESULT && !kKnn) ? TBLAEQ_UNROLL_RANGE_TEST : R;
-    constexpr int kUnrollPass2 = kKnn ? R : TBLAEQ_UNROLL_RANGE_PASS2;
+    // Code size (see TBLAEQ_UNROLL_FRONTIER_TEST).
+    constexpr int kUnrollTest = TO_RESULT ? R : TBLAEQ_UNROLL_FRONTIER_TEST;
+    constexpr int kUnrollPass2 = TBLAEQ_UNROLL_PASS2;
     constexpr bool kFastBox = PRED == kPredRangeBox && TO_RESULT && !STAGED && coalescedBox<D>();
     constexpr uint32_t FULL = 0xffffffffu;
     extern __shared__ __align__(16) unsigned char smem[];
