@@ -195,13 +195,15 @@ struct Staging {
 #ifndef TBLAEQ_EXPAND_MIN_BLOCKS_BOUND
 #define TBLAEQ_EXPAND_MIN_BLOCKS_BOUND 8
 #endif
-// Unroll factors of the per-round loops (build-time knobs, like the launch shape): the item test
-// of levels that output a frontier, and pass 2 of every level. Measured on B200: fully unrolled,
-// the frontier levels stall on instruction fetch (their loop body holds the box prefilter, the
-// radius or bound test, the node loads and the frontier writes); with the test unrolled twice and
-// pass 2 rolled, the mesh-2 range level went from 0.65 to 0.45 ms and the KNN levels above the
-// finest from 1.92 to 1.75 ms (2M x 16, 512 queries); a rolled pass 2 also frees registers at the
-// point levels. The test loop of point levels and the item-to-entry mapping stay fully unrolled.
+// Unroll factors of the per-round loops of the range levels (build-time knobs, like the launch
+// shape): the item test of levels that output a frontier, and pass 2 of every range level.
+// Measured on B200: fully unrolled, the range frontier levels stall on instruction fetch (their
+// loop body holds the box prefilter, the radius test, the node loads and the frontier writes);
+// with the test unrolled twice and pass 2 rolled, the mesh-2 range level went from 0.65 to 0.45 ms;
+// a rolled pass 2 also frees registers at the finest range level. The KNN levels stay fully
+// unrolled: their pass 2 is hot (wave 1 writes every point of its clusters) and the batched KNN
+// step measured about 8% slower rolled. The test loop of point levels and the item-to-entry
+// mapping stay fully unrolled everywhere.
 #ifndef TBLAEQ_UNROLL_FRONTIER_TEST
 #define TBLAEQ_UNROLL_FRONTIER_TEST 2
 #endif
@@ -483,9 +485,10 @@ __global__ void __launch_bounds__(kExpandThreads, expandMinBlocks<PRED>()) expan
     constexpr int R = S::kRounds;
     constexpr int DM = (D > 0) ? D : 32;
     constexpr bool NODE = needsNode<PRED, TO_RESULT>();
-    // Code size (see TBLAEQ_UNROLL_FRONTIER_TEST).
-    constexpr int kUnrollTest = TO_RESULT ? R : TBLAEQ_UNROLL_FRONTIER_TEST;
-    constexpr int kUnrollPass2 = TBLAEQ_UNROLL_PASS2;
+    // Code size (see TBLAEQ_UNROLL_FRONTIER_TEST); the KNN levels unroll every loop.
+    constexpr bool kKnn = PRED == kPredKnnBound || PRED == kPredKnnPoint;
+    constexpr int kUnrollTest = (TO_RESULT || kKnn) ? R : TBLAEQ_UNROLL_FRONTIER_TEST;
+    constexpr int kUnrollPass2 = kKnn ? R : TBLAEQ_UNROLL_PASS2;
     constexpr bool kFastBox = PRED == kPredRangeBox && TO_RESULT && !STAGED && coalescedBox<D>();
     constexpr uint32_t FULL = 0xffffffffu;
     extern __shared__ __align__(16) unsigned char smem[];
