@@ -397,7 +397,7 @@ def run_knn(args, tb, wl, rank, world, local):
                           f"{args.nq} points (data + N(0,(2% extent)^2)), K=20 and K=100 alternating",
               "index_points": cfg["N"], "dim": cfg["D"], "queries_per_step": args.nq, "mode": "exact",
               "l2": "inputs larger than L2 (6.4 GB of rows per step)", "parallelism": f"replicas{world}"}
-    steps = args.steps if args.steps != 200 else 2
+    steps = args.steps if args.steps != 200 else 3
     if args.impl == "reference":
         if rank != 0:
             return
@@ -443,10 +443,11 @@ def run_knn(args, tb, wl, rank, world, local):
     train_s = time.perf_counter() - t0
     stats = h.scorer_stats()
 
-    def leg(two_wave, learned, n_steps):
+    def leg(two_wave, learned, n_steps, n_warm=1):
         h.set_two_wave(two_wave)
         h.scorer_enable(learned)
-        h.query_batch(tb.QueryType.POINT, dP, tb.Mode.EXACT, K=K)  # sizes every workspace
+        for _ in range(max(1, n_warm)):  # the first batch sizes every workspace
+            h.query_batch(tb.QueryType.POINT, dP, tb.Mode.EXACT, K=K)
         ts = []
         if learned:
             torch.cuda.nvtx.range_push("timed")  # profilers select the timed steps by this range
@@ -463,7 +464,7 @@ def run_knn(args, tb, wl, rank, world, local):
         return args.nq * n_steps / sum(ts), c["rows"] / args.nq, ts
 
     with ClockSampler(local) as clk:
-        learned_qps, learned_rows, step_s = leg(True, True, steps)
+        learned_qps, learned_rows, step_s = leg(True, True, steps, args.warmup)
     lb_qps, lb_rows, _ = leg(True, False, 1)
     one_qps, one_rows, _ = leg(False, False, 1)
 
@@ -507,7 +508,7 @@ def run_knn(args, tb, wl, rank, world, local):
     value = learned_qps * world
     print(json.dumps({
         "metric": "exact-result KNN queries/s (batched + learned ranking, 1 B200 per rank)",
-        "value": value, "unit": "queries/s", "n_gpus": world, "steps": steps, "warmup": 1,
+        "value": value, "unit": "queries/s", "n_gpus": world, "steps": steps, "warmup": max(1, args.warmup),
         "ms_per_step": statistics.mean(step_s) * 1e3, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded RandomKmeans-style index and points)",
         "config": config,

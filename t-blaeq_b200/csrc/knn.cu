@@ -376,22 +376,41 @@ __global__ void clampCountsKernel(const uint64_t* off, const uint32_t* K, uint32
     }
 }
 
+// Lower bound of the distance from each frontier entry's query point to the points below its
+// cluster: the larger of (centre distance - subtree radius) and the distance to the cluster's box.
+// D > 0 specialises the dimension loop (pairs of dimensions per 16-byte load when D is even); the
+// products are accumulated in the same order either way, so the bounds are identical.
+template <int D>
 __global__ void entryBoundsKernel(const uint32_t* q, const uint32_t* node, const double* x, const uint32_t* hdr,
-                                  uint32_t cap, int D, const double* points, const NodeRec* nodes, const float* aabb,
-                                  double* lb, double* score) {
+                                  uint32_t cap, int dimRt, const double* points, const NodeRec* nodes,
+                                  const float* aabb, double* lb, double* score) {
+    const int dim = D > 0 ? D : dimRt;
     const uint32_t n = min(hdr[0], cap);
     for (uint32_t e = blockIdx.x * blockDim.x + threadIdx.x; e < n; e += gridDim.x * blockDim.x) {
-        const double* p = points + static_cast<size_t>(q[e]) * D;
-        const double* c = x + static_cast<size_t>(e) * D;
+        const double* p = points + static_cast<size_t>(q[e]) * dim;
+        const double* c = x + static_cast<size_t>(e) * dim;
         const uint32_t k = node[e];
-        const float* b = aabb + static_cast<size_t>(k) * 2 * D;
+        const float* b = aabb + static_cast<size_t>(k) * 2 * dim;
         double dist = 0.0, gap = 0.0;
-        for (int d = 0; d < D; ++d) {
-            const double diff = p[d] - c[d];
+        auto step = [&](double pd, double cd, float lo, float hi) {
+            const double diff = pd - cd;
             dist = __fma_rn(diff, diff, dist);
-            const double l = static_cast<double>(b[d]), h = static_cast<double>(b[D + d]);
-            const double g = fmax(fmax(l - p[d], p[d] - h), 0.0);
+            const double l = static_cast<double>(lo), h = static_cast<double>(hi);
+            const double g = fmax(fmax(l - pd, pd - h), 0.0);
             gap = __fma_rn(g, g, gap);
+        };
+        if constexpr (D > 0 && D % 2 == 0) {
+#pragma unroll
+            for (int d = 0; d < D; d += 2) {
+                const double2 pp = __ldg(reinterpret_cast<const double2*>(p + d));
+                const double2 cc = __ldg(reinterpret_cast<const double2*>(c + d));
+                const float2 lo = __ldg(reinterpret_cast<const float2*>(b + d));
+                const float2 hi = __ldg(reinterpret_cast<const float2*>(b + D + d));
+                step(pp.x, cc.x, lo.x, hi.x);
+                step(pp.y, cc.y, lo.y, hi.y);
+            }
+        } else {
+            for (int d = 0; d < dim; ++d) step(p[d], c[d], b[d], b[dim + d]);
         }
         const double v = fmax(sqrt(dist) - nodes[k].rad, sqrt(gap) * (1.0 - 1e-12));
         lb[e] = v;
@@ -446,7 +465,16 @@ int gridFor(uint64_t n, int threads) {
 void launchEntryBounds(const uint32_t* q, const uint32_t* node, const double* x, const uint32_t* hdr, uint32_t cap,
                        int D, const double* points, const NodeRec* nodes, const float* aabb, double* lb, double* score,
                        cudaStream_t s) {
-    entryBoundsKernel<<<148 * 8, 256, 0, s>>>(q, node, x, hdr, cap, D, points, nodes, aabb, lb, score);
+    auto go = [&](auto kern) { kern<<<148 * 8, 256, 0, s>>>(q, node, x, hdr, cap, D, points, nodes, aabb, lb, score); };
+    switch (D) {
+        case 2: go(entryBoundsKernel<2>); break;
+        case 3: go(entryBoundsKernel<3>); break;
+        case 4: go(entryBoundsKernel<4>); break;
+        case 5: go(entryBoundsKernel<5>); break;
+        case 8: go(entryBoundsKernel<8>); break;
+        case 16: go(entryBoundsKernel<16>); break;
+        default: go(entryBoundsKernel<0>); break;
+    }
     TBLAEQ_CUDA(cudaGetLastError());
 }
 

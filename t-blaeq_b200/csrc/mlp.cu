@@ -318,21 +318,41 @@ __global__ void __launch_bounds__(kTcRows) forwardTcKernel(const __nv_bfloat16* 
         const uint32_t e = static_cast<uint32_t>(tile * kTcRows) + tid;
         const bool live = e < n;
         // Features of this thread's sample, 8 columns (one 16-byte core-matrix row) at a time.
-        for (uint32_t k0 = 0; k0 < L.kp; k0 += 8) {
-            float v[8];
+        if constexpr (FRONTIER) {
+            // The entry's query point and centre are rows of D doubles: chunks of eight features
+            // that lie inside one of them (D even) are read as four 16-byte loads.
+            const double* pt = src.points + static_cast<size_t>(live ? src.q[e] : 0u) * D;
+            const double* xr = src.x + static_cast<size_t>(live ? e : 0u) * D;
+            const bool even = (D & 1) == 0;
+            for (uint32_t k0 = 0; k0 < L.kp; k0 += 8) {
+                const int kb = static_cast<int>(k0);
+                float v[8];
+                const double* run = nullptr;
+                if (live && even && kb + 8 <= D) run = pt + kb;
+                if (live && even && kb >= D && kb + 8 <= 2 * D) run = xr + (kb - D);
+                if (run) {
 #pragma unroll
-            for (int i = 0; i < 8; ++i) {
-                const int k = static_cast<int>(k0) + i;
-                float f = 0.f;
-                if (live && k < in) {
-                    if constexpr (FRONTIER)
-                        f = frontierFeature(src, e, k, D);
-                    else
-                        f = src.X[static_cast<size_t>(e) * in + k];
+                    for (int i = 0; i < 8; i += 2) {
+                        const double2 t = __ldg(reinterpret_cast<const double2*>(run + i));
+                        v[i] = static_cast<float>(t.x * src.inv);
+                        v[i + 1] = static_cast<float>(t.y * src.inv);
+                    }
+                } else {
+#pragma unroll
+                    for (int i = 0; i < 8; ++i) v[i] = (live && kb + i < in) ? frontierFeature(src, e, kb + i, D) : 0.f;
                 }
-                v[i] = f;
+                *reinterpret_cast<uint4*>(smem + L.f + bf16Offset(tid, k0, L.kp)) = packBf16x8(v);
             }
-            *reinterpret_cast<uint4*>(smem + L.f + bf16Offset(tid, k0, L.kp)) = packBf16x8(v);
+        } else {
+            for (uint32_t k0 = 0; k0 < L.kp; k0 += 8) {
+                float v[8];
+#pragma unroll
+                for (int i = 0; i < 8; ++i) {
+                    const int k = static_cast<int>(k0) + i;
+                    v[i] = (live && k < in) ? src.X[static_cast<size_t>(e) * in + k] : 0.f;
+                }
+                *reinterpret_cast<uint4*>(smem + L.f + bf16Offset(tid, k0, L.kp)) = packBf16x8(v);
+            }
         }
         tc::fenceProxyAsync();
         tc::tcFenceBefore();
