@@ -152,8 +152,10 @@ int tblaeq_query_batch(tblaeq_handle* h, const tblaeq_batch* batch, tblaeq_batch
 int tblaeq_query_batch_host(tblaeq_handle* h, const tblaeq_batch* batch, uint64_t* offsets_out, uint64_t* ids_out,
                             uint64_t ids_cap, double* dist2_out, uint64_t* total);
 
-/* Enqueue a batch on the handle's stream and return without waiting (no host synchronisation, so
- * it can be timed with events or overlapped). `queries` must be device memory that stays valid
+/* Enqueue a range batch on the handle's stream and return without waiting (no host
+ * synchronisation, so it can be timed with events or overlapped; KNN batches, which may run as
+ * chunks with host synchronisation between them, go through tblaeq_query_batch). `queries` must be
+ * device memory that stays valid
  * until tblaeq_batch_wait returns, and a synchronous tblaeq_query_batch with the same nq, mode and
  * flags must have run first (it sizes the workspaces). With TBLAEQ_USE_GRAPH the launches are
  * captured once into a CUDA graph and replayed. */

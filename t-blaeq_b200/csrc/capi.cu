@@ -365,7 +365,9 @@ int tblaeq_query_batch_async(tblaeq_handle* h, const tblaeq_batch* b) {
     if (!b->queriesOnDevice && b->nq) return fail(TBLAEQ_ERR_INVALID, "async batches need device queries");
     if (reinterpret_cast<uintptr_t>(b->queries) & 15u)
         return fail(TBLAEQ_ERR_INVALID, "async batches need device queries on a 16-byte boundary");
-    if (b->qtype != TBLAEQ_RANGE) return fail(TBLAEQ_ERR_INVALID, "batched KNN is not available in this build");
+    // A KNN batch may split into chunks with host synchronisation between them: synchronous only.
+    if (b->qtype != TBLAEQ_RANGE)
+        return fail(TBLAEQ_ERR_INVALID, "asynchronous batches are range batches; run KNN with tblaeq_query_batch");
     return guarded([&]() -> int {
         Runtime& rt = h->qh->runtime();
         h->lastNq = b->nq;
