@@ -687,10 +687,47 @@ def run_build(args, tb, rank, world, local):
         "clocks": clk.summary()}))
 
 
+def reference_cuda_range(tb, h, Q, D, n):
+    """The reference's own CUDA build (oracle/_ref/ref_harness: the reference's
+    QueryHandler::performSingleRangeQuery with saveFineMesh=true under policy L0) on this GPU, one
+    query at a time, timed by its per-query timer; like its CLI (QueryEngine.cu:216-227) the mean
+    drops the fastest and the slowest query. It returns the reference's candidate sets: every point
+    of every surviving cluster, without the exact final filter."""
+    harness = os.path.join(REPO, "oracle", "_ref", "ref_harness")
+    if not os.path.exists(harness):
+        return {"unavailable": "the reference build (oracle/_ref) is not present"}
+    import tempfile
+    with tempfile.TemporaryDirectory() as d:
+        idx = os.path.join(d, "idx")
+        h.save_index(idx)
+        qf = os.path.join(d, "q.txt")
+        tb.save_query_file(qf, tb.QueryType.RANGE, Q[:n], D)
+        out = os.path.join(d, "ref.bin")
+        subprocess.run([harness, idx, qf, "0", "0", "L0", out], check=True, timeout=1800,
+                       stdout=subprocess.DEVNULL)
+        raw = open(out, "rb").read()
+    nq, intervals = (int(x) for x in np.frombuffer(raw, np.uint64, 2, 0))
+    off, us, cands = 16, [], 0
+    for _ in range(nq):  # per query: level sizes, microseconds, candidate count, candidate ids
+        off += 8 * intervals
+        us.append(float(np.frombuffer(raw, np.float64, 1, off)[0]))
+        off += 8
+        c = int(np.frombuffer(raw, np.uint64, 1, off)[0])
+        off += 8 + 8 * c
+        cands += c
+    t = sorted(us)
+    kept = t[1:-1] if len(t) > 2 else t
+    mean = sum(kept) / len(kept)
+    return {"value": 1e6 / mean, "unit": "queries/s", "queries": nq, "mean_us": mean, "p50_us": t[len(t) // 2],
+            "candidates": cands, "kind": "reference CUDA build on this GPU, one query at a time, policy L0",
+            "results": "the reference's candidate sets (no exact final filter)"}
+
+
 def run_reference(args, tb, wl, cfg_name, config, rank, world):
     """Reference arm: the CPU restatement of the reference traversal (exact semantics) timed on the
     host cores. The reference has no CPU implementation of its query path (every strategy launches
-    CUDA kernels), so the oracle port stands in for it."""
+    CUDA kernels), so the oracle port stands in for it; the reference's own CUDA build, timed one
+    query at a time on the same GPU, is reported beside it."""
     if rank != 0:
         return
     sys.path.insert(0, REPO)
@@ -721,6 +758,11 @@ def run_reference(args, tb, wl, cfg_name, config, rank, world):
                             "sample": f"{per_step} boxes per step of the {args.nq}-box workload, exact traversal "
                                       f"port, OpenMP over queries"},
            "e2e": {"value": v, "unit": "queries/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    # Beside it: the reference's own implementation, which runs on the GPU only.
+    try:
+        out["reference_cuda_b200"] = reference_cuda_range(tb, h, Q, h.info()["D"], min(args.nq, 256))
+    except Exception as e:  # reported, never fatal to the CPU arm
+        out["reference_cuda_b200"] = {"unavailable": f"{type(e).__name__}: {e}"[:200]}
     print(json.dumps(out))
 
 
