@@ -706,7 +706,14 @@ __global__ void __launch_bounds__(kExpandThreads, expandMinBlocks<PRED>()) expan
             }
         }
 
-        // ---- publish the tile's counts and learn where its output starts.
+        // ---- publish the tile's counts and learn where its output starts. A tile that kept
+        // nothing writes nothing, so it needs no output position: it publishes its empty
+        // aggregate and moves on without waiting for its predecessors (most tiles of the finest
+        // levels); successors sum through it. The last tile still resolves the totals.
+        if (aggCnt == 0 && aggSum == 0 && tile != nTiles - 1) {
+            if (lane == 0) storeDesc(&a.scratch.desc[tile], packDesc(tile == 0 ? kFlagPrefix : kFlagAggregate, 0, 0));
+            continue;
+        }
         unsigned long long exCnt, exSum;
         lookback(a.scratch.desc, tile, aggCnt, aggSum, a.scratch.status, exCnt, exSum);
         if (tile == nTiles - 1 && lane == 0) {
