@@ -479,6 +479,47 @@ __device__ __forceinline__ bool singleEntryRangeBox(const ExpandArgs& a, uint32_
     return ((mine >> ((lane % G) * L)) & kAll) == kAll;
 }
 
+// Exact range frontier levels, a round whose 32 children all belong to one frontier entry: the
+// children are consecutive nodes, so their float boxes (lo[D] then hi[D], 8·D bytes each) form one
+// contiguous block. Each lane takes one 16-byte piece (four lower or four upper bounds) of a box
+// per load and tests it against the matching four upper or lower bounds of the query's box; a
+// ballot per load collects the pieces. Same comparisons as aabbMeets, so the outcome is identical.
+// Returns the prefilter outcome of the calling lane's own child (item `lane` of the round).
+template <int D>
+constexpr bool coalescedAabb() {
+    return D >= 4 && D % 4 == 0 && 32 % (D >= 2 ? D / 2 : 1) == 0;
+}
+template <int D>
+__device__ __forceinline__ bool singleEntryAabb(const ExpandArgs& a, uint32_t kk0, uint32_t q, int lane) {
+    constexpr int L = D / 2;   // pieces per box
+    constexpr int G = 32 / L;  // boxes per load
+    constexpr int LO = D / 4;  // pieces holding lower bounds
+    constexpr int P = L < 4 ? L : 4;
+    constexpr uint32_t kAll = (1u << L) - 1u;
+    const int c = lane % L;
+    const bool lower = c < LO;
+    const float4* cb = reinterpret_cast<const float4*>(a.child.aabb + static_cast<size_t>(kk0) * 2 * D);
+    const float* qb = a.query.boxesF + static_cast<size_t>(q) * 2 * D;
+    // A lower-bound piece is tested against the query's upper bounds, and the other way round.
+    const float4 qv = __ldg(reinterpret_cast<const float4*>(lower ? qb + D + 4 * c : qb + 4 * (c - LO)));
+    uint32_t mine = 0;
+#pragma unroll
+    for (int s0 = 0; s0 < L; s0 += P) {
+        float4 bv[P];
+#pragma unroll
+        for (int i = 0; i < P; ++i) bv[i] = __ldg(cb + (s0 + i) * 32 + lane);
+#pragma unroll
+        for (int i = 0; i < P; ++i) {
+            const float4 v = bv[i];
+            const bool pass = lower ? (v.x <= qv.x) & (v.y <= qv.y) & (v.z <= qv.z) & (v.w <= qv.w)
+                                    : (v.x >= qv.x) & (v.y >= qv.y) & (v.z >= qv.z) & (v.w >= qv.w);
+            const uint32_t b = __ballot_sync(0xffffffffu, pass);
+            if (s0 + i == lane / G) mine = b;
+        }
+    }
+    return ((mine >> ((lane % G) * L)) & kAll) == kAll;
+}
+
 template <int D, int PRED, bool TO_RESULT, bool STAGED>
 __global__ void __launch_bounds__(kExpandThreads, expandMinBlocks<PRED>()) expandKernel(ExpandArgs a) {
     using S = Staging<D, STAGED>;
@@ -490,6 +531,7 @@ __global__ void __launch_bounds__(kExpandThreads, expandMinBlocks<PRED>()) expan
     constexpr int kUnrollTest = (TO_RESULT || kKnn) ? R : TBLAEQ_UNROLL_FRONTIER_TEST;
     constexpr int kUnrollPass2 = kKnn ? R : TBLAEQ_UNROLL_PASS2;
     constexpr bool kFastBox = PRED == kPredRangeBox && TO_RESULT && !STAGED && coalescedBox<D>();
+    constexpr bool kFastAabb = PRED == kPredRangeRadius && coalescedAabb<D>();
     constexpr uint32_t FULL = 0xffffffffu;
     extern __shared__ __align__(16) unsigned char smem[];
     const int dim = (D > 0) ? D : a.D;
@@ -658,6 +700,16 @@ __global__ void __launch_bounds__(kExpandThreads, expandMinBlocks<PRED>()) expan
                     done = true;
                 }
             }
+            bool preKnown = false, preFast = true;
+            if constexpr (kFastAabb) {
+                // Warp-uniform: a full round inside one entry, children keyed by their rows.
+                const uint32_t w0 = sWin[r * 32], w31 = sWin[r * 32 + 31];
+                if (W != 0 && t0 + r * 32 + 32 <= total && w0 == w31 && a.child.aabb && a.query.boxesF &&
+                    !a.child.keys) {
+                    preFast = singleEntryAabb<D>(a, sRow[r * 32], wQ[w0], lane);
+                    preKnown = true;
+                }
+            }
             if (work && !done) {
                 const uint32_t j = sRow[r * 32 + lane];
                 const uint32_t w = sWin[r * 32 + lane];
@@ -666,7 +718,10 @@ __global__ void __launch_bounds__(kExpandThreads, expandMinBlocks<PRED>()) expan
                 const uint32_t kk = a.child.keys ? static_cast<uint32_t>(a.child.keys[j]) : j;
                 bool pre = true;
                 if constexpr (PRED == kPredRangeRadius) {
-                    if (a.child.aabb && a.query.boxesF) pre = aabbMeets<D, DM>(a, dim, kk, q);
+                    if (preKnown)
+                        pre = preFast;
+                    else if (a.child.aabb && a.query.boxesF)
+                        pre = aabbMeets<D, DM>(a, dim, kk, q);
                 }
                 if (pre) {
                     NodeRec nr{0.0, 0u, 0u};

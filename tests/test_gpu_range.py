@@ -142,9 +142,10 @@ def test_large_results_force_workspace_growth(tb, env, oracle_mod):
 
 @pytest.mark.parametrize("D,ratios", [(2, (16, 8, 4)), (3, (10, 10, 10)), (5, (40, 20, 10)), (6, (30, 10, 5)),
                                       (8, (100, 50, 20)), (16, (50, 20, 10)),
-                                      # 100 points per finest cluster: most 32-item rounds lie in one
-                                      # cluster and take the coalesced single-entry test
-                                      (4, (100, 20, 10)), (16, (100, 10, 5))])
+                                      # 40-100 children per node at the two finest levels: many
+                                      # 32-item rounds lie in one entry and take the coalesced
+                                      # single-entry tests (box prefilter and point test)
+                                      (4, (100, 20, 10)), (4, (40, 40, 10)), (16, (40, 40, 10))])
 def test_other_dimensions(tb, oracle_mod, tmp_path, cuda, D, ratios):
     """Both kernel variants (rows read straight into registers, or staged through shared memory by
     warp-wide chunk copies) give the oracle's results at every level, for even and odd D."""
