@@ -419,7 +419,12 @@ BatchOutput BatchEngine::runRange(const double* dBoxes, uint32_t nq, int mode, u
     reserve(caps_, nq, flags);
     for (int attempt = 0; attempt < 16; ++attempt) {
         enqueueRange(dBoxes, nq, mode, flags);
-        const uint32_t st = status();
+        // The status word and the result total come back together: one host synchronisation.
+        uint32_t st = 0;
+        uint64_t total = 0;
+        TBLAEQ_CUDA(cudaMemcpyAsync(&st, zeroBlock_.as<char>() + offStatus_, 4, cudaMemcpyDeviceToHost, stream_));
+        TBLAEQ_CUDA(cudaMemcpyAsync(&total, offsets_.as<uint64_t>() + nq, 8, cudaMemcpyDeviceToHost, stream_));
+        TBLAEQ_CUDA(cudaStreamSynchronize(stream_));
         if (st & (kStatusLookbackTimeout | kStatusWindowOverflow)) {
             throw CudaError(cudaErrorLaunchTimeout, "traversal kernel reported status " + std::to_string(st));
         }
@@ -427,7 +432,7 @@ BatchOutput BatchEngine::runRange(const double* dBoxes, uint32_t nq, int mode, u
             throw SplitBatch("a level generates more than 2^32 items; split the batch");
         if (st == 0) {
             BatchOutput o = output(nq, flags);
-            o.total = lastTotal(nq);
+            o.total = total;
             return o;
         }
         growFromHeaders();
