@@ -20,6 +20,9 @@
 // items to entries with a ballot and an OR-reduction over the 32 entries that can overlap a 32-item
 // round, tests every item in a first pass that keeps one bit per item, publishes its counts through
 // the look-back, and only then rebuilds and writes the kept items (a small fraction at every level).
+// A tile that kept nothing publishes its empty counts and moves on without waiting for its
+// predecessors. Rounds whose 32 items lie in one entry read their consecutive rows (or child boxes)
+// as one coalesced block, a 16-byte piece per lane, and combine the pieces' tests by ballot.
 // Tiles are claimed through an atomic ticket by a persistent grid, so every tile a look-back waits
 // on belongs to a warp that is already running; every spin is bounded and reports a status bit
 // instead of hanging.
