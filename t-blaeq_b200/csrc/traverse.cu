@@ -182,7 +182,15 @@ struct Staging {
     static constexpr int kWindow = kWarpTile + 1;  // most entries a tile can overlap
     static constexpr int kWindowBytes = 3 * kWindow * 4 + 4;
     static constexpr int kWarpBytes = kRowBytes + kNodeBytes + kCacheBytes + ((kWindowBytes + 15) / 16) * 16;
+    // Range frontier levels only (kept out of the others' shared memory, which would shrink their
+    // L1): the tile's prefilter survivors (item indices) and their keep bits.
+    static constexpr int kDeferBytes = kWarpTile * 2 + kRounds * 4;
 };
+
+template <int D, bool STAGED, int PRED>
+constexpr int warpSmemBytes() {
+    return Staging<D, STAGED>::kWarpBytes + (PRED == kPredRangeRadius ? Staging<D, STAGED>::kDeferBytes : 0);
+}
 
 // Launch shape of the expand kernels (independent warps per CTA and the register bound). These are
 // build-time tuning knobs; the defaults are the fastest measured on B200 for the benchmark index.
@@ -221,9 +229,9 @@ constexpr int expandMinBlocks() {
                                                                : TBLAEQ_EXPAND_MIN_BLOCKS;
 }
 
-template <int D, bool STAGED>
+template <int D, bool STAGED, int PRED>
 constexpr size_t expandSmemBytes() {
-    return static_cast<size_t>(Staging<D, STAGED>::kWarpBytes) * (kExpandThreads / 32);
+    return static_cast<size_t>(warpSmemBytes<D, STAGED, PRED>()) * (kExpandThreads / 32);
 }
 
 __device__ __forceinline__ void cpAsync16(void* dst, const void* src) {
@@ -532,6 +540,10 @@ __global__ void __launch_bounds__(kExpandThreads, expandMinBlocks<PRED>()) expan
     constexpr int kUnrollPass2 = kKnn ? R : TBLAEQ_UNROLL_PASS2;
     constexpr bool kFastBox = PRED == kPredRangeBox && TO_RESULT && !STAGED && coalescedBox<D>();
     constexpr bool kFastAabb = PRED == kPredRangeRadius && coalescedAabb<D>();
+    // Exact range frontier levels test children that pass the box prefilter after the rounds,
+    // 32 at a time, so the FP64 radius test runs on full warps instead of in every round that
+    // holds one survivor.
+    constexpr bool kDefer = PRED == kPredRangeRadius;
     constexpr uint32_t FULL = 0xffffffffu;
     extern __shared__ __align__(16) unsigned char smem[];
     const int dim = (D > 0) ? D : a.D;
@@ -539,7 +551,7 @@ __global__ void __launch_bounds__(kExpandThreads, expandMinBlocks<PRED>()) expan
     const int w = threadIdx.x >> 5;
     const uint32_t lanesLe = (2u << lane) - 1u;  // lanes 0..lane (wraps to all lanes for lane 31)
     const uint32_t lanesLt = (1u << lane) - 1u;
-    unsigned char* warpSmem = smem + static_cast<size_t>(w) * S::kWarpBytes;
+    unsigned char* warpSmem = smem + static_cast<size_t>(w) * warpSmemBytes<D, STAGED, PRED>();
     unsigned char* rowBuf = warpSmem;                                    // [kStages][32][kStride]
     NodeRec* nodeBuf = reinterpret_cast<NodeRec*>(warpSmem + S::kRowBytes);  // [kStages][32]
     uint32_t* sRow = reinterpret_cast<uint32_t*>(warpSmem + S::kRowBytes + S::kNodeBytes);  // [R][32]
@@ -547,6 +559,9 @@ __global__ void __launch_bounds__(kExpandThreads, expandMinBlocks<PRED>()) expan
     uint32_t* wCp = reinterpret_cast<uint32_t*>(sWin + R * 32);  // window of the tile's entries: prefix, first child, query
     uint32_t* wCb = wCp + S::kWindow;
     uint32_t* wQ = wCb + S::kWindow;
+    uint16_t* sList = reinterpret_cast<uint16_t*>(warpSmem + S::kRowBytes + S::kNodeBytes + S::kCacheBytes +
+                                                  ((S::kWindowBytes + 15) / 16) * 16);  // deferred items
+    uint32_t* sKeep = reinterpret_cast<uint32_t*>(sList + kWarpTile);                   // [R] keep words
 
     const uint32_t entries = a.in.hdr[0];
     const uint32_t total = a.in.hdr[1];
@@ -665,6 +680,12 @@ __global__ void __launch_bounds__(kExpandThreads, expandMinBlocks<PRED>()) expan
             }
         }
         uint32_t keepBits = 0, aggCnt = 0, aggSum = 0;
+        uint32_t listLen = 0;  // deferred prefilter survivors of this tile (kDefer)
+        const bool deferOn = kDefer && a.child.aabb != nullptr && a.query.boxesF != nullptr;
+        if constexpr (kDefer) {
+            if (lane < R) sKeep[lane] = 0u;
+            __syncwarp();
+        }
 #pragma unroll kUnrollTest
         for (int r = 0; r < R; ++r) {
             if constexpr (S::kOn) {
@@ -678,7 +699,7 @@ __global__ void __launch_bounds__(kExpandThreads, expandMinBlocks<PRED>()) expan
             }
             if (t0 + r * 32 >= total) continue;  // warp-uniform
             const bool valid = (validBits >> r) & 1u;
-            bool keep = false;
+            bool keep = false, defer = false;
             uint32_t cc = 0;
             bool work = valid;
             if (PRED == kPredKnnPoint && valid && a.wave != 0 && a.child.entrySel) {
@@ -723,7 +744,9 @@ __global__ void __launch_bounds__(kExpandThreads, expandMinBlocks<PRED>()) expan
                     else if (a.child.aabb && a.query.boxesF)
                         pre = aabbMeets<D, DM>(a, dim, kk, q);
                 }
-                if (pre) {
+                if (pre && deferOn) {
+                    defer = true;  // radius test after the rounds
+                } else if (pre) {
                     NodeRec nr{0.0, 0u, 0u};
                     const double* xp = a.in.x + static_cast<size_t>(e) * dim;
                     if constexpr (S::kOn) {
@@ -736,6 +759,13 @@ __global__ void __launch_bounds__(kExpandThreads, expandMinBlocks<PRED>()) expan
                         keep = evalItem<D, DM, PRED, TO_RESULT, false>(a, dim, a.child.rows + static_cast<size_t>(j) * dim,
                                                                        xp, q, j, kk, nr, cc);
                     }
+                }
+            }
+            if constexpr (kDefer) {
+                const uint32_t dm = __ballot_sync(FULL, defer);
+                if (dm) {  // warp-uniform
+                    if (defer) sList[listLen + __popc(dm & lanesLt)] = static_cast<uint16_t>(r * 32 + lane);
+                    listLen += __popc(dm);
                 }
             }
             if (a.scratch.work) warpRows += __popc(__ballot_sync(FULL, work));
@@ -758,6 +788,39 @@ __global__ void __launch_bounds__(kExpandThreads, expandMinBlocks<PRED>()) expan
                     for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(FULL, s, o);
                     aggSum += s;
                 }
+            }
+        }
+
+        // ---- deferred radius tests (kDefer): the prefilter survivors of every round, 32 at a time.
+        if constexpr (kDefer) {
+            if (listLen) {  // warp-uniform
+                __syncwarp();
+                for (uint32_t b0 = 0; b0 < listLen; b0 += 32) {
+                    const uint32_t t = b0 + lane;
+                    bool k2 = false;
+                    uint32_t cc2 = 0, idx = 0;
+                    if (t < listLen) {
+                        idx = sList[t];
+                        const uint32_t j = sRow[idx];
+                        const uint32_t w = sWin[idx];
+                        const uint32_t q = wQ[w];
+                        const uint32_t kk = a.child.keys ? static_cast<uint32_t>(a.child.keys[j]) : j;
+                        const NodeRec nr = a.child.nodes[kk];
+                        k2 = evalItem<D, DM, PRED, TO_RESULT, false>(a, dim, a.child.rows + static_cast<size_t>(j) * dim,
+                                                                     a.in.x + static_cast<size_t>(eLo + w) * dim, q, j,
+                                                                     kk, nr, cc2);
+                        if (k2) atomicOr(&sKeep[idx >> 5], 1u << (idx & 31u));
+                    }
+                    const uint32_t kb2 = __ballot_sync(FULL, k2);
+                    aggCnt += __popc(kb2);
+                    uint32_t s2 = k2 ? cc2 : 0u;
+#pragma unroll
+                    for (int o = 16; o > 0; o >>= 1) s2 += __shfl_xor_sync(FULL, s2, o);
+                    aggSum += s2;
+                }
+                __syncwarp();
+#pragma unroll
+                for (int r = 0; r < R; ++r) keepBits |= ((sKeep[r] >> lane) & 1u) << r;
             }
         }
 
@@ -939,7 +1002,7 @@ __global__ void exclusiveScanKernel(const uint32_t* counts, uint64_t* offsets, u
 template <int D, int PRED, bool TO_RESULT, bool STAGED>
 void launchOne(const ExpandArgs& a, int gridBlocks, cudaStream_t s) {
     auto kern = expandKernel<D, PRED, TO_RESULT, STAGED>;
-    constexpr size_t smemBytes = expandSmemBytes<D, STAGED>();
+    constexpr size_t smemBytes = expandSmemBytes<D, STAGED, PRED>();
     static int cached = 0;
     if (cached == 0) {
         int dev = 0, sms = 0, perSm = 0;
