@@ -711,22 +711,39 @@ def reference_cuda_range(tb, h, Q, D, n):
         out = os.path.join(d, "ref.bin")
         subprocess.run([harness, idx, qf, "0", "0", "L0", out], check=True, timeout=1800,
                        stdout=subprocess.DEVNULL)
-        raw = open(out, "rb").read()
+        us, cands = read_harness_times(open(out, "rb").read())
+    t = sorted(us)
+    mean = reference_mean_us(us)
+    return {"value": 1e6 / mean, "unit": "queries/s", "queries": len(us), "mean_us": mean,
+            "p50_us": t[len(t) // 2], "candidates": cands,
+            "kind": "reference CUDA build on this GPU, one query at a time, policy L0",
+            "results": "the reference's candidate sets (no exact final filter)"}
+
+
+def read_harness_times(raw: bytes):
+    """Per-query microseconds and the total candidate count from the reference harness's dump:
+    u64 query count, u64 interval count, then per query: interval u64 level sizes, f64 microseconds,
+    u64 candidate count and that many u64 ids."""
     nq, intervals = (int(x) for x in np.frombuffer(raw, np.uint64, 2, 0))
     off, us, cands = 16, [], 0
-    for _ in range(nq):  # per query: level sizes, microseconds, candidate count, candidate ids
+    for _ in range(nq):
         off += 8 * intervals
         us.append(float(np.frombuffer(raw, np.float64, 1, off)[0]))
         off += 8
         c = int(np.frombuffer(raw, np.uint64, 1, off)[0])
         off += 8 + 8 * c
         cands += c
+    if off != len(raw):
+        raise ValueError("reference harness output has trailing or missing bytes")
+    return us, cands
+
+
+def reference_mean_us(us):
+    """The reference CLI's per-query mean: the fastest and the slowest query dropped when there are
+    more than two (src/core/QueryEngine.cu:216-227)."""
     t = sorted(us)
     kept = t[1:-1] if len(t) > 2 else t
-    mean = sum(kept) / len(kept)
-    return {"value": 1e6 / mean, "unit": "queries/s", "queries": nq, "mean_us": mean, "p50_us": t[len(t) // 2],
-            "candidates": cands, "kind": "reference CUDA build on this GPU, one query at a time, policy L0",
-            "results": "the reference's candidate sets (no exact final filter)"}
+    return sum(kept) / len(kept)
 
 
 def run_reference(args, tb, wl, cfg_name, config, rank, world):
