@@ -18,7 +18,8 @@
 extern "C" {
 #endif
 
-#define TBLAEQ_ABI_VERSION 1
+/* 2: tblaeq_serve_config gained `levels` (and tblaeq_serve_poll_levels was added). */
+#define TBLAEQ_ABI_VERSION 2
 
 typedef struct tblaeq_handle tblaeq_handle; /* QueryHandler: host index + device state */
 

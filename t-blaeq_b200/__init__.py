@@ -25,6 +25,7 @@ import numpy as np
 _HERE = os.path.dirname(os.path.abspath(__file__))
 # TBLAEQ_LIBRARY selects another build of the same library (e.g. a differently tuned one).
 LIB_PATH = os.environ.get("TBLAEQ_LIBRARY") or os.path.join(_HERE, "libtblaeq_b200.so")
+ABI_VERSION = 2  # TBLAEQ_ABI_VERSION of include/tblaeq.h this binding is written against
 HEADER_PATH = os.path.join(os.path.dirname(_HERE), "include", "tblaeq.h")
 
 
@@ -188,6 +189,9 @@ def _load():
         f = getattr(lib, name)
         f.argtypes = args
         f.restype = res
+    if lib.tblaeq_abi_version() != ABI_VERSION:
+        raise ImportError(f"{LIB_PATH} has C ABI version {lib.tblaeq_abi_version()}, this binding expects "
+                          f"{ABI_VERSION}; rebuild it (make -C t-blaeq_b200)")
     _lib = lib
     return lib
 

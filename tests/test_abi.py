@@ -23,7 +23,7 @@ def test_every_declared_symbol_is_exported(tb):
 
 
 def test_abi_version(tb):
-    assert tb.lib().tblaeq_abi_version() == 1
+    assert tb.lib().tblaeq_abi_version() == tb.ABI_VERSION == 2
 
 
 def test_null_arguments_are_rejected(tb):
