@@ -26,6 +26,24 @@ def test_abi_version(tb):
     assert tb.lib().tblaeq_abi_version() == tb.ABI_VERSION == 2
 
 
+def test_header_is_plain_c_and_links(tb, tmp_path):
+    """A C caller (the reference's cgo/ctypes-style bindings see the same thing): the header compiles
+    as strict C99, and a program linked against the library agrees on the ABI version."""
+    import shutil
+    import subprocess
+    if shutil.which("gcc") is None:
+        pytest.skip("no C compiler")
+    src = tmp_path / "abi.c"
+    src.write_text('#include "tblaeq.h"\n'
+                   "int main(void) { return tblaeq_abi_version() == TBLAEQ_ABI_VERSION ? 0 : 1; }\n")
+    exe = tmp_path / "abi"
+    lib_dir = os.path.dirname(tb.LIB_PATH)
+    subprocess.run(["gcc", "-std=c99", "-Wall", "-Wextra", "-pedantic", "-Werror",
+                    "-I", os.path.dirname(tb.HEADER_PATH), str(src), "-o", str(exe),
+                    "-L", lib_dir, "-l:" + os.path.basename(tb.LIB_PATH), "-Wl,-rpath," + lib_dir], check=True)
+    assert subprocess.run([str(exe)]).returncode == 0
+
+
 def test_null_arguments_are_rejected(tb):
     lib = tb.lib()
     assert lib.tblaeq_open(None, None) == 1
