@@ -42,6 +42,15 @@ def _package():
     return mod
 
 
+def _workloads():
+    """t-blaeq_b200/workloads.py on its own (it needs numpy only), without the package around it."""
+    spec = importlib.util.spec_from_file_location("tblaeq_workloads", os.path.join(REPO, "t-blaeq_b200",
+                                                                                   "workloads.py"))
+    mod = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mod)
+    return mod
+
+
 def _peaks():
     p = os.path.join(REPO, "MEASURED_PEAKS.json")
     if os.path.exists(p):
@@ -168,6 +177,121 @@ def cpu_port_qps(oracle, oidx, sub, Q, budget_s=20.0, min_q=32):
     return done / elapsed, threads, done
 
 
+class OracleWorkloadView:
+    """The two calls the workload generators make on a handle (info, decode_points), answered from
+    the oracle's own reading of an index directory: the same boxes and points as the product arm
+    (both decode the same files, one rounded multiply per level), without loading the product."""
+
+    def __init__(self, oracle, oidx):
+        self.oidx = oidx
+        self.pts, self.ids = oracle.decoded_points(oidx)
+
+    def info(self):
+        return {"N": int(self.pts.shape[0]), "D": int(self.oidx.D), "height": int(self.oidx.height)}
+
+    def decode_points(self, positions):
+        p = np.asarray(positions, dtype=np.int64)
+        return self.pts[p], self.ids[p]
+
+
+def cpu_brute_qps(oracle, pts, ids, qtype, queries, K=0, budget_s=15.0, first=16):
+    """The FP64 brute-force scan (oracle.brute_query: every decoded point against every query, OpenMP
+    over points on all host cores) timed over a bounded prefix of the workload: `first` queries, then
+    doubled while the budget lasts. Returns (queries/s, cores, queries timed, their results)."""
+    threads = os.cpu_count() or 1
+    n, done, elapsed, res = min(first, len(queries)), 0, 0.0, None
+    while done < len(queries):
+        t0 = time.perf_counter()
+        r = oracle.brute_query(pts, ids, qtype, queries[done:done + n], K=K, threads=threads)
+        elapsed += time.perf_counter() - t0
+        if res is None:
+            res = (done, r)  # the first block's results (checked against the GPU's)
+        done += n
+        if elapsed * 3 > budget_s:
+            break
+        n = min(len(queries) - done, 2 * n)
+    return done / elapsed, threads, done, res[1]
+
+
+def knn_k(nq):
+    """K of the batched-KNN workload: 20 for even queries, 100 for odd ones."""
+    return np.where(np.arange(nq) % 2 == 0, 20, 100).astype(np.uint32)
+
+
+def knn_legs(tb, h, P, K, steps, warmup, flush, n_plain=64):
+    """Exact KNN over one index: the batched traversal with the learned ranking (timed steps), the
+    same with the lower-bound ranking and with a one-pass finest level (one step each), one query at
+    a time with the lower-bound ranking and the scorer off (the plain traversal), and the learned
+    batch end to end through the host-buffer entry point. Each batch is one synchronous C-ABI call,
+    timed on the host with the device synchronised on both sides (L2 flushed before each step)."""
+    import torch
+    nq, D = P.shape
+    dP = torch.from_numpy(P).cuda()
+
+    def batch_leg(two_wave, learned, n_steps, n_warm):
+        h.set_two_wave(two_wave)
+        h.scorer_enable(learned)
+        for _ in range(max(1, n_warm)):  # the first batch sizes every workspace
+            h.query_batch(tb.QueryType.POINT, dP, tb.Mode.EXACT, K=K)
+        ts = []
+        for _ in range(n_steps):
+            flush.zero_()
+            torch.cuda.synchronize()
+            t1 = time.perf_counter()
+            h.query_batch(tb.QueryType.POINT, dP, tb.Mode.EXACT, K=K)
+            torch.cuda.synchronize()
+            ts.append(time.perf_counter() - t1)
+        c = h.knn_counters()
+        return nq * n_steps / sum(ts), c["rows"] / nq, ts
+
+    learned_qps, learned_rows, step_s = batch_leg(True, True, steps, warmup)
+    r = h.query_batch(tb.QueryType.POINT, dP, tb.Mode.EXACT, K=K)
+    result = (r.offsets.numpy().copy(), r.ids.numpy().copy(), r.dist2.numpy().copy())
+    lb_qps, lb_rows, _ = batch_leg(True, False, 1, 1)
+    one_qps, one_rows, _ = batch_leg(False, False, 1, 1)
+
+    # The plain traversal: one query at a time, lower-bound ranking, scorer off.
+    h.set_two_wave(True)
+    h.scorer_enable(False)
+    n_plain = min(n_plain, nq)
+    for i in range(8):
+        h.query_batch(tb.QueryType.POINT, dP[i:i + 1], tb.Mode.EXACT, K=K[i:i + 1])
+    lat = []
+    for i in range(n_plain):
+        torch.cuda.synchronize()
+        t1 = time.perf_counter()
+        h.query_batch(tb.QueryType.POINT, dP[i:i + 1], tb.Mode.EXACT, K=K[i:i + 1])
+        torch.cuda.synchronize()
+        lat.append(time.perf_counter() - t1)
+    plain_qps = n_plain / sum(lat)
+
+    # End to end: host points in, offsets + ids + squared distances out (learned ranking).
+    h.set_two_wave(True)
+    h.scorer_enable(True)
+    e2e_t, tot = [], 0
+    for _ in range(max(1, steps)):
+        t1 = time.perf_counter()
+        offs, ids_h, d2 = h.query_batch_host(tb.QueryType.POINT, P, tb.Mode.EXACT, K=K, ids_cap=int(K.sum()))
+        e2e_t.append(time.perf_counter() - t1)
+        tot = len(ids_h)
+    pl = sorted(x * 1e3 for x in lat)
+    st = sorted(x * 1e3 for x in step_s)
+    return {
+        "value": learned_qps, "unit": "queries/s", "steps": len(step_s),
+        "ms_per_step": statistics.mean(step_s) * 1e3,
+        "latency_ms": {"batch_p50": st[len(st) // 2], "batch_p99": st[min(len(st) - 1, int(len(st) * 0.99))],
+                       "plain_query_p50": pl[len(pl) // 2], "plain_query_p99": pl[min(len(pl) - 1, int(len(pl) * 0.99))]},
+        "e2e": {"value": nq * len(e2e_t) / sum(e2e_t), "unit": "queries/s",
+                "h2d_bytes_per_step": nq * D * 8 + nq * 4, "d2h_bytes_per_step": (nq + 1) * 8 + tot * 16},
+        "ranking": {"learned": {"qps": learned_qps, "rows_per_query": learned_rows},
+                    "lower_bound": {"qps": lb_qps, "rows_per_query": lb_rows},
+                    "one_pass": {"qps": one_qps, "rows_per_query": one_rows}},
+        "plain": {"value": plain_qps, "unit": "queries/s", "queries": n_plain,
+                  "kind": "one query at a time, lower-bound ranking, scorer off",
+                  "speedup_batched_learned_vs_plain": learned_qps / plain_qps},
+    }, result
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -180,6 +304,9 @@ def main():
     ap.add_argument("--train-queries", type=int, default=2048, help="knn: separately seeded scorer training queries")
     ap.add_argument("--nq", type=int, default=4096)
     ap.add_argument("--plain-queries", type=int, default=512)
+    ap.add_argument("--knn-queries", type=int, default=4096, help="batched: points of the KNN leg")
+    ap.add_argument("--knn-steps", type=int, default=10, help="batched: timed steps of the KNN leg")
+    ap.add_argument("--no-knn", action="store_true", help="batched: skip the KNN leg")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-graph", action="store_true")
     ap.add_argument("--policy", default="L0",
@@ -192,8 +319,11 @@ def main():
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
 
-    tb = _package()
-    wl = sys.modules.get("tblaeq_b200.workloads") or __import__("tblaeq_b200.workloads").workloads
+    if args.impl == "reference":
+        tb, wl = None, _workloads()  # the reference arm never imports the product package
+    else:
+        tb = _package()
+        wl = sys.modules.get("tblaeq_b200.workloads") or __import__("tblaeq_b200.workloads").workloads
     cfg_name = args.config
     if cfg_name == "build":
         return run_build(args, tb, rank, world, local)
@@ -214,7 +344,7 @@ def main():
     if cfg_name == "serving":
         return run_serving(args, tb, wl, rank, world, local)
     if args.impl == "reference":
-        return run_reference(args, tb, wl, cfg_name, config, rank, world)
+        return run_reference(args, wl, cfg_name, config, rank, world)
 
     import torch
     import torch.distributed as dist
@@ -323,16 +453,58 @@ def main():
     e2e_total = max_over_ranks(sum(e2e_t))
     e2e_value = job_throughput(args.nq * args.steps, world, e2e_total)
 
-    cpu = None
+    # The batched-plus-learned KNN leg on the same index (north-star target: batched + learned
+    # exact queries against the plain one-query-at-a-time traversal, at N = 10M, D = 8).
+    knn, knn_result, Pk, Kk = None, None, None, None
+    if cfg_name == "batched" and not args.no_knn:
+        Pk = wl.knn_points(h, args.knn_queries, seed=1234, noise=0.02)
+        Kk = knn_k(args.knn_queries)
+        T = wl.knn_points(h, 2048, seed=4321, noise=0.02)
+        t0 = time.perf_counter()
+        losses = h.scorer_train(T, K=knn_k(2048), max_samples=200000, epochs=8, lr=3e-3, seed=9)
+        train_s = time.perf_counter() - t0
+        with ClockSampler(local) as kclk:
+            knn, knn_result = knn_legs(tb, h, Pk, Kk, args.knn_steps, args.warmup, flush)
+        knn["value"] = knn["value"] * world
+        knn["config"] = {"workload": f"knn on the same index: {args.knn_queries} points (data + N(0,(2% extent)^2)), "
+                                     "K=20 and K=100 alternating", "queries_per_step": args.knn_queries}
+        knn["scorer"] = {"train_queries": 2048, "train_s": train_s, "epoch_loss": losses, **h.scorer_stats()}
+        knn["clocks"] = kclk.summary()
+
+    cpu, port, agreement = None, None, None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         sys.path.insert(0, REPO)
         import oracle
+        pts, pids = h.decode_points(np.arange(h.info()["N"], dtype=np.uint64))
+        qps, cores, sampled, bres = cpu_brute_qps(oracle, pts, pids, oracle.RANGE, Q)
+        cpu = {"value": qps, "unit": "queries/s", "cores": cores, "kind": "port",
+               "sample": f"first {sampled} of the {args.nq} boxes, FP64 brute-force scan of all {len(pts)} "
+                         f"decoded points (lo <= x <= hi), OpenMP over points"}
+        # The scan's results are the exact answers: the batched GPU results must equal them.
+        n_chk = len(bres.offsets) - 1
+        r = h.query_batch(tb.QueryType.RANGE, Q[:n_chk], tb.Mode.EXACT)
+        go, gi = r.offsets.numpy(), r.ids.numpy()
+        same = bool(np.array_equal(go, bres.offsets)) and all(
+            np.array_equal(np.sort(gi[go[q]:go[q + 1]]), bres.query(q)) for q in range(n_chk))
+        agreement = {"range": {"queries": n_chk, "identical_to_fp64_brute_force": same}}
         oidx = oracle_index_from_handler(oracle, h)
         sub = oracle.subtree(oidx)
-        qps, cores, sampled = cpu_port_qps(oracle, oidx, sub, Q)
-        cpu = {"value": qps, "unit": "queries/s", "cores": cores, "kind": "port",
-               "sample": f"first {sampled} of the {args.nq} boxes, exact traversal port (subtree radii + "
-                         f"final filter), OpenMP over queries"}
+        pqps, pcores, psampled = cpu_port_qps(oracle, oidx, sub, Q)
+        port = {"value": pqps, "unit": "queries/s", "cores": pcores, "kind": "port",
+                "sample": f"first {psampled} of the {args.nq} boxes, exact traversal port (subtree radii + "
+                          f"final filter), OpenMP over queries"}
+        if knn is not None:
+            kq, kcores, ksampled, kres = cpu_brute_qps(oracle, pts, pids, oracle.KNN, Pk[:64][Kk[:64] == 20], K=20,
+                                                       budget_s=8.0, first=8)
+            knn["cpu_baseline"] = {"value": kq, "unit": "queries/s", "cores": kcores, "kind": "port",
+                                   "sample": f"{ksampled} of the K=20 points, FP64 brute-force scan of all points"}
+            ko, ki, kd = knn_result
+            sel = np.nonzero(Kk[:64] == 20)[0][:len(kres.offsets) - 1]
+            ok = all(np.array_equal(ki[ko[q]:ko[q + 1]], kres.query(j)) and
+                     np.array_equal(kd[ko[q]:ko[q + 1]], kres.dist2[kres.offsets[j]:kres.offsets[j + 1]])
+                     for j, q in enumerate(sel))
+            agreement["knn"] = {"queries": len(sel), "identical_to_fp64_brute_force": bool(ok)}
+        del pts, pids
 
     if world > 1:
         dist.destroy_process_group()
@@ -378,7 +550,17 @@ def main():
                      "launch_ms": final_mean_s * 1e3},
         "clocks": clk.summary(),
         "cpu_baseline": cpu,
+        "cpu_traversal_port": port,
+        "agreement": agreement,
     }
+    if knn is not None:
+        out["knn"] = knn
+        out["target"] = {
+            "workload": "N=10M, D=8 (one index): 4096 range boxes and 4096 KNN points",
+            "range_batched_vs_plain": value / world / plain_qps,
+            "knn_batched_learned_vs_plain": knn["plain"]["speedup_batched_learned_vs_plain"],
+            "finest_level_hbm_frac": None if finest_streamed else achieved / peak,
+            "needs": ">= 5x batched+learned vs plain, >= 0.60 of HBM in pruning/SpTSpM"}
     print(json.dumps(out))
 
 
@@ -394,9 +576,8 @@ def knn_workload(tb, wl, nq, seed):
 def run_knn(args, tb, wl, rank, world, local):
     """Batched exact KNN (N=50M, D=16, 4096 queries, K in {20, 100}) with the learned frontier
     ranking, beside the lower-bound ranking, the one-pass finest level and one query at a time.
-    Each step is one synchronous batch through the C ABI (a batch this large runs as several
-    traversals, split by the library); it is timed on the host around the call, synchronised on
-    both sides. Replicas only for N > 1."""
+    Each step is one synchronous batch through the C ABI, timed on the host around the call,
+    synchronised on both sides. Replicas only for N > 1."""
     cfg = wl.CONFIGS["knn"]
     config = {"workload": f"knn: RandomKmeans N={cfg['N']} D={cfg['D']} ratios "
                           f"{','.join(map(str, cfg['ratios']))} seed {cfg['seed']} sigma/{cfg['sigma_divisor']}; "
@@ -404,29 +585,30 @@ def run_knn(args, tb, wl, rank, world, local):
               "index_points": cfg["N"], "dim": cfg["D"], "queries_per_step": args.nq, "mode": "exact",
               "l2": "inputs larger than L2 (6.4 GB of rows per step)", "parallelism": f"replicas{world}"}
     steps = args.steps if args.steps != 200 else 3
+    metric = "exact-result KNN queries/s (batched + learned ranking, 1 B200 per rank)"
     if args.impl == "reference":
         if rank != 0:
             return
         sys.path.insert(0, REPO)
         import oracle
-        h, P, K = knn_workload(tb, wl, args.nq, seed=1234)
-        pts, ids = h.decode_points(np.arange(cfg["N"], dtype=np.uint64))
+        view, _ = reference_index(oracle, "knn")
+        P = wl.knn_points(view, args.nq, seed=1234, noise=0.02)
+        K = knn_k(args.nq)
+        per, t = 4, 0.0
         threads = os.cpu_count() or 1
-        per = 4
-        t = 0.0
         for s in range(steps):
             sl = slice((s * per) % args.nq, (s * per) % args.nq + per)
             t0 = time.perf_counter()
             for kv in (20, 100):
                 m = K[sl] == kv
                 if m.any():
-                    oracle.brute_query(pts, ids, oracle.KNN, P[sl][m], K=kv, threads=threads)
+                    oracle.brute_query(view.pts, view.ids, oracle.KNN, P[sl][m], K=kv, threads=threads)
             t += time.perf_counter() - t0
         v = per * steps / t
-        print(json.dumps({"metric": "exact-result KNN queries/s (batched + learned ranking, 1 B200 per rank)",
-                          "value": v, "unit": "queries/s", "impl": "reference", "n_gpus": world, "steps": steps,
-                          "warmup": 0, "ms_per_step": t / steps * 1e3, "higher_is_better": True, "scaling": "weak",
-                          "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": config,
+        print(json.dumps({"metric": metric, "value": v, "unit": "queries/s", "impl": "reference", "n_gpus": world,
+                          "steps": steps, "warmup": 0, "ms_per_step": t / steps * 1e3, "higher_is_better": True,
+                          "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+                          "config": config,
                           "cpu_baseline": {"value": v, "unit": "queries/s", "cores": threads, "kind": "port",
                                            "sample": f"{per} points per step, FP64 brute force over all {cfg['N']} "
                                                      f"points (the reference's KNN is approximate; exact needs a scan)"},
@@ -437,65 +619,16 @@ def run_knn(args, tb, wl, rank, world, local):
     tb.set_device(local)
     h, P, K = knn_workload(tb, wl, args.nq, seed=1234)
     h.prepare_for_query(tb.LevelPolicy.L0)
-    D = cfg["D"]
-    dP = torch.from_numpy(P).cuda()
     flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
 
     # Scorer: trained on traces of separately seeded queries (up to 200,000 samples).
     T = wl.knn_points(h, args.train_queries, seed=4321, noise=0.02)
-    KT = np.where(np.arange(args.train_queries) % 2 == 0, 20, 100).astype(np.uint32)
     t0 = time.perf_counter()
-    losses = h.scorer_train(T, K=KT, max_samples=200000, epochs=8, lr=3e-3, seed=9)
+    losses = h.scorer_train(T, K=knn_k(args.train_queries), max_samples=200000, epochs=8, lr=3e-3, seed=9)
     train_s = time.perf_counter() - t0
     stats = h.scorer_stats()
-
-    def leg(two_wave, learned, n_steps, n_warm=1):
-        h.set_two_wave(two_wave)
-        h.scorer_enable(learned)
-        for _ in range(max(1, n_warm)):  # the first batch sizes every workspace
-            h.query_batch(tb.QueryType.POINT, dP, tb.Mode.EXACT, K=K)
-        ts = []
-        if learned:
-            torch.cuda.nvtx.range_push("timed")  # profilers select the timed steps by this range
-        for _ in range(n_steps):
-            flush.zero_()
-            torch.cuda.synchronize()
-            t1 = time.perf_counter()
-            h.query_batch(tb.QueryType.POINT, dP, tb.Mode.EXACT, K=K)
-            torch.cuda.synchronize()
-            ts.append(time.perf_counter() - t1)
-        if learned:
-            torch.cuda.nvtx.range_pop()
-        c = h.knn_counters()
-        return args.nq * n_steps / sum(ts), c["rows"] / args.nq, ts
-
     with ClockSampler(local) as clk:
-        learned_qps, learned_rows, step_s = leg(True, True, steps, args.warmup)
-    lb_qps, lb_rows, _ = leg(True, False, 1)
-    one_qps, one_rows, _ = leg(False, False, 1)
-
-    # End to end: host points in, offsets + ids + distances out (learned ranking).
-    h.set_two_wave(True)
-    h.scorer_enable(True)
-    e2e_t = []
-    tot = 0
-    for _ in range(steps):
-        t1 = time.perf_counter()
-        offs, ids_h, d2 = h.query_batch_host(tb.QueryType.POINT, P, tb.Mode.EXACT, K=K, ids_cap=int(K.sum()))
-        e2e_t.append(time.perf_counter() - t1)
-        tot = len(ids_h)
-    e2e_value = args.nq * steps / sum(e2e_t)
-
-    # Plain: one query at a time through the same engine (learned ranking on).
-    n_plain = min(args.plain_queries, 32)
-    lat = []
-    for i in range(n_plain):
-        torch.cuda.synchronize()
-        t1 = time.perf_counter()
-        h.query_batch(tb.QueryType.POINT, dP[i:i + 1], tb.Mode.EXACT, K=K[i:i + 1])
-        torch.cuda.synchronize()
-        lat.append(time.perf_counter() - t1)
-    plain_qps = n_plain / sum(lat)
+        leg, (ko, ki, kd) = knn_legs(tb, h, P, K, steps, args.warmup, flush, n_plain=min(args.plain_queries, 32))
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -510,23 +643,13 @@ def run_knn(args, tb, wl, rank, world, local):
                "sample": "the first 4 points, FP64 brute force over all points, OpenMP over points"}
     if rank != 0:
         return
-    pl = sorted(x * 1e3 for x in lat)
-    value = learned_qps * world
     print(json.dumps({
-        "metric": "exact-result KNN queries/s (batched + learned ranking, 1 B200 per rank)",
-        "value": value, "unit": "queries/s", "n_gpus": world, "steps": steps, "warmup": max(1, args.warmup),
-        "ms_per_step": statistics.mean(step_s) * 1e3, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded RandomKmeans-style index and points)",
-        "config": config,
-        "e2e": {"value": e2e_value, "unit": "queries/s", "h2d_bytes_per_step": args.nq * D * 8 + args.nq * 4,
-                "d2h_bytes_per_step": (args.nq + 1) * 8 + tot * 16},
-        "gpu_launches": None,
-        "ranking": {"learned": {"qps": learned_qps, "rows_per_query": learned_rows},
-                    "lower_bound": {"qps": lb_qps, "rows_per_query": lb_rows},
-                    "one_pass": {"qps": one_qps, "rows_per_query": one_rows}},
-        "plain": {"value": plain_qps, "unit": "queries/s", "queries": n_plain,
-                  "speedup_batched_vs_plain": learned_qps / plain_qps,
-                  "latency_ms_p50": pl[len(pl) // 2], "latency_ms_p99": pl[min(len(pl) - 1, int(len(pl) * 0.99))]},
+        "metric": metric, "value": leg["value"] * world, "unit": "queries/s", "n_gpus": world, "steps": steps,
+        "warmup": max(1, args.warmup), "ms_per_step": leg["ms_per_step"], "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (seeded RandomKmeans-style index and points)", "config": config,
+        "e2e": leg["e2e"], "gpu_launches": None, "latency_ms": leg["latency_ms"], "ranking": leg["ranking"],
+        "plain": leg["plain"],
         "scorer": {"train_queries": args.train_queries, "samples": stats["samples"], "positives": stats["positives"],
                    "train_s": train_s, "epoch_loss": losses},
         "clocks": clk.summary(),
@@ -693,31 +816,57 @@ def run_build(args, tb, rank, world, local):
         "clocks": clk.summary()}))
 
 
-def reference_cuda_range(tb, h, Q, D, n):
+def write_query_file(path, rows, D):
+    """The reference's query-file format (src/Data_Structures/File.cu:159-205): a header "n D", then
+    one row per query (2D values lo|hi for range, D values for a point), %.17g so values round-trip."""
+    with open(path, "w") as f:
+        f.write(f"{rows.shape[0]} {D}\n")
+        for r in np.asarray(rows, dtype=np.float64):
+            f.write(" ".join("%.17g" % v for v in r) + "\n")
+
+
+def reference_cuda(idx_dir, Q, D, kind, K=0, timeout=1800):
     """The reference's own CUDA build (oracle/_ref/ref_harness: the reference's
-    QueryHandler::performSingleRangeQuery with saveFineMesh=true under policy L0) on this GPU, one
-    query at a time, timed by its per-query timer; like its CLI (QueryEngine.cu:216-227) the mean
-    drops the fastest and the slowest query. It returns the reference's candidate sets: every point
-    of every surviving cluster, without the exact final filter."""
+    QueryHandler::performSingleRangeQuery / performSingleKNNQuery with saveFineMesh=true under policy
+    L0) on this GPU, one query at a time, timed by its per-query timer; like its CLI
+    (QueryEngine.cu:216-227) the mean drops the fastest and the slowest query. It returns the
+    reference's candidate sets: every point of every surviving cluster, without an exact final
+    filter or top-K."""
     harness = os.path.join(REPO, "oracle", "_ref", "ref_harness")
     if not os.path.exists(harness):
         return {"unavailable": "the reference build (oracle/_ref) is not present"}
     import tempfile
     with tempfile.TemporaryDirectory() as d:
-        idx = os.path.join(d, "idx")
-        h.save_index(idx)
         qf = os.path.join(d, "q.txt")
-        tb.save_query_file(qf, tb.QueryType.RANGE, Q[:n], D)
+        write_query_file(qf, Q, D)
         out = os.path.join(d, "ref.bin")
-        subprocess.run([harness, idx, qf, "0", "0", "L0", out], check=True, timeout=1800,
-                       stdout=subprocess.DEVNULL)
+        subprocess.run([harness, idx_dir, qf, "1" if kind == "knn" else "0", str(K), "L0", out], check=True,
+                       timeout=timeout, stdout=subprocess.DEVNULL)
         us, cands = read_harness_times(open(out, "rb").read())
     t = sorted(us)
     mean = reference_mean_us(us)
     return {"value": 1e6 / mean, "unit": "queries/s", "queries": len(us), "mean_us": mean,
             "p50_us": t[len(t) // 2], "candidates": cands,
-            "kind": "reference CUDA build on this GPU, one query at a time, policy L0",
+            "kind": f"reference CUDA build on this GPU, one {kind} query at a time, policy L0"
+                    + (f", K={K}" if kind == "knn" else ""),
             "results": "the reference's candidate sets (no exact final filter)"}
+
+
+def reference_index(oracle, wl, cfg_name):
+    """The configuration's index as the reference's own generator writes it (oracle/_ref/T-BLAEQ
+    --gen-index, default value range [1, 100]) in a temporary directory, read back by the oracle's
+    reader: (workload view, directory). Neither step loads the product library."""
+    import tempfile
+    cfg = wl.CONFIGS[cfg_name]
+    binary = os.path.join(REPO, "oracle", "_ref", "T-BLAEQ")
+    if not os.path.exists(binary):
+        raise FileNotFoundError("the reference build (oracle/_ref/T-BLAEQ) is not present")
+    d = tempfile.mkdtemp(prefix="tblaeq_ref_idx_")
+    subprocess.run([binary, "--gen-index", "-i", d, "--gen-N", str(cfg["N"]), "--gen-D", str(cfg["D"]),
+                    "--height", str(len(cfg["ratios"]) + 1), "--ratios", ",".join(map(str, cfg["ratios"])),
+                    "--gen-seed", str(cfg["seed"]), "--gen-sigma-divisor", str(cfg["sigma_divisor"])],
+                   check=True, stdout=subprocess.DEVNULL, timeout=1800)
+    return OracleWorkloadView(oracle, oracle.load_index(d)), d
 
 
 def read_harness_times(raw: bytes):
@@ -746,47 +895,75 @@ def reference_mean_us(us):
     return sum(kept) / len(kept)
 
 
-def run_reference(args, tb, wl, cfg_name, config, rank, world):
+def run_reference(args, wl, cfg_name, config, rank, world):
     """Reference arm: the CPU restatement of the reference traversal (exact semantics) timed on the
-    host cores. The reference has no CPU implementation of its query path (every strategy launches
-    CUDA kernels), so the oracle port stands in for it; the reference's own CUDA build, timed one
-    query at a time on the same GPU, is reported beside it."""
+    host cores over whole steps of the workload. The reference has no CPU implementation of its
+    query path (every strategy launches CUDA kernels), so the oracle port stands in for it. The
+    index comes from the reference's own generator and the oracle's reader, so this process never
+    loads the product library. Beside it: the reference's own CUDA build, one query at a time on the
+    same GPU (range, and KNN with K=20 and K=100), and the FP64 brute-force scan."""
     if rank != 0:
         return
+    import shutil
     sys.path.insert(0, REPO)
     import oracle
-    h = wl.generate_index(tb.QueryHandler, cfg_name)
-    boxes_kw = dict(half_width=0.05) if cfg_name == "small" else dict(log_uniform=(0.001, 0.1))
-    Q = wl.range_boxes(h, args.nq, seed=42, **boxes_kw)
-    oidx = oracle_index_from_handler(oracle, h)
-    sub = oracle.subtree(oidx)
-    threads = os.cpu_count() or 1
-    per_step = max(8, min(args.nq, 64))
-    for i in range(args.warmup):
-        oracle.exact_query(oidx, oracle.RANGE, Q[:per_step], sub=sub, threads=threads)
-    t = 0.0
-    done = 0
-    for s in range(args.steps):
-        sl = Q[(s * per_step) % args.nq:(s * per_step) % args.nq + per_step]
-        t0 = time.perf_counter()
-        oracle.exact_query(oidx, oracle.RANGE, sl, sub=sub, threads=threads)
-        t += time.perf_counter() - t0
-        done += len(sl)
-    v = done / t
-    out = {"metric": "exact-result range queries/s (batched, 1 B200 per rank)", "value": v, "unit": "queries/s",
-           "impl": "reference", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
-           "ms_per_step": t / args.steps * 1e3, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-           "dtype": "f64", "data": "synthetic (seeded RandomKmeans-style index and boxes)", "config": config,
-           "cpu_baseline": {"value": v, "unit": "queries/s", "cores": threads, "kind": "port",
-                            "sample": f"{per_step} boxes per step of the {args.nq}-box workload, exact traversal "
-                                      f"port, OpenMP over queries"},
-           "e2e": {"value": v, "unit": "queries/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
-    # Beside it: the reference's own implementation, which runs on the GPU only.
+    metric = "exact-result range queries/s (batched, 1 B200 per rank)"
     try:
-        out["reference_cuda_b200"] = reference_cuda_range(tb, h, Q, h.info()["D"], min(args.nq, 256))
-    except Exception as e:  # reported, never fatal to the CPU arm
-        out["reference_cuda_b200"] = {"unavailable": f"{type(e).__name__}: {e}"[:200]}
-    print(json.dumps(out))
+        view, idx_dir = reference_index(oracle, wl, cfg_name)
+    except Exception as e:
+        print(json.dumps({"impl": "reference", "metric": metric, "unavailable": f"{type(e).__name__}: {e}"[:200]}))
+        return
+    try:
+        oidx = view.oidx
+        D = oidx.D
+        boxes_kw = dict(half_width=0.05) if cfg_name == "small" else dict(log_uniform=(0.001, 0.1))
+        Q = wl.range_boxes(view, args.nq, seed=42, **boxes_kw)
+        sub = oracle.subtree(oidx)
+        threads = os.cpu_count() or 1
+        # Each step is the whole workload (all nq boxes), like the product arm's step.
+        oracle.exact_query(oidx, oracle.RANGE, Q, sub=sub, threads=threads)  # untimed: first touch
+        steps, t = 0, 0.0
+        for s in range(max(1, args.steps)):
+            t0 = time.perf_counter()
+            oracle.exact_query(oidx, oracle.RANGE, Q, sub=sub, threads=threads)
+            t += time.perf_counter() - t0
+            steps += 1
+            if t > 60.0:  # bounded: a slow host ends the arm after about a minute of timed work
+                break
+        v = args.nq * steps / t
+        out = {"metric": metric, "value": v, "unit": "queries/s",
+               "impl": "reference", "n_gpus": world, "steps": steps, "warmup": 1, "ms_per_step": t / steps * 1e3,
+               "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+               "data": "synthetic (seeded RandomKmeans-style index written by the reference's --gen-index; boxes)",
+               "config": config,
+               "cpu_baseline": {"value": v, "unit": "queries/s", "cores": threads, "kind": "port",
+                                "sample": f"all {args.nq} boxes per step ({steps} steps), exact traversal port, "
+                                          f"OpenMP over queries"},
+               "e2e": {"value": v, "unit": "queries/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+        bq, bcores, bn, _ = cpu_brute_qps(oracle, view.pts, view.ids, oracle.RANGE, Q)
+        out["cpu_brute_force"] = {"value": bq, "unit": "queries/s", "cores": bcores,
+                                  "sample": f"first {bn} boxes, FP64 brute-force scan of all decoded points"}
+        # The reference's own implementation runs on the GPU only.
+        try:
+            out["reference_cuda_b200"] = reference_cuda(idx_dir, Q[:min(args.nq, 256)], D, "range")
+        except Exception as e:  # reported, never fatal to the CPU arm
+            out["reference_cuda_b200"] = {"unavailable": f"{type(e).__name__}: {e}"[:200]}
+        if cfg_name == "batched" and not args.no_knn:
+            P = wl.knn_points(view, args.knn_queries, seed=1234, noise=0.02)
+            K = knn_k(args.knn_queries)
+            knn = {}
+            for kv in (20, 100):
+                try:
+                    knn[f"K{kv}"] = reference_cuda(idx_dir, P[:256][K[:256] == kv], D, "knn", K=kv)
+                except Exception as e:
+                    knn[f"K{kv}"] = {"unavailable": f"{type(e).__name__}: {e}"[:200]}
+            ok = [r["value"] for r in knn.values() if "value" in r]
+            if len(ok) == 2:  # the mix of the workload: half K=20, half K=100
+                knn["mixed"] = {"value": 2.0 / (1.0 / ok[0] + 1.0 / ok[1]), "unit": "queries/s"}
+            out["reference_cuda_b200_knn"] = knn
+        print(json.dumps(out))
+    finally:
+        shutil.rmtree(idx_dir, ignore_errors=True)
 
 
 if __name__ == "__main__":

@@ -282,6 +282,16 @@ uint64_t tblaeq_live_device_bytes(void);
 /* Test hook: make the n-th device allocation from now on fail (n = 0 disables). */
 void tblaeq_debug_fail_alloc_after(uint64_t n);
 
+/* Test hook for failure detection (no counterpart in the reference, whose kernels never wait on
+ * one another): from now on, range and per-level plugin traversals (tblaeq_query_batch of range
+ * queries, tblaeq_level, tblaeq_level_range_noalloc) leave work tile `withhold_tile` of every
+ * expand launch unpublished, and their look-back waits give up after `spin_limit` polls. The wait
+ * runs out, the kernel sets its timeout status and returns, later launches of the batch skip their
+ * work, and the call fails with TBLAEQ_ERR_TIMEOUT with the CUDA context intact. withhold_tile =
+ * UINT64_MAX or spin_limit = 0 switches the hook off. Process-wide; KNN batches are never affected;
+ * launches already captured in a CUDA graph keep the setting they were captured with. */
+void tblaeq_debug_lookback_timeout(uint64_t withhold_tile, uint64_t spin_limit);
+
 /* Test hook: treat traversal workspaces above `limit` frontier entries or work items as too large
  * (0 restores the 32-bit limit), so that small indexes exercise the chunked KNN batches. */
 int tblaeq_debug_split_above(tblaeq_handle* h, uint64_t limit);

@@ -164,6 +164,7 @@ def _load():
         "tblaeq_scorer_load": ([vp, ctypes.c_char_p], ctypes.c_int),
         "tblaeq_live_device_bytes": ([], ctypes.c_uint64),
         "tblaeq_debug_fail_alloc_after": ([ctypes.c_uint64], None),
+        "tblaeq_debug_lookback_timeout": ([ctypes.c_uint64, ctypes.c_uint64], None),
         "tblaeq_debug_split_above": ([vp, ctypes.c_uint64], ctypes.c_int),
         "tblaeq_kmeans_build": ([P(ctypes.c_float), ctypes.c_uint64, ctypes.c_uint64, ctypes.c_uint64,
                                  P(ctypes.c_uint64), P(_BuildConfig), P(vp), P(_BuildReport)], ctypes.c_int),

@@ -729,9 +729,15 @@ int tblaeq_decode_points(tblaeq_handle* h, const uint64_t* positions, uint64_t n
 int tblaeq_level_range_noalloc(tblaeq_handle* h, uint64_t l, const tblaeq_grid* in, const double* lo,
                                const double* hi, uint64_t* out_ids, double* out_vals, uint64_t out_cap,
                                uint64_t* out_n) {
-    if (int c = checkPrepared(h)) return c;
+    if (!h || !h->qh) return fail(TBLAEQ_ERR_INVALID, "null handle");
     if (!in || !lo || !hi || !out_n || (out_cap && (!out_ids || !out_vals)))
         return fail(TBLAEQ_ERR_INVALID, "null argument");
+    // A grid of another dimension would make the first expand read nnz * D doubles from a buffer
+    // holding nnz * dim: reject it before any launch (and before the state check), as tblaeq_level does.
+    if (in->dim != h->qh->index().D)
+        return fail(TBLAEQ_ERR_INVALID, "grid dimension mismatch: grid has " + std::to_string(in->dim) +
+                                            ", index has " + std::to_string(h->qh->index().D));
+    if (int c = checkPrepared(h)) return c;
     return guarded([&]() -> int {
         try {
             *out_n = runLevelRangeNoAlloc(h->qh->runtime(), l, in->ids, in->vals, in->nnz, lo, hi, out_ids, out_vals,
@@ -749,6 +755,12 @@ int tblaeq_debug_split_above(tblaeq_handle* h, uint64_t limit) {
     if (int c = checkPrepared(h)) return c;
     h->qh->runtime().engine->setSplitLimit(limit ? limit : 0xffffffffull);
     return TBLAEQ_OK;
+}
+
+void tblaeq_debug_lookback_timeout(uint64_t withhold_tile, uint64_t spin_limit) {
+    const bool off = withhold_tile >= 0xffffffffull || spin_limit == 0;
+    setLookbackTestHook(off ? 0xffffffffu : static_cast<uint32_t>(withhold_tile),
+                        off ? 0u : static_cast<uint32_t>(std::min<uint64_t>(spin_limit, 0xffffffffull)));
 }
 
 void tblaeq_debug_fail_alloc_after(uint64_t n) {

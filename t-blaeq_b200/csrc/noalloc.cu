@@ -15,6 +15,7 @@
 // The control words that must start at zero are cleared at the start of every call. Calls whose
 // work overlaps on the GPU (different streams or handles on the same device) race on the array;
 // callers must serialise them.
+#include <algorithm>
 #include <cstdint>
 #include <mutex>
 
@@ -153,8 +154,10 @@ uint64_t runLevelRangeNoAlloc(Runtime& rt, uint64_t l, const uint64_t* dIds, con
     TBLAEQ_CUDA(cudaStreamSynchronize(st));
     if (stWord & (kStatusLookbackTimeout | kStatusWindowOverflow))
         throw CudaError(cudaErrorLaunchTimeout, "traversal kernel reported status " + std::to_string(stWord));
+    // h[3]: children the survivors generate (what the caller's buffers must hold); h[4]: results
+    // written. When the first launch overflowed, the second returned early and h[4] is 0.
     if (h[3] > kNoAllocMaxOut) throw NoAllocOverflow(h[3]);
-    if (stWord) throw NoAllocOverflow(h[4]);
+    if (stWord) throw NoAllocOverflow(std::max(h[3], h[4]));
     return h[4];
 }
 

@@ -4,6 +4,7 @@
 #include <cuda/atomic>
 
 #include <algorithm>
+#include <atomic>
 
 namespace tblaeq {
 
@@ -32,7 +33,7 @@ __device__ __forceinline__ void storeDesc(unsigned long long* p, unsigned long l
 // Warp 0 of the tile: publish the tile aggregate, look back over predecessors and publish the
 // inclusive prefix. Returns the exclusive prefix (count, child sum) in lanes of warp 0.
 __device__ void lookback(unsigned long long* desc, uint32_t tile, uint32_t aggCnt, uint32_t aggSum,
-                         uint32_t* status, unsigned long long& exCnt, unsigned long long& exSum) {
+                         uint32_t* status, uint32_t spinLimit, unsigned long long& exCnt, unsigned long long& exSum) {
     const int lane = threadIdx.x & 31;
     exCnt = 0;
     exSum = 0;
@@ -51,7 +52,7 @@ __device__ void lookback(unsigned long long* desc, uint32_t tile, uint32_t aggCn
         const uint32_t xmask = __ballot_sync(0xffffffffu, flag == 0);
         const uint32_t needed = pmask ? ((pmask & (~pmask + 1)) << 1) - 1 : 0xffffffffu;  // lanes <= first P
         if (xmask & needed) {
-            if (++spins > kSpinLimit) {
+            if (++spins > spinLimit) {
                 if (lane == 0) atomicOr(status, kStatusLookbackTimeout);
                 break;
             }
@@ -563,6 +564,9 @@ __global__ void __launch_bounds__(kExpandThreads, expandMinBlocks<PRED>()) expan
                                                   ((S::kWindowBytes + 15) / 16) * 16);  // deferred items
     uint32_t* sKeep = reinterpret_cast<uint32_t*>(sList + kWarpTile);                   // [R] keep words
 
+    // A look-back that gave up earlier in this batch left its frontier inconsistent (prefixes
+    // computed without the tile it waited for): never read it; the host reports the status.
+    if (*a.scratch.status & (kStatusLookbackTimeout | kStatusWindowOverflow)) return;
     const uint32_t entries = a.in.hdr[0];
     const uint32_t total = a.in.hdr[1];
     const uint32_t nTiles = (total + kWarpTile - 1) / kWarpTile;
@@ -828,12 +832,14 @@ __global__ void __launch_bounds__(kExpandThreads, expandMinBlocks<PRED>()) expan
         // nothing writes nothing, so it needs no output position: it publishes its empty
         // aggregate and moves on without waiting for its predecessors (most tiles of the finest
         // levels); successors sum through it. The last tile still resolves the totals.
+        if (tile == a.withholdTile) continue;  // test hook: this tile never publishes
         if (aggCnt == 0 && aggSum == 0 && tile != nTiles - 1) {
             if (lane == 0) storeDesc(&a.scratch.desc[tile], packDesc(tile == 0 ? kFlagPrefix : kFlagAggregate, 0, 0));
             continue;
         }
         unsigned long long exCnt, exSum;
-        lookback(a.scratch.desc, tile, aggCnt, aggSum, a.scratch.status, exCnt, exSum);
+        lookback(a.scratch.desc, tile, aggCnt, aggSum, a.scratch.status, a.spinLimit ? a.spinLimit : kSpinLimit,
+                 exCnt, exSum);
         if (tile == nTiles - 1 && lane == 0) {
             const unsigned long long totC = exCnt + aggCnt;
             const unsigned long long totS = exSum + aggSum;
@@ -1049,7 +1055,25 @@ void dispatchStaged(const ExpandArgs& a, int pred, bool toResult, int g, cudaStr
 
 }  // namespace
 
-void launchExpand(const ExpandArgs& a, int pred, bool toResult, int gridBlocks, cudaStream_t stream) {
+namespace {
+std::atomic<uint32_t> gHookWithhold{0xffffffffu};
+std::atomic<uint32_t> gHookSpins{0};
+}  // namespace
+
+void setLookbackTestHook(uint32_t withholdTile, uint32_t spinLimit) {
+    const bool off = withholdTile == 0xffffffffu || spinLimit == 0;
+    gHookWithhold.store(off ? 0xffffffffu : withholdTile);
+    gHookSpins.store(off ? 0u : spinLimit);
+}
+
+void launchExpand(const ExpandArgs& in, int pred, bool toResult, int gridBlocks, cudaStream_t stream) {
+    ExpandArgs a = in;
+    a.withholdTile = 0xffffffffu;
+    a.spinLimit = 0;
+    if (pred != kPredKnnBound && pred != kPredKnnPoint) {
+        a.withholdTile = gHookWithhold.load();
+        a.spinLimit = gHookSpins.load();
+    }
     switch (a.D) {
         case 2: return dispatchStaged<2>(a, pred, toResult, gridBlocks, stream);
         case 3: return dispatchStaged<3>(a, pred, toResult, gridBlocks, stream);

@@ -139,12 +139,25 @@ struct ExpandArgs {
     int useFma;                 // accumulate squared distances with fma (reference kernels' contraction)
     int variant;                // Variant
     int wave;                   // 0: plain; 1 / 2: two-wave KNN final level (see ChildLevel)
+    // Failure-detection test hook (set by launchExpand from setLookbackTestHook for range and
+    // plugin launches only): tile `withholdTile` never publishes its counts, and look-back spins
+    // give up after `spinLimit` polls (0: the default limit).
+    uint32_t withholdTile;
+    uint32_t spinLimit;
 };
 
 // Launch the expand kernel for dimension D with the given predicate; `toResult` selects the
 // result output (final level) instead of the next frontier. gridBlocks <= 0 picks a persistent
 // grid sized from the occupancy of the instantiation.
 void launchExpand(const ExpandArgs& a, int pred, bool toResult, int gridBlocks, cudaStream_t stream);
+
+// Failure-detection test hook: from now on, every range or per-level plugin expand launch (not
+// KNN launches, whose later kernels read the frontier without the status check) leaves tile
+// `withholdTile` unpublished and bounds its look-back spins at `spinLimit` polls, so the batch ends
+// with kStatusLookbackTimeout instead of results. withholdTile = 0xffffffff (or spinLimit = 0)
+// restores normal operation. Process-wide; launches captured in a CUDA graph keep the values they
+// were captured with.
+void setLookbackTestHook(uint32_t withholdTile, uint32_t spinLimit);
 
 // Tile size (work items per tile) used by every expand instantiation.
 inline int expandTile(int) { return kWarpTile; }

@@ -130,3 +130,24 @@ def test_alloc_failure_hook_is_clean_on_cpu(tb):
     tb.lib().tblaeq_debug_fail_alloc_after(1)
     tb.lib().tblaeq_debug_fail_alloc_after(0)
     assert tb.lib().tblaeq_live_device_bytes() == 0
+
+
+def test_noalloc_rejects_a_grid_of_another_dimension(tb):
+    """tblaeq_level_range_noalloc checks the grid's dimension against the index before anything
+    else runs (a narrower grid would otherwise be read as nnz * D doubles): no GPU is needed."""
+    h = tb.QueryHandler.generate(2000, 3, 1.0, 100.0, False, 4, (10, 10, 10), 1, 3.0)
+    lib = tb.lib()
+    lib.tblaeq_level_range_noalloc.restype = ctypes.c_int
+    g = tb.Grid(1, 2, 1, None, None)  # dim 2 against D = 3
+    lo = (ctypes.c_double * 3)(0, 0, 0)
+    hi = (ctypes.c_double * 3)(1, 1, 1)
+    n = ctypes.c_uint64(7)
+    code = lib.tblaeq_level_range_noalloc(h._h, ctypes.c_uint64(0), ctypes.byref(g), lo, hi,
+                                          None, None, ctypes.c_uint64(0), ctypes.byref(n))
+    assert code == 1
+    assert b"dimension mismatch" in lib.tblaeq_last_error()
+    # The right dimension on an unprepared handle reaches the state check instead.
+    g.dim = 3
+    code = lib.tblaeq_level_range_noalloc(h._h, ctypes.c_uint64(0), ctypes.byref(g), lo, hi,
+                                          None, None, ctypes.c_uint64(0), ctypes.byref(n))
+    assert code == 7

@@ -1,0 +1,148 @@
+"""Parity at the benchmarked sizes, not only on small indexes.
+
+* Batched range (N = 10M, D = 8, ratios 100,50,20, seed 1, sigma/3; the 4096 log-uniform boxes of
+  the benchmark, seed 42): every box's exact result equals the FP64 brute-force scan of all decoded
+  points, bit-exact id sets; the graph-replayed asynchronous batch (the benchmark's timed path)
+  returns the same results; every returned coordinate lies inside its box. In ref-parity mode the
+  first 64 boxes return exactly the candidate sets of the reference's own CUDA build run on the same
+  index files (oracle/_ref/ref_harness).
+* The same index answers the benchmark's KNN leg (4096 points, K = 20 / 100, scorer on) exactly:
+  ids identical to the FP64 brute force and squared distances bit-identical.
+* Batched KNN (N = 50M, D = 16, ratios 100,50,20, seed 2, sigma/2.5; 64 points of the benchmark's
+  KNN workload, K = 20 and 100 alternating, learned ranking on): ids identical to the FP64 brute
+  force, squared distances within 1e-6 relative (and in fact bit-identical), and identical with the
+  learned ranking off.
+"""
+import os
+import subprocess
+
+import numpy as np
+import pytest
+
+from conftest import REPO, ids_by_query
+
+pytestmark = pytest.mark.gpu
+
+HARNESS = os.path.join(REPO, "oracle", "_ref", "ref_harness")
+
+
+def _knn_k(n):
+    return np.where(np.arange(n) % 2 == 0, 20, 100).astype(np.uint32)
+
+
+@pytest.fixture(scope="module")
+def batched(tb, wl, cuda):
+    h = wl.generate_index(tb.QueryHandler, "batched")
+    h.prepare_for_query(tb.LevelPolicy.L0)
+    N = h.info()["N"]
+    pts, ids = h.decode_points(np.arange(N, dtype=np.uint64))
+    Q = wl.range_boxes(h, 4096, seed=42, log_uniform=(0.001, 0.1))
+    yield h, pts, ids, Q
+    h.close()
+
+
+def test_batched_range_equals_brute_force_on_every_box(tb, batched, oracle_mod):
+    h, pts, ids, Q = batched
+    r = h.query_batch(tb.QueryType.RANGE, Q, tb.Mode.EXACT, flags=tb.WANT_VALS)
+    offs, got, vals = r.offsets.numpy(), r.ids.numpy(), r.vals.numpy()
+    b = oracle_mod.brute_query(pts, ids, oracle_mod.RANGE, Q)
+    assert np.array_equal(offs, b.offsets)
+    for q, g in enumerate(ids_by_query(offs, got)):
+        assert np.array_equal(g, b.query(q)), q
+    D = Q.shape[1] // 2
+    qi = np.repeat(np.arange(len(Q)), np.diff(offs.astype(np.int64)))
+    assert np.all(vals >= Q[qi, :D]) and np.all(vals <= Q[qi, D:])
+    assert b.offsets[-1] >= len(Q)  # every box holds at least its centre point
+
+
+def test_graph_replayed_batch_equals_synchronous(tb, batched):
+    import torch
+    h, pts, ids, Q = batched
+    dQ = torch.from_numpy(Q).cuda()
+    r = h.query_batch(tb.QueryType.RANGE, dQ, tb.Mode.EXACT)
+    offs, got = r.offsets.numpy().copy(), r.ids.numpy().copy()
+    for _ in range(2):  # capture, then replay
+        h.query_batch_async(tb.QueryType.RANGE, dQ, tb.Mode.EXACT, flags=tb.USE_GRAPH)
+        total = h.batch_wait()
+        assert total == offs[-1]
+        assert np.array_equal(r.offsets.numpy(), offs)
+        assert all(np.array_equal(a, b) for a, b in zip(ids_by_query(offs, r.ids.numpy()), ids_by_query(offs, got)))
+
+
+def test_ref_parity_equals_reference_cuda_build(tb, batched, tmp_path):
+    if not os.path.exists(HARNESS):
+        pytest.skip("reference build not present (make -C oracle ref needs the reference sources)")
+    h, pts, ids, Q = batched
+    idx = str(tmp_path / "idx")
+    h.save_index(idx)
+    qf = str(tmp_path / "q.txt")
+    n = 64
+    tb.save_query_file(qf, tb.QueryType.RANGE, Q[:n], Q.shape[1] // 2)
+    out = str(tmp_path / "ref.bin")
+    subprocess.run([HARNESS, idx, qf, "0", "0", "L0", out], check=True, timeout=900, stdout=subprocess.DEVNULL)
+    raw = open(out, "rb").read()
+    nq, intervals = (int(x) for x in np.frombuffer(raw, np.uint64, 2, 0))
+    assert nq == n
+    r = h.query_batch(tb.QueryType.RANGE, Q[:n], tb.Mode.REF_PARITY, flags=tb.WANT_LEVELS)
+    offs, got = r.offsets.numpy(), r.ids.numpy()
+    levels = r.level_items.numpy().T.astype(np.uint64)
+    off = 16
+    for q in range(n):
+        lv = np.frombuffer(raw, np.uint64, intervals, off); off += 8 * intervals
+        off += 8  # microseconds
+        c = int(np.frombuffer(raw, np.uint64, 1, off)[0]); off += 8
+        ref_ids = np.frombuffer(raw, np.uint64, c, off); off += 8 * c
+        assert np.array_equal(np.sort(got[offs[q]:offs[q + 1]]), ref_ids), q
+        assert np.array_equal(levels[q], lv), q
+    assert off == len(raw)
+
+
+def test_knn_on_the_range_index_equals_brute_force(tb, wl, batched, oracle_mod):
+    h, pts, ids, Q = batched
+    P = wl.knn_points(h, 4096, seed=1234, noise=0.02)
+    K = _knn_k(4096)
+    T = wl.knn_points(h, 512, seed=4321, noise=0.02)
+    h.scorer_train(T, K=_knn_k(512), max_samples=100000, epochs=4, lr=3e-3, seed=9)
+    r = h.query_batch(tb.QueryType.POINT, P, tb.Mode.EXACT, K=K)
+    offs, got, d2 = r.offsets.numpy(), r.ids.numpy(), r.dist2.numpy()
+    assert np.array_equal(np.diff(offs.astype(np.int64)), K.astype(np.int64))
+    sample = np.arange(0, 4096, 16)  # 256 of the 4096 points, both K values
+    for kv in (20, 100):
+        sel = sample[K[sample] == kv]
+        b = oracle_mod.brute_query(pts, ids, oracle_mod.KNN, P[sel], K=kv)
+        for j, q in enumerate(sel):
+            assert np.array_equal(got[offs[q]:offs[q + 1]], b.query(j)), q
+            assert np.array_equal(d2[offs[q]:offs[q + 1]], b.dist2[b.offsets[j]:b.offsets[j + 1]]), q
+
+
+@pytest.fixture(scope="module")
+def knn50m(tb, wl, cuda):
+    h = wl.generate_index(tb.QueryHandler, "knn")
+    h.prepare_for_query(tb.LevelPolicy.L0)
+    P = wl.knn_points(h, 64, seed=1234, noise=0.02)
+    K = _knn_k(64)
+    T = wl.knn_points(h, 256, seed=4321, noise=0.02)
+    h.scorer_train(T, K=_knn_k(256), max_samples=50000, epochs=4, lr=3e-3, seed=9)
+    yield h, P, K
+    h.close()
+
+
+def test_knn_50m_d16_equals_brute_force(tb, knn50m, oracle_mod):
+    h, P, K = knn50m
+    h.scorer_enable(True)
+    r = h.query_batch(tb.QueryType.POINT, P, tb.Mode.EXACT, K=K)
+    offs, got, d2 = r.offsets.numpy().copy(), r.ids.numpy().copy(), r.dist2.numpy().copy()
+    h.scorer_enable(False)
+    r0 = h.query_batch(tb.QueryType.POINT, P, tb.Mode.EXACT, K=K)
+    assert np.array_equal(r0.offsets.numpy(), offs) and np.array_equal(r0.ids.numpy(), got)
+    N = h.info()["N"]
+    pts, ids = h.decode_points(np.arange(N, dtype=np.uint64))
+    for kv in (20, 100):
+        sel = np.nonzero(K == kv)[0]
+        b = oracle_mod.brute_query(pts, ids, oracle_mod.KNN, P[sel], K=kv)
+        for j, q in enumerate(sel):
+            assert np.array_equal(got[offs[q]:offs[q + 1]], b.query(j)), q
+            ref = b.dist2[b.offsets[j]:b.offsets[j + 1]]
+            dq = d2[offs[q]:offs[q + 1]]
+            assert np.all(np.abs(dq - ref) <= 1e-6 * np.abs(ref)), q
+            assert np.array_equal(dq, ref), q

@@ -219,3 +219,34 @@ def test_streamed_levels_equal_resident(tb, oracle_mod, tmp_path, cuda, policy):
     rk = h.query_batch(tb.QueryType.POINT, P, tb.Mode.EXACT, K=15)
     bk = oracle_mod.brute_query(pts, ids, oracle_mod.KNN, P, K=15)
     assert np.array_equal(rk.ids.numpy(), bk.ids) and np.array_equal(rk.dist2.numpy(), bk.dist2)
+
+
+def test_lookback_timeout_is_reported_and_the_handle_recovers(tb, env, oracle_mod):
+    """Failure detection without a fault: a work tile that never publishes its counts makes its
+    successors' look-back waits run out (bounded spins). The kernel sets its timeout status and
+    returns, the later launches of the batch skip their work, and the call fails with
+    TBLAEQ_ERR_TIMEOUT. The CUDA context stays usable: the next batch on the same handle is exact."""
+    h, o, pts, ids = env
+    lib = tb.lib()
+    Q = _boxes(pts, 300, 9)  # 300 queries x 25 coarsest nodes: 30 work tiles at the first level
+    lo, hi = pts.min(0) - 1.0, pts.max(0) + 1.0  # every cluster survives
+    grid = h.run_level(0, h.coarsest_grid(), tb.QueryType.RANGE, lo=lo, hi=hi)  # 250 nodes of mesh 1
+    n_mesh1 = grid.nnz
+    lib.tblaeq_debug_lookback_timeout(1, 2000)
+    try:
+        with pytest.raises(tb.TblaeqError) as e:
+            h.query_batch(tb.QueryType.RANGE, Q, tb.Mode.EXACT)
+        assert e.value.code == 6, e.value
+        with pytest.raises(tb.TblaeqError) as e:
+            h.run_level(1, grid, tb.QueryType.RANGE, lo=lo, hi=hi)  # 5,000 children: 20 work tiles
+        assert e.value.code == 6, e.value
+    finally:
+        lib.tblaeq_debug_lookback_timeout(2**64 - 1, 0)
+    r, offs, got = _batch_ids(tb, h, Q, tb.Mode.EXACT)
+    b = oracle_mod.brute_query(pts, ids, oracle_mod.RANGE, Q)
+    assert np.array_equal(offs, b.offsets)
+    for q, g in enumerate(ids_by_query(offs, got)):
+        assert np.array_equal(g, b.query(q)), q
+    assert n_mesh1 == h.info()["meshSizes"][2]
+    g2 = h.run_level(1, grid, tb.QueryType.RANGE, lo=lo, hi=hi)
+    assert g2.nnz == h.info()["meshSizes"][1]

@@ -70,13 +70,25 @@ def test_reference_cuda_build_agrees(tb, wl, oracle_mod, tmp_path, cuda, case):
         lv, us, ids = ref[q]
         assert np.array_equal(ids, orc.query(q)), f"oracle vs reference CUDA, query {q}"
         assert np.array_equal(lv, orc.level_sizes[q])
+    h.prepare_for_query(tb.LevelPolicy.L0)
     if kind == "range":
-        h.prepare_for_query(tb.LevelPolicy.L0)
         r = h.query_batch(qtype, Q, tb.Mode.REF_PARITY)
         offs = r.offsets.numpy()
         got = r.ids.numpy()
         for q in range(nq):
             assert np.array_equal(np.sort(got[offs[q]:offs[q + 1]]), ref[q][2]), f"B200 vs reference, query {q}"
+    else:
+        # The B200 KNN plugin (IQueryStrategy::runLevel, POINT) level by level against the reference
+        # CUDA build directly: the same per-level grid sizes and the same final candidate ids.
+        for q in range(nq):
+            grid = h.coarsest_grid()
+            sizes = []
+            for l in range(h.info()["intervals"]):
+                grid = h.run_level(l, grid, tb.QueryType.POINT, point=Q[q], K=K)
+                sizes.append(grid.nnz)
+            got, _ = h.grid_arrays(grid)
+            assert np.array_equal(np.array(sizes, np.uint64), ref[q][0]), f"B200 plugin vs reference, query {q}"
+            assert np.array_equal(np.sort(got), ref[q][2]), f"B200 plugin vs reference, query {q}"
     gold = os.environ.get("TBLAEQ_GOLDEN_OUT")
     if gold:
         os.makedirs(gold, exist_ok=True)

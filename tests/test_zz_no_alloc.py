@@ -75,6 +75,28 @@ def test_noalloc_matches_level_step_on_consecutive_calls(tb, env):
     assert calls >= 4
 
 
+def test_noalloc_allocates_no_device_memory(tb, env):
+    """The property the entry point exists for: after one warm-up call (which looks up the scratch
+    array's device address), calls allocate nothing. The library's device allocation count stays
+    unchanged, and with the allocation-failure hook armed (the next allocation fails) the calls
+    still succeed."""
+    h, lib, out_ids, out_vals, cap = env
+    los, his = _boxes(h, 4, 3)
+    grid = h.coarsest_grid()
+    code, _ = _noalloc(tb, h, lib, 0, grid, los[0], his[0], out_ids, out_vals, cap)
+    assert code == 0, lib.tblaeq_last_error()
+    live = lib.tblaeq_live_device_bytes()
+    lib.tblaeq_debug_fail_alloc_after(1)
+    try:
+        for q in range(4):
+            code, n = _noalloc(tb, h, lib, 0, grid, los[q], his[q], out_ids, out_vals, cap)
+            assert code == 0, lib.tblaeq_last_error()
+            assert lib.tblaeq_live_device_bytes() == live
+    finally:
+        lib.tblaeq_debug_fail_alloc_after(0)
+    assert lib.tblaeq_live_device_bytes() == live
+
+
 def test_noalloc_limits(tb, env):
     h, lib, out_ids, out_vals, cap = env
     los, his = _boxes(h, 1, 2)
@@ -89,3 +111,26 @@ def test_noalloc_limits(tb, env):
     assert code == 5  # output larger than the caller's buffers
     code, n = _noalloc(tb, h, lib, 0, grid, los[0], his[0], out_ids, out_vals, cap)
     assert code == 0 and n > 0  # and the next call is clean again
+
+
+def test_noalloc_timeout_then_clean_call(tb, env):
+    """A look-back wait that runs out inside the allocation-free step (test hook: one work tile
+    never publishes) fails the call with TBLAEQ_ERR_TIMEOUT; the next call clears the shared
+    array's control words and matches tblaeq_level again."""
+    h, lib, out_ids, out_vals, cap = env
+    los, his = _boxes(h, 1, 5)
+    lo, hi = los[0] - 1e3, his[0] + 1e3  # every cluster survives
+    grid = h.run_level(0, h.coarsest_grid(), tb.QueryType.RANGE, lo=lo, hi=hi)  # 250 nodes of mesh 1
+    lib.tblaeq_debug_lookback_timeout(1, 2000)
+    try:
+        code, _ = _noalloc(tb, h, lib, 1, grid, lo, hi, out_ids, out_vals, cap)  # 5,000 children
+        assert code == 6, lib.tblaeq_last_error()
+    finally:
+        lib.tblaeq_debug_lookback_timeout(2**64 - 1, 0)
+    code, n = _noalloc(tb, h, lib, 1, grid, lo, hi, out_ids, out_vals, cap)
+    assert code == 0, lib.tblaeq_last_error()
+    ref = h.run_level(1, grid, tb.QueryType.RANGE, lo=lo, hi=hi)
+    ref_ids, ref_vals = h.grid_arrays(ref)
+    assert n == ref.nnz > 256
+    assert np.array_equal(out_ids[:n].cpu().numpy().astype(np.uint64), ref_ids)
+    assert np.array_equal(out_vals[:n * D].cpu().numpy().reshape(n, D), ref_vals)
