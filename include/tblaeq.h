@@ -18,8 +18,9 @@
 extern "C" {
 #endif
 
-/* 2: tblaeq_serve_config gained `levels` (and tblaeq_serve_poll_levels was added). */
-#define TBLAEQ_ABI_VERSION 2
+/* 2: tblaeq_serve_config gained `levels` (and tblaeq_serve_poll_levels was added).
+ * 3: tblaeq_build_config gained `host_assembly`, tblaeq_build_report `assemble_seconds`. */
+#define TBLAEQ_ABI_VERSION 3
 
 typedef struct tblaeq_handle tblaeq_handle; /* QueryHandler: host index + device state */
 
@@ -301,13 +302,17 @@ int tblaeq_debug_split_above(tblaeq_handle* h, uint64_t limit);
  * Genenate_One_P_Tensor / Compute_Max_Radius, src/Setup/Setup.cuh:87-171): Lloyd's k-means per
  * level on the GPU, k = floor(n / ratio) centroids sampled from the data (seeded), `iters`
  * iterations, then the same P-tensor / map / radius assembly (rows grouped by label in input
- * order). precision: 0 = tensor cores (tcgen05; TF32 hi/lo split operands, FP32 accumulation;
- * D <= 16, larger D uses 1), 1 = FP32 CUDA cores, 2 = FP64 CUDA cores (the precision reference).
- * Centroid sums accumulate in FP64; objectives are sum ||x - c(x)||^2 in FP64. */
+ * order), done on the device: labels and centroids never leave it, only the finished index
+ * arrays are copied to the host index. precision: 0 = tensor cores (tcgen05; TF32 hi/lo split
+ * operands, FP32 accumulation; D <= 16, larger D uses 1), 1 = FP32 CUDA cores, 2 = FP64 CUDA cores
+ * (the precision reference). Centroid sums accumulate in FP64; objectives are sum ||x - c(x)||^2 in
+ * FP64. */
 typedef struct {
     int iters;         /* Lloyd iterations per level (0: 20) */
     uint64_t seed;
     int precision;
+    int host_assembly; /* 1: assemble each level on the host from downloaded labels and centroids, as
+                          the reference does (same bytes; for comparisons) */
 } tblaeq_build_config;
 
 typedef struct {
@@ -315,7 +320,8 @@ typedef struct {
     int iters;
     double objective;       /* after the last iteration */
     double assign_seconds;  /* device time of the assignment passes */
-    double seconds;         /* the whole level, including the index assembly on the host */
+    double assemble_seconds; /* the level's index assembly (P-tensor, map, radii) */
+    double seconds;         /* the whole level, including the index assembly */
 } tblaeq_build_report;
 
 /* Builds an index over host FP32 points (N x D) with `height` levels and `ratios` (finest first, as

@@ -25,7 +25,7 @@ import numpy as np
 _HERE = os.path.dirname(os.path.abspath(__file__))
 # TBLAEQ_LIBRARY selects another build of the same library (e.g. a differently tuned one).
 LIB_PATH = os.environ.get("TBLAEQ_LIBRARY") or os.path.join(_HERE, "libtblaeq_b200.so")
-ABI_VERSION = 2  # TBLAEQ_ABI_VERSION of include/tblaeq.h this binding is written against
+ABI_VERSION = 3  # TBLAEQ_ABI_VERSION of include/tblaeq.h this binding is written against
 HEADER_PATH = os.path.join(os.path.dirname(_HERE), "include", "tblaeq.h")
 
 
@@ -68,12 +68,14 @@ class _GenParams(ctypes.Structure):
 
 
 class _BuildConfig(ctypes.Structure):
-    _fields_ = [("iters", ctypes.c_int), ("seed", ctypes.c_uint64), ("precision", ctypes.c_int)]
+    _fields_ = [("iters", ctypes.c_int), ("seed", ctypes.c_uint64), ("precision", ctypes.c_int),
+                ("host_assembly", ctypes.c_int)]
 
 
 class _BuildReport(ctypes.Structure):
     _fields_ = [("n", ctypes.c_uint64), ("k", ctypes.c_uint64), ("iters", ctypes.c_int),
-                ("objective", ctypes.c_double), ("assign_seconds", ctypes.c_double), ("seconds", ctypes.c_double)]
+                ("objective", ctypes.c_double), ("assign_seconds", ctypes.c_double),
+                ("assemble_seconds", ctypes.c_double), ("seconds", ctypes.c_double)]
 
 
 class KmeansPrecision(enum.IntEnum):
@@ -338,14 +340,16 @@ class QueryHandler:
 
     @classmethod
     def build(cls, points, height: int = 4, ratios: Sequence[int] = (100, 50, 20), iters: int = 20, seed: int = 1,
-              precision: "KmeansPrecision" = None) -> tuple:
+              precision: "KmeansPrecision" = None, host_assembly: bool = False) -> tuple:
         """IndexBuilder::build over FP32 points (N x D): GPU k-means per level, then the reference's
-        P-tensor / map / radius assembly. Returns (handler, per-level reports, finest first)."""
+        P-tensor / map / radius assembly, on the device (host_assembly=True: on the host from
+        downloaded labels and centroids, like the reference). Returns (handler, per-level reports,
+        finest first)."""
         X = np.ascontiguousarray(np.asarray(points, dtype=np.float32))
         N, D = X.shape
         r = np.ascontiguousarray(np.array(list(ratios), dtype=np.uint64))
         prec = KmeansPrecision.TENSOR if precision is None else precision
-        cfg = _BuildConfig(iters, seed, int(prec))
+        cfg = _BuildConfig(iters, seed, int(prec), int(host_assembly))
         reps = (_BuildReport * max(1, height - 1))()
         h = ctypes.c_void_p()
         _check(_load().tblaeq_kmeans_build(_dptr(X, ctypes.c_float), N, D, height, _dptr(r, ctypes.c_uint64),
@@ -783,7 +787,7 @@ def kmeans(points, k: int, iters: int = 20, seed: int = 1, precision: KmeansPrec
     C = np.empty((k, D), np.float32)
     L = np.empty(n, np.uint32)
     obj = np.empty(iters, np.float64)
-    cfg = _BuildConfig(iters, seed, int(precision))
+    cfg = _BuildConfig(iters, seed, int(precision), 0)
     _check(_load().tblaeq_kmeans(_dptr(X, ctypes.c_float), n, D, k, ctypes.byref(cfg), _dptr(C, ctypes.c_float),
                                  L.ctypes.data_as(ctypes.POINTER(ctypes.c_uint32)), _dptr(obj)))
     return C, L, obj

@@ -906,6 +906,7 @@ static KmeansConfig kmeansConfigOf(const tblaeq_build_config* cfg) {
         if (cfg->iters > 0) c.iters = cfg->iters;
         c.seed = cfg->seed;
         c.precision = cfg->precision;
+        c.hostAssembly = cfg->host_assembly != 0;
     }
     return c;
 }
@@ -936,6 +937,7 @@ int tblaeq_kmeans_build(const float* points, uint64_t N, uint64_t D, uint64_t he
                 report[i].iters = reps[i].iters;
                 report[i].objective = reps[i].objective;
                 report[i].assign_seconds = reps[i].assignSeconds;
+                report[i].assemble_seconds = reps[i].assembleSeconds;
                 report[i].seconds = reps[i].seconds;
             }
         }

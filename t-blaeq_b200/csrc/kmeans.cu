@@ -1,5 +1,6 @@
 // Hierarchical k-means build (see kmeans.cuh).
 #include "kmeans.cuh"
+#include "knn.cuh"
 #include "tcgen05.cuh"
 
 #include <algorithm>
@@ -474,6 +475,99 @@ void assembleInterval(HostIndex& idx, uint64_t pIdx, uint64_t fineMesh, const fl
     idx.maps[fineMesh] = std::move(order);
 }
 
+// ---- index assembly on the device (replaces the host loop above for builds) --------------------
+// sortKeys[i] = (label << 32) | i: sorting them groups the points by label, in input order within a
+// label (the order the host assembly and the reference's std::sort by label produce).
+__global__ void labelKeysKernel(const uint32_t* labels, uint64_t n, uint64_t* keys, uint32_t* vals) {
+    for (uint64_t i = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x; i < n;
+         i += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
+        keys[i] = (static_cast<uint64_t>(labels[i]) << 32) | i;
+        vals[i] = static_cast<uint32_t>(i);
+    }
+}
+
+// colRes from the sorted keys: colRes[c] = first position whose label is >= c, colRes[k] = n.
+__global__ void colResKernel(const uint64_t* keys, uint64_t n, uint64_t k, uint64_t* colRes) {
+    for (uint64_t p = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x; p <= n;
+         p += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
+        const uint64_t prev = p == 0 ? 0 : (keys[p - 1] >> 32) + 1;  // first label not yet started
+        const uint64_t cur = p == n ? k : (keys[p] >> 32);
+        for (uint64_t c = prev; c <= cur && c <= k; ++c) colRes[c] = p;
+    }
+}
+
+// Row `pos` of the P-tensor: the member point's coordinates divided by its centroid's (FP64
+// division of the FP32 values, like the host assembly), the map entry (the member's input index),
+// and the member's distance to its centroid folded into the centroid's radius (sum of squares in
+// dimension order with separate multiply and add, correctly rounded square root; distances are
+// non-negative, so their bit patterns order like their values and an integer maximum is exact).
+__global__ void assembleRowsKernel(const uint64_t* keys, uint64_t n, int D, const float* fine, const float* coarse,
+                                   double* vals, uint64_t* map, unsigned long long* radiusBits, uint32_t* zero) {
+    for (uint64_t pos = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x; pos < n;
+         pos += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
+        const uint64_t key = keys[pos];
+        const uint64_t c = key >> 32, i = key & 0xffffffffull;
+        double sum = 0.0;
+        bool z = false;
+        for (int d = 0; d < D; ++d) {
+            const double cv = static_cast<double>(coarse[c * D + d]);
+            const double f = static_cast<double>(fine[i * D + d]);
+            z = z || cv == 0.0;
+            vals[pos * D + d] = __ddiv_rn(f, cv);
+            const double diff = __dsub_rn(cv, f);
+            sum = __dadd_rn(sum, __dmul_rn(diff, diff));
+        }
+        if (z) atomicOr(zero, 1u);
+        map[pos] = i;
+        atomicMax(radiusBits + c, static_cast<unsigned long long>(__double_as_longlong(__dsqrt_rn(sum))));
+    }
+}
+
+// Assembles interval pIdx on the device from one level's labels (device), its points (dFine) and
+// centroids (dCoarse), with the same results as assembleInterval, and copies the finished arrays
+// (P values, column offsets and sizes, map, radii) into the host index. Labels and centroids stay
+// on the device.
+void assembleIntervalDevice(HostIndex& idx, uint64_t pIdx, uint64_t fineMesh, const float* dFine, uint64_t nF,
+                            const float* dCoarse, uint64_t nC, const uint32_t* dLabels, cudaStream_t s) {
+    if (nF > 0xffffffffull) throw std::invalid_argument("k-means build: a level above 2^32 points");
+    const uint64_t D = idx.D;
+    DeviceMem keys(nF * 8), keys2(nF * 8), vals(nF * 4), vals2(nF * 4);
+    labelKeysKernel<<<gridFor(nF, 256), 256, 0, s>>>(dLabels, nF, keys.as<uint64_t>(), vals.as<uint32_t>());
+    TBLAEQ_CUDA(cudaGetLastError());
+    sortPairs(keys.as<uint64_t>(), vals.as<uint32_t>(), keys2.as<uint64_t>(), vals2.as<uint32_t>(), nF, s);
+    DeviceMem colRes((nC + 1) * 8), pv(nF * D * 8), map(nF * 8), rad(nC * 8), zero(4);
+    TBLAEQ_CUDA(cudaMemsetAsync(rad.get(), 0, nC * 8, s));
+    TBLAEQ_CUDA(cudaMemsetAsync(zero.get(), 0, 4, s));
+    colResKernel<<<gridFor(nF + 1, 256), 256, 0, s>>>(keys.as<uint64_t>(), nF, nC, colRes.as<uint64_t>());
+    TBLAEQ_CUDA(cudaGetLastError());
+    assembleRowsKernel<<<gridFor(nF, 256), 256, 0, s>>>(keys.as<uint64_t>(), nF, static_cast<int>(D), dFine, dCoarse,
+                                                        pv.as<double>(), map.as<uint64_t>(),
+                                                        rad.as<unsigned long long>(), zero.as<uint32_t>());
+    TBLAEQ_CUDA(cudaGetLastError());
+    PTensor& P = idx.pTensors[pIdx];
+    P.D = D;
+    P.rows = nF;
+    P.cols = nC;
+    P.nnz = nF;
+    P.isAos = 1;
+    P.colRes.resize(nC + 1);
+    P.vals.resize(nF * D);
+    idx.maps[fineMesh].resize(nF);
+    idx.radius[pIdx].resize(nC);
+    uint32_t z = 0;
+    TBLAEQ_CUDA(cudaMemcpyAsync(P.colRes.data(), colRes.get(), (nC + 1) * 8, cudaMemcpyDeviceToHost, s));
+    TBLAEQ_CUDA(cudaMemcpyAsync(P.vals.data(), pv.get(), nF * D * 8, cudaMemcpyDeviceToHost, s));
+    TBLAEQ_CUDA(cudaMemcpyAsync(idx.maps[fineMesh].data(), map.get(), nF * 8, cudaMemcpyDeviceToHost, s));
+    TBLAEQ_CUDA(cudaMemcpyAsync(idx.radius[pIdx].data(), rad.get(), nC * 8, cudaMemcpyDeviceToHost, s));
+    TBLAEQ_CUDA(cudaMemcpyAsync(&z, zero.get(), 4, cudaMemcpyDeviceToHost, s));
+    TBLAEQ_CUDA(cudaStreamSynchronize(s));
+    if (z) throw std::runtime_error("division by zero in P-tensor build: a centroid coordinate is 0");
+    P.nnzPerCol.resize(nC);
+    for (uint64_t c = 0; c < nC; ++c) P.nnzPerCol[c] = P.colRes[c + 1] - P.colRes[c];
+    P.rowIds.resize(nF);
+    std::iota(P.rowIds.begin(), P.rowIds.end(), uint64_t{0});
+}
+
 }  // namespace
 
 void kmeansRun(const float* dX, uint64_t n, uint64_t D, uint64_t k, const KmeansConfig& cfg, DeviceMem& centroids,
@@ -597,8 +691,6 @@ HostIndex kmeansBuild(const float* hostPoints, uint64_t N, uint64_t D, uint64_t 
 
     DeviceMem dX(N * D * 4);
     TBLAEQ_CUDA(cudaMemcpyAsync(dX.get(), hostPoints, N * D * 4, cudaMemcpyHostToDevice, s));
-    std::vector<float> fineHost;  // the current level's data on the host (the points for level 0)
-    const float* fine = hostPoints;
     uint64_t n = N;
     for (uint64_t i = 0; i < idx.intervals; ++i) {
         const auto t0 = std::chrono::steady_clock::now();
@@ -609,13 +701,23 @@ HostIndex kmeansBuild(const float* hostPoints, uint64_t N, uint64_t D, uint64_t 
         KmeansConfig c = cfg;
         c.seed = cfg.seed + i;
         kmeansRun(dX.as<float>(), n, D, k, c, C, L, reports[i], s);
-        std::vector<float> coarse(k * D);
-        std::vector<uint32_t> labels(n);
-        TBLAEQ_CUDA(cudaMemcpyAsync(coarse.data(), C.get(), k * D * 4, cudaMemcpyDeviceToHost, s));
-        TBLAEQ_CUDA(cudaMemcpyAsync(labels.data(), L.get(), n * 4, cudaMemcpyDeviceToHost, s));
-        TBLAEQ_CUDA(cudaStreamSynchronize(s));
-        assembleInterval(idx, pIdx, fineMesh, fine, n, coarse.data(), k, labels.data());
+        const auto ta = std::chrono::steady_clock::now();
+        if (cfg.hostAssembly) {
+            std::vector<float> fine(n * D), coarse(k * D);
+            std::vector<uint32_t> labels(n);
+            TBLAEQ_CUDA(cudaMemcpyAsync(fine.data(), dX.get(), n * D * 4, cudaMemcpyDeviceToHost, s));
+            TBLAEQ_CUDA(cudaMemcpyAsync(coarse.data(), C.get(), k * D * 4, cudaMemcpyDeviceToHost, s));
+            TBLAEQ_CUDA(cudaMemcpyAsync(labels.data(), L.get(), n * 4, cudaMemcpyDeviceToHost, s));
+            TBLAEQ_CUDA(cudaStreamSynchronize(s));
+            assembleInterval(idx, pIdx, fineMesh, fine.data(), n, coarse.data(), k, labels.data());
+        } else {
+            assembleIntervalDevice(idx, pIdx, fineMesh, dX.as<float>(), n, C.as<float>(), k, L.as<uint32_t>(), s);
+        }
+        reports[i].assembleSeconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - ta).count();
         if (i + 2 == height) {
+            std::vector<float> coarse(k * D);
+            TBLAEQ_CUDA(cudaMemcpyAsync(coarse.data(), C.get(), k * D * 4, cudaMemcpyDeviceToHost, s));
+            TBLAEQ_CUDA(cudaStreamSynchronize(s));
             idx.meshSizes.push_back(k);
             idx.coarsest.rows = k;
             idx.coarsest.dim = D;
@@ -625,9 +727,7 @@ HostIndex kmeansBuild(const float* hostPoints, uint64_t N, uint64_t D, uint64_t 
             std::iota(idx.coarsest.ids.begin(), idx.coarsest.ids.end(), uint64_t{0});
             idx.coarsest.vals.assign(coarse.begin(), coarse.end());
         }
-        // The centroids are the next level's data.
-        fineHost = std::move(coarse);
-        fine = fineHost.data();
+        // The centroids are the next level's data (they stay on the device).
         dX = std::move(C);
         n = k;
         reports[i].seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();

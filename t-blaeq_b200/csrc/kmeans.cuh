@@ -34,6 +34,9 @@ struct KmeansConfig {
     int iters = 20;
     uint64_t seed = 1;
     int precision = kKmTensor;
+    // Assemble each interval (P-tensor, map, radii) on the host from downloaded labels and
+    // centroids, as the reference does, instead of on the device (for comparisons).
+    bool hostAssembly = false;
 };
 
 struct KmeansLevelReport {
@@ -41,6 +44,7 @@ struct KmeansLevelReport {
     int iters = 0;
     double objective = 0.0;         // after the last update, FP64
     double assignSeconds = 0.0;     // device time of all assignment passes
+    double assembleSeconds = 0.0;   // the index assembly of the level (grouping, P values, map, radii)
     double seconds = 0.0;           // the whole level (Lloyd + index assembly)
     std::vector<double> objectives; // after every iteration
 };

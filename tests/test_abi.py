@@ -23,7 +23,7 @@ def test_every_declared_symbol_is_exported(tb):
 
 
 def test_abi_version(tb):
-    assert tb.lib().tblaeq_abi_version() == tb.ABI_VERSION == 2
+    assert tb.lib().tblaeq_abi_version() == tb.ABI_VERSION == 3
 
 
 def test_header_is_plain_c_and_links(tb, tmp_path):
