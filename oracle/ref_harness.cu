@@ -7,6 +7,7 @@
 // compare the B200 path against the reference CUDA build on the same index and queries.
 //
 // usage: ref_harness <index_dir> <query_file> <0=range|1=knn> <K> <policy L0..L3> <out.bin>
+//        (b200_drop_in: the same arguments)
 //
 // out.bin (little endian):
 //   u64 nq, u64 intervals
@@ -23,6 +24,12 @@
 #include "src/core/QueryHandler.cuh"
 #include "src/core/MemoryPolicy.cuh"
 #include "src/Data_Structures/File.cuh"
+#ifdef TBLAEQ_DROP_IN
+// Built as b200_drop_in: the same driver, with every L0 level of the reference's QueryEngine
+// dispatched to the B200 library through the reference-side adapter (ref_shim/b200). It also
+// writes <out.bin>.levels: the number of levels the B200 strategy ran.
+#include "b200/dispatch.cuh"
+#endif
 
 int main(int argc, char** argv) {
     if (argc != 7) {
@@ -42,6 +49,15 @@ int main(int argc, char** argv) {
 
     QueryHandler handler(indexDir, /*loadFromIndex=*/true);
     handler.prepareForQuery(IndexPolicy::parseLevel(policy));
+#ifdef TBLAEQ_DROP_IN
+    tblaeq_handle* b200 = nullptr;
+    if (tblaeq_open(indexDir.c_str(), &b200) != TBLAEQ_OK || tblaeq_prepare(b200, nullptr, 0) != TBLAEQ_OK) {
+        std::cout.rdbuf(old);
+        std::fprintf(stderr, "B200 library: %s\n", tblaeq_last_error());
+        return 1;
+    }
+    b200UseHandleForL0(b200);
+#endif
 
     const Query q = (type == 1) ? loadQueryPointFromFile(queryFile) : loadQueryRangeFromFile(queryFile);
     FILE* f = std::fopen(outPath.c_str(), "wb");
@@ -94,5 +110,12 @@ int main(int argc, char** argv) {
     std::fwrite(&intervals, 8, 1, f);
     std::fclose(f);
     std::cout.rdbuf(old);
+#ifdef TBLAEQ_DROP_IN
+    b200UseHandleForL0(nullptr);
+    if (FILE* lv = std::fopen((outPath + ".levels").c_str(), "w")) {
+        std::fprintf(lv, "%llu\n", static_cast<unsigned long long>(b200LevelsDispatched()));
+        std::fclose(lv);
+    }
+#endif
     return 0;
 }

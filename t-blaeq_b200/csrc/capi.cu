@@ -186,14 +186,15 @@ int tblaeq_level(tblaeq_handle* h, uint64_t l, const tblaeq_grid* in, int qtype,
     if (qtype == TBLAEQ_POINT && !q) return fail(TBLAEQ_ERR_INVALID, "KNN query needs a point");
     return guarded([&]() -> int {
         B200Strategy s(h->qh->runtime());
-        Grid g{in->numRows, in->dim, in->nnz, in->ids, in->vals};
+        SparseGrid g{in->numRows, in->dim, in->nnz, in->ids, in->vals};
         const LevelResult r =
-            s.runLevel(l, g, qtype == TBLAEQ_RANGE ? QueryType::RANGE : QueryType::POINT, lo, hi, q, K);
-        out->numRows = r.grid.numRows;
-        out->dim = r.grid.dim;
-        out->nnz = r.grid.nnz;
-        out->ids = r.grid.ids;
-        out->vals = r.grid.vals;
+            s.runLevel(l, &g, qtype == TBLAEQ_RANGE ? QueryType::RANGE : QueryType::POINT, lo, hi, q, K);
+        const std::unique_ptr<SparseGrid> grid(r.grid);  // the buffers stay with the handle
+        out->numRows = grid->numRows;
+        out->dim = grid->dim;
+        out->nnz = grid->nnz;
+        out->ids = grid->ids;
+        out->vals = grid->vals;
         return TBLAEQ_OK;
     });
 }

@@ -4,8 +4,12 @@
 #include "knn.cuh"
 
 #include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <fstream>
 #include <iomanip>
 #include <iostream>
+#include <limits>
 #include <stdexcept>
 
 namespace tblaeq {
@@ -158,9 +162,11 @@ void B200Strategy::prepare(std::ostream& reportOs) {
              << " interval(s) read from mapped host memory\n";
 }
 
-LevelResult B200Strategy::runLevel(size_t l, const Grid& cur, QueryType qType, const double* lo, const double* hi,
+LevelResult B200Strategy::runLevel(size_t l, SparseGrid* curGrid, QueryType qType, const double* lo, const double* hi,
                                    const double* queryPoint, size_t K) {
     const HostIndex& h = *rt_.host;
+    if (!curGrid) throw std::invalid_argument("runLevel: null grid");
+    const SparseGrid& cur = *curGrid;
     if (l >= h.intervals) throw std::out_of_range("runLevel: level out of range");
     if (cur.dim != h.D) throw std::invalid_argument("runLevel: grid dimension mismatch");
     const uint64_t D = h.D;
@@ -209,11 +215,189 @@ LevelResult B200Strategy::runLevel(size_t l, const Grid& cur, QueryType qType, c
                                            out.vals.as<double>(), cap);
     }
     LevelResult r;
-    r.grid.numRows = h.meshCount(l + 1);
-    r.grid.dim = D;
-    r.grid.nnz = n;
-    r.grid.ids = out.ids.as<uint64_t>();
-    r.grid.vals = out.vals.as<double>();
+    r.grid = new SparseGrid{h.meshCount(l + 1), D, n, out.ids.as<uint64_t>(), out.vals.as<double>()};
+    return r;
+}
+
+// ---- the reference's query API on the facade -------------------------------------------------------
+
+Query loadQueryFile(const std::string& path, QueryType type) {
+    std::ifstream in(path);
+    if (!in) throw std::runtime_error("Cannot open query file: " + path);
+    Query q;
+    q.type = type;
+    long long n = -1, d = -1;
+    if (!(in >> n >> d) || n < 0 || d <= 0) throw std::runtime_error("Invalid query file header: " + path);
+    q.length = static_cast<size_t>(n);
+    q.dim = static_cast<size_t>(d);
+    const size_t per = (type == QueryType::RANGE ? 2 : 1) * q.dim;
+    q.data.resize(q.length * per);
+    for (size_t i = 0; i < q.data.size(); ++i)
+        if (!(in >> q.data[i]))
+            throw std::runtime_error("Query file ended after " + std::to_string(i / per) + " of " +
+                                     std::to_string(q.length) + " rows: " + path);
+    return q;
+}
+
+LevelResult QueryEngine::runSingleQuery(QueryHandler& qh, QueryType qType, const double* lo, const double* hi,
+                                        const double* queryPoint, size_t K, size_t* levelFineMeshSize) {
+    Runtime& rt = qh.runtime();
+    const HostIndex& h = *rt.host;
+    // The coarsest mesh as the first grid (QueryEngine.cu:66-70), device-resident.
+    SparseGrid coarsest{h.coarsest.rows, h.D, h.coarsest.nnz, rt.dev->coarseIds.as<uint64_t>(),
+                        rt.dev->coarseVals.as<double>()};
+    B200Strategy strategy(rt);
+    SparseGrid* cur = &coarsest;
+    LevelResult last{};
+    for (size_t l = 0; l < h.intervals; ++l) {
+        LevelResult r = strategy.runLevel(l, cur, qType, lo, hi, queryPoint, K);
+        if (levelFineMeshSize) levelFineMeshSize[l] = r.grid->nnz;
+        if (cur != &coarsest) delete cur;  // the strategy keeps the buffers (ownsIds = ownsVals = false)
+        cur = r.grid;
+        last = r;
+    }
+    return last;
+}
+
+namespace {
+double rangeLogVolume(const double* lo, const double* hi, size_t D) {
+    double v = 0.0;
+    for (size_t i = 0; i < D; ++i) {
+        const double s = hi[i] - lo[i];
+        if (s <= 0.0) return -std::numeric_limits<double>::infinity();
+        v += std::log(s);
+    }
+    return v;
+}
+}  // namespace
+
+QueryResult QueryEngine::run(QueryHandler& qh, const Query& q, const RunConfig& cfg) {
+    if (!qh.prepared()) throw std::logic_error("call prepareForQuery before querying");
+    Runtime& rt = qh.runtime();
+    const HostIndex& h = *rt.host;
+    if (q.dim != h.D) throw std::invalid_argument("query dimension does not match the index");
+    QueryResult res;
+    res.type = q.type;
+    res.datasetName = h.datasetName;
+    res.datasetSize = h.N;
+    res.datasetDim = h.D;
+    res.queryParam = q.type == QueryType::POINT ? "K=" + std::to_string(cfg.K) : "";
+    for (size_t l = 0; l < h.intervals; ++l) res.levelOriginalSize.push_back(h.meshCount(l + 1));
+    const size_t count = std::min(q.length, cfg.maxQueryCount);
+    const bool range = q.type == QueryType::RANGE;
+    long totalUs = 0, maxUs = 0, minUs = std::numeric_limits<long>::max();
+    std::vector<double> row(2 * h.D);
+    for (size_t i = 0; i < count; ++i) {
+        const double* lo = range ? q.getQueryLo(i) : nullptr;
+        const double* hi = range ? q.getQueryHi(i) : nullptr;
+        const double* pt = range ? nullptr : q.getQueryPoint(i);
+        std::vector<size_t> lv(h.intervals, 0);
+        std::vector<uint64_t> ids;
+        std::vector<double> d2;
+        const auto t0 = std::chrono::steady_clock::now();
+        size_t n = 0;
+        if (qh.mode() == kModeRefParity) {
+            LevelResult r = runSingleQuery(qh, q.type, lo, hi, pt, cfg.K, lv.data());
+            n = r.grid->nnz;
+            if (cfg.saveFineMesh && n) {
+                ids.resize(n);
+                TBLAEQ_CUDA(cudaMemcpyAsync(ids.data(), r.grid->ids, n * 8, cudaMemcpyDeviceToHost, rt.stream));
+                TBLAEQ_CUDA(cudaStreamSynchronize(rt.stream));
+            }
+            delete r.grid;
+        } else {
+            // Exact answers: the batched engine with one query (its own per-level counts).
+            const size_t w = range ? 2 * h.D : h.D;
+            std::copy(range ? lo : pt, (range ? lo : pt) + w, row.begin());
+            TBLAEQ_CUDA(cudaMemcpyAsync(rt.scratchQuery.get(), row.data(), w * 8, cudaMemcpyHostToDevice, rt.stream));
+            BatchOutput o;
+            if (range) {
+                o = rt.engine->runRange(rt.scratchQuery.as<double>(), 1, kModeExact, kWantLevels);
+            } else {
+                const uint32_t k32 = static_cast<uint32_t>(cfg.K);
+                TBLAEQ_CUDA(cudaMemcpyAsync(rt.scratchQuery.as<double>() + h.D, &k32, 4, cudaMemcpyHostToDevice,
+                                            rt.stream));
+                o = rt.engine->runKnn(rt.scratchQuery.as<double>(), 1,
+                                      reinterpret_cast<const uint32_t*>(rt.scratchQuery.as<double>() + h.D), cfg.K,
+                                      kWantLevels);
+            }
+            n = o.total;
+            std::vector<uint32_t> items(h.intervals);
+            TBLAEQ_CUDA(cudaMemcpyAsync(items.data(), o.levelItems, h.intervals * 4, cudaMemcpyDeviceToHost, rt.stream));
+            if (cfg.saveFineMesh && n) {
+                ids.resize(n);
+                TBLAEQ_CUDA(cudaMemcpyAsync(ids.data(), o.ids, n * 8, cudaMemcpyDeviceToHost, rt.stream));
+                if (o.dist2) {
+                    d2.resize(n);
+                    TBLAEQ_CUDA(cudaMemcpyAsync(d2.data(), o.dist2, n * 8, cudaMemcpyDeviceToHost, rt.stream));
+                }
+            }
+            TBLAEQ_CUDA(cudaStreamSynchronize(rt.stream));
+            for (size_t l = 0; l < h.intervals; ++l) lv[l] = items[l];
+        }
+        const long us = std::chrono::duration_cast<std::chrono::microseconds>(std::chrono::steady_clock::now() - t0)
+                            .count();
+        maxUs = std::max(maxUs, us);
+        minUs = std::min(minUs, us);
+        totalUs += us;
+        res.queryTimeUs.push_back(us);
+        res.levelFineMeshSize.push_back(std::move(lv));
+        res.fineMeshSize.push_back(n);
+        res.queryRangeVolume.push_back(range ? rangeLogVolume(lo, hi, h.D) : 1.0);
+        if (cfg.saveFineMesh) {
+            res.ids.push_back(std::move(ids));
+            res.dist2.push_back(std::move(d2));
+        }
+    }
+    long cnt = static_cast<long>(count);
+    if (cnt > 2) {  // the reference drops the fastest and the slowest query (QueryEngine.cu:216-220)
+        totalUs -= maxUs + minUs;
+        cnt -= 2;
+    }
+    res.totalTimeUs = totalUs;
+    res.queryCount = static_cast<size_t>(cnt);
+    for (size_t l = 0; l < h.intervals; ++l) {
+        if (l) res.memoryPolicy += "-";
+        res.memoryPolicy += levelPolicyName(qh.activePolicy().levels[l]);
+    }
+    return res;
+}
+
+QueryResult QueryHandler::performQuery(const std::string& path, QueryType type, bool saveFineMesh,
+                                       size_t maxQueryCount, size_t K) {
+    Query q = loadQueryFile(path, type);
+    RunConfig cfg;
+    cfg.maxQueryCount = maxQueryCount;
+    cfg.K = K;
+    cfg.saveFineMesh = saveFineMesh;
+    return QueryEngine::run(*this, q, cfg);
+}
+
+QueryResult QueryHandler::performSingleKNNQuery(const std::vector<double>& point, size_t K, bool saveFineMesh) {
+    Query q;
+    q.type = QueryType::POINT;
+    q.length = 1;
+    q.dim = point.size();
+    q.data = point;
+    RunConfig cfg;
+    cfg.K = K;
+    cfg.saveFineMesh = saveFineMesh;
+    return QueryEngine::run(*this, q, cfg);
+}
+
+QueryResult QueryHandler::performSingleRangeQuery(const std::vector<double>& upper, const std::vector<double>& lower,
+                                                  bool saveFineMesh) {
+    if (upper.size() != lower.size()) throw std::invalid_argument("range bounds of different dimensions");
+    Query q;
+    q.type = QueryType::RANGE;
+    q.length = 1;
+    q.dim = lower.size();
+    q.data = lower;
+    q.data.insert(q.data.end(), upper.begin(), upper.end());
+    RunConfig cfg;
+    cfg.saveFineMesh = saveFineMesh;
+    QueryResult r = QueryEngine::run(*this, q, cfg);
+    r.queryParam = "single-range-query";
     return r;
 }
 
