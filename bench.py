@@ -371,7 +371,9 @@ def main():
     # Warm-up: the first synchronous batch sizes every workspace, the autotuner picks a kernel
     # variant per level on this batch, the rest replay the graph.
     h.query_batch(tb.QueryType.RANGE, dQ, tb.Mode.EXACT)
-    variants, tuned_ms = h.autotune(dQ, tb.Mode.EXACT, reps=5)
+    import tempfile
+    cache = os.environ.get("TBLAEQ_TUNING_CACHE", os.path.join(tempfile.gettempdir(), "tblaeq_tuning.txt"))
+    variants, grids, tuned_ms, tuned_from = h.autotune_cached(dQ, cache, tb.Mode.EXACT, reps=5)
     h.set_timing(True)
     flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
     for _ in range(args.warmup):
@@ -537,7 +539,10 @@ def main():
         "plain": {"value": plain_qps, "unit": "queries/s", "queries": n_plain,
                   "speedup_batched_vs_plain": value / world / plain_qps},
         "results_per_step": results,
-        "autotune": {"variants": ["staged" if v else "direct" for v in variants], "level_ms": tuned_ms},
+        "autotune": {"variants": ["staged" if v else "direct" for v in variants], "grid_percent": grids,
+                     "level_ms": tuned_ms, "source": tuned_from, "cache": cache,
+                     "searched": "variant {direct, staged} x persistent grid {100, 75, 50, 25}% of occupancy, "
+                                 "per level, on the live batch"},
         "level_entries": entries,
         "level_children": items,
         # A finest interval read from mapped host memory is bound by the host link, not HBM.
@@ -799,6 +804,10 @@ def run_build(args, tb, rank, world, local):
     flops = 3 * 2.0 * lvl0["n"] * lvl0["k"] * 16 * lvl0["iters"]
     achieved = flops / lvl0["assign_seconds"] / 1e12
     tf32_peak = peaks.get("bf16_tflops", 1590.0) / 2
+    # The algorithmic distance FLOPs (2 N k D per Lloyd iteration, one product per distance), against
+    # the measured dense BF16 GEMM rate of a seconds-long loop (the assignment runs for seconds).
+    alg = 2.0 * lvl0["n"] * lvl0["k"] * D * lvl0["iters"] / lvl0["assign_seconds"] / 1e12
+    sustained = peaks.get("bf16_tflops_sustained", 1400.0)
     print(json.dumps({
         "metric": "index build: points indexed per second (k-means hierarchy, 1 B200 per rank)",
         "value": args.build_n / total * world, "unit": "points/s", "n_gpus": world, "higher_is_better": True,
@@ -812,7 +821,12 @@ def run_build(args, tb, rank, world, local):
         "roofline": {"bound": "tensor", "kernel": "assignTcKernel (level 0)", "achieved": achieved,
                      "peak": tf32_peak, "unit": "TFLOP/s", "frac": achieved / tf32_peak,
                      "peak_kind": "half the measured bf16 dense GEMM (TF32 rate)",
-                     "note": "3 TF32 products per distance; the per-point argmin epilogue on CUDA cores bounds it"},
+                     "note": "3 TF32 products per distance; the per-point argmin epilogue on CUDA cores bounds it",
+                     "algorithmic": {"achieved": alg, "unit": "TFLOP/s", "flops_per_iteration": 2.0 * lvl0["n"] * lvl0["k"] * D,
+                                     "peak": sustained, "frac": alg / sustained,
+                                     "peak_kind": ("measured" if "bf16_tflops_sustained" in peaks else "fallback")
+                                                  + " bf16_tflops_sustained"}},
+        "assemble_seconds": [r["assemble_seconds"] for r in rep],
         "clocks": clk.summary()}))
 
 

@@ -187,14 +187,36 @@ int tblaeq_set_timing(tblaeq_handle* h, int on);
  * Returns the number of stages written (at most cap), or -1 when timing is off. */
 int tblaeq_stage_times(tblaeq_handle* h, float* ms, int cap);
 
-/* Autotuner: times each expand-kernel variant (registers / cp.async shared-memory ring) on this
- * batch for every level and keeps the fastest per level (device queries, range batches).
- * variants_out (height entries) receives the choice and ms_out (height entries, may be NULL) the
- * median milliseconds of each chosen level. */
+/* Autotuner: times every launch shape (expand-kernel variant -- registers or a cp.async
+ * shared-memory ring -- times persistent-grid size, see tblaeq_set_launch_shapes) on this batch for
+ * every level and keeps the fastest per level (device queries, range batches). variants_out
+ * (height entries) receives the variants chosen, ms_out (height entries, may be NULL) the median
+ * milliseconds of each chosen level; tblaeq_get_launch_shapes returns the grid sizes too. */
 int tblaeq_autotune(tblaeq_handle* h, const tblaeq_batch* batch, int reps, int* variants_out, float* ms_out);
 
 /* Set the expand-kernel variant per level (0 = direct, 1 = staged), e.g. from a tuning cache. */
 int tblaeq_set_variants(tblaeq_handle* h, const int* variants, uint64_t n);
+
+/* ---- Launch shapes and the tuning cache (no counterpart in the reference, whose kernel shapes are
+ * compile-time constants: kCompact* in src/core/strategies/L0Strategy.cu:18-21, UNROLL_FACTOR in
+ * src/Kernel/SpMSpV.cuh:24) ----
+ * A launch shape per expand launch (one per mesh, `height` of them): the kernel variant (0 = direct,
+ * 1 = staged) and the persistent grid as a percentage (1..100) of the kernel's full occupancy.
+ * tblaeq_autotune searches variant x grid {100, 75, 50, 25}% per level on the live batch. */
+int tblaeq_set_launch_shapes(tblaeq_handle* h, const int* variants, const int* grid_percent, uint64_t n);
+int tblaeq_get_launch_shapes(tblaeq_handle* h, int* variants, int* grid_percent, uint64_t cap);
+
+/* The tuning-cache key of this handle for a range batch of nq queries in `mode`: the GPU model and
+ * SM count, the index shape (N, D, height, ratios), the mode and nq rounded up to a power of two.
+ * Written NUL-terminated into buf (cap bytes; TBLAEQ_ERR_INVALID when too small). */
+int tblaeq_tuning_key(tblaeq_handle* h, int mode, uint64_t nq, char* buf, uint64_t cap);
+
+/* The tuning cache is a versioned text file ("tblaeq-tuning-cache 1", then one line per key).
+ * tblaeq_tuning_store adds or replaces the key's shapes (n levels); tblaeq_tuning_lookup copies them
+ * out (*n = levels; *n = 0 when the file or the key is missing, TBLAEQ_ERR_INVALID when cap < levels). */
+int tblaeq_tuning_store(const char* path, const char* key, const int* variants, const int* grid_percent, uint64_t n);
+int tblaeq_tuning_lookup(const char* path, const char* key, int* variants, int* grid_percent, uint64_t cap,
+                         uint64_t* n);
 
 /* ---- Exact KNN tuning and the learned frontier scorer (no counterpart in the reference) ----
  * Exact KNN batches end with a two-wave finest level: each query's surviving finest clusters are

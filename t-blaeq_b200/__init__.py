@@ -150,6 +150,13 @@ def _load():
         "tblaeq_stage_times": ([vp, P(ctypes.c_float), ctypes.c_int], ctypes.c_int),
         "tblaeq_autotune": ([vp, P(_Batch), ctypes.c_int, P(ctypes.c_int), P(ctypes.c_float)], ctypes.c_int),
         "tblaeq_set_variants": ([vp, P(ctypes.c_int), ctypes.c_uint64], ctypes.c_int),
+        "tblaeq_set_launch_shapes": ([vp, P(ctypes.c_int), P(ctypes.c_int), ctypes.c_uint64], ctypes.c_int),
+        "tblaeq_get_launch_shapes": ([vp, P(ctypes.c_int), P(ctypes.c_int), ctypes.c_uint64], ctypes.c_int),
+        "tblaeq_tuning_key": ([vp, ctypes.c_int, ctypes.c_uint64, ctypes.c_char_p, ctypes.c_uint64], ctypes.c_int),
+        "tblaeq_tuning_store": ([ctypes.c_char_p, ctypes.c_char_p, P(ctypes.c_int), P(ctypes.c_int), ctypes.c_uint64],
+                                ctypes.c_int),
+        "tblaeq_tuning_lookup": ([ctypes.c_char_p, ctypes.c_char_p, P(ctypes.c_int), P(ctypes.c_int), ctypes.c_uint64,
+                                  P(ctypes.c_uint64)], ctypes.c_int),
         "tblaeq_set_two_wave": ([vp, ctypes.c_int], ctypes.c_int),
         "tblaeq_knn_counters": ([vp, P(ctypes.c_uint64)], ctypes.c_int),
         "tblaeq_scorer_train": ([vp, P(ctypes.c_double), ctypes.c_uint64, vp, ctypes.c_uint64, ctypes.c_uint64,
@@ -513,7 +520,8 @@ class QueryHandler:
         return list(e[:n]), list(it[:n]), int(r.value)
 
     def autotune(self, dqueries, mode: Mode = Mode.EXACT, reps: int = 5, flags: int = 0):
-        """Pick the fastest expand-kernel variant per level on this batch; returns (variants, ms)."""
+        """Search the launch shapes (variant x persistent-grid size) per level on this batch and keep
+        the fastest; returns (variants, ms)."""
         H = self.info()["height"]
         ptr = dqueries.__cuda_array_interface__["data"][0]
         b = _Batch(int(QueryType.RANGE), int(mode), int(dqueries.shape[0]), ptr, 1, 0, flags, None)
@@ -521,6 +529,37 @@ class QueryHandler:
         ms = (ctypes.c_float * H)()
         _check(_load().tblaeq_autotune(self._h, ctypes.byref(b), reps, v, ms))
         return list(v), list(ms)
+
+    def launch_shapes(self):
+        """(variants, grid percentages) per expand launch."""
+        H = self.info()["height"]
+        v, g = (ctypes.c_int * H)(), (ctypes.c_int * H)()
+        _check(_load().tblaeq_get_launch_shapes(self._h, v, g, H))
+        return list(v), list(g)
+
+    def set_launch_shapes(self, variants, grid_percent):
+        n = len(variants)
+        _check(_load().tblaeq_set_launch_shapes(self._h, (ctypes.c_int * n)(*variants),
+                                                (ctypes.c_int * n)(*grid_percent), n))
+
+    def tuning_key(self, mode: Mode, nq: int) -> str:
+        buf = ctypes.create_string_buffer(512)
+        _check(_load().tblaeq_tuning_key(self._h, int(mode), nq, buf, 512))
+        return buf.value.decode()
+
+    def autotune_cached(self, dqueries, cache_path: str, mode: Mode = Mode.EXACT, reps: int = 5, flags: int = 0):
+        """Launch shapes from the tuning cache when it holds this GPU, index shape, mode and batch
+        size; otherwise autotune on this batch and store the result. Returns (variants, grid
+        percentages, per-level ms or None when cached, "cache" | "tuned")."""
+        key = self.tuning_key(mode, int(dqueries.shape[0]))
+        hit = tuning_lookup(cache_path, key)
+        if hit is not None:
+            self.set_launch_shapes(*hit)
+            return hit[0], hit[1], None, "cache"
+        _, ms = self.autotune(dqueries, mode, reps, flags)
+        v, g = self.launch_shapes()
+        tuning_store(cache_path, key, v, g)
+        return v, g, ms, "tuned"
 
     def set_variants(self, variants):
         arr = (ctypes.c_int * len(variants))(*[int(x) for x in variants])
@@ -856,6 +895,21 @@ def load_query_file(path: str, q_type: QueryType):
                 raise ValueError(f"loadQueryFromFile: expected {cols} values at row {i + 1}")
             rows[i] = [float(v) for v in vals[:cols]]
     return rows, q_type
+
+
+def tuning_store(path: str, key: str, variants, grid_percent):
+    """Adds or replaces `key`'s launch shapes in the tuning-cache file at `path`."""
+    n = len(variants)
+    _check(_load().tblaeq_tuning_store(path.encode(), key.encode(), (ctypes.c_int * n)(*variants),
+                                       (ctypes.c_int * n)(*grid_percent), n))
+
+
+def tuning_lookup(path: str, key: str):
+    """(variants, grid percentages) stored for `key`, or None."""
+    cap = 64
+    v, g, n = (ctypes.c_int * cap)(), (ctypes.c_int * cap)(), ctypes.c_uint64()
+    _check(_load().tblaeq_tuning_lookup(path.encode(), key.encode(), v, g, cap, ctypes.byref(n)))
+    return None if n.value == 0 else (list(v[:n.value]), list(g[:n.value]))
 
 
 def set_device(device: int):

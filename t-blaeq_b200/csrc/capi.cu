@@ -11,6 +11,7 @@
 #include "scorer.hpp"
 #include "serve.hpp"
 #include "kmeans.cuh"
+#include "tuning.hpp"
 
 using namespace tblaeq;
 
@@ -473,6 +474,81 @@ int tblaeq_set_variants(tblaeq_handle* h, const int* variants, uint64_t n) {
     if (!variants) return fail(TBLAEQ_ERR_INVALID, "null variants");
     return guarded([&]() -> int {
         h->qh->runtime().engine->setVariants(std::vector<int>(variants, variants + n));
+        return TBLAEQ_OK;
+    });
+}
+
+int tblaeq_set_launch_shapes(tblaeq_handle* h, const int* variants, const int* grid_percent, uint64_t n) {
+    if (int c = checkPrepared(h)) return c;
+    if (!variants || !grid_percent) return fail(TBLAEQ_ERR_INVALID, "null launch shapes");
+    return guarded([&]() -> int {
+        h->qh->runtime().engine->setLaunchShapes(std::vector<int>(variants, variants + n),
+                                                 std::vector<int>(grid_percent, grid_percent + n));
+        return TBLAEQ_OK;
+    });
+}
+
+int tblaeq_get_launch_shapes(tblaeq_handle* h, int* variants, int* grid_percent, uint64_t cap) {
+    if (int c = checkPrepared(h)) return c;
+    if (!variants || !grid_percent) return fail(TBLAEQ_ERR_INVALID, "null output");
+    const BatchEngine& e = *h->qh->runtime().engine;
+    if (cap < e.variants().size()) return fail(TBLAEQ_ERR_INVALID, "output smaller than the index height");
+    for (size_t i = 0; i < e.variants().size(); ++i) {
+        variants[i] = e.variants()[i];
+        grid_percent[i] = e.gridPercents()[i];
+    }
+    return TBLAEQ_OK;
+}
+
+int tblaeq_tuning_key(tblaeq_handle* h, int mode, uint64_t nq, char* buf, uint64_t cap) {
+    if (!h || !h->qh) return fail(TBLAEQ_ERR_INVALID, "null handle");
+    if (!buf) return fail(TBLAEQ_ERR_INVALID, "null buffer");
+    return guarded([&]() -> int {
+        int dev = 0;
+        TBLAEQ_CUDA(cudaGetDevice(&dev));
+        cudaDeviceProp prop{};
+        TBLAEQ_CUDA(cudaGetDeviceProperties(&prop, dev));
+        const HostIndex& x = h->qh->index();
+        uint64_t bucket = 1;
+        while (bucket < nq) bucket <<= 1;
+        std::string key = std::string(prop.name) + "/" + std::to_string(prop.multiProcessorCount) + "sm|N=" +
+                          std::to_string(x.N) + "|D=" + std::to_string(x.D) + "|H=" + std::to_string(x.height) +
+                          "|ratios=";
+        for (size_t i = 0; i < x.ratios.size(); ++i) key += (i ? "," : "") + std::to_string(x.ratios[i]);
+        key += "|mode=" + std::to_string(mode) + "|nq=" + std::to_string(bucket);
+        for (char& c : key)
+            if (c == '\t' || c == '\n' || c == '\r') c = ' ';
+        if (key.size() + 1 > cap) return fail(TBLAEQ_ERR_INVALID, "key buffer too small");
+        std::memcpy(buf, key.c_str(), key.size() + 1);
+        return TBLAEQ_OK;
+    });
+}
+
+int tblaeq_tuning_store(const char* path, const char* key, const int* variants, const int* grid_percent, uint64_t n) {
+    if (!path || !key || !variants || !grid_percent) return fail(TBLAEQ_ERR_INVALID, "null argument");
+    return guarded([&]() -> int {
+        LaunchShapes s;
+        s.variants.assign(variants, variants + n);
+        s.gridPercent.assign(grid_percent, grid_percent + n);
+        tuningStore(path, key, s);
+        return TBLAEQ_OK;
+    });
+}
+
+int tblaeq_tuning_lookup(const char* path, const char* key, int* variants, int* grid_percent, uint64_t cap,
+                         uint64_t* n) {
+    if (!path || !key || !n) return fail(TBLAEQ_ERR_INVALID, "null argument");
+    return guarded([&]() -> int {
+        *n = 0;
+        LaunchShapes s;
+        if (!tuningLookup(path, key, s)) return TBLAEQ_OK;
+        if (cap < s.variants.size() || !variants || !grid_percent)
+            return fail(TBLAEQ_ERR_INVALID, "output smaller than the cached entry");
+        for (size_t i = 0; i < s.variants.size(); ++i) {
+            variants[i] = s.variants[i];
+            grid_percent[i] = s.gridPercent[i];
+        }
+        *n = s.variants.size();
         return TBLAEQ_OK;
     });
 }

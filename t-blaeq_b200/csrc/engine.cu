@@ -15,7 +15,16 @@ size_t align256(size_t v) { return (v + 255) & ~size_t(255); }
 
 BatchEngine::BatchEngine(const DeviceIndex& di, cudaStream_t stream)
     : di_(di), stream_(stream), tile_(expandTile(static_cast<int>(di.D))),
-      variants_(static_cast<size_t>(di.height), kVariantDirect) {}
+      variants_(static_cast<size_t>(di.height), kVariantDirect), grids_(static_cast<size_t>(di.height), 100) {}
+
+void BatchEngine::setLaunchShapes(const std::vector<int>& v, const std::vector<int>& g) {
+    if (g.size() != grids_.size()) throw std::invalid_argument("setLaunchShapes: one grid percentage per expand launch");
+    for (int x : g)
+        if (x < 1 || x > 100) throw std::invalid_argument("setLaunchShapes: grid percentage must be in [1, 100]");
+    setVariants(v);
+    if (g != grids_) dropGraph();
+    grids_ = g;
+}
 
 void BatchEngine::setVariants(const std::vector<int>& v) {
     if (v.size() != variants_.size()) throw std::invalid_argument("setVariants: one variant per expand launch");
@@ -30,10 +39,15 @@ std::vector<float> BatchEngine::autotuneRange(const double* dBoxes, uint32_t nq,
     const bool wasTiming = timing_;
     setTiming(true);
     runRange(dBoxes, nq, mode, flags & ~kUseGraph);  // sizes the workspace
-    const std::vector<int> candidates{kVariantDirect, kVariantStaged};
+    struct Shape {
+        int variant, grid;
+    };
+    std::vector<Shape> candidates;
+    for (int v : {kVariantDirect, kVariantStaged})
+        for (int g : {100, 75, 50, 25}) candidates.push_back({v, g});
     std::vector<std::vector<float>> med(candidates.size(), std::vector<float>(H, 0.f));
     for (size_t c = 0; c < candidates.size(); ++c) {
-        setVariants(std::vector<int>(H, candidates[c]));
+        setLaunchShapes(std::vector<int>(H, candidates[c].variant), std::vector<int>(H, candidates[c].grid));
         enqueueRange(dBoxes, nq, mode, flags & ~kUseGraph);
         status();
         std::vector<std::vector<float>> samples(H);
@@ -48,16 +62,17 @@ std::vector<float> BatchEngine::autotuneRange(const double* dBoxes, uint32_t nq,
             med[c][m] = samples[m][samples[m].size() / 2];
         }
     }
-    std::vector<int> best(H, kVariantDirect);
+    std::vector<int> best(H, kVariantDirect), bestG(H, 100);
     std::vector<float> bestT(H, 0.f);
     for (int m = 0; m < H; ++m) {
         size_t bi = 0;
         for (size_t c = 1; c < candidates.size(); ++c)
             if (med[c][m] < med[bi][m]) bi = c;
-        best[m] = candidates[bi];
+        best[m] = candidates[bi].variant;
+        bestG[m] = candidates[bi].grid;
         bestT[m] = med[bi][m];
     }
-    setVariants(best);
+    setLaunchShapes(best, bestG);
     setTiming(wasTiming);
     return bestT;
 }
@@ -314,6 +329,7 @@ void BatchEngine::enqueueLaunches(const double* dBoxes, uint32_t nq, int mode, u
         a.D = D;
         a.useFma = 1;
         a.variant = variants_[m];
+        a.gridPercent = grids_[m];
         if (m < H - 1) {
             a.child.nodes = (mode == kModeExact) ? di_.nodeSub[m].as<NodeRec>() : di_.nodeRef[m].as<NodeRec>();
             a.child.aabb = (mode == kModeExact) ? di_.aabb[m].as<float>() : nullptr;

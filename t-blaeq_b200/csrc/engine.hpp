@@ -93,8 +93,13 @@ public:
     // Kernel variant (Variant) per expand launch m = 0..height-1; default direct everywhere.
     void setVariants(const std::vector<int>& v);
     const std::vector<int>& variants() const { return variants_; }
-    // Times every variant on this batch (median of `reps` runs per variant after a warm-up) and
-    // keeps the fastest per level. Returns the per-level median milliseconds of the choice.
+    // Launch shape per expand launch: the variant and the persistent grid as a percentage of full
+    // occupancy (gridPercent of ExpandArgs; 100 = every CTA the SMs hold).
+    void setLaunchShapes(const std::vector<int>& variants, const std::vector<int>& gridPercent);
+    const std::vector<int>& gridPercents() const { return grids_; }
+    // Searches the launch shapes on this batch: every combination of variant {direct, staged} and
+    // grid {100, 75, 50, 25}% is timed (median of `reps` runs after a warm-up) and each level keeps
+    // its fastest. Returns the per-level median milliseconds of the choice.
     std::vector<float> autotuneRange(const double* dBoxes, uint32_t nq, int mode, unsigned flags, int reps);
 
     // (entries, items) of every frontier header of the last batch, and the result count.
@@ -164,6 +169,7 @@ private:
     EntryScorer scorer_ = nullptr;
     void* scorerCtx_ = nullptr;
     std::vector<int> variants_;
+    std::vector<int> grids_;
     void record(int i);
     std::vector<cudaEvent_t> events_;
     cudaGraphExec_t graphExec_ = nullptr;

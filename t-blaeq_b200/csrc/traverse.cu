@@ -1019,7 +1019,10 @@ void launchOne(const ExpandArgs& a, int gridBlocks, cudaStream_t s) {
         TBLAEQ_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, kern, kExpandThreads, smemBytes));
         cached = std::max(1, sms * std::max(1, perSm));
     }
-    if (gridBlocks <= 0) gridBlocks = cached;
+    if (gridBlocks <= 0) {
+        const int pct = (a.gridPercent > 0 && a.gridPercent < 100) ? a.gridPercent : 100;
+        gridBlocks = std::max(1, static_cast<int>((static_cast<long long>(cached) * pct + 99) / 100));
+    }
     kern<<<gridBlocks, kExpandThreads, smemBytes, s>>>(a);
     TBLAEQ_CUDA(cudaGetLastError());
 }

@@ -144,6 +144,10 @@ struct ExpandArgs {
     // give up after `spinLimit` polls (0: the default limit).
     uint32_t withholdTile;
     uint32_t spinLimit;
+    // Persistent grid as a percentage of the instantiation's full occupancy (resident CTAs per SM x
+    // SMs); 0 means 100. An autotuner knob: fewer resident warps contend less on the tile ticket and
+    // the look-back, more hide more memory latency.
+    int gridPercent;
 };
 
 // Launch the expand kernel for dimension D with the given predicate; `toResult` selects the

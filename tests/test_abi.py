@@ -151,3 +151,27 @@ def test_noalloc_rejects_a_grid_of_another_dimension(tb):
     code = lib.tblaeq_level_range_noalloc(h._h, ctypes.c_uint64(0), ctypes.byref(g), lo, hi,
                                           None, None, ctypes.c_uint64(0), ctypes.byref(n))
     assert code == 7
+
+
+def test_tuning_cache_round_trip(tb, tmp_path):
+    """The autotuner's cache file: versioned, one line per key, entries added and replaced, other
+    keys kept, a file of another format ignored and then replaced."""
+    path = str(tmp_path / "tuning.txt")
+    assert tb.tuning_lookup(path, "gpu|N=1") is None            # no file yet
+    tb.tuning_store(path, "gpu|N=1", [0, 1, 0, 0], [100, 75, 50, 25])
+    tb.tuning_store(path, "gpu|N=2", [1, 1, 0], [25, 25, 100])
+    assert tb.tuning_lookup(path, "gpu|N=1") == ([0, 1, 0, 0], [100, 75, 50, 25])
+    assert tb.tuning_lookup(path, "gpu|N=2") == ([1, 1, 0], [25, 25, 100])
+    tb.tuning_store(path, "gpu|N=1", [1, 0, 0, 1], [50, 50, 50, 50])  # replaced, the other kept
+    assert tb.tuning_lookup(path, "gpu|N=1") == ([1, 0, 0, 1], [50, 50, 50, 50])
+    assert tb.tuning_lookup(path, "gpu|N=2") == ([1, 1, 0], [25, 25, 100])
+    lines = open(path).read().splitlines()
+    assert lines[0] == "tblaeq-tuning-cache 1" and len(lines) == 3
+    assert tb.tuning_lookup(path, "gpu|N=3") is None
+    with open(path, "w") as f:
+        f.write("some-other-format 7\ngpu|N=1\t4\t0:100,0:100,0:100,0:100\n")
+    assert tb.tuning_lookup(path, "gpu|N=1") is None             # another format is not read
+    tb.tuning_store(path, "gpu|N=9", [0, 0], [100, 100])
+    assert open(path).read().splitlines()[0] == "tblaeq-tuning-cache 1"
+    with pytest.raises(tb.TblaeqError):
+        tb.tuning_store(path, "bad\tkey", [0], [100])

@@ -250,3 +250,26 @@ def test_lookback_timeout_is_reported_and_the_handle_recovers(tb, env, oracle_mo
     assert n_mesh1 == h.info()["meshSizes"][2]
     g2 = h.run_level(1, grid, tb.QueryType.RANGE, lo=lo, hi=hi)
     assert g2.nnz == h.info()["meshSizes"][1]
+
+
+def test_autotuned_launch_shapes_keep_results_and_round_trip(tb, env, oracle_mod, tmp_path):
+    """Every launch shape the autotuner searches (variant x persistent grid size) returns the same
+    exact results; the chosen shapes go to the tuning cache and come back on the next lookup."""
+    import torch
+    h, o, pts, ids = env
+    Q = _boxes(pts, 256, 21)
+    dQ = torch.from_numpy(Q).cuda()
+    b = oracle_mod.brute_query(pts, ids, oracle_mod.RANGE, Q)
+    H = h.info()["height"]
+    for v, g in ((0, 25), (1, 50), (0, 75), (1, 100)):
+        h.set_launch_shapes([v] * H, [g] * H)
+        r, offs, got = _batch_ids(tb, h, dQ, tb.Mode.EXACT)
+        assert np.array_equal(offs, b.offsets), (v, g)
+        assert all(np.array_equal(a, c) for a, c in zip(ids_by_query(offs, got), [b.query(q) for q in range(len(Q))]))
+    cache = str(tmp_path / "tuning.txt")
+    v1, g1, ms, src = h.autotune_cached(dQ, cache, tb.Mode.EXACT, reps=2)
+    assert src == "tuned" and len(v1) == len(g1) == H and all(x in (25, 50, 75, 100) for x in g1)
+    h.set_launch_shapes([0] * H, [100] * H)
+    v2, g2, _, src2 = h.autotune_cached(dQ, cache, tb.Mode.EXACT, reps=2)
+    assert src2 == "cache" and (v2, g2) == (v1, g1) and h.launch_shapes() == (v1, g1)
+    h.set_launch_shapes([0] * H, [100] * H)
