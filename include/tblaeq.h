@@ -197,6 +197,11 @@ int tblaeq_autotune(tblaeq_handle* h, const tblaeq_batch* batch, int reps, int* 
 /* Set the expand-kernel variant per level (0 = direct, 1 = staged), e.g. from a tuning cache. */
 int tblaeq_set_variants(tblaeq_handle* h, const int* variants, uint64_t n);
 
+/* Exact range batches test their inner levels node-major (1, the default: one warp per node and 32
+ * of the queries holding it) or entry-major (0: one work item per query and child). Same results;
+ * node-major returns each query's ids in no particular order. No counterpart in the reference. */
+int tblaeq_set_node_major(tblaeq_handle* h, int on);
+
 /* ---- Launch shapes and the tuning cache (no counterpart in the reference, whose kernel shapes are
  * compile-time constants: kCompact* in src/core/strategies/L0Strategy.cu:18-21, UNROLL_FACTOR in
  * src/Kernel/SpMSpV.cuh:24) ----

@@ -150,6 +150,7 @@ def _load():
         "tblaeq_stage_times": ([vp, P(ctypes.c_float), ctypes.c_int], ctypes.c_int),
         "tblaeq_autotune": ([vp, P(_Batch), ctypes.c_int, P(ctypes.c_int), P(ctypes.c_float)], ctypes.c_int),
         "tblaeq_set_variants": ([vp, P(ctypes.c_int), ctypes.c_uint64], ctypes.c_int),
+        "tblaeq_set_node_major": ([vp, ctypes.c_int], ctypes.c_int),
         "tblaeq_set_launch_shapes": ([vp, P(ctypes.c_int), P(ctypes.c_int), ctypes.c_uint64], ctypes.c_int),
         "tblaeq_get_launch_shapes": ([vp, P(ctypes.c_int), P(ctypes.c_int), ctypes.c_uint64], ctypes.c_int),
         "tblaeq_tuning_key": ([vp, ctypes.c_int, ctypes.c_uint64, ctypes.c_char_p, ctypes.c_uint64], ctypes.c_int),
@@ -529,6 +530,10 @@ class QueryHandler:
         ms = (ctypes.c_float * H)()
         _check(_load().tblaeq_autotune(self._h, ctypes.byref(b), reps, v, ms))
         return list(v), list(ms)
+
+    def set_node_major(self, on: bool = True):
+        """Exact range batches: node-major inner levels (default) or entry-major."""
+        _check(_load().tblaeq_set_node_major(self._h, int(on)))
 
     def launch_shapes(self):
         """(variants, grid percentages) per expand launch."""

@@ -478,6 +478,12 @@ int tblaeq_set_variants(tblaeq_handle* h, const int* variants, uint64_t n) {
     });
 }
 
+int tblaeq_set_node_major(tblaeq_handle* h, int on) {
+    if (int c = checkPrepared(h)) return c;
+    h->qh->runtime().engine->setNodeMajor(on != 0);
+    return TBLAEQ_OK;
+}
+
 int tblaeq_set_launch_shapes(tblaeq_handle* h, const int* variants, const int* grid_percent, uint64_t n) {
     if (int c = checkPrepared(h)) return c;
     if (!variants || !grid_percent) return fail(TBLAEQ_ERR_INVALID, "null launch shapes");

@@ -142,7 +142,9 @@ uint64_t BatchEngine::lastTotal(uint32_t nq) {
 
 size_t BatchEngine::workspaceBytes() const {
     size_t t = zeroBlock_.bytes() + offsets_.bytes() + resIds_.bytes() + resVals_.bytes() + resQ_.bytes() +
-               resDist_.bytes();
+               resDist_.bytes() + v_.q.bytes() + v_.cbeg.bytes() + v_.cpre.bytes() + v_.x.bytes() +
+               v_.tileStart.bytes() + nmList_.bytes() + nmNodeOff_.bytes() + nmUnitOff_.bytes() + rawIds_.bytes() +
+               rawQ_.bytes() + rawVals_.bytes();
     for (const auto& f : f_) t += f.q.bytes() + f.node.bytes() + f.cbeg.bytes() + f.cpre.bytes() + f.x.bytes() +
                                   f.tileStart.bytes();
     return t;
@@ -236,6 +238,17 @@ void BatchEngine::reserve(const EngineCaps& want, uint32_t nq, unsigned flags) {
         off = align256(off + static_cast<size_t>(qcap_) * 4);
         offWork_ = off;
         off = align256(off + 2 * 8);
+        // Node-major range levels: a unit ticket and a survivor count per level, the per-node entry
+        // counts and cursors of every inner level, and the per-query result cursors.
+        offNm_ = off;
+        off = align256(off + 2 * H * 4);
+        offNodeCnt_.assign(H, 0);
+        for (uint64_t m = 1; m + 1 < H; ++m) {
+            offNodeCnt_[m] = off;
+            off = align256(off + 2 * di_.meshCount[m - 1] * 4);
+        }
+        offRcursor_ = off;
+        off = align256(off + static_cast<size_t>(qcap_) * 4);
         zeroBytes_ = off;
         zeroBlock_.alloc(zeroBytes_);
         offsets_.alloc((static_cast<size_t>(qcap_) + 1) * 8);
@@ -294,6 +307,111 @@ void BatchEngine::enqueueRange(const double* dBoxes, uint32_t nq, int mode, unsi
     TBLAEQ_CUDA(cudaGraphLaunch(graphExec_, stream_));
 }
 
+bool BatchEngine::useNodeMajor(int mode) const {
+    if (!nodeMajor_ || mode != kModeExact || di_.height < 2) return false;
+    for (uint64_t m = 0; m + 1 < di_.height; ++m)
+        if (!di_.aabb[m].bytes()) return false;
+    return true;
+}
+
+void BatchEngine::reserveNodeMajor(unsigned flags) {
+    const uint64_t D = di_.D;
+    if (nmEntryCap_ < caps_.entries || v_.tileStart.bytes() < tileCap_ * 4) {
+        dropGraph();
+        v_.q.alloc(caps_.entries * 4);
+        v_.cbeg.alloc(caps_.entries * 4);
+        v_.cpre.alloc(caps_.entries * 4);
+        v_.x.alloc(caps_.entries * D * 8);
+        v_.tileStart.alloc(tileCap_ * 4);
+        nmList_.alloc(caps_.entries * 4);
+        uint64_t maxM = 1;
+        for (uint64_t m = 0; m + 2 < di_.height; ++m) maxM = std::max<uint64_t>(maxM, di_.meshCount[m]);
+        nmNodeOff_.alloc((maxM + 1) * 4);
+        nmUnitOff_.alloc((maxM + 1) * 4);
+        nmEntryCap_ = caps_.entries;
+    }
+    const bool vals = (flags & kWantVals) != 0;
+    if (nmResultCap_ < caps_.results || (vals && !nmVals_)) {
+        dropGraph();
+        rawIds_.alloc(caps_.results * 8);
+        rawQ_.alloc(caps_.results * 4);
+        if (vals || nmVals_) {
+            rawVals_.alloc(caps_.results * D * 8);
+            nmVals_ = true;
+        }
+        nmResultCap_ = caps_.results;
+    }
+}
+
+// Level m of an exact range batch, node-major: group frontier `buf` by node (m >= 1), test every
+// node's children against the query boxes holding it (survivors into v_), then expand v_ with
+// kPredAll into the next frontier (1 - buf).
+void BatchEngine::enqueueNodeMajorLevel(int m, int buf, const double* dBoxes, uint32_t nq, bool wantLevels) {
+    const int D = static_cast<int>(di_.D);
+    char* z = zeroBlock_.as<char>();
+    auto* nmTicket = reinterpret_cast<uint32_t*>(z + offNm_);
+    auto* nmCount = nmTicket + di_.height;
+    auto* status = reinterpret_cast<uint32_t*>(z + offStatus_);
+    const FrontierBufs& in = f_[buf];
+    NodeMajorArgs n{};
+    n.inQ = in.q.as<uint32_t>();
+    n.inX = in.x.as<double>();
+    n.inHdr = hdrPtr(m);
+    n.inCap = static_cast<uint32_t>(caps_.entries);
+    if (m == 0) {
+        n.nNodes = 0;
+        n.rootChildren = static_cast<uint32_t>(di_.meshCount[0]);
+    } else {
+        const uint32_t M = static_cast<uint32_t>(di_.meshCount[m - 1]);
+        auto* nodeCnt = reinterpret_cast<uint32_t*>(z + offNodeCnt_[m]);
+        launchNodeTranspose(in.node.as<uint32_t>(), hdrPtr(m), n.inCap, M, nodeCnt, nmNodeOff_.as<uint32_t>(),
+                            nmUnitOff_.as<uint32_t>(), nodeCnt + M, nmList_.as<uint32_t>(), stream_);
+        n.list = nmList_.as<uint32_t>();
+        n.nodeOff = nmNodeOff_.as<uint32_t>();
+        n.unitOff = nmUnitOff_.as<uint32_t>();
+        n.nNodes = M;
+        n.parents = di_.nodeSub[m - 1].as<NodeRec>();
+    }
+    n.rows = (m == 0) ? di_.coarseVals.as<double>() : di_.rows[m - 1];
+    n.rowsOnHost = (m == 0) ? 0 : di_.rowsOnHost[m - 1];
+    n.aabb = di_.aabb[m].as<float>();
+    n.children = di_.nodeSub[m].as<NodeRec>();
+    n.boxes = dBoxes;
+    n.boxesF = boxF_.as<float>();
+    n.vq = v_.q.as<uint32_t>();
+    n.vcbeg = v_.cbeg.as<uint32_t>();
+    n.vcpre = v_.cpre.as<uint32_t>();
+    n.vx = v_.x.as<double>();
+    n.vtile = v_.tileStart.as<uint32_t>();
+    n.vcap = static_cast<uint32_t>(caps_.entries);
+    n.vtileCap = static_cast<uint32_t>(tileCap_);
+    n.vcount = nmCount + m;
+    n.ticket = nmTicket + m;
+    n.status = status;
+    n.levelItems = (wantLevels && m > 0)
+                       ? reinterpret_cast<uint32_t*>(z + offLevels_) + static_cast<size_t>(m - 1) * nq
+                       : nullptr;
+    n.D = D;
+    launchNodeMajorRange(n, grids_[m], stream_);
+    uint32_t* vHdr = hdrPtr(static_cast<int>(di_.height) + 2);
+    launchOneItemHeader(nmCount + m, vHdr, stream_);
+    ExpandArgs a{};
+    a.in = FrontierIn{v_.q.as<uint32_t>(),         v_.cbeg.as<uint32_t>(), v_.cpre.as<uint32_t>(), v_.x.as<double>(),
+                      v_.tileStart.as<uint32_t>(), vHdr,                   n.vcap,                  n.vtileCap};
+    a.child.rows = n.rows;
+    a.child.rowsOnHost = n.rowsOnHost;
+    a.child.nodes = n.children;
+    a.fout = outView(1 - buf, hdrPtr(m + 1));
+    a.scratch.desc = reinterpret_cast<unsigned long long*>(z + offDesc_) + static_cast<size_t>(m) * tileCap_;
+    a.scratch.ticket = reinterpret_cast<uint32_t*>(z + offTickets_) + m;
+    a.scratch.status = status;
+    a.D = D;
+    a.useFma = 1;
+    a.variant = variants_[m];
+    a.gridPercent = grids_[m];
+    launchExpand(a, kPredAll, false, 0, stream_);
+}
+
 void BatchEngine::enqueueLaunches(const double* dBoxes, uint32_t nq, int mode, unsigned flags) {
     lastKnn_ = false;
     const int H = static_cast<int>(di_.height);
@@ -314,8 +432,18 @@ void BatchEngine::enqueueLaunches(const double* dBoxes, uint32_t nq, int mode, u
                        stream_);
     if (mode == kModeExact) launchRoundBoxes(dBoxes, nq, D, boxF_.as<float>(), stream_);
     if (timing_) record(1);
+    // Node-major levels need their buffers at the current capacities (sized by the synchronous
+    // batch that must precede asynchronous ones); without them the batch runs entry-major.
+    const bool nodeMajor = useNodeMajor(mode) && nmEntryCap_ >= caps_.entries && nmResultCap_ >= caps_.results &&
+                           v_.tileStart.bytes() >= tileCap_ * 4 && (!(flags & kWantVals) || nmVals_);
     int buf = 0;
     for (int m = 0; m < H; ++m) {
+        if (nodeMajor && m < H - 1) {
+            enqueueNodeMajorLevel(m, buf, dBoxes, nq, wantLevels);
+            buf = 1 - buf;
+            if (timing_) record(2 + m);
+            continue;
+        }
         ExpandArgs a{};
         a.in = inView(buf, hdrPtr(m));
         a.child.rows = (m == 0) ? di_.coarseVals.as<double>() : di_.rows[m - 1];
@@ -338,16 +466,30 @@ void BatchEngine::enqueueLaunches(const double* dBoxes, uint32_t nq, int mode, u
             buf = 1 - buf;
         } else {
             a.child.outMap = di_.mapPtr[H - 1];
-            a.rout.ids = resIds_.as<uint64_t>();
-            a.rout.vals = (flags & kWantVals) ? resVals_.as<double>() : nullptr;
             a.rout.qcount = qcount;
             a.rout.hdr = hdrPtr(H);
             a.rout.cap = static_cast<uint32_t>(caps_.results);
+            if (nodeMajor) {
+                // The frontier is in no particular query order: results go out raw, with their query,
+                // and are grouped by query below.
+                a.rout.ids = rawIds_.as<uint64_t>();
+                a.rout.q = rawQ_.as<uint32_t>();
+                a.rout.vals = (flags & kWantVals) ? rawVals_.as<double>() : nullptr;
+            } else {
+                a.rout.ids = resIds_.as<uint64_t>();
+                a.rout.vals = (flags & kWantVals) ? resVals_.as<double>() : nullptr;
+            }
             launchExpand(a, (mode == kModeExact) ? kPredRangeBox : kPredAll, true, 0, stream_);
         }
         if (timing_) record(2 + m);
     }
     launchExclusiveScan(qcount, offsets_.as<uint64_t>(), nq, stream_);
+    if (nodeMajor)
+        launchGroupResults(rawIds_.as<uint64_t>(), rawQ_.as<uint32_t>(),
+                           (flags & kWantVals) ? rawVals_.as<double>() : nullptr, hdrPtr(H),
+                           static_cast<uint32_t>(caps_.results), D, offsets_.as<uint64_t>(),
+                           reinterpret_cast<uint32_t*>(z + offRcursor_), resIds_.as<uint64_t>(),
+                           (flags & kWantVals) ? resVals_.as<double>() : nullptr, stream_);
     if (timing_) record(2 + H);
 }
 
@@ -386,6 +528,26 @@ void BatchEngine::growFromHeaders() {
         if (items > caps_.items) {
             want.items = std::max<uint64_t>(want.items, items + items / 4 + 4096);
             grew = true;
+        }
+    }
+    // Node-major levels: the survivors of level lv form a frontier of one item per entry.
+    {
+        std::vector<uint32_t> nm(H, 0);
+        TBLAEQ_CUDA(cudaMemcpyAsync(nm.data(), zeroBlock_.as<char>() + offNm_ + H * 4, H * 4, cudaMemcpyDeviceToHost,
+                                    stream_));
+        TBLAEQ_CUDA(cudaStreamSynchronize(stream_));
+        for (int lv = 0; lv < H; ++lv) {
+            const uint64_t c = nm[lv];
+            if (c > splitLimit_)
+                throw SplitBatch("level " + std::to_string(lv) + " exceeds the traversal limit; split the batch");
+            if (c > caps_.entries) {
+                want.entries = std::max<uint64_t>(want.entries, c + c / 4 + 1024);
+                grew = true;
+            }
+            if (c > caps_.items || c / kWarpTile + 2 > tileCap_) {
+                want.items = std::max<uint64_t>(want.items, c + c / 4 + 4096);
+                grew = true;
+            }
         }
     }
     // Results: slot H holds the one-pass (or wave-1) results, slot H+1 the wave-2 results of a
@@ -434,6 +596,7 @@ BatchOutput BatchEngine::output(uint32_t nq, unsigned flags) const {
 BatchOutput BatchEngine::runRange(const double* dBoxes, uint32_t nq, int mode, unsigned flags) {
     reserve(caps_, nq, flags);
     for (int attempt = 0; attempt < 16; ++attempt) {
+        if (useNodeMajor(mode)) reserveNodeMajor(flags);
         enqueueRange(dBoxes, nq, mode, flags);
         // The status word and the result total come back together: one host synchronisation.
         uint32_t st = 0;

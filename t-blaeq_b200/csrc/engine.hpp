@@ -59,6 +59,13 @@ public:
     void setTwoWave(bool on) { twoWave_ = on; }
     // Largest entry / item capacity a batch may use before it must be split (tests lower it).
     void setSplitLimit(uint64_t limit) { splitLimit_ = limit; }
+    // Exact range batches test the inner levels node-major (default on; see NodeMajorArgs): same
+    // results, each query's ids in no particular order. Off: the entry-major kernel at every level.
+    void setNodeMajor(bool on) {
+        if (on != nodeMajor_) dropGraph();
+        nodeMajor_ = on;
+    }
+    bool nodeMajor() const { return nodeMajor_; }
     bool twoWave() const { return twoWave_; }
     // Optional device scorer of the last frontier's entries (higher = expand earlier); when unset
     // the entries are ranked by their lower bound. Called with (frontier, hdr, cap, points, out scores).
@@ -137,6 +144,18 @@ private:
     uint32_t qcap_ = 0;
     bool haveVals_ = false;
     FrontierBufs f_[2];
+    // Node-major range levels: the one-item-per-entry survivor frontier, the node grouping of the
+    // input frontier, and the raw (frontier-order) results before they are grouped by query.
+    bool nodeMajor_ = true;
+    FrontierBufs v_;
+    DeviceMem nmNodeOff_, nmUnitOff_, nmList_, rawIds_, rawQ_, rawVals_;
+    uint64_t nmEntryCap_ = 0, nmResultCap_ = 0;
+    bool nmVals_ = false;
+    size_t offNm_ = 0, offRcursor_ = 0;
+    std::vector<size_t> offNodeCnt_;  // per level m: nodeCnt then cursor (meshCount[m-1] each), in zeroBlock_
+    void reserveNodeMajor(unsigned flags);
+    bool useNodeMajor(int mode) const;
+    void enqueueNodeMajorLevel(int m, int buf, const double* dBoxes, uint32_t nq, bool wantLevels);
     DeviceMem resIds_, resVals_, resQ_, resDist_;
     DeviceMem zeroBlock_;  // desc | tickets | status | hdrs | qcount | levelItems
     uint64_t splitLimit_ = 0xffffffffull;

@@ -1122,4 +1122,291 @@ void launchExclusiveScan(const uint32_t* counts, uint64_t* offsets, uint32_t n, 
     TBLAEQ_CUDA(cudaGetLastError());
 }
 
+// ---- node-major range levels (exact mode) -------------------------------------------------------
+
+namespace {
+
+// Node keys at or above M (only an inconsistent frontier has them) are skipped by the count and the
+// scatter alike, so the grouping stays within its arrays.
+__global__ void nodeCountKernel(const uint32_t* node, const uint32_t* hdr, uint32_t cap, uint32_t M,
+                                uint32_t* nodeCnt) {
+    const uint32_t n = min(hdr[0], cap);
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const uint32_t nd = node[i];
+        if (nd < M) atomicAdd(&nodeCnt[nd], 1u);
+    }
+}
+
+// One CTA: nodeOff = exclusive scan of the entry counts, unitOff = exclusive scan of their units of 32.
+__global__ void __launch_bounds__(1024) nodeScanKernel(const uint32_t* nodeCnt, uint32_t M, uint32_t* nodeOff,
+                                                       uint32_t* unitOff) {
+    __shared__ uint32_t sWarpA[32], sWarpB[32];
+    __shared__ uint32_t sCarryA, sCarryB;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    if (tid == 0) {
+        sCarryA = 0;
+        sCarryB = 0;
+    }
+    __syncthreads();
+    for (uint32_t base = 0; base < M; base += blockDim.x) {
+        const uint32_t i = base + tid;
+        const uint32_t va = i < M ? nodeCnt[i] : 0u;
+        const uint32_t vb = (va + 31u) / 32u;
+        uint32_t ia = va, ib = vb;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t ta = __shfl_up_sync(0xffffffffu, ia, o), tb = __shfl_up_sync(0xffffffffu, ib, o);
+            if (lane >= o) {
+                ia += ta;
+                ib += tb;
+            }
+        }
+        if (lane == 31) {
+            sWarpA[warp] = ia;
+            sWarpB[warp] = ib;
+        }
+        __syncthreads();
+        if (warp == 0) {
+            const int nw = blockDim.x / 32;
+            uint32_t wa = lane < nw ? sWarpA[lane] : 0u, wb = lane < nw ? sWarpB[lane] : 0u;
+            uint32_t xa = wa, xb = wb;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const uint32_t ta = __shfl_up_sync(0xffffffffu, xa, o), tb = __shfl_up_sync(0xffffffffu, xb, o);
+                if (lane >= o) {
+                    xa += ta;
+                    xb += tb;
+                }
+            }
+            if (lane < nw) {
+                sWarpA[lane] = xa - wa;
+                sWarpB[lane] = xb - wb;
+            }
+        }
+        __syncthreads();
+        const uint32_t ca = sCarryA, cb = sCarryB;
+        if (i < M) {
+            nodeOff[i] = ca + sWarpA[warp] + ia - va;
+            unitOff[i] = cb + sWarpB[warp] + ib - vb;
+        }
+        __syncthreads();
+        if (tid == static_cast<int>(blockDim.x) - 1) {
+            sCarryA = ca + sWarpA[warp] + ia;
+            sCarryB = cb + sWarpB[warp] + ib;
+        }
+        __syncthreads();
+    }
+    if (tid == 0) {
+        nodeOff[M] = sCarryA;
+        unitOff[M] = sCarryB;
+    }
+}
+
+__global__ void nodeScatterKernel(const uint32_t* node, const uint32_t* hdr, uint32_t cap, uint32_t M,
+                                  const uint32_t* nodeOff, uint32_t* cursor, uint32_t* list) {
+    const uint32_t n = min(hdr[0], cap);
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const uint32_t nd = node[i];
+        if (nd < M) list[nodeOff[nd] + atomicAdd(&cursor[nd], 1u)] = i;
+    }
+}
+
+constexpr int kNodeMajorThreads = 128;
+
+// One warp per unit (a node and up to 32 of the entries holding it), claimed through a ticket.
+// Lanes hold one query box each; the loop runs over the node's children with a warp-uniform
+// trip count, so every child's float box is one broadcast load for the whole warp.
+template <int D>
+__global__ void __launch_bounds__(kNodeMajorThreads) nodeMajorRangeKernel(NodeMajorArgs a) {
+    constexpr uint32_t FULL = 0xffffffffu;
+    constexpr int DM = D > 0 ? D : 32;
+    if (*a.status & (kStatusLookbackTimeout | kStatusWindowOverflow)) return;
+    const int dim = D > 0 ? D : a.D;
+    const int lane = threadIdx.x & 31;
+    const uint32_t lanesLt = (1u << lane) - 1u;
+    if (a.inHdr[0] > a.inCap) {
+        if (blockIdx.x == 0 && threadIdx.x == 0) atomicOr(a.status, kStatusOverflowEntries);
+        return;
+    }
+    const uint32_t entries = a.inHdr[0];
+    const bool root = a.nNodes == 0;
+    const uint32_t units = root ? (entries + 31u) / 32u : a.unitOff[a.nNodes];
+    while (true) {
+        uint32_t u = 0;
+        if (lane == 0) u = atomicAdd(a.ticket, 1u);
+        u = __shfl_sync(FULL, u, 0);
+        if (u >= units) break;
+        uint32_t base, count, cbeg, cnt;
+        if (root) {
+            base = u * 32u;
+            count = min(32u, entries - base);
+            cbeg = 0;
+            cnt = a.rootChildren;
+        } else {
+            uint32_t lo = 0, hi = a.nNodes - 1;  // the node whose units hold u: last unitOff[n] <= u
+            while (lo < hi) {
+                const uint32_t mid = (lo + hi + 1) >> 1;
+                if (__ldg(a.unitOff + mid) <= u) lo = mid; else hi = mid - 1;
+            }
+            base = __ldg(a.nodeOff + lo) + (u - __ldg(a.unitOff + lo)) * 32u;
+            count = min(32u, __ldg(a.nodeOff + lo + 1) - base);
+            const NodeRec pr = a.parents[lo];
+            cbeg = pr.cbeg;
+            cnt = pr.cnt;
+        }
+        const bool active = static_cast<uint32_t>(lane) < count;
+        uint32_t e = 0, q = 0;
+        if (active) {
+            e = root ? base + lane : __ldg(a.list + base + lane);
+            q = __ldg(a.inQ + e);
+            if (a.levelItems) atomicAdd(&a.levelItems[q], cnt);
+        }
+        // Every entry of the node carries the node's coordinates: take the first one's.
+        const double* xp = a.inX + static_cast<size_t>(__shfl_sync(FULL, e, 0)) * dim;
+        float ql[DM], qh[DM];
+        {
+            const float* f = a.boxesF + static_cast<size_t>(q) * 2 * dim;
+#pragma unroll
+            for (int d = 0; d < DM; ++d) {
+                if (D > 0 || d < dim) {
+                    ql[d] = active ? __ldg(f + d) : 0.f;
+                    qh[d] = active ? __ldg(f + dim + d) : -1.f;
+                }
+            }
+        }
+        for (uint32_t c = 0; c < cnt; ++c) {
+            const uint32_t j = cbeg + c;
+            const float* b = a.aabb + static_cast<size_t>(j) * 2 * dim;
+            bool pass = active;
+#pragma unroll
+            for (int d = 0; d < DM; ++d)
+                if (D > 0 || d < dim) pass = pass && __ldg(b + d) <= qh[d] && __ldg(b + dim + d) >= ql[d];
+            if (__ballot_sync(FULL, pass) == 0) continue;
+            bool keep = false;
+            if (pass) {
+                // The entry-major kernel's radius test (kPredRangeRadius): the child's coordinates
+                // rebuilt with one rounded multiply per dimension, the box gap accumulated with fma
+                // in dimension order, against the child's subtree radius.
+                const NodeRec nr = a.children[j];
+                const double* row = a.rows + static_cast<size_t>(j) * dim;
+                const double* box = a.boxes + static_cast<size_t>(q) * 2 * dim;
+                double dist = 0.0;
+#pragma unroll
+                for (int d = 0; d < DM; ++d) {
+                    if (D > 0 || d < dim) {
+                        const double r = a.rowsOnHost ? row[d] : __ldg(row + d);
+                        const double y = __dmul_rn(r, __ldg(xp + d));
+                        dist = boxGapAcc(y, __ldg(box + d), __ldg(box + dim + d), dist, 1);
+                    }
+                }
+                keep = nr.cnt > 0 && dist <= __dmul_rn(nr.rad, nr.rad);
+            }
+            const uint32_t kb = __ballot_sync(FULL, keep);
+            if (kb == 0) continue;
+            const int leader = __ffs(kb) - 1;
+            uint32_t pos0 = 0;
+            if (lane == leader) pos0 = atomicAdd(a.vcount, static_cast<uint32_t>(__popc(kb)));
+            pos0 = __shfl_sync(FULL, pos0, leader);
+            if (keep) {
+                const uint32_t pos = pos0 + __popc(kb & lanesLt);
+                if (pos < a.vcap) {
+                    a.vq[pos] = q;
+                    a.vcbeg[pos] = j;
+                    a.vcpre[pos] = pos;
+                    double* xo = a.vx + static_cast<size_t>(pos) * dim;
+#pragma unroll
+                    for (int d = 0; d < DM; ++d)
+                        if (D > 0 || d < dim) xo[d] = __ldg(xp + d);
+                    if ((pos % kWarpTile) == 0 && pos / kWarpTile < a.vtileCap) a.vtile[pos / kWarpTile] = pos;
+                } else {
+                    atomicOr(a.status, kStatusOverflowEntries);
+                }
+            }
+        }
+    }
+}
+
+__global__ void oneItemHeaderKernel(const uint32_t* count, uint32_t* hdr) {
+    const uint32_t c = *count;
+    hdr[0] = c;
+    hdr[1] = c;
+}
+
+__global__ void groupResultsKernel(const uint64_t* rawIds, const uint32_t* rawQ, const double* rawVals,
+                                   const uint32_t* hdr, uint32_t cap, int D, const uint64_t* offsets, uint32_t* cursor,
+                                   uint64_t* ids, double* vals) {
+    const uint32_t n = min(hdr[0], cap);
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const uint32_t q = rawQ[i];
+        const uint64_t pos = offsets[q] + atomicAdd(&cursor[q], 1u);
+        if (pos >= cap) continue;  // more results than the buffers hold: the batch reruns after growth
+        ids[pos] = rawIds[i];
+        if (vals)
+            for (int d = 0; d < D; ++d) vals[pos * D + d] = rawVals[static_cast<size_t>(i) * D + d];
+    }
+}
+
+int residentGrid(const void* kern, int threads, int percent) {
+    static int sms = 0;
+    if (sms == 0) {
+        int dev = 0;
+        TBLAEQ_CUDA(cudaGetDevice(&dev));
+        TBLAEQ_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    }
+    int perSm = 0;
+    TBLAEQ_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, kern, threads, 0));
+    const int pct = (percent > 0 && percent < 100) ? percent : 100;
+    return std::max(1, (sms * std::max(1, perSm) * pct + 99) / 100);
+}
+
+template <int D>
+void launchNodeMajorD(const NodeMajorArgs& a, int gridPercent, cudaStream_t s) {
+    static int full = 0;
+    if (full == 0) full = residentGrid(reinterpret_cast<const void*>(nodeMajorRangeKernel<D>), kNodeMajorThreads, 100);
+    const int pct = (gridPercent > 0 && gridPercent < 100) ? gridPercent : 100;
+    const int grid = std::max(1, (full * pct + 99) / 100);
+    nodeMajorRangeKernel<D><<<grid, kNodeMajorThreads, 0, s>>>(a);
+    TBLAEQ_CUDA(cudaGetLastError());
+}
+
+int smallGrid(uint64_t work) { return static_cast<int>(std::max<uint64_t>(1, std::min<uint64_t>((work + 255) / 256, 148 * 8))); }
+
+}  // namespace
+
+void launchNodeTranspose(const uint32_t* node, const uint32_t* hdr, uint32_t cap, uint32_t nNodes, uint32_t* nodeCnt,
+                         uint32_t* nodeOff, uint32_t* unitOff, uint32_t* cursor, uint32_t* list, cudaStream_t s) {
+    nodeCountKernel<<<smallGrid(cap), 256, 0, s>>>(node, hdr, cap, nNodes, nodeCnt);
+    TBLAEQ_CUDA(cudaGetLastError());
+    nodeScanKernel<<<1, 1024, 0, s>>>(nodeCnt, nNodes, nodeOff, unitOff);
+    TBLAEQ_CUDA(cudaGetLastError());
+    nodeScatterKernel<<<smallGrid(cap), 256, 0, s>>>(node, hdr, cap, nNodes, nodeOff, cursor, list);
+    TBLAEQ_CUDA(cudaGetLastError());
+}
+
+void launchNodeMajorRange(const NodeMajorArgs& a, int gridPercent, cudaStream_t s) {
+    switch (a.D) {
+        case 2: return launchNodeMajorD<2>(a, gridPercent, s);
+        case 3: return launchNodeMajorD<3>(a, gridPercent, s);
+        case 4: return launchNodeMajorD<4>(a, gridPercent, s);
+        case 5: return launchNodeMajorD<5>(a, gridPercent, s);
+        case 8: return launchNodeMajorD<8>(a, gridPercent, s);
+        case 16: return launchNodeMajorD<16>(a, gridPercent, s);
+        default:
+            if (a.D < 1 || a.D > 32) throw std::invalid_argument("node-major level: D must be in [1, 32]");
+            return launchNodeMajorD<0>(a, gridPercent, s);
+    }
+}
+
+void launchOneItemHeader(const uint32_t* count, uint32_t* hdr, cudaStream_t s) {
+    oneItemHeaderKernel<<<1, 1, 0, s>>>(count, hdr);
+    TBLAEQ_CUDA(cudaGetLastError());
+}
+
+void launchGroupResults(const uint64_t* rawIds, const uint32_t* rawQ, const double* rawVals, const uint32_t* hdr,
+                        uint32_t cap, int D, const uint64_t* offsets, uint32_t* cursor, uint64_t* ids, double* vals,
+                        cudaStream_t s) {
+    groupResultsKernel<<<smallGrid(cap), 256, 0, s>>>(rawIds, rawQ, rawVals, hdr, cap, D, offsets, cursor, ids, vals);
+    TBLAEQ_CUDA(cudaGetLastError());
+}
+
 }  // namespace tblaeq

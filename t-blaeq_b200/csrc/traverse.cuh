@@ -166,6 +166,67 @@ void setLookbackTestHook(uint32_t withholdTile, uint32_t spinLimit);
 // Tile size (work items per tile) used by every expand instantiation.
 inline int expandTile(int) { return kWarpTile; }
 
+// ---- node-major range levels (exact mode) ----------------------------------------------------------
+// A frontier level of an exact range batch tests every (query, child) pair. In a frontier the same
+// node sits in many queries' entries (a mesh-1 node in about 240 of 4,096 at N = 10M, D = 8), and
+// entry by entry every one of them re-reads the node's children. Node-major, a warp takes one node
+// and 32 of the queries holding it: each query box stays in registers, each child's float box is
+// read once per 32 queries (a broadcast load), and only children that pass it are tested in FP64
+// against the radius (the same prefilter and the same radius test as the entry-major kernel, so the
+// same children survive). Survivors are appended, in no particular order, to a one-item-per-entry
+// frontier (query, child row, the parent's coordinates); an ordinary kPredAll expand of it rebuilds
+// the children's coordinates and writes the next frontier.
+
+struct NodeMajorArgs {
+    // Input frontier, grouped by node: entry list[nodeOff[n] .. nodeOff[n+1]) hold node n, in units
+    // of 32 entries (unitOff[n] = first unit of node n, unitOff[nNodes] = all units). nNodes = 0: the
+    // root level (every entry holds the virtual root, whose children are rows 0 .. rootChildren-1).
+    const uint32_t* inQ;
+    const double* inX;
+    const uint32_t* inHdr;
+    uint32_t inCap;
+    const uint32_t* list;
+    const uint32_t* nodeOff;
+    const uint32_t* unitOff;
+    uint32_t nNodes;
+    const NodeRec* parents;     // records of the input level's nodes (first child row, child count)
+    uint32_t rootChildren;
+    // The children: rows, float boxes and records (by row).
+    const double* rows;
+    const float* aabb;
+    const NodeRec* children;
+    int rowsOnHost;
+    // Query boxes: double lo|hi, and as floats rounded outward.
+    const double* boxes;
+    const float* boxesF;
+    // Survivors: a frontier with one item per entry (cbeg = the child row, cpre = the position).
+    uint32_t* vq;
+    uint32_t* vcbeg;
+    uint32_t* vcpre;
+    double* vx;
+    uint32_t* vtile;
+    uint32_t vcap, vtileCap;
+    uint32_t* vcount;           // survivors (may exceed vcap: the host grows the workspace)
+    uint32_t* ticket;           // unit ticket, zeroed before launch
+    uint32_t* status;
+    uint32_t* levelItems;       // optional per-query generated-children counts
+    int D;
+};
+
+// Groups the entries of a frontier by node (node keys < nNodes): nodeCnt and cursor (nNodes each)
+// must be zero; writes nodeOff / unitOff (nNodes + 1) and list (entries).
+void launchNodeTranspose(const uint32_t* node, const uint32_t* hdr, uint32_t cap, uint32_t nNodes, uint32_t* nodeCnt,
+                         uint32_t* nodeOff, uint32_t* unitOff, uint32_t* cursor, uint32_t* list, cudaStream_t s);
+// The node-major test of one level (persistent grid; gridPercent as for the expand kernel).
+void launchNodeMajorRange(const NodeMajorArgs& a, int gridPercent, cudaStream_t s);
+// hdr[0] = hdr[1] = *count: the header of a one-item-per-entry frontier.
+void launchOneItemHeader(const uint32_t* count, uint32_t* hdr, cudaStream_t s);
+// Moves results written in frontier order (rawIds/rawQ/rawVals, count = *hdr) to their query's slot
+// offsets[q] + k (cursor: nq zeros), so every query's results are contiguous.
+void launchGroupResults(const uint64_t* rawIds, const uint32_t* rawQ, const double* rawVals, const uint32_t* hdr,
+                        uint32_t cap, int D, const uint64_t* offsets, uint32_t* cursor, uint64_t* ids, double* vals,
+                        cudaStream_t s);
+
 // Builds a root frontier of `nq` entries, each with `nChildren` children starting at row 0 and
 // x = 1 (so the first expand reproduces the coarsest coordinates exactly). Capacities must hold
 // nq entries and ceil(nq*nChildren / tile) tile starts.

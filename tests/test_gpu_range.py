@@ -273,3 +273,34 @@ def test_autotuned_launch_shapes_keep_results_and_round_trip(tb, env, oracle_mod
     v2, g2, _, src2 = h.autotune_cached(dQ, cache, tb.Mode.EXACT, reps=2)
     assert src2 == "cache" and (v2, g2) == (v1, g1) and h.launch_shapes() == (v1, g1)
     h.set_launch_shapes([0] * H, [100] * H)
+
+
+@pytest.mark.parametrize("flags", [0, 2, 1])  # plain, WANT_LEVELS, WANT_VALS
+def test_node_major_levels_equal_entry_major(tb, env, oracle_mod, flags):
+    """Node-major inner levels (one warp per node and 32 of its queries) keep exactly the children the
+    entry-major kernel keeps: identical per-level frontier sizes and per-query level counts, and the
+    same exact results (as sets; node-major leaves each query's ids in no particular order)."""
+    h, o, pts, ids = env
+    Q = _boxes(pts, 700, 31, hi_frac=0.3)  # a workspace that grows: several growth steps
+    b = oracle_mod.brute_query(pts, ids, oracle_mod.RANGE, Q)
+    out = {}
+    for nm in (False, True):
+        h.set_node_major(nm)
+        r = h.query_batch(tb.QueryType.RANGE, Q, tb.Mode.EXACT, flags=flags)
+        offs, got = r.offsets.numpy(), r.ids.numpy()
+        lv = r.level_items.numpy().copy() if r.level_items is not None else None
+        vals = r.vals.numpy().copy() if r.vals is not None else None
+        out[nm] = (offs.copy(), ids_by_query(offs, got), h.level_counts(), lv, vals, got.copy())
+        assert np.array_equal(offs, b.offsets)
+        assert all(np.array_equal(g, b.query(q)) for q, g in enumerate(out[nm][1]))
+    assert out[False][2] == out[True][2]  # same frontier entries and children at every level
+    if flags == 2:
+        assert np.array_equal(out[False][3], out[True][3])
+    if flags == 1:
+        # Each id keeps its own coordinates.
+        for nm in (False, True):
+            o_, _, _, _, vals, got = out[nm]
+            order = np.argsort(got)
+            rows = dict(zip(ids.tolist(), range(len(ids))))
+            assert np.array_equal(vals[order], pts[[rows[int(i)] for i in got[order]]])
+    h.set_node_major(True)
