@@ -233,6 +233,15 @@ int tblaeq_tuning_lookup(const char* path, const char* key, int* variants, int* 
 /* 1 (default) = two-wave finest level, 0 = one pass over every surviving cluster. */
 int tblaeq_set_two_wave(tblaeq_handle* h, int on);
 
+/* Exact KNN batches with the two-wave finest level: `beam` (0..32, default 32) is the probe's beam
+ * -- at every level above the clusters each query keeps its `beam` entries of smallest lower bound,
+ * and wave 1 ranks only the clusters under them (0: every surviving cluster is ranked) -- and
+ * node_major_completion (default 1) selects how the points within wave 1's bound are found: the
+ * hierarchy walked again node-major (one warp per node and 32 of its queries; each cluster's points
+ * read once per 32 of its queries), or 0: every remaining frontier entry expanded query by query.
+ * Exactness never depends on either. No counterpart in the reference. */
+int tblaeq_set_knn_probe(tblaeq_handle* h, uint32_t beam, int node_major_completion);
+
 /* Counters of the last KNN batch (summed over its chunks when it ran in several): [0] final-frontier
  * clusters, [1] wave-1 candidates,
  * [2] wave-2 candidates, [3] points whose rows wave 1 loaded and tested (the single pass, when

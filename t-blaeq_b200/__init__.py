@@ -151,6 +151,7 @@ def _load():
         "tblaeq_autotune": ([vp, P(_Batch), ctypes.c_int, P(ctypes.c_int), P(ctypes.c_float)], ctypes.c_int),
         "tblaeq_set_variants": ([vp, P(ctypes.c_int), ctypes.c_uint64], ctypes.c_int),
         "tblaeq_set_node_major": ([vp, ctypes.c_int], ctypes.c_int),
+        "tblaeq_set_knn_probe": ([vp, ctypes.c_uint32, ctypes.c_int], ctypes.c_int),
         "tblaeq_set_launch_shapes": ([vp, P(ctypes.c_int), P(ctypes.c_int), ctypes.c_uint64], ctypes.c_int),
         "tblaeq_get_launch_shapes": ([vp, P(ctypes.c_int), P(ctypes.c_int), ctypes.c_uint64], ctypes.c_int),
         "tblaeq_tuning_key": ([vp, ctypes.c_int, ctypes.c_uint64, ctypes.c_char_p, ctypes.c_uint64], ctypes.c_int),
@@ -530,6 +531,11 @@ class QueryHandler:
         ms = (ctypes.c_float * H)()
         _check(_load().tblaeq_autotune(self._h, ctypes.byref(b), reps, v, ms))
         return list(v), list(ms)
+
+    def set_knn_probe(self, beam: int = 32, node_major_completion: bool = True):
+        """Exact KNN: the probe's beam (0 = rank every surviving cluster) and the node-major
+        completion after wave 1 (False: the query-major wave 2)."""
+        _check(_load().tblaeq_set_knn_probe(self._h, beam, int(node_major_completion)))
 
     def set_node_major(self, on: bool = True):
         """Exact range batches: node-major inner levels (default) or entry-major."""

@@ -478,6 +478,14 @@ int tblaeq_set_variants(tblaeq_handle* h, const int* variants, uint64_t n) {
     });
 }
 
+int tblaeq_set_knn_probe(tblaeq_handle* h, uint32_t beam, int node_major_completion) {
+    if (int c = checkPrepared(h)) return c;
+    return guarded([&]() -> int {
+        h->qh->runtime().engine->setKnnProbe(beam, node_major_completion != 0);
+        return TBLAEQ_OK;
+    });
+}
+
 int tblaeq_set_node_major(tblaeq_handle* h, int on) {
     if (int c = checkPrepared(h)) return c;
     h->qh->runtime().engine->setNodeMajor(on != 0);

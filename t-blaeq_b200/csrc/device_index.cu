@@ -107,6 +107,8 @@ DerivedArrays computeDerived(const HostIndex& idx) {
         }
     }
 
+    out.nodeX.resize(H - 1);
+    for (uint64_t m = 0; m + 1 < H; ++m) out.nodeX[m] = dec[m];
     // Box of the finest points below every node (exact min / max of decoded coordinates), stored
     // as floats rounded outward.
     {
@@ -324,6 +326,7 @@ std::unique_ptr<DeviceIndex> buildDeviceIndex(const HostIndex& idx, const Derive
     di->nodeSub.resize(idx.height - 1);
     di->leaf.resize(idx.height - 1);
     di->aabb.resize(idx.height - 1);
+    di->nodeX.resize(idx.height - 1);
     for (uint64_t m = 0; m + 1 < idx.height; ++m) {
         const size_t n = der.cbeg[m].size();
         std::vector<NodeRec> ref(n), sub(n);
@@ -335,6 +338,7 @@ std::unique_ptr<DeviceIndex> buildDeviceIndex(const HostIndex& idx, const Derive
         di->nodeSub[m] = upload(sub, s);
         di->leaf[m] = upload(der.leaf[m], s);
         di->aabb[m] = upload(der.aabb[m], s);
+        di->nodeX[m] = upload(der.nodeX[m], s);
         TBLAEQ_CUDA(cudaStreamSynchronize(s));
     }
     TBLAEQ_CUDA(cudaStreamSynchronize(s));
@@ -343,7 +347,7 @@ std::unique_ptr<DeviceIndex> buildDeviceIndex(const HostIndex& idx, const Derive
 
 size_t DeviceIndex::deviceBytes() const {
     size_t t = coarseVals.bytes() + coarseIds.bytes();
-    for (auto* v : {&pvals, &nodeRef, &nodeSub, &leaf, &aabb, &nodeOrig, &maps})
+    for (auto* v : {&pvals, &nodeRef, &nodeSub, &leaf, &aabb, &nodeX, &nodeOrig, &maps})
         for (auto& m : *v) t += m.bytes();
     return t;
 }

@@ -80,6 +80,9 @@ struct DerivedArrays {
     // Axis-aligned box of the finest points below each node: lo[D] then hi[D] per node, in float
     // rounded outward (lo down, hi up), so it always contains the decoded points.
     std::vector<std::vector<float>> aabb;
+    // Decoded coordinates of every node (position order, D per node), as the traversal rebuilds
+    // them (y = P[j] * x_parent, one rounded multiply per level).
+    std::vector<std::vector<double>> nodeX;
 };
 
 // Host computation of the position-space node arrays, including subtree radii from the decoded
@@ -130,6 +133,7 @@ struct DeviceIndex {
     std::vector<DeviceMem> nodeRef, nodeSub; // mesh m < height-1: NodeRec {radius, first child, children}
     std::vector<DeviceMem> leaf;             // mesh m < height-1: finest points below each node (uint32)
     std::vector<DeviceMem> aabb;             // mesh m < height-1: outward-rounded float box of the points below
+    std::vector<DeviceMem> nodeX;            // mesh m < height-1: decoded coordinates (D doubles per node)
 
     // original-id space (per-level plugin)
     DeviceMem coarseIds;                     // uint64

@@ -249,6 +249,20 @@ void BatchEngine::reserve(const EngineCaps& want, uint32_t nq, unsigned flags) {
         }
         offRcursor_ = off;
         off = align256(off + static_cast<size_t>(qcap_) * 4);
+        // Node-major KNN completion: H+1 tickets, H pair counts and the candidate count; the probe's
+        // per-level query counts; per-node counts and cursors of meshes 0..H-2; the per-query
+        // candidate cursors.
+        offKnnTick_ = off;
+        off = align256(off + (2 * H + 2) * 4);
+        offQcountP_ = off;
+        off = align256(off + H * static_cast<size_t>(qcap_) * 4);
+        offKnnNodeCnt_.assign(H, 0);
+        for (uint64_t m = 0; m + 1 < H; ++m) {
+            offKnnNodeCnt_[m] = off;
+            off = align256(off + 2 * di_.meshCount[m] * 4);
+        }
+        offCandCursor_ = off;
+        off = align256(off + static_cast<size_t>(qcap_) * 4);
         zeroBytes_ = off;
         zeroBlock_.alloc(zeroBytes_);
         offsets_.alloc((static_cast<size_t>(qcap_) + 1) * 8);
@@ -798,6 +812,10 @@ void BatchEngine::enqueueKnn(const double* dPoints, uint32_t nq, const uint32_t*
         a.variant = kVariantDirect;
         return a;
     };
+    const bool probe = twoWave_ && probeBeam_ > 0;
+    const bool completion = twoWave_ && knnNodeMajor_;
+    auto* qcountP = reinterpret_cast<uint32_t*>(z + offQcountP_);
+    if (probe) launchFillU32(probeK_.as<uint32_t>(), probeBeam_, nq, stream_);
     int buf = 0;
     for (int m = 0; m < H - 1; ++m) {
         ExpandArgs a = base(m, buf);
@@ -805,9 +823,30 @@ void BatchEngine::enqueueKnn(const double* dPoints, uint32_t nq, const uint32_t*
         a.child.aabb = di_.aabb[m].as<float>();
         a.child.leaf = di_.leaf[m].as<uint32_t>();
         a.fout = outView(1 - buf, hdrPtr(m + 1));
-        a.fout.qcount = (m == H - 2) ? qcountF : nullptr;
+        a.fout.qcount = (m == H - 2) ? qcountF : (probe ? qcountP + static_cast<size_t>(m) * qcap_ : nullptr);
         launchExpand(a, kPredKnnBound, false, 0, stream_);
         buf = 1 - buf;
+        if (probe && m < H - 2) {
+            // The probe's beam: every query keeps its probeBeam_ entries of smallest lower bound
+            // (order kept), so the levels below and wave 1 see only the clusters under them.
+            const FrontierIn Fm = inView(buf, hdrPtr(m + 1));
+            const uint32_t cap = static_cast<uint32_t>(caps_.entries);
+            launchExclusiveScan(qcountP + static_cast<size_t>(m) * qcap_, offF_.as<uint64_t>(), nq, stream_);
+            launchEntryBounds(Fm.q, f_[buf].node.as<uint32_t>(), Fm.x, Fm.hdr, cap, D, dPoints,
+                              di_.nodeSub[m].as<NodeRec>(), di_.aabb[m].as<float>(), lbE_.as<double>(),
+                              scoreE_.as<double>(), stream_);
+            launchClampCounts(offF_.as<uint64_t>(), probeK_.as<uint32_t>(), nq, selCount_.as<uint32_t>(), stream_);
+            launchExclusiveScan(selCount_.as<uint32_t>(), selOff_.as<uint64_t>(), nq, stream_);
+            launchTopK(offF_.as<uint64_t>(), nullptr, lbE_.as<double>(), cap, nullptr, nullptr, nullptr, 0,
+                       probeK_.as<uint32_t>(), nq, selOff_.as<uint64_t>(), selIds_.as<uint64_t>(),
+                       selD2_.as<double>(), selCount_.as<uint32_t>(), status, stream_);
+            TBLAEQ_CUDA(cudaMemsetAsync(sel_.get(), 0, entryCap_, stream_));
+            launchScatterSel(selIds_.as<uint64_t>(), selOff_.as<uint64_t>(), nq, cap, sel_.as<uint8_t>(), stream_);
+            launchCompactFrontier(Fm, cap, 1, sel_.as<uint8_t>(), lbE_.as<double>(), tau, D, cmpCnt_.as<uint32_t>(),
+                                  cmpKids_.as<uint32_t>(), cmpEntryOff_.as<uint64_t>(), cmpKidOff_.as<uint64_t>(),
+                                  outView(1 - buf, hdrPtr(m + 1)), stream_);
+            buf = 1 - buf;
+        }
         if (timing_) record(2 + m);
     }
     // `buf` now holds the last frontier F: the surviving finest clusters, query-major.
@@ -872,6 +911,100 @@ void BatchEngine::enqueueKnn(const double* dPoints, uint32_t nq, const uint32_t*
                nullptr, 0, dK, nq, knnOff_.as<uint64_t>(), knnIds_.as<uint64_t>(), knnD2_.as<double>(),
                knnCount_.as<uint32_t>(), status, stream_);
     launchTauFromTopK(knnOff_.as<uint64_t>(), knnD2_.as<double>(), dK, nq, tau, stream_);
+    if (completion) {
+        // Every point within tau, outside the clusters wave 1 read: the hierarchy again from the
+        // root, node-major, then the clusters' points, each read once per 32 of its queries.
+        auto* tick = reinterpret_cast<uint32_t*>(z + offKnnTick_);
+        uint32_t* pairCnt = tick + (H + 1);
+        uint32_t* candCnt = pairCnt + H;
+        launchWaveOneClusters(selIds_.as<uint64_t>(), selOff_.as<uint64_t>(), selCount_.as<uint32_t>(),
+                              fb.node.as<uint32_t>(), fcap, nq, 32, excl_.as<uint32_t>(), stream_);
+        const uint32_t pcap = static_cast<uint32_t>(pairCap_);
+        int pb = 0;
+        auto group = [&](int mesh, int from) {
+            const uint32_t M = static_cast<uint32_t>(di_.meshCount[mesh]);
+            auto* nodeCnt = reinterpret_cast<uint32_t*>(z + offKnnNodeCnt_[mesh]);
+            launchNodeTranspose(pairNode_[from].as<uint32_t>(), pairCnt + mesh, pcap, M, nodeCnt,
+                                pairNodeOff_.as<uint32_t>(), pairUnitOff_.as<uint32_t>(), nodeCnt + M,
+                                pairList_.as<uint32_t>(), stream_);
+            return M;
+        };
+        for (int m = 0; m < H - 1; ++m) {
+            KnnBoundLevelArgs b{};
+            b.nq = nq;
+            if (m == 0) {
+                b.nNodes = 0;
+                b.rootChildren = static_cast<uint32_t>(di_.meshCount[0]);
+            } else {
+                b.inQ = pairQ_[pb].as<uint32_t>();
+                b.inCount = pairCnt + (m - 1);
+                b.inCap = pcap;
+                b.nNodes = group(m - 1, pb);
+                b.list = pairList_.as<uint32_t>();
+                b.nodeOff = pairNodeOff_.as<uint32_t>();
+                b.unitOff = pairUnitOff_.as<uint32_t>();
+                b.parents = di_.nodeSub[m - 1].as<NodeRec>();
+            }
+            b.x = di_.nodeX[m].as<double>();
+            b.aabb = di_.aabb[m].as<float>();
+            b.nodes = di_.nodeSub[m].as<NodeRec>();
+            b.points = dPoints;
+            b.tau = tau;
+            b.outQ = pairQ_[1 - pb].as<uint32_t>();
+            b.outNode = pairNode_[1 - pb].as<uint32_t>();
+            b.outCap = pcap;
+            b.outCount = pairCnt + m;
+            b.ticket = tick + m;
+            b.status = status;
+            b.D = D;
+            launchKnnBoundLevel(b, stream_);
+            pb = 1 - pb;
+        }
+        KnnClusterArgs c{};
+        c.inQ = pairQ_[pb].as<uint32_t>();
+        c.inCount = pairCnt + (H - 2);
+        c.inCap = pcap;
+        c.nNodes = group(H - 2, pb);
+        c.list = pairList_.as<uint32_t>();
+        c.nodeOff = pairNodeOff_.as<uint32_t>();
+        c.unitOff = pairUnitOff_.as<uint32_t>();
+        c.clusters = di_.nodeSub[H - 2].as<NodeRec>();
+        c.x = di_.nodeX[H - 2].as<double>();
+        c.rows = di_.rows[H - 2];
+        c.rowsOnHost = di_.rowsOnHost[H - 2];
+        c.map = di_.mapPtr[H - 1];
+        c.points = dPoints;
+        c.tau = tau;
+        c.excl = excl_.as<uint32_t>();
+        c.exclStride = 32;
+        c.outQ = candQ_.as<uint32_t>();
+        c.outId = candId_.as<uint64_t>();
+        c.outD2 = candD2_.as<double>();
+        c.outCap = static_cast<uint32_t>(candCap_);
+        c.outCount = candCnt;
+        c.qcount = qcountB;
+        c.work = reinterpret_cast<unsigned long long*>(z + offWork_) + 1;
+        c.ticket = tick + H;
+        c.status = status;
+        c.D = D;
+        launchKnnClusterPoints(c, stream_);
+        if (timing_) record(1 + H);
+        launchExclusiveScan(qcountB, candOffB_.as<uint64_t>(), nq, stream_);
+        launchGroupResults(candId_.as<uint64_t>(), candQ_.as<uint32_t>(), candD2_.as<double>(), candCnt,
+                           static_cast<uint32_t>(std::min<uint64_t>(candCap_, resCapB_)), 1, candOffB_.as<uint64_t>(),
+                           reinterpret_cast<uint32_t*>(z + offCandCursor_), resIdsB_.as<uint64_t>(),
+                           resDistB_.as<double>(), stream_);
+        launchOneItemHeader(candCnt, hdrPtr(H + 1), stream_);  // the wave-2 candidate count (counters)
+        launchClampCounts2(candOff_.as<uint64_t>(), candOffB_.as<uint64_t>(), dK, nq, knnCount_.as<uint32_t>(),
+                           stream_);
+        launchExclusiveScan(knnCount_.as<uint32_t>(), knnOff_.as<uint64_t>(), nq, stream_);
+        launchTopK(candOff_.as<uint64_t>(), resIds_.as<uint64_t>(), resDist_.as<double>(), caps_.results,
+                   candOffB_.as<uint64_t>(), resIdsB_.as<uint64_t>(), resDistB_.as<double>(), resCapB_, dK, nq,
+                   knnOff_.as<uint64_t>(), knnIds_.as<uint64_t>(), knnD2_.as<double>(), knnCount_.as<uint32_t>(),
+                   status, stream_);
+        if (timing_) record(2 + H);
+        return;
+    }
     // Wave 2: the other clusters whose lower bound tau cannot exclude, points within tau.
     compact(2);
     ExpandArgs w2 = fin;
@@ -898,6 +1031,62 @@ void BatchEngine::enqueueKnn(const double* dPoints, uint32_t nq, const uint32_t*
     if (timing_) record(2 + H);
 }
 
+void BatchEngine::reserveKnnMajor(uint32_t nq) {
+    const size_t q1 = std::max<uint32_t>(nq, 1);
+    if (excl_.bytes() < q1 * 32 * 4) {
+        excl_.alloc(q1 * 32 * 4);
+        probeK_.alloc(q1 * 4);
+    }
+    if (pairCap_ == 0) {
+        pairCap_ = std::max<uint64_t>(caps_.entries, 1u << 20);
+        uint64_t maxM = 1;
+        for (uint64_t m = 0; m + 1 < di_.height; ++m) maxM = std::max<uint64_t>(maxM, di_.meshCount[m]);
+        pairNodeOff_.alloc((maxM + 1) * 4);
+        pairUnitOff_.alloc((maxM + 1) * 4);
+    }
+    if (pairQ_[0].bytes() < pairCap_ * 4) {
+        for (int b = 0; b < 2; ++b) {
+            pairQ_[b].alloc(pairCap_ * 4);
+            pairNode_[b].alloc(pairCap_ * 4);
+        }
+        pairList_.alloc(pairCap_ * 4);
+    }
+    if (candCap_ == 0) candCap_ = std::max<uint64_t>(caps_.results, 1u << 20);
+    if (candQ_.bytes() < candCap_ * 4) {
+        candQ_.alloc(candCap_ * 4);
+        candId_.alloc(candCap_ * 8);
+        candD2_.alloc(candCap_ * 8);
+    }
+    if (resCapB_ < candCap_) {
+        resCapB_ = candCap_;
+        resIdsB_.alloc(resCapB_ * 8);
+        resQB_.alloc(resCapB_ * 4);
+        resDistB_.alloc(resCapB_ * 8);
+    }
+}
+
+bool BatchEngine::growKnnMajor() {
+    const int H = static_cast<int>(di_.height);
+    std::vector<uint32_t> c(H + 1, 0);
+    TBLAEQ_CUDA(cudaMemcpyAsync(c.data(), zeroBlock_.as<char>() + offKnnTick_ + (H + 1) * 4, (H + 1) * 4,
+                                cudaMemcpyDeviceToHost, stream_));
+    TBLAEQ_CUDA(cudaStreamSynchronize(stream_));
+    bool grew = false;
+    for (int m = 0; m + 1 < H; ++m) {
+        if (c[m] > pairCap_) {
+            pairCap_ = static_cast<uint64_t>(c[m]) + c[m] / 4 + 4096;
+            grew = true;
+        }
+    }
+    if (c[H] > candCap_) {
+        candCap_ = static_cast<uint64_t>(c[H]) + c[H] / 4 + 4096;
+        grew = true;
+    }
+    if (pairCap_ >= 0x80000000ull || candCap_ >= 0x80000000ull)
+        throw SplitBatch("node-major KNN pairs exceed 2^31; split the batch");
+    return grew;
+}
+
 BatchOutput BatchEngine::runKnn(const double* dPoints, uint32_t nq, const uint32_t* dK, uint64_t sumK,
                                 unsigned flags) {
     reserve(caps_, nq, flags);
@@ -908,6 +1097,7 @@ BatchOutput BatchEngine::runKnn(const double* dPoints, uint32_t nq, const uint32
         knnD2_.alloc(knnCap_ * 8);
     }
     for (int attempt = 0; attempt < 16; ++attempt) {
+        reserveKnnMajor(nq);
         enqueueKnn(dPoints, nq, dK, flags);
         const uint32_t st = status();
         if (st & (kStatusLookbackTimeout | kStatusWindowOverflow))
@@ -920,7 +1110,8 @@ BatchOutput BatchEngine::runKnn(const double* dPoints, uint32_t nq, const uint32
             o.total = lastTotal(nq);
             return o;
         }
-        growFromHeaders();
+        const bool grewMajor = (twoWave_ && knnNodeMajor_) ? growKnnMajor() : false;
+        if (!grewMajor) growFromHeaders();
         reserveKnn(nq);
     }
     throw CudaError(cudaErrorMemoryAllocation, "KNN workspace did not converge after 16 growth steps");

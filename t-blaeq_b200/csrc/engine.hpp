@@ -3,6 +3,7 @@
 #pragma once
 
 #include <cstdint>
+#include <stdexcept>
 #include <memory>
 #include <vector>
 
@@ -57,6 +58,18 @@ public:
     // query to bound the K-th distance by real points, then expand only the clusters that bound
     // cannot exclude. Off: one pass over every surviving cluster.
     void setTwoWave(bool on) { twoWave_ = on; }
+    // Exact KNN with the two-wave finest level: beam width of the probe (each query keeps its
+    // probeBeam entries of smallest lower bound at every level above the clusters, so wave 1 ranks
+    // only the clusters under them; 0: no beam, every surviving cluster is ranked), and whether the
+    // completion after wave 1 walks the hierarchy node-major (default) or expands every remaining
+    // frontier entry query by query.
+    void setKnnProbe(uint32_t beam, bool nodeMajorCompletion) {
+        if (beam > 32) throw std::invalid_argument("probe beam must be at most 32");
+        probeBeam_ = beam;
+        knnNodeMajor_ = nodeMajorCompletion;
+    }
+    uint32_t probeBeam() const { return probeBeam_; }
+    bool knnNodeMajor() const { return knnNodeMajor_; }
     // Largest entry / item capacity a batch may use before it must be split (tests lower it).
     void setSplitLimit(uint64_t limit) { splitLimit_ = limit; }
     // Exact range batches test the inner levels node-major (default on; see NodeMajorArgs): same
@@ -156,6 +169,17 @@ private:
     void reserveNodeMajor(unsigned flags);
     bool useNodeMajor(int mode) const;
     void enqueueNodeMajorLevel(int m, int buf, const double* dBoxes, uint32_t nq, bool wantLevels);
+    // Node-major KNN completion: pair lists (query, node) per level, their grouping by node, the raw
+    // candidates of the point level and the clusters wave 1 read per query.
+    uint32_t probeBeam_ = 32;
+    bool knnNodeMajor_ = true;
+    DeviceMem pairQ_[2], pairNode_[2], pairList_, pairNodeOff_, pairUnitOff_;
+    DeviceMem candQ_, candId_, candD2_, excl_, probeK_;
+    uint64_t pairCap_ = 0, candCap_ = 0;
+    size_t offKnnTick_ = 0, offQcountP_ = 0, offCandCursor_ = 0;
+    std::vector<size_t> offKnnNodeCnt_;  // per mesh m <= height-2: nodeCnt then cursor, in zeroBlock_
+    void reserveKnnMajor(uint32_t nq);
+    bool growKnnMajor();                 // after an overflow: true when a capacity grew
     DeviceMem resIds_, resVals_, resQ_, resDist_;
     DeviceMem zeroBlock_;  // desc | tickets | status | hdrs | qcount | levelItems
     uint64_t splitLimit_ = 0xffffffffull;

@@ -87,3 +87,87 @@ void launchFillDouble(double* v, double value, uint32_t n, cudaStream_t s);
 void launchClampCounts(const uint64_t* off, const uint32_t* K, uint32_t nq, uint32_t* out, cudaStream_t s);
 
 }  // namespace tblaeq
+
+namespace tblaeq {
+
+// ---- Exact KNN completion, node-major (see BatchEngine::enqueueKnn) --------------------------------
+// Once wave 1 has bounded every query's K-th distance by tau, every point within tau lies in a
+// cluster whose lower bound is within tau, below ancestors whose bounds are within tau too. The
+// hierarchy is walked again node-major: a warp takes one node and 32 of the queries holding it
+// (query points and tau in registers, every child's decoded centre, box and record read once per
+// warp), and the surviving (query, child) pairs form the next level's input. At the cluster level
+// a warp loads each of a cluster's points once for 32 queries and keeps the points within tau, so
+// a cluster's rows are read once per batch per 32 of its queries instead of once per query.
+
+// One bound level (children of mesh m). Input pairs (query, node of mesh m-1) grouped by node
+// through list / nodeOff / unitOff (nNodes = 0: the root level, every query with the virtual root).
+struct KnnBoundLevelArgs {
+    const uint32_t* inQ;
+    const uint32_t* inCount;
+    uint32_t inCap;
+    uint32_t nq;
+    const uint32_t* list;
+    const uint32_t* nodeOff;
+    const uint32_t* unitOff;
+    uint32_t nNodes;
+    const NodeRec* parents;
+    uint32_t rootChildren;
+    const double* x;           // decoded centres of the children (mesh m)
+    const float* aabb;         // their point boxes
+    const NodeRec* nodes;      // their subtree radius and child counts
+    const double* points;
+    const double* tau;
+    uint32_t* outQ;            // surviving pairs
+    uint32_t* outNode;
+    uint32_t outCap;
+    uint32_t* outCount;
+    uint32_t* ticket;
+    uint32_t* status;
+    int D;
+};
+void launchKnnBoundLevel(const KnnBoundLevelArgs& a, cudaStream_t s);
+
+// The point level: pairs (query, cluster) grouped by cluster; every point of the cluster within
+// tau of the query (squared FP64 distance <= tau^2 (1 + 1e-9), accumulated like the expand kernel's
+// point test) becomes a candidate (query, id, squared distance), except in the clusters wave 1
+// already read for that query (excl: per query exclStride cluster positions, ~0 for none).
+struct KnnClusterArgs {
+    const uint32_t* inQ;
+    const uint32_t* inCount;
+    uint32_t inCap;
+    const uint32_t* list;
+    const uint32_t* nodeOff;
+    const uint32_t* unitOff;
+    uint32_t nNodes;
+    const NodeRec* clusters;
+    const double* x;
+    const double* rows;
+    int rowsOnHost;
+    const uint64_t* map;
+    const double* points;
+    const double* tau;
+    const uint32_t* excl;
+    uint32_t exclStride;
+    uint32_t* outQ;
+    uint64_t* outId;
+    double* outD2;
+    uint32_t outCap;
+    uint32_t* outCount;
+    uint32_t* qcount;
+    unsigned long long* work;  // optional: point rows tested
+    uint32_t* ticket;
+    uint32_t* status;
+    int D;
+};
+void launchKnnClusterPoints(const KnnClusterArgs& a, cudaStream_t s);
+
+// excl[q * stride + i] = node[selIds[selOff[q] + i]] for the selCount[q] entries wave 1 read, ~0
+// for the rest of the row.
+void launchWaveOneClusters(const uint64_t* selIds, const uint64_t* selOff, const uint32_t* selCount,
+                           const uint32_t* node, uint64_t cap, uint32_t nq, uint32_t stride, uint32_t* excl,
+                           cudaStream_t s);
+
+// v[i] = value for i < n.
+void launchFillU32(uint32_t* v, uint32_t value, uint32_t n, cudaStream_t s);
+
+}  // namespace tblaeq

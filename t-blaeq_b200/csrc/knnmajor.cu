@@ -1,0 +1,279 @@
+// Exact KNN completion, node-major (see knn.cuh for the design).
+#include <algorithm>
+
+#include "knn.cuh"
+
+namespace tblaeq {
+
+namespace {
+
+constexpr int kThreadsNm = 128;
+constexpr uint32_t FULL = 0xffffffffu;
+
+// The unit (node, up to 32 of its pairs) of ticket u: the node is the last one whose units start at
+// or before u (nodes without pairs own no unit).
+struct Unit {
+    uint32_t node, base, count;
+};
+__device__ __forceinline__ Unit unitOf(uint32_t u, const uint32_t* nodeOff, const uint32_t* unitOff, uint32_t nNodes) {
+    uint32_t lo = 0, hi = nNodes - 1;
+    while (lo < hi) {
+        const uint32_t mid = (lo + hi + 1) >> 1;
+        if (__ldg(unitOff + mid) <= u) lo = mid; else hi = mid - 1;
+    }
+    Unit r;
+    r.node = lo;
+    r.base = __ldg(nodeOff + lo) + (u - __ldg(unitOff + lo)) * 32u;
+    r.count = min(32u, __ldg(nodeOff + lo + 1) - r.base);
+    return r;
+}
+
+// Appends the pairs of the lanes in `keep` at consecutive positions of a shared counter. A counter
+// past 2^31 raises kStatusOverflowSum (the batch must be split) before it could wrap, and returns
+// positions no capacity reaches.
+__device__ __forceinline__ uint32_t appendPos(bool keep, uint32_t* counter, uint32_t* status, int lane) {
+    const uint32_t kb = __ballot_sync(FULL, keep);
+    if (kb == 0) return 0xffffffffu;
+    const int leader = __ffs(kb) - 1;
+    uint32_t base = 0;
+    if (lane == leader) {
+        base = atomicAdd(counter, static_cast<uint32_t>(__popc(kb)));
+        if (base >= 0x80000000u) atomicOr(status, kStatusOverflowSum);
+    }
+    base = __shfl_sync(FULL, base, leader);
+    if (base >= 0x80000000u) return 0xffffffffu;
+    return base + __popc(kb & ((1u << lane) - 1u));
+}
+
+template <int D>
+__global__ void __launch_bounds__(kThreadsNm) knnBoundLevelKernel(KnnBoundLevelArgs a) {
+    constexpr int DM = D > 0 ? D : 32;
+    if (*a.status & (kStatusLookbackTimeout | kStatusWindowOverflow)) return;
+    const int dim = D > 0 ? D : a.D;
+    const int lane = threadIdx.x & 31;
+    const bool root = a.nNodes == 0;
+    const uint32_t entries = root ? a.nq : *a.inCount;
+    if (!root && entries > a.inCap) {
+        if (blockIdx.x == 0 && threadIdx.x == 0) atomicOr(a.status, kStatusOverflowEntries);
+        return;
+    }
+    const uint32_t units = root ? (entries + 31u) / 32u : a.unitOff[a.nNodes];
+    while (true) {
+        uint32_t u = 0;
+        if (lane == 0) u = atomicAdd(a.ticket, 1u);
+        u = __shfl_sync(FULL, u, 0);
+        if (u >= units) break;
+        Unit un;
+        uint32_t cbeg = 0, cnt = a.rootChildren;
+        if (root) {
+            un.node = 0;
+            un.base = u * 32u;
+            un.count = min(32u, entries - un.base);
+        } else {
+            un = unitOf(u, a.nodeOff, a.unitOff, a.nNodes);
+            const NodeRec pr = a.parents[un.node];
+            cbeg = pr.cbeg;
+            cnt = pr.cnt;
+        }
+        const bool active = static_cast<uint32_t>(lane) < un.count;
+        uint32_t q = 0;
+        if (active) q = root ? un.base + lane : __ldg(a.inQ + __ldg(a.list + un.base + lane));
+        double p[DM];
+#pragma unroll
+        for (int d = 0; d < DM; ++d)
+            if (D > 0 || d < dim) p[d] = active ? __ldg(a.points + static_cast<size_t>(q) * dim + d) : 0.0;
+        const double tau = active ? __ldcg(a.tau + q) : -1.0;
+        for (uint32_t c = 0; c < cnt; ++c) {
+            const uint32_t j = cbeg + c;
+            const NodeRec nr = a.nodes[j];
+            const double* xc = a.x + static_cast<size_t>(j) * dim;
+            const float* b = a.aabb + static_cast<size_t>(j) * 2 * dim;
+            // The expand kernel's KNN bound (kPredKnnBound): centre distance minus the subtree radius,
+            // and the distance to the outward-rounded box, slightly reduced.
+            double dist = 0.0, gap = 0.0;
+#pragma unroll
+            for (int d = 0; d < DM; ++d) {
+                if (D > 0 || d < dim) {
+                    const double diff = p[d] - __ldg(xc + d);
+                    dist = __fma_rn(diff, diff, dist);
+                    const double l = static_cast<double>(__ldg(b + d)), h = static_cast<double>(__ldg(b + dim + d));
+                    const double g = fmax(fmax(l - p[d], p[d] - h), 0.0);
+                    gap = __fma_rn(g, g, gap);
+                }
+            }
+            const double lb = fmax(sqrt(dist) - nr.rad, sqrt(gap) * (1.0 - 1e-12));
+            const bool keep = active && nr.cnt > 0 && lb <= tau;
+            if (__ballot_sync(FULL, keep) == 0) continue;
+            const uint32_t pos = appendPos(keep, a.outCount, a.status, lane);
+            if (keep) {
+                if (pos < a.outCap) {
+                    a.outQ[pos] = q;
+                    a.outNode[pos] = j;
+                } else {
+                    atomicOr(a.status, kStatusOverflowEntries);
+                }
+            }
+        }
+    }
+}
+
+template <int D>
+__global__ void __launch_bounds__(kThreadsNm) knnClusterPointsKernel(KnnClusterArgs a) {
+    constexpr int DM = D > 0 ? D : 32;
+    if (*a.status & (kStatusLookbackTimeout | kStatusWindowOverflow)) return;
+    const int dim = D > 0 ? D : a.D;
+    const int lane = threadIdx.x & 31;
+    const uint32_t entries = *a.inCount;
+    if (entries > a.inCap) {
+        if (blockIdx.x == 0 && threadIdx.x == 0) atomicOr(a.status, kStatusOverflowEntries);
+        return;
+    }
+    const uint32_t units = a.unitOff[a.nNodes];
+    unsigned long long rows = 0;
+    while (true) {
+        uint32_t u = 0;
+        if (lane == 0) u = atomicAdd(a.ticket, 1u);
+        u = __shfl_sync(FULL, u, 0);
+        if (u >= units) break;
+        const Unit un = unitOf(u, a.nodeOff, a.unitOff, a.nNodes);
+        const NodeRec cr = a.clusters[un.node];
+        bool active = static_cast<uint32_t>(lane) < un.count;
+        uint32_t q = 0;
+        if (active) {
+            q = __ldg(a.inQ + __ldg(a.list + un.base + lane));
+            for (uint32_t i = 0; i < a.exclStride; ++i)
+                if (__ldg(a.excl + static_cast<size_t>(q) * a.exclStride + i) == un.node) active = false;
+        }
+        const uint32_t am = __ballot_sync(FULL, active);
+        if (am == 0) continue;
+        if (lane == 0) rows += static_cast<unsigned long long>(__popc(am)) * cr.cnt;
+        double p[DM], xc[DM];
+#pragma unroll
+        for (int d = 0; d < DM; ++d) {
+            if (D > 0 || d < dim) {
+                p[d] = active ? __ldg(a.points + static_cast<size_t>(q) * dim + d) : 0.0;
+                xc[d] = __ldg(a.x + static_cast<size_t>(un.node) * dim + d);
+            }
+        }
+        const double t = active ? __ldcg(a.tau + q) : 0.0;
+        const double t2 = t * t * (1.0 + 1e-9);
+        for (uint32_t c = 0; c < cr.cnt; ++c) {
+            const uint32_t j = cr.cbeg + c;
+            const double* row = a.rows + static_cast<size_t>(j) * dim;
+            // The expand kernel's point test (kPredKnnPoint): the point rebuilt with one rounded
+            // multiply per dimension, the squared distance accumulated with fma in dimension order.
+            double dist = 0.0;
+#pragma unroll
+            for (int d = 0; d < DM; ++d) {
+                if (D > 0 || d < dim) {
+                    const double r = a.rowsOnHost ? row[d] : __ldg(row + d);
+                    const double diff = p[d] - __dmul_rn(r, xc[d]);
+                    dist = __fma_rn(diff, diff, dist);
+                }
+            }
+            const bool keep = active && dist <= t2;
+            if (__ballot_sync(FULL, keep) == 0) continue;
+            const uint32_t pos = appendPos(keep, a.outCount, a.status, lane);
+            if (keep) {
+                atomicAdd(&a.qcount[q], 1u);
+                if (pos < a.outCap) {
+                    a.outQ[pos] = q;
+                    a.outId[pos] = a.map[j];
+                    a.outD2[pos] = dist;
+                } else {
+                    atomicOr(a.status, kStatusOverflowEntries);
+                }
+            }
+        }
+    }
+    if (a.work && lane == 0 && rows) atomicAdd(a.work, rows);
+}
+
+__global__ void waveOneClustersKernel(const uint64_t* selIds, const uint64_t* selOff, const uint32_t* selCount,
+                                      const uint32_t* node, uint64_t cap, uint32_t nq, uint32_t stride, uint32_t* excl) {
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < nq * stride; i += gridDim.x * blockDim.x) {
+        const uint32_t q = i / stride, k = i % stride;
+        uint32_t v = 0xffffffffu;
+        if (k < selCount[q]) {
+            const uint64_t e = selIds[selOff[q] + k];
+            if (e < cap) v = node[e];
+        }
+        excl[i] = v;
+    }
+}
+
+__global__ void fillU32Kernel(uint32_t* v, uint32_t value, uint32_t n) {
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) v[i] = value;
+}
+
+template <class K>
+int persistentGrid(K kern) {
+    int dev = 0, sms = 0, perSm = 0;
+    TBLAEQ_CUDA(cudaGetDevice(&dev));
+    TBLAEQ_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    TBLAEQ_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, kern, kThreadsNm, 0));
+    return std::max(1, sms * std::max(1, perSm));
+}
+
+template <int D>
+void boundLevelD(const KnnBoundLevelArgs& a, cudaStream_t s) {
+    static const int g = persistentGrid(knnBoundLevelKernel<D>);
+    knnBoundLevelKernel<D><<<g, kThreadsNm, 0, s>>>(a);
+    TBLAEQ_CUDA(cudaGetLastError());
+}
+
+template <int D>
+void clusterPointsD(const KnnClusterArgs& a, cudaStream_t s) {
+    static const int g = persistentGrid(knnClusterPointsKernel<D>);
+    knnClusterPointsKernel<D><<<g, kThreadsNm, 0, s>>>(a);
+    TBLAEQ_CUDA(cudaGetLastError());
+}
+
+int smallGridNm(uint64_t n) { return static_cast<int>(std::max<uint64_t>(1, std::min<uint64_t>((n + 255) / 256, 148 * 8))); }
+
+}  // namespace
+
+void launchKnnBoundLevel(const KnnBoundLevelArgs& a, cudaStream_t s) {
+    switch (a.D) {
+        case 2: return boundLevelD<2>(a, s);
+        case 3: return boundLevelD<3>(a, s);
+        case 4: return boundLevelD<4>(a, s);
+        case 5: return boundLevelD<5>(a, s);
+        case 8: return boundLevelD<8>(a, s);
+        case 16: return boundLevelD<16>(a, s);
+        default:
+            if (a.D < 1 || a.D > 32) throw std::invalid_argument("KNN bound level: D must be in [1, 32]");
+            return boundLevelD<0>(a, s);
+    }
+}
+
+void launchKnnClusterPoints(const KnnClusterArgs& a, cudaStream_t s) {
+    switch (a.D) {
+        case 2: return clusterPointsD<2>(a, s);
+        case 3: return clusterPointsD<3>(a, s);
+        case 4: return clusterPointsD<4>(a, s);
+        case 5: return clusterPointsD<5>(a, s);
+        case 8: return clusterPointsD<8>(a, s);
+        case 16: return clusterPointsD<16>(a, s);
+        default:
+            if (a.D < 1 || a.D > 32) throw std::invalid_argument("KNN point level: D must be in [1, 32]");
+            return clusterPointsD<0>(a, s);
+    }
+}
+
+void launchWaveOneClusters(const uint64_t* selIds, const uint64_t* selOff, const uint32_t* selCount,
+                           const uint32_t* node, uint64_t cap, uint32_t nq, uint32_t stride, uint32_t* excl,
+                           cudaStream_t s) {
+    if (nq == 0 || stride == 0) return;
+    waveOneClustersKernel<<<smallGridNm(static_cast<uint64_t>(nq) * stride), 256, 0, s>>>(selIds, selOff, selCount, node,
+                                                                                        cap, nq, stride, excl);
+    TBLAEQ_CUDA(cudaGetLastError());
+}
+
+void launchFillU32(uint32_t* v, uint32_t value, uint32_t n, cudaStream_t s) {
+    if (n == 0) return;
+    fillU32Kernel<<<smallGridNm(n), 256, 0, s>>>(v, value, n);
+    TBLAEQ_CUDA(cudaGetLastError());
+}
+
+}  // namespace tblaeq

@@ -1278,9 +1278,17 @@ __global__ void __launch_bounds__(kNodeMajorThreads) nodeMajorRangeKernel(NodeMa
             const uint32_t j = cbeg + c;
             const float* b = a.aabb + static_cast<size_t>(j) * 2 * dim;
             bool pass = active;
+            constexpr int C = chunkOf<D>();
 #pragma unroll
-            for (int d = 0; d < DM; ++d)
-                if (D > 0 || d < dim) pass = pass && __ldg(b + d) <= qh[d] && __ldg(b + dim + d) >= ql[d];
+            for (int d = 0; d < DM; d += C) {
+                if (D > 0 || d < dim) {
+                    float bl[C], bh[C];
+                    ldChunkF<C>(b + d, bl);
+                    ldChunkF<C>(b + dim + d, bh);
+#pragma unroll
+                    for (int i = 0; i < C; ++i) pass = pass && bl[i] <= qh[d + i] && bh[i] >= ql[d + i];
+                }
+            }
             if (__ballot_sync(FULL, pass) == 0) continue;
             bool keep = false;
             if (pass) {

@@ -148,3 +148,28 @@ def test_knn_batch_split_into_chunks(tb, env, oracle_mod):
     b = oracle_mod.brute_query(pts, ids, oracle_mod.KNN, P[:50], K=20)
     r2 = h.query_batch(tb.QueryType.POINT, P[:50], tb.Mode.EXACT, K=20)
     assert np.array_equal(r2.ids.numpy(), b.ids) and np.array_equal(r2.dist2.numpy(), b.dist2)
+
+
+@pytest.mark.parametrize("beam,completion", [(0, False), (32, False), (0, True), (32, True), (2, True)])
+def test_probe_and_node_major_completion_stay_exact(tb, env, oracle_mod, beam, completion):
+    """Every combination of the probe's beam (0: wave 1 ranks every surviving cluster) and the
+    completion after wave 1 (node-major walk with the clusters' points read once per 32 queries, or
+    the query-major wave 2) returns the FP64 brute force's ids and bit-identical squared distances."""
+    h, o, pts, ids = env
+    P = _points(pts, 300, 41)
+    Kq = np.where(np.arange(300) % 3 == 0, 50, 10).astype(np.uint32)
+    b = oracle_mod.brute_query(pts, ids, oracle_mod.KNN, P[Kq == 10], K=10)
+    b50 = oracle_mod.brute_query(pts, ids, oracle_mod.KNN, P[Kq == 50], K=50)
+    h.set_knn_probe(beam, completion)
+    try:
+        for _ in range(2):  # the first batch may grow the workspaces and rerun
+            r = h.query_batch(tb.QueryType.POINT, P, tb.Mode.EXACT, K=Kq)
+            offs, got, d2 = r.offsets.numpy(), r.ids.numpy(), r.dist2.numpy()
+            for bb, sel in ((b, np.nonzero(Kq == 10)[0]), (b50, np.nonzero(Kq == 50)[0])):
+                for j, q in enumerate(sel):
+                    assert np.array_equal(got[offs[q]:offs[q + 1]], bb.query(j)), (beam, completion, q)
+                    assert np.array_equal(d2[offs[q]:offs[q + 1]], bb.dist2[bb.offsets[j]:bb.offsets[j + 1]])
+        c = h.knn_counters()
+        assert c["rows"] > 0
+    finally:
+        h.set_knn_probe(32, True)
