@@ -307,6 +307,9 @@ def main():
     ap.add_argument("--knn-queries", type=int, default=4096, help="batched: points of the KNN leg")
     ap.add_argument("--knn-steps", type=int, default=10, help="batched: timed steps of the KNN leg")
     ap.add_argument("--no-knn", action="store_true", help="batched: skip the KNN leg")
+    ap.add_argument("--variants", default=None,
+                    help="range configs: launch variant per level (0 direct, 1 staged, 2 node-major), comma "
+                         "list; skips the autotuner (A/B timing, profiling one kind of kernel)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-graph", action="store_true")
     ap.add_argument("--policy", default="L0",
@@ -373,7 +376,12 @@ def main():
     h.query_batch(tb.QueryType.RANGE, dQ, tb.Mode.EXACT)
     import tempfile
     cache = os.environ.get("TBLAEQ_TUNING_CACHE", os.path.join(tempfile.gettempdir(), "tblaeq_tuning.txt"))
-    variants, grids, tuned_ms, tuned_from = h.autotune_cached(dQ, cache, tb.Mode.EXACT, reps=5)
+    if args.variants:
+        variants = [int(v) for v in args.variants.split(",")]
+        grids, tuned_ms, tuned_from = [100] * len(variants), None, "--variants"
+        h.set_launch_shapes(variants, grids)
+    else:
+        variants, grids, tuned_ms, tuned_from = h.autotune_cached(dQ, cache, tb.Mode.EXACT, reps=5)
     h.set_timing(True)
     flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
     for _ in range(args.warmup):
@@ -539,10 +547,10 @@ def main():
         "plain": {"value": plain_qps, "unit": "queries/s", "queries": n_plain,
                   "speedup_batched_vs_plain": value / world / plain_qps},
         "results_per_step": results,
-        "autotune": {"variants": ["staged" if v else "direct" for v in variants], "grid_percent": grids,
+        "autotune": {"variants": [["direct", "staged", "node-major"][v] for v in variants], "grid_percent": grids,
                      "level_ms": tuned_ms, "source": tuned_from, "cache": cache,
-                     "searched": "variant {direct, staged} x persistent grid {100, 75, 50, 25}% of occupancy, "
-                                 "per level, on the live batch"},
+                     "searched": "variant {direct, staged, node-major} x persistent grid {100, 75, 50, 25}% of "
+                                 "occupancy, per level, on the live batch"},
         "level_entries": entries,
         "level_children": items,
         # A finest interval read from mapped host memory is bound by the host link, not HBM.

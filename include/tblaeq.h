@@ -347,8 +347,10 @@ typedef struct {
     int iters;         /* Lloyd iterations per level (0: 20) */
     uint64_t seed;
     int precision;
-    int host_assembly; /* 1: assemble each level on the host from downloaded labels and centroids, as
-                          the reference does (same bytes; for comparisons) */
+    int host_assembly; /* 0: on the device; 1: on the host from downloaded labels and centroids, as the
+                          reference does; 2: both from the same labels and centroids, the device
+                          result kept and checked byte for byte against the host's (an error if they
+                          differ) */
 } tblaeq_build_config;
 
 typedef struct {

@@ -349,11 +349,11 @@ class QueryHandler:
 
     @classmethod
     def build(cls, points, height: int = 4, ratios: Sequence[int] = (100, 50, 20), iters: int = 20, seed: int = 1,
-              precision: "KmeansPrecision" = None, host_assembly: bool = False) -> tuple:
+              precision: "KmeansPrecision" = None, host_assembly: int = 0) -> tuple:
         """IndexBuilder::build over FP32 points (N x D): GPU k-means per level, then the reference's
-        P-tensor / map / radius assembly, on the device (host_assembly=True: on the host from
-        downloaded labels and centroids, like the reference). Returns (handler, per-level reports,
-        finest first)."""
+        P-tensor / map / radius assembly, on the device (host_assembly=1: on the host from
+        downloaded labels and centroids, like the reference; 2: both, the device result checked
+        byte for byte against the host's). Returns (handler, per-level reports, finest first)."""
         X = np.ascontiguousarray(np.asarray(points, dtype=np.float32))
         N, D = X.shape
         r = np.ascontiguousarray(np.array(list(ratios), dtype=np.uint64))

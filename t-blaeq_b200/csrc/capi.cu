@@ -997,7 +997,7 @@ static KmeansConfig kmeansConfigOf(const tblaeq_build_config* cfg) {
         if (cfg->iters > 0) c.iters = cfg->iters;
         c.seed = cfg->seed;
         c.precision = cfg->precision;
-        c.hostAssembly = cfg->host_assembly != 0;
+        c.hostAssembly = cfg->host_assembly;
     }
     return c;
 }
@@ -1006,6 +1006,7 @@ int tblaeq_kmeans_build(const float* points, uint64_t N, uint64_t D, uint64_t he
                         const tblaeq_build_config* cfg, tblaeq_handle** out, tblaeq_build_report* report) {
     if (!points || !out || (height > 1 && !ratios)) return fail(TBLAEQ_ERR_INVALID, "null argument");
     if (cfg && (cfg->precision < 0 || cfg->precision > 2)) return fail(TBLAEQ_ERR_INVALID, "bad precision");
+    if (cfg && (cfg->host_assembly < 0 || cfg->host_assembly > 2)) return fail(TBLAEQ_ERR_INVALID, "bad host_assembly");
     *out = nullptr;
     return guarded([&]() -> int {
         const KmeansConfig c = kmeansConfigOf(cfg);

@@ -29,7 +29,8 @@ void BatchEngine::setLaunchShapes(const std::vector<int>& v, const std::vector<i
 void BatchEngine::setVariants(const std::vector<int>& v) {
     if (v.size() != variants_.size()) throw std::invalid_argument("setVariants: one variant per expand launch");
     for (int x : v)
-        if (x != kVariantDirect && x != kVariantStaged) throw std::invalid_argument("setVariants: unknown variant");
+        if (x != kVariantDirect && x != kVariantStaged && x != kVariantNodeMajor)
+            throw std::invalid_argument("setVariants: unknown variant");
     if (v != variants_) dropGraph();
     variants_ = v;
 }
@@ -43,8 +44,11 @@ std::vector<float> BatchEngine::autotuneRange(const double* dBoxes, uint32_t nq,
         int variant, grid;
     };
     std::vector<Shape> candidates;
-    for (int v : {kVariantDirect, kVariantStaged})
+    const bool nm = useNodeMajor(mode);
+    for (int v : {kVariantDirect, kVariantStaged, kVariantNodeMajor}) {
+        if (v == kVariantNodeMajor && !nm) continue;
         for (int g : {100, 75, 50, 25}) candidates.push_back({v, g});
+    }
     std::vector<std::vector<float>> med(candidates.size(), std::vector<float>(H, 0.f));
     for (size_t c = 0; c < candidates.size(); ++c) {
         setLaunchShapes(std::vector<int>(H, candidates[c].variant), std::vector<int>(H, candidates[c].grid));
@@ -446,13 +450,17 @@ void BatchEngine::enqueueLaunches(const double* dBoxes, uint32_t nq, int mode, u
                        stream_);
     if (mode == kModeExact) launchRoundBoxes(dBoxes, nq, D, boxF_.as<float>(), stream_);
     if (timing_) record(1);
-    // Node-major levels need their buffers at the current capacities (sized by the synchronous
-    // batch that must precede asynchronous ones); without them the batch runs entry-major.
-    const bool nodeMajor = useNodeMajor(mode) && nmEntryCap_ >= caps_.entries && nmResultCap_ >= caps_.results &&
-                           v_.tileStart.bytes() >= tileCap_ * 4 && (!(flags & kWantVals) || nmVals_);
+    // Node-major levels (the variant the autotuner may choose per inner level) need their buffers at
+    // the current capacities (sized by the synchronous batch that must precede asynchronous ones);
+    // without them every level runs entry-major. Once a level ran node-major, the frontiers below it
+    // are in no particular query order, and the results are grouped by query at the end.
+    const bool nmReady = useNodeMajor(mode) && nmEntryCap_ >= caps_.entries && nmResultCap_ >= caps_.results &&
+                         v_.tileStart.bytes() >= tileCap_ * 4 && (!(flags & kWantVals) || nmVals_);
+    bool nodeMajor = false;
     int buf = 0;
     for (int m = 0; m < H; ++m) {
-        if (nodeMajor && m < H - 1) {
+        if (nmReady && m < H - 1 && variants_[m] == kVariantNodeMajor) {
+            nodeMajor = true;
             enqueueNodeMajorLevel(m, buf, dBoxes, nq, wantLevels);
             buf = 1 - buf;
             if (timing_) record(2 + m);

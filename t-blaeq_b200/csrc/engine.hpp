@@ -72,8 +72,9 @@ public:
     bool knnNodeMajor() const { return knnNodeMajor_; }
     // Largest entry / item capacity a batch may use before it must be split (tests lower it).
     void setSplitLimit(uint64_t limit) { splitLimit_ = limit; }
-    // Exact range batches test the inner levels node-major (default on; see NodeMajorArgs): same
-    // results, each query's ids in no particular order. Off: the entry-major kernel at every level.
+    // Exact range batches may run inner levels node-major (see NodeMajorArgs) where the level's
+    // variant is kVariantNodeMajor (the autotuner's choice): same results, each query's ids in no
+    // particular order. Off: those levels run entry-major.
     void setNodeMajor(bool on) {
         if (on != nodeMajor_) dropGraph();
         nodeMajor_ = on;

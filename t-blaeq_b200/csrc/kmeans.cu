@@ -6,6 +6,7 @@
 #include <algorithm>
 #include <chrono>
 #include <cmath>
+#include <cstring>
 #include <limits>
 #include <numeric>
 #include <random>
@@ -702,7 +703,7 @@ HostIndex kmeansBuild(const float* hostPoints, uint64_t N, uint64_t D, uint64_t 
         c.seed = cfg.seed + i;
         kmeansRun(dX.as<float>(), n, D, k, c, C, L, reports[i], s);
         const auto ta = std::chrono::steady_clock::now();
-        if (cfg.hostAssembly) {
+        if (cfg.hostAssembly != kAssembleDevice) {
             std::vector<float> fine(n * D), coarse(k * D);
             std::vector<uint32_t> labels(n);
             TBLAEQ_CUDA(cudaMemcpyAsync(fine.data(), dX.get(), n * D * 4, cudaMemcpyDeviceToHost, s));
@@ -710,8 +711,32 @@ HostIndex kmeansBuild(const float* hostPoints, uint64_t N, uint64_t D, uint64_t 
             TBLAEQ_CUDA(cudaMemcpyAsync(labels.data(), L.get(), n * 4, cudaMemcpyDeviceToHost, s));
             TBLAEQ_CUDA(cudaStreamSynchronize(s));
             assembleInterval(idx, pIdx, fineMesh, fine.data(), n, coarse.data(), k, labels.data());
-        } else {
+        }
+        if (cfg.hostAssembly != kAssembleHost) {
+            // Both: the host result is kept aside and the device result must equal it byte for byte
+            // (the same labels and centroids feed both; k-means itself is not bitwise repeatable,
+            // its FP64 sums are atomic).
+            HostIndex ref;
+            const bool both = cfg.hostAssembly == kAssembleBoth;
+            if (both) {
+                ref.pTensors.push_back(std::move(idx.pTensors[pIdx]));
+                ref.maps.push_back(std::move(idx.maps[fineMesh]));
+                ref.radius.push_back(std::move(idx.radius[pIdx]));
+            }
             assembleIntervalDevice(idx, pIdx, fineMesh, dX.as<float>(), n, C.as<float>(), k, L.as<uint32_t>(), s);
+            if (both) {
+                const PTensor& a = idx.pTensors[pIdx];
+                const PTensor& b = ref.pTensors[0];
+                const bool same = a.colRes == b.colRes && a.nnzPerCol == b.nnzPerCol && a.rowIds == b.rowIds &&
+                                  std::memcmp(a.vals.data(), b.vals.data(), a.vals.size() * 8) == 0 &&
+                                  a.vals.size() == b.vals.size() && idx.maps[fineMesh] == ref.maps[0] &&
+                                  idx.radius[pIdx].size() == ref.radius[0].size() &&
+                                  std::memcmp(idx.radius[pIdx].data(), ref.radius[0].data(),
+                                              ref.radius[0].size() * 8) == 0;
+                if (!same)
+                    throw std::runtime_error("k-means build: device and host assembly differ at interval " +
+                                             std::to_string(pIdx));
+            }
         }
         reports[i].assembleSeconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - ta).count();
         if (i + 2 == height) {

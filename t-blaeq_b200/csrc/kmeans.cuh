@@ -30,13 +30,17 @@ namespace tblaeq {
 
 enum KmeansPrecision : int { kKmTensor = 0, kKmFp32 = 1, kKmFp64 = 2 };
 
+enum AssemblyMode : int { kAssembleDevice = 0, kAssembleHost = 1, kAssembleBoth = 2 };
+
 struct KmeansConfig {
     int iters = 20;
     uint64_t seed = 1;
     int precision = kKmTensor;
-    // Assemble each interval (P-tensor, map, radii) on the host from downloaded labels and
-    // centroids, as the reference does, instead of on the device (for comparisons).
-    bool hostAssembly = false;
+    // Where each interval (P-tensor, map, radii) is assembled: kAssembleDevice (labels and
+    // centroids stay on the device), kAssembleHost (from downloaded labels and centroids, as the
+    // reference does), or kAssembleBoth (device result, checked byte for byte against the host's
+    // from the same labels and centroids; an error when they differ).
+    int hostAssembly = 0;
 };
 
 struct KmeansLevelReport {

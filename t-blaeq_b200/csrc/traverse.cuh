@@ -126,7 +126,10 @@ enum Pred : int {
 
 // Kernel variants an autotuner chooses between per level: rows loaded straight into registers,
 // or streamed through a per-warp cp.async ring in shared memory.
-enum Variant : int { kVariantDirect = 0, kVariantStaged = 1 };
+// A third choice exists for the inner levels of exact range batches only: kVariantNodeMajor runs the
+// level node-major (nodeMajorRangeKernel + a kPredAll expand, see NodeMajorArgs); elsewhere it
+// launches as kVariantDirect.
+enum Variant : int { kVariantDirect = 0, kVariantStaged = 1, kVariantNodeMajor = 2 };
 
 struct ExpandArgs {
     FrontierIn in;

@@ -86,19 +86,15 @@ def test_built_index_objective_and_exact_queries(tb, oracle_mod, tmp_path, cuda)
 
 def test_device_assembly_writes_the_host_assembly_bytes(tb, tmp_path, cuda):
     """The P-tensors, maps and radii assembled on the device (labels and centroids never leave it)
-    are byte-identical to the host assembly from downloaded labels and centroids (the reference's
-    Genenate_One_P_Tensor / Compute_Max_Radius order of work), file by file."""
-    import filecmp
-    import os
+    are byte-identical to the host assembly (the reference's Genenate_One_P_Tensor /
+    Compute_Max_Radius order of work) from the same labels and centroids: the build's `both` mode
+    assembles every level both ways and fails on any difference. (Two separate builds are not
+    compared: k-means itself is not bitwise repeatable, its FP64 sums are atomic.)"""
     X = _mixture(300000, 8, 13, nclusters=700)
-    hd, rd = tb.QueryHandler.build(X, height=4, ratios=(50, 20, 10), iters=4, seed=3)
-    hh, rh = tb.QueryHandler.build(X, height=4, ratios=(50, 20, 10), iters=4, seed=3, host_assembly=True)
-    assert [r["objective"] for r in rd] == [r["objective"] for r in rh]
-    a, b = str(tmp_path / "dev"), str(tmp_path / "host")
-    hd.save_index(a)
-    hh.save_index(b)
-    names = sorted(os.listdir(a))
-    assert names == sorted(os.listdir(b)) and len(names) >= 9
-    for n in names:
-        assert filecmp.cmp(os.path.join(a, n), os.path.join(b, n), shallow=False), n
-    assert all(r["assemble_seconds"] > 0 for r in rd)
+    h, rep = tb.QueryHandler.build(X, height=4, ratios=(50, 20, 10), iters=4, seed=3, host_assembly=2)
+    assert [r["k"] for r in rep] == [6000, 300, 30]
+    assert all(r["assemble_seconds"] > 0 for r in rep)
+    hd, _ = tb.QueryHandler.build(X, height=4, ratios=(50, 20, 10), iters=4, seed=3)
+    info = hd.info()
+    assert info["meshSizes"][:4] == [300000, 6000, 300, 30]
+    h.save_index(str(tmp_path / "both"))

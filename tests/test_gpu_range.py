@@ -284,8 +284,9 @@ def test_node_major_levels_equal_entry_major(tb, env, oracle_mod, flags):
     Q = _boxes(pts, 700, 31, hi_frac=0.3)  # a workspace that grows: several growth steps
     b = oracle_mod.brute_query(pts, ids, oracle_mod.RANGE, Q)
     out = {}
+    H = h.info()["height"]
     for nm in (False, True):
-        h.set_node_major(nm)
+        h.set_launch_shapes([2 if nm else 0] * H, [100] * H)  # variant 2: node-major inner levels
         r = h.query_batch(tb.QueryType.RANGE, Q, tb.Mode.EXACT, flags=flags)
         offs, got = r.offsets.numpy(), r.ids.numpy()
         lv = r.level_items.numpy().copy() if r.level_items is not None else None
@@ -303,4 +304,13 @@ def test_node_major_levels_equal_entry_major(tb, env, oracle_mod, flags):
             order = np.argsort(got)
             rows = dict(zip(ids.tolist(), range(len(ids))))
             assert np.array_equal(vals[order], pts[[rows[int(i)] for i in got[order]]])
+    # Mixed: node-major at one level only, entry-major below it.
+    h.set_launch_shapes([0, 2] + [0] * (H - 2), [100] * H)
+    r = h.query_batch(tb.QueryType.RANGE, Q, tb.Mode.EXACT, flags=flags)
+    assert np.array_equal(r.offsets.numpy(), b.offsets)
+    assert all(np.array_equal(g, b.query(q)) for q, g in enumerate(ids_by_query(r.offsets.numpy(), r.ids.numpy())))
+    h.set_node_major(False)  # node-major disabled: the variant launches entry-major
+    r = h.query_batch(tb.QueryType.RANGE, Q, tb.Mode.EXACT, flags=flags)
+    assert np.array_equal(r.ids.numpy(), out[False][5])
     h.set_node_major(True)
+    h.set_launch_shapes([0] * H, [100] * H)
