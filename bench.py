@@ -859,7 +859,9 @@ def reference_cuda(idx_dir, Q, D, kind, K=0, timeout=1800):
         return {"unavailable": "the reference build (oracle/_ref) is not present"}
     import tempfile
     with tempfile.TemporaryDirectory() as d:
-        qf = os.path.join(d, "q.txt")
+        # The reference labels a query file by the text after the last '_' of its path
+        # (src/utils/Utils.cu:18-35): keep it free of '-'.
+        qf = os.path.join(d, "q_" + kind + ".txt")
         write_query_file(qf, Q, D)
         out = os.path.join(d, "ref.bin")
         subprocess.run([harness, idx_dir, qf, "1" if kind == "knn" else "0", str(K), "L0", out], check=True,

@@ -238,8 +238,9 @@ int tblaeq_set_two_wave(tblaeq_handle* h, int on);
  * and wave 1 ranks only the clusters under them (0: every surviving cluster is ranked) -- and
  * node_major_completion (default 1) selects how the points within wave 1's bound are found: the
  * hierarchy walked again node-major (one warp per node and 32 of its queries; each cluster's points
- * read once per 32 of its queries), or 0: every remaining frontier entry expanded query by query.
- * Exactness never depends on either. No counterpart in the reference. */
+ * read once per 32 of its queries), or 0: every remaining frontier entry expanded query by query
+ * (the beam is then not applied: that wave only covers the frontier). Exactness never depends on
+ * either. No counterpart in the reference. */
 int tblaeq_set_knn_probe(tblaeq_handle* h, uint32_t beam, int node_major_completion);
 
 /* Counters of the last KNN batch (summed over its chunks when it ran in several): [0] final-frontier

@@ -4,10 +4,10 @@
 //
 // It calls the reference's own refine service, tblaeq::file_index::run_query_service
 // (src/file_index/IndexJsonTblaeqQuery.cu:294-380), once per request over one QueryHandler
-// prepared with policy L0 (the reference tool itself prepares L3, src/file_index/IndexJsonTblaeqQuery.cu:387,
-// whose grid-ownership flags are known to be wrong, src/core/strategies/L3Strategy.cu:124; the
-// candidate sets do not depend on the policy), and writes every request's result as text so the
-// parity tests can compare the B200 refine service with it.
+// prepared with policy L3, as the reference tool's own query does (src/file_index/IndexJsonTblaeqQuery.cu:387):
+// the service reads the final grid's ids on the host, which only L3's host-resident grids allow
+// (with L0 the grid is device memory). The results go out as text so the parity tests can compare
+// the B200 refine service with them.
 //
 // usage: file_index_harness <index_root> <requests.txt> <out.txt>
 //
@@ -46,7 +46,7 @@ int main(int argc, char** argv) {
     std::ostringstream sink;
     std::streambuf* old = std::cout.rdbuf(sink.rdbuf());
     QueryHandler handler(root + "/" + kDefaultTblaeqDir, /*loadFromIndex=*/true);
-    handler.prepareForQuery(LevelPolicy::L0);
+    handler.prepareForQuery(LevelPolicy::L3);
 
     std::string line;
     while (std::getline(req, line)) {

@@ -820,8 +820,10 @@ void BatchEngine::enqueueKnn(const double* dPoints, uint32_t nq, const uint32_t*
         a.variant = kVariantDirect;
         return a;
     };
-    const bool probe = twoWave_ && probeBeam_ > 0;
+    // The beam leaves clusters out of the last frontier, so only the completion that walks the
+    // hierarchy again from the root (not the query-major wave 2 over that frontier) may follow it.
     const bool completion = twoWave_ && knnNodeMajor_;
+    const bool probe = completion && probeBeam_ > 0;
     auto* qcountP = reinterpret_cast<uint32_t*>(z + offQcountP_);
     if (probe) launchFillU32(probeK_.as<uint32_t>(), probeBeam_, nq, stream_);
     int buf = 0;

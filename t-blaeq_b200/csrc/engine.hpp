@@ -62,7 +62,7 @@ public:
     // probeBeam entries of smallest lower bound at every level above the clusters, so wave 1 ranks
     // only the clusters under them; 0: no beam, every surviving cluster is ranked), and whether the
     // completion after wave 1 walks the hierarchy node-major (default) or expands every remaining
-    // frontier entry query by query.
+    // frontier entry query by query (the beam then stays off: that wave only covers the frontier).
     void setKnnProbe(uint32_t beam, bool nodeMajorCompletion) {
         if (beam > 32) throw std::invalid_argument("probe beam must be at most 32");
         probeBeam_ = beam;

@@ -1212,17 +1212,34 @@ __global__ void nodeScatterKernel(const uint32_t* node, const uint32_t* hdr, uin
 }
 
 constexpr int kNodeMajorThreads = 128;
+constexpr int kNodeMajorStage = 128;  // survivors a warp stages in shared memory between appends
+constexpr int kNodeMajorChunk = 64;   // children whose float boxes a warp stages in shared memory at once
 
 // One warp per unit (a node and up to 32 of the entries holding it), claimed through a ticket.
-// Lanes hold one query box each; the loop runs over the node's children with a warp-uniform
-// trip count, so every child's float box is one broadcast load for the whole warp.
+// Lanes hold one query's float box each. The loop runs over the node's children with a
+// warp-uniform trip count; the children's float boxes are staged in shared memory a chunk at a
+// time, so each box is read from memory once per 32 queries. Survivors are staged per warp in
+// shared memory and appended with one atomic per flush (at most kNodeMajorStage of them, and at
+// the end of the unit), not one per child.
 template <int D>
 __global__ void __launch_bounds__(kNodeMajorThreads) nodeMajorRangeKernel(NodeMajorArgs a) {
     constexpr uint32_t FULL = 0xffffffffu;
     constexpr int DM = D > 0 ? D : 32;
+    // The FP64 test is rare (children whose float box meets the query's): its double box and the
+    // node's coordinates stay in memory (L1) rather than in registers, which would cost occupancy.
+    constexpr int DR = 1;
+    constexpr bool kRegs = false;
+    __shared__ uint32_t sQ[kNodeMajorThreads / 32][kNodeMajorStage];
+    __shared__ uint32_t sJ[kNodeMajorThreads / 32][kNodeMajorStage];
+    // The float boxes of up to kNodeMajorChunk children of the unit's node, copied in with coalesced
+    // 16-byte loads by the whole warp (one round of loads instead of one dependent load per child).
+    constexpr int kBoxFloats = 2 * (D > 0 ? D : 16);
+    constexpr bool kStageBoxes = D > 0 && D % 2 == 0 && D <= 16;
+    __shared__ __align__(16) float sBox[kStageBoxes ? kNodeMajorThreads / 32 : 1][kStageBoxes ? kNodeMajorChunk * kBoxFloats : 1];
     if (*a.status & (kStatusLookbackTimeout | kStatusWindowOverflow)) return;
     const int dim = D > 0 ? D : a.D;
     const int lane = threadIdx.x & 31;
+    const int w = threadIdx.x >> 5;
     const uint32_t lanesLt = (1u << lane) - 1u;
     if (a.inHdr[0] > a.inCap) {
         if (blockIdx.x == 0 && threadIdx.x == 0) atomicOr(a.status, kStatusOverflowEntries);
@@ -1231,6 +1248,34 @@ __global__ void __launch_bounds__(kNodeMajorThreads) nodeMajorRangeKernel(NodeMa
     const uint32_t entries = a.inHdr[0];
     const bool root = a.nNodes == 0;
     const uint32_t units = root ? (entries + 31u) / 32u : a.unitOff[a.nNodes];
+    uint32_t staged = 0;  // warp-uniform
+    const double* xp = nullptr;
+    // Appends the staged survivors of the current unit (all children of one node, so they share the
+    // node's coordinates xp) at consecutive positions.
+    auto flush = [&]() {
+        if (staged == 0) return;
+        uint32_t base = 0;
+        if (lane == 0) base = atomicAdd(a.vcount, staged);
+        base = __shfl_sync(FULL, base, 0);
+        __syncwarp();
+        for (uint32_t i = lane; i < staged; i += 32) {
+            const uint32_t pos = base + i;
+            if (pos < a.vcap) {
+                a.vq[pos] = sQ[w][i];
+                a.vcbeg[pos] = sJ[w][i];
+                a.vcpre[pos] = pos;
+                double* xo = a.vx + static_cast<size_t>(pos) * dim;
+#pragma unroll
+                for (int d = 0; d < DM; ++d)
+                    if (D > 0 || d < dim) xo[d] = __ldg(xp + d);
+                if ((pos % kWarpTile) == 0 && pos / kWarpTile < a.vtileCap) a.vtile[pos / kWarpTile] = pos;
+            } else {
+                atomicOr(a.status, kStatusOverflowEntries);
+            }
+        }
+        __syncwarp();
+        staged = 0;
+    };
     while (true) {
         uint32_t u = 0;
         if (lane == 0) u = atomicAdd(a.ticket, 1u);
@@ -1262,10 +1307,12 @@ __global__ void __launch_bounds__(kNodeMajorThreads) nodeMajorRangeKernel(NodeMa
             if (a.levelItems) atomicAdd(&a.levelItems[q], cnt);
         }
         // Every entry of the node carries the node's coordinates: take the first one's.
-        const double* xp = a.inX + static_cast<size_t>(__shfl_sync(FULL, e, 0)) * dim;
+        xp = a.inX + static_cast<size_t>(__shfl_sync(FULL, e, 0)) * dim;
         float ql[DM], qh[DM];
+        double xr[DR], bl[DR], bh[DR];
         {
             const float* f = a.boxesF + static_cast<size_t>(q) * 2 * dim;
+            const double* box = a.boxes + static_cast<size_t>(q) * 2 * dim;
 #pragma unroll
             for (int d = 0; d < DM; ++d) {
                 if (D > 0 || d < dim) {
@@ -1273,20 +1320,47 @@ __global__ void __launch_bounds__(kNodeMajorThreads) nodeMajorRangeKernel(NodeMa
                     qh[d] = active ? __ldg(f + dim + d) : -1.f;
                 }
             }
+            if constexpr (kRegs) {
+#pragma unroll
+                for (int d = 0; d < DR; ++d) {
+                    xr[d] = __ldg(xp + d);
+                    bl[d] = active ? __ldg(box + d) : 0.0;
+                    bh[d] = active ? __ldg(box + dim + d) : 0.0;
+                }
+            }
         }
         for (uint32_t c = 0; c < cnt; ++c) {
             const uint32_t j = cbeg + c;
             const float* b = a.aabb + static_cast<size_t>(j) * 2 * dim;
+            if constexpr (kStageBoxes) {
+                if (c % kNodeMajorChunk == 0) {  // warp-uniform: stage the next chunk of boxes
+                    const uint32_t n = min(static_cast<uint32_t>(kNodeMajorChunk), cnt - c);
+                    const float4* src = reinterpret_cast<const float4*>(b);
+                    float4* dst = reinterpret_cast<float4*>(sBox[w]);
+                    __syncwarp();
+                    for (uint32_t i = lane; i < n * (kBoxFloats / 4); i += 32) dst[i] = __ldg(src + i);
+                    __syncwarp();
+                }
+                b = sBox[w] + (c % kNodeMajorChunk) * kBoxFloats;
+            }
             bool pass = active;
             constexpr int C = chunkOf<D>();
 #pragma unroll
             for (int d = 0; d < DM; d += C) {
                 if (D > 0 || d < dim) {
-                    float bl[C], bh[C];
-                    ldChunkF<C>(b + d, bl);
-                    ldChunkF<C>(b + dim + d, bh);
+                    float cl[C], ch[C];
+                    if constexpr (kStageBoxes) {
 #pragma unroll
-                    for (int i = 0; i < C; ++i) pass = pass && bl[i] <= qh[d + i] && bh[i] >= ql[d + i];
+                        for (int i = 0; i < C; ++i) {
+                            cl[i] = b[d + i];
+                            ch[i] = b[dim + d + i];
+                        }
+                    } else {
+                        ldChunkF<C>(b + d, cl);
+                        ldChunkF<C>(b + dim + d, ch);
+                    }
+#pragma unroll
+                    for (int i = 0; i < C; ++i) pass = pass && cl[i] <= qh[d + i] && ch[i] >= ql[d + i];
                 }
             }
             if (__ballot_sync(FULL, pass) == 0) continue;
@@ -1297,40 +1371,37 @@ __global__ void __launch_bounds__(kNodeMajorThreads) nodeMajorRangeKernel(NodeMa
                 // in dimension order, against the child's subtree radius.
                 const NodeRec nr = a.children[j];
                 const double* row = a.rows + static_cast<size_t>(j) * dim;
-                const double* box = a.boxes + static_cast<size_t>(q) * 2 * dim;
                 double dist = 0.0;
+                if constexpr (kRegs) {
+                    double r[DR];
 #pragma unroll
-                for (int d = 0; d < DM; ++d) {
-                    if (D > 0 || d < dim) {
-                        const double r = a.rowsOnHost ? row[d] : __ldg(row + d);
-                        const double y = __dmul_rn(r, __ldg(xp + d));
-                        dist = boxGapAcc(y, __ldg(box + d), __ldg(box + dim + d), dist, 1);
+                    for (int d = 0; d < DR; ++d) r[d] = a.rowsOnHost ? row[d] : __ldg(row + d);
+#pragma unroll
+                    for (int d = 0; d < DR; ++d) dist = boxGapAcc(__dmul_rn(r[d], xr[d]), bl[d], bh[d], dist, 1);
+                } else {
+                    const double* box = a.boxes + static_cast<size_t>(q) * 2 * dim;
+#pragma unroll
+                    for (int d = 0; d < DM; ++d) {
+                        if (D > 0 || d < dim) {
+                            const double r = a.rowsOnHost ? row[d] : __ldg(row + d);
+                            const double y = __dmul_rn(r, __ldg(xp + d));
+                            dist = boxGapAcc(y, __ldg(box + d), __ldg(box + dim + d), dist, 1);
+                        }
                     }
                 }
                 keep = nr.cnt > 0 && dist <= __dmul_rn(nr.rad, nr.rad);
             }
             const uint32_t kb = __ballot_sync(FULL, keep);
             if (kb == 0) continue;
-            const int leader = __ffs(kb) - 1;
-            uint32_t pos0 = 0;
-            if (lane == leader) pos0 = atomicAdd(a.vcount, static_cast<uint32_t>(__popc(kb)));
-            pos0 = __shfl_sync(FULL, pos0, leader);
             if (keep) {
-                const uint32_t pos = pos0 + __popc(kb & lanesLt);
-                if (pos < a.vcap) {
-                    a.vq[pos] = q;
-                    a.vcbeg[pos] = j;
-                    a.vcpre[pos] = pos;
-                    double* xo = a.vx + static_cast<size_t>(pos) * dim;
-#pragma unroll
-                    for (int d = 0; d < DM; ++d)
-                        if (D > 0 || d < dim) xo[d] = __ldg(xp + d);
-                    if ((pos % kWarpTile) == 0 && pos / kWarpTile < a.vtileCap) a.vtile[pos / kWarpTile] = pos;
-                } else {
-                    atomicOr(a.status, kStatusOverflowEntries);
-                }
+                const uint32_t slot = staged + __popc(kb & lanesLt);
+                sQ[w][slot] = q;
+                sJ[w][slot] = j;
             }
+            staged += __popc(kb);
+            if (staged + 32 > static_cast<uint32_t>(kNodeMajorStage)) flush();
         }
+        flush();
     }
 }
 

@@ -17,9 +17,12 @@ reference's selection and ordering rules. Two coarse modes:
 
 * Mode.REF_PARITY: the reference's candidate sets (its non-conservative per-level pruning and
   STEP selection), so the matches equal the reference tool's, request for request;
-* Mode.EXACT: range candidates are exactly the records whose index vector lies in the query box
-  (the reference's pruning can miss some), KNN candidates exactly the K nearest points of the
-  index (its decoded coordinates, FP64 distances, smaller id first on ties).
+* Mode.EXACT: range candidates are exactly the records whose index vector encodes a timestamp in
+  [start, end] (and a sequence between the smallest and largest requested): the interval is queried
+  as the few boxes whose union it is (`interval_boxes`). The reference queries one box of per-limb
+  minima and maxima and prunes non-conservatively, so it can miss such records. KNN candidates are
+  exactly the K nearest points of the index (its decoded coordinates, FP64 distances, smaller id
+  first on ties).
 
 Refinement (same rules as the reference):
 * knn: slots of candidate records of the request's sequence, ordered by |timestamp_us - target|,
@@ -63,6 +66,40 @@ def split_timestamp_3d(timestamp: float):
         raise RuntimeError("negative timestamp is not supported")
     mask = (1 << 21) - 1
     return (float(((us >> 42) & mask) + 1), float(((us >> 21) & mask) + 1), float((us & mask) + 1))
+
+
+def interval_boxes(start: float, end: float, seq_lo: int, seq_hi: int):
+    """Boxes in index-vector space (lo[4] | hi[4]) whose union holds exactly the vectors of the
+    microsecond timestamps in [start, end] (sequences seq_lo..seq_hi). The vector splits a timestamp
+    into three 21-bit limbs, so the interval is a run in lexicographic limb order: at most five boxes
+    (a partial low limb, partial middle limbs, whole top limbs, and the mirror images at the end).
+    The reference's single box of per-limb minima and maxima is not this set: it misses timestamps
+    whose low limbs fall outside the end points' (and can hold ones outside the interval)."""
+    s_us, e_us = timestamp_to_us(start), timestamp_to_us(end)
+    if s_us < 0 or e_us < 0:
+        raise RuntimeError("negative timestamp is not supported")
+    m = (1 << 21) - 1
+    a0, b0, c0 = s_us >> 42, (s_us >> 21) & m, s_us & m
+    a1, b1, c1 = e_us >> 42, (e_us >> 21) & m, e_us & m
+    runs = []  # (a range, b range, c range), limb values before the + 1
+    if a0 == a1 and b0 == b1:
+        runs.append(((a0, a0), (b0, b0), (c0, c1)))
+    elif a0 == a1:
+        runs.append(((a0, a0), (b0, b0), (c0, m)))
+        if b0 + 1 <= b1 - 1:
+            runs.append(((a0, a0), (b0 + 1, b1 - 1), (0, m)))
+        runs.append(((a0, a0), (b1, b1), (0, c1)))
+    else:
+        runs.append(((a0, a0), (b0, b0), (c0, m)))
+        if b0 < m:
+            runs.append(((a0, a0), (b0 + 1, m), (0, m)))
+        if a0 + 1 <= a1 - 1:
+            runs.append(((a0 + 1, a1 - 1), (0, m), (0, m)))
+        if b1 > 0:
+            runs.append(((a1, a1), (0, b1 - 1), (0, m)))
+        runs.append(((a1, a1), (b1, b1), (0, c1)))
+    return [np.array([ra[0] + 1, rb[0] + 1, rc[0] + 1, seq_lo, ra[1] + 1, rb[1] + 1, rc[1] + 1, seq_hi],
+                     dtype=np.float64) for ra, rb, rc in runs]
 
 
 def binary_index_record_size(n: int, file_name_bytes: int) -> int:
@@ -363,17 +400,26 @@ class FileIndexService:
         cands = {}
         rng = [(i, s, v) for i, s, v in checked if requests[i].mode == "range"]
         if rng:
-            boxes = np.ascontiguousarray(np.stack([v for _, _, v in rng]))
             if mode == Mode.EXACT:
-                # Index vectors are integers (limbs + 1, sequence numbers), and the index's decoded
-                # coordinates differ from them by rounding only (far below 0.25): the box widened by
-                # a quarter holds exactly the records whose stored vector lies in the box.
+                # The boxes whose union is exactly the request's interval (and sequence range).
+                # Index vectors are integers (limbs + 1, sequence numbers) and the index's decoded
+                # coordinates differ from them by rounding only (far below 0.25): boxes widened by a
+                # quarter hold exactly the records whose stored vector lies in them.
+                per = [interval_boxes(requests[i].start, requests[i].end, sq[0], sq[-1]) for i, sq, _ in rng]
+                boxes = np.stack([b for bs in per for b in bs])
                 boxes[:, :KNN_DIM] -= 0.25
                 boxes[:, KNN_DIM:] += 0.25
-            res = self.handler.query_batch(QueryType.RANGE, boxes, mode)
+                owner = np.repeat(np.arange(len(rng)), [len(bs) for bs in per])
+            else:
+                boxes = np.stack([v for _, _, v in rng])
+                owner = np.arange(len(rng))
+            res = self.handler.query_batch(QueryType.RANGE, np.ascontiguousarray(boxes), mode)
             offs, ids = res.offsets.numpy(), (res.ids.numpy() if res.total else np.zeros(0, np.uint64))
+            parts = [[] for _ in rng]
+            for b, j in enumerate(owner):
+                parts[j].append(ids[offs[b]:offs[b + 1]])
             for j, (i, _, _) in enumerate(rng):
-                cands[i] = ids[offs[j]:offs[j + 1]]
+                cands[i] = np.concatenate(parts[j]) if parts[j] else np.zeros(0, np.uint64)
         knn = [(i, s, v) for i, s, v in checked if requests[i].mode == "knn"]
         if knn and mode == Mode.EXACT:
             pts = np.ascontiguousarray(np.stack([v for _, _, v in knn]))

@@ -175,3 +175,28 @@ def test_payload_dump_returns_the_source_bytes(fi, dataset, tmp_path):
             assert data == by_ts["%.6f" % m.timestamp]
             checked += 1
     assert checked == 40 + 30 + 25
+
+
+def test_interval_boxes_cover_exactly_the_interval(fi):
+    """The boxes of an interval hold exactly the timestamps in it, whichever limbs the end points
+    share (checked against every microsecond of short intervals and random ones across limbs)."""
+    rng = np.random.default_rng(9)
+    m = (1 << 21) - 1
+
+    def inside(us, boxes):
+        v = np.array([((us >> 42) & m) + 1, ((us >> 21) & m) + 1, (us & m) + 1, 1.0])
+        return sum(bool(np.all(b[:4] <= v) and np.all(v <= b[4:])) for b in boxes)
+
+    for s_us, e_us in [(5 << 21, (5 << 21) + 10), ((7 << 21) - 3, (7 << 21) + 3), ((1 << 42) - 2, (1 << 42) + 2),
+                       (123, 123)]:
+        boxes = fi.interval_boxes(s_us / 1e6, e_us / 1e6, 1, 1)
+        lo_us, hi_us = fi.timestamp_to_us(s_us / 1e6), fi.timestamp_to_us(e_us / 1e6)
+        for us in range(lo_us - 5, hi_us + 6):
+            assert inside(us, boxes) == (1 if lo_us <= us <= hi_us else 0), (s_us, e_us, us)
+    for _ in range(200):
+        a = float(rng.uniform(T0, T0 + 50))
+        b = a + float(np.exp(rng.uniform(np.log(1e-5), np.log(1e5))))
+        boxes = fi.interval_boxes(a, b, 1, 1)
+        lo_us, hi_us = fi.timestamp_to_us(a), fi.timestamp_to_us(b)
+        for us in list(rng.integers(lo_us, hi_us + 1, 20)) + [lo_us, hi_us, lo_us - 1, hi_us + 1]:
+            assert inside(int(us), boxes) == (1 if lo_us <= us <= hi_us else 0)

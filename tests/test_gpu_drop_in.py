@@ -47,7 +47,10 @@ def index(tb, wl, tmp_path_factory, cuda):
     h.save_index(idx)
     Q = wl.range_boxes(h, 40, seed=5, half_width=0.05)
     P = wl.knn_points(h, 20, seed=6, noise=0.01)
-    fq, fp = str(d / "range.txt"), str(d / "knn.txt")
+    # The reference derives a label from the query file's name (the text after the last '_' of the
+    # whole path, src/utils/Utils.cu:18-35) and aborts when that text holds a '-' that is not
+    # "<int>-<int>": name the files so that it reads "range" / "knn".
+    fq, fp = str(d / "q_range.txt"), str(d / "q_knn.txt")
     tb.save_query_file(fq, tb.QueryType.RANGE, Q, 5)
     tb.save_query_file(fp, tb.QueryType.POINT, P, 5)
     return d, idx, fq, fp, Q, P

@@ -7,11 +7,10 @@ answers all of them in two batched traversals:
 * in ref-parity mode the matches are identical to the reference's, request for request (rank,
   record, slot, sequence, type, timestamp, difference, payload offset and size, data file), and so
   are the candidate, record and slot counts;
-* in exact mode the coarse candidates are exactly the records whose index vector lies in the query
-  box (range: the stored index vectors of the JSONL index) or the K nearest points of the T-BLAEQ
-  index (KNN: the FP64 brute force over its decoded points, id tie-break), and the refined matches
-  equal the refine of those candidates;
-  range requests never lose a match against ref-parity mode.
+* in exact mode the coarse candidates are exactly the records whose stored index vector encodes a
+  timestamp in the request's interval (range) or the K nearest points of the T-BLAEQ index (KNN:
+  the FP64 brute force over its decoded points, id tie-break), and the refined matches equal the
+  refine of those candidates; range requests never lose a match against ref-parity mode.
 """
 import os
 import subprocess
@@ -113,8 +112,11 @@ def test_exact_mode_equals_brute_force_candidates(service, oracle_mod):
     for q, r in enumerate(reqs):
         seqs, v = fi._check_request(r)
         if r.mode == "range":
-            lo, hi = v[:4], v[4:]
-            cand = ids[np.all((vecs >= lo) & (vecs <= hi), axis=1)]
+            # Records whose index vector encodes a timestamp in [start, end], sequences in range.
+            lim = vecs[:, :3].astype(np.int64) - 1
+            us = (lim[:, 0] << 42) | (lim[:, 1] << 21) | lim[:, 2]
+            s_us, e_us = fi.timestamp_to_us(r.start), fi.timestamp_to_us(r.end)
+            cand = ids[(us >= s_us) & (us <= e_us) & (vecs[:, 3] >= seqs[0]) & (vecs[:, 3] <= seqs[-1])]
         else:
             b = oracle_mod.brute_query(dec_pts, dec_ids, oracle_mod.KNN, v[None, :], K=r.knn_k)
             cand = b.ids
