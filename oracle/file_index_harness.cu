@@ -19,6 +19,7 @@
 //   M <rank> <item_no> <seq> <dtype> <slot> <timestamp %.17g> <diff_us> <payload_offset> <payload_size> <data_file>
 // or, when the reference throws:
 //   E <message>
+// The output is flushed after every request, so a run that dies leaves the requests before it.
 #include <cstdio>
 #include <fstream>
 #include <iostream>
@@ -90,6 +91,7 @@ int main(int argc, char** argv) {
                 if (c == '\n') c = ' ';
             std::fprintf(out, "E %s\n", msg.c_str());
         }
+        std::fflush(out);  // a request's lines are complete on disk before the next one runs
     }
     std::fclose(out);
     std::cout.rdbuf(old);

@@ -1128,12 +1128,17 @@ namespace {
 
 // Node keys at or above M (only an inconsistent frontier has them) are skipped by the count and the
 // scatter alike, so the grouping stays within its arrays.
+// Entries come in runs of the same node (a unit's survivors are appended child by child), so the
+// lanes of a warp holding one node add to its count (and claim its list slots) with one atomic.
 __global__ void nodeCountKernel(const uint32_t* node, const uint32_t* hdr, uint32_t cap, uint32_t M,
                                 uint32_t* nodeCnt) {
     const uint32_t n = min(hdr[0], cap);
-    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-        const uint32_t nd = node[i];
-        if (nd < M) atomicAdd(&nodeCnt[nd], 1u);
+    const uint32_t lane = threadIdx.x & 31u;
+    for (uint32_t base = blockIdx.x * blockDim.x + (threadIdx.x & ~31u); base < n; base += gridDim.x * blockDim.x) {
+        const uint32_t i = base + lane;
+        const uint32_t nd = i < n ? node[i] : M;
+        const uint32_t peers = __match_any_sync(0xffffffffu, nd);
+        if (nd < M && lane == static_cast<uint32_t>(__ffs(peers) - 1)) atomicAdd(&nodeCnt[nd], __popc(peers));
     }
 }
 
@@ -1205,9 +1210,16 @@ __global__ void __launch_bounds__(1024) nodeScanKernel(const uint32_t* nodeCnt, 
 __global__ void nodeScatterKernel(const uint32_t* node, const uint32_t* hdr, uint32_t cap, uint32_t M,
                                   const uint32_t* nodeOff, uint32_t* cursor, uint32_t* list) {
     const uint32_t n = min(hdr[0], cap);
-    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-        const uint32_t nd = node[i];
-        if (nd < M) list[nodeOff[nd] + atomicAdd(&cursor[nd], 1u)] = i;
+    const uint32_t lane = threadIdx.x & 31u;
+    for (uint32_t base = blockIdx.x * blockDim.x + (threadIdx.x & ~31u); base < n; base += gridDim.x * blockDim.x) {
+        const uint32_t i = base + lane;
+        const uint32_t nd = i < n ? node[i] : M;
+        const uint32_t peers = __match_any_sync(0xffffffffu, nd);
+        const int leader = __ffs(peers) - 1;
+        uint32_t b = 0;
+        if (nd < M && static_cast<int>(lane) == leader) b = atomicAdd(&cursor[nd], __popc(peers));
+        b = __shfl_sync(0xffffffffu, b, leader);
+        if (nd < M) list[nodeOff[nd] + b + __popc(peers & ((1u << lane) - 1u))] = i;
     }
 }
 

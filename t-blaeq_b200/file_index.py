@@ -17,12 +17,15 @@ reference's selection and ordering rules. Two coarse modes:
 
 * Mode.REF_PARITY: the reference's candidate sets (its non-conservative per-level pruning and
   STEP selection), so the matches equal the reference tool's, request for request;
-* Mode.EXACT: range candidates are exactly the records whose index vector encodes a timestamp in
-  [start, end] (and a sequence between the smallest and largest requested): the interval is queried
-  as the few boxes whose union it is (`interval_boxes`). The reference queries one box of per-limb
-  minima and maxima and prunes non-conservatively, so it can miss such records. KNN candidates are
-  exactly the K nearest points of the index (its decoded coordinates, FP64 distances, smaller id
-  first on ties).
+* Mode.EXACT: range candidates are exactly the records holding a slot whose timestamp lies in
+  [start, end] (and whose sequence lies between the smallest and largest requested). A record's
+  index vector encodes its group's mean timestamp, so the slots of a record lie within a fixed
+  spread of that key (the largest over the index, measured when the service opens it): the interval
+  widened by that spread is queried as the few boxes whose union it is (`interval_boxes_us`), and
+  the records without a slot in the interval are dropped. The reference queries one box of
+  per-limb minima and maxima of the bare interval and prunes non-conservatively, so it can miss
+  such records. KNN candidates are exactly the K nearest points of the index (its decoded
+  coordinates, FP64 distances, smaller id first on ties).
 
 Refinement (same rules as the reference):
 * knn: slots of candidate records of the request's sequence, ordered by |timestamp_us - target|,
@@ -75,7 +78,11 @@ def interval_boxes(start: float, end: float, seq_lo: int, seq_hi: int):
     (a partial low limb, partial middle limbs, whole top limbs, and the mirror images at the end).
     The reference's single box of per-limb minima and maxima is not this set: it misses timestamps
     whose low limbs fall outside the end points' (and can hold ones outside the interval)."""
-    s_us, e_us = timestamp_to_us(start), timestamp_to_us(end)
+    return interval_boxes_us(timestamp_to_us(start), timestamp_to_us(end), seq_lo, seq_hi)
+
+
+def interval_boxes_us(s_us: int, e_us: int, seq_lo: int, seq_hi: int):
+    """`interval_boxes` of the microsecond interval [s_us, e_us]."""
     if s_us < 0 or e_us < 0:
         raise RuntimeError("negative timestamp is not supported")
     m = (1 << 21) - 1
@@ -170,6 +177,12 @@ class Records:
     bin_size: int
     file_name: List[str]
     group_size: int
+
+
+def record_keys_us(records: Records) -> np.ndarray:
+    """Each record's key in microseconds: the timestamp its index vector's limbs encode."""
+    lim = np.rint(records.index_vector[:, :3]).astype(np.int64) - 1
+    return (lim[:, 0] << 42) | (lim[:, 1] << 21) | lim[:, 2]
 
 
 def load_records(index_dir: str, meta: Meta) -> Records:
@@ -383,6 +396,11 @@ class FileIndexService:
             self.handler.prepare_for_query(policy if policy is not None else LevelPolicy.L0)
         if self.handler.info()["D"] != KNN_DIM:
             raise RuntimeError("the T-BLAEQ index of a file index must be 4-dimensional")
+        # How far a record's slots reach below and above its key (exact range candidates).
+        key = record_keys_us(self.records)
+        ts = self.records.timestamp_us
+        self.slot_spread_us = ((int(max(0, np.max(key - ts.min(1)))), int(max(0, np.max(ts.max(1) - key))))
+                               if len(key) else (0, 0))
 
     def query(self, requests: Sequence[Request], mode=None) -> List[ServiceResult]:
         """Answers every request; a request whose arguments the reference would reject carries the
@@ -401,11 +419,15 @@ class FileIndexService:
         rng = [(i, s, v) for i, s, v in checked if requests[i].mode == "range"]
         if rng:
             if mode == Mode.EXACT:
-                # The boxes whose union is exactly the request's interval (and sequence range).
-                # Index vectors are integers (limbs + 1, sequence numbers) and the index's decoded
-                # coordinates differ from them by rounding only (far below 0.25): boxes widened by a
-                # quarter hold exactly the records whose stored vector lies in them.
-                per = [interval_boxes(requests[i].start, requests[i].end, sq[0], sq[-1]) for i, sq, _ in rng]
+                # The boxes whose union is exactly the keys of the request's interval widened by the
+                # slots' spread (and the sequence range). Index vectors are integers (limbs + 1,
+                # sequence numbers) and the index's decoded coordinates differ from them by rounding
+                # only (far below 0.25): boxes widened by a quarter hold exactly the records whose
+                # stored vector lies in them.
+                below, above = self.slot_spread_us
+                per = [interval_boxes_us(max(0, timestamp_to_us(requests[i].start) - above),
+                                         timestamp_to_us(requests[i].end) + below, sq[0], sq[-1])
+                       for i, sq, _ in rng]
                 boxes = np.stack([b for bs in per for b in bs])
                 boxes[:, :KNN_DIM] -= 0.25
                 boxes[:, KNN_DIM:] += 0.25
@@ -419,7 +441,14 @@ class FileIndexService:
             for b, j in enumerate(owner):
                 parts[j].append(ids[offs[b]:offs[b + 1]])
             for j, (i, _, _) in enumerate(rng):
-                cands[i] = np.concatenate(parts[j]) if parts[j] else np.zeros(0, np.uint64)
+                c = np.concatenate(parts[j]) if parts[j] else np.zeros(0, np.uint64)
+                if mode == Mode.EXACT and len(c):
+                    c = np.unique(c)
+                    if int(c[-1]) < len(self.records.item_no):  # else refine reports the missing records
+                        t = self.records.timestamp_us[c.astype(np.int64)]
+                        lo, hi = timestamp_to_us(requests[i].start), timestamp_to_us(requests[i].end)
+                        c = c[np.any((t >= lo) & (t <= hi), axis=1)]
+                cands[i] = c
         knn = [(i, s, v) for i, s, v in checked if requests[i].mode == "knn"]
         if knn and mode == Mode.EXACT:
             pts = np.ascontiguousarray(np.stack([v for _, _, v in knn]))

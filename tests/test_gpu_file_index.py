@@ -7,10 +7,14 @@ answers all of them in two batched traversals:
 * in ref-parity mode the matches are identical to the reference's, request for request (rank,
   record, slot, sequence, type, timestamp, difference, payload offset and size, data file), and so
   are the candidate, record and slot counts;
-* in exact mode the coarse candidates are exactly the records whose stored index vector encodes a
-  timestamp in the request's interval (range) or the K nearest points of the T-BLAEQ index (KNN:
-  the FP64 brute force over its decoded points, id tie-break), and the refined matches equal the
-  refine of those candidates; range requests never lose a match against ref-parity mode.
+* in exact mode the coarse candidates are exactly the records holding a slot whose timestamp lies
+  in the request's interval (range) or the K nearest points of the T-BLAEQ index (KNN: the FP64
+  brute force over its decoded points, id tie-break), and the refined matches equal the refine of
+  those candidates; range requests without a match limit never lose a match against ref-parity
+  mode (with a limit, each mode keeps the earliest of its own matches).
+
+A request on which the reference's harness process dies is recorded with its exit status and the
+harness restarts after it; the parity test names such requests and compares all the others.
 """
 import os
 import subprocess
@@ -42,28 +46,46 @@ def _requests(fi, n, seed):
     return out
 
 
-def _run_reference(idx, reqs, tmp):
-    path = os.path.join(tmp, "req.txt")
-    with open(path, "w") as f:
-        for r in reqs:
-            if r.mode == "knn":
-                f.write(f"knn {r.timestamp!r} {r.knn_k} {int(r.include_padding)} {r.seqs[0]}\n")
-            else:
-                f.write(f"range {r.start!r} {r.end!r} {r.range_limit} {int(r.include_padding)} {len(r.seqs)} "
-                        + " ".join(str(s) for s in r.seqs) + "\n")
-    out = os.path.join(tmp, "out.txt")
-    subprocess.run([HARNESS, idx, path, out], check=True, timeout=600, stdout=subprocess.DEVNULL)
-    res, cur = [], None
+def _parse_reference(out):
+    """Complete requests of a harness output file (the harness flushes after each request)."""
+    res, cur, want = [], None, 0
     for line in open(out):
         f = line.split()
         if f[0] == "R":
             cur = {"counts": tuple(int(x) for x in f[1:4]), "matches": []}
+            want = int(f[4])
             res.append(cur)
         elif f[0] == "M":
             cur["matches"].append((int(f[1]), int(f[2]), int(f[3]), int(f[4]), int(f[5]), float(f[6]), int(f[7]),
                                    int(f[8]), int(f[9]), f[10]))
         else:
             res.append({"error": line[2:].strip()})
+    if cur is not None and len(cur["matches"]) != want:
+        res.pop()  # cut off inside its last request
+    return res
+
+
+def _run_reference(idx, reqs, tmp):
+    """The reference service's answer to each request, or {"crashed": status, "stderr": tail} for a
+    request on which the harness process died."""
+    res = []
+    while len(res) < len(reqs):
+        path = os.path.join(tmp, "req.txt")
+        with open(path, "w") as f:
+            for r in reqs[len(res):]:
+                if r.mode == "knn":
+                    f.write(f"knn {r.timestamp!r} {r.knn_k} {int(r.include_padding)} {r.seqs[0]}\n")
+                else:
+                    f.write(f"range {r.start!r} {r.end!r} {r.range_limit} {int(r.include_padding)} {len(r.seqs)} "
+                            + " ".join(str(s) for s in r.seqs) + "\n")
+        out = os.path.join(tmp, "out.txt")
+        p = subprocess.run([HARNESS, idx, path, out], timeout=600, stdout=subprocess.DEVNULL, stderr=subprocess.PIPE)
+        got = _parse_reference(out)
+        res.extend(got)
+        if p.returncode == 0:
+            assert len(res) == len(reqs)
+            break
+        res.append({"crashed": p.returncode, "stderr": p.stderr.decode(errors="replace")[-300:]})
     return res
 
 
@@ -84,8 +106,14 @@ def test_ref_parity_matches_the_reference_service(service):
     ref = _run_reference(idx, reqs, base)
     got = svc.query(reqs, mode=svc_mode(svc, "REF_PARITY"))
     assert len(ref) == len(got)
+    crashed = [(q, reqs[q], r) for q, r in enumerate(ref) if "crashed" in r]
+    for c in crashed:
+        print("the reference harness died on request", c)
+    assert len(crashed) <= len(reqs) // 4
     n_matches = 0
     for q, (r, g) in enumerate(zip(ref, got)):
+        if "crashed" in r:
+            continue
         assert "error" not in r and g.error is None, (q, r, g.error)
         assert (g.candidate_count, g.record_count, g.slot_count) == r["counts"], q
         mine = [(m.rank, m.item_no, m.seq, m.dtype, m.slot, m.timestamp, m.diff_us, m.payload_offset, m.payload_size,
@@ -112,18 +140,18 @@ def test_exact_mode_equals_brute_force_candidates(service, oracle_mod):
     for q, r in enumerate(reqs):
         seqs, v = fi._check_request(r)
         if r.mode == "range":
-            # Records whose index vector encodes a timestamp in [start, end], sequences in range.
-            lim = vecs[:, :3].astype(np.int64) - 1
-            us = (lim[:, 0] << 42) | (lim[:, 1] << 21) | lim[:, 2]
+            # Records holding a slot with a timestamp in [start, end], sequences in range.
+            ts = svc.records.timestamp_us
             s_us, e_us = fi.timestamp_to_us(r.start), fi.timestamp_to_us(r.end)
-            cand = ids[(us >= s_us) & (us <= e_us) & (vecs[:, 3] >= seqs[0]) & (vecs[:, 3] <= seqs[-1])]
+            inside = np.any((ts >= s_us) & (ts <= e_us), axis=1)
+            cand = ids[inside & (vecs[:, 3] >= seqs[0]) & (vecs[:, 3] <= seqs[-1])]
         else:
             b = oracle_mod.brute_query(dec_pts, dec_ids, oracle_mod.KNN, v[None, :], K=r.knn_k)
             cand = b.ids
         want = fi.refine(svc.records, r, seqs, cand)
         assert got[q].candidate_count == want.candidate_count, q
         assert [(m.item_no, m.slot) for m in got[q].matches] == [(m.item_no, m.slot) for m in want.matches], q
-        if r.mode == "range":
+        if r.mode == "range" and r.range_limit == 0:
             assert set((m.item_no, m.slot) for m in par[q].matches) <= set((m.item_no, m.slot) for m in got[q].matches)
             gained += len(got[q].matches) - len(par[q].matches)
     print(f"range matches the reference's candidates missed and exact mode found: {gained}")
