@@ -146,7 +146,7 @@ def job_throughput(units_per_rank: float, world: int, seconds_max: float) -> flo
     return units_per_rank * world / seconds_max
 
 
-def profiled_traffic(cfg_name, nq):
+def profiled_traffic(cfg_name, nq, float_points):
     """DRAM bytes (read + write) of one finest-level expand launch of this exact workload, from the
     committed ncu summary (one capture of the same command; ncu is never run by the benchmark)."""
     if cfg_name != "batched" or nq != 4096:
@@ -155,7 +155,8 @@ def profiled_traffic(cfg_name, nq):
     if not os.path.exists(path):
         return None
     import re
-    m = re.search(r"^traffic_bytes_per_launch_finest:\s*(\d+)", open(path).read(), re.M)
+    key = "traffic_bytes_per_launch_finest_float" if float_points else "traffic_bytes_per_launch_finest"
+    m = re.search(r"^" + key + r":\s*(\d+)", open(path).read(), re.M)
     return int(m.group(1)) if m else None
 
 
@@ -310,6 +311,8 @@ def main():
     ap.add_argument("--variants", default=None,
                     help="range configs: launch variant per level (0 direct, 1 staged, 2 node-major), comma "
                          "list; skips the autotuner (A/B timing, profiling one kind of kernel)")
+    ap.add_argument("--no-float-points", action="store_true",
+                    help="range configs: finest level tests every point in FP64 (no float copy first)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-graph", action="store_true")
     ap.add_argument("--policy", default="L0",
@@ -364,6 +367,11 @@ def main():
         policy = policy * h.info()["intervals"]
     h.prepare_for_query(policy)
     finest_streamed = policy[-1] in (tb.LevelPolicy.L2, tb.LevelPolicy.L3)
+    if args.no_float_points:
+        h.set_float_points(False)
+    # The finest level decides points from their float copies (4·D bytes) where the library has them.
+    float_points = not args.no_float_points and not finest_streamed and cfg["D"] in (4, 8, 16)
+    config["finest_points"] = "float32 copy, FP64 near faces" if float_points else "FP64 rows"
     if args.policy != "L0":
         config["policy"] = [p.name for p in policy]
     Q = wl.range_boxes(h, args.nq, seed=42, **boxes_kw)
@@ -413,7 +421,9 @@ def main():
     # Roofline of the finest-level expand (dominant kernel): algorithmic bytes per launch.
     H = len(entries)
     ent_in, kids = entries[H - 1], items[H - 1]
-    alg_bytes = ent_in * (12 + 8 * D) + kids * 8 * D + results * 16
+    # Per entry: query slot, first row, prefix and the parent's coordinates; per child: its point
+    # (float copy or FP64 row); per result: id and query slot.
+    alg_bytes = ent_in * (12 + 8 * D) + kids * (4 if float_points else 8) * D + results * 16
     final_mean_s = statistics.mean(final_ms) / 1e3
     peak, peak_kind = _peaks()
     achieved = alg_bytes / final_mean_s / 1e9
@@ -557,7 +567,7 @@ def main():
         "roofline": {"bound": "host link" if finest_streamed else "hbm", "achieved": achieved,
                      "peak": None if finest_streamed else peak, "unit": "GB/s",
                      "frac": None if finest_streamed else achieved / peak,
-                     "traffic": None if finest_streamed else profiled_traffic(cfg_name, args.nq),
+                     "traffic": None if finest_streamed else profiled_traffic(cfg_name, args.nq, float_points),
                      "kernel": "expandKernel<8, RangeBox, result> (finest level)",
                      "peak_kind": f"{peak_kind} hbm_gbs", "algorithmic_bytes_per_launch": alg_bytes,
                      "launch_ms": final_mean_s * 1e3},

@@ -202,6 +202,13 @@ int tblaeq_set_variants(tblaeq_handle* h, const int* variants, uint64_t n);
  * node-major returns each query's ids in no particular order. No counterpart in the reference. */
 int tblaeq_set_node_major(tblaeq_handle* h, int on);
 
+/* Exact range batches: the finest level decides each point from a float copy of the decoded points
+ * (4·D bytes a point instead of the 8·D of its P row) and takes the FP64 test only for a point with
+ * a coordinate within float rounding of a face of the box, so the results are the same either way
+ * (on = default; for D = 4, 8, 16 with the last interval device-resident). No counterpart in the
+ * reference, whose final filter reads every surviving point's doubles. */
+int tblaeq_set_float_points(tblaeq_handle* h, int on);
+
 /* ---- Launch shapes and the tuning cache (no counterpart in the reference, whose kernel shapes are
  * compile-time constants: kCompact* in src/core/strategies/L0Strategy.cu:18-21, UNROLL_FACTOR in
  * src/Kernel/SpMSpV.cuh:24) ----

@@ -151,6 +151,7 @@ def _load():
         "tblaeq_autotune": ([vp, P(_Batch), ctypes.c_int, P(ctypes.c_int), P(ctypes.c_float)], ctypes.c_int),
         "tblaeq_set_variants": ([vp, P(ctypes.c_int), ctypes.c_uint64], ctypes.c_int),
         "tblaeq_set_node_major": ([vp, ctypes.c_int], ctypes.c_int),
+        "tblaeq_set_float_points": ([vp, ctypes.c_int], ctypes.c_int),
         "tblaeq_set_knn_probe": ([vp, ctypes.c_uint32, ctypes.c_int], ctypes.c_int),
         "tblaeq_set_launch_shapes": ([vp, P(ctypes.c_int), P(ctypes.c_int), ctypes.c_uint64], ctypes.c_int),
         "tblaeq_get_launch_shapes": ([vp, P(ctypes.c_int), P(ctypes.c_int), ctypes.c_uint64], ctypes.c_int),
@@ -540,6 +541,11 @@ class QueryHandler:
     def set_node_major(self, on: bool = True):
         """Exact range batches: node-major inner levels (default) or entry-major."""
         _check(_load().tblaeq_set_node_major(self._h, int(on)))
+
+    def set_float_points(self, on: bool = True):
+        """Exact range batches: finest points decided from their float copies first (default;
+        same results), or every point's FP64 test."""
+        _check(_load().tblaeq_set_float_points(self._h, int(on)))
 
     def launch_shapes(self):
         """(variants, grid percentages) per expand launch."""

@@ -492,6 +492,12 @@ int tblaeq_set_node_major(tblaeq_handle* h, int on) {
     return TBLAEQ_OK;
 }
 
+int tblaeq_set_float_points(tblaeq_handle* h, int on) {
+    if (int c = checkPrepared(h)) return c;
+    h->qh->runtime().engine->setFloatPoints(on != 0);
+    return TBLAEQ_OK;
+}
+
 int tblaeq_set_launch_shapes(tblaeq_handle* h, const int* variants, const int* grid_percent, uint64_t n) {
     if (int c = checkPrepared(h)) return c;
     if (!variants || !grid_percent) return fail(TBLAEQ_ERR_INVALID, "null launch shapes");

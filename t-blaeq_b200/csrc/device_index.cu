@@ -1,5 +1,6 @@
 // Device-resident index and its derived position-space arrays.
 #include "device_index.hpp"
+#include "traverse.cuh"
 
 #include <omp.h>
 
@@ -109,6 +110,13 @@ DerivedArrays computeDerived(const HostIndex& idx) {
 
     out.nodeX.resize(H - 1);
     for (uint64_t m = 0; m + 1 < H; ++m) out.nodeX[m] = dec[m];
+    if (floatPointsSupported(D)) {
+        const std::vector<double>& pts = dec[H - 1];
+        out.pointsF.resize(pts.size());
+        const int64_t n = static_cast<int64_t>(pts.size());
+#pragma omp parallel for schedule(static)
+        for (int64_t i = 0; i < n; ++i) out.pointsF[i] = static_cast<float>(pts[i]);
+    }
     // Box of the finest points below every node (exact min / max of decoded coordinates), stored
     // as floats rounded outward.
     {
@@ -341,6 +349,10 @@ std::unique_ptr<DeviceIndex> buildDeviceIndex(const HostIndex& idx, const Derive
         di->nodeX[m] = upload(der.nodeX[m], s);
         TBLAEQ_CUDA(cudaStreamSynchronize(s));
     }
+    if (!der.pointsF.empty() && idx.intervals > 0 && res(idx.intervals - 1) == kResident) {
+        di->pointsF = upload(der.pointsF, s);
+        TBLAEQ_CUDA(cudaStreamSynchronize(s));
+    }
     TBLAEQ_CUDA(cudaStreamSynchronize(s));
     return di;
 }
@@ -349,7 +361,7 @@ size_t DeviceIndex::deviceBytes() const {
     size_t t = coarseVals.bytes() + coarseIds.bytes();
     for (auto* v : {&pvals, &nodeRef, &nodeSub, &leaf, &aabb, &nodeX, &nodeOrig, &maps})
         for (auto& m : *v) t += m.bytes();
-    return t;
+    return t + pointsF.bytes();
 }
 
 }  // namespace tblaeq

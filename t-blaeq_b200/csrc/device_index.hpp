@@ -83,6 +83,9 @@ struct DerivedArrays {
     // Decoded coordinates of every node (position order, D per node), as the traversal rebuilds
     // them (y = P[j] * x_parent, one rounded multiply per level).
     std::vector<std::vector<double>> nodeX;
+    // Decoded finest points (row order of the last interval) as floats rounded to nearest, for the
+    // finest exact range level's float test; empty where that test has no kernel (D not 4, 8, 16).
+    std::vector<float> pointsF;
 };
 
 // Host computation of the position-space node arrays, including subtree radii from the decoded
@@ -134,6 +137,8 @@ struct DeviceIndex {
     std::vector<DeviceMem> leaf;             // mesh m < height-1: finest points below each node (uint32)
     std::vector<DeviceMem> aabb;             // mesh m < height-1: outward-rounded float box of the points below
     std::vector<DeviceMem> nodeX;            // mesh m < height-1: decoded coordinates (D doubles per node)
+    DeviceMem pointsF;                       // finest points as floats (DerivedArrays::pointsF), when the
+                                             // last interval's rows are device-resident; else empty
 
     // original-id space (per-level plugin)
     DeviceMem coarseIds;                     // uint64

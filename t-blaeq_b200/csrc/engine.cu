@@ -146,8 +146,7 @@ uint64_t BatchEngine::lastTotal(uint32_t nq) {
 
 size_t BatchEngine::workspaceBytes() const {
     size_t t = zeroBlock_.bytes() + offsets_.bytes() + resIds_.bytes() + resVals_.bytes() + resQ_.bytes() +
-               resDist_.bytes() + v_.q.bytes() + v_.cbeg.bytes() + v_.cpre.bytes() + v_.x.bytes() +
-               v_.tileStart.bytes() + nmList_.bytes() + nmNodeOff_.bytes() + nmUnitOff_.bytes() + rawIds_.bytes() +
+               resDist_.bytes() + nmList_.bytes() + nmNodeOff_.bytes() + nmUnitOff_.bytes() + rawIds_.bytes() +
                rawQ_.bytes() + rawVals_.bytes();
     for (const auto& f : f_) t += f.q.bytes() + f.node.bytes() + f.cbeg.bytes() + f.cpre.bytes() + f.x.bytes() +
                                   f.tileStart.bytes();
@@ -242,10 +241,10 @@ void BatchEngine::reserve(const EngineCaps& want, uint32_t nq, unsigned flags) {
         off = align256(off + static_cast<size_t>(qcap_) * 4);
         offWork_ = off;
         off = align256(off + 2 * 8);
-        // Node-major range levels: a unit ticket and a survivor count per level, the per-node entry
-        // counts and cursors of every inner level, and the per-query result cursors.
+        // Node-major range levels: a packed survivor counter (64 bits) and a unit ticket per level,
+        // the per-node entry counts and cursors of every inner level, and the per-query result cursors.
         offNm_ = off;
-        off = align256(off + 2 * H * 4);
+        off = align256(off + H * 8 + H * 4);
         offNodeCnt_.assign(H, 0);
         for (uint64_t m = 1; m + 1 < H; ++m) {
             offNodeCnt_[m] = off;
@@ -270,7 +269,7 @@ void BatchEngine::reserve(const EngineCaps& want, uint32_t nq, unsigned flags) {
         zeroBytes_ = off;
         zeroBlock_.alloc(zeroBytes_);
         offsets_.alloc((static_cast<size_t>(qcap_) + 1) * 8);
-        boxF_.alloc(static_cast<size_t>(qcap_) * 2 * D * 4);
+        boxF_.alloc(static_cast<size_t>(qcap_) * 4 * D * 4);  // rounded outward, then inward
     }
     caps_ = c;
 }
@@ -334,13 +333,8 @@ bool BatchEngine::useNodeMajor(int mode) const {
 
 void BatchEngine::reserveNodeMajor(unsigned flags) {
     const uint64_t D = di_.D;
-    if (nmEntryCap_ < caps_.entries || v_.tileStart.bytes() < tileCap_ * 4) {
+    if (nmEntryCap_ < caps_.entries) {
         dropGraph();
-        v_.q.alloc(caps_.entries * 4);
-        v_.cbeg.alloc(caps_.entries * 4);
-        v_.cpre.alloc(caps_.entries * 4);
-        v_.x.alloc(caps_.entries * D * 8);
-        v_.tileStart.alloc(tileCap_ * 4);
         nmList_.alloc(caps_.entries * 4);
         uint64_t maxM = 1;
         for (uint64_t m = 0; m + 2 < di_.height; ++m) maxM = std::max<uint64_t>(maxM, di_.meshCount[m]);
@@ -362,13 +356,13 @@ void BatchEngine::reserveNodeMajor(unsigned flags) {
 }
 
 // Level m of an exact range batch, node-major: group frontier `buf` by node (m >= 1), test every
-// node's children against the query boxes holding it (survivors into v_), then expand v_ with
-// kPredAll into the next frontier (1 - buf).
+// node's children against the query boxes holding it, and append the survivors to the next frontier
+// (1 - buf).
 void BatchEngine::enqueueNodeMajorLevel(int m, int buf, const double* dBoxes, uint32_t nq, bool wantLevels) {
     const int D = static_cast<int>(di_.D);
     char* z = zeroBlock_.as<char>();
-    auto* nmTicket = reinterpret_cast<uint32_t*>(z + offNm_);
-    auto* nmCount = nmTicket + di_.height;
+    auto* nmCounter = reinterpret_cast<unsigned long long*>(z + offNm_);
+    auto* nmTicket = reinterpret_cast<uint32_t*>(z + offNm_ + di_.height * 8);
     auto* status = reinterpret_cast<uint32_t*>(z + offStatus_);
     const FrontierBufs& in = f_[buf];
     NodeMajorArgs n{};
@@ -396,14 +390,8 @@ void BatchEngine::enqueueNodeMajorLevel(int m, int buf, const double* dBoxes, ui
     n.children = di_.nodeSub[m].as<NodeRec>();
     n.boxes = dBoxes;
     n.boxesF = boxF_.as<float>();
-    n.vq = v_.q.as<uint32_t>();
-    n.vcbeg = v_.cbeg.as<uint32_t>();
-    n.vcpre = v_.cpre.as<uint32_t>();
-    n.vx = v_.x.as<double>();
-    n.vtile = v_.tileStart.as<uint32_t>();
-    n.vcap = static_cast<uint32_t>(caps_.entries);
-    n.vtileCap = static_cast<uint32_t>(tileCap_);
-    n.vcount = nmCount + m;
+    n.out = outView(1 - buf, hdrPtr(m + 1));
+    n.counter = nmCounter + m;
     n.ticket = nmTicket + m;
     n.status = status;
     n.levelItems = (wantLevels && m > 0)
@@ -411,23 +399,7 @@ void BatchEngine::enqueueNodeMajorLevel(int m, int buf, const double* dBoxes, ui
                        : nullptr;
     n.D = D;
     launchNodeMajorRange(n, grids_[m], stream_);
-    uint32_t* vHdr = hdrPtr(static_cast<int>(di_.height) + 2);
-    launchOneItemHeader(nmCount + m, vHdr, stream_);
-    ExpandArgs a{};
-    a.in = FrontierIn{v_.q.as<uint32_t>(),         v_.cbeg.as<uint32_t>(), v_.cpre.as<uint32_t>(), v_.x.as<double>(),
-                      v_.tileStart.as<uint32_t>(), vHdr,                   n.vcap,                  n.vtileCap};
-    a.child.rows = n.rows;
-    a.child.rowsOnHost = n.rowsOnHost;
-    a.child.nodes = n.children;
-    a.fout = outView(1 - buf, hdrPtr(m + 1));
-    a.scratch.desc = reinterpret_cast<unsigned long long*>(z + offDesc_) + static_cast<size_t>(m) * tileCap_;
-    a.scratch.ticket = reinterpret_cast<uint32_t*>(z + offTickets_) + m;
-    a.scratch.status = status;
-    a.D = D;
-    a.useFma = 1;
-    a.variant = variants_[m];
-    a.gridPercent = grids_[m];
-    launchExpand(a, kPredAll, false, 0, stream_);
+    launchFrontierHeader(n.counter, hdrPtr(m + 1), n.out.cap, n.out.tileCap, status, stream_);
 }
 
 void BatchEngine::enqueueLaunches(const double* dBoxes, uint32_t nq, int mode, unsigned flags) {
@@ -448,14 +420,15 @@ void BatchEngine::enqueueLaunches(const double* dBoxes, uint32_t nq, int mode, u
     launchRootFrontier(r0.q.as<uint32_t>(), r0.cbeg.as<uint32_t>(), r0.cpre.as<uint32_t>(), r0.x.as<double>(),
                        r0.tileStart.as<uint32_t>(), hdrPtr(0), nq, static_cast<uint32_t>(di_.meshCount[0]), D, tile_,
                        stream_);
-    if (mode == kModeExact) launchRoundBoxes(dBoxes, nq, D, boxF_.as<float>(), stream_);
+    float* boxFi = boxF_.as<float>() + static_cast<size_t>(qcap_) * 2 * D;
+    if (mode == kModeExact) launchRoundBoxes(dBoxes, nq, D, boxF_.as<float>(), boxFi, stream_);
     if (timing_) record(1);
     // Node-major levels (the variant the autotuner may choose per inner level) need their buffers at
     // the current capacities (sized by the synchronous batch that must precede asynchronous ones);
     // without them every level runs entry-major. Once a level ran node-major, the frontiers below it
     // are in no particular query order, and the results are grouped by query at the end.
     const bool nmReady = useNodeMajor(mode) && nmEntryCap_ >= caps_.entries && nmResultCap_ >= caps_.results &&
-                         v_.tileStart.bytes() >= tileCap_ * 4 && (!(flags & kWantVals) || nmVals_);
+                         (!(flags & kWantVals) || nmVals_);
     bool nodeMajor = false;
     int buf = 0;
     for (int m = 0; m < H; ++m) {
@@ -488,6 +461,10 @@ void BatchEngine::enqueueLaunches(const double* dBoxes, uint32_t nq, int mode, u
             buf = 1 - buf;
         } else {
             a.child.outMap = di_.mapPtr[H - 1];
+            if (mode == kModeExact && floatPoints_ && di_.pointsF.bytes()) {
+                a.child.rowsF = di_.pointsF.as<float>();
+                a.query.boxesFi = boxFi;
+            }
             a.rout.qcount = qcount;
             a.rout.hdr = hdrPtr(H);
             a.rout.cap = static_cast<uint32_t>(caps_.results);
@@ -550,26 +527,6 @@ void BatchEngine::growFromHeaders() {
         if (items > caps_.items) {
             want.items = std::max<uint64_t>(want.items, items + items / 4 + 4096);
             grew = true;
-        }
-    }
-    // Node-major levels: the survivors of level lv form a frontier of one item per entry.
-    {
-        std::vector<uint32_t> nm(H, 0);
-        TBLAEQ_CUDA(cudaMemcpyAsync(nm.data(), zeroBlock_.as<char>() + offNm_ + H * 4, H * 4, cudaMemcpyDeviceToHost,
-                                    stream_));
-        TBLAEQ_CUDA(cudaStreamSynchronize(stream_));
-        for (int lv = 0; lv < H; ++lv) {
-            const uint64_t c = nm[lv];
-            if (c > splitLimit_)
-                throw SplitBatch("level " + std::to_string(lv) + " exceeds the traversal limit; split the batch");
-            if (c > caps_.entries) {
-                want.entries = std::max<uint64_t>(want.entries, c + c / 4 + 1024);
-                grew = true;
-            }
-            if (c > caps_.items || c / kWarpTile + 2 > tileCap_) {
-                want.items = std::max<uint64_t>(want.items, c + c / 4 + 4096);
-                grew = true;
-            }
         }
     }
     // Results: slot H holds the one-pass (or wave-1) results, slot H+1 the wave-2 results of a

@@ -80,6 +80,12 @@ public:
         nodeMajor_ = on;
     }
     bool nodeMajor() const { return nodeMajor_; }
+    // Finest exact range level: decide points from their float copies first (default on; the
+    // results are the same either way).
+    void setFloatPoints(bool on) {
+        if (on != floatPoints_) dropGraph();
+        floatPoints_ = on;
+    }
     bool twoWave() const { return twoWave_; }
     // Optional device scorer of the last frontier's entries (higher = expand earlier); when unset
     // the entries are ranked by their lower bound. Called with (frontier, hdr, cap, points, out scores).
@@ -158,10 +164,10 @@ private:
     uint32_t qcap_ = 0;
     bool haveVals_ = false;
     FrontierBufs f_[2];
-    // Node-major range levels: the one-item-per-entry survivor frontier, the node grouping of the
-    // input frontier, and the raw (frontier-order) results before they are grouped by query.
+    // Node-major range levels: the node grouping of the input frontier, and the raw (frontier-order)
+    // results before they are grouped by query.
     bool nodeMajor_ = true;
-    FrontierBufs v_;
+    bool floatPoints_ = true;
     DeviceMem nmNodeOff_, nmUnitOff_, nmList_, rawIds_, rawQ_, rawVals_;
     uint64_t nmEntryCap_ = 0, nmResultCap_ = 0;
     bool nmVals_ = false;

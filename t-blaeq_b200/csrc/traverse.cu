@@ -224,9 +224,13 @@ constexpr int kExpandThreads = TBLAEQ_EXPAND_THREADS;
 // Resident CTAs per SM the register allocation is sized for (128 threads: 10 CTAs = 51 registers,
 // 8 CTAs = 64). Levels that prune inner nodes (range radius + box, KNN sphere + box bounds) keep
 // more state live and get the larger budget; point levels and plain expansions the smaller one.
+#ifndef TBLAEQ_EXPAND_MIN_BLOCKS_BOX
+#define TBLAEQ_EXPAND_MIN_BLOCKS_BOX 10
+#endif
 template <int PRED>
 constexpr int expandMinBlocks() {
     return (PRED == kPredKnnBound || PRED == kPredRangeRadius) ? TBLAEQ_EXPAND_MIN_BLOCKS_BOUND
+           : PRED == kPredRangeBox                             ? TBLAEQ_EXPAND_MIN_BLOCKS_BOX
                                                                : TBLAEQ_EXPAND_MIN_BLOCKS;
 }
 
@@ -267,7 +271,7 @@ constexpr bool prefetchesRows() {
 // children without loading their rows (the box prefilter, two-wave KNN) prefetch nothing.
 template <int D, int PRED>
 __device__ __forceinline__ void prefetchTileRows(const ExpandArgs& a, uint32_t t, uint32_t nTiles, uint32_t entries,
-                                                 uint32_t total, int lane) {
+                                                 uint32_t total, int lane, bool floatRows) {
     if (t >= nTiles) return;
     if (a.child.rowsOnHost) return;  // bulk prefetches are for device memory
     if (PRED == kPredRangeRadius && a.child.aabb) return;
@@ -277,14 +281,18 @@ __device__ __forceinline__ void prefetchTileRows(const ExpandArgs& a, uint32_t t
     const uint32_t eLo = a.in.tileStart[t];
     uint32_t eHi = (t + 1 < nTiles) ? a.in.tileStart[t + 1] : entries - 1;
     if (eHi >= entries) eHi = entries - 1;
+    // The finest exact range level with float points reads those (4·D bytes a row) instead.
+    const bool f = floatRows;
+    const unsigned char* base = f ? reinterpret_cast<const unsigned char*>(a.child.rowsF)
+                                  : reinterpret_cast<const unsigned char*>(a.child.rows);
+    const uint32_t rowBytes = f ? 4u * D : 8u * D;
     for (uint32_t e = eLo + lane; e <= eHi; e += 32) {
         const uint32_t cpi = a.in.cpre[e];
         const uint32_t from = max(t0, cpi);
         const uint32_t to = (e + 1 < entries) ? min(itemEnd, a.in.cpre[e + 1]) : itemEnd;
         if (to > from) {
-            const unsigned char* src = reinterpret_cast<const unsigned char*>(a.child.rows) +
-                                       (static_cast<size_t>(a.in.cbeg[e]) + (from - cpi)) * (8 * D);
-            bulkPrefetchL2(src, (to - from) * (8u * D));
+            const unsigned char* src = base + (static_cast<size_t>(a.in.cbeg[e]) + (from - cpi)) * rowBytes;
+            bulkPrefetchL2(src, (to - from) * rowBytes);
         }
     }
 }
@@ -488,6 +496,97 @@ __device__ __forceinline__ bool singleEntryRangeBox(const ExpandArgs& a, uint32_
     return ((mine >> ((lane % G) * L)) & kAll) == kAll;
 }
 
+// The FP64 test of one finest point (row j below entry e) against query q's box: the products and
+// comparisons of evalItem's kPredRangeBox branch. Out of line: it is rare, and inlined its registers
+// would count against the float test around it.
+template <int D>
+__device__ __noinline__ bool exactPointInBoxRow(const double* r, const double* x, const double* box) {
+    bool in = true;
+#pragma unroll
+    for (int d = 0; d < D; ++d) {
+        const double y = __dmul_rn(__ldg(r + d), __ldg(x + d));
+        in = in && (__ldg(box + d) <= y) && (y <= __ldg(box + D + d));
+    }
+    return in;
+}
+template <int D>
+__device__ __forceinline__ bool exactPointInBox(const ExpandArgs& a, uint32_t j, uint32_t e, uint32_t q) {
+    return exactPointInBoxRow<D>(a.child.rows + static_cast<size_t>(j) * D, a.in.x + static_cast<size_t>(e) * D,
+                                 a.query.boxes + static_cast<size_t>(q) * 2 * D);
+}
+
+// Float decisions of one 4-dimension piece of a point: `in` when every coordinate lies strictly
+// inside the inward-rounded box (then the exact coordinate lies inside the box), `out` when one
+// lies outside the outward-rounded box (then the exact one lies outside). Rounding to nearest is
+// monotone, which gives both implications; a piece that is neither is undecided.
+__device__ __forceinline__ void pieceF(const float4 v, const float4 lo, const float4 hi, const float4 li,
+                                       const float4 hiI, bool& in, bool& out) {
+    in = (v.x > li.x) & (v.y > li.y) & (v.z > li.z) & (v.w > li.w) & (v.x < hiI.x) & (v.y < hiI.y) &
+         (v.z < hiI.z) & (v.w < hiI.w);
+    out = (v.x < lo.x) | (v.y < lo.y) | (v.z < lo.z) | (v.w < lo.w) | (v.x > hi.x) | (v.y > hi.y) |
+          (v.z > hi.z) | (v.w > hi.w);
+}
+
+// Finest exact range level, one item tested from its float point (any round): kept when every
+// piece is inside, dropped when one is outside, else the FP64 test.
+template <int D>
+__device__ __forceinline__ bool pointInBoxF(const ExpandArgs& a, uint32_t j, uint32_t e, uint32_t q) {
+    constexpr int L = D / 4;
+    const float4* p = reinterpret_cast<const float4*>(a.child.rowsF + static_cast<size_t>(j) * D);
+    const float4* fo = reinterpret_cast<const float4*>(a.query.boxesF + static_cast<size_t>(q) * 2 * D);
+    const float4* fi = reinterpret_cast<const float4*>(a.query.boxesFi + static_cast<size_t>(q) * 2 * D);
+    bool allIn = true, anyOut = false;
+#pragma unroll
+    for (int c = 0; c < L; ++c) {
+        bool in, out;
+        pieceF(__ldcs(p + c), __ldg(fo + c), __ldg(fo + L + c), __ldg(fi + c), __ldg(fi + L + c), in, out);
+        allIn = allIn && in;
+        anyOut = anyOut || out;
+    }
+    if (allIn) return true;
+    if (anyOut) return false;
+    return exactPointInBox<D>(a, j, e, q);
+}
+
+// Finest exact range level, a round whose 32 items all belong to one frontier entry, from the
+// float points: the items' float rows are one contiguous block of 32·4·D bytes, each lane loads
+// one 16-byte piece (four coordinates) per load and a ballot per load collects the pieces'
+// decisions. Half the bytes of singleEntryRangeBox; identical outcome (pointInBoxF's rule).
+template <int D>
+constexpr bool coalescedBoxF() {
+    return floatPointsSupported(D);
+}
+template <int D>
+__device__ __forceinline__ bool singleEntryRangeBoxF(const ExpandArgs& a, uint32_t j0, uint32_t e, uint32_t q,
+                                                     int lane) {
+    constexpr int L = D / 4;   // pieces per point
+    constexpr int G = 32 / L;  // points per load
+    constexpr uint32_t kAll = (1u << L) - 1u;
+    const int c = lane % L;
+    const float4* rows4 = reinterpret_cast<const float4*>(a.child.rowsF + static_cast<size_t>(j0) * D);
+    const float4* fo = reinterpret_cast<const float4*>(a.query.boxesF + static_cast<size_t>(q) * 2 * D);
+    const float4* fi = reinterpret_cast<const float4*>(a.query.boxesFi + static_cast<size_t>(q) * 2 * D);
+    const float4 lo = __ldg(fo + c), hi = __ldg(fo + L + c), li = __ldg(fi + c), hiI = __ldg(fi + L + c);
+    float4 v[L];
+#pragma unroll
+    for (int i = 0; i < L; ++i) v[i] = __ldcs(rows4 + i * 32 + lane);
+    uint32_t inMine = 0, outMine = 0;
+#pragma unroll
+    for (int i = 0; i < L; ++i) {
+        bool in, out;
+        pieceF(v[i], lo, hi, li, hiI, in, out);
+        const uint32_t bi = __ballot_sync(0xffffffffu, in), bo = __ballot_sync(0xffffffffu, out);
+        if (i == lane / G) {
+            inMine = bi;
+            outMine = bo;
+        }
+    }
+    const int sh = (lane % G) * L;
+    if (((inMine >> sh) & kAll) == kAll) return true;
+    if (((outMine >> sh) & kAll) != 0) return false;
+    return exactPointInBox<D>(a, j0 + lane, e, q);
+}
+
 // Exact range frontier levels, a round whose 32 children all belong to one frontier entry: the
 // children are consecutive nodes, so their float boxes (lo[D] then hi[D], 8·D bytes each) form one
 // contiguous block. Each lane takes one 16-byte piece (four lower or four upper bounds) of a box
@@ -540,6 +639,8 @@ __global__ void __launch_bounds__(kExpandThreads, expandMinBlocks<PRED>()) expan
     constexpr int kUnrollTest = (TO_RESULT || kKnn) ? R : TBLAEQ_UNROLL_FRONTIER_TEST;
     constexpr int kUnrollPass2 = kKnn ? R : TBLAEQ_UNROLL_PASS2;
     constexpr bool kFastBox = PRED == kPredRangeBox && TO_RESULT && !STAGED && coalescedBox<D>();
+    // Finest exact range level with float points (a.child.rowsF): every round tests them first.
+    constexpr bool kFloatPts = PRED == kPredRangeBox && TO_RESULT && !STAGED && coalescedBoxF<D>();
     constexpr bool kFastAabb = PRED == kPredRangeRadius && coalescedAabb<D>();
     // Exact range frontier levels test children that pass the box prefilter after the rounds,
     // 32 at a time, so the FP64 radius test runs on full warps instead of in every round that
@@ -589,7 +690,8 @@ __global__ void __launch_bounds__(kExpandThreads, expandMinBlocks<PRED>()) expan
         }
         // The tile's rows are one contiguous run per entry: the TMA unit brings each run into L2
         // now (one instruction per run, no registers), ahead of the per-round row loads.
-        if constexpr (prefetchesRows<D, PRED>()) prefetchTileRows<D, PRED>(a, tile, nTiles, entries, total, lane);
+        if constexpr (prefetchesRows<D, PRED>())
+            prefetchTileRows<D, PRED>(a, tile, nTiles, entries, total, lane, kFloatPts && a.child.rowsF != nullptr);
         const uint32_t t0 = tile * kWarpTile;
 
         // ---- phase A: stage the tile's entries in shared memory (one round of parallel loads),
@@ -721,7 +823,12 @@ __global__ void __launch_bounds__(kExpandThreads, expandMinBlocks<PRED>()) expan
                 // Warp-uniform: a full round inside one entry (its first and last item share it).
                 const uint32_t w0 = sWin[r * 32], w31 = sWin[r * 32 + 31];
                 if (W != 0 && t0 + r * 32 + 32 <= total && w0 == w31 && !a.child.rowsOnHost) {
-                    keep = singleEntryRangeBox<D>(a, sRow[r * 32], eLo + w0, wQ[w0], lane);
+                    if constexpr (kFloatPts) {
+                        keep = a.child.rowsF ? singleEntryRangeBoxF<D>(a, sRow[r * 32], eLo + w0, wQ[w0], lane)
+                                             : singleEntryRangeBox<D>(a, sRow[r * 32], eLo + w0, wQ[w0], lane);
+                    } else {
+                        keep = singleEntryRangeBox<D>(a, sRow[r * 32], eLo + w0, wQ[w0], lane);
+                    }
                     done = true;
                 }
             }
@@ -758,6 +865,8 @@ __global__ void __launch_bounds__(kExpandThreads, expandMinBlocks<PRED>()) expan
                         const double* rowp = reinterpret_cast<const double*>(rowBuf + (slot * 32 + lane) * S::kStride);
                         if constexpr (NODE) nr = nodeBuf[slot * 32 + lane];
                         keep = evalItem<D, DM, PRED, TO_RESULT, true>(a, dim, rowp, xp, q, j, kk, nr, cc);
+                    } else if (kFloatPts && a.child.rowsF) {
+                        if constexpr (kFloatPts) keep = pointInBoxF<D>(a, j, e, q);
                     } else {
                         if constexpr (NODE) nr = a.child.nodes[kk];
                         keep = evalItem<D, DM, PRED, TO_RESULT, false>(a, dim, a.child.rows + static_cast<size_t>(j) * dim,
@@ -1100,20 +1209,21 @@ void launchRootFrontier(uint32_t* q, uint32_t* cbeg, uint32_t* cpre, double* x, 
     TBLAEQ_CUDA(cudaGetLastError());
 }
 
-__global__ void roundBoxesKernel(const double* boxes, uint32_t nq, int D, float* boxesF) {
+__global__ void roundBoxesKernel(const double* boxes, uint32_t nq, int D, float* boxesF, float* boxesFi) {
     const uint64_t n = static_cast<uint64_t>(nq) * 2 * D;
     for (uint64_t i = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x; i < n;
          i += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
         const bool upper = (i % (2 * D)) >= static_cast<uint64_t>(D);
         boxesF[i] = upper ? __double2float_ru(boxes[i]) : __double2float_rd(boxes[i]);
+        if (boxesFi) boxesFi[i] = upper ? __double2float_rd(boxes[i]) : __double2float_ru(boxes[i]);
     }
 }
 
-void launchRoundBoxes(const double* boxes, uint32_t nq, int D, float* boxesF, cudaStream_t stream) {
+void launchRoundBoxes(const double* boxes, uint32_t nq, int D, float* boxesF, float* boxesFi, cudaStream_t stream) {
     if (nq == 0) return;
     const uint64_t n = static_cast<uint64_t>(nq) * 2 * D;
     const int blocks = static_cast<int>(std::min<uint64_t>(148 * 4, (n + 255) / 256));
-    roundBoxesKernel<<<blocks, 256, 0, stream>>>(boxes, nq, D, boxesF);
+    roundBoxesKernel<<<blocks, 256, 0, stream>>>(boxes, nq, D, boxesF, boxesFi);
     TBLAEQ_CUDA(cudaGetLastError());
 }
 
@@ -1263,27 +1373,52 @@ __global__ void __launch_bounds__(kNodeMajorThreads) nodeMajorRangeKernel(NodeMa
     uint32_t staged = 0;  // warp-uniform
     const double* xp = nullptr;
     // Appends the staged survivors of the current unit (all children of one node, so they share the
-    // node's coordinates xp) at consecutive positions.
+    // node's coordinates xp) to the next frontier: one packed atomic claims their entry positions and
+    // their children's item range together, a warp scan gives each survivor its child prefix, and
+    // each writes its entry (query, node, first child, prefix, coordinates rebuilt as y = P[j] * x)
+    // and the tile starts of the next level that fall inside its children.
     auto flush = [&]() {
         if (staged == 0) return;
-        uint32_t base = 0;
-        if (lane == 0) base = atomicAdd(a.vcount, staged);
-        base = __shfl_sync(FULL, base, 0);
         __syncwarp();
-        for (uint32_t i = lane; i < staged; i += 32) {
-            const uint32_t pos = base + i;
-            if (pos < a.vcap) {
-                a.vq[pos] = sQ[w][i];
-                a.vcbeg[pos] = sJ[w][i];
-                a.vcpre[pos] = pos;
-                double* xo = a.vx + static_cast<size_t>(pos) * dim;
+        uint32_t sum = 0;
+        for (uint32_t i = lane; i < staged; i += 32) sum += __ldg(&a.children[sJ[w][i]].cnt);
 #pragma unroll
-                for (int d = 0; d < DM; ++d)
-                    if (D > 0 || d < dim) xo[d] = __ldg(xp + d);
-                if ((pos % kWarpTile) == 0 && pos / kWarpTile < a.vtileCap) a.vtile[pos / kWarpTile] = pos;
-            } else {
-                atomicOr(a.status, kStatusOverflowEntries);
+        for (int o = 16; o > 0; o >>= 1) sum += __shfl_xor_sync(FULL, sum, o);
+        unsigned long long old = 0;
+        if (lane == 0) old = atomicAdd(a.counter, (static_cast<unsigned long long>(sum) << 32) | staged);
+        old = __shfl_sync(FULL, old, 0);
+        const uint32_t ePos = static_cast<uint32_t>(old);
+        const unsigned long long iPos = old >> 32;
+        if (lane == 0 && iPos + sum > 0xffffffffull) atomicOr(a.status, kStatusOverflowSum);
+        unsigned long long run = iPos;
+        for (uint32_t i0 = 0; i0 < staged; i0 += 32) {  // warp-uniform
+            const uint32_t i = i0 + lane;
+            const bool v = i < staged;
+            const uint32_t j = v ? sJ[w][i] : 0u;
+            const NodeRec nr = v ? a.children[j] : NodeRec{0.0, 0u, 0u};
+            const uint32_t c = v ? nr.cnt : 0u;
+            uint32_t inc = c;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const uint32_t t = __shfl_up_sync(FULL, inc, o);
+                if (lane >= o) inc += t;
             }
+            const unsigned long long cp = run + (inc - c);
+            run += __shfl_sync(FULL, inc, 31);
+            if (!v) continue;
+            const uint32_t pos = ePos + i;
+            if (pos >= a.out.cap) continue;  // the header kernel reports the overflow
+            a.out.q[pos] = sQ[w][i];
+            a.out.node[pos] = j;
+            a.out.cbeg[pos] = nr.cbeg;
+            a.out.cpre[pos] = static_cast<uint32_t>(cp);
+            const double* row = a.rows + static_cast<size_t>(j) * dim;
+            double* xo = a.out.x + static_cast<size_t>(pos) * dim;
+#pragma unroll
+            for (int d = 0; d < DM; ++d)
+                if (D > 0 || d < dim) xo[d] = __dmul_rn(a.rowsOnHost ? row[d] : __ldg(row + d), __ldg(xp + d));
+            for (unsigned long long b = (cp + kWarpTile - 1) / kWarpTile; b * kWarpTile < cp + c; ++b)
+                if (b < a.out.tileCap) a.out.tileStart[b] = pos;
         }
         __syncwarp();
         staged = 0;
@@ -1417,6 +1552,17 @@ __global__ void __launch_bounds__(kNodeMajorThreads) nodeMajorRangeKernel(NodeMa
     }
 }
 
+__global__ void frontierHeaderKernel(const unsigned long long* counter, uint32_t* hdr, uint32_t cap, uint32_t tileCap,
+                                     uint32_t* status) {
+    const unsigned long long c = *counter;
+    const uint32_t entries = static_cast<uint32_t>(c), items = static_cast<uint32_t>(c >> 32);
+    hdr[0] = entries;
+    hdr[1] = items;
+    if (entries > cap) atomicOr(status, kStatusOverflowEntries);
+    if ((static_cast<unsigned long long>(items) + kWarpTile - 1) / kWarpTile > tileCap)
+        atomicOr(status, kStatusOverflowItems);
+}
+
 __global__ void oneItemHeaderKernel(const uint32_t* count, uint32_t* hdr) {
     const uint32_t c = *count;
     hdr[0] = c;
@@ -1486,6 +1632,12 @@ void launchNodeMajorRange(const NodeMajorArgs& a, int gridPercent, cudaStream_t 
             if (a.D < 1 || a.D > 32) throw std::invalid_argument("node-major level: D must be in [1, 32]");
             return launchNodeMajorD<0>(a, gridPercent, s);
     }
+}
+
+void launchFrontierHeader(const unsigned long long* counter, uint32_t* hdr, uint32_t cap, uint32_t tileCap,
+                          uint32_t* status, cudaStream_t s) {
+    frontierHeaderKernel<<<1, 1, 0, s>>>(counter, hdr, cap, tileCap, status);
+    TBLAEQ_CUDA(cudaGetLastError());
 }
 
 void launchOneItemHeader(const uint32_t* count, uint32_t* hdr, cudaStream_t s) {

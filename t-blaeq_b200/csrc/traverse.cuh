@@ -95,12 +95,18 @@ struct ChildLevel {
     const double* entryLb;
     const uint8_t* mask;        // keep flags (by row) for kPredMask
     const uint64_t* outMap;     // final output id of row j (null: id = key)
+    // Optional, finest exact range level: the decoded point of row j (the product y above) as D
+    // floats rounded to nearest. Compared with the query box rounded outward and inward, a point
+    // is decided from these 4·D bytes unless a coordinate lies within float rounding of a face,
+    // where the FP64 test on the row decides.
+    const float* rowsF;
     int rowsOnHost;             // rows (and possibly outMap) are mapped host memory: plain loads only
 };
 
 struct QueryArgs {
     const double* boxes;        // range: per query lo[D] then hi[D]
     const float* boxesF;        // range, exact mode: the same boxes as floats rounded outward
+    const float* boxesFi;       // range, exact mode: the boxes as floats rounded inward (lo up, hi down)
     const double* points;       // knn: per query point[D]
     double* tau;                // knn: per query upper bound on the K-th neighbour distance (tightened
                                 //      in place with an atomic minimum)
@@ -202,14 +208,12 @@ struct NodeMajorArgs {
     // Query boxes: double lo|hi, and as floats rounded outward.
     const double* boxes;
     const float* boxesF;
-    // Survivors: a frontier with one item per entry (cbeg = the child row, cpre = the position).
-    uint32_t* vq;
-    uint32_t* vcbeg;
-    uint32_t* vcpre;
-    double* vx;
-    uint32_t* vtile;
-    uint32_t vcap, vtileCap;
-    uint32_t* vcount;           // survivors (may exceed vcap: the host grows the workspace)
+    // Survivors: the next frontier itself (entries in no particular query order). Each warp appends
+    // a batch of survivors through one 64-bit atomic on `counter` (entries in the low half, their
+    // children in the high half), so entry positions and child prefixes stay in the same order;
+    // out.hdr is written from the counter afterwards (launchFrontierHeader).
+    FrontierOut out;
+    unsigned long long* counter;  // zeroed before launch
     uint32_t* ticket;           // unit ticket, zeroed before launch
     uint32_t* status;
     uint32_t* levelItems;       // optional per-query generated-children counts
@@ -222,6 +226,10 @@ void launchNodeTranspose(const uint32_t* node, const uint32_t* hdr, uint32_t cap
                          uint32_t* nodeOff, uint32_t* unitOff, uint32_t* cursor, uint32_t* list, cudaStream_t s);
 // The node-major test of one level (persistent grid; gridPercent as for the expand kernel).
 void launchNodeMajorRange(const NodeMajorArgs& a, int gridPercent, cudaStream_t s);
+// hdr[0] / hdr[1] = the entries and children a node-major level appended (its packed counter);
+// sets the overflow bits of `status` when they exceed the frontier's capacities.
+void launchFrontierHeader(const unsigned long long* counter, uint32_t* hdr, uint32_t cap, uint32_t tileCap,
+                          uint32_t* status, cudaStream_t s);
 // hdr[0] = hdr[1] = *count: the header of a one-item-per-entry frontier.
 void launchOneItemHeader(const uint32_t* count, uint32_t* hdr, cudaStream_t s);
 // Moves results written in frontier order (rawIds/rawQ/rawVals, count = *hdr) to their query's slot
@@ -237,8 +245,11 @@ void launchRootFrontier(uint32_t* q, uint32_t* cbeg, uint32_t* cpre, double* x, 
                         uint32_t nq, uint32_t nChildren, int D, int tile, cudaStream_t stream);
 
 // boxesF = the nq query boxes (lo[D] hi[D]) as floats, lower corners rounded down and upper
-// corners rounded up.
-void launchRoundBoxes(const double* boxes, uint32_t nq, int D, float* boxesF, cudaStream_t stream);
+// corners rounded up; boxesFi (optional) = the same rounded inward (lower up, upper down).
+void launchRoundBoxes(const double* boxes, uint32_t nq, int D, float* boxesF, float* boxesFi, cudaStream_t stream);
+
+// Whether the finest range level decides points from their float copies (rowsF) at dimension D.
+constexpr bool floatPointsSupported(uint64_t D) { return D == 4 || D == 8 || D == 16; }
 
 // offsets[q] = exclusive scan of counts[0..n), offsets[n] = total (single CTA).
 void launchExclusiveScan(const uint32_t* counts, uint64_t* offsets, uint32_t n, cudaStream_t stream);

@@ -314,3 +314,39 @@ def test_node_major_levels_equal_entry_major(tb, env, oracle_mod, flags):
     assert np.array_equal(r.ids.numpy(), out[False][5])
     h.set_node_major(True)
     h.set_launch_shapes([0] * H, [100] * H)
+
+
+@pytest.mark.parametrize("D,ratios", [(4, (100, 20, 10)), (8, (100, 50, 20)), (16, (40, 40, 10))])
+def test_float_points_decide_exactly_at_box_faces(tb, oracle_mod, tmp_path, cuda, D, ratios):
+    """The finest level decides points from their float copies and takes the FP64 test only near a
+    face. Boxes whose faces lie exactly on decoded coordinates, one double ulp beside them or one
+    float ulp beside them give the FP64 brute force's results, with the float copies on and off."""
+    h = tb.QueryHandler.generate(60000 if D != 8 else 200000, D, 1.0, 100.0, False, 4, ratios, 5 + D, 3.0)
+    h.prepare_for_query(tb.LevelPolicy.L0)
+    o = oracle_from_handler(oracle_mod, h, tmp_path)
+    pts, ids = oracle_mod.decoded_points(o)
+    rng = np.random.default_rng(100 + D)
+    n = 480
+    c = pts[rng.integers(0, len(pts), n)]
+    hw = np.exp(rng.uniform(np.log(0.01), np.log(0.2), c.shape)) * (pts.max(0) - pts.min(0))
+    lo, hi = c - hw, c + hw
+    g = n // 6
+    fulp = np.spacing(np.abs(c).astype(np.float32)).astype(np.float64)
+    lo[0 * g:1 * g] = c[0 * g:1 * g]                                # the centre on every lower face
+    hi[1 * g:2 * g] = c[1 * g:2 * g]                                # ... on every upper face
+    lo[2 * g:3 * g] = np.nextafter(c[2 * g:3 * g], np.inf)          # one double ulp above it: out
+    hi[3 * g:4 * g] = np.nextafter(c[3 * g:4 * g], -np.inf)         # one double ulp below it: out
+    lo[4 * g:5 * g] = c[4 * g:5 * g] - fulp[4 * g:5 * g] / 2        # half a float ulp below it
+    hi[5 * g:6 * g] = c[5 * g:6 * g] + fulp[5 * g:6 * g] / 2        # half a float ulp above it
+    Q = np.ascontiguousarray(np.concatenate([lo, hi], 1))
+    b = oracle_mod.brute_query(pts, ids, oracle_mod.RANGE, Q)
+    try:
+        for on in (True, False):
+            h.set_float_points(on)
+            r, offs, got = _batch_ids(tb, h, Q, tb.Mode.EXACT)
+            assert np.array_equal(offs, b.offsets), on
+            assert all(np.array_equal(gq, b.query(q)) for q, gq in enumerate(ids_by_query(offs, got))), on
+    finally:
+        h.set_float_points(True)
+    sizes = np.diff(b.offsets.astype(np.int64))
+    assert np.all(sizes[:2 * g] >= 1) and np.all(sizes[2 * g:4 * g] >= 0)
