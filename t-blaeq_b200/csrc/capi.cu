@@ -213,7 +213,8 @@ int tblaeq_coarsest_grid(tblaeq_handle* h, tblaeq_grid* out) {
 }
 
 // A KNN batch too large for one traversal (high dimensions keep most clusters alive, so the
-// frontier outgrows the 32-bit item space) runs as consecutive chunks, halved until each fits; the
+// frontier outgrows the 32-bit item space or the free device memory) runs as consecutive chunks,
+// halved until each fits; the
 // chunks' results are gathered into the handle's buffers in query order. Per-level counts are not
 // kept for chunked batches.
 static BatchOutput runKnnChunked(tblaeq_handle* h, const double* dQueries, uint64_t nq, const std::vector<uint32_t>& k,
@@ -238,8 +239,10 @@ static BatchOutput runKnnChunked(tblaeq_handle* h, const double* dQueries, uint6
         try {
             co = rt.engine->runKnn(dQueries + i * D, static_cast<uint32_t>(c), h->kStage.as<uint32_t>() + i, sk,
                                    flags & ~static_cast<unsigned>(TBLAEQ_WANT_LEVELS));
-        } catch (const SplitBatch&) {
-            if (c == 1) throw;
+        } catch (const CudaError& e) {
+            // Too large for the 32-bit traversal space or for the free device memory (the engine
+            // released its workspace on the way out): halve the chunk.
+            if (e.code != cudaErrorMemoryAllocation || c == 1) throw;
             chunk = (c + 1) / 2;
             continue;
         }
@@ -290,8 +293,8 @@ static int runBatch(tblaeq_handle* h, const tblaeq_batch* b, const double* dQuer
         h->knnSum.clear();
         try {
             o = rt.engine->runKnn(dQueries, static_cast<uint32_t>(b->nq), h->kStage.as<uint32_t>(), sumK, b->flags);
-        } catch (const SplitBatch&) {
-            if (b->nq < 2) throw;
+        } catch (const CudaError& e) {
+            if (e.code != cudaErrorMemoryAllocation || b->nq < 2) throw;
             o = runKnnChunked(h, dQueries, b->nq, k, b->flags);
         }
     } else {

@@ -1,6 +1,7 @@
 // Batched traversal engine (range queries; see engine.hpp).
 #include "engine.hpp"
 
+#include <exception>
 #include <limits>
 
 #include "knn.cuh"
@@ -8,6 +9,48 @@
 #include <algorithm>
 
 namespace tblaeq {
+
+namespace {
+// Resets the engine's workspace when the scope it guards exits by an exception.
+class WorkspaceGuard {
+public:
+    explicit WorkspaceGuard(BatchEngine& e) : e_(e), n_(std::uncaught_exceptions()) {}
+    ~WorkspaceGuard() {
+        if (std::uncaught_exceptions() > n_) e_.resetWorkspace();
+    }
+    WorkspaceGuard(const WorkspaceGuard&) = delete;
+    WorkspaceGuard& operator=(const WorkspaceGuard&) = delete;
+
+private:
+    BatchEngine& e_;
+    int n_;
+};
+}  // namespace
+
+void BatchEngine::resetWorkspace() noexcept {
+    dropGraph();
+    for (auto& f : f_)
+        for (DeviceMem* m : {&f.q, &f.node, &f.cbeg, &f.cpre, &f.x, &f.tileStart}) m->release();
+    for (DeviceMem* m : {&nmNodeOff_, &nmUnitOff_, &nmList_, &rawIds_, &rawQ_, &rawVals_, &pairQ_[0], &pairQ_[1],
+                         &pairNode_[0], &pairNode_[1], &pairList_, &pairNodeOff_, &pairUnitOff_, &candQ_, &candId_,
+                         &candD2_, &excl_, &probeK_, &resIds_, &resVals_, &resQ_, &resDist_, &zeroBlock_, &cmpCnt_,
+                         &cmpKids_, &cmpEntryOff_, &cmpKidOff_, &offsets_, &boxF_, &tau_, &candOff_, &knnCount_,
+                         &knnOff_, &knnIds_, &knnD2_, &lbE_, &scoreE_, &sel_, &offF_, &waveM_, &selCount_, &selOff_,
+                         &selIds_, &selD2_, &candOffB_, &resIdsB_, &resQB_, &resDistB_})
+        m->release();
+    caps_ = EngineCaps{};
+    qcap_ = 0;
+    haveVals_ = false;
+    nmEntryCap_ = nmResultCap_ = 0;
+    nmVals_ = false;
+    pairCap_ = candCap_ = 0;
+    knnCap_ = 0;
+    entryCap_ = resCapB_ = 0;
+    knnQcap_ = 0;
+    tileCap_ = 0;
+    zeroBytes_ = 0;
+}
+
 
 namespace {
 size_t align256(size_t v) { return (v + 255) & ~size_t(255); }
@@ -36,6 +79,7 @@ void BatchEngine::setVariants(const std::vector<int>& v) {
 }
 
 std::vector<float> BatchEngine::autotuneRange(const double* dBoxes, uint32_t nq, int mode, unsigned flags, int reps) {
+    WorkspaceGuard guard(*this);
     const int H = static_cast<int>(di_.height);
     const bool wasTiming = timing_;
     setTiming(true);
@@ -573,6 +617,7 @@ BatchOutput BatchEngine::output(uint32_t nq, unsigned flags) const {
 }
 
 BatchOutput BatchEngine::runRange(const double* dBoxes, uint32_t nq, int mode, unsigned flags) {
+    WorkspaceGuard guard(*this);
     reserve(caps_, nq, flags);
     for (int attempt = 0; attempt < 16; ++attempt) {
         if (useNodeMajor(mode)) reserveNodeMajor(flags);
@@ -605,6 +650,7 @@ namespace tblaeq {
 uint64_t BatchEngine::runGridLevel(int l, const uint64_t* dIds, const double* dVals, uint64_t p, bool range,
                                    const double* dQuery, const uint8_t* dMask, uint64_t* outIds, double* outVals,
                                    uint64_t outCap) {
+    WorkspaceGuard guard(*this);
     if (p == 0) return 0;
     if (p > 0xffffffffull || outCap > 0xffffffffull) throw std::invalid_argument("grid too large for one level");
     const int D = static_cast<int>(di_.D);
@@ -1056,6 +1102,7 @@ bool BatchEngine::growKnnMajor() {
 
 BatchOutput BatchEngine::runKnn(const double* dPoints, uint32_t nq, const uint32_t* dK, uint64_t sumK,
                                 unsigned flags) {
+    WorkspaceGuard guard(*this);
     reserve(caps_, nq, flags);
     reserveKnn(nq);
     if (knnCap_ < std::max<uint64_t>(sumK, 1)) {

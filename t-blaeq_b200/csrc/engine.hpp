@@ -148,6 +148,10 @@ public:
 
     // Reserve workspace for at least these capacities and this many queries.
     void reserve(const EngineCaps& caps, uint32_t nq, unsigned flags);
+    // Releases every workspace buffer and forgets every capacity, so the next batch allocates
+    // afresh. A batch that throws (an allocation that failed part-way through a growth, a split,
+    // a timeout) calls it on the way out: no later launch can see a capacity whose buffer is gone.
+    void resetWorkspace() noexcept;
     const EngineCaps& caps() const { return caps_; }
     size_t workspaceBytes() const;
     int launchesPerBatch() const { return static_cast<int>(di_.height) + 2; }

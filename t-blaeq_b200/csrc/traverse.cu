@@ -1317,6 +1317,52 @@ __global__ void __launch_bounds__(1024) nodeScanKernel(const uint32_t* nodeCnt, 
     }
 }
 
+// Levels with few nodes (the upper meshes: hundreds to thousands of nodes, each in thousands of
+// entries) count and place entries through a per-block shared-memory histogram instead: one global
+// atomic per (block, node) and shared-memory atomics for the rest. The scatter block takes a
+// contiguous slice of the entries, counts it, claims a range per node, then places the slice.
+constexpr uint32_t kSmemNodes = 6144;
+
+__global__ void nodeCountSmemKernel(const uint32_t* node, const uint32_t* hdr, uint32_t cap, uint32_t M,
+                                    uint32_t* nodeCnt) {
+    __shared__ uint32_t hist[kSmemNodes];
+    for (uint32_t i = threadIdx.x; i < M; i += blockDim.x) hist[i] = 0;
+    __syncthreads();
+    const uint32_t n = min(hdr[0], cap);
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const uint32_t nd = node[i];
+        if (nd < M) atomicAdd(&hist[nd], 1u);
+    }
+    __syncthreads();
+    for (uint32_t i = threadIdx.x; i < M; i += blockDim.x)
+        if (hist[i]) atomicAdd(&nodeCnt[i], hist[i]);
+}
+
+__global__ void nodeScatterSmemKernel(const uint32_t* node, const uint32_t* hdr, uint32_t cap, uint32_t M,
+                                      const uint32_t* nodeOff, uint32_t* cursor, uint32_t* list) {
+    __shared__ uint32_t slot[kSmemNodes];
+    for (uint32_t i = threadIdx.x; i < M; i += blockDim.x) slot[i] = 0;
+    __syncthreads();
+    const uint64_t n = min(hdr[0], cap);
+    const uint64_t per = (n + gridDim.x - 1) / gridDim.x;
+    const uint64_t lo = blockIdx.x * per < n ? blockIdx.x * per : n;
+    const uint64_t hi = lo + per < n ? lo + per : n;
+    for (uint64_t i = lo + threadIdx.x; i < hi; i += blockDim.x) {
+        const uint32_t nd = node[i];
+        if (nd < M) atomicAdd(&slot[nd], 1u);
+    }
+    __syncthreads();
+    for (uint32_t i = threadIdx.x; i < M; i += blockDim.x) {
+        const uint32_t c = slot[i];
+        slot[i] = c ? nodeOff[i] + atomicAdd(&cursor[i], c) : 0u;
+    }
+    __syncthreads();
+    for (uint64_t i = lo + threadIdx.x; i < hi; i += blockDim.x) {
+        const uint32_t nd = node[i];
+        if (nd < M) list[atomicAdd(&slot[nd], 1u)] = static_cast<uint32_t>(i);
+    }
+}
+
 __global__ void nodeScatterKernel(const uint32_t* node, const uint32_t* hdr, uint32_t cap, uint32_t M,
                                   const uint32_t* nodeOff, uint32_t* cursor, uint32_t* list) {
     const uint32_t n = min(hdr[0], cap);
@@ -1612,11 +1658,18 @@ int smallGrid(uint64_t work) { return static_cast<int>(std::max<uint64_t>(1, std
 
 void launchNodeTranspose(const uint32_t* node, const uint32_t* hdr, uint32_t cap, uint32_t nNodes, uint32_t* nodeCnt,
                          uint32_t* nodeOff, uint32_t* unitOff, uint32_t* cursor, uint32_t* list, cudaStream_t s) {
-    nodeCountKernel<<<smallGrid(cap), 256, 0, s>>>(node, hdr, cap, nNodes, nodeCnt);
+    const bool smem = nNodes <= kSmemNodes;
+    if (smem)
+        nodeCountSmemKernel<<<smallGrid(cap), 256, 0, s>>>(node, hdr, cap, nNodes, nodeCnt);
+    else
+        nodeCountKernel<<<smallGrid(cap), 256, 0, s>>>(node, hdr, cap, nNodes, nodeCnt);
     TBLAEQ_CUDA(cudaGetLastError());
     nodeScanKernel<<<1, 1024, 0, s>>>(nodeCnt, nNodes, nodeOff, unitOff);
     TBLAEQ_CUDA(cudaGetLastError());
-    nodeScatterKernel<<<smallGrid(cap), 256, 0, s>>>(node, hdr, cap, nNodes, nodeOff, cursor, list);
+    if (smem)
+        nodeScatterSmemKernel<<<smallGrid(cap), 256, 0, s>>>(node, hdr, cap, nNodes, nodeOff, cursor, list);
+    else
+        nodeScatterKernel<<<smallGrid(cap), 256, 0, s>>>(node, hdr, cap, nNodes, nodeOff, cursor, list);
     TBLAEQ_CUDA(cudaGetLastError());
 }
 
