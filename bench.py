@@ -243,13 +243,15 @@ def knn_legs(tb, h, P, K, steps, warmup, flush, n_plain=64):
             torch.cuda.synchronize()
             ts.append(time.perf_counter() - t1)
         c = h.knn_counters()
-        return nq * n_steps / sum(ts), c["rows"] / nq, ts
+        info = dict(h.knn_batch_info(), device_free_gb=torch.cuda.mem_get_info()[0] / 1e9,
+                    library_device_gb=tb.lib().tblaeq_live_device_bytes() / 1e9)
+        return nq * n_steps / sum(ts), c["rows"] / nq, ts, info
 
-    learned_qps, learned_rows, step_s = batch_leg(True, True, steps, warmup)
+    learned_qps, learned_rows, step_s, learned_info = batch_leg(True, True, steps, warmup)
     r = h.query_batch(tb.QueryType.POINT, dP, tb.Mode.EXACT, K=K)
     result = (r.offsets.numpy().copy(), r.ids.numpy().copy(), r.dist2.numpy().copy())
-    lb_qps, lb_rows, _ = batch_leg(True, False, 1, 1)
-    one_qps, one_rows, _ = batch_leg(False, False, 1, 1)
+    lb_qps, lb_rows, _, lb_info = batch_leg(True, False, 1, 1)
+    one_qps, one_rows, _, one_info = batch_leg(False, False, 1, 1)
 
     # The plain traversal: one query at a time, lower-bound ranking, scorer off.
     h.set_two_wave(True)
@@ -284,9 +286,9 @@ def knn_legs(tb, h, P, K, steps, warmup, flush, n_plain=64):
                        "plain_query_p50": pl[len(pl) // 2], "plain_query_p99": pl[min(len(pl) - 1, int(len(pl) * 0.99))]},
         "e2e": {"value": nq * len(e2e_t) / sum(e2e_t), "unit": "queries/s",
                 "h2d_bytes_per_step": nq * D * 8 + nq * 4, "d2h_bytes_per_step": (nq + 1) * 8 + tot * 16},
-        "ranking": {"learned": {"qps": learned_qps, "rows_per_query": learned_rows},
-                    "lower_bound": {"qps": lb_qps, "rows_per_query": lb_rows},
-                    "one_pass": {"qps": one_qps, "rows_per_query": one_rows}},
+        "ranking": {"learned": {"qps": learned_qps, "rows_per_query": learned_rows, "traversal": learned_info},
+                    "lower_bound": {"qps": lb_qps, "rows_per_query": lb_rows, "traversal": lb_info},
+                    "one_pass": {"qps": one_qps, "rows_per_query": one_rows, "traversal": one_info}},
         "plain": {"value": plain_qps, "unit": "queries/s", "queries": n_plain,
                   "kind": "one query at a time, lower-bound ranking, scorer off",
                   "speedup_batched_learned_vs_plain": learned_qps / plain_qps},
@@ -308,6 +310,12 @@ def main():
     ap.add_argument("--knn-queries", type=int, default=4096, help="batched: points of the KNN leg")
     ap.add_argument("--knn-steps", type=int, default=10, help="batched: timed steps of the KNN leg")
     ap.add_argument("--no-knn", action="store_true", help="batched: skip the KNN leg")
+    ap.add_argument("--knn-probe", type=int, default=-1,
+                    help="KNN: probe beam (clusters per query per level before wave 1; 0 = no probe; "
+                         "-1 = the library's default)")
+    ap.add_argument("--knn-completion", type=int, choices=[0, 1], default=1,
+                    help="KNN: 1 = node-major completion after wave 1, 0 = the query-major wave 2")
+    ap.add_argument("--knn-chunk", type=int, default=0, help="KNN: queries per traversal (0 = automatic)")
     ap.add_argument("--variants", default=None,
                     help="range configs: launch variant per level (0 direct, 1 staged, 2 node-major), comma "
                          "list; skips the autotuner (A/B timing, profiling one kind of kernel)")
@@ -479,6 +487,8 @@ def main():
     if cfg_name == "batched" and not args.no_knn:
         Pk = wl.knn_points(h, args.knn_queries, seed=1234, noise=0.02)
         Kk = knn_k(args.knn_queries)
+        kcfg = {}
+        knn_options(h, args, kcfg)
         T = wl.knn_points(h, 2048, seed=4321, noise=0.02)
         t0 = time.perf_counter()
         losses = h.scorer_train(T, K=knn_k(2048), max_samples=200000, epochs=8, lr=3e-3, seed=9)
@@ -487,7 +497,7 @@ def main():
             knn, knn_result = knn_legs(tb, h, Pk, Kk, args.knn_steps, args.warmup, flush)
         knn["value"] = knn["value"] * world
         knn["config"] = {"workload": f"knn on the same index: {args.knn_queries} points (data + N(0,(2% extent)^2)), "
-                                     "K=20 and K=100 alternating", "queries_per_step": args.knn_queries}
+                                     "K=20 and K=100 alternating", "queries_per_step": args.knn_queries, **kcfg}
         knn["scorer"] = {"train_queries": 2048, "train_s": train_s, "epoch_loss": losses, **h.scorer_stats()}
         knn["clocks"] = kclk.summary()
 
@@ -596,6 +606,17 @@ def knn_workload(tb, wl, nq, seed):
     return h, P, K
 
 
+def knn_options(h, args, config):
+    """Applies the KNN command-line options to a prepared handle and names them in `config`."""
+    if args.knn_probe >= 0 or args.knn_completion != 1:
+        beam = args.knn_probe if args.knn_probe >= 0 else 32
+        h.set_knn_probe(beam, bool(args.knn_completion))
+        config["knn_probe"] = {"beam": beam, "node_major_completion": bool(args.knn_completion)}
+    if args.knn_chunk:
+        h.set_knn_chunk(args.knn_chunk)
+        config["knn_chunk"] = args.knn_chunk
+
+
 def run_knn(args, tb, wl, rank, world, local):
     """Batched exact KNN (N=50M, D=16, 4096 queries, K in {20, 100}) with the learned frontier
     ranking, beside the lower-bound ranking, the one-pass finest level and one query at a time.
@@ -642,6 +663,7 @@ def run_knn(args, tb, wl, rank, world, local):
     tb.set_device(local)
     h, P, K = knn_workload(tb, wl, args.nq, seed=1234)
     h.prepare_for_query(tb.LevelPolicy.L0)
+    knn_options(h, args, config)
     flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
 
     # Scorer: trained on traces of separately seeded queries (up to 200,000 samples).

@@ -250,6 +250,15 @@ int tblaeq_set_two_wave(tblaeq_handle* h, int on);
  * either. No counterpart in the reference. */
 int tblaeq_set_knn_probe(tblaeq_handle* h, uint32_t beam, int node_major_completion);
 
+/* Queries per traversal of a KNN batch. A batch whose workspace exceeds the 32-bit traversal space or
+ * the free device memory runs as consecutive traversals of a halved size; later batches start at the
+ * size that fitted. max_queries > 0 caps every traversal at that many queries; 0 restores the
+ * automatic choice (and forgets the size learnt). No counterpart in the reference, which runs one
+ * query at a time. */
+int tblaeq_set_knn_chunk(tblaeq_handle* h, uint64_t max_queries);
+/* The last KNN batch: out2[0] = queries per traversal, out2[1] = traversals. */
+int tblaeq_knn_batch_info(tblaeq_handle* h, uint64_t* out2);
+
 /* Counters of the last KNN batch (summed over its chunks when it ran in several): [0] final-frontier
  * clusters, [1] wave-1 candidates,
  * [2] wave-2 candidates, [3] points whose rows wave 1 loaded and tested (the single pass, when

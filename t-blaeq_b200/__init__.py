@@ -152,6 +152,8 @@ def _load():
         "tblaeq_set_variants": ([vp, P(ctypes.c_int), ctypes.c_uint64], ctypes.c_int),
         "tblaeq_set_node_major": ([vp, ctypes.c_int], ctypes.c_int),
         "tblaeq_set_float_points": ([vp, ctypes.c_int], ctypes.c_int),
+        "tblaeq_set_knn_chunk": ([vp, ctypes.c_uint64], ctypes.c_int),
+        "tblaeq_knn_batch_info": ([vp, P(ctypes.c_uint64)], ctypes.c_int),
         "tblaeq_set_knn_probe": ([vp, ctypes.c_uint32, ctypes.c_int], ctypes.c_int),
         "tblaeq_set_launch_shapes": ([vp, P(ctypes.c_int), P(ctypes.c_int), ctypes.c_uint64], ctypes.c_int),
         "tblaeq_get_launch_shapes": ([vp, P(ctypes.c_int), P(ctypes.c_int), ctypes.c_uint64], ctypes.c_int),
@@ -585,6 +587,17 @@ class QueryHandler:
     # -- exact KNN tuning and the learned scorer ----------------------------------------------------
     def set_two_wave(self, on: bool):
         _check(_load().tblaeq_set_two_wave(self._h, int(on)))
+
+    def set_knn_chunk(self, max_queries: int = 0):
+        """KNN batches: at most this many queries per traversal (0: automatic, halving on overflow
+        or out-of-memory and starting later batches at the size that fitted)."""
+        _check(_load().tblaeq_set_knn_chunk(self._h, int(max_queries)))
+
+    def knn_batch_info(self) -> dict:
+        """The last KNN batch: queries per traversal and traversals."""
+        out = (ctypes.c_uint64 * 2)()
+        _check(_load().tblaeq_knn_batch_info(self._h, out))
+        return {"chunk": out[0], "traversals": out[1]}
 
     def knn_counters(self) -> dict:
         out = (ctypes.c_uint64 * 5)()

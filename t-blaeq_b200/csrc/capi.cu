@@ -23,6 +23,9 @@ struct tblaeq_handle {
     DeviceMem kStage;                           // per-query K of KNN batches
     DeviceMem knnOff, knnIds, knnD2;            // results of KNN batches run in chunks
     std::vector<uint64_t> knnSum;               // counters summed over the last batch's chunks (empty: one run)
+    uint64_t knnChunkHint = 0;                  // queries per traversal that last fitted after a split (0: none)
+    uint64_t knnChunkMax = 0;                   // caller's limit on queries per traversal (0: automatic)
+    uint64_t lastKnnChunk = 0, lastKnnRuns = 0; // the last KNN batch: queries per traversal, traversals
     uint64_t lastNq = 0;                        // last asynchronously enqueued batch
     unsigned lastFlags = 0;
 };
@@ -218,7 +221,7 @@ int tblaeq_coarsest_grid(tblaeq_handle* h, tblaeq_grid* out) {
 // chunks' results are gathered into the handle's buffers in query order. Per-level counts are not
 // kept for chunked batches.
 static BatchOutput runKnnChunked(tblaeq_handle* h, const double* dQueries, uint64_t nq, const std::vector<uint32_t>& k,
-                                 unsigned flags) {
+                                 unsigned flags, uint64_t firstChunk) {
     Runtime& rt = h->qh->runtime();
     const uint64_t D = rt.dev->D;
     uint64_t sumK = 0;
@@ -230,7 +233,7 @@ static BatchOutput runKnnChunked(tblaeq_handle* h, const double* dQueries, uint6
     if (h->knnOff.bytes() < (nq + 1) * 8) h->knnOff.alloc((nq + 1) * 8);
     std::vector<uint64_t> offs(nq + 1, 0), part;
     std::vector<uint64_t> sum(5, 0);
-    uint64_t chunk = (nq + 1) / 2, i = 0;
+    uint64_t chunk = std::max<uint64_t>(1, std::min(firstChunk, nq)), i = 0, runs = 0;
     while (i < nq) {
         const uint64_t c = std::min(chunk, nq - i);
         uint64_t sk = 0;
@@ -259,8 +262,14 @@ static BatchOutput runKnnChunked(tblaeq_handle* h, const double* dQueries, uint6
         const std::vector<uint64_t> cn = rt.engine->knnCounters();
         for (size_t t = 0; t < sum.size() && t < cn.size(); ++t) sum[t] += cn[t];
         i += c;
+        ++runs;
     }
     h->knnSum = sum;
+    // Later batches start at the size that fitted instead of failing at the full size first (each
+    // failure costs the growth steps and the workspace reset before the split).
+    h->knnChunkHint = chunk;
+    h->lastKnnChunk = chunk;
+    h->lastKnnRuns = runs;
     TBLAEQ_CUDA(cudaMemcpyAsync(h->knnOff.get(), offs.data(), (nq + 1) * 8, cudaMemcpyHostToDevice, rt.stream));
     TBLAEQ_CUDA(cudaStreamSynchronize(rt.stream));
     BatchOutput o;
@@ -291,11 +300,18 @@ static int runBatch(tblaeq_handle* h, const tblaeq_batch* b, const double* dQuer
         if (b->nq)
             TBLAEQ_CUDA(cudaMemcpyAsync(h->kStage.get(), k.data(), b->nq * 4, cudaMemcpyHostToDevice, rt.stream));
         h->knnSum.clear();
-        try {
-            o = rt.engine->runKnn(dQueries, static_cast<uint32_t>(b->nq), h->kStage.as<uint32_t>(), sumK, b->flags);
-        } catch (const CudaError& e) {
-            if (e.code != cudaErrorMemoryAllocation || b->nq < 2) throw;
-            o = runKnnChunked(h, dQueries, b->nq, k, b->flags);
+        const uint64_t limit = h->knnChunkMax ? h->knnChunkMax : h->knnChunkHint;
+        if (limit && b->nq > limit) {
+            o = runKnnChunked(h, dQueries, b->nq, k, b->flags, limit);
+        } else {
+            try {
+                o = rt.engine->runKnn(dQueries, static_cast<uint32_t>(b->nq), h->kStage.as<uint32_t>(), sumK, b->flags);
+                h->lastKnnChunk = b->nq;
+                h->lastKnnRuns = 1;
+            } catch (const CudaError& e) {
+                if (e.code != cudaErrorMemoryAllocation || b->nq < 2) throw;
+                o = runKnnChunked(h, dQueries, b->nq, k, b->flags, (b->nq + 1) / 2);
+            }
         }
     } else {
         o = rt.engine->runRange(dQueries, static_cast<uint32_t>(b->nq), b->mode, b->flags);
@@ -582,6 +598,21 @@ int tblaeq_set_two_wave(tblaeq_handle* h, int on) {
     return TBLAEQ_OK;
 }
 
+int tblaeq_set_knn_chunk(tblaeq_handle* h, uint64_t max_queries) {
+    if (int c = checkPrepared(h)) return c;
+    h->knnChunkMax = max_queries;
+    if (max_queries == 0) h->knnChunkHint = 0;
+    return TBLAEQ_OK;
+}
+
+int tblaeq_knn_batch_info(tblaeq_handle* h, uint64_t* out2) {
+    if (int c = checkPrepared(h)) return c;
+    if (!out2) return fail(TBLAEQ_ERR_INVALID, "null output");
+    out2[0] = h->lastKnnChunk;
+    out2[1] = h->lastKnnRuns;
+    return TBLAEQ_OK;
+}
+
 int tblaeq_knn_counters(tblaeq_handle* h, uint64_t* out5) {
     if (int c = checkPrepared(h)) return c;
     if (!out5) return fail(TBLAEQ_ERR_INVALID, "null output");
@@ -854,6 +885,7 @@ uint64_t tblaeq_live_device_bytes(void) { return liveDeviceBytes(); }
 int tblaeq_debug_split_above(tblaeq_handle* h, uint64_t limit) {
     if (int c = checkPrepared(h)) return c;
     h->qh->runtime().engine->setSplitLimit(limit ? limit : 0xffffffffull);
+    h->knnChunkHint = 0;  // a size learnt under another limit does not carry over
     return TBLAEQ_OK;
 }
 

@@ -173,3 +173,38 @@ def test_probe_and_node_major_completion_stay_exact(tb, env, oracle_mod, beam, c
         assert c["rows"] > 0
     finally:
         h.set_knn_probe(32, True)
+
+
+@pytest.mark.parametrize("fail_at", [3, 8, 20])
+def test_knn_batch_splits_when_an_allocation_fails(tb, oracle_mod, cuda, fail_at):
+    """An allocation that fails while a KNN batch grows its workspace (the fail_at-th device
+    allocation from the batch's start) leaves no buffer behind a stale capacity: the engine releases
+    its workspace, the batch reruns as smaller traversals with the brute force's results, later
+    batches start at the size that fitted, and closing the handle returns every byte."""
+    lib = tb.lib()
+    before = lib.tblaeq_live_device_bytes()
+    h = tb.QueryHandler.generate(100000, 6, 1.0, 100.0, False, 4, (40, 20, 10), 77, 2.5)
+    h.prepare_for_query(tb.LevelPolicy.L0)
+    pts, ids = h.decode_points(np.arange(100000))
+    P = _points(pts, 256, 5, noise=0.5)
+    b = oracle_mod.brute_query(pts, ids, oracle_mod.KNN, P, K=10)
+    lib.tblaeq_debug_fail_alloc_after(fail_at)
+    try:
+        r = h.query_batch(tb.QueryType.POINT, P, tb.Mode.EXACT, K=10)
+    finally:
+        lib.tblaeq_debug_fail_alloc_after(0)
+    assert np.array_equal(r.offsets.numpy(), b.offsets)
+    assert np.array_equal(r.ids.numpy(), b.ids) and np.array_equal(r.dist2.numpy(), b.dist2)
+    info = h.knn_batch_info()
+    r2 = h.query_batch(tb.QueryType.POINT, P, tb.Mode.EXACT, K=10)
+    assert np.array_equal(r2.ids.numpy(), b.ids)
+    if info["traversals"] > 1:  # the failure hit the batch's growth: the next batch starts split
+        assert h.knn_batch_info()["chunk"] == info["chunk"] < 256
+    h.set_knn_chunk(0)
+    r3 = h.query_batch(tb.QueryType.POINT, P, tb.Mode.EXACT, K=10)
+    assert np.array_equal(r3.ids.numpy(), b.ids) and h.knn_batch_info() == {"chunk": 256, "traversals": 1}
+    h.set_knn_chunk(64)
+    r4 = h.query_batch(tb.QueryType.POINT, P, tb.Mode.EXACT, K=10)
+    assert np.array_equal(r4.ids.numpy(), b.ids) and h.knn_batch_info() == {"chunk": 64, "traversals": 4}
+    h.close()
+    assert lib.tblaeq_live_device_bytes() == before
