@@ -229,12 +229,14 @@ def knn_legs(tb, h, P, K, steps, warmup, flush, n_plain=64):
     nq, D = P.shape
     dP = torch.from_numpy(P).cuda()
 
-    def batch_leg(two_wave, learned, n_steps, n_warm):
+    def batch_leg(two_wave, learned, n_steps, n_warm, nvtx=None):
         h.set_two_wave(two_wave)
         h.scorer_enable(learned)
         for _ in range(max(1, n_warm)):  # the first batch sizes every workspace
             h.query_batch(tb.QueryType.POINT, dP, tb.Mode.EXACT, K=K)
         ts = []
+        if nvtx:
+            torch.cuda.nvtx.range_push(nvtx)  # profilers select these steps by the range
         for _ in range(n_steps):
             flush.zero_()
             torch.cuda.synchronize()
@@ -242,12 +244,14 @@ def knn_legs(tb, h, P, K, steps, warmup, flush, n_plain=64):
             h.query_batch(tb.QueryType.POINT, dP, tb.Mode.EXACT, K=K)
             torch.cuda.synchronize()
             ts.append(time.perf_counter() - t1)
+        if nvtx:
+            torch.cuda.nvtx.range_pop()
         c = h.knn_counters()
         info = dict(h.knn_batch_info(), device_free_gb=torch.cuda.mem_get_info()[0] / 1e9,
                     library_device_gb=tb.lib().tblaeq_live_device_bytes() / 1e9)
         return nq * n_steps / sum(ts), c["rows"] / nq, ts, info
 
-    learned_qps, learned_rows, step_s, learned_info = batch_leg(True, True, steps, warmup)
+    learned_qps, learned_rows, step_s, learned_info = batch_leg(True, True, steps, warmup, nvtx="knn_timed")
     r = h.query_batch(tb.QueryType.POINT, dP, tb.Mode.EXACT, K=K)
     result = (r.offsets.numpy().copy(), r.ids.numpy().copy(), r.dist2.numpy().copy())
     lb_qps, lb_rows, _, lb_info = batch_leg(True, False, 1, 1)
@@ -316,6 +320,8 @@ def main():
     ap.add_argument("--knn-completion", type=int, choices=[0, 1], default=1,
                     help="KNN: 1 = node-major completion after wave 1, 0 = the query-major wave 2")
     ap.add_argument("--knn-chunk", type=int, default=0, help="KNN: queries per traversal (0 = automatic)")
+    ap.add_argument("--knn-wave1", type=float, default=0.0,
+                    help="KNN: wave-1 scale (clusters = ceil(scale*K/leaf)+1, 2..32; 0 = the library's default)")
     ap.add_argument("--variants", default=None,
                     help="range configs: launch variant per level (0 direct, 1 staged, 2 node-major), comma "
                          "list; skips the autotuner (A/B timing, profiling one kind of kernel)")
@@ -615,6 +621,9 @@ def knn_options(h, args, config):
     if args.knn_chunk:
         h.set_knn_chunk(args.knn_chunk)
         config["knn_chunk"] = args.knn_chunk
+    if args.knn_wave1 > 0:
+        h.set_knn_wave1(args.knn_wave1)
+        config["knn_wave1_scale"] = args.knn_wave1
 
 
 def run_knn(args, tb, wl, rank, world, local):

@@ -250,6 +250,13 @@ int tblaeq_set_two_wave(tblaeq_handle* h, int on);
  * either. No counterpart in the reference. */
 int tblaeq_set_knn_probe(tblaeq_handle* h, uint32_t beam, int node_major_completion);
 
+/* Wave 1 of a two-wave KNN batch reads every point of each query's ceil(scale * K / leaf) + 1
+ * best-ranked finest clusters (at least 2, at most 32; leaf = the index's points per finest cluster)
+ * and takes the K-th distance among them as the bound the rest of the batch prunes with. A larger
+ * wave 1 costs more rows up front and tightens the bound (default scale 1). Same results for every
+ * scale. No counterpart in the reference (its KNN keeps the STEP candidate set). */
+int tblaeq_set_knn_wave1(tblaeq_handle* h, double scale);
+
 /* Queries per traversal of a KNN batch. A batch whose workspace exceeds the 32-bit traversal space or
  * the free device memory runs as consecutive traversals of a halved size; later batches start at the
  * size that fitted. max_queries > 0 caps every traversal at that many queries; 0 restores the

@@ -153,6 +153,7 @@ def _load():
         "tblaeq_set_node_major": ([vp, ctypes.c_int], ctypes.c_int),
         "tblaeq_set_float_points": ([vp, ctypes.c_int], ctypes.c_int),
         "tblaeq_set_knn_chunk": ([vp, ctypes.c_uint64], ctypes.c_int),
+        "tblaeq_set_knn_wave1": ([vp, ctypes.c_double], ctypes.c_int),
         "tblaeq_knn_batch_info": ([vp, P(ctypes.c_uint64)], ctypes.c_int),
         "tblaeq_set_knn_probe": ([vp, ctypes.c_uint32, ctypes.c_int], ctypes.c_int),
         "tblaeq_set_launch_shapes": ([vp, P(ctypes.c_int), P(ctypes.c_int), ctypes.c_uint64], ctypes.c_int),
@@ -592,6 +593,11 @@ class QueryHandler:
         """KNN batches: at most this many queries per traversal (0: automatic, halving on overflow
         or out-of-memory and starting later batches at the size that fitted)."""
         _check(_load().tblaeq_set_knn_chunk(self._h, int(max_queries)))
+
+    def set_knn_wave1(self, scale: float = 1.0):
+        """Two-wave KNN: wave 1 reads each query's ceil(scale * K / leaf) + 1 best-ranked clusters
+        (2..32); larger tightens the bound the rest of the batch prunes with. Same results."""
+        _check(_load().tblaeq_set_knn_wave1(self._h, float(scale)))
 
     def knn_batch_info(self) -> dict:
         """The last KNN batch: queries per traversal and traversals."""

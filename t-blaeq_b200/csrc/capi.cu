@@ -300,7 +300,8 @@ static int runBatch(tblaeq_handle* h, const tblaeq_batch* b, const double* dQuer
         if (b->nq)
             TBLAEQ_CUDA(cudaMemcpyAsync(h->kStage.get(), k.data(), b->nq * 4, cudaMemcpyHostToDevice, rt.stream));
         h->knnSum.clear();
-        const uint64_t limit = h->knnChunkMax ? h->knnChunkMax : h->knnChunkHint;
+        const uint64_t limit = (h->knnChunkMax && h->knnChunkHint) ? std::min(h->knnChunkMax, h->knnChunkHint)
+                                                                     : (h->knnChunkMax ? h->knnChunkMax : h->knnChunkHint);
         if (limit && b->nq > limit) {
             o = runKnnChunked(h, dQueries, b->nq, k, b->flags, limit);
         } else {
@@ -595,6 +596,13 @@ int tblaeq_tuning_lookup(const char* path, const char* key, int* variants, int* 
 int tblaeq_set_two_wave(tblaeq_handle* h, int on) {
     if (int c = checkPrepared(h)) return c;
     h->qh->runtime().engine->setTwoWave(on != 0);
+    return TBLAEQ_OK;
+}
+
+int tblaeq_set_knn_wave1(tblaeq_handle* h, double scale) {
+    if (int c = checkPrepared(h)) return c;
+    if (!(scale > 0.0) || scale > 1e6) return fail(TBLAEQ_ERR_INVALID, "wave-1 scale must be in (0, 1e6]");
+    h->qh->runtime().engine->setWaveScale(scale);
     return TBLAEQ_OK;
 }
 

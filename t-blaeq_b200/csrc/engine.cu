@@ -505,9 +505,12 @@ void BatchEngine::enqueueLaunches(const double* dBoxes, uint32_t nq, int mode, u
             buf = 1 - buf;
         } else {
             a.child.outMap = di_.mapPtr[H - 1];
-            if (mode == kModeExact && floatPoints_ && di_.pointsF.bytes()) {
+            int finestPred = (mode == kModeExact) ? kPredRangeBox : kPredAll;
+            if (mode == kModeExact && floatPoints_ && di_.pointsF.bytes() && floatPointsSupported(di_.D) &&
+                variants_[m] != kVariantStaged) {
                 a.child.rowsF = di_.pointsF.as<float>();
                 a.query.boxesFi = boxFi;
+                finestPred = kPredRangeBoxF;
             }
             a.rout.qcount = qcount;
             a.rout.hdr = hdrPtr(H);
@@ -522,7 +525,7 @@ void BatchEngine::enqueueLaunches(const double* dBoxes, uint32_t nq, int mode, u
                 a.rout.ids = resIds_.as<uint64_t>();
                 a.rout.vals = (flags & kWantVals) ? resVals_.as<double>() : nullptr;
             }
-            launchExpand(a, (mode == kModeExact) ? kPredRangeBox : kPredAll, true, 0, stream_);
+            launchExpand(a, finestPred, true, 0, stream_);
         }
         if (timing_) record(2 + m);
     }
@@ -893,7 +896,7 @@ void BatchEngine::enqueueKnn(const double* dPoints, uint32_t nq, const uint32_t*
                       di_.aabb[H - 2].as<float>(), lbE_.as<double>(), scoreE_.as<double>(), stream_);
     if (scorer_) scorer_(scorerCtx_, F, fb.node.as<uint32_t>(), fcap, dPoints, scoreE_.as<double>(), stream_);
     const double avgLeaf = static_cast<double>(di_.meshCount[H - 1]) / static_cast<double>(di_.meshCount[H - 2]);
-    launchWaveWidth(dK, nq, 1.0 / avgLeaf, waveM_.as<uint32_t>(), stream_);
+    launchWaveWidth(dK, nq, waveScale_ / avgLeaf, waveM_.as<uint32_t>(), stream_);
     launchClampCounts(offF_.as<uint64_t>(), waveM_.as<uint32_t>(), nq, selCount_.as<uint32_t>(), stream_);
     launchExclusiveScan(selCount_.as<uint32_t>(), selOff_.as<uint64_t>(), nq, stream_);
     launchTopK(offF_.as<uint64_t>(), nullptr, scoreE_.as<double>(), fcap, nullptr, nullptr, nullptr, 0,

@@ -58,6 +58,10 @@ public:
     // query to bound the K-th distance by real points, then expand only the clusters that bound
     // cannot exclude. Off: one pass over every surviving cluster.
     void setTwoWave(bool on) { twoWave_ = on; }
+    // Wave 1 of a two-wave KNN batch reads the ceil(scale * K / leaf) + 1 best-ranked clusters of
+    // each query (2..32; leaf = points per finest cluster on average); default scale 1.
+    void setWaveScale(double scale) { waveScale_ = scale > 0 ? scale : 1.0; }
+    double waveScale() const { return waveScale_; }
     // Exact KNN with the two-wave finest level: beam width of the probe (each query keeps its
     // probeBeam entries of smallest lower bound at every level above the clusters, so wave 1 ranks
     // only the clusters under them; 0: no beam, every surviving cluster is ranked), and whether the
@@ -220,6 +224,7 @@ private:
     bool timing_ = false;
     bool capturing_ = false;
     bool twoWave_ = true;
+    double waveScale_ = 1.0;
     EntryScorer scorer_ = nullptr;
     void* scorerCtx_ = nullptr;
     std::vector<int> variants_;

@@ -219,6 +219,10 @@ constexpr int warpSmemBytes() {
 #ifndef TBLAEQ_UNROLL_PASS2
 #define TBLAEQ_UNROLL_PASS2 1
 #endif
+// The finest exact range level with float points (kPredRangeBoxF).
+#ifndef TBLAEQ_UNROLL_FLOAT_TEST
+#define TBLAEQ_UNROLL_FLOAT_TEST 8
+#endif
 constexpr int kExpandThreads = TBLAEQ_EXPAND_THREADS;
 
 // Resident CTAs per SM the register allocation is sized for (128 threads: 10 CTAs = 51 registers,
@@ -230,7 +234,7 @@ constexpr int kExpandThreads = TBLAEQ_EXPAND_THREADS;
 template <int PRED>
 constexpr int expandMinBlocks() {
     return (PRED == kPredKnnBound || PRED == kPredRangeRadius) ? TBLAEQ_EXPAND_MIN_BLOCKS_BOUND
-           : PRED == kPredRangeBox                             ? TBLAEQ_EXPAND_MIN_BLOCKS_BOX
+           : (PRED == kPredRangeBox || PRED == kPredRangeBoxF) ? TBLAEQ_EXPAND_MIN_BLOCKS_BOX
                                                                : TBLAEQ_EXPAND_MIN_BLOCKS;
 }
 
@@ -263,7 +267,8 @@ __device__ __forceinline__ void bulkPrefetchL2(const void* p, uint32_t bytes) {
 template <int D, int PRED>
 constexpr bool prefetchesRows() {
     return D > 0 && (8 * D) % 16 == 0 &&
-           (PRED == kPredRangeBox || PRED == kPredKnnPoint || PRED == kPredKnnBound || PRED == kPredRangeRadius);
+           (PRED == kPredRangeBox || PRED == kPredRangeBoxF || PRED == kPredKnnPoint || PRED == kPredKnnBound ||
+            PRED == kPredRangeRadius);
 }
 
 // Prefetches into L2 the child rows of tile `t`: one contiguous run per frontier entry that the
@@ -350,7 +355,7 @@ __device__ __forceinline__ bool evalItem(const ExpandArgs& a, int dim, const dou
             return cc > 0;
         }
         return true;
-    } else if constexpr (PRED == kPredRangeRadius || PRED == kPredRangeBox) {
+    } else if constexpr (PRED == kPredRangeRadius || PRED == kPredRangeBox || PRED == kPredRangeBoxF) {
         const double* box = a.query.boxes + static_cast<size_t>(q) * 2 * dim;
         double dist = 0.0;
         bool in = true;
@@ -636,11 +641,13 @@ __global__ void __launch_bounds__(kExpandThreads, expandMinBlocks<PRED>()) expan
     constexpr bool NODE = needsNode<PRED, TO_RESULT>();
     // Code size (see TBLAEQ_UNROLL_FRONTIER_TEST); the KNN levels unroll every loop.
     constexpr bool kKnn = PRED == kPredKnnBound || PRED == kPredKnnPoint;
-    constexpr int kUnrollTest = (TO_RESULT || kKnn) ? R : TBLAEQ_UNROLL_FRONTIER_TEST;
+    constexpr int kUnrollTest = (PRED == kPredRangeBoxF) ? TBLAEQ_UNROLL_FLOAT_TEST
+                                : (TO_RESULT || kKnn)     ? R
+                                                          : TBLAEQ_UNROLL_FRONTIER_TEST;
     constexpr int kUnrollPass2 = kKnn ? R : TBLAEQ_UNROLL_PASS2;
     constexpr bool kFastBox = PRED == kPredRangeBox && TO_RESULT && !STAGED && coalescedBox<D>();
     // Finest exact range level with float points (a.child.rowsF): every round tests them first.
-    constexpr bool kFloatPts = PRED == kPredRangeBox && TO_RESULT && !STAGED && coalescedBoxF<D>();
+    constexpr bool kFloatPts = PRED == kPredRangeBoxF && TO_RESULT && !STAGED && coalescedBoxF<D>();
     constexpr bool kFastAabb = PRED == kPredRangeRadius && coalescedAabb<D>();
     // Exact range frontier levels test children that pass the box prefilter after the rounds,
     // 32 at a time, so the FP64 radius test runs on full warps instead of in every round that
@@ -691,7 +698,7 @@ __global__ void __launch_bounds__(kExpandThreads, expandMinBlocks<PRED>()) expan
         // The tile's rows are one contiguous run per entry: the TMA unit brings each run into L2
         // now (one instruction per run, no registers), ahead of the per-round row loads.
         if constexpr (prefetchesRows<D, PRED>())
-            prefetchTileRows<D, PRED>(a, tile, nTiles, entries, total, lane, kFloatPts && a.child.rowsF != nullptr);
+            prefetchTileRows<D, PRED>(a, tile, nTiles, entries, total, lane, kFloatPts);
         const uint32_t t0 = tile * kWarpTile;
 
         // ---- phase A: stage the tile's entries in shared memory (one round of parallel loads),
@@ -823,12 +830,14 @@ __global__ void __launch_bounds__(kExpandThreads, expandMinBlocks<PRED>()) expan
                 // Warp-uniform: a full round inside one entry (its first and last item share it).
                 const uint32_t w0 = sWin[r * 32], w31 = sWin[r * 32 + 31];
                 if (W != 0 && t0 + r * 32 + 32 <= total && w0 == w31 && !a.child.rowsOnHost) {
-                    if constexpr (kFloatPts) {
-                        keep = a.child.rowsF ? singleEntryRangeBoxF<D>(a, sRow[r * 32], eLo + w0, wQ[w0], lane)
-                                             : singleEntryRangeBox<D>(a, sRow[r * 32], eLo + w0, wQ[w0], lane);
-                    } else {
-                        keep = singleEntryRangeBox<D>(a, sRow[r * 32], eLo + w0, wQ[w0], lane);
-                    }
+                    keep = singleEntryRangeBox<D>(a, sRow[r * 32], eLo + w0, wQ[w0], lane);
+                    done = true;
+                }
+            }
+            if constexpr (kFloatPts) {
+                const uint32_t w0 = sWin[r * 32], w31 = sWin[r * 32 + 31];
+                if (W != 0 && t0 + r * 32 + 32 <= total && w0 == w31) {
+                    keep = singleEntryRangeBoxF<D>(a, sRow[r * 32], eLo + w0, wQ[w0], lane);
                     done = true;
                 }
             }
@@ -865,8 +874,8 @@ __global__ void __launch_bounds__(kExpandThreads, expandMinBlocks<PRED>()) expan
                         const double* rowp = reinterpret_cast<const double*>(rowBuf + (slot * 32 + lane) * S::kStride);
                         if constexpr (NODE) nr = nodeBuf[slot * 32 + lane];
                         keep = evalItem<D, DM, PRED, TO_RESULT, true>(a, dim, rowp, xp, q, j, kk, nr, cc);
-                    } else if (kFloatPts && a.child.rowsF) {
-                        if constexpr (kFloatPts) keep = pointInBoxF<D>(a, j, e, q);
+                    } else if constexpr (kFloatPts) {
+                        keep = pointInBoxF<D>(a, j, e, q);
                     } else {
                         if constexpr (NODE) nr = a.child.nodes[kk];
                         keep = evalItem<D, DM, PRED, TO_RESULT, false>(a, dim, a.child.rows + static_cast<size_t>(j) * dim,
@@ -1142,6 +1151,7 @@ void dispatchPred(const ExpandArgs& a, int pred, bool toResult, int g, cudaStrea
         switch (pred) {
             case kPredAll: return launchOne<D, kPredAll, true, ST>(a, g, s);
             case kPredRangeBox: return launchOne<D, kPredRangeBox, true, ST>(a, g, s);
+            case kPredRangeBoxF: return launchOne<D, kPredRangeBoxF, true, ST>(a, g, s);
             case kPredMask: return launchOne<D, kPredMask, true, ST>(a, g, s);
             case kPredKnnPoint: return launchOne<D, kPredKnnPoint, true, ST>(a, g, s);
             default: break;

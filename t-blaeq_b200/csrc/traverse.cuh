@@ -128,6 +128,8 @@ enum Pred : int {
     kPredRangeBox = 3,          // keep point if lo <= y <= hi on every dimension
     kPredKnnBound = 4,          // keep child if dist - rad <= tau (and it has children)
     kPredKnnPoint = 5,          // keep point if dist2 <= tau^2 (records dist2)
+    kPredRangeBoxF = 6,         // kPredRangeBox decided from the points' float copies (child.rowsF,
+                                // query.boxesFi), with the FP64 test only near a face: same keeps
 };
 
 // Kernel variants an autotuner chooses between per level: rows loaded straight into registers,

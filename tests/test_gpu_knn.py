@@ -208,3 +208,18 @@ def test_knn_batch_splits_when_an_allocation_fails(tb, oracle_mod, cuda, fail_at
     assert np.array_equal(r4.ids.numpy(), b.ids) and h.knn_batch_info() == {"chunk": 64, "traversals": 4}
     h.close()
     assert lib.tblaeq_live_device_bytes() == before
+
+
+@pytest.mark.parametrize("scale", [0.5, 4.0, 64.0])
+def test_wave_one_width_keeps_results(tb, env, oracle_mod, scale):
+    """Wave 1's width (how many best-ranked clusters per query it reads before the bound is set)
+    changes the work, never the results."""
+    h, o, pts, ids = env
+    P = _points(pts, 200, 51)
+    b = oracle_mod.brute_query(pts, ids, oracle_mod.KNN, P, K=30)
+    h.set_knn_wave1(scale)
+    try:
+        r = h.query_batch(tb.QueryType.POINT, P, tb.Mode.EXACT, K=30)
+        assert np.array_equal(r.ids.numpy(), b.ids) and np.array_equal(r.dist2.numpy(), b.dist2)
+    finally:
+        h.set_knn_wave1(1.0)
