@@ -209,6 +209,19 @@ int tblaeq_set_node_major(tblaeq_handle* h, int on);
  * reference, whose final filter reads every surviving point's doubles. */
 int tblaeq_set_float_points(tblaeq_handle* h, int on);
 
+/* Exact range batches with float points: every finest cluster's points are kept in point groups
+ * of at most 32 (a median split along the widest dimension, repeated; the rows of a cluster are
+ * reordered within the cluster's own range when the index is prepared), each with the box of its
+ * points. The finest level first keeps the groups whose box meets the query box and then tests
+ * only their points (on = default; off = every point of every surviving cluster). Same results.
+ * Batches that ask for per-level counts (TBLAEQ_WANT_LEVELS) test every point: those counts are
+ * the points of the surviving clusters. No counterpart in the reference. */
+int tblaeq_set_point_groups(tblaeq_handle* h, int on);
+/* The last range batch's point groups: out3[0] groups tested, out3[1] (query, group) pairs kept,
+ * out3[2] points tested; zeros when it tested no groups. With groups, tblaeq_level_counts'
+ * children of the finest clusters are their groups. */
+int tblaeq_group_counts(tblaeq_handle* h, uint64_t* out3);
+
 /* ---- Launch shapes and the tuning cache (no counterpart in the reference, whose kernel shapes are
  * compile-time constants: kCompact* in src/core/strategies/L0Strategy.cu:18-21, UNROLL_FACTOR in
  * src/Kernel/SpMSpV.cuh:24) ----

@@ -152,6 +152,8 @@ def _load():
         "tblaeq_set_variants": ([vp, P(ctypes.c_int), ctypes.c_uint64], ctypes.c_int),
         "tblaeq_set_node_major": ([vp, ctypes.c_int], ctypes.c_int),
         "tblaeq_set_float_points": ([vp, ctypes.c_int], ctypes.c_int),
+        "tblaeq_set_point_groups": ([vp, ctypes.c_int], ctypes.c_int),
+        "tblaeq_group_counts": ([vp, P(ctypes.c_uint64)], ctypes.c_int),
         "tblaeq_set_knn_chunk": ([vp, ctypes.c_uint64], ctypes.c_int),
         "tblaeq_set_knn_wave1": ([vp, ctypes.c_double], ctypes.c_int),
         "tblaeq_knn_batch_info": ([vp, P(ctypes.c_uint64)], ctypes.c_int),
@@ -549,6 +551,17 @@ class QueryHandler:
         """Exact range batches: finest points decided from their float copies first (default;
         same results), or every point's FP64 test."""
         _check(_load().tblaeq_set_float_points(self._h, int(on)))
+
+    def set_point_groups(self, on: bool = True):
+        """Exact range batches with float points: test the finest clusters' point groups (at most
+        32 points each, with their boxes) before their points (default; same results)."""
+        _check(_load().tblaeq_set_point_groups(self._h, int(on)))
+
+    def group_counts(self) -> dict:
+        """The last range batch's point groups: tested, (query, group) pairs kept, points tested."""
+        out = (ctypes.c_uint64 * 3)()
+        _check(_load().tblaeq_group_counts(self._h, out))
+        return {"groups": out[0], "kept": out[1], "points": out[2]}
 
     def launch_shapes(self):
         """(variants, grid percentages) per expand launch."""

@@ -518,6 +518,22 @@ int tblaeq_set_float_points(tblaeq_handle* h, int on) {
     return TBLAEQ_OK;
 }
 
+int tblaeq_set_point_groups(tblaeq_handle* h, int on) {
+    if (int c = checkPrepared(h)) return c;
+    h->qh->runtime().engine->setPointGroups(on != 0);
+    return TBLAEQ_OK;
+}
+
+int tblaeq_group_counts(tblaeq_handle* h, uint64_t* out3) {
+    if (int c = checkPrepared(h)) return c;
+    if (!out3) return fail(TBLAEQ_ERR_INVALID, "null output");
+    return guarded([&]() -> int {
+        const std::vector<uint64_t> v = h->qh->runtime().engine->groupCounts();
+        for (int i = 0; i < 3; ++i) out3[i] = v[i];
+        return TBLAEQ_OK;
+    });
+}
+
 int tblaeq_set_launch_shapes(tblaeq_handle* h, const int* variants, const int* grid_percent, uint64_t n) {
     if (int c = checkPrepared(h)) return c;
     if (!variants || !grid_percent) return fail(TBLAEQ_ERR_INVALID, "null launch shapes");

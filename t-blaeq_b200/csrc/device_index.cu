@@ -5,6 +5,7 @@
 #include <omp.h>
 
 #include <algorithm>
+#include <functional>
 #include <atomic>
 #include <cmath>
 #include <limits>
@@ -110,12 +111,91 @@ DerivedArrays computeDerived(const HostIndex& idx) {
 
     out.nodeX.resize(H - 1);
     for (uint64_t m = 0; m + 1 < H; ++m) out.nodeX[m] = dec[m];
-    if (floatPointsSupported(D)) {
+    if (floatPointsSupported(D) && H >= 2) {
+        // Point groups: every finest cluster's rows, reordered within the cluster's own row range by
+        // median splits along the widest dimension until at most kPointGroup rows remain, and the
+        // float copy of the points in that order.
         const std::vector<double>& pts = dec[H - 1];
-        out.pointsF.resize(pts.size());
-        const int64_t n = static_cast<int64_t>(pts.size());
-#pragma omp parallel for schedule(static)
-        for (int64_t i = 0; i < n; ++i) out.pointsF[i] = static_cast<float>(pts[i]);
+        const uint64_t nRows = pts.size() / D;
+        const uint64_t nCl = out.cbeg[H - 2].size();
+        std::function<uint32_t(uint32_t)> leaves = [&](uint32_t n) -> uint32_t {
+            return n <= kPointGroup ? 1u : leaves(n / 2) + leaves(n - n / 2);
+        };
+        out.clusterGroup.assign(nCl + 1, 0);
+        for (uint64_t c = 0; c < nCl; ++c)
+            out.clusterGroup[c + 1] = out.clusterGroup[c] + (out.ccnt[H - 2][c] ? leaves(out.ccnt[H - 2][c]) : 0u);
+        const uint64_t G = out.clusterGroup[nCl];
+        out.pointPerm.resize(nRows);
+        out.pointsF.resize(nRows * D);
+        out.groupFirst.resize(G);
+        out.groupCount.resize(G);
+        out.groupBox.resize(G * 2 * D);
+        auto down = [](double v) {
+            float f = static_cast<float>(v);
+            if (static_cast<double>(f) > v) f = std::nextafter(f, -std::numeric_limits<float>::infinity());
+            return f;
+        };
+        auto up = [](double v) {
+            float f = static_cast<float>(v);
+            if (static_cast<double>(f) < v) f = std::nextafter(f, std::numeric_limits<float>::infinity());
+            return f;
+        };
+#pragma omp parallel for schedule(dynamic, 256)
+        for (int64_t c = 0; c < static_cast<int64_t>(nCl); ++c) {
+            const uint32_t b = out.cbeg[H - 2][c], n = out.ccnt[H - 2][c];
+            std::vector<uint32_t> rows(n);
+            for (uint32_t i = 0; i < n; ++i) rows[i] = b + i;
+            uint32_t g = out.clusterGroup[c];
+            // Explicit stack of (first, count) ranges of `rows`, split in order (left before right).
+            std::vector<std::pair<uint32_t, uint32_t>> stack;
+            if (n) stack.emplace_back(0u, n);
+            while (!stack.empty()) {
+                const auto [f, k] = stack.back();
+                stack.pop_back();
+                if (k <= kPointGroup) {
+                    out.groupFirst[g] = b + f;
+                    out.groupCount[g] = k;
+                    float* box = &out.groupBox[static_cast<size_t>(g) * 2 * D];
+                    for (uint64_t d = 0; d < D; ++d) {
+                        double lo = std::numeric_limits<double>::infinity(), hi = -lo;
+                        for (uint32_t i = f; i < f + k; ++i) {
+                            lo = std::min(lo, pts[rows[i] * D + d]);
+                            hi = std::max(hi, pts[rows[i] * D + d]);
+                        }
+                        box[d] = down(lo);
+                        box[D + d] = up(hi);
+                    }
+                    ++g;
+                    continue;
+                }
+                uint64_t best = 0;
+                double bestExt = -1.0;
+                for (uint64_t d = 0; d < D; ++d) {
+                    double lo = std::numeric_limits<double>::infinity(), hi = -lo;
+                    for (uint32_t i = f; i < f + k; ++i) {
+                        lo = std::min(lo, pts[rows[i] * D + d]);
+                        hi = std::max(hi, pts[rows[i] * D + d]);
+                    }
+                    if (hi - lo > bestExt) {
+                        bestExt = hi - lo;
+                        best = d;
+                    }
+                }
+                const uint32_t h = k / 2;
+                std::nth_element(rows.begin() + f, rows.begin() + f + h, rows.begin() + f + k,
+                                 [&](uint32_t x, uint32_t y) {
+                                     const double vx = pts[x * D + best], vy = pts[y * D + best];
+                                     return vx < vy || (vx == vy && x < y);
+                                 });
+                stack.emplace_back(f + h, k - h);
+                stack.emplace_back(f, h);
+            }
+            for (uint32_t i = 0; i < n; ++i) {
+                out.pointPerm[b + i] = rows[i];
+                for (uint64_t d = 0; d < D; ++d)
+                    out.pointsF[(static_cast<size_t>(b) + i) * D + d] = static_cast<float>(pts[static_cast<size_t>(rows[i]) * D + d]);
+            }
+        }
     }
     // Box of the finest points below every node (exact min / max of decoded coordinates), stored
     // as floats rounded outward.
@@ -351,6 +431,16 @@ std::unique_ptr<DeviceIndex> buildDeviceIndex(const HostIndex& idx, const Derive
     }
     if (!der.pointsF.empty() && idx.intervals > 0 && res(idx.intervals - 1) == kResident) {
         di->pointsF = upload(der.pointsF, s);
+        di->pointPerm = upload(der.pointPerm, s);
+        const size_t G = der.groupFirst.size(), nCl = der.clusterGroup.size() - 1;
+        std::vector<NodeRec> grec(G), crec(nCl);
+        for (size_t g = 0; g < G; ++g) grec[g] = NodeRec{0.0, der.groupFirst[g], der.groupCount[g]};
+        for (size_t c = 0; c < nCl; ++c)
+            crec[c] = NodeRec{der.radSub[idx.height - 2][c], der.clusterGroup[c],
+                              der.clusterGroup[c + 1] - der.clusterGroup[c]};
+        di->groupRec = upload(grec, s);
+        di->groupBox = upload(der.groupBox, s);
+        di->clusterGroups = upload(crec, s);
         TBLAEQ_CUDA(cudaStreamSynchronize(s));
     }
     TBLAEQ_CUDA(cudaStreamSynchronize(s));
@@ -361,7 +451,7 @@ size_t DeviceIndex::deviceBytes() const {
     size_t t = coarseVals.bytes() + coarseIds.bytes();
     for (auto* v : {&pvals, &nodeRef, &nodeSub, &leaf, &aabb, &nodeX, &nodeOrig, &maps})
         for (auto& m : *v) t += m.bytes();
-    return t + pointsF.bytes();
+    return t + pointsF.bytes() + pointPerm.bytes() + groupRec.bytes() + groupBox.bytes() + clusterGroups.bytes();
 }
 
 }  // namespace tblaeq

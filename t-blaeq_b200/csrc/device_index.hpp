@@ -83,10 +83,20 @@ struct DerivedArrays {
     // Decoded coordinates of every node (position order, D per node), as the traversal rebuilds
     // them (y = P[j] * x_parent, one rounded multiply per level).
     std::vector<std::vector<double>> nodeX;
-    // Decoded finest points (row order of the last interval) as floats rounded to nearest, for the
-    // finest exact range level's float test; empty where that test has no kernel (D not 4, 8, 16).
-    std::vector<float> pointsF;
+    // Point groups of the finest exact range level (empty where its float test has no kernel: D not
+    // 4, 8, 16). Every finest cluster's rows are reordered within the cluster's own row range by
+    // median splits along the widest dimension until at most kPointGroup rows remain; each run so
+    // formed is a point group, with the box of its points.
+    std::vector<float> pointsF;          // decoded finest points in that order, floats rounded to nearest
+    std::vector<uint32_t> pointPerm;     // reordered row -> row of the last interval's P tensor
+    std::vector<uint32_t> groupFirst;    // per group: first reordered row
+    std::vector<uint32_t> groupCount;    // per group: its rows
+    std::vector<float> groupBox;         // per group: lo[D] hi[D] of its points, rounded outward
+    std::vector<uint32_t> clusterGroup;  // per finest cluster (mesh H-2 position): first group; one more at the end
 };
+
+// Most points of one point group.
+constexpr uint32_t kPointGroup = 32;
 
 // Host computation of the position-space node arrays, including subtree radii from the decoded
 // hierarchy (decoded exactly like the traversal: y = P[j] * x_parent, one rounded multiply).
@@ -137,8 +147,11 @@ struct DeviceIndex {
     std::vector<DeviceMem> leaf;             // mesh m < height-1: finest points below each node (uint32)
     std::vector<DeviceMem> aabb;             // mesh m < height-1: outward-rounded float box of the points below
     std::vector<DeviceMem> nodeX;            // mesh m < height-1: decoded coordinates (D doubles per node)
-    DeviceMem pointsF;                       // finest points as floats (DerivedArrays::pointsF), when the
-                                             // last interval's rows are device-resident; else empty
+    // Finest exact range level, when the last interval's rows are device-resident (else empty): the
+    // points as floats in point-group order (DerivedArrays::pointsF), that order's row map, every
+    // group's record {0, first row, rows} and box, and every finest cluster's record
+    // {subtree radius, first group, groups}.
+    DeviceMem pointsF, pointPerm, groupRec, groupBox, clusterGroups;
 
     // original-id space (per-level plugin)
     DeviceMem coarseIds;                     // uint64

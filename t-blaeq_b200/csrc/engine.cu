@@ -274,7 +274,7 @@ void BatchEngine::reserve(const EngineCaps& want, uint32_t nq, unsigned flags) {
         offStatus_ = off;
         off = align256(off + 4);
         offHdr_ = off;
-        off = align256(off + (H + 3) * 2 * 4);
+        off = align256(off + (H + 4) * 2 * 4);  // levels 0..H-1, results, wave 2, compaction, point groups
         offQcount_ = off;
         off = align256(off + static_cast<size_t>(qcap_) * 4);
         offLevels_ = off;
@@ -399,6 +399,14 @@ void BatchEngine::reserveNodeMajor(unsigned flags) {
     }
 }
 
+// Records of the children of level m (mesh m) in an exact range batch: the subtree radii with the
+// children's own children, or, for the finest clusters when this batch tests point groups, with
+// their groups.
+const NodeRec* BatchEngine::innerRecords(int m) const {
+    if (groupsThisBatch_ && m == static_cast<int>(di_.height) - 2) return di_.clusterGroups.as<NodeRec>();
+    return di_.nodeSub[m].as<NodeRec>();
+}
+
 // Level m of an exact range batch, node-major: group frontier `buf` by node (m >= 1), test every
 // node's children against the query boxes holding it, and append the survivors to the next frontier
 // (1 - buf).
@@ -431,7 +439,7 @@ void BatchEngine::enqueueNodeMajorLevel(int m, int buf, const double* dBoxes, ui
     n.rows = (m == 0) ? di_.coarseVals.as<double>() : di_.rows[m - 1];
     n.rowsOnHost = (m == 0) ? 0 : di_.rowsOnHost[m - 1];
     n.aabb = di_.aabb[m].as<float>();
-    n.children = di_.nodeSub[m].as<NodeRec>();
+    n.children = innerRecords(m);
     n.boxes = dBoxes;
     n.boxesF = boxF_.as<float>();
     n.out = outView(1 - buf, hdrPtr(m + 1));
@@ -475,6 +483,14 @@ void BatchEngine::enqueueLaunches(const double* dBoxes, uint32_t nq, int mode, u
                          (!(flags & kWantVals) || nmVals_);
     bool nodeMajor = false;
     int buf = 0;
+    // The finest exact level decides points from their float copies (not with the staged variant),
+    // and, unless per-level counts are wanted (they count the points of every surviving cluster),
+    // tests the clusters' point groups first: the last inner level then hands on (query, cluster)
+    // entries whose children are the cluster's groups, a group level keeps the groups whose box
+    // meets the query's, and the point level tests only their points.
+    const bool floatPath = mode == kModeExact && floatPoints_ && di_.pointsF.bytes() &&
+                           floatPointsSupported(di_.D) && variants_[H - 1] != kVariantStaged;
+    groupsThisBatch_ = floatPath && pointGroups_ && !wantLevels && di_.groupRec.bytes() && H >= 2;
     for (int m = 0; m < H; ++m) {
         if (nmReady && m < H - 1 && variants_[m] == kVariantNodeMajor) {
             nodeMajor = true;
@@ -498,17 +514,37 @@ void BatchEngine::enqueueLaunches(const double* dBoxes, uint32_t nq, int mode, u
         a.variant = variants_[m];
         a.gridPercent = grids_[m];
         if (m < H - 1) {
-            a.child.nodes = (mode == kModeExact) ? di_.nodeSub[m].as<NodeRec>() : di_.nodeRef[m].as<NodeRec>();
+            a.child.nodes = (mode == kModeExact) ? innerRecords(m) : di_.nodeRef[m].as<NodeRec>();
             a.child.aabb = (mode == kModeExact) ? di_.aabb[m].as<float>() : nullptr;
             a.fout = outView(1 - buf, hdrPtr(m + 1));
             launchExpand(a, kPredRangeRadius, false, 0, stream_);
             buf = 1 - buf;
         } else {
+            if (groupsThisBatch_) {
+                ExpandArgs g{};
+                g.in = inView(buf, hdrPtr(H - 1));
+                g.child.rows = nullptr;  // a group entry keeps its cluster's coordinates
+                g.child.nodes = di_.groupRec.as<NodeRec>();
+                g.child.aabb = di_.groupBox.as<float>();
+                g.query.boxes = dBoxes;
+                g.query.boxesF = boxF_.as<float>();
+                g.scratch.desc = desc + static_cast<size_t>(H) * tileCap_;
+                g.scratch.ticket = tickets + H;
+                g.scratch.status = status;
+                g.D = D;
+                g.useFma = 1;
+                g.variant = kVariantDirect;
+                g.gridPercent = 100;
+                g.fout = outView(1 - buf, hdrPtr(H + 3));
+                launchExpand(g, kPredGroupBox, false, 0, stream_);
+                buf = 1 - buf;
+                a.in = inView(buf, hdrPtr(H + 3));
+            }
             a.child.outMap = di_.mapPtr[H - 1];
             int finestPred = (mode == kModeExact) ? kPredRangeBox : kPredAll;
-            if (mode == kModeExact && floatPoints_ && di_.pointsF.bytes() && floatPointsSupported(di_.D) &&
-                variants_[m] != kVariantStaged) {
+            if (floatPath) {
                 a.child.rowsF = di_.pointsF.as<float>();
+                a.child.perm = di_.pointPerm.as<uint32_t>();
                 a.query.boxesFi = boxFi;
                 finestPred = kPredRangeBoxF;
             }
@@ -539,6 +575,20 @@ void BatchEngine::enqueueLaunches(const double* dBoxes, uint32_t nq, int mode, u
     if (timing_) record(2 + H);
 }
 
+std::vector<uint64_t> BatchEngine::groupCounts() {
+    std::vector<uint64_t> out(3, 0);
+    if (lastKnn_ || !groupsThisBatch_ || !zeroBlock_.bytes()) return out;
+    const int H = static_cast<int>(di_.height);
+    uint32_t a[2] = {0, 0}, b[2] = {0, 0};
+    TBLAEQ_CUDA(cudaMemcpyAsync(a, hdrPtr(H - 1), 8, cudaMemcpyDeviceToHost, stream_));
+    TBLAEQ_CUDA(cudaMemcpyAsync(b, hdrPtr(H + 3), 8, cudaMemcpyDeviceToHost, stream_));
+    TBLAEQ_CUDA(cudaStreamSynchronize(stream_));
+    out[0] = a[1];
+    out[1] = b[0];
+    out[2] = b[1];
+    return out;
+}
+
 uint32_t BatchEngine::status() {
     uint32_t st = 0;
     TBLAEQ_CUDA(cudaMemcpyAsync(&st, zeroBlock_.as<char>() + offStatus_, 4, cudaMemcpyDeviceToHost, stream_));
@@ -558,12 +608,13 @@ void BatchEngine::checkSplitLimit() {
 
 void BatchEngine::growFromHeaders() {
     const int H = static_cast<int>(di_.height);
-    std::vector<uint32_t> h((H + 2) * 2);
+    std::vector<uint32_t> h((H + 4) * 2);
     TBLAEQ_CUDA(cudaMemcpyAsync(h.data(), hdrPtr(0), h.size() * 4, cudaMemcpyDeviceToHost, stream_));
     TBLAEQ_CUDA(cudaStreamSynchronize(stream_));
     EngineCaps want = caps_;
     bool grew = false;
-    for (int lv = 1; lv < H; ++lv) {
+    for (int lv = 1; lv <= H + 3; ++lv) {
+        if (lv >= H && lv < H + 3) continue;  // result and KNN slots: below
         const uint64_t cnt = h[2 * lv], items = h[2 * lv + 1];
         if (cnt > splitLimit_ || items > splitLimit_)
             throw SplitBatch("level " + std::to_string(lv) + " exceeds the traversal limit; split the batch");

@@ -90,6 +90,14 @@ public:
         if (on != floatPoints_) dropGraph();
         floatPoints_ = on;
     }
+    // Finest exact range level with float points: test the clusters' point groups first (default
+    // on; same results). groupCounts: of the last range batch, the groups tested, the (query,
+    // group) pairs kept and the points tested, or zeros when it tested no groups.
+    void setPointGroups(bool on) {
+        if (on != pointGroups_) dropGraph();
+        pointGroups_ = on;
+    }
+    std::vector<uint64_t> groupCounts();
     bool twoWave() const { return twoWave_; }
     // Optional device scorer of the last frontier's entries (higher = expand earlier); when unset
     // the entries are ranked by their lower bound. Called with (frontier, hdr, cap, points, out scores).
@@ -176,6 +184,9 @@ private:
     // results before they are grouped by query.
     bool nodeMajor_ = true;
     bool floatPoints_ = true;
+    bool pointGroups_ = true;
+    bool groupsThisBatch_ = false;
+    const NodeRec* innerRecords(int m) const;
     DeviceMem nmNodeOff_, nmUnitOff_, nmList_, rawIds_, rawQ_, rawVals_;
     uint64_t nmEntryCap_ = 0, nmResultCap_ = 0;
     bool nmVals_ = false;

@@ -150,15 +150,20 @@ template <int D, int DM, typename Sink>
 __device__ __forceinline__ void rebuildChunks(const ExpandArgs& a, int dim, uint32_t e, uint32_t j, Sink&& sink) {
     constexpr int C = chunkOf<D>();
     const double* xp = a.in.x + static_cast<size_t>(e) * dim;
-    const double* rp = a.child.rows + static_cast<size_t>(j) * dim;
+    const double* rp = a.child.rows ? a.child.rows + static_cast<size_t>(j) * dim : nullptr;
 #pragma unroll
     for (int d = 0; d < DM; d += C) {
         if (D > 0 || d < dim) {
             double r[C], x[C], y[C];
-            ldChunk<C, false>(rp + d, r);
             ldChunk<C, false>(xp + d, x);
+            if (rp) {  // warp-uniform; no rows: the child takes its parent's coordinates (point groups)
+                ldChunk<C, false>(rp + d, r);
 #pragma unroll
-            for (int i = 0; i < C; ++i) y[i] = __dmul_rn(r[i], x[i]);
+                for (int i = 0; i < C; ++i) y[i] = __dmul_rn(r[i], x[i]);
+            } else {
+#pragma unroll
+                for (int i = 0; i < C; ++i) y[i] = x[i];
+            }
             sink(d, y);
         }
     }
@@ -304,7 +309,8 @@ __device__ __forceinline__ void prefetchTileRows(const ExpandArgs& a, uint32_t t
 
 template <int PRED, bool TO_RESULT>
 constexpr bool needsNode() {
-    return PRED == kPredRangeRadius || PRED == kPredKnnBound || (!TO_RESULT && (PRED == kPredMask || PRED == kPredAll));
+    return PRED == kPredRangeRadius || PRED == kPredKnnBound || PRED == kPredGroupBox ||
+           (!TO_RESULT && (PRED == kPredMask || PRED == kPredAll));
 }
 
 // Exact-mode prefilter of range levels: whether the query box meets the box of the points below
@@ -349,6 +355,9 @@ __device__ __forceinline__ bool evalItem(const ExpandArgs& a, int dim, const dou
             keep = keep && cc > 0;
         }
         return keep;
+    } else if constexpr (PRED == kPredGroupBox) {
+        cc = nr.cnt;
+        return cc > 0 && aabbMeets<D, DM>(a, dim, kk, q);
     } else if constexpr (PRED == kPredAll) {
         if constexpr (!TO_RESULT) {
             cc = nr.cnt;
@@ -516,7 +525,8 @@ __device__ __noinline__ bool exactPointInBoxRow(const double* r, const double* x
 }
 template <int D>
 __device__ __forceinline__ bool exactPointInBox(const ExpandArgs& a, uint32_t j, uint32_t e, uint32_t q) {
-    return exactPointInBoxRow<D>(a.child.rows + static_cast<size_t>(j) * D, a.in.x + static_cast<size_t>(e) * D,
+    const uint32_t jr = a.child.perm ? __ldg(a.child.perm + j) : j;
+    return exactPointInBoxRow<D>(a.child.rows + static_cast<size_t>(jr) * D, a.in.x + static_cast<size_t>(e) * D,
                                  a.query.boxes + static_cast<size_t>(q) * 2 * D);
 }
 
@@ -1008,7 +1018,9 @@ __global__ void __launch_bounds__(kExpandThreads, expandMinBlocks<PRED>()) expan
                 const unsigned long long pos = runCnt + __popc(kb & lanesLt);
                 if constexpr (TO_RESULT) {
                     if (pos < a.rout.cap) {
-                        a.rout.ids[pos] = a.child.outMap ? a.child.outMap[j] : static_cast<uint64_t>(kk);
+                        // Float points in point-group order: the row's place in the P tensor.
+                        const uint32_t jr = (PRED == kPredRangeBoxF && a.child.perm) ? a.child.perm[j] : j;
+                        a.rout.ids[pos] = a.child.outMap ? a.child.outMap[jr] : static_cast<uint64_t>(kk);
                         if (a.rout.q) a.rout.q[pos] = qr;
                         double* vals = a.rout.vals ? a.rout.vals + pos * dim : nullptr;
                         if constexpr (PRED == kPredKnnPoint) {
@@ -1030,7 +1042,7 @@ __global__ void __launch_bounds__(kExpandThreads, expandMinBlocks<PRED>()) expan
                             }
                         } else if (vals) {
                             constexpr int C = chunkOf<D>();
-                            rebuildChunks<D, DM>(a, dim, er, j,
+                            rebuildChunks<D, DM>(a, dim, er, jr,
                                                  [&](int d, const double (&y)[C]) { stChunk<C>(vals + d, y); });
                         }
                     }
@@ -1161,6 +1173,7 @@ void dispatchPred(const ExpandArgs& a, int pred, bool toResult, int g, cudaStrea
             case kPredRangeRadius: return launchOne<D, kPredRangeRadius, false, ST>(a, g, s);
             case kPredMask: return launchOne<D, kPredMask, false, ST>(a, g, s);
             case kPredAll: return launchOne<D, kPredAll, false, ST>(a, g, s);
+            case kPredGroupBox: return launchOne<D, kPredGroupBox, false, false>(a, g, s);
             case kPredKnnBound: return launchOne<D, kPredKnnBound, false, ST>(a, g, s);
             default: break;
         }

@@ -100,6 +100,9 @@ struct ChildLevel {
     // is decided from these 4·D bytes unless a coordinate lies within float rounding of a face,
     // where the FP64 test on the row decides.
     const float* rowsF;
+    // Optional with rowsF: rowsF is in point-group order, and its row j is row perm[j] of `rows` and
+    // of outMap (the FP64 test, the output id and the written coordinates use perm[j]).
+    const uint32_t* perm;
     int rowsOnHost;             // rows (and possibly outMap) are mapped host memory: plain loads only
 };
 
@@ -130,6 +133,8 @@ enum Pred : int {
     kPredKnnPoint = 5,          // keep point if dist2 <= tau^2 (records dist2)
     kPredRangeBoxF = 6,         // kPredRangeBox decided from the points' float copies (child.rowsF,
                                 // query.boxesFi), with the FP64 test only near a face: same keeps
+    kPredGroupBox = 7,          // keep point group if its float box meets the query's (frontier
+                                // output; child.rows null: the entry's coordinates pass through)
 };
 
 // Kernel variants an autotuner chooses between per level: rows loaded straight into registers,

@@ -350,3 +350,48 @@ def test_float_points_decide_exactly_at_box_faces(tb, oracle_mod, tmp_path, cuda
         h.set_float_points(True)
     sizes = np.diff(b.offsets.astype(np.int64))
     assert np.all(sizes[:2 * g] >= 1) and np.all(sizes[2 * g:4 * g] >= 0)
+
+
+@pytest.mark.parametrize("D,ratios", [(4, (100, 20, 10)), (8, (100, 50, 20)), (16, (40, 40, 10))])
+def test_point_groups_keep_results(tb, oracle_mod, tmp_path, cuda, D, ratios):
+    """Testing the finest clusters' point groups (at most 32 points, with their boxes) before their
+    points changes which points are tested, never the results: ids equal the FP64 brute force with
+    groups on and off, entry-major and node-major, and so do the coordinates (WANT_VALS: every id
+    keeps its own point). Far fewer points are tested with the groups."""
+    h = tb.QueryHandler.generate(60000 if D != 8 else 200000, D, 1.0, 100.0, False, 4, ratios, 15 + D, 3.0)
+    h.prepare_for_query(tb.LevelPolicy.L0)
+    o = oracle_from_handler(oracle_mod, h, tmp_path)
+    pts, ids = oracle_mod.decoded_points(o)
+    Q = _boxes(pts, 300, 60 + D, 0.005, 0.2)
+    b = oracle_mod.brute_query(pts, ids, oracle_mod.RANGE, Q)
+    rows = {int(i): k for k, i in enumerate(ids)}
+    H = h.info()["height"]
+    tested = {}
+    try:
+        for groups in (True, False):
+            h.set_point_groups(groups)
+            for shapes in ([0] * H, [0, 2, 2, 0][:H]):
+                h.set_launch_shapes(shapes, [100] * H)
+                r = h.query_batch(tb.QueryType.RANGE, Q, tb.Mode.EXACT, flags=tb.WANT_VALS)
+                offs, got, vals = r.offsets.numpy(), r.ids.numpy(), r.vals.numpy()
+                assert np.array_equal(offs, b.offsets), (groups, shapes)
+                assert all(np.array_equal(g, b.query(q)) for q, g in enumerate(ids_by_query(offs, got))), (groups, shapes)
+                assert np.array_equal(vals, pts[[rows[int(i)] for i in got]]), (groups, shapes)
+                c = h.group_counts()
+                if groups:
+                    assert 0 < c["kept"] <= c["groups"] and c["points"] > 0
+                    tested[groups] = c["points"]
+                else:
+                    assert c == {"groups": 0, "kept": 0, "points": 0}
+                    tested[groups] = h.level_counts()[1][H - 1]
+        # Per-level counts are the points of the surviving clusters: the batch tests every point.
+        h.set_point_groups(True)
+        h.set_launch_shapes([0] * H, [100] * H)
+        r = h.query_batch(tb.QueryType.RANGE, Q, tb.Mode.EXACT, flags=tb.WANT_LEVELS)
+        assert h.group_counts()["groups"] == 0
+        ref = oracle_mod.exact_query(o, oracle_mod.RANGE, Q)
+        assert np.array_equal(r.offsets.numpy(), ref.offsets)
+    finally:
+        h.set_point_groups(True)
+        h.set_launch_shapes([0] * H, [100] * H)
+    assert tested[True] < tested[False]
