@@ -146,17 +146,17 @@ def job_throughput(units_per_rank: float, world: int, seconds_max: float) -> flo
     return units_per_rank * world / seconds_max
 
 
-def profiled_traffic(cfg_name, nq, float_points):
-    """DRAM bytes (read + write) of one finest-level expand launch of this exact workload, from the
-    committed ncu summary (one capture of the same command; ncu is never run by the benchmark)."""
+def profiled_traffic(cfg_name, nq, level, height):
+    """DRAM bytes (read + write) of one launch of `level` at this exact workload, from the committed
+    ncu summary (`traffic_bytes_per_launch_level<m>:` lines; one capture of the same command; ncu
+    is never run by the benchmark)."""
     if cfg_name != "batched" or nq != 4096:
         return None
     path = os.path.join(REPO, "profiles", "expand_batched_range_n10m_d8.md")
     if not os.path.exists(path):
         return None
     import re
-    key = "traffic_bytes_per_launch_finest_float" if float_points else "traffic_bytes_per_launch_finest"
-    m = re.search(r"^" + key + r":\s*(\d+)", open(path).read(), re.M)
+    m = re.search(r"^traffic_bytes_per_launch_level" + str(level) + r":\s*(\d+)", open(path).read(), re.M)
     return int(m.group(1)) if m else None
 
 
@@ -411,7 +411,8 @@ def main():
         h.batch_wait()
 
     entries, items, results = h.level_counts()
-    step_ms, final_ms = [], []
+    groups = h.group_counts()
+    step_ms, final_ms, stage_rows = [], [], []
     if world > 1:
         dist.barrier()
     torch.cuda.synchronize()
@@ -425,6 +426,7 @@ def main():
             st = h.stage_times()
             step_ms.append(sum(st))
             final_ms.append(st[-2])
+            stage_rows.append(st)
     torch.cuda.synchronize()
     torch.cuda.nvtx.range_pop()
     if world > 1:
@@ -432,15 +434,34 @@ def main():
     total_ms = max_over_ranks(sum(step_ms))
     value = job_throughput(args.nq * args.steps, world, total_ms / 1e3)
 
-    # Roofline of the finest-level expand (dominant kernel): algorithmic bytes per launch.
+    # Roofline of the dominant level (largest event time): its algorithmic bytes per launch.
     H = len(entries)
-    ent_in, kids = entries[H - 1], items[H - 1]
-    # Per entry: query slot, first row, prefix and the parent's coordinates; per child: its point
-    # (float copy or FP64 row); per result: id and query slot.
-    alg_bytes = ent_in * (12 + 8 * D) + kids * (4 if float_points else 8) * D + results * 16
-    final_mean_s = statistics.mean(final_ms) / 1e3
+
+    def level_bytes(m):
+        """Bytes level m must move: per input entry its query slot, first child, prefix and
+        coordinates (12 + 8·D); per tested child its P row and node record (8·D + 16), or at the
+        finest level its point (float copy 4·D, FP64 row 8·D); per surviving entry the same entry
+        fields written; per result its id and query slot (16). With point groups the finest level
+        reads, per (query, cluster) entry, its groups' boxes and records (8·D + 16 each), and per
+        kept (query, group) pair the points of the group."""
+        if m < H - 1:
+            return entries[m] * (12 + 8 * D) + items[m] * (8 * D + 16) + entries[m + 1] * (12 + 8 * D)
+        if groups["groups"]:
+            return (entries[m] * (12 + 8 * D) + groups["groups"] * (8 * D + 16) + groups["kept"] * 2 * (12 + 8 * D)
+                    + groups["points"] * 4 * D + results * 16)
+        return entries[m] * (12 + 8 * D) + items[m] * (4 if float_points else 8) * D + results * 16
+
+    level_ms = [statistics.mean(r[1 + m] for r in stage_rows) for m in range(H)]
+    dom = max(range(H), key=lambda m: level_ms[m])
+    alg_bytes = level_bytes(dom)
+    final_mean_s = level_ms[dom] / 1e3
     peak, peak_kind = _peaks()
     achieved = alg_bytes / final_mean_s / 1e9
+    per_level = [{"level": m, "ms": level_ms[m], "algorithmic_bytes": level_bytes(m),
+                  "GB/s": level_bytes(m) / (level_ms[m] / 1e3) / 1e9} for m in range(H)]
+    dom_kind = (["direct", "staged", "node-major"][variants[dom]] if dom < len(variants) else "direct")
+    dom_name = ("finest level: point groups + float points" if dom == H - 1 and groups["groups"]
+                else "finest level" if dom == H - 1 else f"level {dom} (mesh {dom - 1} -> mesh {dom}), {dom_kind}")
 
     # Plain: one query at a time through the same engine (no batching, no graph).
     plain_lat = []
@@ -583,10 +604,10 @@ def main():
         "roofline": {"bound": "host link" if finest_streamed else "hbm", "achieved": achieved,
                      "peak": None if finest_streamed else peak, "unit": "GB/s",
                      "frac": None if finest_streamed else achieved / peak,
-                     "traffic": None if finest_streamed else profiled_traffic(cfg_name, args.nq, float_points),
-                     "kernel": "expandKernel<8, RangeBox, result> (finest level)",
+                     "traffic": None if finest_streamed else profiled_traffic(cfg_name, args.nq, dom, H),
+                     "kernel": dom_name,
                      "peak_kind": f"{peak_kind} hbm_gbs", "algorithmic_bytes_per_launch": alg_bytes,
-                     "launch_ms": final_mean_s * 1e3},
+                     "launch_ms": final_mean_s * 1e3, "per_level": per_level, "point_groups": groups},
         "clocks": clk.summary(),
         "cpu_baseline": cpu,
         "cpu_traversal_port": port,
@@ -598,7 +619,7 @@ def main():
             "workload": "N=10M, D=8 (one index): 4096 range boxes and 4096 KNN points",
             "range_batched_vs_plain": value / world / plain_qps,
             "knn_batched_learned_vs_plain": knn["plain"]["speedup_batched_learned_vs_plain"],
-            "finest_level_hbm_frac": None if finest_streamed else achieved / peak,
+            "dominant_level_hbm_frac": None if finest_streamed else achieved / peak,
             "needs": ">= 5x batched+learned vs plain, >= 0.60 of HBM in pruning/SpTSpM"}
     print(json.dumps(out))
 

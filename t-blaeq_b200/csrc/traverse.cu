@@ -226,7 +226,7 @@ constexpr int warpSmemBytes() {
 #endif
 // The finest exact range level with float points (kPredRangeBoxF).
 #ifndef TBLAEQ_UNROLL_FLOAT_TEST
-#define TBLAEQ_UNROLL_FLOAT_TEST 8
+#define TBLAEQ_UNROLL_FLOAT_TEST 2
 #endif
 constexpr int kExpandThreads = TBLAEQ_EXPAND_THREADS;
 
