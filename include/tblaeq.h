@@ -278,6 +278,9 @@ int tblaeq_set_knn_wave1(tblaeq_handle* h, double scale);
 int tblaeq_set_knn_chunk(tblaeq_handle* h, uint64_t max_queries);
 /* The last KNN batch: out2[0] = queries per traversal, out2[1] = traversals. */
 int tblaeq_knn_batch_info(tblaeq_handle* h, uint64_t* out2);
+/* Why a KNN batch of this handle was last split: the traversal size that did not fit and the
+ * error it met (empty if none was split), NUL-terminated into buf (cap bytes). */
+int tblaeq_knn_split_reason(tblaeq_handle* h, char* buf, uint64_t cap);
 
 /* Counters of the last KNN batch (summed over its chunks when it ran in several): [0] final-frontier
  * clusters, [1] wave-1 candidates,

@@ -156,6 +156,7 @@ def _load():
         "tblaeq_group_counts": ([vp, P(ctypes.c_uint64)], ctypes.c_int),
         "tblaeq_set_knn_chunk": ([vp, ctypes.c_uint64], ctypes.c_int),
         "tblaeq_set_knn_wave1": ([vp, ctypes.c_double], ctypes.c_int),
+        "tblaeq_knn_split_reason": ([vp, ctypes.c_char_p, ctypes.c_uint64], ctypes.c_int),
         "tblaeq_knn_batch_info": ([vp, P(ctypes.c_uint64)], ctypes.c_int),
         "tblaeq_set_knn_probe": ([vp, ctypes.c_uint32, ctypes.c_int], ctypes.c_int),
         "tblaeq_set_launch_shapes": ([vp, P(ctypes.c_int), P(ctypes.c_int), ctypes.c_uint64], ctypes.c_int),
@@ -616,7 +617,9 @@ class QueryHandler:
         """The last KNN batch: queries per traversal and traversals."""
         out = (ctypes.c_uint64 * 2)()
         _check(_load().tblaeq_knn_batch_info(self._h, out))
-        return {"chunk": out[0], "traversals": out[1]}
+        buf = ctypes.create_string_buffer(512)
+        _check(_load().tblaeq_knn_split_reason(self._h, buf, 512))
+        return {"chunk": out[0], "traversals": out[1], "split_reason": buf.value.decode()}
 
     def knn_counters(self) -> dict:
         out = (ctypes.c_uint64 * 5)()

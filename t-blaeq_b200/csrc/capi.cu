@@ -26,6 +26,7 @@ struct tblaeq_handle {
     uint64_t knnChunkHint = 0;                  // queries per traversal that last fitted after a split (0: none)
     uint64_t knnChunkMax = 0;                   // caller's limit on queries per traversal (0: automatic)
     uint64_t lastKnnChunk = 0, lastKnnRuns = 0; // the last KNN batch: queries per traversal, traversals
+    std::string knnSplitReason;                 // why the last split KNN batch was split
     uint64_t lastNq = 0;                        // last asynchronously enqueued batch
     unsigned lastFlags = 0;
 };
@@ -246,6 +247,7 @@ static BatchOutput runKnnChunked(tblaeq_handle* h, const double* dQueries, uint6
             // Too large for the 32-bit traversal space or for the free device memory (the engine
             // released its workspace on the way out): halve the chunk.
             if (e.code != cudaErrorMemoryAllocation || c == 1) throw;
+            h->knnSplitReason = std::to_string(c) + " queries: " + e.what();
             chunk = (c + 1) / 2;
             continue;
         }
@@ -311,6 +313,7 @@ static int runBatch(tblaeq_handle* h, const tblaeq_batch* b, const double* dQuer
                 h->lastKnnRuns = 1;
             } catch (const CudaError& e) {
                 if (e.code != cudaErrorMemoryAllocation || b->nq < 2) throw;
+                h->knnSplitReason = std::to_string(b->nq) + " queries: " + e.what();
                 o = runKnnChunked(h, dQueries, b->nq, k, b->flags, (b->nq + 1) / 2);
             }
         }
@@ -626,6 +629,15 @@ int tblaeq_set_knn_chunk(tblaeq_handle* h, uint64_t max_queries) {
     if (int c = checkPrepared(h)) return c;
     h->knnChunkMax = max_queries;
     if (max_queries == 0) h->knnChunkHint = 0;
+    return TBLAEQ_OK;
+}
+
+int tblaeq_knn_split_reason(tblaeq_handle* h, char* buf, uint64_t cap) {
+    if (int c = checkPrepared(h)) return c;
+    if (!buf || cap == 0) return fail(TBLAEQ_ERR_INVALID, "null output");
+    const size_t n = std::min<size_t>(cap - 1, h->knnSplitReason.size());
+    std::memcpy(buf, h->knnSplitReason.data(), n);
+    buf[n] = '\0';
     return TBLAEQ_OK;
 }
 

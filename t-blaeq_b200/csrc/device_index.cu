@@ -324,6 +324,7 @@ DerivedArrays computeDerived(const HostIndex& idx) {
             out.leaf[m][s] = static_cast<uint32_t>(C[m][s]);
         }
     }
+    out.pointsD = std::move(dec[H - 1]);
     return out;
 }
 
@@ -429,6 +430,10 @@ std::unique_ptr<DeviceIndex> buildDeviceIndex(const HostIndex& idx, const Derive
         di->nodeX[m] = upload(der.nodeX[m], s);
         TBLAEQ_CUDA(cudaStreamSynchronize(s));
     }
+    if (!der.pointsD.empty() && idx.intervals > 0 && res(idx.intervals - 1) == kResident) {
+        di->pointsD = upload(der.pointsD, s);
+        TBLAEQ_CUDA(cudaStreamSynchronize(s));
+    }
     if (!der.pointsF.empty() && idx.intervals > 0 && res(idx.intervals - 1) == kResident) {
         di->pointsF = upload(der.pointsF, s);
         di->pointPerm = upload(der.pointPerm, s);
@@ -451,7 +456,7 @@ size_t DeviceIndex::deviceBytes() const {
     size_t t = coarseVals.bytes() + coarseIds.bytes();
     for (auto* v : {&pvals, &nodeRef, &nodeSub, &leaf, &aabb, &nodeX, &nodeOrig, &maps})
         for (auto& m : *v) t += m.bytes();
-    return t + pointsF.bytes() + pointPerm.bytes() + groupRec.bytes() + groupBox.bytes() + clusterGroups.bytes();
+    return t + pointsD.bytes() + pointsF.bytes() + pointPerm.bytes() + groupRec.bytes() + groupBox.bytes() + clusterGroups.bytes();
 }
 
 }  // namespace tblaeq

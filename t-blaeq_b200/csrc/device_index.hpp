@@ -93,6 +93,8 @@ struct DerivedArrays {
     std::vector<uint32_t> groupCount;    // per group: its rows
     std::vector<float> groupBox;         // per group: lo[D] hi[D] of its points, rounded outward
     std::vector<uint32_t> clusterGroup;  // per finest cluster (mesh H-2 position): first group; one more at the end
+    // Decoded finest points in row order (y = P[j] * x_parent, one rounded multiply per dimension).
+    std::vector<double> pointsD;
 };
 
 // Most points of one point group.
@@ -152,6 +154,9 @@ struct DeviceIndex {
     // group's record {0, first row, rows} and box, and every finest cluster's record
     // {subtree radius, first group, groups}.
     DeviceMem pointsF, pointPerm, groupRec, groupBox, clusterGroups;
+    // Decoded finest points (DerivedArrays::pointsD) for the KNN point kernels, when the last
+    // interval's rows are device-resident; else empty.
+    DeviceMem pointsD;
 
     // original-id space (per-level plugin)
     DeviceMem coarseIds;                     // uint64

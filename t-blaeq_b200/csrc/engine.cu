@@ -1039,6 +1039,7 @@ void BatchEngine::enqueueKnn(const double* dPoints, uint32_t nq, const uint32_t*
         c.x = di_.nodeX[H - 2].as<double>();
         c.rows = di_.rows[H - 2];
         c.rowsOnHost = di_.rowsOnHost[H - 2];
+        c.decoded = di_.pointsD.bytes() ? di_.pointsD.as<double>() : nullptr;
         c.map = di_.mapPtr[H - 1];
         c.points = dPoints;
         c.tau = tau;

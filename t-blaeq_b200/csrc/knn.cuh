@@ -143,6 +143,7 @@ struct KnnClusterArgs {
     const double* x;
     const double* rows;
     int rowsOnHost;
+    const double* decoded;  // optional: the decoded finest points by row (else rebuilt from rows and x)
     const uint64_t* map;
     const double* points;
     const double* tau;

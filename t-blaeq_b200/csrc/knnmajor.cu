@@ -147,32 +147,15 @@ __global__ void __launch_bounds__(kThreadsNm) knnClusterPointsKernel(KnnClusterA
         const uint32_t am = __ballot_sync(FULL, active);
         if (am == 0) continue;
         if (lane == 0) rows += static_cast<unsigned long long>(__popc(am)) * cr.cnt;
-        double p[DM], xc[DM];
+        double p[DM];
 #pragma unroll
-        for (int d = 0; d < DM; ++d) {
-            if (D > 0 || d < dim) {
-                p[d] = active ? __ldg(a.points + static_cast<size_t>(q) * dim + d) : 0.0;
-                xc[d] = __ldg(a.x + static_cast<size_t>(un.node) * dim + d);
-            }
-        }
+        for (int d = 0; d < DM; ++d)
+            if (D > 0 || d < dim) p[d] = active ? __ldg(a.points + static_cast<size_t>(q) * dim + d) : 0.0;
         const double t = active ? __ldcg(a.tau + q) : 0.0;
         const double t2 = t * t * (1.0 + 1e-9);
-        for (uint32_t c = 0; c < cr.cnt; ++c) {
-            const uint32_t j = cr.cbeg + c;
-            const double* row = a.rows + static_cast<size_t>(j) * dim;
-            // The expand kernel's point test (kPredKnnPoint): the point rebuilt with one rounded
-            // multiply per dimension, the squared distance accumulated with fma in dimension order.
-            double dist = 0.0;
-#pragma unroll
-            for (int d = 0; d < DM; ++d) {
-                if (D > 0 || d < dim) {
-                    const double r = a.rowsOnHost ? row[d] : __ldg(row + d);
-                    const double diff = p[d] - __dmul_rn(r, xc[d]);
-                    dist = __fma_rn(diff, diff, dist);
-                }
-            }
-            const bool keep = active && dist <= t2;
-            if (__ballot_sync(FULL, keep) == 0) continue;
+        // Appends the candidate (query q, row j) when kept.
+        auto emit = [&](bool keep, uint32_t j, double dist) {
+            if (__ballot_sync(FULL, keep) == 0) return;
             const uint32_t pos = appendPos(keep, a.outCount, a.status, lane);
             if (keep) {
                 atomicAdd(&a.qcount[q], 1u);
@@ -183,6 +166,50 @@ __global__ void __launch_bounds__(kThreadsNm) knnClusterPointsKernel(KnnClusterA
                 } else {
                     atomicOr(a.status, kStatusOverflowEntries);
                 }
+            }
+        };
+        if (a.decoded) {
+            // The decoded points (the products below, made once when the index was prepared), four
+            // at a time: four independent fma chains per lane instead of one. A group past the
+            // cluster's end repeats its last point, which is never emitted twice.
+            const double* yb = a.decoded + static_cast<size_t>(cr.cbeg) * dim;
+            for (uint32_t c0 = 0; c0 < cr.cnt; c0 += 4) {
+                const uint32_t nIn = min(4u, cr.cnt - c0);
+                double dist[4] = {0.0, 0.0, 0.0, 0.0};
+                const double* y4[4];
+#pragma unroll
+                for (int i = 0; i < 4; ++i) y4[i] = yb + static_cast<size_t>(c0 + min(static_cast<uint32_t>(i), nIn - 1)) * dim;
+#pragma unroll
+                for (int d = 0; d < DM; ++d) {
+                    if (D > 0 || d < dim) {
+#pragma unroll
+                        for (int i = 0; i < 4; ++i) {
+                            const double diff = p[d] - __ldg(y4[i] + d);
+                            dist[i] = __fma_rn(diff, diff, dist[i]);
+                        }
+                    }
+                }
+#pragma unroll
+                for (int i = 0; i < 4; ++i)
+                    if (static_cast<uint32_t>(i) < nIn) emit(active && dist[i] <= t2, cr.cbeg + c0 + i, dist[i]);
+            }
+        } else {
+            for (uint32_t c = 0; c < cr.cnt; ++c) {
+                const uint32_t j = cr.cbeg + c;
+                const double* row = a.rows + static_cast<size_t>(j) * dim;
+                const double* xc = a.x + static_cast<size_t>(un.node) * dim;
+                // The expand kernel's point test (kPredKnnPoint): the point rebuilt with one rounded
+                // multiply per dimension, the squared distance accumulated with fma in dimension order.
+                double dist = 0.0;
+#pragma unroll
+                for (int d = 0; d < DM; ++d) {
+                    if (D > 0 || d < dim) {
+                        const double r = a.rowsOnHost ? row[d] : __ldg(row + d);
+                        const double diff = p[d] - __dmul_rn(r, __ldg(xc + d));
+                        dist = __fma_rn(diff, diff, dist);
+                    }
+                }
+                emit(active && dist <= t2, j, dist);
             }
         }
     }
