@@ -320,6 +320,8 @@ def main():
     ap.add_argument("--knn-completion", type=int, choices=[0, 1], default=1,
                     help="KNN: 1 = node-major completion after wave 1, 0 = the query-major wave 2")
     ap.add_argument("--knn-chunk", type=int, default=0, help="KNN: queries per traversal (0 = automatic)")
+    ap.add_argument("--knn-refine", type=int, default=-1,
+                    help="KNN: stride of the bound-refinement sample (0 = off; -1 = the library's default)")
     ap.add_argument("--knn-wave1", type=float, default=0.0,
                     help="KNN: wave-1 scale (clusters = ceil(scale*K/leaf)+1, 2..32; 0 = the library's default)")
     ap.add_argument("--variants", default=None,
@@ -445,12 +447,20 @@ def main():
         reads, per (query, cluster) entry, its groups' boxes and records (8·D + 16 each), and per
         kept (query, group) pair the points of the group."""
         if m < H - 1:
+            if m < len(variants) and variants[m] == 2 and m > 0:
+                # Node-major: every unit (a node and up to 32 of its entries) reads the node's
+                # children once (float box 8·D, row 8·D, record 16), not once per entry.
+                per_node = items[m] / max(1, entries[m])
+                units = entries[m] / 32 + mesh_nodes[m - 1] / 2
+                return (entries[m] * (12 + 8 * D) + units * per_node * (16 * D + 16)
+                        + entries[m + 1] * (12 + 8 * D))
             return entries[m] * (12 + 8 * D) + items[m] * (8 * D + 16) + entries[m + 1] * (12 + 8 * D)
         if groups["groups"]:
             return (entries[m] * (12 + 8 * D) + groups["groups"] * (8 * D + 16) + groups["kept"] * 2 * (12 + 8 * D)
                     + groups["points"] * 4 * D + results * 16)
         return entries[m] * (12 + 8 * D) + items[m] * (4 if float_points else 8) * D + results * 16
 
+    mesh_nodes = h.info()["meshSizes"][::-1]  # coarsest mesh first
     level_ms = [statistics.mean(r[1 + m] for r in stage_rows) for m in range(H)]
     dom = max(range(H), key=lambda m: level_ms[m])
     alg_bytes = level_bytes(dom)
@@ -642,6 +652,9 @@ def knn_options(h, args, config):
     if args.knn_chunk:
         h.set_knn_chunk(args.knn_chunk)
         config["knn_chunk"] = args.knn_chunk
+    if args.knn_refine >= 0:
+        h.set_knn_refine(args.knn_refine)
+        config["knn_refine_stride"] = args.knn_refine
     if args.knn_wave1 > 0:
         h.set_knn_wave1(args.knn_wave1)
         config["knn_wave1_scale"] = args.knn_wave1

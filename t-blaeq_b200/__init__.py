@@ -156,6 +156,7 @@ def _load():
         "tblaeq_group_counts": ([vp, P(ctypes.c_uint64)], ctypes.c_int),
         "tblaeq_set_knn_chunk": ([vp, ctypes.c_uint64], ctypes.c_int),
         "tblaeq_set_knn_wave1": ([vp, ctypes.c_double], ctypes.c_int),
+        "tblaeq_set_knn_refine": ([vp, ctypes.c_uint32], ctypes.c_int),
         "tblaeq_knn_split_reason": ([vp, ctypes.c_char_p, ctypes.c_uint64], ctypes.c_int),
         "tblaeq_knn_batch_info": ([vp, P(ctypes.c_uint64)], ctypes.c_int),
         "tblaeq_set_knn_probe": ([vp, ctypes.c_uint32, ctypes.c_int], ctypes.c_int),
@@ -612,6 +613,11 @@ class QueryHandler:
         """Two-wave KNN: wave 1 reads each query's ceil(scale * K / leaf) + 1 best-ranked clusters
         (2..32); larger tightens the bound the rest of the batch prunes with. Same results."""
         _check(_load().tblaeq_set_knn_wave1(self._h, float(scale)))
+
+    def set_knn_refine(self, stride: int = 8):
+        """Node-major KNN completion: a pass over every stride-th point of the listed clusters first
+        tightens each query's bound (0 or 1: off). Same results."""
+        _check(_load().tblaeq_set_knn_refine(self._h, int(stride)))
 
     def knn_batch_info(self) -> dict:
         """The last KNN batch: queries per traversal and traversals."""

@@ -625,6 +625,12 @@ int tblaeq_set_knn_wave1(tblaeq_handle* h, double scale) {
     return TBLAEQ_OK;
 }
 
+int tblaeq_set_knn_refine(tblaeq_handle* h, uint32_t stride) {
+    if (int c = checkPrepared(h)) return c;
+    h->qh->runtime().engine->setKnnRefine(stride);
+    return TBLAEQ_OK;
+}
+
 int tblaeq_set_knn_chunk(tblaeq_handle* h, uint64_t max_queries) {
     if (int c = checkPrepared(h)) return c;
     h->knnChunkMax = max_queries;

@@ -36,7 +36,7 @@ void BatchEngine::resetWorkspace() noexcept {
                          &candD2_, &excl_, &probeK_, &resIds_, &resVals_, &resQ_, &resDist_, &zeroBlock_, &cmpCnt_,
                          &cmpKids_, &cmpEntryOff_, &cmpKidOff_, &offsets_, &boxF_, &tau_, &candOff_, &knnCount_,
                          &knnOff_, &knnIds_, &knnD2_, &lbE_, &scoreE_, &sel_, &offF_, &waveM_, &selCount_, &selOff_,
-                         &selIds_, &selD2_, &candOffB_, &resIdsB_, &resQB_, &resDistB_})
+                         &selIds_, &selD2_, &candOffB_, &candOffS_, &resIdsB_, &resQB_, &resDistB_})
         m->release();
     caps_ = EngineCaps{};
     qcap_ = 0;
@@ -300,7 +300,7 @@ void BatchEngine::reserve(const EngineCaps& want, uint32_t nq, unsigned flags) {
         // per-level query counts; per-node counts and cursors of meshes 0..H-2; the per-query
         // candidate cursors.
         offKnnTick_ = off;
-        off = align256(off + (2 * H + 2) * 4);
+        off = align256(off + (2 * H + 4) * 4);  // H+1 tickets, H pair counts, candidates, refine ticket and count
         offQcountP_ = off;
         off = align256(off + H * static_cast<size_t>(qcap_) * 4);
         offKnnNodeCnt_.assign(H, 0);
@@ -817,6 +817,7 @@ void BatchEngine::reserveKnn(uint32_t nq) {
         selIds_.alloc(knnQcap_ * 32ull * 8);
         selD2_.alloc(knnQcap_ * 32ull * 8);
         candOffB_.alloc((knnQcap_ + 1ull) * 8);
+        candOffS_.alloc((knnQcap_ + 1ull) * 8);
     }
     if (entryCap_ < caps_.entries) {
         entryCap_ = caps_.entries;
@@ -1055,6 +1056,36 @@ void BatchEngine::enqueueKnn(const double* dPoints, uint32_t nq, const uint32_t*
         c.ticket = tick + H;
         c.status = status;
         c.D = D;
+        if (refineStride_ > 1) {
+            // Refine the bound first: every refineStride_-th point of the listed clusters, whose K
+            // nearest (with wave 1's) are real points, so their K-th distance bounds tau; the pass
+            // below then skips every cluster whose sphere lies beyond it. The sample's candidates
+            // serve only the bound (the pass below tests those points again).
+            uint32_t* sTick = candCnt + 1;
+            uint32_t* sCnt = candCnt + 2;
+            uint32_t* qcS = qcountP;           // the probe's per-level counts are free again
+            uint32_t* curS = qcountP + qcap_;
+            TBLAEQ_CUDA(cudaMemsetAsync(qcountP, 0, 2 * static_cast<size_t>(qcap_) * 4, stream_));
+            KnnClusterArgs sc = c;
+            sc.sampleStride = refineStride_;
+            sc.outCount = sCnt;
+            sc.qcount = qcS;
+            sc.ticket = sTick;
+            launchKnnClusterPoints(sc, stream_);
+            launchExclusiveScan(qcS, candOffS_.as<uint64_t>(), nq, stream_);
+            launchGroupResults(candId_.as<uint64_t>(), candQ_.as<uint32_t>(), candD2_.as<double>(), sCnt,
+                               static_cast<uint32_t>(std::min<uint64_t>(candCap_, resCapB_)), 1,
+                               candOffS_.as<uint64_t>(), curS, resIdsB_.as<uint64_t>(), resDistB_.as<double>(),
+                               stream_);
+            launchClampCounts2(candOff_.as<uint64_t>(), candOffS_.as<uint64_t>(), dK, nq, knnCount_.as<uint32_t>(),
+                               stream_);
+            launchExclusiveScan(knnCount_.as<uint32_t>(), knnOff_.as<uint64_t>(), nq, stream_);
+            launchTopK(candOff_.as<uint64_t>(), resIds_.as<uint64_t>(), resDist_.as<double>(), caps_.results,
+                       candOffS_.as<uint64_t>(), resIdsB_.as<uint64_t>(), resDistB_.as<double>(), resCapB_, dK, nq,
+                       knnOff_.as<uint64_t>(), knnIds_.as<uint64_t>(), knnD2_.as<double>(), knnCount_.as<uint32_t>(),
+                       status, stream_);
+            launchTauFromTopK(knnOff_.as<uint64_t>(), knnD2_.as<double>(), dK, nq, tau, stream_);
+        }
         launchKnnClusterPoints(c, stream_);
         if (timing_) record(1 + H);
         launchExclusiveScan(qcountB, candOffB_.as<uint64_t>(), nq, stream_);
@@ -1135,8 +1166,8 @@ void BatchEngine::reserveKnnMajor(uint32_t nq) {
 
 bool BatchEngine::growKnnMajor() {
     const int H = static_cast<int>(di_.height);
-    std::vector<uint32_t> c(H + 1, 0);
-    TBLAEQ_CUDA(cudaMemcpyAsync(c.data(), zeroBlock_.as<char>() + offKnnTick_ + (H + 1) * 4, (H + 1) * 4,
+    std::vector<uint32_t> c(H + 3, 0);  // pair counts, candidates, refine ticket, refine candidates
+    TBLAEQ_CUDA(cudaMemcpyAsync(c.data(), zeroBlock_.as<char>() + offKnnTick_ + (H + 1) * 4, (H + 3) * 4,
                                 cudaMemcpyDeviceToHost, stream_));
     TBLAEQ_CUDA(cudaStreamSynchronize(stream_));
     bool grew = false;
@@ -1146,8 +1177,9 @@ bool BatchEngine::growKnnMajor() {
             grew = true;
         }
     }
-    if (c[H] > candCap_) {
-        candCap_ = static_cast<uint64_t>(c[H]) + c[H] / 4 + 4096;
+    const uint32_t cand = std::max(c[H], c[H + 2]);
+    if (cand > candCap_) {
+        candCap_ = static_cast<uint64_t>(cand) + cand / 4 + 4096;
         grew = true;
     }
     if (pairCap_ >= 0x80000000ull || candCap_ >= 0x80000000ull)

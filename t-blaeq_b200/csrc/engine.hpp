@@ -61,6 +61,10 @@ public:
     // Wave 1 of a two-wave KNN batch reads the ceil(scale * K / leaf) + 1 best-ranked clusters of
     // each query (2..32; leaf = points per finest cluster on average); default scale 1.
     void setWaveScale(double scale) { waveScale_ = scale > 0 ? scale : 1.0; }
+    // Node-major completion: before its point pass, a pass over every stride-th point of the listed
+    // clusters tightens each query's bound (0 or 1: off; default 8).
+    void setKnnRefine(uint32_t stride) { refineStride_ = stride; }
+    uint32_t knnRefine() const { return refineStride_; }
     double waveScale() const { return waveScale_; }
     // Exact KNN with the two-wave finest level: beam width of the probe (each query keeps its
     // probeBeam entries of smallest lower bound at every level above the clusters, so wave 1 ranks
@@ -236,6 +240,8 @@ private:
     bool capturing_ = false;
     bool twoWave_ = true;
     double waveScale_ = 1.0;
+    uint32_t refineStride_ = 8;
+    DeviceMem candOffS_;
     EntryScorer scorer_ = nullptr;
     void* scorerCtx_ = nullptr;
     std::vector<int> variants_;

@@ -144,6 +144,10 @@ struct KnnClusterArgs {
     const double* rows;
     int rowsOnHost;
     const double* decoded;  // optional: the decoded finest points by row (else rebuilt from rows and x)
+    // Test only every sampleStride-th point of each cluster (0 or 1: every point). Lanes whose
+    // cluster's lower bound (centre distance - subtree radius) already exceeds the query's bound
+    // skip the cluster either way.
+    uint32_t sampleStride;
     const uint64_t* map;
     const double* points;
     const double* tau;

@@ -146,13 +146,31 @@ __global__ void __launch_bounds__(kThreadsNm) knnClusterPointsKernel(KnnClusterA
         }
         const uint32_t am = __ballot_sync(FULL, active);
         if (am == 0) continue;
-        if (lane == 0) rows += static_cast<unsigned long long>(__popc(am)) * cr.cnt;
         double p[DM];
 #pragma unroll
         for (int d = 0; d < DM; ++d)
             if (D > 0 || d < dim) p[d] = active ? __ldg(a.points + static_cast<size_t>(q) * dim + d) : 0.0;
         const double t = active ? __ldcg(a.tau + q) : 0.0;
         const double t2 = t * t * (1.0 + 1e-9);
+        if (active) {
+            // The pair was listed under an earlier (looser) bound: skip it when the cluster's sphere
+            // lies beyond the current one (the slack keeps the test conservative).
+            const double* xc = a.x + static_cast<size_t>(un.node) * dim;
+            double dc = 0.0;
+#pragma unroll
+            for (int d = 0; d < DM; ++d) {
+                if (D > 0 || d < dim) {
+                    const double diff = p[d] - __ldg(xc + d);
+                    dc = __fma_rn(diff, diff, dc);
+                }
+            }
+            if ((sqrt(dc) - cr.rad) * (1.0 - 1e-9) > t + 1e-12) active = false;
+        }
+        const uint32_t live = __ballot_sync(FULL, active);
+        if (live == 0) continue;
+        const uint32_t stride = a.sampleStride > 1 ? a.sampleStride : 1u;
+        const uint32_t nPts = (cr.cnt + stride - 1) / stride;  // points this pass tests
+        if (lane == 0) rows += static_cast<unsigned long long>(__popc(live)) * nPts;
         // Appends the candidate (query q, row j) when kept.
         auto emit = [&](bool keep, uint32_t j, double dist) {
             if (__ballot_sync(FULL, keep) == 0) return;
@@ -173,12 +191,13 @@ __global__ void __launch_bounds__(kThreadsNm) knnClusterPointsKernel(KnnClusterA
             // at a time: four independent fma chains per lane instead of one. A group past the
             // cluster's end repeats its last point, which is never emitted twice.
             const double* yb = a.decoded + static_cast<size_t>(cr.cbeg) * dim;
-            for (uint32_t c0 = 0; c0 < cr.cnt; c0 += 4) {
-                const uint32_t nIn = min(4u, cr.cnt - c0);
+            for (uint32_t c0 = 0; c0 < nPts; c0 += 4) {
+                const uint32_t nIn = min(4u, nPts - c0);
                 double dist[4] = {0.0, 0.0, 0.0, 0.0};
                 const double* y4[4];
 #pragma unroll
-                for (int i = 0; i < 4; ++i) y4[i] = yb + static_cast<size_t>(c0 + min(static_cast<uint32_t>(i), nIn - 1)) * dim;
+                for (int i = 0; i < 4; ++i)
+                    y4[i] = yb + static_cast<size_t>((c0 + min(static_cast<uint32_t>(i), nIn - 1)) * stride) * dim;
 #pragma unroll
                 for (int d = 0; d < DM; ++d) {
                     if (D > 0 || d < dim) {
@@ -191,11 +210,11 @@ __global__ void __launch_bounds__(kThreadsNm) knnClusterPointsKernel(KnnClusterA
                 }
 #pragma unroll
                 for (int i = 0; i < 4; ++i)
-                    if (static_cast<uint32_t>(i) < nIn) emit(active && dist[i] <= t2, cr.cbeg + c0 + i, dist[i]);
+                    if (static_cast<uint32_t>(i) < nIn) emit(active && dist[i] <= t2, cr.cbeg + (c0 + i) * stride, dist[i]);
             }
         } else {
-            for (uint32_t c = 0; c < cr.cnt; ++c) {
-                const uint32_t j = cr.cbeg + c;
+            for (uint32_t c = 0; c < nPts; ++c) {
+                const uint32_t j = cr.cbeg + c * stride;
                 const double* row = a.rows + static_cast<size_t>(j) * dim;
                 const double* xc = a.x + static_cast<size_t>(un.node) * dim;
                 // The expand kernel's point test (kPredKnnPoint): the point rebuilt with one rounded

@@ -223,3 +223,24 @@ def test_wave_one_width_keeps_results(tb, env, oracle_mod, scale):
         assert np.array_equal(r.ids.numpy(), b.ids) and np.array_equal(r.dist2.numpy(), b.dist2)
     finally:
         h.set_knn_wave1(1.0)
+
+
+@pytest.mark.parametrize("stride", [0, 3, 8])
+def test_bound_refinement_keeps_results(tb, env, oracle_mod, stride):
+    """The completion's bound refinement (a pass over every stride-th point of the listed clusters
+    before the full point pass) changes the work, never the results."""
+    h, o, pts, ids = env
+    P = _points(pts, 250, 71)
+    Kq = np.where(np.arange(250) % 2 == 0, 5, 40).astype(np.uint32)
+    h.set_knn_refine(stride)
+    try:
+        r = h.query_batch(tb.QueryType.POINT, P, tb.Mode.EXACT, K=Kq)
+        offs, got, d2 = r.offsets.numpy(), r.ids.numpy(), r.dist2.numpy()
+        for kv in (5, 40):
+            sel = np.nonzero(Kq == kv)[0]
+            b = oracle_mod.brute_query(pts, ids, oracle_mod.KNN, P[sel], K=kv)
+            for j, q in enumerate(sel):
+                assert np.array_equal(got[offs[q]:offs[q + 1]], b.query(j)), (stride, q)
+                assert np.array_equal(d2[offs[q]:offs[q + 1]], b.dist2[b.offsets[j]:b.offsets[j + 1]]), (stride, q)
+    finally:
+        h.set_knn_refine(8)
