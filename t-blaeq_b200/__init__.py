@@ -614,7 +614,7 @@ class QueryHandler:
         (2..32); larger tightens the bound the rest of the batch prunes with. Same results."""
         _check(_load().tblaeq_set_knn_wave1(self._h, float(scale)))
 
-    def set_knn_refine(self, stride: int = 8):
+    def set_knn_refine(self, stride: int = 16):
         """Node-major KNN completion: a pass over every stride-th point of the listed clusters first
         tightens each query's bound (0 or 1: off). Same results."""
         _check(_load().tblaeq_set_knn_refine(self._h, int(stride)))

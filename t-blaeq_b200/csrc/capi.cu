@@ -24,6 +24,7 @@ struct tblaeq_handle {
     DeviceMem knnOff, knnIds, knnD2;            // results of KNN batches run in chunks
     std::vector<uint64_t> knnSum;               // counters summed over the last batch's chunks (empty: one run)
     uint64_t knnChunkHint = 0;                  // queries per traversal that last fitted after a split (0: none)
+    bool knnHintTwoWave = true;                 // the finest-level mode that size was learnt under
     uint64_t knnChunkMax = 0;                   // caller's limit on queries per traversal (0: automatic)
     uint64_t lastKnnChunk = 0, lastKnnRuns = 0; // the last KNN batch: queries per traversal, traversals
     std::string knnSplitReason;                 // why the last split KNN batch was split
@@ -270,6 +271,7 @@ static BatchOutput runKnnChunked(tblaeq_handle* h, const double* dQueries, uint6
     // Later batches start at the size that fitted instead of failing at the full size first (each
     // failure costs the growth steps and the workspace reset before the split).
     h->knnChunkHint = chunk;
+    h->knnHintTwoWave = rt.engine->twoWave();
     h->lastKnnChunk = chunk;
     h->lastKnnRuns = runs;
     TBLAEQ_CUDA(cudaMemcpyAsync(h->knnOff.get(), offs.data(), (nq + 1) * 8, cudaMemcpyHostToDevice, rt.stream));
@@ -302,8 +304,10 @@ static int runBatch(tblaeq_handle* h, const tblaeq_batch* b, const double* dQuer
         if (b->nq)
             TBLAEQ_CUDA(cudaMemcpyAsync(h->kStage.get(), k.data(), b->nq * 4, cudaMemcpyHostToDevice, rt.stream));
         h->knnSum.clear();
-        const uint64_t limit = (h->knnChunkMax && h->knnChunkHint) ? std::min(h->knnChunkMax, h->knnChunkHint)
-                                                                     : (h->knnChunkMax ? h->knnChunkMax : h->knnChunkHint);
+        // A size learnt under the other finest-level mode (one pass or two waves) does not apply.
+        const uint64_t hint = (h->knnHintTwoWave == rt.engine->twoWave()) ? h->knnChunkHint : 0;
+        const uint64_t limit = (h->knnChunkMax && hint) ? std::min(h->knnChunkMax, hint)
+                                                        : (h->knnChunkMax ? h->knnChunkMax : hint);
         if (limit && b->nq > limit) {
             o = runKnnChunked(h, dQueries, b->nq, k, b->flags, limit);
         } else {

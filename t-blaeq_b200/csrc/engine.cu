@@ -1203,7 +1203,10 @@ BatchOutput BatchEngine::runKnn(const double* dPoints, uint32_t nq, const uint32
         const uint32_t st = status();
         if (st & (kStatusLookbackTimeout | kStatusWindowOverflow))
             throw CudaError(cudaErrorLaunchTimeout, "traversal kernel reported status " + std::to_string(st));
-        if (st & kStatusOverflowSum)
+        // A count past the 32-bit space calls for a split only when nothing earlier overflowed: a
+        // capacity overflow upstream (wave 1's results, a pair list) leaves bounds unset, and the
+        // stages after it then see far more than the batch holds. Grow first; rerun; decide then.
+        if ((st & kStatusOverflowSum) && !(st & (kStatusOverflowEntries | kStatusOverflowItems)))
             throw SplitBatch("a level generates more than 2^32 items; split the batch");
         if (st == 0) {
             if (splitLimit_ < 0xffffffffull) checkSplitLimit();

@@ -62,7 +62,7 @@ public:
     // each query (2..32; leaf = points per finest cluster on average); default scale 1.
     void setWaveScale(double scale) { waveScale_ = scale > 0 ? scale : 1.0; }
     // Node-major completion: before its point pass, a pass over every stride-th point of the listed
-    // clusters tightens each query's bound (0 or 1: off; default 8).
+    // clusters tightens each query's bound (0 or 1: off; default 16).
     void setKnnRefine(uint32_t stride) { refineStride_ = stride; }
     uint32_t knnRefine() const { return refineStride_; }
     double waveScale() const { return waveScale_; }
@@ -240,7 +240,7 @@ private:
     bool capturing_ = false;
     bool twoWave_ = true;
     double waveScale_ = 1.0;
-    uint32_t refineStride_ = 8;
+    uint32_t refineStride_ = 16;
     DeviceMem candOffS_;
     EntryScorer scorer_ = nullptr;
     void* scorerCtx_ = nullptr;

@@ -243,4 +243,4 @@ def test_bound_refinement_keeps_results(tb, env, oracle_mod, stride):
                 assert np.array_equal(got[offs[q]:offs[q + 1]], b.query(j)), (stride, q)
                 assert np.array_equal(d2[offs[q]:offs[q + 1]], b.dist2[b.offsets[j]:b.offsets[j + 1]]), (stride, q)
     finally:
-        h.set_knn_refine(8)
+        h.set_knn_refine(16)
