@@ -411,7 +411,8 @@ int tblaeq_batch_wait(tblaeq_handle* h, tblaeq_batch_result* out) {
     return guarded([&]() -> int {
         Runtime& rt = h->qh->runtime();
         const uint32_t st = rt.engine->status();
-        if (st & (kStatusLookbackTimeout | kStatusWindowOverflow))
+        const uint32_t over = st & (kStatusOverflowEntries | kStatusOverflowItems | kStatusOverflowSum);
+        if ((st & (kStatusLookbackTimeout | kStatusWindowOverflow)) && !over)
             return fail(TBLAEQ_ERR_TIMEOUT, "traversal kernel reported status " + std::to_string(st));
         if (st) return fail(TBLAEQ_ERR_OVERFLOW, "workspace overflow; rerun with tblaeq_query_batch");
         if (out) {

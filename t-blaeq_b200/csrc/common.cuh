@@ -18,6 +18,9 @@ enum DeviceStatus : uint32_t {
     kStatusLookbackTimeout = 1u << 3,   // a decoupled look-back spin gave up
     kStatusWindowOverflow = 1u << 4,    // a tile spanned more frontier entries than it can stage
 };
+// After any of these the frontiers that follow are not to be read (a wrapped child prefix, a
+// look-back that gave up): the kernels of the rest of the batch return at once.
+constexpr uint32_t kStatusInconsistent = kStatusOverflowSum | kStatusLookbackTimeout | kStatusWindowOverflow;
 
 struct CudaError : std::runtime_error {
     cudaError_t code;

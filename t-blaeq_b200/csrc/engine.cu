@@ -682,7 +682,11 @@ BatchOutput BatchEngine::runRange(const double* dBoxes, uint32_t nq, int mode, u
         TBLAEQ_CUDA(cudaMemcpyAsync(&st, zeroBlock_.as<char>() + offStatus_, 4, cudaMemcpyDeviceToHost, stream_));
         TBLAEQ_CUDA(cudaMemcpyAsync(&total, offsets_.as<uint64_t>() + nq, 8, cudaMemcpyDeviceToHost, stream_));
         TBLAEQ_CUDA(cudaStreamSynchronize(stream_));
-        if (st & (kStatusLookbackTimeout | kStatusWindowOverflow)) {
+        // A 32-bit prefix overflow leaves the next frontier's item mapping meaningless, so the
+        // launches after it may report window overflows and look-back timeouts of their own: those
+        // count as failures only when no overflow explains them.
+        const uint32_t over = st & (kStatusOverflowEntries | kStatusOverflowItems | kStatusOverflowSum);
+        if ((st & (kStatusLookbackTimeout | kStatusWindowOverflow)) && !over) {
             throw CudaError(cudaErrorLaunchTimeout, "traversal kernel reported status " + std::to_string(st));
         }
         if (st & kStatusOverflowSum)
@@ -1197,17 +1201,24 @@ BatchOutput BatchEngine::runKnn(const double* dPoints, uint32_t nq, const uint32
         knnIds_.alloc(knnCap_ * 8);
         knnD2_.alloc(knnCap_ * 8);
     }
+    bool sumSeen = false;
     for (int attempt = 0; attempt < 16; ++attempt) {
         reserveKnnMajor(nq);
         enqueueKnn(dPoints, nq, dK, flags);
         const uint32_t st = status();
-        if (st & (kStatusLookbackTimeout | kStatusWindowOverflow))
+        // Window overflows and look-back timeouts that follow an overflow are its consequences (see
+        // runRange); alone they are failures.
+        const uint32_t over = st & (kStatusOverflowEntries | kStatusOverflowItems | kStatusOverflowSum);
+        if ((st & (kStatusLookbackTimeout | kStatusWindowOverflow)) && !over)
             throw CudaError(cudaErrorLaunchTimeout, "traversal kernel reported status " + std::to_string(st));
-        // A count past the 32-bit space calls for a split only when nothing earlier overflowed: a
-        // capacity overflow upstream (wave 1's results, a pair list) leaves bounds unset, and the
-        // stages after it then see far more than the batch holds. Grow first; rerun; decide then.
-        if ((st & kStatusOverflowSum) && !(st & (kStatusOverflowEntries | kStatusOverflowItems)))
-            throw SplitBatch("a level generates more than 2^32 items; split the batch");
+        // A count past the 32-bit space calls for a split unless a capacity upstream overflowed in
+        // the same run (wave 1's results, a pair list: bounds left unset make every stage after it
+        // see far more than the batch holds); then the engine grows once and decides on the rerun.
+        if (st & kStatusOverflowSum) {
+            if (sumSeen || !(st & (kStatusOverflowEntries | kStatusOverflowItems)))
+                throw SplitBatch("a level generates more than 2^32 items; split the batch");
+            sumSeen = true;
+        }
         if (st == 0) {
             if (splitLimit_ < 0xffffffffull) checkSplitLimit();
             BatchOutput o = output(nq, flags);

@@ -48,7 +48,7 @@ __device__ __forceinline__ uint32_t appendPos(bool keep, uint32_t* counter, uint
 template <int D>
 __global__ void __launch_bounds__(kThreadsNm) knnBoundLevelKernel(KnnBoundLevelArgs a) {
     constexpr int DM = D > 0 ? D : 32;
-    if (*a.status & (kStatusLookbackTimeout | kStatusWindowOverflow)) return;
+    if (*a.status & kStatusInconsistent) return;
     const int dim = D > 0 ? D : a.D;
     const int lane = threadIdx.x & 31;
     const bool root = a.nNodes == 0;
@@ -120,7 +120,7 @@ __global__ void __launch_bounds__(kThreadsNm) knnBoundLevelKernel(KnnBoundLevelA
 template <int D>
 __global__ void __launch_bounds__(kThreadsNm) knnClusterPointsKernel(KnnClusterArgs a) {
     constexpr int DM = D > 0 ? D : 32;
-    if (*a.status & (kStatusLookbackTimeout | kStatusWindowOverflow)) return;
+    if (*a.status & kStatusInconsistent) return;
     const int dim = D > 0 ? D : a.D;
     const int lane = threadIdx.x & 31;
     const uint32_t entries = *a.inCount;

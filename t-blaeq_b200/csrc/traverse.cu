@@ -682,9 +682,9 @@ __global__ void __launch_bounds__(kExpandThreads, expandMinBlocks<PRED>()) expan
                                                   ((S::kWindowBytes + 15) / 16) * 16);  // deferred items
     uint32_t* sKeep = reinterpret_cast<uint32_t*>(sList + kWarpTile);                   // [R] keep words
 
-    // A look-back that gave up earlier in this batch left its frontier inconsistent (prefixes
-    // computed without the tile it waited for): never read it; the host reports the status.
-    if (*a.scratch.status & (kStatusLookbackTimeout | kStatusWindowOverflow)) return;
+    // A look-back that gave up earlier in this batch, or a child prefix that passed 32 bits, left
+    // the frontiers after it inconsistent: never read them; the host reports the status.
+    if (*a.scratch.status & kStatusInconsistent) return;
     const uint32_t entries = a.in.hdr[0];
     const uint32_t total = a.in.hdr[1];
     const uint32_t nTiles = (total + kWarpTile - 1) / kWarpTile;
@@ -1427,7 +1427,7 @@ __global__ void __launch_bounds__(kNodeMajorThreads) nodeMajorRangeKernel(NodeMa
     constexpr int kBoxFloats = 2 * (D > 0 ? D : 16);
     constexpr bool kStageBoxes = D > 0 && D % 2 == 0 && D <= 16;
     __shared__ __align__(16) float sBox[kStageBoxes ? kNodeMajorThreads / 32 : 1][kStageBoxes ? kNodeMajorChunk * kBoxFloats : 1];
-    if (*a.status & (kStatusLookbackTimeout | kStatusWindowOverflow)) return;
+    if (*a.status & kStatusInconsistent) return;
     const int dim = D > 0 ? D : a.D;
     const int lane = threadIdx.x & 31;
     const int w = threadIdx.x >> 5;
