@@ -215,7 +215,9 @@ int tblaeq_set_float_points(tblaeq_handle* h, int on);
  * points. The finest level first keeps the groups whose box meets the query box and then tests
  * only their points (on = default; off = every point of every surviving cluster). Same results.
  * Batches that ask for per-level counts (TBLAEQ_WANT_LEVELS) test every point: those counts are
- * the points of the surviving clusters. No counterpart in the reference. */
+ * the points of the surviving clusters. The same switch governs exact KNN batches, whose
+ * node-major point pass skips every group whose box lies beyond the query's bound. No counterpart
+ * in the reference. */
 int tblaeq_set_point_groups(tblaeq_handle* h, int on);
 /* The last range batch's point groups: out3[0] groups tested, out3[1] (query, group) pairs kept,
  * out3[2] points tested; zeros when it tested no groups. With groups, tblaeq_level_counts'

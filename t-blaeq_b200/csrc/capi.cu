@@ -529,6 +529,7 @@ int tblaeq_set_float_points(tblaeq_handle* h, int on) {
 int tblaeq_set_point_groups(tblaeq_handle* h, int on) {
     if (int c = checkPrepared(h)) return c;
     h->qh->runtime().engine->setPointGroups(on != 0);
+    h->qh->runtime().engine->setKnnGroups(on != 0);
     return TBLAEQ_OK;
 }
 

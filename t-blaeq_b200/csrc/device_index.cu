@@ -324,7 +324,18 @@ DerivedArrays computeDerived(const HostIndex& idx) {
             out.leaf[m][s] = static_cast<uint32_t>(C[m][s]);
         }
     }
-    out.pointsD = std::move(dec[H - 1]);
+    if (!out.pointPerm.empty()) {
+        // In point-group order, like the float copy (the KNN point kernel walks the groups).
+        const std::vector<double>& pts = dec[H - 1];
+        out.pointsD.resize(pts.size());
+        const int64_t n = static_cast<int64_t>(out.pointPerm.size());
+#pragma omp parallel for schedule(static)
+        for (int64_t i = 0; i < n; ++i)
+            for (uint64_t d = 0; d < D; ++d)
+                out.pointsD[static_cast<size_t>(i) * D + d] = pts[static_cast<size_t>(out.pointPerm[i]) * D + d];
+    } else {
+        out.pointsD = std::move(dec[H - 1]);
+    }
     return out;
 }
 

@@ -93,7 +93,8 @@ struct DerivedArrays {
     std::vector<uint32_t> groupCount;    // per group: its rows
     std::vector<float> groupBox;         // per group: lo[D] hi[D] of its points, rounded outward
     std::vector<uint32_t> clusterGroup;  // per finest cluster (mesh H-2 position): first group; one more at the end
-    // Decoded finest points in row order (y = P[j] * x_parent, one rounded multiply per dimension).
+    // Decoded finest points (y = P[j] * x_parent, one rounded multiply per dimension), in
+    // point-group order when the groups exist (pointPerm maps back to rows), else in row order.
     std::vector<double> pointsD;
 };
 

@@ -1045,6 +1045,14 @@ void BatchEngine::enqueueKnn(const double* dPoints, uint32_t nq, const uint32_t*
         c.rows = di_.rows[H - 2];
         c.rowsOnHost = di_.rowsOnHost[H - 2];
         c.decoded = di_.pointsD.bytes() ? di_.pointsD.as<double>() : nullptr;
+        if (c.decoded && di_.pointPerm.bytes()) {  // decoded points in point-group order
+            c.perm = di_.pointPerm.as<uint32_t>();
+            if (knnGroups_) {
+                c.clusterGroups = di_.clusterGroups.as<NodeRec>();
+                c.groupRec = di_.groupRec.as<NodeRec>();
+                c.groupBox = di_.groupBox.as<float>();
+            }
+        }
         c.map = di_.mapPtr[H - 1];
         c.points = dPoints;
         c.tau = tau;

@@ -64,6 +64,9 @@ public:
     // Node-major completion: before its point pass, a pass over every stride-th point of the listed
     // clusters tightens each query's bound (0 or 1: off; default 16).
     void setKnnRefine(uint32_t stride) { refineStride_ = stride; }
+    // Node-major completion's point pass: walk each cluster's point groups, skipping a group whose
+    // box lies beyond the query's bound (default on; with the range path's point groups).
+    void setKnnGroups(bool on) { knnGroups_ = on; }
     uint32_t knnRefine() const { return refineStride_; }
     double waveScale() const { return waveScale_; }
     // Exact KNN with the two-wave finest level: beam width of the probe (each query keeps its
@@ -241,6 +244,7 @@ private:
     bool twoWave_ = true;
     double waveScale_ = 1.0;
     uint32_t refineStride_ = 16;
+    bool knnGroups_ = true;
     DeviceMem candOffS_;
     EntryScorer scorer_ = nullptr;
     void* scorerCtx_ = nullptr;

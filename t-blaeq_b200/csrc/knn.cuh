@@ -143,7 +143,13 @@ struct KnnClusterArgs {
     const double* x;
     const double* rows;
     int rowsOnHost;
-    const double* decoded;  // optional: the decoded finest points by row (else rebuilt from rows and x)
+    const double* decoded;  // optional: the decoded finest points (else rebuilt from rows and x)
+    // With decoded: perm non-null means decoded is in point-group order (perm maps a position to
+    // its row, for the output id); the groups, when given, are walked with their boxes.
+    const uint32_t* perm;
+    const NodeRec* clusterGroups;  // per cluster: {-, first group, groups}
+    const NodeRec* groupRec;       // per group: {-, first position, points}
+    const float* groupBox;         // per group: lo[D] hi[D], rounded outward
     // Test only every sampleStride-th point of each cluster (0 or 1: every point). Lanes whose
     // cluster's lower bound (centre distance - subtree radius) already exceeds the query's bound
     // skip the cluster either way.

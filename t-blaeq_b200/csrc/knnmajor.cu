@@ -171,7 +171,7 @@ __global__ void __launch_bounds__(kThreadsNm) knnClusterPointsKernel(KnnClusterA
         const uint32_t stride = a.sampleStride > 1 ? a.sampleStride : 1u;
         const uint32_t nPts = (cr.cnt + stride - 1) / stride;  // points this pass tests
         if (lane == 0) rows += static_cast<unsigned long long>(__popc(live)) * nPts;
-        // Appends the candidate (query q, row j) when kept.
+        // Appends the candidate (query q, row j; a position when decoded is in group order) when kept.
         auto emit = [&](bool keep, uint32_t j, double dist) {
             if (__ballot_sync(FULL, keep) == 0) return;
             const uint32_t pos = appendPos(keep, a.outCount, a.status, lane);
@@ -179,25 +179,25 @@ __global__ void __launch_bounds__(kThreadsNm) knnClusterPointsKernel(KnnClusterA
                 atomicAdd(&a.qcount[q], 1u);
                 if (pos < a.outCap) {
                     a.outQ[pos] = q;
-                    a.outId[pos] = a.map[j];
+                    a.outId[pos] = a.map[(a.decoded && a.perm) ? __ldg(a.perm + j) : j];
                     a.outD2[pos] = dist;
                 } else {
                     atomicOr(a.status, kStatusOverflowEntries);
                 }
             }
         };
-        if (a.decoded) {
-            // The decoded points (the products below, made once when the index was prepared), four
-            // at a time: four independent fma chains per lane instead of one. A group past the
-            // cluster's end repeats its last point, which is never emitted twice.
-            const double* yb = a.decoded + static_cast<size_t>(cr.cbeg) * dim;
-            for (uint32_t c0 = 0; c0 < nPts; c0 += 4) {
-                const uint32_t nIn = min(4u, nPts - c0);
+        // Four decoded points at a time (the products below, made once when the index was
+        // prepared): four independent fma chains per lane instead of one. A run past its end
+        // repeats its last point, which is never emitted twice.
+        auto run = [&](bool act, uint32_t first, uint32_t n, uint32_t step) {
+            const double* yb = a.decoded + static_cast<size_t>(first) * dim;
+            for (uint32_t c0 = 0; c0 < n; c0 += 4) {
+                const uint32_t nIn = min(4u, n - c0);
                 double dist[4] = {0.0, 0.0, 0.0, 0.0};
                 const double* y4[4];
 #pragma unroll
                 for (int i = 0; i < 4; ++i)
-                    y4[i] = yb + static_cast<size_t>((c0 + min(static_cast<uint32_t>(i), nIn - 1)) * stride) * dim;
+                    y4[i] = yb + static_cast<size_t>((c0 + min(static_cast<uint32_t>(i), nIn - 1)) * step) * dim;
 #pragma unroll
                 for (int d = 0; d < DM; ++d) {
                     if (D > 0 || d < dim) {
@@ -210,8 +210,37 @@ __global__ void __launch_bounds__(kThreadsNm) knnClusterPointsKernel(KnnClusterA
                 }
 #pragma unroll
                 for (int i = 0; i < 4; ++i)
-                    if (static_cast<uint32_t>(i) < nIn) emit(active && dist[i] <= t2, cr.cbeg + (c0 + i) * stride, dist[i]);
+                    if (static_cast<uint32_t>(i) < nIn) emit(act && dist[i] <= t2, first + (c0 + i) * step, dist[i]);
             }
+        };
+        if (a.decoded && a.groupRec && stride == 1) {
+            // The cluster's point groups: a lane skips a group whose box lies beyond its bound.
+            const NodeRec cg = a.clusterGroups[un.node];
+            unsigned long long tested = 0;
+            for (uint32_t g = cg.cbeg; g < cg.cbeg + cg.cnt; ++g) {
+                const NodeRec gr = a.groupRec[g];
+                bool act = active;
+                if (act) {
+                    const float* b = a.groupBox + static_cast<size_t>(g) * 2 * dim;
+                    double gap = 0.0;
+#pragma unroll
+                    for (int d = 0; d < DM; ++d) {
+                        if (D > 0 || d < dim) {
+                            const double lo = static_cast<double>(__ldg(b + d)), hi = static_cast<double>(__ldg(b + dim + d));
+                            const double e = fmax(fmax(lo - p[d], p[d] - hi), 0.0);
+                            gap = __fma_rn(e, e, gap);
+                        }
+                    }
+                    act = gap * (1.0 - 1e-9) <= t2;
+                }
+                const uint32_t gm = __ballot_sync(FULL, act);
+                if (gm == 0) continue;
+                tested += static_cast<unsigned long long>(__popc(gm)) * gr.cnt;
+                run(act, gr.cbeg, gr.cnt, 1);
+            }
+            if (lane == 0) rows += tested - static_cast<unsigned long long>(__popc(live)) * nPts;
+        } else if (a.decoded) {
+            run(active, cr.cbeg, nPts, stride);
         } else {
             for (uint32_t c = 0; c < nPts; ++c) {
                 const uint32_t j = cr.cbeg + c * stride;

@@ -244,3 +244,35 @@ def test_bound_refinement_keeps_results(tb, env, oracle_mod, stride):
                 assert np.array_equal(d2[offs[q]:offs[q + 1]], b.dist2[b.offsets[j]:b.offsets[j + 1]]), (stride, q)
     finally:
         h.set_knn_refine(16)
+
+
+@pytest.mark.parametrize("D,ratios", [(8, (40, 20, 10)), (16, (40, 20, 10))])
+def test_knn_point_groups_keep_results(tb, oracle_mod, cuda, D, ratios):
+    """The completion's point pass over point groups (a group whose box lies beyond the query's
+    bound is skipped; the decoded points are kept in group order) returns the FP64 brute force's
+    ids and bit-identical squared distances, with the groups on and off and with and without the
+    bound refinement."""
+    h = tb.QueryHandler.generate(150000, D, 1.0, 100.0, False, 4, ratios, 90 + D, 2.5)
+    h.prepare_for_query(tb.LevelPolicy.L0)
+    N = h.info()["N"]
+    pts, ids = h.decode_points(np.arange(N))
+    P = _points(pts, 200, 91 + D, noise=1.0)
+    Kq = np.where(np.arange(200) % 2 == 0, 10, 60).astype(np.uint32)
+    bs = {kv: oracle_mod.brute_query(pts, ids, oracle_mod.KNN, P[Kq == kv], K=kv) for kv in (10, 60)}
+    rows = {}
+    try:
+        for groups in (True, False):
+            for stride in (16, 0):
+                h.set_point_groups(groups)
+                h.set_knn_refine(stride)
+                r = h.query_batch(tb.QueryType.POINT, P, tb.Mode.EXACT, K=Kq)
+                offs, got, d2 = r.offsets.numpy(), r.ids.numpy(), r.dist2.numpy()
+                for kv, b in bs.items():
+                    for j, q in enumerate(np.nonzero(Kq == kv)[0]):
+                        assert np.array_equal(got[offs[q]:offs[q + 1]], b.query(j)), (groups, stride, q)
+                        assert np.array_equal(d2[offs[q]:offs[q + 1]], b.dist2[b.offsets[j]:b.offsets[j + 1]])
+                rows[(groups, stride)] = h.knn_counters()["rows"]
+    finally:
+        h.set_point_groups(True)
+        h.set_knn_refine(16)
+    assert rows[(True, 16)] <= rows[(False, 16)]
