@@ -272,11 +272,12 @@ int tblaeq_set_knn_probe(tblaeq_handle* h, uint32_t beam, int node_major_complet
  * scale. No counterpart in the reference (its KNN keeps the STEP candidate set). */
 int tblaeq_set_knn_wave1(tblaeq_handle* h, double scale);
 
-/* The node-major KNN completion (after wave 1) first tests every stride-th point of the clusters it
- * listed; with wave 1's points they are real points, so each query's K-th distance among them
- * bounds its K-th neighbour distance, and the full point pass then skips every cluster whose sphere
- * lies beyond that bound (fewer points tested and far fewer candidates kept). stride 0 or 1: off;
- * default 16. Same results for every stride. No counterpart in the reference. */
+/* The node-major KNN completion (after wave 1) first tests every stride²-th and then every
+ * stride-th point of the clusters it listed; with wave 1's points they are real points, so each
+ * query's K-th distance among them bounds its K-th neighbour distance, and each later pass (the
+ * full point pass last) skips every cluster whose sphere lies beyond the bound so far (fewer points
+ * tested and far fewer candidates kept). stride 0 or 1: off; default 16. Same results for every
+ * stride. No counterpart in the reference. */
 int tblaeq_set_knn_refine(tblaeq_handle* h, uint32_t stride);
 
 /* Queries per traversal of a KNN batch. A batch whose workspace exceeds the 32-bit traversal space or

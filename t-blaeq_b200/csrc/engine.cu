@@ -300,7 +300,8 @@ void BatchEngine::reserve(const EngineCaps& want, uint32_t nq, unsigned flags) {
         // per-level query counts; per-node counts and cursors of meshes 0..H-2; the per-query
         // candidate cursors.
         offKnnTick_ = off;
-        off = align256(off + (2 * H + 4) * 4);  // H+1 tickets, H pair counts, candidates, refine ticket and count
+        // H+1 tickets, H pair counts, candidates, then a ticket and a candidate count per refine stage
+        off = align256(off + (2 * H + 2 + 2 * kMaxRefineStages) * 4);
         offQcountP_ = off;
         off = align256(off + H * static_cast<size_t>(qcap_) * 4);
         offKnnNodeCnt_.assign(H, 0);
@@ -1069,34 +1070,42 @@ void BatchEngine::enqueueKnn(const double* dPoints, uint32_t nq, const uint32_t*
         c.status = status;
         c.D = D;
         if (refineStride_ > 1) {
-            // Refine the bound first: every refineStride_-th point of the listed clusters, whose K
-            // nearest (with wave 1's) are real points, so their K-th distance bounds tau; the pass
-            // below then skips every cluster whose sphere lies beyond it. The sample's candidates
-            // serve only the bound (the pass below tests those points again).
-            uint32_t* sTick = candCnt + 1;
-            uint32_t* sCnt = candCnt + 2;
+            // Refine the bound first, in stages of decreasing stride (refineStride_^k, ..., the
+            // stride itself): each stage tests every stride-th point of the listed clusters within
+            // the current bound; with wave 1's they are real points, so their K-th distance bounds
+            // tau again, and the next stage (and the full pass below, which skips every cluster
+            // whose sphere lies beyond it) works under the tighter bound. A coarse first stage keeps
+            // the candidate lists small while the bound is still loose. The stages' candidates serve
+            // only the bound (the pass below tests those points again).
             uint32_t* qcS = qcountP;           // the probe's per-level counts are free again
             uint32_t* curS = qcountP + qcap_;
-            TBLAEQ_CUDA(cudaMemsetAsync(qcountP, 0, 2 * static_cast<size_t>(qcap_) * 4, stream_));
-            KnnClusterArgs sc = c;
-            sc.sampleStride = refineStride_;
-            sc.outCount = sCnt;
-            sc.qcount = qcS;
-            sc.ticket = sTick;
-            launchKnnClusterPoints(sc, stream_);
-            launchExclusiveScan(qcS, candOffS_.as<uint64_t>(), nq, stream_);
-            launchGroupResults(candId_.as<uint64_t>(), candQ_.as<uint32_t>(), candD2_.as<double>(), sCnt,
-                               static_cast<uint32_t>(std::min<uint64_t>(candCap_, resCapB_)), 1,
-                               candOffS_.as<uint64_t>(), curS, resIdsB_.as<uint64_t>(), resDistB_.as<double>(),
-                               stream_);
-            launchClampCounts2(candOff_.as<uint64_t>(), candOffS_.as<uint64_t>(), dK, nq, knnCount_.as<uint32_t>(),
-                               stream_);
-            launchExclusiveScan(knnCount_.as<uint32_t>(), knnOff_.as<uint64_t>(), nq, stream_);
-            launchTopK(candOff_.as<uint64_t>(), resIds_.as<uint64_t>(), resDist_.as<double>(), caps_.results,
-                       candOffS_.as<uint64_t>(), resIdsB_.as<uint64_t>(), resDistB_.as<double>(), resCapB_, dK, nq,
-                       knnOff_.as<uint64_t>(), knnIds_.as<uint64_t>(), knnD2_.as<double>(), knnCount_.as<uint32_t>(),
-                       status, stream_);
-            launchTauFromTopK(knnOff_.as<uint64_t>(), knnD2_.as<double>(), dK, nq, tau, stream_);
+            uint64_t stride = 1;
+            for (uint32_t k = 0; k < refineStages_; ++k) stride *= refineStride_;
+            for (uint32_t st = 0; st < refineStages_; ++st, stride /= refineStride_) {
+                if (stride > 0xffffffffull) continue;
+                uint32_t* sTick = candCnt + 1 + 2 * st;
+                uint32_t* sCnt = candCnt + 2 + 2 * st;
+                TBLAEQ_CUDA(cudaMemsetAsync(qcountP, 0, 2 * static_cast<size_t>(qcap_) * 4, stream_));
+                KnnClusterArgs sc = c;
+                sc.sampleStride = static_cast<uint32_t>(stride);
+                sc.outCount = sCnt;
+                sc.qcount = qcS;
+                sc.ticket = sTick;
+                launchKnnClusterPoints(sc, stream_);
+                launchExclusiveScan(qcS, candOffS_.as<uint64_t>(), nq, stream_);
+                launchGroupResults(candId_.as<uint64_t>(), candQ_.as<uint32_t>(), candD2_.as<double>(), sCnt,
+                                   static_cast<uint32_t>(std::min<uint64_t>(candCap_, resCapB_)), 1,
+                                   candOffS_.as<uint64_t>(), curS, resIdsB_.as<uint64_t>(), resDistB_.as<double>(),
+                                   stream_);
+                launchClampCounts2(candOff_.as<uint64_t>(), candOffS_.as<uint64_t>(), dK, nq,
+                                   knnCount_.as<uint32_t>(), stream_);
+                launchExclusiveScan(knnCount_.as<uint32_t>(), knnOff_.as<uint64_t>(), nq, stream_);
+                launchTopK(candOff_.as<uint64_t>(), resIds_.as<uint64_t>(), resDist_.as<double>(), caps_.results,
+                           candOffS_.as<uint64_t>(), resIdsB_.as<uint64_t>(), resDistB_.as<double>(), resCapB_, dK,
+                           nq, knnOff_.as<uint64_t>(), knnIds_.as<uint64_t>(), knnD2_.as<double>(),
+                           knnCount_.as<uint32_t>(), status, stream_);
+                launchTauFromTopK(knnOff_.as<uint64_t>(), knnD2_.as<double>(), dK, nq, tau, stream_);
+            }
         }
         launchKnnClusterPoints(c, stream_);
         if (timing_) record(1 + H);
@@ -1178,8 +1187,9 @@ void BatchEngine::reserveKnnMajor(uint32_t nq) {
 
 bool BatchEngine::growKnnMajor() {
     const int H = static_cast<int>(di_.height);
-    std::vector<uint32_t> c(H + 3, 0);  // pair counts, candidates, refine ticket, refine candidates
-    TBLAEQ_CUDA(cudaMemcpyAsync(c.data(), zeroBlock_.as<char>() + offKnnTick_ + (H + 1) * 4, (H + 3) * 4,
+    // pair counts, candidates, then (ticket, candidates) per refine stage
+    std::vector<uint32_t> c(H + 1 + 2 * kMaxRefineStages, 0);
+    TBLAEQ_CUDA(cudaMemcpyAsync(c.data(), zeroBlock_.as<char>() + offKnnTick_ + (H + 1) * 4, c.size() * 4,
                                 cudaMemcpyDeviceToHost, stream_));
     TBLAEQ_CUDA(cudaStreamSynchronize(stream_));
     bool grew = false;
@@ -1189,7 +1199,8 @@ bool BatchEngine::growKnnMajor() {
             grew = true;
         }
     }
-    const uint32_t cand = std::max(c[H], c[H + 2]);
+    uint32_t cand = c[H];
+    for (uint32_t st = 0; st < kMaxRefineStages; ++st) cand = std::max(cand, c[H + 2 + 2 * st]);
     if (cand > candCap_) {
         candCap_ = static_cast<uint64_t>(cand) + cand / 4 + 4096;
         grew = true;

@@ -39,6 +39,9 @@ struct EngineCaps {
     uint64_t results = 1u << 20;  // final results per batch
 };
 
+// Most stages of the KNN completion's bound refinement.
+constexpr uint32_t kMaxRefineStages = 4;
+
 class BatchEngine {
 public:
     BatchEngine(const DeviceIndex& di, cudaStream_t stream);
@@ -61,9 +64,13 @@ public:
     // Wave 1 of a two-wave KNN batch reads the ceil(scale * K / leaf) + 1 best-ranked clusters of
     // each query (2..32; leaf = points per finest cluster on average); default scale 1.
     void setWaveScale(double scale) { waveScale_ = scale > 0 ? scale : 1.0; }
-    // Node-major completion: before its point pass, a pass over every stride-th point of the listed
-    // clusters tightens each query's bound (0 or 1: off; default 16).
-    void setKnnRefine(uint32_t stride) { refineStride_ = stride; }
+    // Node-major completion: before its point pass, passes over every stride^k-th, ..., stride-th
+    // point of the listed clusters (`stages` of them) tighten each query's bound (stride 0 or 1:
+    // off; default 16 in two stages, 256 then 16).
+    void setKnnRefine(uint32_t stride, uint32_t stages = 2) {
+        refineStride_ = stride;
+        refineStages_ = stages < 1 ? 1 : (stages > kMaxRefineStages ? kMaxRefineStages : stages);
+    }
     // Node-major completion's point pass: walk each cluster's point groups, skipping a group whose
     // box lies beyond the query's bound (default on; with the range path's point groups).
     void setKnnGroups(bool on) { knnGroups_ = on; }
@@ -244,6 +251,7 @@ private:
     bool twoWave_ = true;
     double waveScale_ = 1.0;
     uint32_t refineStride_ = 16;
+    uint32_t refineStages_ = 2;
     bool knnGroups_ = true;
     DeviceMem candOffS_;
     EntryScorer scorer_ = nullptr;
