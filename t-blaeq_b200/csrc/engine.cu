@@ -31,8 +31,8 @@ void BatchEngine::resetWorkspace() noexcept {
     dropGraph();
     for (auto& f : f_)
         for (DeviceMem* m : {&f.q, &f.node, &f.cbeg, &f.cpre, &f.x, &f.tileStart}) m->release();
-    for (DeviceMem* m : {&nmNodeOff_, &nmUnitOff_, &nmList_, &rawIds_, &rawQ_, &rawVals_, &pairQ_[0], &pairQ_[1],
-                         &pairNode_[0], &pairNode_[1], &pairList_, &pairNodeOff_, &pairUnitOff_, &candQ_, &candId_,
+    for (DeviceMem* m : {&nmNodeOff_, &nmUnitOff_, &nmUnitNode_, &nmList_, &rawIds_, &rawQ_, &rawVals_, &pairQ_[0], &pairQ_[1],
+                         &pairNode_[0], &pairNode_[1], &pairList_, &pairNodeOff_, &pairUnitOff_, &pairUnitNode_, &candQ_, &candId_,
                          &candD2_, &excl_, &probeK_, &resIds_, &resVals_, &resQ_, &resDist_, &zeroBlock_, &cmpCnt_,
                          &cmpKids_, &cmpEntryOff_, &cmpKidOff_, &offsets_, &boxF_, &tau_, &candOff_, &knnCount_,
                          &knnOff_, &knnIds_, &knnD2_, &lbE_, &scoreE_, &sel_, &offF_, &waveM_, &selCount_, &selOff_,
@@ -385,6 +385,7 @@ void BatchEngine::reserveNodeMajor(unsigned flags) {
         for (uint64_t m = 0; m + 2 < di_.height; ++m) maxM = std::max<uint64_t>(maxM, di_.meshCount[m]);
         nmNodeOff_.alloc((maxM + 1) * 4);
         nmUnitOff_.alloc((maxM + 1) * 4);
+        nmUnitNode_.alloc((caps_.entries / 32 + maxM + 2) * 4);  // units <= entries / 32 + nodes
         nmEntryCap_ = caps_.entries;
     }
     const bool vals = (flags & kWantVals) != 0;
@@ -430,10 +431,12 @@ void BatchEngine::enqueueNodeMajorLevel(int m, int buf, const double* dBoxes, ui
         const uint32_t M = static_cast<uint32_t>(di_.meshCount[m - 1]);
         auto* nodeCnt = reinterpret_cast<uint32_t*>(z + offNodeCnt_[m]);
         launchNodeTranspose(in.node.as<uint32_t>(), hdrPtr(m), n.inCap, M, nodeCnt, nmNodeOff_.as<uint32_t>(),
-                            nmUnitOff_.as<uint32_t>(), nodeCnt + M, nmList_.as<uint32_t>(), stream_);
+                            nmUnitOff_.as<uint32_t>(), nodeCnt + M, nmList_.as<uint32_t>(), stream_,
+                            nmUnitNode_.as<uint32_t>(), static_cast<uint32_t>(nmUnitNode_.bytes() / 4));
         n.list = nmList_.as<uint32_t>();
         n.nodeOff = nmNodeOff_.as<uint32_t>();
         n.unitOff = nmUnitOff_.as<uint32_t>();
+        n.unitNode = nmUnitNode_.as<uint32_t>();
         n.nNodes = M;
         n.parents = di_.nodeSub[m - 1].as<NodeRec>();
     }
@@ -999,7 +1002,8 @@ void BatchEngine::enqueueKnn(const double* dPoints, uint32_t nq, const uint32_t*
             auto* nodeCnt = reinterpret_cast<uint32_t*>(z + offKnnNodeCnt_[mesh]);
             launchNodeTranspose(pairNode_[from].as<uint32_t>(), pairCnt + mesh, pcap, M, nodeCnt,
                                 pairNodeOff_.as<uint32_t>(), pairUnitOff_.as<uint32_t>(), nodeCnt + M,
-                                pairList_.as<uint32_t>(), stream_);
+                                pairList_.as<uint32_t>(), stream_, pairUnitNode_.as<uint32_t>(),
+                                static_cast<uint32_t>(pairUnitNode_.bytes() / 4));
             return M;
         };
         for (int m = 0; m < H - 1; ++m) {
@@ -1016,6 +1020,7 @@ void BatchEngine::enqueueKnn(const double* dPoints, uint32_t nq, const uint32_t*
                 b.list = pairList_.as<uint32_t>();
                 b.nodeOff = pairNodeOff_.as<uint32_t>();
                 b.unitOff = pairUnitOff_.as<uint32_t>();
+                b.unitNode = pairUnitNode_.as<uint32_t>();
                 b.parents = di_.nodeSub[m - 1].as<NodeRec>();
             }
             b.x = di_.nodeX[m].as<double>();
@@ -1041,6 +1046,7 @@ void BatchEngine::enqueueKnn(const double* dPoints, uint32_t nq, const uint32_t*
         c.list = pairList_.as<uint32_t>();
         c.nodeOff = pairNodeOff_.as<uint32_t>();
         c.unitOff = pairUnitOff_.as<uint32_t>();
+        c.unitNode = pairUnitNode_.as<uint32_t>();
         c.clusters = di_.nodeSub[H - 2].as<NodeRec>();
         c.x = di_.nodeX[H - 2].as<double>();
         c.rows = di_.rows[H - 2];
@@ -1170,6 +1176,9 @@ void BatchEngine::reserveKnnMajor(uint32_t nq) {
             pairNode_[b].alloc(pairCap_ * 4);
         }
         pairList_.alloc(pairCap_ * 4);
+        uint64_t maxM = 1;
+        for (uint64_t m = 0; m + 1 < di_.height; ++m) maxM = std::max<uint64_t>(maxM, di_.meshCount[m]);
+        pairUnitNode_.alloc((pairCap_ / 32 + maxM + 2) * 4);  // units <= pairs / 32 + nodes
     }
     if (candCap_ == 0) candCap_ = std::max<uint64_t>(caps_.results, 1u << 20);
     if (candQ_.bytes() < candCap_ * 4) {

@@ -201,7 +201,7 @@ private:
     bool pointGroups_ = true;
     bool groupsThisBatch_ = false;
     const NodeRec* innerRecords(int m) const;
-    DeviceMem nmNodeOff_, nmUnitOff_, nmList_, rawIds_, rawQ_, rawVals_;
+    DeviceMem nmNodeOff_, nmUnitOff_, nmUnitNode_, nmList_, rawIds_, rawQ_, rawVals_;
     uint64_t nmEntryCap_ = 0, nmResultCap_ = 0;
     bool nmVals_ = false;
     size_t offNm_ = 0, offRcursor_ = 0;
@@ -213,7 +213,7 @@ private:
     // candidates of the point level and the clusters wave 1 read per query.
     uint32_t probeBeam_ = 32;
     bool knnNodeMajor_ = true;
-    DeviceMem pairQ_[2], pairNode_[2], pairList_, pairNodeOff_, pairUnitOff_;
+    DeviceMem pairQ_[2], pairNode_[2], pairList_, pairNodeOff_, pairUnitOff_, pairUnitNode_;
     DeviceMem candQ_, candId_, candD2_, excl_, probeK_;
     uint64_t pairCap_ = 0, candCap_ = 0;
     size_t offKnnTick_ = 0, offQcountP_ = 0, offCandCursor_ = 0;

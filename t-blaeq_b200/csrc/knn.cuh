@@ -109,6 +109,7 @@ struct KnnBoundLevelArgs {
     const uint32_t* list;
     const uint32_t* nodeOff;
     const uint32_t* unitOff;
+    const uint32_t* unitNode;    // optional: the node of every unit (from the transpose)
     uint32_t nNodes;
     const NodeRec* parents;
     uint32_t rootChildren;
@@ -138,6 +139,7 @@ struct KnnClusterArgs {
     const uint32_t* list;
     const uint32_t* nodeOff;
     const uint32_t* unitOff;
+    const uint32_t* unitNode;    // optional: the node of every unit (from the transpose)
     uint32_t nNodes;
     const NodeRec* clusters;
     const double* x;

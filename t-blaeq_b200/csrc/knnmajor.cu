@@ -15,11 +15,16 @@ constexpr uint32_t FULL = 0xffffffffu;
 struct Unit {
     uint32_t node, base, count;
 };
-__device__ __forceinline__ Unit unitOf(uint32_t u, const uint32_t* nodeOff, const uint32_t* unitOff, uint32_t nNodes) {
+__device__ __forceinline__ Unit unitOf(uint32_t u, const uint32_t* nodeOff, const uint32_t* unitOff, uint32_t nNodes,
+                                      const uint32_t* unitNode) {
     uint32_t lo = 0, hi = nNodes - 1;
-    while (lo < hi) {
-        const uint32_t mid = (lo + hi + 1) >> 1;
-        if (__ldg(unitOff + mid) <= u) lo = mid; else hi = mid - 1;
+    if (unitNode) {
+        lo = min(__ldg(unitNode + u), nNodes - 1);  // the transpose's map (clamped for safety)
+    } else {
+        while (lo < hi) {
+            const uint32_t mid = (lo + hi + 1) >> 1;
+            if (__ldg(unitOff + mid) <= u) lo = mid; else hi = mid - 1;
+        }
     }
     Unit r;
     r.node = lo;
@@ -70,7 +75,7 @@ __global__ void __launch_bounds__(kThreadsNm) knnBoundLevelKernel(KnnBoundLevelA
             un.base = u * 32u;
             un.count = min(32u, entries - un.base);
         } else {
-            un = unitOf(u, a.nodeOff, a.unitOff, a.nNodes);
+            un = unitOf(u, a.nodeOff, a.unitOff, a.nNodes, a.unitNode);
             const NodeRec pr = a.parents[un.node];
             cbeg = pr.cbeg;
             cnt = pr.cnt;
@@ -135,14 +140,18 @@ __global__ void __launch_bounds__(kThreadsNm) knnClusterPointsKernel(KnnClusterA
         if (lane == 0) u = atomicAdd(a.ticket, 1u);
         u = __shfl_sync(FULL, u, 0);
         if (u >= units) break;
-        const Unit un = unitOf(u, a.nodeOff, a.unitOff, a.nNodes);
+        const Unit un = unitOf(u, a.nodeOff, a.unitOff, a.nNodes, a.unitNode);
         const NodeRec cr = a.clusters[un.node];
         bool active = static_cast<uint32_t>(lane) < un.count;
         uint32_t q = 0;
         if (active) {
             q = __ldg(a.inQ + __ldg(a.list + un.base + lane));
-            for (uint32_t i = 0; i < a.exclStride; ++i)
-                if (__ldg(a.excl + static_cast<size_t>(q) * a.exclStride + i) == un.node) active = false;
+            // Wave 1's clusters of this query fill its row from the start; ~0 ends them.
+            for (uint32_t i = 0; i < a.exclStride; ++i) {
+                const uint32_t c = __ldg(a.excl + static_cast<size_t>(q) * a.exclStride + i);
+                if (c == 0xffffffffu) break;
+                if (c == un.node) active = false;
+            }
         }
         const uint32_t am = __ballot_sync(FULL, active);
         if (am == 0) continue;

@@ -1505,9 +1505,13 @@ __global__ void __launch_bounds__(kNodeMajorThreads) nodeMajorRangeKernel(NodeMa
             cnt = a.rootChildren;
         } else {
             uint32_t lo = 0, hi = a.nNodes - 1;  // the node whose units hold u: last unitOff[n] <= u
-            while (lo < hi) {
-                const uint32_t mid = (lo + hi + 1) >> 1;
-                if (__ldg(a.unitOff + mid) <= u) lo = mid; else hi = mid - 1;
+            if (a.unitNode) {
+                lo = min(__ldg(a.unitNode + u), a.nNodes - 1);
+            } else {
+                while (lo < hi) {
+                    const uint32_t mid = (lo + hi + 1) >> 1;
+                    if (__ldg(a.unitOff + mid) <= u) lo = mid; else hi = mid - 1;
+                }
             }
             base = __ldg(a.nodeOff + lo) + (u - __ldg(a.unitOff + lo)) * 32u;
             count = min(32u, __ldg(a.nodeOff + lo + 1) - base);
@@ -1679,8 +1683,16 @@ int smallGrid(uint64_t work) { return static_cast<int>(std::max<uint64_t>(1, std
 
 }  // namespace
 
+__global__ void unitNodeKernel(const uint32_t* unitOff, uint32_t M, uint32_t* unitNode, uint32_t unitCap) {
+    for (uint32_t n = blockIdx.x * blockDim.x + threadIdx.x; n < M; n += gridDim.x * blockDim.x) {
+        const uint32_t u1 = min(unitOff[n + 1], unitCap);
+        for (uint32_t u = unitOff[n]; u < u1; ++u) unitNode[u] = n;
+    }
+}
+
 void launchNodeTranspose(const uint32_t* node, const uint32_t* hdr, uint32_t cap, uint32_t nNodes, uint32_t* nodeCnt,
-                         uint32_t* nodeOff, uint32_t* unitOff, uint32_t* cursor, uint32_t* list, cudaStream_t s) {
+                         uint32_t* nodeOff, uint32_t* unitOff, uint32_t* cursor, uint32_t* list, cudaStream_t s,
+                         uint32_t* unitNode, uint32_t unitCap) {
     const bool smem = nNodes <= kSmemNodes;
     if (smem)
         nodeCountSmemKernel<<<smallGrid(cap), 256, 0, s>>>(node, hdr, cap, nNodes, nodeCnt);
@@ -1689,6 +1701,10 @@ void launchNodeTranspose(const uint32_t* node, const uint32_t* hdr, uint32_t cap
     TBLAEQ_CUDA(cudaGetLastError());
     nodeScanKernel<<<1, 1024, 0, s>>>(nodeCnt, nNodes, nodeOff, unitOff);
     TBLAEQ_CUDA(cudaGetLastError());
+    if (unitNode) {
+        unitNodeKernel<<<smallGrid(nNodes), 256, 0, s>>>(unitOff, nNodes, unitNode, unitCap);
+        TBLAEQ_CUDA(cudaGetLastError());
+    }
     if (smem)
         nodeScatterSmemKernel<<<smallGrid(cap), 256, 0, s>>>(node, hdr, cap, nNodes, nodeOff, cursor, list);
     else

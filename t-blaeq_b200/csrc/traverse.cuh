@@ -204,6 +204,7 @@ struct NodeMajorArgs {
     const uint32_t* list;
     const uint32_t* nodeOff;
     const uint32_t* unitOff;
+    const uint32_t* unitNode;   // optional: the node of every unit (from the transpose)
     uint32_t nNodes;
     const NodeRec* parents;     // records of the input level's nodes (first child row, child count)
     uint32_t rootChildren;
@@ -229,8 +230,11 @@ struct NodeMajorArgs {
 
 // Groups the entries of a frontier by node (node keys < nNodes): nodeCnt and cursor (nNodes each)
 // must be zero; writes nodeOff / unitOff (nNodes + 1) and list (entries).
+// unitNode (optional, unitCap words >= cap / 32 + nNodes): the node of every unit, so a unit's
+// node is one load instead of a binary search over unitOff.
 void launchNodeTranspose(const uint32_t* node, const uint32_t* hdr, uint32_t cap, uint32_t nNodes, uint32_t* nodeCnt,
-                         uint32_t* nodeOff, uint32_t* unitOff, uint32_t* cursor, uint32_t* list, cudaStream_t s);
+                         uint32_t* nodeOff, uint32_t* unitOff, uint32_t* cursor, uint32_t* list, cudaStream_t s,
+                         uint32_t* unitNode = nullptr, uint32_t unitCap = 0);
 // The node-major test of one level (persistent grid; gridPercent as for the expand kernel).
 void launchNodeMajorRange(const NodeMajorArgs& a, int gridPercent, cudaStream_t s);
 // hdr[0] / hdr[1] = the entries and children a node-major level appended (its packed counter);
