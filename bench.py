@@ -272,9 +272,12 @@ def knn_legs(tb, h, P, K, steps, warmup, flush, n_plain=64):
         lat.append(time.perf_counter() - t1)
     plain_qps = n_plain / sum(lat)
 
-    # End to end: host points in, offsets + ids + squared distances out (learned ranking).
+    # End to end: host points in, offsets + ids + squared distances out (learned ranking). One
+    # untimed call first: a leg before may have split (and released the workspace), so the first
+    # call can be the one that grows it again.
     h.set_two_wave(True)
     h.scorer_enable(True)
+    h.query_batch_host(tb.QueryType.POINT, P, tb.Mode.EXACT, K=K, ids_cap=int(K.sum()))
     e2e_t, tot = [], 0
     for _ in range(max(1, steps)):
         t1 = time.perf_counter()

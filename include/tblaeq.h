@@ -268,7 +268,7 @@ int tblaeq_set_knn_probe(tblaeq_handle* h, uint32_t beam, int node_major_complet
 /* Wave 1 of a two-wave KNN batch reads every point of each query's ceil(scale * K / leaf) + 1
  * best-ranked finest clusters (at least 2, at most 32; leaf = the index's points per finest cluster)
  * and takes the K-th distance among them as the bound the rest of the batch prunes with. A larger
- * wave 1 costs more rows up front and tightens the bound (default scale 1). Same results for every
+ * wave 1 costs more rows up front and tightens the bound (default scale 16). Same results for every
  * scale. No counterpart in the reference (its KNN keeps the STEP candidate set). */
 int tblaeq_set_knn_wave1(tblaeq_handle* h, double scale);
 

@@ -609,7 +609,7 @@ class QueryHandler:
         or out-of-memory and starting later batches at the size that fitted)."""
         _check(_load().tblaeq_set_knn_chunk(self._h, int(max_queries)))
 
-    def set_knn_wave1(self, scale: float = 1.0):
+    def set_knn_wave1(self, scale: float = 16.0):
         """Two-wave KNN: wave 1 reads each query's ceil(scale * K / leaf) + 1 best-ranked clusters
         (2..32); larger tightens the bound the rest of the batch prunes with. Same results."""
         _check(_load().tblaeq_set_knn_wave1(self._h, float(scale)))

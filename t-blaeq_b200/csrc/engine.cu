@@ -460,6 +460,7 @@ void BatchEngine::enqueueNodeMajorLevel(int m, int buf, const double* dBoxes, ui
 
 void BatchEngine::enqueueLaunches(const double* dBoxes, uint32_t nq, int mode, unsigned flags) {
     lastKnn_ = false;
+    lastCompletion_ = false;
     const int H = static_cast<int>(di_.height);
     const int D = static_cast<int>(di_.D);
     char* z = zeroBlock_.as<char>();
@@ -633,7 +634,9 @@ void BatchEngine::growFromHeaders() {
     }
     // Results: slot H holds the one-pass (or wave-1) results, slot H+1 the wave-2 results of a
     // two-wave KNN batch (whose buffer follows the same capacity).
-    const uint64_t res = std::max<uint64_t>(h[2 * H], h[2 * (H + 1)]);
+    // (After a node-major completion slot H+1 only counts its candidates, whose buffers follow
+    // their own capacity: growKnnMajor.)
+    const uint64_t res = lastCompletion_ ? h[2 * H] : std::max<uint64_t>(h[2 * H], h[2 * (H + 1)]);
     if (res > caps_.results) {
         want.results = std::max<uint64_t>(want.results, res + res / 4 + 4096);
         grew = true;
@@ -987,6 +990,7 @@ void BatchEngine::enqueueKnn(const double* dPoints, uint32_t nq, const uint32_t*
                nullptr, 0, dK, nq, knnOff_.as<uint64_t>(), knnIds_.as<uint64_t>(), knnD2_.as<double>(),
                knnCount_.as<uint32_t>(), status, stream_);
     launchTauFromTopK(knnOff_.as<uint64_t>(), knnD2_.as<double>(), dK, nq, tau, stream_);
+    lastCompletion_ = completion;
     if (completion) {
         // Every point within tau, outside the clusters wave 1 read: the hierarchy again from the
         // root, node-major, then the clusters' points, each read once per 32 of its queries.

@@ -62,8 +62,8 @@ public:
     // cannot exclude. Off: one pass over every surviving cluster.
     void setTwoWave(bool on) { twoWave_ = on; }
     // Wave 1 of a two-wave KNN batch reads the ceil(scale * K / leaf) + 1 best-ranked clusters of
-    // each query (2..32; leaf = points per finest cluster on average); default scale 1.
-    void setWaveScale(double scale) { waveScale_ = scale > 0 ? scale : 1.0; }
+    // each query (2..32; leaf = points per finest cluster on average); default scale 16.
+    void setWaveScale(double scale) { waveScale_ = scale > 0 ? scale : 16.0; }
     // Node-major completion: before its point pass, passes over every stride^k-th, ..., stride-th
     // point of the listed clusters (`stages` of them) tighten each query's bound (stride 0 or 1:
     // off; default 16 in two stages, 256 then 16).
@@ -229,6 +229,7 @@ private:
     DeviceMem tau_, candOff_, knnCount_, knnOff_, knnIds_, knnD2_;
     uint64_t knnCap_ = 0;
     bool lastKnn_ = false;
+    bool lastCompletion_ = false;  // the last KNN batch ran the node-major completion
     // Two-wave final level of exact KNN (see enqueueKnn).
     DeviceMem lbE_, scoreE_, sel_, offF_, waveM_, selCount_, selOff_, selIds_, selD2_, candOffB_;
     DeviceMem resIdsB_, resQB_, resDistB_;
@@ -249,7 +250,7 @@ private:
     bool timing_ = false;
     bool capturing_ = false;
     bool twoWave_ = true;
-    double waveScale_ = 1.0;
+    double waveScale_ = 16.0;
     uint32_t refineStride_ = 16;
     uint32_t refineStages_ = 2;
     bool knnGroups_ = true;

@@ -222,7 +222,7 @@ def test_wave_one_width_keeps_results(tb, env, oracle_mod, scale):
         r = h.query_batch(tb.QueryType.POINT, P, tb.Mode.EXACT, K=30)
         assert np.array_equal(r.ids.numpy(), b.ids) and np.array_equal(r.dist2.numpy(), b.dist2)
     finally:
-        h.set_knn_wave1(1.0)
+        h.set_knn_wave1(16.0)
 
 
 @pytest.mark.parametrize("stride", [0, 3, 8])
