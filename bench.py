@@ -325,6 +325,8 @@ def main():
     ap.add_argument("--knn-chunk", type=int, default=0, help="KNN: queries per traversal (0 = automatic)")
     ap.add_argument("--knn-refine", type=int, default=-1,
                     help="KNN: stride of the bound-refinement sample (0 = off; -1 = the library's default)")
+    ap.add_argument("--knn-refine-stages", type=int, default=0,
+                    help="KNN: refinement stages (1..4; 0 = the library's default)")
     ap.add_argument("--knn-wave1", type=float, default=0.0,
                     help="KNN: wave-1 scale (clusters = ceil(scale*K/leaf)+1, 2..32; 0 = the library's default)")
     ap.add_argument("--variants", default=None,
@@ -521,8 +523,8 @@ def main():
     e2e_total = max_over_ranks(sum(e2e_t))
     e2e_value = job_throughput(args.nq * args.steps, world, e2e_total)
 
-    # The batched-plus-learned KNN leg on the same index (north-star target: batched + learned
-    # exact queries against the plain one-query-at-a-time traversal, at N = 10M, D = 8).
+    # The batched-plus-learned KNN leg on the same index: batched + learned exact queries against
+    # the plain one-query-at-a-time traversal, at N = 10M, D = 8.
     knn, knn_result, Pk, Kk = None, None, None, None
     if cfg_name == "batched" and not args.no_knn:
         Pk = wl.knn_points(h, args.knn_queries, seed=1234, noise=0.02)
@@ -658,6 +660,9 @@ def knn_options(h, args, config):
     if args.knn_refine >= 0:
         h.set_knn_refine(args.knn_refine)
         config["knn_refine_stride"] = args.knn_refine
+    if args.knn_refine_stages > 0:
+        h.set_knn_refine_stages(args.knn_refine_stages)
+        config["knn_refine_stages"] = args.knn_refine_stages
     if args.knn_wave1 > 0:
         h.set_knn_wave1(args.knn_wave1)
         config["knn_wave1_scale"] = args.knn_wave1

@@ -279,6 +279,8 @@ int tblaeq_set_knn_wave1(tblaeq_handle* h, double scale);
  * tested and far fewer candidates kept). stride 0 or 1: off; default 16. Same results for every
  * stride. No counterpart in the reference. */
 int tblaeq_set_knn_refine(tblaeq_handle* h, uint32_t stride);
+/* How many refinement stages run (1..4; default 2): strides stride^stages, ..., stride. */
+int tblaeq_set_knn_refine_stages(tblaeq_handle* h, uint32_t stages);
 
 /* Queries per traversal of a KNN batch. A batch whose workspace exceeds the 32-bit traversal space or
  * the free device memory runs as consecutive traversals of a halved size; later batches start at the

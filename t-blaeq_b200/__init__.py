@@ -157,6 +157,7 @@ def _load():
         "tblaeq_set_knn_chunk": ([vp, ctypes.c_uint64], ctypes.c_int),
         "tblaeq_set_knn_wave1": ([vp, ctypes.c_double], ctypes.c_int),
         "tblaeq_set_knn_refine": ([vp, ctypes.c_uint32], ctypes.c_int),
+        "tblaeq_set_knn_refine_stages": ([vp, ctypes.c_uint32], ctypes.c_int),
         "tblaeq_knn_split_reason": ([vp, ctypes.c_char_p, ctypes.c_uint64], ctypes.c_int),
         "tblaeq_knn_batch_info": ([vp, P(ctypes.c_uint64)], ctypes.c_int),
         "tblaeq_set_knn_probe": ([vp, ctypes.c_uint32, ctypes.c_int], ctypes.c_int),
@@ -618,6 +619,10 @@ class QueryHandler:
         """Node-major KNN completion: a pass over every stride-th point of the listed clusters first
         tightens each query's bound (0 or 1: off). Same results."""
         _check(_load().tblaeq_set_knn_refine(self._h, int(stride)))
+
+    def set_knn_refine_stages(self, stages: int = 2):
+        """How many refinement stages run (1..4): strides stride^stages, ..., stride."""
+        _check(_load().tblaeq_set_knn_refine_stages(self._h, int(stages)))
 
     def knn_batch_info(self) -> dict:
         """The last KNN batch: queries per traversal and traversals."""

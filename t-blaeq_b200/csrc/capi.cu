@@ -633,7 +633,15 @@ int tblaeq_set_knn_wave1(tblaeq_handle* h, double scale) {
 
 int tblaeq_set_knn_refine(tblaeq_handle* h, uint32_t stride) {
     if (int c = checkPrepared(h)) return c;
-    h->qh->runtime().engine->setKnnRefine(stride);
+    h->qh->runtime().engine->setKnnRefine(stride, h->qh->runtime().engine->knnRefineStages());
+    return TBLAEQ_OK;
+}
+
+int tblaeq_set_knn_refine_stages(tblaeq_handle* h, uint32_t stages) {
+    if (int c = checkPrepared(h)) return c;
+    if (stages < 1 || stages > kMaxRefineStages) return fail(TBLAEQ_ERR_INVALID, "refine stages must be in [1, 4]");
+    auto& e = *h->qh->runtime().engine;
+    e.setKnnRefine(e.knnRefine(), stages);
     return TBLAEQ_OK;
 }
 

@@ -75,6 +75,7 @@ public:
     // box lies beyond the query's bound (default on; with the range path's point groups).
     void setKnnGroups(bool on) { knnGroups_ = on; }
     uint32_t knnRefine() const { return refineStride_; }
+    uint32_t knnRefineStages() const { return refineStages_; }
     double waveScale() const { return waveScale_; }
     // Exact KNN with the two-wave finest level: beam width of the probe (each query keeps its
     // probeBeam entries of smallest lower bound at every level above the clusters, so wave 1 ranks
