@@ -891,7 +891,10 @@ void BatchEngine::enqueueKnn(const double* dPoints, uint32_t nq, const uint32_t*
     };
     // The beam leaves clusters out of the last frontier, so only the completion that walks the
     // hierarchy again from the root (not the query-major wave 2 over that frontier) may follow it.
-    const bool completion = twoWave_ && knnNodeMajor_;
+    // A batch of fewer queries than one node-major unit holds gains nothing from that walk (each
+    // unit would carry a few lanes) and pays its launches and passes in latency: it runs the
+    // query-major wave 2.
+    const bool completion = twoWave_ && knnNodeMajor_ && nq >= kCompletionMinQueries;
     const bool probe = completion && probeBeam_ > 0;
     auto* qcountP = reinterpret_cast<uint32_t*>(z + offQcountP_);
     if (probe) launchFillU32(probeK_.as<uint32_t>(), probeBeam_, nq, stream_);
@@ -938,6 +941,7 @@ void BatchEngine::enqueueKnn(const double* dPoints, uint32_t nq, const uint32_t*
     fin.rout.qcount = qcount;
     fin.rout.hdr = hdrPtr(H);
     fin.rout.cap = static_cast<uint32_t>(caps_.results);
+    lastCompletion_ = completion;
     if (!twoWave_) {
         launchExpand(fin, kPredKnnPoint, true, 0, stream_);
         if (timing_) record(1 + H);
@@ -990,7 +994,6 @@ void BatchEngine::enqueueKnn(const double* dPoints, uint32_t nq, const uint32_t*
                nullptr, 0, dK, nq, knnOff_.as<uint64_t>(), knnIds_.as<uint64_t>(), knnD2_.as<double>(),
                knnCount_.as<uint32_t>(), status, stream_);
     launchTauFromTopK(knnOff_.as<uint64_t>(), knnD2_.as<double>(), dK, nq, tau, stream_);
-    lastCompletion_ = completion;
     if (completion) {
         // Every point within tau, outside the clusters wave 1 read: the hierarchy again from the
         // root, node-major, then the clusters' points, each read once per 32 of its queries.
@@ -1257,7 +1260,7 @@ BatchOutput BatchEngine::runKnn(const double* dPoints, uint32_t nq, const uint32
             o.total = lastTotal(nq);
             return o;
         }
-        const bool grewMajor = (twoWave_ && knnNodeMajor_) ? growKnnMajor() : false;
+        const bool grewMajor = lastCompletion_ ? growKnnMajor() : false;
         if (!grewMajor) growFromHeaders();
         reserveKnn(nq);
     }

@@ -41,6 +41,8 @@ struct EngineCaps {
 
 // Most stages of the KNN completion's bound refinement.
 constexpr uint32_t kMaxRefineStages = 4;
+// Smallest KNN batch that runs the node-major completion (smaller ones: the query-major wave 2).
+constexpr uint32_t kCompletionMinQueries = 32;
 
 class BatchEngine {
 public:
