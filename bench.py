@@ -237,6 +237,7 @@ def knn_legs(tb, h, P, K, steps, warmup, flush, n_plain=64):
         ts = []
         if nvtx:
             torch.cuda.nvtx.range_push(nvtx)  # profilers select these steps by the range
+        runs = []
         for _ in range(n_steps):
             flush.zero_()
             torch.cuda.synchronize()
@@ -244,11 +245,13 @@ def knn_legs(tb, h, P, K, steps, warmup, flush, n_plain=64):
             h.query_batch(tb.QueryType.POINT, dP, tb.Mode.EXACT, K=K)
             torch.cuda.synchronize()
             ts.append(time.perf_counter() - t1)
+            runs.append(h.knn_batch_info()["runs"])
         if nvtx:
             torch.cuda.nvtx.range_pop()
         c = h.knn_counters()
         info = dict(h.knn_batch_info(), device_free_gb=torch.cuda.mem_get_info()[0] / 1e9,
-                    library_device_gb=tb.lib().tblaeq_live_device_bytes() / 1e9)
+                    library_device_gb=tb.lib().tblaeq_live_device_bytes() / 1e9, runs_per_step=runs,
+                    step_ms=[round(t * 1e3, 3) for t in ts])
         return nq * n_steps / sum(ts), c["rows"] / nq, ts, info
 
     learned_qps, learned_rows, step_s, learned_info = batch_leg(True, True, steps, warmup, nvtx="knn_timed")

@@ -288,6 +288,9 @@ int tblaeq_set_knn_refine_stages(tblaeq_handle* h, uint32_t stages);
  * automatic choice (and forgets the size learnt). No counterpart in the reference, which runs one
  * query at a time. */
 int tblaeq_set_knn_chunk(tblaeq_handle* h, uint64_t max_queries);
+/* Traversals the last synchronous batch (range or KNN, the last chunk of a split one) ran: 1, plus
+ * one rerun after every workspace growth. */
+int tblaeq_last_batch_runs(tblaeq_handle* h, uint64_t* runs);
 /* The last KNN batch: out2[0] = queries per traversal, out2[1] = traversals. */
 int tblaeq_knn_batch_info(tblaeq_handle* h, uint64_t* out2);
 /* Why a KNN batch of this handle was last split: the traversal size that did not fit and the

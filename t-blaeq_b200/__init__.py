@@ -159,6 +159,7 @@ def _load():
         "tblaeq_set_knn_refine": ([vp, ctypes.c_uint32], ctypes.c_int),
         "tblaeq_set_knn_refine_stages": ([vp, ctypes.c_uint32], ctypes.c_int),
         "tblaeq_knn_split_reason": ([vp, ctypes.c_char_p, ctypes.c_uint64], ctypes.c_int),
+        "tblaeq_last_batch_runs": ([vp, P(ctypes.c_uint64)], ctypes.c_int),
         "tblaeq_knn_batch_info": ([vp, P(ctypes.c_uint64)], ctypes.c_int),
         "tblaeq_set_knn_probe": ([vp, ctypes.c_uint32, ctypes.c_int], ctypes.c_int),
         "tblaeq_set_launch_shapes": ([vp, P(ctypes.c_int), P(ctypes.c_int), ctypes.c_uint64], ctypes.c_int),
@@ -630,7 +631,9 @@ class QueryHandler:
         _check(_load().tblaeq_knn_batch_info(self._h, out))
         buf = ctypes.create_string_buffer(512)
         _check(_load().tblaeq_knn_split_reason(self._h, buf, 512))
-        return {"chunk": out[0], "traversals": out[1], "split_reason": buf.value.decode()}
+        runs = ctypes.c_uint64()
+        _check(_load().tblaeq_last_batch_runs(self._h, ctypes.byref(runs)))
+        return {"chunk": out[0], "traversals": out[1], "split_reason": buf.value.decode(), "runs": runs.value}
 
     def knn_counters(self) -> dict:
         out = (ctypes.c_uint64 * 5)()

@@ -661,6 +661,13 @@ int tblaeq_knn_split_reason(tblaeq_handle* h, char* buf, uint64_t cap) {
     return TBLAEQ_OK;
 }
 
+int tblaeq_last_batch_runs(tblaeq_handle* h, uint64_t* runs) {
+    if (int c = checkPrepared(h)) return c;
+    if (!runs) return fail(TBLAEQ_ERR_INVALID, "null output");
+    *runs = h->qh->runtime().engine->lastRuns();
+    return TBLAEQ_OK;
+}
+
 int tblaeq_knn_batch_info(tblaeq_handle* h, uint64_t* out2) {
     if (int c = checkPrepared(h)) return c;
     if (!out2) return fail(TBLAEQ_ERR_INVALID, "null output");

@@ -681,6 +681,7 @@ BatchOutput BatchEngine::runRange(const double* dBoxes, uint32_t nq, int mode, u
     WorkspaceGuard guard(*this);
     reserve(caps_, nq, flags);
     for (int attempt = 0; attempt < 16; ++attempt) {
+        lastRuns_ = static_cast<uint32_t>(attempt + 1);
         if (useNodeMajor(mode)) reserveNodeMajor(flags);
         enqueueRange(dBoxes, nq, mode, flags);
         // The status word and the result total come back together: one host synchronisation.
@@ -1238,6 +1239,7 @@ BatchOutput BatchEngine::runKnn(const double* dPoints, uint32_t nq, const uint32
     }
     bool sumSeen = false;
     for (int attempt = 0; attempt < 16; ++attempt) {
+        lastRuns_ = static_cast<uint32_t>(attempt + 1);
         reserveKnnMajor(nq);
         enqueueKnn(dPoints, nq, dK, flags);
         const uint32_t st = status();

@@ -115,6 +115,8 @@ public:
         pointGroups_ = on;
     }
     std::vector<uint64_t> groupCounts();
+    // Enqueues of the last synchronous batch: 1, plus one rerun per workspace growth.
+    uint32_t lastRuns() const { return lastRuns_; }
     bool twoWave() const { return twoWave_; }
     // Optional device scorer of the last frontier's entries (higher = expand earlier); when unset
     // the entries are ranked by their lower bound. Called with (frontier, hdr, cap, points, out scores).
@@ -240,6 +242,7 @@ private:
     uint32_t knnQcap_ = 0;
     size_t offQcountF_ = 0, offQcountB_ = 0, offWork_ = 0;
     int lastKnnBuf_ = 0;
+    uint32_t lastRuns_ = 0;  // enqueues of the last synchronous batch (1 + growth reruns)
     void reserveKnn(uint32_t nq);
     size_t zeroBytes_ = 0;
     // offsets into zeroBlock_
