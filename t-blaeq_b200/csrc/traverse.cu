@@ -497,8 +497,11 @@ __device__ __forceinline__ bool singleEntryRangeBox(const ExpandArgs& a, uint32_
 #pragma unroll 1
     for (int s0 = 0; s0 < L; s0 += P) {
         double2 rv[P];
+        // Mapped host rows (a streamed interval) take plain loads; the block is just as contiguous,
+        // so each load instruction still moves whole lines across the host link.
 #pragma unroll
-        for (int i = 0; i < P; ++i) rv[i] = __ldg(rows2 + (s0 + i) * 32 + lane);
+        for (int i = 0; i < P; ++i)
+            rv[i] = a.child.rowsOnHost ? rows2[(s0 + i) * 32 + lane] : __ldg(rows2 + (s0 + i) * 32 + lane);
 #pragma unroll
         for (int i = 0; i < P; ++i) {
             const double y0 = __dmul_rn(rv[i].x, xv.x), y1 = __dmul_rn(rv[i].y, xv.y);
@@ -839,7 +842,7 @@ __global__ void __launch_bounds__(kExpandThreads, expandMinBlocks<PRED>()) expan
             if constexpr (kFastBox) {
                 // Warp-uniform: a full round inside one entry (its first and last item share it).
                 const uint32_t w0 = sWin[r * 32], w31 = sWin[r * 32 + 31];
-                if (W != 0 && t0 + r * 32 + 32 <= total && w0 == w31 && !a.child.rowsOnHost) {
+                if (W != 0 && t0 + r * 32 + 32 <= total && w0 == w31) {
                     keep = singleEntryRangeBox<D>(a, sRow[r * 32], eLo + w0, wQ[w0], lane);
                     done = true;
                 }
