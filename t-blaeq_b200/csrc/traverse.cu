@@ -283,7 +283,7 @@ template <int D, int PRED>
 __device__ __forceinline__ void prefetchTileRows(const ExpandArgs& a, uint32_t t, uint32_t nTiles, uint32_t entries,
                                                  uint32_t total, int lane, bool floatRows) {
     if (t >= nTiles) return;
-    if (a.child.rowsOnHost) return;  // bulk prefetches are for device memory
+    if (a.child.rowsOnHost && !floatRows) return;  // bulk prefetches are for device memory
     if (PRED == kPredRangeRadius && a.child.aabb) return;
     if (PRED == kPredKnnPoint && a.wave != 0 && a.child.entrySel) return;
     const uint32_t t0 = t * kWarpTile;
