@@ -196,9 +196,10 @@ def test_allocation_failure_surfaces_cleanly(tb, cuda):
 @pytest.mark.parametrize("policy", [("L0", "L0", "L2"), ("L3", "L3", "L3"), ("L2", "L3", "L1")])
 def test_streamed_levels_equal_resident(tb, oracle_mod, tmp_path, cuda, policy):
     """Intervals under L2 / L3 read their P rows (L3: and their maps) from page-locked host memory
-    mapped into the device address space; every variant falls back to plain loads there. Results
-    equal the resident index's: exact range and KNN against the FP64 brute force, ref-parity range
-    against the oracle's restatement of the reference, in the reference's order."""
+    mapped into the device address space (the float copy and the point groups stay on the device
+    when they fit). Results equal the resident index's: exact range (ids and coordinates) and KNN
+    against the FP64 brute force, ref-parity range against the oracle's restatement of the
+    reference, in the reference's order."""
     h = tb.QueryHandler.generate(200000, 8, 1.0, 100.0, False, 4, (100, 50, 20), 9, 3.0)
     h.prepare_for_query([tb.LevelPolicy[p] for p in policy])
     assert [p.name for p in h.info()["policy"]] == list(policy)
@@ -214,6 +215,9 @@ def test_streamed_levels_equal_resident(tb, oracle_mod, tmp_path, cuda, policy):
         assert all(np.array_equal(g, b.query(q)) for q, g in enumerate(ids_by_query(offs, got))), variant
         r2, offs2, got2 = _batch_ids(tb, h, Q, tb.Mode.REF_PARITY)
         assert np.array_equal(offs2, ref.offsets) and np.array_equal(got2, ref.ids), variant
+        rv = h.query_batch(tb.QueryType.RANGE, Q, tb.Mode.EXACT, flags=tb.WANT_VALS)
+        rows = {int(i): k for k, i in enumerate(ids)}
+        assert np.array_equal(rv.vals.numpy(), pts[[rows[int(i)] for i in rv.ids.numpy()]]), variant
     rng = np.random.default_rng(4)
     P = np.ascontiguousarray(pts[rng.integers(0, len(pts), 60)] + rng.normal(0, 0.5, (60, 8)))
     rk = h.query_batch(tb.QueryType.POINT, P, tb.Mode.EXACT, K=15)
