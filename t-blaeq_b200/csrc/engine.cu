@@ -301,7 +301,7 @@ void BatchEngine::reserve(const EngineCaps& want, uint32_t nq, unsigned flags) {
         // candidate cursors.
         offKnnTick_ = off;
         // H+1 tickets, H pair counts, candidates, then a ticket and a candidate count per refine stage
-        off = align256(off + (2 * H + 2 + 2 * kMaxRefineStages) * 4);
+        off = align256(off + (2 * H + 2 + 3 * kMaxRefineStages) * 4);  // ... and a filtered-pair count per stage
         offQcountP_ = off;
         off = align256(off + H * static_cast<size_t>(qcap_) * 4);
         offKnnNodeCnt_.assign(H, 0);
@@ -1005,10 +1005,10 @@ void BatchEngine::enqueueKnn(const double* dPoints, uint32_t nq, const uint32_t*
                               fb.node.as<uint32_t>(), fcap, nq, 32, excl_.as<uint32_t>(), stream_);
         const uint32_t pcap = static_cast<uint32_t>(pairCap_);
         int pb = 0;
-        auto group = [&](int mesh, int from) {
+        auto group = [&](int mesh, int from, const uint32_t* count = nullptr) {
             const uint32_t M = static_cast<uint32_t>(di_.meshCount[mesh]);
             auto* nodeCnt = reinterpret_cast<uint32_t*>(z + offKnnNodeCnt_[mesh]);
-            launchNodeTranspose(pairNode_[from].as<uint32_t>(), pairCnt + mesh, pcap, M, nodeCnt,
+            launchNodeTranspose(pairNode_[from].as<uint32_t>(), count ? count : pairCnt + mesh, pcap, M, nodeCnt,
                                 pairNodeOff_.as<uint32_t>(), pairUnitOff_.as<uint32_t>(), nodeCnt + M,
                                 pairList_.as<uint32_t>(), stream_, pairUnitNode_.as<uint32_t>(),
                                 static_cast<uint32_t>(pairUnitNode_.bytes() / 4));
@@ -1083,6 +1083,37 @@ void BatchEngine::enqueueKnn(const double* dPoints, uint32_t nq, const uint32_t*
         c.ticket = tick + H;
         c.status = status;
         c.D = D;
+        // After each refinement stage the cluster-level pairs are filtered under the tighter bound
+        // and grouped by cluster again, so the next pass's units hold live lanes only (under wave
+        // 1's bound at D = 16 nearly every cluster is listed for every query, and most lanes of a
+        // unit would skip).
+        uint32_t* filt = candCnt + 1 + 2 * kMaxRefineStages;
+        auto refilter = [&](uint32_t k) {
+            const int M2 = H - 2;
+            TBLAEQ_CUDA(cudaMemsetAsync(z + offKnnNodeCnt_[M2], 0, 2 * di_.meshCount[M2] * 4, stream_));
+            KnnFilterArgs f{};
+            f.inQ = pairQ_[pb].as<uint32_t>();
+            f.inNode = pairNode_[pb].as<uint32_t>();
+            f.inCount = c.inCount;
+            f.inCap = pcap;
+            f.clusters = di_.nodeSub[M2].as<NodeRec>();
+            f.x = di_.nodeX[M2].as<double>();
+            f.points = dPoints;
+            f.tau = tau;
+            f.excl = excl_.as<uint32_t>();
+            f.exclStride = 32;
+            f.outQ = pairQ_[1 - pb].as<uint32_t>();
+            f.outNode = pairNode_[1 - pb].as<uint32_t>();
+            f.outCap = pcap;
+            f.outCount = filt + k;
+            f.status = status;
+            f.D = D;
+            launchKnnFilterPairs(f, stream_);
+            pb = 1 - pb;
+            c.inQ = pairQ_[pb].as<uint32_t>();
+            c.inCount = filt + k;
+            c.nNodes = group(M2, pb, filt + k);
+        };
         if (refineStride_ > 1) {
             // Refine the bound first, in stages of decreasing stride (refineStride_^k, ..., the
             // stride itself): each stage tests every stride-th point of the listed clusters within
@@ -1119,6 +1150,7 @@ void BatchEngine::enqueueKnn(const double* dPoints, uint32_t nq, const uint32_t*
                            nq, knnOff_.as<uint64_t>(), knnIds_.as<uint64_t>(), knnD2_.as<double>(),
                            knnCount_.as<uint32_t>(), status, stream_);
                 launchTauFromTopK(knnOff_.as<uint64_t>(), knnD2_.as<double>(), dK, nq, tau, stream_);
+                refilter(st);
             }
         }
         launchKnnClusterPoints(c, stream_);

@@ -174,6 +174,30 @@ struct KnnClusterArgs {
 };
 void launchKnnClusterPoints(const KnnClusterArgs& a, cudaStream_t s);
 
+// Keeps the (query, cluster) pairs whose cluster sphere (centre distance - subtree radius, with the
+// point kernel's slack) is within the query's current bound and whose cluster wave 1 did not read,
+// appending them (no particular order) to outQ/outNode through outCount; the units the point
+// kernel forms from them afterwards are full of live lanes again.
+struct KnnFilterArgs {
+    const uint32_t* inQ;
+    const uint32_t* inNode;
+    const uint32_t* inCount;
+    uint32_t inCap;
+    const NodeRec* clusters;
+    const double* x;
+    const double* points;
+    const double* tau;
+    const uint32_t* excl;
+    uint32_t exclStride;
+    uint32_t* outQ;
+    uint32_t* outNode;
+    uint32_t outCap;
+    uint32_t* outCount;
+    uint32_t* status;
+    int D;
+};
+void launchKnnFilterPairs(const KnnFilterArgs& a, cudaStream_t s);
+
 // excl[q * stride + i] = node[selIds[selOff[q] + i]] for the selCount[q] entries wave 1 read, ~0
 // for the rest of the row.
 void launchWaveOneClusters(const uint64_t* selIds, const uint64_t* selOff, const uint32_t* selCount,

@@ -273,6 +273,55 @@ __global__ void __launch_bounds__(kThreadsNm) knnClusterPointsKernel(KnnClusterA
     if (a.work && lane == 0 && rows) atomicAdd(a.work, rows);
 }
 
+template <int D>
+__global__ void __launch_bounds__(256) knnFilterPairsKernel(KnnFilterArgs a) {
+    constexpr int DM = D > 0 ? D : 32;
+    if (*a.status & kStatusInconsistent) return;
+    const int dim = D > 0 ? D : a.D;
+    const int lane = threadIdx.x & 31;
+    const uint32_t n = *a.inCount;
+    if (n > a.inCap) {
+        if (blockIdx.x == 0 && threadIdx.x == 0) atomicOr(a.status, kStatusOverflowEntries);
+        return;
+    }
+    const uint32_t stride = gridDim.x * blockDim.x;
+    for (uint32_t base = blockIdx.x * blockDim.x + (threadIdx.x & ~31u); base < n; base += stride) {  // warp-uniform
+        const uint32_t i = base + lane;
+        bool keep = i < n;
+        uint32_t q = 0, c = 0;
+        if (keep) {
+            q = __ldg(a.inQ + i);
+            c = __ldg(a.inNode + i);
+            for (uint32_t k = 0; k < a.exclStride; ++k) {
+                const uint32_t e = __ldg(a.excl + static_cast<size_t>(q) * a.exclStride + k);
+                if (e == 0xffffffffu) break;
+                if (e == c) keep = false;
+            }
+        }
+        if (keep) {
+            const double* p = a.points + static_cast<size_t>(q) * dim;
+            const double* xc = a.x + static_cast<size_t>(c) * dim;
+            double dc = 0.0;
+#pragma unroll
+            for (int d = 0; d < DM; ++d) {
+                if (D > 0 || d < dim) {
+                    const double diff = __ldg(p + d) - __ldg(xc + d);
+                    dc = __fma_rn(diff, diff, dc);
+                }
+            }
+            const double t = __ldcg(a.tau + q);
+            keep = !((sqrt(dc) - a.clusters[c].rad) * (1.0 - 1e-9) > t + 1e-12);
+        }
+        const uint32_t pos = appendPos(keep, a.outCount, a.status, lane);
+        if (keep && pos < a.outCap) {
+            a.outQ[pos] = q;
+            a.outNode[pos] = c;
+        } else if (keep) {
+            atomicOr(a.status, kStatusOverflowEntries);
+        }
+    }
+}
+
 __global__ void waveOneClustersKernel(const uint64_t* selIds, const uint64_t* selOff, const uint32_t* selCount,
                                       const uint32_t* node, uint64_t cap, uint32_t nq, uint32_t stride, uint32_t* excl) {
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < nq * stride; i += gridDim.x * blockDim.x) {
@@ -342,6 +391,22 @@ void launchKnnClusterPoints(const KnnClusterArgs& a, cudaStream_t s) {
         default:
             if (a.D < 1 || a.D > 32) throw std::invalid_argument("KNN point level: D must be in [1, 32]");
             return clusterPointsD<0>(a, s);
+    }
+}
+
+template <int D>
+void filterPairsD(const KnnFilterArgs& a, cudaStream_t s) {
+    knnFilterPairsKernel<D><<<148 * 8, 256, 0, s>>>(a);
+    TBLAEQ_CUDA(cudaGetLastError());
+}
+
+void launchKnnFilterPairs(const KnnFilterArgs& a, cudaStream_t s) {
+    switch (a.D) {
+        case 8: return filterPairsD<8>(a, s);
+        case 16: return filterPairsD<16>(a, s);
+        default:
+            if (a.D < 1 || a.D > 32) throw std::invalid_argument("KNN pair filter: D must be in [1, 32]");
+            return filterPairsD<0>(a, s);
     }
 }
 
