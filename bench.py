@@ -237,21 +237,23 @@ def knn_legs(tb, h, P, K, steps, warmup, flush, n_plain=64):
         ts = []
         if nvtx:
             torch.cuda.nvtx.range_push(nvtx)  # profilers select these steps by the range
-        runs = []
+        runs, launches = [], 0
         for _ in range(n_steps):
             flush.zero_()
             torch.cuda.synchronize()
+            l0 = tb.kernel_launches()
             t1 = time.perf_counter()
             h.query_batch(tb.QueryType.POINT, dP, tb.Mode.EXACT, K=K)
             torch.cuda.synchronize()
             ts.append(time.perf_counter() - t1)
+            launches += tb.kernel_launches() - l0
             runs.append(h.knn_batch_info()["runs"])
         if nvtx:
             torch.cuda.nvtx.range_pop()
         c = h.knn_counters()
         info = dict(h.knn_batch_info(), device_free_gb=torch.cuda.mem_get_info()[0] / 1e9,
                     library_device_gb=tb.lib().tblaeq_live_device_bytes() / 1e9, runs_per_step=runs,
-                    step_ms=[round(t * 1e3, 3) for t in ts])
+                    step_ms=[round(t * 1e3, 3) for t in ts], gpu_launches=launches)
         return nq * n_steps / sum(ts), c["rows"] / nq, ts, info
 
     learned_qps, learned_rows, step_s, learned_info = batch_leg(True, True, steps, warmup, nvtx="knn_timed")
@@ -291,6 +293,7 @@ def knn_legs(tb, h, P, K, steps, warmup, flush, n_plain=64):
     st = sorted(x * 1e3 for x in step_s)
     return {
         "value": learned_qps, "unit": "queries/s", "steps": len(step_s),
+        "gpu_launches": learned_info["gpu_launches"],
         "ms_per_step": statistics.mean(step_s) * 1e3,
         "latency_ms": {"batch_p50": st[len(st) // 2], "batch_p99": st[min(len(st) - 1, int(len(st) * 0.99))],
                        "plain_query_p50": pl[len(pl) // 2], "plain_query_p99": pl[min(len(pl) - 1, int(len(pl) * 0.99))]},
@@ -443,6 +446,13 @@ def main():
         dist.barrier()
     total_ms = max_over_ranks(sum(step_ms))
     value = job_throughput(args.nq * args.steps, world, total_ms / 1e3)
+    # Kernels per step, counted from the nodes of the captured graph (one untimed capture when the
+    # timed steps ran without one).
+    graph = h.graph_launches()
+    if not graph["kernels"]:
+        h.query_batch_async(tb.QueryType.RANGE, dQ, tb.Mode.EXACT, flags=tb.USE_GRAPH)
+        h.batch_wait()
+        graph = h.graph_launches()
 
     # Roofline of the dominant level (largest event time): its algorithmic bytes per launch.
     H = len(entries)
@@ -603,8 +613,10 @@ def main():
         "config": config,
         "e2e": {"value": e2e_value, "unit": "queries/s", "h2d_bytes_per_step": args.nq * 2 * D * 8,
                 "d2h_bytes_per_step": (args.nq + 1) * 8 + int(tot.value) * 8},
-        # per step: root frontier, query-box rounding, one expand per level, offsets scan
-        "gpu_launches": args.steps * (H + 3),
+        # per step: the kernel nodes of the replayed graph (root frontier, box rounding, the level
+        # kernels, transposes, headers, scans, result grouping)
+        "gpu_launches": args.steps * graph["kernels"],
+        "graph_nodes_per_step": graph,
         "latency_ms": {"batch_p50": lat_ms[len(lat_ms) // 2], "batch_p99": lat_ms[min(len(lat_ms) - 1,
                                                                                      int(len(lat_ms) * 0.99))],
                        "plain_query_p50": pl[len(pl) // 2], "plain_query_p99": pl[min(len(pl) - 1,
@@ -747,7 +759,7 @@ def run_knn(args, tb, wl, rank, world, local):
         "warmup": max(1, args.warmup), "ms_per_step": leg["ms_per_step"], "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic (seeded RandomKmeans-style index and points)", "config": config,
-        "e2e": leg["e2e"], "gpu_launches": None, "latency_ms": leg["latency_ms"], "ranking": leg["ranking"],
+        "e2e": leg["e2e"], "gpu_launches": leg["gpu_launches"], "latency_ms": leg["latency_ms"], "ranking": leg["ranking"],
         "plain": leg["plain"],
         "scorer": {"train_queries": args.train_queries, "samples": stats["samples"], "positives": stats["positives"],
                    "train_s": train_s, "epoch_loss": losses},
@@ -828,8 +840,10 @@ def run_serving(args, tb, wl, rank, world, local):
         return out
 
     with ClockSampler(local) as clk:
+        l0 = tb.kernel_launches()
         with tb.Server(h, max_batch=4096, learned=True) as srv:
             batched = sweep(srv, loads, args.serve_requests, 100)
+        launches = tb.kernel_launches() - l0
     with tb.Server(h, max_batch=1, lanes=1, learned=False) as srv:
         plain = sweep(srv, [1e3, 1e4, 1e6], min(args.serve_requests, 400), 200)
     if rank != 0:
@@ -842,7 +856,7 @@ def run_serving(args, tb, wl, rank, world, local):
         "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded RandomKmeans-style index, Poisson stream)",
         "config": config,
         "e2e": {"value": best * world, "unit": "queries/s", "note": "requests enter and leave on the host"},
-        "loads": batched, "plain_one_at_a_time": plain,
+        "gpu_launches": launches, "loads": batched, "plain_one_at_a_time": plain,
         "speedup_vs_plain_at_saturation": best / best_plain if best_plain else None, "scorer_train_s": train_s,
         "clocks": clk.summary()}))
 
@@ -882,9 +896,11 @@ def run_build(args, tb, rank, world, local):
     tb.set_device(local)
     X = build_points(args.build_n, D)
     with ClockSampler(local) as clk:
+        l0 = tb.kernel_launches()
         t0 = time.perf_counter()
         h, rep = tb.QueryHandler.build(X, height=4, ratios=(100, 50, 20), iters=20, seed=1)
         total = time.perf_counter() - t0
+        launches = tb.kernel_launches() - l0
     sub = min(args.build_n, 2_000_000)
     _, rt = tb.QueryHandler.build(X[:sub], height=4, ratios=(100, 50, 20), iters=20, seed=1)
     _, r64 = tb.QueryHandler.build(X[:sub], height=4, ratios=(100, 50, 20), iters=20, seed=1,
@@ -906,7 +922,7 @@ def run_build(args, tb, rank, world, local):
         "metric": "index build: points indexed per second (k-means hierarchy, 1 B200 per rank)",
         "value": args.build_n / total * world, "unit": "points/s", "n_gpus": world, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "tf32x3 (fp32 accumulate)", "data": "synthetic",
-        "config": config, "seconds": total,
+        "config": config, "seconds": total, "gpu_launches": launches,
         "levels": rep,
         "objective_vs_fp64": {"points": sub, "tensor": [r["objective"] for r in rt],
                               "fp64": [r["objective"] for r in r64],

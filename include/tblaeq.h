@@ -163,6 +163,16 @@ int tblaeq_query_batch_host(tblaeq_handle* h, const tblaeq_batch* batch, uint64_
  * captured once into a CUDA graph and replayed. */
 int tblaeq_query_batch_async(tblaeq_handle* h, const tblaeq_batch* batch);
 
+/* Nodes of the CUDA graph that TBLAEQ_USE_GRAPH replays: *kernels = kernel launches per replay,
+ * *nodes = all nodes (kernels, memsets, copies, event records). Both 0 when no graph is held (no
+ * graph batch yet, or a setting or workspace growth since dropped it). */
+int tblaeq_graph_launches(tblaeq_handle* h, uint64_t* kernels, uint64_t* nodes);
+
+/* Kernel launches this library has issued in the process so far (index build, scorer training
+ * and queries; a launch captured into a CUDA graph counts once, at capture, and graph replays are
+ * not counted: tblaeq_graph_launches gives the kernels per replay). */
+uint64_t tblaeq_kernel_launches(void);
+
 /* Wait for the last enqueued batch, check its device status (workspace overflow ->
  * TBLAEQ_ERR_OVERFLOW: rerun it with tblaeq_query_batch) and describe its results. */
 int tblaeq_batch_wait(tblaeq_handle* h, tblaeq_batch_result* out);

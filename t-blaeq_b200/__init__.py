@@ -142,6 +142,8 @@ def _load():
                                   P(ctypes.c_uint64)], ctypes.c_int),
         "tblaeq_query_batch_async": ([vp, P(_Batch)], ctypes.c_int),
         "tblaeq_batch_wait": ([vp, P(_BatchResult)], ctypes.c_int),
+        "tblaeq_graph_launches": ([vp, P(ctypes.c_uint64), P(ctypes.c_uint64)], ctypes.c_int),
+        "tblaeq_kernel_launches": ([], ctypes.c_uint64),
         "tblaeq_stream": ([vp], vp),
         "tblaeq_level_counts": ([vp, P(ctypes.c_uint64), P(ctypes.c_uint64), ctypes.c_int, P(ctypes.c_uint64)],
                                 ctypes.c_int),
@@ -701,6 +703,13 @@ class QueryHandler:
     def set_timing(self, on: bool = True):
         _check(_load().tblaeq_set_timing(self._h, int(on)))
 
+    def graph_launches(self) -> dict:
+        """Kernel nodes and all nodes of the CUDA graph that USE_GRAPH batches replay (zeros when none
+        is held)."""
+        k, n = ctypes.c_uint64(), ctypes.c_uint64()
+        _check(_load().tblaeq_graph_launches(self._h, ctypes.byref(k), ctypes.byref(n)))
+        return {"kernels": k.value, "nodes": n.value}
+
     def stage_times(self) -> list:
         buf = (ctypes.c_float * 64)()
         n = _load().tblaeq_stage_times(self._h, buf, 64)
@@ -981,3 +990,9 @@ def tuning_lookup(path: str, key: str):
 def set_device(device: int):
     """cudaSetDevice for this library's CUDA runtime on the calling thread (before prepare)."""
     _check(_load().tblaeq_set_device(int(device)))
+
+
+def kernel_launches() -> int:
+    """Kernel launches this library has issued in the process so far (captures count once, graph
+    replays not at all)."""
+    return int(_load().tblaeq_kernel_launches())

@@ -15,6 +15,8 @@
 
 using namespace tblaeq;
 
+std::atomic<uint64_t> tblaeq::gKernelLaunches{0};
+
 struct tblaeq_handle {
     std::unique_ptr<QueryHandler> qh;
     DeviceMem stage;                            // device staging for host-side query batches
@@ -405,6 +407,16 @@ int tblaeq_query_batch_async(tblaeq_handle* h, const tblaeq_batch* b) {
         return TBLAEQ_OK;
     });
 }
+
+int tblaeq_graph_launches(tblaeq_handle* h, uint64_t* kernels, uint64_t* nodes) {
+    if (int c = checkPrepared(h)) return c;
+    const BatchEngine& e = *h->qh->runtime().engine;
+    if (kernels) *kernels = e.graphKernels();
+    if (nodes) *nodes = e.graphNodes();
+    return TBLAEQ_OK;
+}
+
+uint64_t tblaeq_kernel_launches(void) { return gKernelLaunches.load(std::memory_order_relaxed); }
 
 int tblaeq_batch_wait(tblaeq_handle* h, tblaeq_batch_result* out) {
     if (int c = checkPrepared(h)) return c;

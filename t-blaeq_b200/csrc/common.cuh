@@ -2,6 +2,7 @@
 #pragma once
 
 #include <cuda_runtime.h>
+#include <atomic>
 #include <cstdint>
 #include <cstdio>
 #include <stdexcept>
@@ -27,6 +28,10 @@ struct CudaError : std::runtime_error {
     CudaError(cudaError_t c, const std::string& what) : std::runtime_error(what), code(c) {}
 };
 
+// Kernel launches issued by this library since load (a launch captured into a CUDA graph counts
+// once, at capture; replays of the graph do not count here).
+extern std::atomic<uint64_t> gKernelLaunches;
+
 // A batch whose traversal does not fit the 32-bit item and entry space; smaller batches do.
 struct SplitBatch : CudaError {
     explicit SplitBatch(const std::string& what) : CudaError(cudaErrorMemoryAllocation, what) {}
@@ -39,6 +44,13 @@ struct SplitBatch : CudaError {
             throw ::tblaeq::CudaError(e_, std::string(#call) + " failed: " + cudaGetErrorString(e_) + " at " + \
                                               __FILE__ + ":" + std::to_string(__LINE__));                      \
         }                                                                                                     \
+    } while (0)
+
+// Error check after a kernel launch; counts the launch.
+#define TBLAEQ_LAUNCHED()                                                     \
+    do {                                                                      \
+        ::tblaeq::gKernelLaunches.fetch_add(1, std::memory_order_relaxed);    \
+        TBLAEQ_CUDA(cudaGetLastError());                                      \
     } while (0)
 
 }  // namespace tblaeq

@@ -358,6 +358,16 @@ void BatchEngine::enqueueRange(const double* dBoxes, uint32_t nq, int mode, unsi
             throw;
         }
         TBLAEQ_CUDA(cudaStreamEndCapture(stream_, &g));
+        size_t nNodes = 0;
+        cudaGraphGetNodes(g, nullptr, &nNodes);
+        std::vector<cudaGraphNode_t> nodes(nNodes);
+        uint64_t nKernels = 0;
+        if (nNodes && cudaGraphGetNodes(g, nodes.data(), &nNodes) == cudaSuccess) {
+            for (size_t i = 0; i < nNodes; ++i) {
+                cudaGraphNodeType t;
+                if (cudaGraphNodeGetType(nodes[i], &t) == cudaSuccess && t == cudaGraphNodeTypeKernel) ++nKernels;
+            }
+        }
         const cudaError_t e = cudaGraphInstantiate(&graphExec_, g, 0);
         cudaGraphDestroy(g);
         if (e != cudaSuccess) {
@@ -365,6 +375,8 @@ void BatchEngine::enqueueRange(const double* dBoxes, uint32_t nq, int mode, unsi
             throw CudaError(e, std::string("cudaGraphInstantiate failed: ") + cudaGetErrorString(e));
         }
         graphKey_ = key;
+        graphKernels_ = nKernels;
+        graphNodes_ = nNodes;
     }
     TBLAEQ_CUDA(cudaGraphLaunch(graphExec_, stream_));
 }

@@ -117,6 +117,9 @@ public:
     std::vector<uint64_t> groupCounts();
     // Enqueues of the last synchronous batch: 1, plus one rerun per workspace growth.
     uint32_t lastRuns() const { return lastRuns_; }
+    // Kernel nodes and all nodes of the captured range graph (0, 0 when none is held).
+    uint64_t graphKernels() const { return graphExec_ ? graphKernels_ : 0; }
+    uint64_t graphNodes() const { return graphExec_ ? graphNodes_ : 0; }
     bool twoWave() const { return twoWave_; }
     // Optional device scorer of the last frontier's entries (higher = expand earlier); when unset
     // the entries are ranked by their lower bound. Called with (frontier, hdr, cap, points, out scores).
@@ -268,6 +271,7 @@ private:
     void record(int i);
     std::vector<cudaEvent_t> events_;
     cudaGraphExec_t graphExec_ = nullptr;
+    uint64_t graphKernels_ = 0, graphNodes_ = 0;
     struct GraphKey {
         const double* boxes = nullptr;
         uint32_t nq = 0;

@@ -534,17 +534,17 @@ void assembleIntervalDevice(HostIndex& idx, uint64_t pIdx, uint64_t fineMesh, co
     const uint64_t D = idx.D;
     DeviceMem keys(nF * 8), keys2(nF * 8), vals(nF * 4), vals2(nF * 4);
     labelKeysKernel<<<gridFor(nF, 256), 256, 0, s>>>(dLabels, nF, keys.as<uint64_t>(), vals.as<uint32_t>());
-    TBLAEQ_CUDA(cudaGetLastError());
+    TBLAEQ_LAUNCHED();
     sortPairs(keys.as<uint64_t>(), vals.as<uint32_t>(), keys2.as<uint64_t>(), vals2.as<uint32_t>(), nF, s);
     DeviceMem colRes((nC + 1) * 8), pv(nF * D * 8), map(nF * 8), rad(nC * 8), zero(4);
     TBLAEQ_CUDA(cudaMemsetAsync(rad.get(), 0, nC * 8, s));
     TBLAEQ_CUDA(cudaMemsetAsync(zero.get(), 0, 4, s));
     colResKernel<<<gridFor(nF + 1, 256), 256, 0, s>>>(keys.as<uint64_t>(), nF, nC, colRes.as<uint64_t>());
-    TBLAEQ_CUDA(cudaGetLastError());
+    TBLAEQ_LAUNCHED();
     assembleRowsKernel<<<gridFor(nF, 256), 256, 0, s>>>(keys.as<uint64_t>(), nF, static_cast<int>(D), dFine, dCoarse,
                                                         pv.as<double>(), map.as<uint64_t>(),
                                                         rad.as<unsigned long long>(), zero.as<uint32_t>());
-    TBLAEQ_CUDA(cudaGetLastError());
+    TBLAEQ_LAUNCHED();
     PTensor& P = idx.pTensors[pIdx];
     P.D = D;
     P.rows = nF;
@@ -602,7 +602,7 @@ void kmeansRun(const float* dX, uint64_t n, uint64_t D, uint64_t k, const Kmeans
     DeviceMem Cd(k * D * 8), sums(k * D * 8), counts(k * 8), obj(8);
     labels.alloc(n * 4);
     gatherKernel<<<gridFor(k * D, 256), 256, 0, s>>>(dX, dPick.as<uint64_t>(), k, Di, Cd.as<double>(), centroids.as<float>());
-    TBLAEQ_CUDA(cudaGetLastError());
+    TBLAEQ_LAUNCHED();
 
     const uint64_t nTilesP = (n + kTileM - 1) / kTileM, nTilesC = (k + kTileN - 1) / kTileN;
     DeviceMem packedP, packedC, cand, status(4);
@@ -612,7 +612,7 @@ void kmeansRun(const float* dX, uint64_t n, uint64_t D, uint64_t k, const Kmeans
         packedC.alloc(nTilesC * kCentTileBytes);
         TBLAEQ_CUDA(cudaMemsetAsync(packedP.get(), 0, nTilesP * kPointTileBytes, s));
         packPointsKernel<<<gridFor(n, 256), 256, 0, s>>>(dX, n, Di, packedP.as<uint8_t>());
-        TBLAEQ_CUDA(cudaGetLastError());
+        TBLAEQ_LAUNCHED();
         TBLAEQ_CUDA(cudaFuncSetAttribute(assignTcKernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          static_cast<int>(kAssignSmem)));
     }
@@ -627,32 +627,36 @@ void kmeansRun(const float* dX, uint64_t n, uint64_t D, uint64_t k, const Kmeans
             packCentroidsKernel<<<gridFor(nTilesC * kTileN, 256), 256, 0, s>>>(centroids.as<float>(), k,
                                                                               nTilesC * kTileN, Di,
                                                                               packedC.as<uint8_t>());
-            TBLAEQ_CUDA(cudaGetLastError());
+            TBLAEQ_LAUNCHED();
             assignTcKernel<<<static_cast<unsigned>(nTilesP), kAssignThreads, kAssignSmem, s>>>(
                 packedP.as<uint8_t>(), packedC.as<uint8_t>(), n, static_cast<uint32_t>(nTilesC), cand.as<uint2>(),
                 status.as<uint32_t>());
-            TBLAEQ_CUDA(cudaGetLastError());
+            TBLAEQ_LAUNCHED();
             refineKernel<<<gridFor(n, 256), 256, 0, s>>>(dX, cand.as<uint2>(), Cd.as<double>(), n, Di,
                                                          labels.as<uint32_t>());
+            TBLAEQ_LAUNCHED();
         } else if (precision == kKmFp32) {
             assignScalarKernel<float><<<static_cast<unsigned>((n + 255) / 256), 256, 128 * D * 4, s>>>(
                 dX, n, Di, centroids.as<float>(), k, labels.as<uint32_t>());
+            TBLAEQ_LAUNCHED();
         } else {
             assignScalarKernel<double><<<static_cast<unsigned>((n + 255) / 256), 256, 128 * D * 8, s>>>(
                 dX, n, Di, Cd.as<double>(), k, labels.as<uint32_t>());
+            TBLAEQ_LAUNCHED();
         }
-        TBLAEQ_CUDA(cudaGetLastError());
         TBLAEQ_CUDA(cudaEventRecord(e1, s));
         TBLAEQ_CUDA(cudaMemsetAsync(sums.get(), 0, k * D * 8, s));
         TBLAEQ_CUDA(cudaMemsetAsync(counts.get(), 0, k * 8, s));
         accumulateKernel<<<gridFor(n, 256), 256, 0, s>>>(dX, labels.as<uint32_t>(), n, Di, sums.as<double>(),
                                                          counts.as<unsigned long long>());
+        TBLAEQ_LAUNCHED();
         finalizeKernel<<<gridFor(k * D, 256), 256, 0, s>>>(sums.as<double>(), counts.as<unsigned long long>(), k, Di,
                                                            Cd.as<double>(), centroids.as<float>());
+        TBLAEQ_LAUNCHED();
         TBLAEQ_CUDA(cudaMemsetAsync(obj.get(), 0, 8, s));
         objectiveKernel<<<gridFor(n, 256), 256, 0, s>>>(dX, labels.as<uint32_t>(), Cd.as<double>(), n, Di,
                                                         obj.as<double>());
-        TBLAEQ_CUDA(cudaGetLastError());
+        TBLAEQ_LAUNCHED();
         double o = 0.0;
         uint32_t st = 0;
         TBLAEQ_CUDA(cudaMemcpyAsync(&o, obj.get(), 8, cudaMemcpyDeviceToHost, s));

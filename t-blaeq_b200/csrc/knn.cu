@@ -475,45 +475,45 @@ void launchEntryBounds(const uint32_t* q, const uint32_t* node, const double* x,
         case 16: go(entryBoundsKernel<16>); break;
         default: go(entryBoundsKernel<0>); break;
     }
-    TBLAEQ_CUDA(cudaGetLastError());
+    TBLAEQ_LAUNCHED();
 }
 
 void launchWaveWidth(const uint32_t* K, uint32_t nq, double factor, uint32_t* M, cudaStream_t s) {
     if (nq == 0) return;
     waveWidthKernel<<<gridFor(nq, 256), 256, 0, s>>>(K, nq, factor, M);
-    TBLAEQ_CUDA(cudaGetLastError());
+    TBLAEQ_LAUNCHED();
 }
 
 void launchScatterSel(const uint64_t* ids, const uint64_t* off, uint32_t nq, uint64_t cap, uint8_t* sel,
                       cudaStream_t s) {
     scatterSelKernel<<<148 * 4, 256, 0, s>>>(ids, off, nq, cap, sel);
-    TBLAEQ_CUDA(cudaGetLastError());
+    TBLAEQ_LAUNCHED();
 }
 
 void launchTauFromTopK(const uint64_t* off, const double* d2, const uint32_t* K, uint32_t nq, double* tau,
                        cudaStream_t s) {
     if (nq == 0) return;
     tauFromTopKKernel<<<gridFor(nq, 256), 256, 0, s>>>(off, d2, K, nq, tau);
-    TBLAEQ_CUDA(cudaGetLastError());
+    TBLAEQ_LAUNCHED();
 }
 
 void launchClampCounts2(const uint64_t* offA, const uint64_t* offB, const uint32_t* K, uint32_t nq, uint32_t* out,
                         cudaStream_t s) {
     if (nq == 0) return;
     clampCounts2Kernel<<<gridFor(nq, 256), 256, 0, s>>>(offA, offB, K, nq, out);
-    TBLAEQ_CUDA(cudaGetLastError());
+    TBLAEQ_LAUNCHED();
 }
 
 void launchFillDouble(double* v, double value, uint32_t n, cudaStream_t s) {
     if (n == 0) return;
     fillDoubleKernel<<<gridFor(n, 256), 256, 0, s>>>(v, value, n);
-    TBLAEQ_CUDA(cudaGetLastError());
+    TBLAEQ_LAUNCHED();
 }
 
 void launchClampCounts(const uint64_t* off, const uint32_t* K, uint32_t nq, uint32_t* out, cudaStream_t s) {
     if (nq == 0) return;
     clampCountsKernel<<<gridFor(nq, 256), 256, 0, s>>>(off, K, nq, out);
-    TBLAEQ_CUDA(cudaGetLastError());
+    TBLAEQ_LAUNCHED();
 }
 
 void launchKnnLowerBound(const uint64_t* ids, const double* vals, uint64_t p, int D, const double* dPoint,
@@ -521,21 +521,21 @@ void launchKnnLowerBound(const uint64_t* ids, const double* vals, uint64_t p, in
                          cudaStream_t s) {
     if (p == 0) return;
     knnLowerBoundKernel<<<gridFor(p, 256), 256, 0, s>>>(ids, vals, p, D, dPoint, nodes, keys, labels, cnt, rr);
-    TBLAEQ_CUDA(cudaGetLastError());
+    TBLAEQ_LAUNCHED();
 }
 
 void sortPairs(uint64_t* keys, uint32_t* labels, uint64_t* keys2, uint32_t* labels2, uint64_t n, cudaStream_t s) {
     if (n <= 1) return;
     const uint64_t tiles = (n + kSortTile - 1) / kSortTile;
     bitonicTileKernel<<<static_cast<unsigned>(tiles), 1024, 0, s>>>(keys, labels, n);
-    TBLAEQ_CUDA(cudaGetLastError());
+    TBLAEQ_LAUNCHED();
     uint64_t* ka = keys;
     uint32_t* va = labels;
     uint64_t* kb = keys2;
     uint32_t* vb = labels2;
     for (uint64_t w = kSortTile; w < n; w *= 2) {
         mergePassKernel<<<gridFor((n + kMergeItems - 1) / kMergeItems, 256), 256, 0, s>>>(ka, va, kb, vb, n, w);
-        TBLAEQ_CUDA(cudaGetLastError());
+        TBLAEQ_LAUNCHED();
         std::swap(ka, kb);
         std::swap(va, vb);
     }
@@ -549,7 +549,7 @@ void launchStep(const uint64_t* keys, const uint32_t* labels, const uint32_t* cn
                 uint64_t K, uint8_t* mask, cudaStream_t s) {
     if (n == 0) return;
     stepKernel<<<1, 1024, 0, s>>>(keys, labels, cnt, rr, n, K, mask);
-    TBLAEQ_CUDA(cudaGetLastError());
+    TBLAEQ_LAUNCHED();
 }
 
 void launchTopK(const uint64_t* offA, const uint64_t* idsA, const double* d2A, uint64_t capA, const uint64_t* offB,
@@ -566,7 +566,7 @@ void launchTopK(const uint64_t* offA, const uint64_t* idsA, const double* d2A, u
     }
     topKKernel<<<nq, 512, smem, s>>>(offA, idsA, d2A, capA, offB, idsB, d2B, capB, K, outOff, outIds, outD2, outCount,
                                      status);
-    TBLAEQ_CUDA(cudaGetLastError());
+    TBLAEQ_LAUNCHED();
 }
 
 // ---- frontier compaction for the two finest-level waves ------------------------------------------
@@ -704,13 +704,13 @@ void launchCompactFrontier(const FrontierIn& F, uint32_t cap, int mode, const ui
                            uint64_t* kidOff, const FrontierOut& out, cudaStream_t s) {
     const uint32_t nSeg = std::max<uint32_t>(1u, (cap + kSegment - 1) / kSegment);
     compactCountKernel<<<nSeg, kCompactThreads, 0, s>>>(F, mode, sel, lb, tau, cnt, kids);
-    TBLAEQ_CUDA(cudaGetLastError());
+    TBLAEQ_LAUNCHED();
     launchExclusiveScan(cnt, entryOff, nSeg, s);
     launchExclusiveScan(kids, kidOff, nSeg, s);
     compactWriteKernel<<<nSeg, kCompactThreads, 0, s>>>(F, mode, sel, lb, tau, entryOff, kidOff, D, out);
-    TBLAEQ_CUDA(cudaGetLastError());
+    TBLAEQ_LAUNCHED();
     compactHeaderKernel<<<1, 1, 0, s>>>(entryOff, kidOff, nSeg, out.hdr);
-    TBLAEQ_CUDA(cudaGetLastError());
+    TBLAEQ_LAUNCHED();
 }
 
 uint32_t compactSegments(uint64_t cap) { return static_cast<uint32_t>(std::max<uint64_t>(1, (cap + kSegment - 1) / kSegment)); }

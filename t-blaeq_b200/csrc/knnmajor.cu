@@ -352,14 +352,14 @@ template <int D>
 void boundLevelD(const KnnBoundLevelArgs& a, cudaStream_t s) {
     static const int g = persistentGrid(knnBoundLevelKernel<D>);
     knnBoundLevelKernel<D><<<g, kThreadsNm, 0, s>>>(a);
-    TBLAEQ_CUDA(cudaGetLastError());
+    TBLAEQ_LAUNCHED();
 }
 
 template <int D>
 void clusterPointsD(const KnnClusterArgs& a, cudaStream_t s) {
     static const int g = persistentGrid(knnClusterPointsKernel<D>);
     knnClusterPointsKernel<D><<<g, kThreadsNm, 0, s>>>(a);
-    TBLAEQ_CUDA(cudaGetLastError());
+    TBLAEQ_LAUNCHED();
 }
 
 int smallGridNm(uint64_t n) { return static_cast<int>(std::max<uint64_t>(1, std::min<uint64_t>((n + 255) / 256, 148 * 8))); }
@@ -397,7 +397,7 @@ void launchKnnClusterPoints(const KnnClusterArgs& a, cudaStream_t s) {
 template <int D>
 void filterPairsD(const KnnFilterArgs& a, cudaStream_t s) {
     knnFilterPairsKernel<D><<<148 * 8, 256, 0, s>>>(a);
-    TBLAEQ_CUDA(cudaGetLastError());
+    TBLAEQ_LAUNCHED();
 }
 
 void launchKnnFilterPairs(const KnnFilterArgs& a, cudaStream_t s) {
@@ -416,13 +416,13 @@ void launchWaveOneClusters(const uint64_t* selIds, const uint64_t* selOff, const
     if (nq == 0 || stride == 0) return;
     waveOneClustersKernel<<<smallGridNm(static_cast<uint64_t>(nq) * stride), 256, 0, s>>>(selIds, selOff, selCount, node,
                                                                                         cap, nq, stride, excl);
-    TBLAEQ_CUDA(cudaGetLastError());
+    TBLAEQ_LAUNCHED();
 }
 
 void launchFillU32(uint32_t* v, uint32_t value, uint32_t n, cudaStream_t s) {
     if (n == 0) return;
     fillU32Kernel<<<smallGridNm(n), 256, 0, s>>>(v, value, n);
-    TBLAEQ_CUDA(cudaGetLastError());
+    TBLAEQ_LAUNCHED();
 }
 
 }  // namespace tblaeq

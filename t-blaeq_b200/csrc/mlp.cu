@@ -465,7 +465,7 @@ Mlp::Mlp(MlpShape shape) : shape_(shape) {
 void Mlp::refreshBf16(cudaStream_t s) {
     const size_t n = shape_.params();
     toBf16Kernel<<<gridFor(n, 256), 256, 0, s>>>(master_.as<float>(), n, bf16_.as<__nv_bfloat16>());
-    TBLAEQ_CUDA(cudaGetLastError());
+    TBLAEQ_LAUNCHED();
 }
 
 std::vector<float> Mlp::getParams() const {
@@ -503,7 +503,7 @@ void Mlp::buildFeatures(const double* points, const uint32_t* q, const double* c
     if (n == 0) return;
     featuresKernel<<<gridFor(n, 256), 256, 0, s>>>(points, q, centres, radius, level, n, shape_.D, shape_.levels,
                                                    invScale, X);
-    TBLAEQ_CUDA(cudaGetLastError());
+    TBLAEQ_LAUNCHED();
 }
 
 float Mlp::lossAndGrad(const float* X, const float* y, uint32_t n, float* grad, cudaStream_t s) {
@@ -524,11 +524,11 @@ float Mlp::lossAndGrad(const float* X, const float* y, uint32_t n, float* grad, 
     TBLAEQ_CUDA(cudaFuncSetAttribute(sampleGradKernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
     sampleGradKernel<<<gridFor(n, 128), 128, smem, s>>>(bf16_.as<__nv_bfloat16>(), static_cast<int>(o.total), X, y, n,
                                                        o.in, h1, h2, dh1, dh2, dz, lt);
-    TBLAEQ_CUDA(cudaGetLastError());
+    TBLAEQ_LAUNCHED();
     paramGradKernel<<<gridFor(o.total, 128), 128, 0, s>>>(X, h1, h2, dh1, dh2, dz, n, o.in, grad);
-    TBLAEQ_CUDA(cudaGetLastError());
+    TBLAEQ_LAUNCHED();
     sumKernel<<<1, 1024, 0, s>>>(lt, n, loss);
-    TBLAEQ_CUDA(cudaGetLastError());
+    TBLAEQ_LAUNCHED();
     float hl = 0.f;
     TBLAEQ_CUDA(cudaMemcpyAsync(&hl, loss, 4, cudaMemcpyDeviceToHost, s));
     TBLAEQ_CUDA(cudaStreamSynchronize(s));
@@ -543,7 +543,7 @@ void Mlp::adamStep(const float* grad, float lr, cudaStream_t s) {
     const size_t n = shape_.params();
     adamKernel<<<gridFor(n, 256), 256, 0, s>>>(master_.as<float>(), adamM_.as<float>(), adamV_.as<float>(), grad, n, lr,
                                                b1, b2, 1e-8f, c1, c2, bf16_.as<__nv_bfloat16>());
-    TBLAEQ_CUDA(cudaGetLastError());
+    TBLAEQ_LAUNCHED();
 }
 
 void Mlp::logits(const float* X, uint32_t n, float* z, cudaStream_t s) const {
@@ -552,7 +552,7 @@ void Mlp::logits(const float* X, uint32_t n, float* z, cudaStream_t s) const {
     const size_t smem = o.total * 4;
     TBLAEQ_CUDA(cudaFuncSetAttribute(logitsKernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
     logitsKernel<<<gridFor(n, 128), 128, smem, s>>>(bf16_.as<__nv_bfloat16>(), static_cast<int>(o.total), X, n, o.in, z);
-    TBLAEQ_CUDA(cudaGetLastError());
+    TBLAEQ_LAUNCHED();
 }
 
 void Mlp::frontierFeatures(const FrontierIn& f, const uint32_t* node, const uint32_t* idx, uint32_t n,
@@ -561,7 +561,7 @@ void Mlp::frontierFeatures(const FrontierIn& f, const uint32_t* node, const uint
     if (n == 0) return;
     frontierFeaturesKernel<<<gridFor(n, 256), 256, 0, s>>>(f.q, node, f.x, idx, n, points, nodes, level, shape_.levels,
                                                            shape_.D, invScale, X);
-    TBLAEQ_CUDA(cudaGetLastError());
+    TBLAEQ_LAUNCHED();
 }
 
 void Mlp::launchTc(bool frontier, const void* srcPtr, const uint32_t* hdr, uint32_t n, uint32_t cap, void* out,
@@ -576,7 +576,7 @@ void Mlp::launchTc(bool frontier, const void* srcPtr, const uint32_t* hdr, uint3
                                      static_cast<int>(kTcSmemRequest)));
     kern<<<grid, kTcRows, kTcSmemRequest, s>>>(bf16_.as<__nv_bfloat16>(), shape_.D, shape_.levels, *src, hdr, n, cap,
                                                out, tcStatus_.as<uint32_t>());
-    TBLAEQ_CUDA(cudaGetLastError());
+    TBLAEQ_LAUNCHED();
 }
 
 void Mlp::scoreFrontier(const FrontierIn& f, const uint32_t* node, uint32_t cap, const double* points,

@@ -145,7 +145,7 @@ std::vector<float> trainScorer(Runtime& rt, const double* hostPoints, uint32_t n
             labelFrontierKernel<<<std::min<uint32_t>(c, 4096), 128, 0, s>>>(
                 res.offsets, res.ids, fv.offsets, fv.node, rt.invMapFinest.as<uint32_t>(),
                 rt.parentFinest.as<uint32_t>(), c, label.as<uint8_t>());
-            TBLAEQ_CUDA(cudaGetLastError());
+            TBLAEQ_LAUNCHED();
             std::vector<uint8_t> hl(fCount);
             TBLAEQ_CUDA(cudaMemcpyAsync(hl.data(), label.get(), fCount, cudaMemcpyDeviceToHost, s));
             TBLAEQ_CUDA(cudaStreamSynchronize(s));
@@ -162,7 +162,7 @@ std::vector<float> trainScorer(Runtime& rt, const double* hostPoints, uint32_t n
             mlp.frontierFeatures(fv.in, fv.node, dIdx.as<uint32_t>(), n, pts, rt.dev->nodeSub[level].as<NodeRec>(), level,
                                  rt.scorerInvScale, X.as<float>(), s);
             gatherLabelsKernel<<<148, 256, 0, s>>>(label.as<uint8_t>(), dIdx.as<uint32_t>(), n, y.as<float>());
-            TBLAEQ_CUDA(cudaGetLastError());
+            TBLAEQ_LAUNCHED();
             const size_t x0 = hostX.size(), y0 = hostY.size();
             hostX.resize(x0 + static_cast<size_t>(n) * in);
             hostY.resize(y0 + n);
@@ -198,7 +198,7 @@ std::vector<float> trainScorer(Runtime& rt, const double* hostPoints, uint32_t n
         DeviceMem dPerm = upload(perm, s);
         permuteKernel<<<148 * 2, 256, 0, s>>>(X.as<float>(), y.as<float>(), dPerm.as<uint32_t>(), n, in, Xp.as<float>(),
                                               yp.as<float>());
-        TBLAEQ_CUDA(cudaGetLastError());
+        TBLAEQ_LAUNCHED();
         double sum = 0.0;
         int batches = 0;
         for (uint32_t b = 0; b < n; b += cfg.batch) {

@@ -1157,7 +1157,7 @@ void launchOne(const ExpandArgs& a, int gridBlocks, cudaStream_t s) {
         gridBlocks = std::max(1, static_cast<int>((static_cast<long long>(cached) * pct + 99) / 100));
     }
     kern<<<gridBlocks, kExpandThreads, smemBytes, s>>>(a);
-    TBLAEQ_CUDA(cudaGetLastError());
+    TBLAEQ_LAUNCHED();
 }
 
 template <int D, bool ST>
@@ -1232,7 +1232,7 @@ void launchRootFrontier(uint32_t* q, uint32_t* cbeg, uint32_t* cpre, double* x, 
     const uint64_t work = std::max<uint64_t>(nq, nTiles);
     const int blocks = static_cast<int>(std::min<uint64_t>(1024, (work + 255) / 256 + 1));
     rootFrontierKernel<<<blocks, 256, 0, stream>>>(q, cbeg, cpre, x, tileStart, hdr, nq, nChildren, D, tile);
-    TBLAEQ_CUDA(cudaGetLastError());
+    TBLAEQ_LAUNCHED();
 }
 
 __global__ void roundBoxesKernel(const double* boxes, uint32_t nq, int D, float* boxesF, float* boxesFi) {
@@ -1250,12 +1250,12 @@ void launchRoundBoxes(const double* boxes, uint32_t nq, int D, float* boxesF, fl
     const uint64_t n = static_cast<uint64_t>(nq) * 2 * D;
     const int blocks = static_cast<int>(std::min<uint64_t>(148 * 4, (n + 255) / 256));
     roundBoxesKernel<<<blocks, 256, 0, stream>>>(boxes, nq, D, boxesF, boxesFi);
-    TBLAEQ_CUDA(cudaGetLastError());
+    TBLAEQ_LAUNCHED();
 }
 
 void launchExclusiveScan(const uint32_t* counts, uint64_t* offsets, uint32_t n, cudaStream_t stream) {
     exclusiveScanKernel<<<1, 1024, 0, stream>>>(counts, offsets, n);
-    TBLAEQ_CUDA(cudaGetLastError());
+    TBLAEQ_LAUNCHED();
 }
 
 // ---- node-major range levels (exact mode) -------------------------------------------------------
@@ -1679,7 +1679,7 @@ void launchNodeMajorD(const NodeMajorArgs& a, int gridPercent, cudaStream_t s) {
     const int pct = (gridPercent > 0 && gridPercent < 100) ? gridPercent : 100;
     const int grid = std::max(1, (full * pct + 99) / 100);
     nodeMajorRangeKernel<D><<<grid, kNodeMajorThreads, 0, s>>>(a);
-    TBLAEQ_CUDA(cudaGetLastError());
+    TBLAEQ_LAUNCHED();
 }
 
 int smallGrid(uint64_t work) { return static_cast<int>(std::max<uint64_t>(1, std::min<uint64_t>((work + 255) / 256, 148 * 8))); }
@@ -1701,18 +1701,18 @@ void launchNodeTranspose(const uint32_t* node, const uint32_t* hdr, uint32_t cap
         nodeCountSmemKernel<<<smallGrid(cap), 256, 0, s>>>(node, hdr, cap, nNodes, nodeCnt);
     else
         nodeCountKernel<<<smallGrid(cap), 256, 0, s>>>(node, hdr, cap, nNodes, nodeCnt);
-    TBLAEQ_CUDA(cudaGetLastError());
+    TBLAEQ_LAUNCHED();
     nodeScanKernel<<<1, 1024, 0, s>>>(nodeCnt, nNodes, nodeOff, unitOff);
-    TBLAEQ_CUDA(cudaGetLastError());
+    TBLAEQ_LAUNCHED();
     if (unitNode) {
         unitNodeKernel<<<smallGrid(nNodes), 256, 0, s>>>(unitOff, nNodes, unitNode, unitCap);
-        TBLAEQ_CUDA(cudaGetLastError());
+        TBLAEQ_LAUNCHED();
     }
     if (smem)
         nodeScatterSmemKernel<<<smallGrid(cap), 256, 0, s>>>(node, hdr, cap, nNodes, nodeOff, cursor, list);
     else
         nodeScatterKernel<<<smallGrid(cap), 256, 0, s>>>(node, hdr, cap, nNodes, nodeOff, cursor, list);
-    TBLAEQ_CUDA(cudaGetLastError());
+    TBLAEQ_LAUNCHED();
 }
 
 void launchNodeMajorRange(const NodeMajorArgs& a, int gridPercent, cudaStream_t s) {
@@ -1732,19 +1732,19 @@ void launchNodeMajorRange(const NodeMajorArgs& a, int gridPercent, cudaStream_t 
 void launchFrontierHeader(const unsigned long long* counter, uint32_t* hdr, uint32_t cap, uint32_t tileCap,
                           uint32_t* status, cudaStream_t s) {
     frontierHeaderKernel<<<1, 1, 0, s>>>(counter, hdr, cap, tileCap, status);
-    TBLAEQ_CUDA(cudaGetLastError());
+    TBLAEQ_LAUNCHED();
 }
 
 void launchOneItemHeader(const uint32_t* count, uint32_t* hdr, cudaStream_t s) {
     oneItemHeaderKernel<<<1, 1, 0, s>>>(count, hdr);
-    TBLAEQ_CUDA(cudaGetLastError());
+    TBLAEQ_LAUNCHED();
 }
 
 void launchGroupResults(const uint64_t* rawIds, const uint32_t* rawQ, const double* rawVals, const uint32_t* hdr,
                         uint32_t cap, int D, const uint64_t* offsets, uint32_t* cursor, uint64_t* ids, double* vals,
                         cudaStream_t s) {
     groupResultsKernel<<<smallGrid(cap), 256, 0, s>>>(rawIds, rawQ, rawVals, hdr, cap, D, offsets, cursor, ids, vals);
-    TBLAEQ_CUDA(cudaGetLastError());
+    TBLAEQ_LAUNCHED();
 }
 
 }  // namespace tblaeq

@@ -61,9 +61,18 @@ def test_graph_replayed_batch_equals_synchronous(tb, batched):
     dQ = torch.from_numpy(Q).cuda()
     r = h.query_batch(tb.QueryType.RANGE, dQ, tb.Mode.EXACT)
     offs, got = r.offsets.numpy().copy(), r.ids.numpy().copy()
-    for _ in range(2):  # capture, then replay
+    l0 = tb.kernel_launches()
+    h.query_batch_async(tb.QueryType.RANGE, dQ, tb.Mode.EXACT)
+    h.batch_wait()
+    direct = tb.kernel_launches() - l0  # kernels one batch launches from the host
+    assert direct > 0
+    for i in range(2):  # capture, then replay
+        l0 = tb.kernel_launches()
         h.query_batch_async(tb.QueryType.RANGE, dQ, tb.Mode.EXACT, flags=tb.USE_GRAPH)
         total = h.batch_wait()
+        # the capture records the same launches once; a replay issues none from the host
+        assert tb.kernel_launches() - l0 == (direct if i == 0 else 0)
+        assert h.graph_launches()["kernels"] == direct
         assert total == offs[-1]
         assert np.array_equal(r.offsets.numpy(), offs)
         assert all(np.array_equal(a, b) for a, b in zip(ids_by_query(offs, r.ids.numpy()), ids_by_query(offs, got)))
