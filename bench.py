@@ -73,10 +73,15 @@ class ClockSampler:
              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
         try:
             self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={q}", "--format=csv,noheader,nounits",
-                                          "-i", str(self.gpu), "-lms", "100"], stdout=subprocess.PIPE,
+                                          "-i", str(self.gpu), "-lms", "20"], stdout=subprocess.PIPE,
                                          stderr=subprocess.DEVNULL, text=True)
             self.t = threading.Thread(target=self._read, daemon=True)
             self.t.start()
+            # nvidia-smi takes a moment to start: wait for its first sample, so that a timed region
+            # of a fraction of a second is sampled throughout.
+            t0 = time.perf_counter()
+            while not self.lines and self.proc.poll() is None and time.perf_counter() - t0 < 5.0:
+                time.sleep(0.005)
         except Exception:
             self.proc = None
         return self
