@@ -1419,12 +1419,12 @@ template <int D>
 __global__ void __launch_bounds__(kNodeMajorThreads) nodeMajorRangeKernel(NodeMajorArgs a) {
     constexpr uint32_t FULL = 0xffffffffu;
     constexpr int DM = D > 0 ? D : 32;
-    // The FP64 test is rare (children whose float box meets the query's): its double box and the
-    // node's coordinates stay in memory (L1) rather than in registers, which would cost occupancy.
-    constexpr int DR = 1;
-    constexpr bool kRegs = false;
     __shared__ uint32_t sQ[kNodeMajorThreads / 32][kNodeMajorStage];
     __shared__ uint32_t sJ[kNodeMajorThreads / 32][kNodeMajorStage];
+    // (lane, child) pairs whose float boxes meet: the FP64 radius test runs on them 32 at a time,
+    // one pair per lane, instead of once per child with the few lanes that passed.
+    __shared__ uint32_t sCandJ[kNodeMajorThreads / 32][64];
+    __shared__ uint8_t sCandL[kNodeMajorThreads / 32][64];
     // The float boxes of up to kNodeMajorChunk children of the unit's node, copied in with coalesced
     // 16-byte loads by the whole warp (one round of loads instead of one dependent load per child).
     constexpr int kBoxFloats = 2 * (D > 0 ? D : 16);
@@ -1532,10 +1532,8 @@ __global__ void __launch_bounds__(kNodeMajorThreads) nodeMajorRangeKernel(NodeMa
         // Every entry of the node carries the node's coordinates: take the first one's.
         xp = a.inX + static_cast<size_t>(__shfl_sync(FULL, e, 0)) * dim;
         float ql[DM], qh[DM];
-        double xr[DR], bl[DR], bh[DR];
         {
             const float* f = a.boxesF + static_cast<size_t>(q) * 2 * dim;
-            const double* box = a.boxes + static_cast<size_t>(q) * 2 * dim;
 #pragma unroll
             for (int d = 0; d < DM; ++d) {
                 if (D > 0 || d < dim) {
@@ -1543,15 +1541,55 @@ __global__ void __launch_bounds__(kNodeMajorThreads) nodeMajorRangeKernel(NodeMa
                     qh[d] = active ? __ldg(f + dim + d) : -1.f;
                 }
             }
-            if constexpr (kRegs) {
-#pragma unroll
-                for (int d = 0; d < DR; ++d) {
-                    xr[d] = __ldg(xp + d);
-                    bl[d] = active ? __ldg(box + d) : 0.0;
-                    bh[d] = active ? __ldg(box + dim + d) : 0.0;
-                }
-            }
         }
+        // The entry-major kernel's radius test (kPredRangeRadius) on the first n queued pairs, one
+        // per lane: the child's coordinates rebuilt with one rounded multiply per dimension, the box
+        // gap accumulated with fma in dimension order, against the child's subtree radius. Kept
+        // pairs are staged for the next frontier.
+        uint32_t nCand = 0;  // warp-uniform
+        auto testCandidates = [&](uint32_t n) {
+            __syncwarp();
+            const bool v = static_cast<uint32_t>(lane) < n;
+            const uint32_t j = v ? sCandJ[w][lane] : 0u;
+            const uint32_t cq = __shfl_sync(FULL, q, v ? sCandL[w][lane] : 0);
+            bool keep = false;
+            if (v) {
+                const NodeRec nr = a.children[j];
+                const double* row = a.rows + static_cast<size_t>(j) * dim;
+                const double* box = a.boxes + static_cast<size_t>(cq) * 2 * dim;
+                double dist = 0.0;
+#pragma unroll
+                for (int d = 0; d < DM; ++d) {
+                    if (D > 0 || d < dim) {
+                        const double r = a.rowsOnHost ? row[d] : __ldg(row + d);
+                        const double y = __dmul_rn(r, __ldg(xp + d));
+                        dist = boxGapAcc(y, __ldg(box + d), __ldg(box + dim + d), dist, 1);
+                    }
+                }
+                keep = nr.cnt > 0 && dist <= __dmul_rn(nr.rad, nr.rad);
+            }
+            const uint32_t kb = __ballot_sync(FULL, keep);
+            if (keep) {
+                const uint32_t slot = staged + __popc(kb & lanesLt);
+                sQ[w][slot] = cq;
+                sJ[w][slot] = j;
+            }
+            staged += __popc(kb);
+            if (staged + 32 > static_cast<uint32_t>(kNodeMajorStage)) flush();
+            // Move the pairs past the first n to the front of the queue.
+            const uint32_t rest = nCand - n;
+            uint32_t tj = 0, tl = 0;
+            if (static_cast<uint32_t>(lane) < rest) {
+                tj = sCandJ[w][n + lane];
+                tl = sCandL[w][n + lane];
+            }
+            __syncwarp();
+            if (static_cast<uint32_t>(lane) < rest) {
+                sCandJ[w][lane] = tj;
+                sCandL[w][lane] = static_cast<uint8_t>(tl);
+            }
+            nCand = rest;
+        };
         for (uint32_t c = 0; c < cnt; ++c) {
             const uint32_t j = cbeg + c;
             const float* b = a.aabb + static_cast<size_t>(j) * 2 * dim;
@@ -1586,44 +1624,17 @@ __global__ void __launch_bounds__(kNodeMajorThreads) nodeMajorRangeKernel(NodeMa
                     for (int i = 0; i < C; ++i) pass = pass && cl[i] <= qh[d + i] && ch[i] >= ql[d + i];
                 }
             }
-            if (__ballot_sync(FULL, pass) == 0) continue;
-            bool keep = false;
+            const uint32_t pb = __ballot_sync(FULL, pass);
+            if (pb == 0) continue;
             if (pass) {
-                // The entry-major kernel's radius test (kPredRangeRadius): the child's coordinates
-                // rebuilt with one rounded multiply per dimension, the box gap accumulated with fma
-                // in dimension order, against the child's subtree radius.
-                const NodeRec nr = a.children[j];
-                const double* row = a.rows + static_cast<size_t>(j) * dim;
-                double dist = 0.0;
-                if constexpr (kRegs) {
-                    double r[DR];
-#pragma unroll
-                    for (int d = 0; d < DR; ++d) r[d] = a.rowsOnHost ? row[d] : __ldg(row + d);
-#pragma unroll
-                    for (int d = 0; d < DR; ++d) dist = boxGapAcc(__dmul_rn(r[d], xr[d]), bl[d], bh[d], dist, 1);
-                } else {
-                    const double* box = a.boxes + static_cast<size_t>(q) * 2 * dim;
-#pragma unroll
-                    for (int d = 0; d < DM; ++d) {
-                        if (D > 0 || d < dim) {
-                            const double r = a.rowsOnHost ? row[d] : __ldg(row + d);
-                            const double y = __dmul_rn(r, __ldg(xp + d));
-                            dist = boxGapAcc(y, __ldg(box + d), __ldg(box + dim + d), dist, 1);
-                        }
-                    }
-                }
-                keep = nr.cnt > 0 && dist <= __dmul_rn(nr.rad, nr.rad);
+                const uint32_t slot = nCand + __popc(pb & lanesLt);
+                sCandJ[w][slot] = j;
+                sCandL[w][slot] = static_cast<uint8_t>(lane);
             }
-            const uint32_t kb = __ballot_sync(FULL, keep);
-            if (kb == 0) continue;
-            if (keep) {
-                const uint32_t slot = staged + __popc(kb & lanesLt);
-                sQ[w][slot] = q;
-                sJ[w][slot] = j;
-            }
-            staged += __popc(kb);
-            if (staged + 32 > static_cast<uint32_t>(kNodeMajorStage)) flush();
+            nCand += __popc(pb);  // at most 31 + 32 < 64
+            if (nCand >= 32) testCandidates(32);
         }
+        if (nCand) testCandidates(nCand);
         flush();
     }
 }
