@@ -439,6 +439,11 @@ void BatchEngine::enqueueNodeMajorLevel(int m, int buf, const double* dBoxes, ui
     if (m == 0) {
         n.nNodes = 0;
         n.rootChildren = static_cast<uint32_t>(di_.meshCount[0]);
+        // About 4,096 units (32 entries and a chunk of at least 4 of the root's children each).
+        const uint64_t qUnits = (static_cast<uint64_t>(nq) + 31) / 32;
+        const uint64_t maxChunks = std::max<uint64_t>(1, (n.rootChildren + 3) / 4);
+        const uint64_t chunks = std::min<uint64_t>(maxChunks, std::max<uint64_t>(1, (4096 + qUnits - 1) / qUnits));
+        n.rootChunk = static_cast<uint32_t>((n.rootChildren + chunks - 1) / chunks);
     } else {
         const uint32_t M = static_cast<uint32_t>(di_.meshCount[m - 1]);
         auto* nodeCnt = reinterpret_cast<uint32_t*>(z + offNodeCnt_[m]);

@@ -1100,15 +1100,23 @@ __global__ void rootFrontierKernel(uint32_t* q, uint32_t* cbeg, uint32_t* cpre, 
     }
 }
 
+// One block; each thread scans kScanItems consecutive counts per pass (independent loads), then the
+// block scans the threads' sums.
+constexpr int kScanItems = 4;
 __global__ void exclusiveScanKernel(const uint32_t* counts, uint64_t* offsets, uint32_t n) {
     __shared__ unsigned long long sCarry;
     __shared__ unsigned long long sWarp[32];
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     if (tid == 0) sCarry = 0;
     __syncthreads();
-    for (uint32_t base = 0; base < n; base += blockDim.x) {
-        const uint32_t i = base + tid;
-        const unsigned long long v = (i < n) ? counts[i] : 0;
+    for (uint64_t base = 0; base < n; base += static_cast<uint64_t>(blockDim.x) * kScanItems) {
+        const uint64_t i0 = base + static_cast<uint64_t>(tid) * kScanItems;
+        uint32_t c[kScanItems];
+#pragma unroll
+        for (int k = 0; k < kScanItems; ++k) c[k] = (i0 + k < n) ? counts[i0 + k] : 0u;
+        unsigned long long v = 0;
+#pragma unroll
+        for (int k = 0; k < kScanItems; ++k) v += c[k];
         unsigned long long inc = v;
 #pragma unroll
         for (int o = 1; o < 32; o <<= 1) {
@@ -1130,7 +1138,12 @@ __global__ void exclusiveScanKernel(const uint32_t* counts, uint64_t* offsets, u
         }
         __syncthreads();
         const unsigned long long carry = sCarry;
-        if (i < n) offsets[i] = carry + sWarp[warp] + inc - v;
+        unsigned long long run = carry + sWarp[warp] + inc - v;
+#pragma unroll
+        for (int k = 0; k < kScanItems; ++k) {
+            if (i0 + k < n) offsets[i0 + k] = run;
+            run += c[k];
+        }
         __syncthreads();
         if (tid == blockDim.x - 1) sCarry = carry + sWarp[warp] + inc;
         __syncthreads();
@@ -1441,7 +1454,9 @@ __global__ void __launch_bounds__(kNodeMajorThreads) nodeMajorRangeKernel(NodeMa
     }
     const uint32_t entries = a.inHdr[0];
     const bool root = a.nNodes == 0;
-    const uint32_t units = root ? (entries + 31u) / 32u : a.unitOff[a.nNodes];
+    const uint32_t rootChunk = (a.rootChunk && a.rootChunk < a.rootChildren) ? a.rootChunk : max(1u, a.rootChildren);
+    const uint32_t rootChunks = (a.rootChildren + rootChunk - 1) / rootChunk;
+    const uint32_t units = root ? (entries + 31u) / 32u * rootChunks : a.unitOff[a.nNodes];
     uint32_t staged = 0;  // warp-uniform
     const double* xp = nullptr;
     // Appends the staged survivors of the current unit (all children of one node, so they share the
@@ -1502,10 +1517,11 @@ __global__ void __launch_bounds__(kNodeMajorThreads) nodeMajorRangeKernel(NodeMa
         if (u >= units) break;
         uint32_t base, count, cbeg, cnt;
         if (root) {
-            base = u * 32u;
+            const uint32_t qu = u / rootChunks;
+            base = qu * 32u;
             count = min(32u, entries - base);
-            cbeg = 0;
-            cnt = a.rootChildren;
+            cbeg = (u - qu * rootChunks) * rootChunk;
+            cnt = min(rootChunk, a.rootChildren - cbeg);
         } else {
             uint32_t lo = 0, hi = a.nNodes - 1;  // the node whose units hold u: last unitOff[n] <= u
             if (a.unitNode) {
@@ -1697,10 +1713,13 @@ int smallGrid(uint64_t work) { return static_cast<int>(std::max<uint64_t>(1, std
 
 }  // namespace
 
+// One warp per node; its lanes write the node's units.
 __global__ void unitNodeKernel(const uint32_t* unitOff, uint32_t M, uint32_t* unitNode, uint32_t unitCap) {
-    for (uint32_t n = blockIdx.x * blockDim.x + threadIdx.x; n < M; n += gridDim.x * blockDim.x) {
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint32_t warps = gridDim.x * blockDim.x / 32u;
+    for (uint32_t n = (blockIdx.x * blockDim.x + threadIdx.x) / 32u; n < M; n += warps) {
         const uint32_t u1 = min(unitOff[n + 1], unitCap);
-        for (uint32_t u = unitOff[n]; u < u1; ++u) unitNode[u] = n;
+        for (uint32_t u = unitOff[n] + lane; u < u1; u += 32u) unitNode[u] = n;
     }
 }
 
@@ -1716,7 +1735,7 @@ void launchNodeTranspose(const uint32_t* node, const uint32_t* hdr, uint32_t cap
     nodeScanKernel<<<1, 1024, 0, s>>>(nodeCnt, nNodes, nodeOff, unitOff);
     TBLAEQ_LAUNCHED();
     if (unitNode) {
-        unitNodeKernel<<<smallGrid(nNodes), 256, 0, s>>>(unitOff, nNodes, unitNode, unitCap);
+        unitNodeKernel<<<smallGrid(static_cast<uint64_t>(nNodes) * 32), 256, 0, s>>>(unitOff, nNodes, unitNode, unitCap);
         TBLAEQ_LAUNCHED();
     }
     if (smem)

@@ -208,6 +208,9 @@ struct NodeMajorArgs {
     uint32_t nNodes;
     const NodeRec* parents;     // records of the input level's nodes (first child row, child count)
     uint32_t rootChildren;
+    // Root level: children per unit (0: all). A root unit is 32 entries and one chunk of the root's
+    // children, so that a small batch still spreads over the whole GPU.
+    uint32_t rootChunk;
     // The children: rows, float boxes and records (by row).
     const double* rows;
     const float* aabb;
