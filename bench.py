@@ -12,7 +12,8 @@ Reported on one JSON line (rank 0):
   e2e             the same through the public host-buffer API (boxes H2D from pinned memory,
                   offsets + ids D2H, every step inside the timed region)
   plain           one query at a time through the same engine (the >=5x denominator)
-  roofline        the finest-level expand kernel: algorithmic bytes / its event-timed duration
+  roofline        the dominant level (longest event time): its algorithmic bytes / its duration,
+                  with every level's bytes and rate
   cpu_baseline    the CPU port of the traversal (oracle) on all host cores, bounded sample
 Multi-GPU: replicas only (the path needs no exchange); every rank runs its own batches and the
 time is the max over ranks.
@@ -226,7 +227,8 @@ def knn_k(nq):
 
 def knn_legs(tb, h, P, K, steps, warmup, flush, n_plain=64):
     """Exact KNN over one index: the batched traversal with the learned ranking (timed steps), the
-    same with the lower-bound ranking and with a one-pass finest level (one step each), one query at
+    same with the lower-bound ranking and with a one-pass finest level (three steps each, the median
+    step reported), one query at
     a time with the lower-bound ranking and the scorer off (the plain traversal), and the learned
     batch end to end through the host-buffer entry point. Each batch is one synchronous C-ABI call,
     timed on the host with the device synchronised on both sides (L2 flushed before each step)."""
@@ -234,7 +236,7 @@ def knn_legs(tb, h, P, K, steps, warmup, flush, n_plain=64):
     nq, D = P.shape
     dP = torch.from_numpy(P).cuda()
 
-    def batch_leg(two_wave, learned, n_steps, n_warm, nvtx=None):
+    def batch_leg(two_wave, learned, n_steps, n_warm, nvtx=None, median=False):
         h.set_two_wave(two_wave)
         h.scorer_enable(learned)
         for _ in range(max(1, n_warm)):  # the first batch sizes every workspace
@@ -259,13 +261,15 @@ def knn_legs(tb, h, P, K, steps, warmup, flush, n_plain=64):
         info = dict(h.knn_batch_info(), device_free_gb=torch.cuda.mem_get_info()[0] / 1e9,
                     library_device_gb=tb.lib().tblaeq_live_device_bytes() / 1e9, runs_per_step=runs,
                     step_ms=[round(t * 1e3, 3) for t in ts], gpu_launches=launches)
+        if median:  # the comparison legs: the median step, so one slow step on a busy host does not decide
+            return nq / statistics.median(ts), c["rows"] / nq, ts, info
         return nq * n_steps / sum(ts), c["rows"] / nq, ts, info
 
     learned_qps, learned_rows, step_s, learned_info = batch_leg(True, True, steps, warmup, nvtx="knn_timed")
     r = h.query_batch(tb.QueryType.POINT, dP, tb.Mode.EXACT, K=K)
     result = (r.offsets.numpy().copy(), r.ids.numpy().copy(), r.dist2.numpy().copy())
-    lb_qps, lb_rows, _, lb_info = batch_leg(True, False, 1, 1)
-    one_qps, one_rows, _, one_info = batch_leg(False, False, 1, 1)
+    lb_qps, lb_rows, _, lb_info = batch_leg(True, False, 3, 1, median=True)
+    one_qps, one_rows, _, one_info = batch_leg(False, False, 3, 1, median=True)
 
     # The plain traversal: one query at a time, lower-bound ranking, scorer off.
     h.set_two_wave(True)
