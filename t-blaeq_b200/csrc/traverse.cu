@@ -1428,12 +1428,8 @@ constexpr int kNodeMajorChunk = 64;   // children whose float boxes a warp stage
 // time, so each box is read from memory once per 32 queries. Survivors are staged per warp in
 // shared memory and appended with one atomic per flush (at most kNodeMajorStage of them, and at
 // the end of the unit), not one per child.
-// Resident blocks per SM the register budget is sized for: 10 up to D = 8 (48 registers; shared
-// memory allows 10 at D = 8), 5 above (the staged boxes allow 5 at D = 16), 4 for any D.
-constexpr int nodeMajorMinBlocks(int D) { return D == 0 ? 4 : D <= 8 ? 10 : 5; }
-
 template <int D>
-__global__ void __launch_bounds__(kNodeMajorThreads, nodeMajorMinBlocks(D)) nodeMajorRangeKernel(NodeMajorArgs a) {
+__global__ void __launch_bounds__(kNodeMajorThreads) nodeMajorRangeKernel(NodeMajorArgs a) {
     constexpr uint32_t FULL = 0xffffffffu;
     constexpr int DM = D > 0 ? D : 32;
     __shared__ uint32_t sQ[kNodeMajorThreads / 32][kNodeMajorStage];
