@@ -175,3 +175,15 @@ def test_tuning_cache_round_trip(tb, tmp_path):
     assert open(path).read().splitlines()[0] == "tblaeq-tuning-cache 1"
     with pytest.raises(tb.TblaeqError):
         tb.tuning_store(path, "bad\tkey", [0], [100])
+
+
+def test_launch_counts_need_no_gpu(tb):
+    """The launch counter is a process-wide count, readable before any device work; the graph's
+    kernel count needs a prepared handle and rejects a null one before touching the device."""
+    n = tb.kernel_launches()
+    assert isinstance(n, int) and n >= 0
+    assert tb.kernel_launches() == n  # nothing launched in between
+    lib = tb.lib()
+    k, nodes = ctypes.c_uint64(7), ctypes.c_uint64(7)
+    assert tb.ERR_NAMES[lib.tblaeq_graph_launches(None, ctypes.byref(k), ctypes.byref(nodes))] == "INVALID"
+    assert (k.value, nodes.value) == (7, 7)
